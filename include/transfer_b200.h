@@ -1,0 +1,323 @@
+/*
+ * transfer_b200.h -- C ABI of the B200-native radiative-transfer hot path.
+ *
+ * The path: the matrix-free even-parity spherical-harmonics Galerkin operator
+ * on a P1 tetrahedral mesh (reference kernels.cu: volumePart/surfacePart and
+ * their Diag variants, rightHandSide, the BLAS-1 and reduction kernels), the
+ * Conjugate Gradient solve that drives it (main.cpp:125-160, invprec at
+ * main.cpp:223-248), the Lanczos estimate of lambda_max (Eigenvalue.cpp:5-83)
+ * and the reduction of the solution to energy density U, radiation pressure
+ * tensor T and flux W (MeshData.cpp:96-136).
+ *
+ * Every entry point below replaces one member of the reference's
+ * `struct CudaContext` (CudaContext.h:9-50) or one host routine it is used
+ * with; each declaration cites the reference symbol it stands in for.
+ *
+ * Conventions
+ *  - All functions return a tr_status; TR_OK == 0.  tr_last_error() gives a
+ *    human-readable message for the last failure on a context (or globally,
+ *    for failures before a context exists).
+ *  - Vectors are DEVICE pointers laid out like the reference's:
+ *    f[vertex][lm] at f[vertex*aslm + lm], aslm = slm rounded up to 8 doubles
+ *    (64 bytes; common.cuh:5-6 with REAL=double) for the FP64 entry points and
+ *    to 16 floats for the *_f32 ones.  Padding entries are written as zero.
+ *  - Every call runs on the context's stream (tr_ctx_set_stream) and has
+ *    completed when the call returns (as the reference's synchronous
+ *    driver-API calls had), unless the name ends in _async.
+ *  - No entry point falls back to a CPU implementation: without a usable
+ *    CUDA device tr_ctx_create returns TR_ERR_NO_DEVICE.
+ */
+#ifndef TRANSFER_B200_H
+#define TRANSFER_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TR_ABI_VERSION 1
+
+/* Vertex / element index type (util.h:6 `typedef uint32_t idx`). */
+typedef uint32_t tr_idx;
+
+/* Maximum padded angular size (common.cuh:7 ASLM_MAX = 128, so maxk <= 7). */
+#define TR_ASLM_MAX 128
+#define TR_MAXK_MAX 7
+
+/* Element record, byte-compatible with the reference's `tetrahedron`
+ * built with REAL=double (tetrahedron.h:7-20, 128 bytes):
+ *   p[4]          vertex indices
+ *   kappa_volume  kappa(region) * volume            (MeshData.cpp:63)
+ *   I_p           Planck intensity of the region      (MeshData.cpp:64)
+ *   s[j][0..2]    area-weighted normal of the face opposite local vertex j;
+ *                 sum_j s[j] = 0 (MeshData.cpp:65-76). */
+typedef struct tr_tetrahedron {
+    tr_idx p[4];
+    double kappa_volume;
+    double I_p;
+    double s[4][3];
+} tr_tetrahedron;
+
+/* Boundary face record, byte-compatible with the reference's `face`
+ * with REAL=double (face.h:8-18, 64 bytes).  p[3] is padding. */
+typedef struct tr_face {
+    tr_idx p[4];
+    double s[3];
+    double _pad[3];
+} tr_face;
+
+/* Host view of the reference's MeshData (MeshData.h:13-32).  All arrays are
+ * HOST pointers owned by the caller; tr_ctx_create copies them. */
+typedef struct tr_mesh_view {
+    tr_idx nP, nF, nT;
+    const tr_idx *tetstart;          /* [nP+1]  vertex -> incident tets (CSR) */
+    const tr_idx *tetidx;            /* [tetstart[nP]] */
+    const tr_idx *tetpos;            /* [tetstart[nP]] local vertex 0..3 */
+    const tr_tetrahedron *mesh;      /* [nT] */
+    const tr_idx *facestart;         /* [nP+1]  vertex -> boundary faces */
+    const tr_idx *faceidx;           /* [facestart[nP]] */
+    const tr_idx *facepos;           /* [facestart[nP]] local vertex 0..2 */
+    const tr_face *bnd;              /* [nF] */
+} tr_mesh_view;
+
+/* Host view of the reference's AngularData (AngularData.h:8-18): UNPADDED
+ * tables with stride slm, omega[i][lm1][lm2] at omega[i*slm*slm+lm1*slm+lm2],
+ * omega_pos likewise (0..2), O_x/O_y/O_z [slm][slm]. */
+typedef struct tr_angular_view {
+    tr_idx slm;
+    const double *omega;
+    const tr_idx *omega_pos;
+    const double *Ox, *Oy, *Oz;
+} tr_angular_view;
+
+/* Physics beyond the reference (all optional; a NULL view or NULL member
+ * reproduces the reference exactly: absorption + emission, vacuum).
+ *  kappa_abs_volume[nT]  coefficient of the l=0 mass term (sigma_a * V) for
+ *                        isotropic scattering; NULL -> kappa_volume.
+ *  face_bc[nF]           TR_BC_VACUUM (reference), TR_BC_REFLECTIVE or
+ *                        TR_BC_INCIDENT (vacuum + isotropic inflow).
+ *  face_incident[nF]     isotropic incoming intensity for TR_BC_INCIDENT.
+ *  surface_mode          TR_SURFACE_AXIS (reference: dominant-axis |Omega.n|,
+ *                        kernels.cu:419-425) or TR_SURFACE_EXACT. */
+enum { TR_BC_VACUUM = 0, TR_BC_REFLECTIVE = 1, TR_BC_INCIDENT = 2 };
+enum { TR_SURFACE_AXIS = 0, TR_SURFACE_EXACT = 1 };
+typedef struct tr_physics_view {
+    const double *kappa_abs_volume;
+    const int32_t *face_bc;
+    const double *face_incident;
+    int32_t surface_mode;
+} tr_physics_view;
+
+typedef enum tr_status {
+    TR_OK = 0,
+    TR_ERR_INVALID_ARG = 1,
+    TR_ERR_CUDA = 2,
+    TR_ERR_NOT_CONVERGED = 3,
+    TR_ERR_NAN = 4,
+    TR_ERR_NO_DEVICE = 5,
+    TR_ERR_MESH = 6,
+    TR_ERR_CONFIG = 7,
+    TR_ERR_OUT_OF_MEMORY = 8,
+    TR_ERR_UNSUPPORTED = 9,
+    TR_ERR_IO = 10
+} tr_status;
+
+typedef struct tr_ctx tr_ctx;
+
+typedef struct tr_ctx_info {
+    tr_idx nP, nT, nF;
+    tr_idx slm;
+    tr_idx aslm;          /* FP64 vector padding (8 doubles)  */
+    tr_idx aslm_f32;      /* FP32 vector padding (16 floats)  */
+    uint64_t n_edges;     /* assembled vertex-vertex couplings */
+    uint64_t n_bnd_edges; /* boundary couplings                */
+    uint64_t device_bytes;/* device memory held by the context */
+    int device;
+} tr_ctx_info;
+
+/* ---- context (CudaContext::CudaContext / ~CudaContext, CudaContext.cpp:24-58) */
+tr_status tr_ctx_create(int device, const tr_mesh_view *mesh,
+                        const tr_angular_view *ang, tr_ctx **out);
+tr_status tr_ctx_create_ex(int device, const tr_mesh_view *mesh,
+                           const tr_angular_view *ang,
+                           const tr_physics_view *phys, tr_ctx **out);
+tr_status tr_ctx_destroy(tr_ctx *ctx);
+tr_status tr_ctx_info_get(const tr_ctx *ctx, tr_ctx_info *info);
+/* cudaStream_t passed as void*; NULL selects the context's own stream. */
+tr_status tr_ctx_set_stream(tr_ctx *ctx, void *stream);
+const char *tr_last_error(const tr_ctx *ctx);
+const char *tr_status_string(tr_status st);
+int tr_abi_version(void);
+
+/* ---- operator (CudaContext::computeLhs/computeLhsDiag/computeRhs,
+ *      CudaContext.cpp:99-130; kernels.cu:135-493) ------------------------ */
+/* Af = A f : volumePart (kernels.cu:200-287) + surfacePart (:383-438). */
+tr_status tr_compute_lhs(tr_ctx *ctx, const double *f, double *Af);
+/* Af = D f : volumePartDiag (:290-357) + surfacePartDiag (:440-493). */
+tr_status tr_compute_lhs_diag(tr_ctx *ctx, const double *f, double *Af);
+/* b = (e_i, kappa I_p) : rightHandSide (:135-165), plus inflow terms. */
+tr_status tr_compute_rhs(tr_ctx *ctx, double *b);
+
+/* ---- BLAS-1 over all nP*aslm entries (kernels.cu:12-50,
+ *      CudaContext.cpp:137-173) ------------------------------------------ */
+tr_status tr_scale(tr_ctx *ctx, double *x, double wx);                  /* x *= wx */
+tr_status tr_add_prod(tr_ctx *ctx, double *x, const double *y, double wy); /* x += wy*y */
+tr_status tr_mul_add(tr_ctx *ctx, double *x, double wx, const double *y);  /* x = wx*x+y */
+tr_status tr_mul_add_prod(tr_ctx *ctx, double *x, double wx,
+                          const double *y, double wy);                  /* x = wx*x+wy*y */
+/* Reductions over vertices and lm < slm (normKern/dotKern, kernels.cu:55-115;
+ * CudaContext::norm/dot, CudaContext.cpp:175-198).  Deterministic order. */
+tr_status tr_norm(tr_ctx *ctx, const double *x, double *out);
+tr_status tr_dot(tr_ctx *ctx, const double *x, const double *y, double *out);
+
+/* FP32 variants (the reference's default REAL=float build): vectors with
+ * aslm_f32 padding, operator tables rounded to float once at creation. */
+tr_status tr_compute_lhs_f32(tr_ctx *ctx, const float *f, float *Af);
+tr_status tr_compute_lhs_diag_f32(tr_ctx *ctx, const float *f, float *Af);
+tr_status tr_compute_rhs_f32(tr_ctx *ctx, float *b);
+tr_status tr_dot_f32(tr_ctx *ctx, const float *x, const float *y, double *out);
+
+/* ---- solver (main.cpp:125-160 CG; main.cpp:223-248 invprec) ------------ */
+enum {
+    TR_PREC_NONE = 0,        /* z = r                                       */
+    TR_PREC_REFERENCE = 1,   /* invprec: inner CG on computeLhsDiag to 1e-8 */
+    TR_PREC_JACOBI = 2       /* z = diag(A)^-1 r                            */
+};
+enum {
+    TR_MODE_FP64 = 0,        /* plain FP64 CG (the drop-in)                 */
+    TR_MODE_MIXED = 1        /* FP32 CG inside FP64 defect correction       */
+};
+typedef struct tr_solve_opts {
+    int32_t mode;            /* TR_MODE_*                                   */
+    int32_t precondition;    /* TR_PREC_*                                   */
+    int32_t max_iter;        /* outer CG iterations (reference: 1000)       */
+    int32_t relative;        /* 0: stop when ||r|| < tol (reference),
+                                1: stop when ||r||/||b|| < tol              */
+    double  tol;             /* reference: 1e-4 absolute                    */
+    double  inner_tol;       /* invprec tolerance (reference 1e-8, absolute);
+                                mixed mode: relative reduction per inner
+                                FP32 solve (0 -> 1e-4)                      */
+    int32_t inner_max_iter;  /* invprec / FP32 inner cap (0 -> 1000)       */
+    int32_t max_outer;       /* mixed mode: defect-correction steps (0->30) */
+    int32_t use_graph;       /* 1: replay captured CUDA graphs (default)    */
+    int32_t history_len;     /* capacity of history[] (may be 0)            */
+    double *history;         /* host array: ||r|| after each CG iteration   */
+} tr_solve_opts;
+
+typedef struct tr_solve_report {
+    int32_t converged;
+    int32_t iterations;          /* outer CG iterations (FP64 mode) or total
+                                    FP32 CG iterations (mixed mode)         */
+    int32_t inner_iterations;    /* invprec iterations summed (main.cpp:247) */
+    int32_t outer_steps;         /* mixed mode defect-correction steps       */
+    int64_t lhs_applications_f64;/* operator applications, FP64              */
+    int64_t lhs_applications_f32;/* operator applications, FP32              */
+    int64_t diag_applications;   /* preconditioner operator applications     */
+    double  initial_residual;    /* ||b - A f0||_2, FP64                      */
+    double  final_residual;      /* ||b - A f||_2 recomputed in FP64          */
+    double  rhs_norm;            /* ||b||_2                                   */
+    double  device_ms;           /* device time of the solve (CUDA events)    */
+} tr_solve_report;
+
+void tr_solve_opts_default(tr_solve_opts *opts);   /* reference settings */
+
+/* Solve A f = b from f = 0.  b: device vector, or NULL to use computeRhs.
+ * f: device vector (output). */
+tr_status tr_solve(tr_ctx *ctx, const tr_solve_opts *opts, const double *b,
+                   double *f, tr_solve_report *report);
+/* Same with HOST buffers: copies b in (pinned staging) and f out. */
+tr_status tr_solve_host(tr_ctx *ctx, const tr_solve_opts *opts,
+                        const double *b_host, double *f_host,
+                        tr_solve_report *report);
+
+/* ---- post-processing (MeshData::ComputeMoments / ComputeFlux,
+ *      MeshData.cpp:96-136), on the device ----------------------------- */
+/* U[nP] = 4 pi I_00 ; T[3][3][nP] = 4 pi sum_lm omega_i[lm][0] I_lm. */
+tr_status tr_compute_moments(tr_ctx *ctx, const double *f, double *U, double *T);
+/* W[3][nT] = (1/3) sum_k sum_a s_k,a T_aj(p_k) / kappa_volume. */
+tr_status tr_compute_flux(tr_ctx *ctx, const double *T, double *W);
+
+/* ---- Lanczos lambda_max estimate (eigest/trieig, Eigenvalue.cpp:5-83) -- */
+/* v: device vector, overwritten; w, v0: device work vectors.  Up to
+ * max_steps (reference: 30) steps, stop when |dl| < 1e-6 lmax. */
+tr_status tr_eig_lanczos(tr_ctx *ctx, double *v, double *v0, double *w,
+                         int max_steps, double *lmax, double *extrapolated,
+                         int *steps);
+/* Largest eigenvalue of the symmetric tridiagonal (a[0..n-1], b[1..n-1] as
+ * b[0..n-2]) by Newton on the characteristic polynomial (trieig). */
+double tr_trieig(const double *a, const double *b, int n);
+
+/* ---- host problem data (C++ host code behind the C ABI) ---------------- */
+/* AngularData(maxk) (AngularData.cpp:9-67): tables for the even harmonics
+ * l = 0,2,..,2maxk; slm = (1+maxk)(1+2maxk). */
+typedef struct tr_angular tr_angular;
+tr_status tr_angular_create(int maxk, tr_angular **out);
+tr_status tr_angular_view_get(const tr_angular *a, tr_angular_view *view);
+void      tr_angular_destroy(tr_angular *a);
+
+/* Spherical::value(l, m, x, y, z) (Spherical.cpp:62-82): real harmonic,
+ * orthonormal on average over the sphere, no Condon-Shortley phase. */
+double tr_spherical_value(int l, int m, double x, double y, double z);
+/* HemiQuad(mindegree) (HemiQuad.cpp:265-286) / LebedevQuad(mindegree)
+ * (LebedevQuad.cpp:6269-6277): returns the rule's number of points and, if
+ * cap >= that number, fills x, y, z, w (weights sum to 1).  Returns -1 for
+ * an unsupported degree. */
+int tr_hemiquad(int mindegree, double *x, double *y, double *z, double *w, int cap);
+int tr_lebedev(int mindegree, double *x, double *y, double *z, double *w, int cap);
+
+/* Config(const char*) (Config.cpp:8-131): the radiation.cfg grammar. */
+typedef struct tr_config tr_config;
+tr_status tr_config_load(const char *path, tr_config **out);
+void      tr_config_destroy(tr_config *c);
+int       tr_config_get_int(const tr_config *c, const char *key, int *ok);
+double    tr_config_get_double(const tr_config *c, const char *key, int *ok);
+const char *tr_config_get_string(const tr_config *c, const char *key);
+int       tr_config_num_regions(const tr_config *c);
+double    tr_config_region_double(const tr_config *c, int region,
+                                  const char *key, int *ok);
+
+/* MeshData (MeshData.cpp:9-94) built from a tetrahedral mesh given by
+ * vertex coordinates and connectivity, or generated (Kuhn-split box). */
+typedef struct tr_meshdata tr_meshdata;
+typedef struct tr_region_params {
+    int32_t nreg;              /* regions are numbered 1..nreg            */
+    const double *kappa;       /* [nreg+1], index 0 unused (Config.cpp)    */
+    const double *Ip;          /* [nreg+1]                                 */
+    const double *albedo;      /* [nreg+1] or NULL (no scattering)         */
+} tr_region_params;
+tr_status tr_meshdata_from_tets(tr_idx nP, const double *xyz, tr_idx nT,
+                                const tr_idx *tets, const int32_t *region,
+                                const tr_region_params *rp, tr_meshdata **out);
+/* Kuhn box: n[3] cells, box = {x0,x1,y0,y1,z0,z1}, interior vertices jittered
+ * uniformly by +-jitter*h (splitmix64 seeded); region_kind selects the
+ * region map: 0 all region 1; 1 sphere (centre cx,cy,cz radius r -> region 1,
+ * else 2); 2 half space x < x_split -> region 1, else 2. */
+typedef struct tr_kuhn_params {
+    int32_t n[3];
+    double box[6];
+    double jitter;
+    uint64_t seed;
+    int32_t region_kind;
+    double region_arg[4];
+    int32_t ball;              /* 1: keep only tets with centroid |c-c0|<=R */
+    double ball_center[3];
+    double ball_radius;
+} tr_kuhn_params;
+tr_status tr_meshdata_kuhn(const tr_kuhn_params *kp, const tr_region_params *rp,
+                           tr_meshdata **out);
+tr_status tr_meshdata_view_get(const tr_meshdata *md, tr_mesh_view *view);
+/* Vertex coordinates [nP][3] and region id per tet [nT]. */
+const double  *tr_meshdata_coords(const tr_meshdata *md);
+const int32_t *tr_meshdata_regions(const tr_meshdata *md);
+/* Per-tet sigma_a*V (NULL when no region scatters) and per-face box side
+ * (0..5 for x0,x1,y0,y1,z0,z1; -1 otherwise). */
+const double  *tr_meshdata_kappa_abs_volume(const tr_meshdata *md);
+const int32_t *tr_meshdata_face_side(const tr_meshdata *md);
+void tr_meshdata_destroy(tr_meshdata *md);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TRANSFER_B200_H */

@@ -1,0 +1,14 @@
+"""B200-native radiative-transfer hot path of uranix/Transfer.
+
+The even-parity spherical-harmonics Galerkin operator on P1 tetrahedral
+meshes, its CG / defect-correction solves and the moment reduction, as CUDA
+kernels for sm_100a behind a C ABI (include/transfer_b200.h).  This package
+is the Python binding of that library; it has no CPU fallback.
+"""
+from ._lib import (TR_BC_INCIDENT, TR_BC_REFLECTIVE, TR_BC_VACUUM, TR_MODE_FP64, TR_MODE_MIXED,  # noqa: F401
+                   TR_PREC_JACOBI, TR_PREC_NONE, TR_PREC_REFERENCE, LIB_PATH, TransferError, check, lib)
+from .core import (FACE_DTYPE, TET_DTYPE, AngularData, Config, CudaContext, MeshData, Physics,  # noqa: F401
+                   solve_options, trieig)
+
+__all__ = ["AngularData", "Config", "CudaContext", "MeshData", "Physics", "TransferError", "solve_options",
+           "trieig", "lib", "LIB_PATH"]

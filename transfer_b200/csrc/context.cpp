@@ -1,0 +1,421 @@
+// tr_ctx creation (CudaContext::CudaContext + DeviceMeshData +
+// DeviceAngularData, CudaContext.cpp:24-50, DeviceMeshData.cpp:8-52,
+// DeviceAngularData.cpp:7-67): validates the reference's MeshData /
+// AngularData arrays, assembles the vertex-pair operator described in
+// internal.h on the host, and uploads it in FP64 and FP32.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+#include "solver.h"
+
+namespace transfer {
+
+namespace {
+
+struct Edge {
+    uint32_t u;
+    double c[kCoefStride];
+};
+struct BEdge {
+    uint32_t u;
+    double e[kBCoefStride];
+};
+
+// reference axis choice for a boundary face (kernels.cu:419-425)
+inline int face_axis(const tr_face &f, double *surf) {
+    double s = std::fabs(f.s[0] + f.s[1] + f.s[2]);
+    *surf = s;
+    if (2 * std::fabs(f.s[0]) > s) return 0;
+    if (2 * std::fabs(f.s[1]) > s) return 1;
+    return 2;
+}
+
+std::string validate(const tr_mesh_view *m, const tr_angular_view *a) {
+    if (!m || !a) return "null mesh or angular view";
+    if (m->nP == 0 || m->nT == 0) return "empty mesh";
+    if (!m->tetstart || !m->tetidx || !m->tetpos || !m->mesh) return "null tet arrays";
+    if (m->nF && (!m->bnd)) return "null boundary face array";
+    if (!m->facestart || !m->faceidx || !m->facepos) return "null boundary CSR arrays";
+    if (!a->omega || !a->omega_pos || !a->Ox || !a->Oy || !a->Oz) return "null angular tables";
+    bool slm_ok = false;
+    for (int k = 0; k <= TR_MAXK_MAX; ++k)
+        if (a->slm == static_cast<tr_idx>((1 + k) * (1 + 2 * k))) slm_ok = true;
+    if (!slm_ok) return "slm is not (1+maxk)(1+2maxk) for maxk <= 7";
+    if (static_cast<uint64_t>(m->nP) * 128 > 0xFFFFFFFFULL * 8ULL) return "mesh too large";
+    if (m->tetstart[0] != 0) return "tetstart[0] != 0";
+    for (tr_idx v = 0; v < m->nP; ++v)
+        if (m->tetstart[v + 1] < m->tetstart[v]) return "tetstart not monotonic";
+    for (tr_idx j = 0; j < m->tetstart[m->nP]; ++j) {
+        if (m->tetidx[j] >= m->nT) return "tetidx out of range";
+        if (m->tetpos[j] > 3) return "tetpos out of range";
+    }
+    for (tr_idx t = 0; t < m->nT; ++t) {
+        const tr_tetrahedron &T = m->mesh[t];
+        for (int k = 0; k < 4; ++k)
+            if (T.p[k] >= m->nP) return "tetrahedron vertex out of range";
+        if (!(T.kappa_volume > 0.0) || !std::isfinite(T.kappa_volume)) return "kappa_volume must be positive";
+        for (int k = 0; k < 4; ++k)
+            for (int d = 0; d < 3; ++d)
+                if (!std::isfinite(T.s[k][d])) return "non-finite face normal";
+    }
+    for (tr_idx v = 0; v < m->nP; ++v)
+        for (tr_idx j = m->tetstart[v]; j < m->tetstart[v + 1]; ++j)
+            if (m->mesh[m->tetidx[j]].p[m->tetpos[j]] != v) return "tetidx/tetpos inconsistent with tet vertices";
+    if (m->facestart[0] != 0) return "facestart[0] != 0";
+    for (tr_idx v = 0; v < m->nP; ++v)
+        if (m->facestart[v + 1] < m->facestart[v]) return "facestart not monotonic";
+    for (tr_idx j = 0; j < m->facestart[m->nP]; ++j) {
+        if (m->faceidx[j] >= m->nF) return "faceidx out of range";
+        if (m->facepos[j] > 2) return "facepos out of range";
+    }
+    for (tr_idx f = 0; f < m->nF; ++f)
+        for (int k = 0; k < 3; ++k)
+            if (m->bnd[f].p[k] >= m->nP) return "face vertex out of range";
+    const size_t n3 = 3ULL * a->slm * a->slm;
+    for (size_t i = 0; i < n3; ++i)
+        if (a->omega_pos[i] > 2) return "omega_pos out of range";
+    return "";
+}
+
+template <typename T>
+cudaError_t upload(tr_ctx *c, T **dst, const void *src, size_t bytes) {
+    if (bytes == 0) bytes = sizeof(T);
+    cudaError_t e = cudaMalloc(reinterpret_cast<void **>(dst), bytes);
+    if (e != cudaSuccess) return e;
+    c->allocations.push_back(*dst);
+    c->device_bytes += bytes;
+    if (src) return cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice);
+    return cudaMemset(*dst, 0, bytes);
+}
+
+template <typename T>
+std::vector<T> to_type(const std::vector<double> &v) {
+    std::vector<T> o(v.size());
+    for (size_t i = 0; i < v.size(); ++i) o[i] = static_cast<T>(v[i]);
+    return o;
+}
+
+}  // namespace
+
+cudaError_t operator_init_attributes();
+
+void ctx_free(tr_ctx *c) {
+    if (!c) return;
+    for (auto &g : c->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    for (void *p : c->allocations) cudaFree(p);
+    if (c->host_pinned) cudaFreeHost(c->host_pinned);
+    if (c->stage_in) cudaFreeHost(c->stage_in);
+    if (c->stage_out) cudaFreeHost(c->stage_out);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+}
+
+tr_status ctx_create(int device, const tr_mesh_view *m, const tr_angular_view *a, const tr_physics_view *ph,
+                     tr_ctx **out, std::string &err) {
+    err = validate(m, a);
+    if (!err.empty()) return TR_ERR_MESH;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        err = "no CUDA device available (this library has no CPU fallback)";
+        return TR_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= ndev) {
+        err = "device index out of range";
+        return TR_ERR_INVALID_ARG;
+    }
+    if (cudaSetDevice(device) != cudaSuccess) {
+        err = "cudaSetDevice failed";
+        return TR_ERR_NO_DEVICE;
+    }
+    const tr_idx nP = m->nP, nT = m->nT, nF = m->nF, slm = a->slm;
+    const int32_t *bc = ph ? ph->face_bc : nullptr;
+    const double *finc = ph ? ph->face_incident : nullptr;
+    const double *kva = ph ? ph->kappa_abs_volume : nullptr;
+    if (ph && ph->surface_mode != TR_SURFACE_AXIS) {
+        err = "surface_mode other than TR_SURFACE_AXIS is not supported";
+        return TR_ERR_UNSUPPORTED;
+    }
+    if (bc)
+        for (tr_idx f = 0; f < nF; ++f)
+            if (bc[f] < 0 || bc[f] > 2) {
+                err = "face_bc value out of range";
+                return TR_ERR_INVALID_ARG;
+            }
+    if (bc)
+        for (tr_idx f = 0; f < nF; ++f)
+            if (bc[f] == TR_BC_INCIDENT && !finc) {
+                err = "TR_BC_INCIDENT faces need face_incident";
+                return TR_ERR_INVALID_ARG;
+            }
+    if (bc)
+        for (tr_idx f = 0; f < nF; ++f)
+            if (bc[f] == TR_BC_REFLECTIVE) {
+                err = "TR_BC_REFLECTIVE is not supported by this build";
+                return TR_ERR_UNSUPPORTED;
+            }
+
+    tr_ctx *c = new tr_ctx();
+    c->device = device;
+    c->nP = nP;
+    c->nT = nT;
+    c->nF = nF;
+    c->slm = slm;
+    c->aslm = (slm + 7) & ~7u;
+    c->aslm32 = (slm + 15) & ~15u;
+    auto bail = [&](const std::string &msg, tr_status st) {
+        err = msg;
+        ctx_free(c);
+        return st;
+    };
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return bail("cudaGetDeviceProperties failed", TR_ERR_CUDA);
+    c->num_sms = prop.multiProcessorCount;
+
+    // ---------------------------------------------------- assembled operator
+    std::vector<uint32_t> row(nP + 1, 0), brow(nP + 1, 0);
+    std::vector<std::vector<Edge>> edges(nP);
+    std::vector<std::vector<BEdge>> bedges(nP);
+    std::vector<double> inflow;
+    bool any_inflow = false;
+    if (bc)
+        for (tr_idx f = 0; f < nF; ++f)
+            if (bc[f] == TR_BC_INCIDENT) any_inflow = true;
+    if (any_inflow) inflow.assign(3ULL * nP, 0.0);
+#pragma omp parallel for schedule(dynamic, 256)
+    for (long vv = 0; vv < static_cast<long>(nP); ++vv) {
+        const tr_idx v = static_cast<tr_idx>(vv);
+        std::vector<Edge> &E = edges[v];
+        auto find = [&](uint32_t u) -> Edge & {
+            for (Edge &e : E)
+                if (e.u == u) return e;
+            Edge ne;
+            ne.u = u;
+            std::memset(ne.c, 0, sizeof(ne.c));
+            E.push_back(ne);
+            return E.back();
+        };
+        for (tr_idx j = m->tetstart[v]; j < m->tetstart[v + 1]; ++j) {
+            const tr_idx t = m->tetidx[j], loc = m->tetpos[j];
+            const tr_tetrahedron &T = m->mesh[t];
+            const double kv = T.kappa_volume, ka = kva ? kva[t] : kv;
+            for (int k = 0; k < 4; ++k) {
+                Edge &e = find(T.p[k]);
+                for (int i = 0; i < 3; ++i)
+                    for (int jj = 0; jj < 3; ++jj) e.c[3 * i + jj] += T.s[loc][i] / kv * (1.0 / 9.0) * T.s[k][jj];
+                const double mult = (k == static_cast<int>(loc)) ? 2.0 : 1.0;
+                e.c[9] += kv * mult * (1.0 / 20.0);
+                e.c[10] += ka * mult * (1.0 / 20.0);
+            }
+        }
+        std::sort(E.begin(), E.end(), [](const Edge &x, const Edge &y) { return x.u < y.u; });
+        std::vector<BEdge> &B = bedges[v];
+        for (tr_idx j = m->facestart[v]; j < m->facestart[v + 1]; ++j) {
+            const tr_idx fi = m->faceidx[j], loc = m->facepos[j];
+            const int kind = bc ? bc[fi] : TR_BC_VACUUM;
+            if (kind == TR_BC_REFLECTIVE) continue;
+            const tr_face &F = m->bnd[fi];
+            double surf;
+            const int ax = face_axis(F, &surf);
+            if (kind == TR_BC_INCIDENT) inflow[3ULL * v + ax] += finc[fi] * surf * (1.0 / 3.0);
+            for (int k = 0; k < 3; ++k) {
+                BEdge *e = nullptr;
+                for (BEdge &b : B)
+                    if (b.u == F.p[k]) e = &b;
+                if (!e) {
+                    BEdge nb;
+                    nb.u = F.p[k];
+                    std::memset(nb.e, 0, sizeof(nb.e));
+                    B.push_back(nb);
+                    e = &B.back();
+                }
+                e->e[ax] += surf * ((k == static_cast<int>(loc)) ? 2.0 : 1.0) * (1.0 / 12.0);
+            }
+        }
+        std::sort(B.begin(), B.end(), [](const BEdge &x, const BEdge &y) { return x.u < y.u; });
+    }
+    for (tr_idx v = 0; v < nP; ++v) {
+        row[v + 1] = row[v] + static_cast<uint32_t>(edges[v].size());
+        brow[v + 1] = brow[v] + static_cast<uint32_t>(bedges[v].size());
+    }
+    const size_t nnz = row[nP], nbnz = brow[nP];
+    c->n_edges = nnz;
+    c->n_bnd_edges = nbnz;
+    std::vector<uint32_t> col(nnz), bcol(std::max<size_t>(nbnz, 1));
+    std::vector<double> coef(nnz * kCoefStride), bcoef(std::max<size_t>(nbnz, 1) * kBCoefStride, 0.0);
+    for (tr_idx v = 0; v < nP; ++v) {
+        size_t o = row[v];
+        for (const Edge &e : edges[v]) {
+            col[o] = e.u;
+            std::memcpy(&coef[o * kCoefStride], e.c, sizeof(e.c));
+            ++o;
+        }
+        o = brow[v];
+        for (const BEdge &e : bedges[v]) {
+            bcol[o] = e.u;
+            std::memcpy(&bcoef[o * kBCoefStride], e.e, sizeof(e.e));
+            ++o;
+        }
+    }
+
+    // ---------------------------------------------------- angular tables
+    const size_t ss = static_cast<size_t>(slm) * slm;
+    double maxabs = 0.0;
+    for (size_t i = 0; i < 3 * ss; ++i) maxabs = std::max(maxabs, std::fabs(a->omega[i]));
+    const double drop = 1e-14 * maxabs;
+    std::vector<uint32_t> ang_start(slm + 1, 0);
+    std::vector<uint16_t> ang_src;
+    std::vector<double> ang_w;
+    for (tr_idx lm = 0; lm < slm; ++lm) {
+        for (int i = 0; i < 3; ++i)
+            for (tr_idx lms = 0; lms < slm; ++lms) {
+                // kernels.cu:276-282 reads omega[i][lms][lm] and omega_pos[i][lms][lm]
+                const size_t q = (static_cast<size_t>(i) * slm + lms) * slm + lm;
+                const double w = a->omega[q];
+                if (std::fabs(w) <= drop) continue;
+                ang_src.push_back(static_cast<uint16_t>(((3 * i + a->omega_pos[q]) << 8) | lms));
+                ang_w.push_back(w);
+            }
+        ang_start[lm + 1] = static_cast<uint32_t>(ang_w.size());
+    }
+    std::vector<double> O(3 * ss), ang_diag(3 * slm), O_diag(3 * slm);
+    const double *On[3] = {a->Ox, a->Oy, a->Oz};
+    for (int n = 0; n < 3; ++n) {
+        std::memcpy(&O[n * ss], On[n], ss * sizeof(double));
+        for (tr_idx lm = 0; lm < slm; ++lm) {
+            ang_diag[n * slm + lm] = a->omega[(static_cast<size_t>(n) * slm + lm) * slm + lm];
+            O_diag[n * slm + lm] = On[n][static_cast<size_t>(lm) * slm + lm];
+        }
+    }
+    // Jacobi: 1 / diag(A)
+    std::vector<double> dinv(static_cast<size_t>(nP) * c->aslm, 0.0);
+    std::vector<float> dinv32(static_cast<size_t>(nP) * c->aslm32, 0.0f);
+    for (tr_idx v = 0; v < nP; ++v) {
+        const double *cv = nullptr;
+        for (uint32_t e = row[v]; e < row[v + 1]; ++e)
+            if (col[e] == v) cv = &coef[static_cast<size_t>(e) * kCoefStride];
+        const double *bv = nullptr;
+        for (uint32_t e = brow[v]; e < brow[v + 1]; ++e)
+            if (bcol[e] == v) bv = &bcoef[static_cast<size_t>(e) * kBCoefStride];
+        for (tr_idx lm = 0; lm < slm; ++lm) {
+            double d = 0.0;
+            if (cv) {
+                d += (lm == 0) ? cv[10] : cv[9];
+                for (int i = 0; i < 3; ++i) {
+                    const size_t q = (static_cast<size_t>(i) * slm + lm) * slm + lm;
+                    d += a->omega[q] * cv[3 * i + a->omega_pos[q]];
+                }
+            }
+            if (bv)
+                for (int n = 0; n < 3; ++n) d += O_diag[n * slm + lm] * bv[n];
+            const double inv = (d != 0.0) ? 1.0 / d : 0.0;
+            dinv[static_cast<size_t>(v) * c->aslm + lm] = inv;
+            dinv32[static_cast<size_t>(v) * c->aslm32 + lm] = static_cast<float>(inv);
+        }
+    }
+    // moments: omega_i[lm][0] and its j (MeshData.cpp:105-110)
+    std::vector<double> mom_w(3 * slm);
+    std::vector<uint32_t> mom_pos(3 * slm);
+    for (int i = 0; i < 3; ++i)
+        for (tr_idx lm = 0; lm < slm; ++lm) {
+            mom_w[i * slm + lm] = a->omega[(static_cast<size_t>(i) * slm + lm) * slm];
+            mom_pos[i * slm + lm] = a->omega_pos[(static_cast<size_t>(i) * slm + lm) * slm];
+        }
+    // per-tet data for the right-hand side and the flux
+    std::vector<uint32_t> tetp(4ULL * nT);
+    std::vector<double> tets(12ULL * nT), tetkv(nT), tetq(nT);
+    for (tr_idx t = 0; t < nT; ++t) {
+        const tr_tetrahedron &T = m->mesh[t];
+        for (int k = 0; k < 4; ++k) tetp[4ULL * t + k] = T.p[k];
+        for (int k = 0; k < 4; ++k)
+            for (int d = 0; d < 3; ++d) tets[12ULL * t + 3 * k + d] = T.s[k][d];
+        tetkv[t] = T.kappa_volume;
+        tetq[t] = T.kappa_volume * T.I_p;
+    }
+
+    // ---------------------------------------------------- upload
+    cudaError_t e = cudaSuccess;
+    auto ok = [&](cudaError_t x) {
+        if (e == cudaSuccess) e = x;
+        return e == cudaSuccess;
+    };
+    DeviceOp<double> &o64 = c->op64;
+    DeviceOp<float> &o32 = c->op32;
+    o64.aslm = c->aslm;
+    o32.aslm = c->aslm32;
+    ok(upload(c, &o64.row, row.data(), row.size() * 4));
+    ok(upload(c, &o64.col, col.data(), col.size() * 4));
+    ok(upload(c, &o64.brow, brow.data(), brow.size() * 4));
+    ok(upload(c, &o64.bcol, bcol.data(), bcol.size() * 4));
+    ok(upload(c, &o64.ang_start, ang_start.data(), ang_start.size() * 4));
+    ok(upload(c, &o64.ang_src, ang_src.data(), ang_src.size() * 2));
+    ok(upload(c, &o64.coef, coef.data(), coef.size() * 8));
+    ok(upload(c, &o64.bcoef, bcoef.data(), bcoef.size() * 8));
+    ok(upload(c, &o64.ang_w, ang_w.data(), ang_w.size() * 8));
+    ok(upload(c, &o64.O, O.data(), O.size() * 8));
+    ok(upload(c, &o64.ang_diag, ang_diag.data(), ang_diag.size() * 8));
+    ok(upload(c, &o64.O_diag, O_diag.data(), O_diag.size() * 8));
+    ok(upload(c, &o64.dinv, dinv.data(), dinv.size() * 8));
+    o32.row = o64.row;
+    o32.col = o64.col;
+    o32.brow = o64.brow;
+    o32.bcol = o64.bcol;
+    o32.ang_start = o64.ang_start;
+    o32.ang_src = o64.ang_src;
+    {
+        auto c32 = to_type<float>(coef);
+        ok(upload(c, &o32.coef, c32.data(), c32.size() * 4));
+        auto b32 = to_type<float>(bcoef);
+        ok(upload(c, &o32.bcoef, b32.data(), b32.size() * 4));
+        auto w32 = to_type<float>(ang_w);
+        ok(upload(c, &o32.ang_w, w32.data(), w32.size() * 4));
+        auto O32 = to_type<float>(O);
+        ok(upload(c, &o32.O, O32.data(), O32.size() * 4));
+        auto d32 = to_type<float>(ang_diag);
+        ok(upload(c, &o32.ang_diag, d32.data(), d32.size() * 4));
+        auto od32 = to_type<float>(O_diag);
+        ok(upload(c, &o32.O_diag, od32.data(), od32.size() * 4));
+        ok(upload(c, &o32.dinv, dinv32.data(), dinv32.size() * 4));
+    }
+    ok(upload(c, &c->vt_start, m->tetstart, (nP + 1) * 4ULL));
+    ok(upload(c, &c->vt_tet, m->tetidx, std::max<size_t>(m->tetstart[nP], 1) * 4ULL));
+    ok(upload(c, &c->tet_q, tetq.data(), tetq.size() * 8));
+    if (any_inflow) ok(upload(c, &c->inflow, inflow.data(), inflow.size() * 8));
+    ok(upload(c, &c->O64, O.data(), O.size() * 8));
+    ok(upload(c, reinterpret_cast<uint32_t **>(&c->tet_p), tetp.data(), tetp.size() * 4));
+    ok(upload(c, &c->tet_s, tets.data(), tets.size() * 8));
+    ok(upload(c, &c->tet_kv, tetkv.data(), tetkv.size() * 8));
+    ok(upload(c, &c->mom_w, mom_w.data(), mom_w.size() * 8));
+    ok(upload(c, &c->mom_pos, mom_pos.data(), mom_pos.size() * 4));
+    ok(upload(c, &c->partials, nullptr, 4 * 4096 * sizeof(double)));
+    ok(upload(c, &c->counters, nullptr, 16 * sizeof(unsigned int)));
+    ok(upload(c, &c->red_out, nullptr, 16 * sizeof(double)));
+    if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void **>(&c->host_pinned), 16 * sizeof(double));
+    if (e == cudaSuccess) e = cudaStreamCreate(&c->own_stream);
+    if (e == cudaSuccess) e = operator_init_attributes();
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return bail(std::string("device setup failed: ") + cudaGetErrorString(e),
+                    e == cudaErrorMemoryAllocation ? TR_ERR_OUT_OF_MEMORY : TR_ERR_CUDA);
+    }
+    // grids: whole waves of resident 256-thread blocks, capped by the work
+    const size_t n64 = static_cast<size_t>(nP) * c->aslm;
+    c->grid_vec = static_cast<int>(std::min<size_t>(static_cast<size_t>(c->num_sms) * 8, (n64 + kBlock - 1) / kBlock));
+    const uint32_t G = c->aslm <= 8 ? 8 : c->aslm <= 16 ? 16 : 32;
+    const size_t groups_per_block = kBlock / G;
+    c->grid_op = static_cast<int>(
+        std::min<size_t>(static_cast<size_t>(c->num_sms) * 8, (nP + groups_per_block - 1) / groups_per_block));
+    c->grid_vec = std::max(c->grid_vec, 1);
+    c->grid_op = std::max(c->grid_op, 1);
+    *out = c;
+    return TR_OK;
+}
+
+}  // namespace transfer

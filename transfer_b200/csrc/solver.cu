@@ -1,0 +1,405 @@
+// Solvers: the reference's CG (main.cpp:125-160) with its optional inner-CG
+// preconditioner invprec (main.cpp:223-248), a Jacobi variant, and the
+// FP32-in-FP64 defect-correction solve.
+//
+// All CG scalars live in device memory (CgScalars): each iteration is three
+// launches -- A p with <p, A p> and alpha fused, the x/r update with ||r||,
+// the stop test and beta fused, and the new direction -- none of which
+// returns to the host.  Iterations run in chunks; a chunk is captured once
+// as a CUDA graph and replayed, and the host reads one 8-byte status word
+// per chunk.  Kernels of a chunk that starts after convergence return
+// immediately, so the result is the same as with a per-iteration test.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+
+#include "internal.h"
+#include "solver.h"
+
+namespace transfer {
+
+template <typename T>
+cudaError_t launch_cg_start(const tr_ctx *c, uint32_t aslm, const T *b, T *f, T *r, T *z, T *p, const T *dinv,
+                            CgScalars *s, cudaStream_t st);
+template <typename T>
+cudaError_t launch_cg_update(const tr_ctx *c, uint32_t aslm, T *f, T *r, const T *p, const T *Ap, T *z,
+                             const T *dinv, CgScalars *s, double *hist, int hist_cap, int defer_beta,
+                             cudaStream_t st);
+template <typename T>
+cudaError_t launch_cg_direction(const tr_ctx *c, uint32_t aslm, T *p, const T *z, const CgScalars *s,
+                                cudaStream_t st);
+cudaError_t launch_residual(const tr_ctx *c, const double *b, const double *Ax, double *r, CgScalars *s,
+                            cudaStream_t st);
+cudaError_t launch_to_f32(const tr_ctx *c, const double *r64, float *r32, const CgScalars *s, cudaStream_t st);
+cudaError_t launch_correct(const tr_ctx *c, double *x, const float *d32, const CgScalars *s, cudaStream_t st);
+
+// alpha = nrz / *dot (invprec's inner CG, whose operator launch has no fused dot)
+__global__ void k_set_alpha(CgScalars *s, const double *dot) {
+    if (s->done) return;
+    s->alpha = s->nrz / *dot;
+}
+// nrz = (r, z) at the start of a preconditioned CG (main.cpp:141)
+__global__ void k_set_nrz(CgScalars *s, const double *dot) { s->nrz = *dot; }
+// beta = (z, r) / nrz ; nrz = (z, r)   (main.cpp:155-157)
+__global__ void k_set_beta(CgScalars *s, const double *dot) {
+    if (s->done) return;
+    s->beta = *dot / s->nrz;
+    s->nrz = *dot;
+}
+
+#define TRY(...)                                                    \
+    do {                                                            \
+        cudaError_t _e = (__VA_ARGS__);                             \
+        if (_e != cudaSuccess) return fail(c, _e, #__VA_ARGS__);    \
+    } while (0)
+
+static tr_status fail(tr_ctx *c, cudaError_t e, const char *what) {
+    c->last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return TR_ERR_CUDA;
+}
+
+static cudaStream_t stream_of(const tr_ctx *c) { return c->stream ? c->stream : c->own_stream; }
+
+tr_status ensure_workspace(tr_ctx *c, int hist_cap) {
+    const size_t n64 = static_cast<size_t>(c->nP) * c->aslm, n32 = static_cast<size_t>(c->nP) * c->aslm32;
+    auto alloc = [&](void **p, size_t bytes) -> bool {
+        if (*p) return true;
+        if (cudaMalloc(p, bytes) != cudaSuccess) return false;
+        cudaMemset(*p, 0, bytes);
+        c->allocations.push_back(*p);
+        c->device_bytes += bytes;
+        return true;
+    };
+    for (int i = 0; i < 6; ++i)
+        if (!alloc(reinterpret_cast<void **>(&c->w64[i]), n64 * sizeof(double))) {
+            c->last_error = "out of device memory (solver work vectors)";
+            return TR_ERR_OUT_OF_MEMORY;
+        }
+    for (int i = 0; i < 5; ++i)
+        if (!alloc(reinterpret_cast<void **>(&c->w32[i]), n32 * sizeof(float))) {
+            c->last_error = "out of device memory (solver work vectors)";
+            return TR_ERR_OUT_OF_MEMORY;
+        }
+    for (int i = 0; i < 2; ++i)
+        if (!alloc(reinterpret_cast<void **>(&c->io[i]), n64 * sizeof(double))) {
+            c->last_error = "out of device memory (solver work vectors)";
+            return TR_ERR_OUT_OF_MEMORY;
+        }
+    for (int i = 0; i < 3; ++i)
+        if (!alloc(reinterpret_cast<void **>(&c->inner[i]), n64 * sizeof(double))) {
+            c->last_error = "out of device memory (solver work vectors)";
+            return TR_ERR_OUT_OF_MEMORY;
+        }
+    if (!alloc(reinterpret_cast<void **>(&c->cg), 4 * sizeof(CgScalars))) {
+        c->last_error = "out of device memory";
+        return TR_ERR_OUT_OF_MEMORY;
+    }
+    if (hist_cap > c->hist_cap) {
+        if (c->dhist) {
+            cudaFree(c->dhist);
+            c->allocations.erase(std::find(c->allocations.begin(), c->allocations.end(), (void *)c->dhist));
+            c->dhist = nullptr;
+        }
+        int cap = std::max(hist_cap, 1024);
+        if (!alloc(reinterpret_cast<void **>(&c->dhist), cap * sizeof(double))) {
+            c->last_error = "out of device memory";
+            return TR_ERR_OUT_OF_MEMORY;
+        }
+        c->hist_cap = cap;
+        for (auto &g : c->graphs) g.valid = false;  // history pointer changed
+    }
+    return TR_OK;
+}
+
+static tr_status init_scalars(tr_ctx *c, CgScalars *s, double tol, int maxit, cudaStream_t st) {
+    CgScalars h;
+    std::memset(&h, 0, sizeof(h));
+    h.tol = tol;
+    h.maxit = maxit;
+    TRY(cudaMemcpyAsync(s, &h, sizeof(h), cudaMemcpyHostToDevice, st));
+    return TR_OK;
+}
+
+// read k and done of a scalar block (one small D2H)
+static tr_status read_status(tr_ctx *c, const CgScalars *s, int *k, int *done, cudaStream_t st) {
+    int32_t *h = reinterpret_cast<int32_t *>(c->host_pinned);
+    TRY(cudaMemcpyAsync(h, &s->k, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    TRY(cudaStreamSynchronize(st));
+    *k = h[0];
+    *done = h[1];
+    return TR_OK;
+}
+static tr_status read_double(tr_ctx *c, const double *d, double *out, cudaStream_t st) {
+    TRY(cudaMemcpyAsync(c->host_pinned + 2, d, sizeof(double), cudaMemcpyDeviceToHost, st));
+    TRY(cudaStreamSynchronize(st));
+    *out = c->host_pinned[2];
+    return TR_OK;
+}
+
+// One CG iteration of precision T (three launches, all on device state).
+template <typename T>
+static cudaError_t cg_iteration(tr_ctx *c, const DeviceOp<T> &op, uint32_t aslm, T *x, T *r, T *p, T *Ap, T *z,
+                                const T *dinv, CgScalars *s, double *hist, int hcap, cudaStream_t st) {
+    cudaError_t e = launch_lhs<T>(c, op, p, Ap, 2, nullptr, s, &s->done, st);
+    if (e == cudaSuccess) e = launch_cg_update<T>(c, aslm, x, r, p, Ap, z, dinv, s, hist, hcap, 0, st);
+    if (e == cudaSuccess) e = launch_cg_direction<T>(c, aslm, p, dinv ? z : r, s, st);
+    return e;
+}
+
+// Runs CG iterations from a started state until done (converged, cap or
+// non-finite).  Graph slot `slot` caches the captured chunk.
+template <typename T>
+static tr_status run_cg(tr_ctx *c, int slot, const DeviceOp<T> &op, uint32_t aslm, T *x, T *r, T *p, T *Ap, T *z,
+                        const T *dinv, CgScalars *s, double *hist, int hcap, int use_graph, int *iters,
+                        int *done_out) {
+    cudaStream_t st = stream_of(c);
+    const int chunk = kCgChunk;
+    CachedGraph &g = c->graphs[slot];
+    if (use_graph && (!g.valid || g.stream != st)) {
+        if (g.exec) {
+            cudaGraphExecDestroy(g.exec);
+            g.exec = nullptr;
+        }
+        cudaGraph_t graph = nullptr;
+        TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        cudaError_t ce = cudaSuccess;
+        for (int i = 0; i < chunk && ce == cudaSuccess; ++i)
+            ce = cg_iteration<T>(c, op, aslm, x, r, p, Ap, z, dinv, s, hist, hcap, st);
+        cudaError_t ee = cudaStreamEndCapture(st, &graph);
+        if (ce != cudaSuccess) return fail(c, ce, "capture of CG chunk");
+        if (ee != cudaSuccess) return fail(c, ee, "cudaStreamEndCapture");
+        cudaError_t ie = cudaGraphInstantiate(&g.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (ie != cudaSuccess) return fail(c, ie, "cudaGraphInstantiate");
+        g.valid = true;
+        g.stream = st;
+    }
+    int k = 0, done = 0;
+    for (int guard = 0; guard < (1 << 24); ++guard) {
+        if (use_graph) {
+            TRY(cudaGraphLaunch(g.exec, st));
+        } else {
+            for (int i = 0; i < chunk; ++i) TRY((cg_iteration<T>(c, op, aslm, x, r, p, Ap, z, dinv, s, hist, hcap, st)));
+        }
+        tr_status rs = read_status(c, s, &k, &done, st);
+        if (rs != TR_OK) return rs;
+        if (done) break;
+    }
+    *iters = k;
+    *done_out = done;
+    return TR_OK;
+}
+
+// invprec (main.cpp:223-248): z = approximately D^-1 r by an inner CG on
+// computeLhsDiag from z = 0 to ||r_inner|| < inner_tol (absolute).
+static tr_status invprec(tr_ctx *c, const double *b, double *z, int inner_max, double inner_tol, int *inner_k,
+                         int64_t *diag_apps) {
+    cudaStream_t st = stream_of(c);
+    double *ip = c->inner[0], *iAp = c->inner[1], *ir = c->inner[2];
+    CgScalars *s = c->cg + 1;
+    tr_status ts = init_scalars(c, s, inner_tol, inner_max, st);
+    if (ts != TR_OK) return ts;
+    TRY(launch_cg_start<double>(c, c->aslm, b, z, ir, nullptr, ip, nullptr, s, st));
+    int k = 0, done = 0;
+    for (int guard = 0; guard < (1 << 24); ++guard) {
+        for (int i = 0; i < kCgChunk; ++i) {
+            TRY(launch_lhs_diag<double>(c, c->op64, ip, iAp, &s->done, st));
+            TRY(launch_dot<double, double>(c, c->aslm, ip, iAp, c->red_out + 4, st));
+            k_set_alpha<<<1, 1, 0, st>>>(s, c->red_out + 4);
+            TRY(cudaGetLastError());
+            TRY(launch_cg_update<double>(c, c->aslm, z, ir, ip, iAp, nullptr, nullptr, s, nullptr, 0, 0, st));
+            TRY(launch_cg_direction<double>(c, c->aslm, ip, ir, s, st));
+        }
+        ts = read_status(c, s, &k, &done, st);
+        if (ts != TR_OK) return ts;
+        if (done) break;
+    }
+    // reference count: the loop index at exit (main.cpp:232-247)
+    *inner_k += (done == 1) ? k - 1 : k;
+    *diag_apps += k;
+    return TR_OK;
+}
+
+// ----------------------------------------------------------------- FP64
+static tr_status solve_fp64(tr_ctx *c, const tr_solve_opts *o, const double *b, double *x,
+                            tr_solve_report *rep) {
+    cudaStream_t st = stream_of(c);
+    double *r = c->w64[1], *p = c->w64[2], *Ap = c->w64[3], *z = c->w64[4];
+    CgScalars *s = c->cg;
+    const int maxit = o->max_iter > 0 ? o->max_iter : 1000;
+    const double *dinv = (o->precondition == TR_PREC_JACOBI) ? c->op64.dinv : nullptr;
+
+    TRY(launch_dot<double, double>(c, c->aslm, b, b, c->red_out, st));
+    double bb = 0.0;
+    tr_status ts = read_double(c, c->red_out, &bb, st);
+    if (ts != TR_OK) return ts;
+    const double bnorm = std::sqrt(bb);
+    rep->rhs_norm = bnorm;
+    rep->initial_residual = bnorm;
+    const double tol = o->relative ? o->tol * bnorm : o->tol;
+    ts = init_scalars(c, s, tol, maxit, st);
+    if (ts != TR_OK) return ts;
+
+    int k = 0, done = 0;
+    if (o->precondition != TR_PREC_REFERENCE) {
+        TRY(launch_cg_start<double>(c, c->aslm, b, x, r, z, p, dinv, s, st));
+        int slot = dinv ? 1 : 0;
+        ts = run_cg<double>(c, slot, c->op64, c->aslm, x, r, p, Ap, z, dinv, s, c->dhist, c->hist_cap,
+                            o->use_graph, &k, &done);
+        if (ts != TR_OK) return ts;
+        rep->lhs_applications_f64 += k;
+    } else {
+        // host-driven outer loop around the inner CG (main.cpp:131-160)
+        const int imax = o->inner_max_iter > 0 ? o->inner_max_iter : 1000;
+        const double itol = o->inner_tol > 0 ? o->inner_tol : 1e-8;
+        int inner = 0;
+        int64_t dapps = 0;
+        TRY(cudaMemsetAsync(x, 0, sizeof(double) * c->nP * c->aslm, st));
+        TRY(cudaMemcpyAsync(r, b, sizeof(double) * c->nP * c->aslm, cudaMemcpyDeviceToDevice, st));
+        ts = invprec(c, r, z, imax, itol, &inner, &dapps);
+        if (ts != TR_OK) return ts;
+        TRY(cudaMemcpyAsync(p, z, sizeof(double) * c->nP * c->aslm, cudaMemcpyDeviceToDevice, st));
+        TRY(launch_dot<double, double>(c, c->aslm, r, z, c->red_out + 1, st));
+        k_set_nrz<<<1, 1, 0, st>>>(s, c->red_out + 1);
+        TRY(cudaGetLastError());
+        for (int it = 0; it < maxit; ++it) {
+            TRY(launch_lhs<double>(c, c->op64, p, Ap, 2, nullptr, s, &s->done, st));
+            // x += alpha p, r -= alpha Ap, stop test; beta follows invprec
+            TRY(launch_cg_update<double>(c, c->aslm, x, r, p, Ap, nullptr, nullptr, s, c->dhist, c->hist_cap, 1,
+                                         st));
+            rep->lhs_applications_f64 += 1;
+            ts = read_status(c, s, &k, &done, st);
+            if (ts != TR_OK) return ts;
+            if (done) break;
+            ts = invprec(c, r, z, imax, itol, &inner, &dapps);
+            if (ts != TR_OK) return ts;
+            TRY(launch_dot<double, double>(c, c->aslm, z, r, c->red_out + 1, st));
+            k_set_beta<<<1, 1, 0, st>>>(s, c->red_out + 1);
+            TRY(cudaGetLastError());
+            TRY(launch_cg_direction<double>(c, c->aslm, p, z, s, st));
+        }
+        rep->inner_iterations = inner;
+        rep->diag_applications = dapps;
+    }
+    rep->iterations = k;
+    rep->converged = (done == 1);
+    if (done == 3) {
+        c->last_error = "CG produced a non-finite residual";
+        return TR_ERR_NAN;
+    }
+    return TR_OK;
+}
+
+// ---------------------------------------------------------------- mixed
+static tr_status solve_mixed(tr_ctx *c, const tr_solve_opts *o, const double *b, double *x,
+                             tr_solve_report *rep) {
+    cudaStream_t st = stream_of(c);
+    double *r64 = c->w64[1], *Ax = c->w64[3];
+    float *d = c->w32[0], *r = c->w32[1], *p = c->w32[2], *Ap = c->w32[3], *z = c->w32[4];
+    CgScalars *so = c->cg + 2, *si = c->cg + 3;
+    const double *bb_src = b;
+    const float *dinv = (o->precondition == TR_PREC_JACOBI) ? c->op32.dinv : nullptr;
+    const int max_outer = o->max_outer > 0 ? o->max_outer : 30;
+    const int inner_max = o->inner_max_iter > 0 ? o->inner_max_iter : (o->max_iter > 0 ? o->max_iter : 1000);
+    const double inner_tol = o->inner_tol > 0 ? o->inner_tol : 1e-4;
+
+    tr_status ts = init_scalars(c, so, 0.0, 0, st);
+    if (ts != TR_OK) return ts;
+    TRY(cudaMemsetAsync(x, 0, sizeof(double) * c->nP * c->aslm, st));
+    TRY(cudaMemsetAsync(Ax, 0, sizeof(double) * c->nP * c->aslm, st));
+    TRY(launch_residual(c, bb_src, Ax, r64, so, st));  // r = b, scale = ||b||
+    double bnorm = 0.0;
+    ts = read_double(c, &so->scale, &bnorm, st);
+    if (ts != TR_OK) return ts;
+    rep->rhs_norm = bnorm;
+    rep->initial_residual = bnorm;
+    const double target = o->relative ? o->tol * bnorm : o->tol;
+    double rn = bnorm;
+    int total = 0, outer = 0, hist_used = 0;
+    bool converged = (rn < target);
+    while (!converged && outer < max_outer && total < (o->max_iter > 0 ? o->max_iter : 1 << 30)) {
+        TRY(launch_to_f32(c, r64, r, so, st));
+        ts = init_scalars(c, si, inner_tol, inner_max, st);
+        if (ts != TR_OK) return ts;
+        TRY(launch_cg_start<float>(c, c->aslm32, r, d, r, z, p, dinv, si, st));
+        int k = 0, done = 0;
+        int slot = dinv ? 3 : 2;
+        ts = run_cg<float>(c, slot, c->op32, c->aslm32, d, r, p, Ap, z, dinv, si, nullptr, 0, o->use_graph, &k,
+                           &done);
+        if (ts != TR_OK) return ts;
+        total += k;
+        rep->lhs_applications_f32 += k;
+        TRY(launch_correct(c, x, d, so, st));
+        TRY(launch_lhs<double>(c, c->op64, x, Ax, 0, nullptr, nullptr, nullptr, st));
+        rep->lhs_applications_f64 += 1;
+        TRY(launch_residual(c, bb_src, Ax, r64, so, st));
+        ts = read_double(c, &so->scale, &rn, st);
+        if (ts != TR_OK) return ts;
+        if (o->history && hist_used < o->history_len) o->history[hist_used++] = rn;
+        ++outer;
+        if (!std::isfinite(rn)) {
+            c->last_error = "defect correction produced a non-finite residual";
+            return TR_ERR_NAN;
+        }
+        converged = rn < target;
+        if (done == 3) {
+            c->last_error = "FP32 inner CG produced a non-finite residual";
+            return TR_ERR_NAN;
+        }
+    }
+    rep->iterations = total;
+    rep->outer_steps = outer;
+    rep->converged = converged;
+    rep->final_residual = rn;
+    return TR_OK;
+}
+
+tr_status solve(tr_ctx *c, const tr_solve_opts *o, const double *b_in, double *f, tr_solve_report *rep) {
+    cudaStream_t st = stream_of(c);
+    std::memset(rep, 0, sizeof(*rep));
+    tr_status ts = ensure_workspace(c, std::max(o->max_iter, 1));
+    if (ts != TR_OK) return ts;
+    cudaEvent_t e0, e1;
+    TRY(cudaEventCreate(&e0));
+    TRY(cudaEventCreate(&e1));
+    TRY(cudaEventRecord(e0, st));
+    double *b = c->w64[5];
+    if (b_in) TRY(cudaMemcpyAsync(b, b_in, sizeof(double) * c->nP * c->aslm, cudaMemcpyDeviceToDevice, st));
+    else TRY(launch_rhs(c, b, st));
+    double *x = c->w64[0];
+    if (o->mode == TR_MODE_MIXED) ts = solve_mixed(c, o, b, x, rep);
+    else ts = solve_fp64(c, o, b, x, rep);
+    if (ts != TR_OK && ts != TR_ERR_NAN) return ts;
+    tr_status solve_status = ts;
+    if (o->mode != TR_MODE_MIXED) {
+        // true FP64 residual of the returned solution
+        CgScalars *sr = c->cg + 2;
+        TRY(launch_lhs<double>(c, c->op64, x, c->w64[3], 0, nullptr, nullptr, nullptr, st));
+        TRY(launch_residual(c, b, c->w64[3], c->w64[1], sr, st));
+        tr_status rs = read_double(c, &sr->scale, &rep->final_residual, st);
+        if (rs != TR_OK) return rs;
+        if (o->history && o->history_len > 0) {
+            int n = std::min(rep->iterations, std::min(o->history_len, c->hist_cap));
+            if (n > 0) TRY(cudaMemcpyAsync(o->history, c->dhist, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+        }
+    }
+    TRY(cudaMemcpyAsync(f, x, sizeof(double) * c->nP * c->aslm, cudaMemcpyDeviceToDevice, st));
+    TRY(cudaEventRecord(e1, st));
+    TRY(cudaEventSynchronize(e1));
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    rep->device_ms = ms;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (solve_status != TR_OK) return solve_status;
+    if (!rep->converged) {
+        c->last_error = "solver reached its iteration limit before the tolerance";
+        return TR_ERR_NOT_CONVERGED;
+    }
+    return TR_OK;
+}
+
+}  // namespace transfer
