@@ -1,0 +1,321 @@
+#!/usr/bin/env python3
+"""Benchmark of the radiative-transfer hot path: cell-ordinate updates/s and
+time to a 1e-6 FP64 residual, FP32-mixed vs FP64, on B200.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload milne_slab|config1|cube64]
+
+A step is one solve of A f = b from f = 0 to ||b - A f|| / ||b|| < 1e-6
+(FP64 residual) on the workload, with the right-hand side resident in HBM.
+The headline solver is the FP32-CG-in-FP64-defect-correction solve; the
+plain FP64 CG (the drop-in) is timed in the same run.  A cell-ordinate
+update is one (tetrahedron, harmonic) pair of one operator application:
+nT * slm per application, FP32 and FP64 applications both counted.
+
+--gpus N runs N independent replicas (one process per GPU under torchrun):
+the solve does not shard (one GPU per problem), value = total updates of
+all ranks / the slowest rank's time.  --impl reference times the FP64 CPU
+restatement of the reference path (the reference has no CPU solve of its
+own) on all host cores, rank 0 only.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+TOL = 1e-6
+UNIT = "cell-ordinate updates/s"
+METRIC = "cell-ordinate updates/s and time to 1e-6 residual, FP32-mixed vs FP64, 1 B200"
+
+
+def parse_args():
+    p = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--workload", default="milne_slab")
+    p.add_argument("--cpu-iters", type=int, default=0, help="CG iterations per CPU-baseline sample (0: auto)")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        load = [x for x in sm if smax and x > 0.3 * smax] or sm
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# ----------------------------------------------------------------- CPU arm
+def cpu_sample(workload, iters, steps=1):
+    """FP64 oracle CG iterations on the workload (all host threads);
+    returns (updates/s, threads, seconds, iterations)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle_py as op
+    from transfer_b200 import workloads as W
+    md, ad, phys, _ = W.WORKLOADS[workload]()
+    kw = {}
+    if phys is not None:
+        kw = dict(kappa_abs_volume=phys.kappa_abs_volume, face_bc=phys.face_bc, face_incident=phys.face_incident)
+    O = op.Oracle(md, ad, **kw)
+    b = O.rhs()
+    total, n = 0.0, 0
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        O.cg(b, max_iter=iters, tol=0.0)
+        total += time.perf_counter() - t0
+        n += iters
+    return n * md.nT * ad.slm / total, op.lib.oracle_num_threads(), total, n
+
+
+def auto_cpu_iters(workload):
+    return {"config1": 60, "milne_slab": 40, "cube64": 2}.get(workload, 10)
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    iters = args.cpu_iters or auto_cpu_iters(args.workload)
+    for _ in range(max(0, min(args.warmup, 1))):
+        cpu_sample(args.workload, max(1, iters // 4))
+    v, threads, secs, n = cpu_sample(args.workload, iters, steps=args.steps)
+    sample = f"{n} FP64 CG iterations ({iters} per step) of the CPU restatement on {args.workload}"
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": args.workload},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------- GPU arm
+def run_ours(args, rank, world, local):
+    import numpy as np
+    import torch
+    import transfer_b200 as tr
+    from transfer_b200 import workloads as W
+
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    md, ad, phys, desc = W.WORKLOADS[args.workload]()
+    ctx = tr.CudaContext(local, md, ad, phys)
+    nT, slm, nP = ctx.nT, ctx.slm, ctx.nP
+    per_app = nT * slm
+    mixed = dict(mode=tr.TR_MODE_MIXED, tol=TOL, relative=1, max_iter=200000)
+    fp64 = dict(mode=tr.TR_MODE_FP64, tol=TOL, relative=1, max_iter=200000)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")   # 256 MiB > L2
+
+    def barrier():
+        if pg:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    def timed(opts, steps):
+        tot_ms, updates, launches, iters, reps = 0.0, 0, 0, [], []
+        for s in range(steps):
+            flush.fill_(float(s))
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            f, rep = ctx.solve(**opts)
+            e1.record()
+            torch.cuda.synchronize()
+            if not rep.converged:
+                raise RuntimeError(f"solve did not converge: {dict(rep)}")
+            tot_ms += e0.elapsed_time(e1)
+            updates += (rep.lhs_applications_f64 + rep.lhs_applications_f32) * per_app
+            launches += rep.kernel_launches
+            reps.append(rep)
+        return tot_ms, updates, launches, reps, f
+
+    for _ in range(args.warmup):
+        ctx.solve(**mixed)
+        ctx.solve(**fp64)
+    barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    t_mixed, u_mixed, l_mixed, reps_mixed, f_mixed = timed(mixed, args.steps)
+    clocks = sampler.stop()
+    t_fp64, u_fp64, l_fp64, reps_fp64, _ = timed(fp64, args.steps)
+    # end to end through the C ABI with host buffers (pinned staging inside)
+    b = ctx.allocVector()
+    ctx.computeRhs(b)
+    b_host = b.cpu().numpy()
+    f_host = np.zeros(ctx.N())
+    ctx.solve_host(b_host, f_host, **mixed)   # allocate the staging buffers once
+    t_e2e, u_e2e = 0.0, 0
+    for s in range(args.steps):
+        flush.fill_(float(s))
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        f_host, rep = ctx.solve_host(b_host, f_host, **mixed)
+        e1.record()
+        torch.cuda.synchronize()
+        t_e2e += e0.elapsed_time(e1)
+        u_e2e += (rep.lhs_applications_f64 + rep.lhs_applications_f32) * per_app
+    # the dominant kernel in isolation (back-to-back launches on the context stream)
+    x32 = ctx.allocVector(torch.float32)
+    x32.view(nP, -1)[:, :slm].normal_()
+    y32 = ctx.allocVector(torch.float32)
+    x64 = ctx.allocVector()
+    x64.view(nP, -1)[:, :slm].normal_()
+    y64 = ctx.allocVector()
+    import ctypes as C
+    ms32, ms64 = C.c_double(), C.c_double()
+    tr.check(tr.lib.tr_bench_lhs(ctx._h, 32, x32.data_ptr(), y32.data_ptr(), 200, C.byref(ms32)), ctx._h)
+    tr.check(tr.lib.tr_bench_lhs(ctx._h, 64, x64.data_ptr(), y64.data_ptr(), 200, C.byref(ms64)), ctx._h)
+
+    vals = torch.tensor([t_mixed, t_fp64, t_e2e], dtype=torch.float64, device=f"cuda:{local}")
+    if pg:
+        pg.all_reduce(vals, op=pg.ReduceOp.MAX)
+    t_mixed, t_fp64, t_e2e = [float(x) for x in vals.cpu()]
+
+    if rank == 0:
+        peak, peak_kind = load_peaks()
+        bytes32, flops = W.algorithmic_work(md, ad, real_bytes=4)
+        bytes64, _ = W.algorithmic_work(md, ad, real_bytes=8)
+        ach32 = bytes32 / (ms32.value * 1e-3) / 1e9
+        ach64 = bytes64 / (ms64.value * 1e-3) / 1e9
+        it_mixed = statistics.mean(r.iterations for r in reps_mixed)
+        it_fp64 = statistics.mean(r.iterations for r in reps_fp64)
+        line = {
+            "metric": METRIC,
+            "value": world * u_mixed / (t_mixed * 1e-3),
+            "unit": UNIT,
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": t_mixed / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32+f64",
+            "data": "synthetic",
+            "config": {
+                **desc, "nP": nP, "nT": nT, "nF": ctx.nF, "slm": slm, "tol": TOL,
+                "solver": "FP32 CG inside FP64 defect correction (headline); plain FP64 CG timed alongside",
+                "l2": "256 MiB buffer written before every solve (inputs of one solve fit in L2)",
+                "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+            },
+            "time_to_solution_ms": {"mixed": t_mixed / args.steps, "fp64": t_fp64 / args.steps,
+                                    "speedup_mixed_vs_fp64": t_fp64 / t_mixed},
+            "fp64": {"value": world * u_fp64 / (t_fp64 * 1e-3), "unit": UNIT, "iterations": it_fp64},
+            "iterations": {"mixed_fp32_cg": it_mixed,
+                           "mixed_outer": statistics.mean(r.outer_steps for r in reps_mixed),
+                           "fp64_cg": it_fp64},
+            "final_relative_residual": {"mixed": max(r.final_residual / r.rhs_norm for r in reps_mixed),
+                                        "fp64": max(r.final_residual / r.rhs_norm for r in reps_fp64)},
+            "e2e": {"value": world * u_e2e / (t_e2e * 1e-3), "unit": UNIT,
+                    "h2d_bytes_per_step": 8 * ctx.N(), "d2h_bytes_per_step": 8 * ctx.N()},
+            "gpu_launches": int(l_mixed),
+            "roofline": {"bound": "hbm", "achieved": ach32, "peak": peak, "unit": "GB/s", "frac": ach32 / peak,
+                         "traffic": None, "peak_source": peak_kind,
+                         "kernel": "k_lhs<float> (FP32 operator, the inner-solve matvec)",
+                         "us_per_launch": 1e3 * ms32.value, "algorithmic_bytes": bytes32,
+                         "algorithmic_gflop": flops / 1e9, "gflops": flops / (ms32.value * 1e-3) / 1e9,
+                         "fp64_kernel": {"us_per_launch": 1e3 * ms64.value, "achieved": ach64,
+                                         "gflops": flops / (ms64.value * 1e-3) / 1e9}},
+            "clocks": clocks,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            iters = args.cpu_iters or auto_cpu_iters(args.workload)
+            v, threads, secs, n = cpu_sample(args.workload, iters)
+            line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                                    "sample": f"{n} FP64 CG iterations of the CPU restatement on {args.workload}"
+                                              f" ({secs:.1f} s)"}
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if pg:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    run_ours(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -219,6 +219,8 @@ typedef struct tr_solve_report {
     double  final_residual;      /* ||b - A f||_2 recomputed in FP64          */
     double  rhs_norm;            /* ||b||_2                                   */
     double  device_ms;           /* device time of the solve (CUDA events)    */
+    int64_t kernel_launches;     /* kernels of this library launched (graph
+                                    nodes counted one by one)               */
 } tr_solve_report;
 
 void tr_solve_opts_default(tr_solve_opts *opts);   /* reference settings */
@@ -231,6 +233,13 @@ tr_status tr_solve(tr_ctx *ctx, const tr_solve_opts *opts, const double *b,
 tr_status tr_solve_host(tr_ctx *ctx, const tr_solve_opts *opts,
                         const double *b_host, double *f_host,
                         tr_solve_report *report);
+
+/* Measurement helper (no reference counterpart): launches the operator
+ * (precision 64: tr_compute_lhs, 32: tr_compute_lhs_f32) `iters` times back
+ * to back on the context stream from x into y (device vectors of that
+ * precision) and returns the mean device time per launch from CUDA events. */
+tr_status tr_bench_lhs(tr_ctx *ctx, int precision, const void *x, void *y,
+                       int iters, double *ms_per_launch);
 
 /* ---- post-processing (MeshData::ComputeMoments / ComputeFlux,
  *      MeshData.cpp:96-136), on the device ----------------------------- */

@@ -8,8 +8,7 @@ import os
 
 import numpy as np
 
-ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-ORACLE_SO = os.path.join(ROOT, "oracle", "liboracle.so")
+ORACLE_SO = os.path.join(os.path.dirname(os.path.abspath(__file__)), "liboracle.so")
 
 
 class or_mesh(C.Structure):

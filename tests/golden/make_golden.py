@@ -155,7 +155,7 @@ def ref_cfg(tmp, meshfile, maxk, kappa, Ip, prec=0, dump=0, out="sol.txt"):
     lines = [f"numregs = {len(kappa) - 1}", f"meshfile = {meshfile}", f"outfile = {out}", "device = 0",
              f"angorder = {maxk}", f"dump = {dump}", f"precondition = {prec}", "soltype = 0"]
     for r in range(1, len(kappa)):
-        lines += [f"[region {r}]", f"kappa = {kappa[r]!r}", f"Ip = {Ip[r]!r}"]
+        lines += [f"[region {r}]", f"kappa = {float(kappa[r])!r}", f"Ip = {float(Ip[r])!r}"]
     fn = os.path.join(tmp, "run.cfg")
     with open(fn, "w") as f:
         f.write("\n".join(lines) + "\n")

@@ -1,0 +1,147 @@
+"""GPU parity of the solvers (main.cpp:125-160 CG, invprec main.cpp:223-248),
+the moment/flux reduction (MeshData.cpp:96-136) and the Lanczos estimate
+(Eigenvalue.cpp:5-83) against the reference program's outputs and the FP64
+oracle.
+
+Tolerances: with the reference's stop rule (||r|| < 1e-4) the iteration
+counts are equal and U agrees to 1e-7 relative (the iterates of a CG stopped
+that early amplify the rounding differences of the re-associated operator
+sums by up to ~1e2); converged FP64 solves agree
+with the oracle to 1e-10 relative in U (the parity target); mixed-precision
+solves reach an FP64 residual of 1e-8 relative with U within 1e-6."""
+import numpy as np
+import pytest
+import torch
+
+import oracle_py as op
+import transfer_b200 as tr
+from common import c1_mesh, golden, golden_angular, random_vector, refrun_mesh, rel_err, small_mesh
+
+pytestmark = pytest.mark.gpu
+
+
+def dev(x):
+    return torch.from_numpy(np.ascontiguousarray(x)).cuda()
+
+
+def host(t):
+    return t.detach().cpu().numpy()
+
+
+@pytest.mark.parametrize("name", ["small_k1", "small_k2", "c1_k1"])
+def test_cg_matches_reference_program(cuda, name):
+    r = golden(f"refrun_{name}.npz")
+    md, ad = refrun_mesh(r), golden_angular(int(r["maxk"]))
+    ctx = tr.CudaContext(0, md, ad)
+    f, rep, hist = ctx.solve(tol=1e-4, relative=0, max_iter=1000, history=2000)
+    ks = r["k"]
+    assert rep.converged and rep.iterations == len(ks)
+    assert abs(hist[len(ks) - 1] / r["residual"][-1] - 1) < 1e-6
+    U, T = ctx.computeMoments(f)
+    assert rel_err(host(U), r["U"]) < 1e-7
+    W = ctx.computeFlux(T)
+    assert rel_err(host(W).reshape(-1), r["W"]) < 1e-6
+
+
+def test_cg_with_reference_preconditioner(cuda):
+    r = golden("refrun_small_k1_prec.npz")
+    md, ad = refrun_mesh(r), golden_angular(int(r["maxk"]))
+    ctx = tr.CudaContext(0, md, ad)
+    f, rep = ctx.solve(tol=1e-4, precondition=tr.TR_PREC_REFERENCE)
+    assert rep.converged and rep.iterations == len(r["k"])
+    assert rep.inner_iterations == int(r["preck"])
+    U, _ = ctx.computeMoments(f)
+    assert rel_err(host(U), r["U"]) < 1e-7
+
+
+@pytest.mark.parametrize("maxk", [1, 3])
+def test_converged_solution_matches_oracle(cuda, maxk):
+    md = c1_mesh() if maxk == 1 else small_mesh(n=(6, 6, 6))
+    ad = golden_angular(maxk)
+    ctx, O = tr.CudaContext(0, md, ad), op.Oracle(md, ad)
+    f, rep = ctx.solve(tol=1e-12, relative=1, max_iter=5000)
+    assert rep.converged and rep.final_residual / rep.rhs_norm < 1e-11
+    fo, res = O.cg(tol=1e-12, relative=1, max_iter=5000)
+    assert res["converged"]
+    U, T = ctx.computeMoments(f)
+    Uo, To = O.moments(fo)
+    assert rel_err(host(U), Uo) < 1e-10
+    assert rel_err(host(T), To) < 1e-9
+
+
+def test_jacobi_preconditioned_solution(cuda):
+    md, ad = c1_mesh(), golden_angular(1)
+    ctx, O = tr.CudaContext(0, md, ad), op.Oracle(md, ad)
+    f, rep = ctx.solve(tol=1e-12, relative=1, precondition=tr.TR_PREC_JACOBI, max_iter=5000)
+    assert rep.converged and rep.final_residual / rep.rhs_norm < 1e-11
+    fo, res = O.cg(tol=1e-12, relative=1, precondition=2, max_iter=5000)
+    assert abs(rep.iterations - res["iterations"]) <= 2
+    assert rel_err(host(ctx.computeMoments(f)[0]), O.moments(fo)[0]) < 1e-10
+
+
+@pytest.mark.parametrize("prec", [tr.TR_PREC_NONE, tr.TR_PREC_JACOBI])
+def test_mixed_precision_defect_correction(cuda, prec):
+    md, ad = c1_mesh(), golden_angular(1)
+    ctx, O = tr.CudaContext(0, md, ad), op.Oracle(md, ad)
+    f, rep = ctx.solve(mode=tr.TR_MODE_MIXED, tol=1e-8, relative=1, precondition=prec, max_iter=20000)
+    assert rep.converged and rep.final_residual / rep.rhs_norm < 1e-8
+    assert rep.outer_steps >= 2 and rep.lhs_applications_f32 > 0
+    fo, _ = O.cg(tol=1e-12, relative=1, max_iter=5000)
+    assert rel_err(host(ctx.computeMoments(f)[0]), O.moments(fo)[0]) < 1e-6
+    f2, rep2 = ctx.solve(mode=tr.TR_MODE_MIXED, tol=1e-10, relative=1, precondition=prec, max_iter=20000)
+    assert rep2.converged and rep2.final_residual / rep2.rhs_norm < 1e-10
+    assert rel_err(host(ctx.computeMoments(f2)[0]), O.moments(fo)[0]) < 1e-9
+
+
+def test_graph_replay_is_bitwise_equal_to_direct_launches(cuda):
+    md, ad = c1_mesh(), golden_angular(1)
+    ctx = tr.CudaContext(0, md, ad)
+    f1, r1 = ctx.solve(tol=1e-10, relative=1, use_graph=1)
+    f2, r2 = ctx.solve(tol=1e-10, relative=1, use_graph=0)
+    f3, r3 = ctx.solve(tol=1e-10, relative=1, use_graph=1)
+    assert r1.iterations == r2.iterations == r3.iterations
+    assert torch.equal(f1, f2) and torch.equal(f1, f3)
+
+
+def test_host_buffers_and_explicit_rhs(cuda):
+    md, ad = small_mesh(), golden_angular(2)
+    ctx = tr.CudaContext(0, md, ad)
+    b = ctx.allocVector()
+    ctx.computeRhs(b)
+    f1, r1 = ctx.solve(b=b, tol=1e-10, relative=1)
+    fh, rh = ctx.solve_host(b_host=host(b), tol=1e-10, relative=1)
+    f0, r0 = ctx.solve(tol=1e-10, relative=1)
+    assert r1.iterations == rh.iterations == r0.iterations
+    assert np.array_equal(host(f1), fh) and torch.equal(f0, f1)
+
+
+def test_iteration_limit_and_zero_rhs(cuda):
+    md, ad = small_mesh(), golden_angular(1)
+    ctx = tr.CudaContext(0, md, ad)
+    f, rep = ctx.solve(tol=1e-14, relative=1, max_iter=3)
+    assert rep.status == tr._lib.TR_ERR_NOT_CONVERGED and rep.iterations == 3 and not rep.converged
+    z = ctx.allocVector()
+    f, rep = ctx.solve(b=z, tol=1e-10, relative=1)
+    assert rep.converged and float(f.abs().max()) == 0.0
+
+
+def test_moments_and_flux_match_oracle(cuda):
+    md, ad = small_mesh(), golden_angular(3)
+    ctx, O = tr.CudaContext(0, md, ad), op.Oracle(md, ad)
+    f = random_vector(md.nP, ad.slm, ctx.aslm, 4)
+    U, T = ctx.computeMoments(dev(f))
+    Uo, To = O.moments(f)
+    assert rel_err(host(U), Uo) < 1e-15
+    assert rel_err(host(T), To) < 1e-14
+    W = ctx.computeFlux(T)
+    assert rel_err(host(W), O.flux(To)) < 1e-13
+
+
+def test_lanczos_matches_oracle(cuda):
+    md, ad = small_mesh(), golden_angular(1)
+    ctx, O = tr.CudaContext(0, md, ad), op.Oracle(md, ad)
+    v = random_vector(md.nP, ad.slm, ctx.aslm, 6)
+    lmax, extra, steps = ctx.eig_lanczos(dev(v))
+    lo, eo, so, _ = O.eigest(v)
+    assert steps == so
+    assert abs(lmax / lo - 1) < 1e-9

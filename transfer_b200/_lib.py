@@ -76,7 +76,7 @@ class tr_solve_report(C.Structure):
                 ("outer_steps", C.c_int32), ("lhs_applications_f64", C.c_int64),
                 ("lhs_applications_f32", C.c_int64), ("diag_applications", C.c_int64),
                 ("initial_residual", C.c_double), ("final_residual", C.c_double),
-                ("rhs_norm", C.c_double), ("device_ms", C.c_double)]
+                ("rhs_norm", C.c_double), ("device_ms", C.c_double), ("kernel_launches", C.c_int64)]
 
 
 class tr_region_params(C.Structure):
@@ -121,6 +121,7 @@ PROTOTYPES = [
     ("tr_solve_opts_default", None, [C.POINTER(tr_solve_opts)]),
     ("tr_solve", S, [P, C.POINTER(tr_solve_opts), P, P, C.POINTER(tr_solve_report)]),
     ("tr_solve_host", S, [P, C.POINTER(tr_solve_opts), P, P, C.POINTER(tr_solve_report)]),
+    ("tr_bench_lhs", S, [P, I, P, P, I, C.POINTER(D)]),
     ("tr_compute_moments", S, [P, P, P, P]),
     ("tr_compute_flux", S, [P, P, P]),
     ("tr_eig_lanczos", S, [P, P, P, P, I, C.POINTER(D), C.POINTER(D), C.POINTER(I)]),

@@ -300,6 +300,36 @@ tr_status tr_solve_host(tr_ctx *c, const tr_solve_opts *o, const double *b_host,
     return ss;
 }
 
+tr_status tr_bench_lhs(tr_ctx *c, int precision, const void *x, void *y, int iters, double *ms) {
+    CHECK_CTX(c);
+    CHECK_PTR(c, x);
+    CHECK_PTR(c, y);
+    CHECK_PTR(c, ms);
+    if ((precision != 32 && precision != 64) || iters < 1 || x == y)
+        return set_err(c, TR_ERR_INVALID_ARG, "precision must be 32 or 64, iters >= 1, x != y");
+    cudaStream_t st = stream_of(c);
+    cudaEvent_t e0, e1;
+    tr_status s = check_cuda(c, cudaEventCreate(&e0), "event");
+    if (s != TR_OK) return s;
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, st);
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < iters && e == cudaSuccess; ++i)
+        e = precision == 64 ? launch_lhs<double>(c, c->op64, static_cast<const double *>(x), static_cast<double *>(y),
+                                                 0, nullptr, nullptr, nullptr, st)
+                            : launch_lhs<float>(c, c->op32, static_cast<const float *>(x), static_cast<float *>(y), 0,
+                                                nullptr, nullptr, nullptr, st);
+    cudaEventRecord(e1, st);
+    s = check_cuda(c, e, "bench launch");
+    if (s == TR_OK) s = check_cuda(c, cudaEventSynchronize(e1), "bench sync");
+    float t = 0.0f;
+    if (s == TR_OK) cudaEventElapsedTime(&t, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *ms = static_cast<double>(t) / iters;
+    return s;
+}
+
 // --------------------------------------------------------------- moments
 tr_status tr_compute_moments(tr_ctx *c, const double *f, double *U, double *T) {
     CHECK_CTX(c);

@@ -161,6 +161,7 @@ struct tr_ctx {
     size_t stage_bytes = 0;
 
     std::vector<void *> allocations;
+    int64_t launches = 0;            // kernels launched (for solve reports)
 };
 
 namespace transfer {

@@ -56,6 +56,13 @@ __global__ void k_set_beta(CgScalars *s, const double *dot) {
         if (_e != cudaSuccess) return fail(c, _e, #__VA_ARGS__);    \
     } while (0)
 
+// a kernel launch of this library: checked and counted
+#define LAUNCH(...)          \
+    do {                     \
+        TRY(__VA_ARGS__);    \
+        ++c->launches;       \
+    } while (0)
+
 static tr_status fail(tr_ctx *c, cudaError_t e, const char *what) {
     c->last_error = std::string(what) + ": " + cudaGetErrorString(e);
     return TR_ERR_CUDA;
@@ -146,6 +153,7 @@ static cudaError_t cg_iteration(tr_ctx *c, const DeviceOp<T> &op, uint32_t aslm,
     cudaError_t e = launch_lhs<T>(c, op, p, Ap, 2, nullptr, s, &s->done, st);
     if (e == cudaSuccess) e = launch_cg_update<T>(c, aslm, x, r, p, Ap, z, dinv, s, hist, hcap, 0, st);
     if (e == cudaSuccess) e = launch_cg_direction<T>(c, aslm, p, dinv ? z : r, s, st);
+    c->launches += 3;
     return e;
 }
 
@@ -164,11 +172,13 @@ static tr_status run_cg(tr_ctx *c, int slot, const DeviceOp<T> &op, uint32_t asl
             g.exec = nullptr;
         }
         cudaGraph_t graph = nullptr;
+        const int64_t counted = c->launches;  // capturing launches nothing
         TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         cudaError_t ce = cudaSuccess;
         for (int i = 0; i < chunk && ce == cudaSuccess; ++i)
             ce = cg_iteration<T>(c, op, aslm, x, r, p, Ap, z, dinv, s, hist, hcap, st);
         cudaError_t ee = cudaStreamEndCapture(st, &graph);
+        c->launches = counted;
         if (ce != cudaSuccess) return fail(c, ce, "capture of CG chunk");
         if (ee != cudaSuccess) return fail(c, ee, "cudaStreamEndCapture");
         cudaError_t ie = cudaGraphInstantiate(&g.exec, graph, 0);
@@ -181,6 +191,7 @@ static tr_status run_cg(tr_ctx *c, int slot, const DeviceOp<T> &op, uint32_t asl
     for (int guard = 0; guard < (1 << 24); ++guard) {
         if (use_graph) {
             TRY(cudaGraphLaunch(g.exec, st));
+            c->launches += 3 * chunk;
         } else {
             for (int i = 0; i < chunk; ++i) TRY((cg_iteration<T>(c, op, aslm, x, r, p, Ap, z, dinv, s, hist, hcap, st)));
         }
@@ -202,16 +213,16 @@ static tr_status invprec(tr_ctx *c, const double *b, double *z, int inner_max, d
     CgScalars *s = c->cg + 1;
     tr_status ts = init_scalars(c, s, inner_tol, inner_max, st);
     if (ts != TR_OK) return ts;
-    TRY(launch_cg_start<double>(c, c->aslm, b, z, ir, nullptr, ip, nullptr, s, st));
+    LAUNCH(launch_cg_start<double>(c, c->aslm, b, z, ir, nullptr, ip, nullptr, s, st));
     int k = 0, done = 0;
     for (int guard = 0; guard < (1 << 24); ++guard) {
         for (int i = 0; i < kCgChunk; ++i) {
-            TRY(launch_lhs_diag<double>(c, c->op64, ip, iAp, &s->done, st));
-            TRY(launch_dot<double, double>(c, c->aslm, ip, iAp, c->red_out + 4, st));
-            k_set_alpha<<<1, 1, 0, st>>>(s, c->red_out + 4);
+            LAUNCH(launch_lhs_diag<double>(c, c->op64, ip, iAp, &s->done, st));
+            LAUNCH(launch_dot<double, double>(c, c->aslm, ip, iAp, c->red_out + 4, st));
+            k_set_alpha<<<1, 1, 0, st>>>(s, c->red_out + 4); ++c->launches;
             TRY(cudaGetLastError());
-            TRY(launch_cg_update<double>(c, c->aslm, z, ir, ip, iAp, nullptr, nullptr, s, nullptr, 0, 0, st));
-            TRY(launch_cg_direction<double>(c, c->aslm, ip, ir, s, st));
+            LAUNCH(launch_cg_update<double>(c, c->aslm, z, ir, ip, iAp, nullptr, nullptr, s, nullptr, 0, 0, st));
+            LAUNCH(launch_cg_direction<double>(c, c->aslm, ip, ir, s, st));
         }
         ts = read_status(c, s, &k, &done, st);
         if (ts != TR_OK) return ts;
@@ -232,7 +243,8 @@ static tr_status solve_fp64(tr_ctx *c, const tr_solve_opts *o, const double *b, 
     const int maxit = o->max_iter > 0 ? o->max_iter : 1000;
     const double *dinv = (o->precondition == TR_PREC_JACOBI) ? c->op64.dinv : nullptr;
 
-    TRY(launch_dot<double, double>(c, c->aslm, b, b, c->red_out, st));
+    LAUNCH(launch_dot<double, double>(c, c->aslm, b, b, c->red_out, st));
+
     double bb = 0.0;
     tr_status ts = read_double(c, c->red_out, &bb, st);
     if (ts != TR_OK) return ts;
@@ -245,7 +257,7 @@ static tr_status solve_fp64(tr_ctx *c, const tr_solve_opts *o, const double *b, 
 
     int k = 0, done = 0;
     if (o->precondition != TR_PREC_REFERENCE) {
-        TRY(launch_cg_start<double>(c, c->aslm, b, x, r, z, p, dinv, s, st));
+        LAUNCH(launch_cg_start<double>(c, c->aslm, b, x, r, z, p, dinv, s, st));
         int slot = dinv ? 1 : 0;
         ts = run_cg<double>(c, slot, c->op64, c->aslm, x, r, p, Ap, z, dinv, s, c->dhist, c->hist_cap,
                             o->use_graph, &k, &done);
@@ -262,13 +274,13 @@ static tr_status solve_fp64(tr_ctx *c, const tr_solve_opts *o, const double *b, 
         ts = invprec(c, r, z, imax, itol, &inner, &dapps);
         if (ts != TR_OK) return ts;
         TRY(cudaMemcpyAsync(p, z, sizeof(double) * c->nP * c->aslm, cudaMemcpyDeviceToDevice, st));
-        TRY(launch_dot<double, double>(c, c->aslm, r, z, c->red_out + 1, st));
-        k_set_nrz<<<1, 1, 0, st>>>(s, c->red_out + 1);
+        LAUNCH(launch_dot<double, double>(c, c->aslm, r, z, c->red_out + 1, st));
+        k_set_nrz<<<1, 1, 0, st>>>(s, c->red_out + 1); ++c->launches;
         TRY(cudaGetLastError());
         for (int it = 0; it < maxit; ++it) {
-            TRY(launch_lhs<double>(c, c->op64, p, Ap, 2, nullptr, s, &s->done, st));
+            LAUNCH(launch_lhs<double>(c, c->op64, p, Ap, 2, nullptr, s, &s->done, st));
             // x += alpha p, r -= alpha Ap, stop test; beta follows invprec
-            TRY(launch_cg_update<double>(c, c->aslm, x, r, p, Ap, nullptr, nullptr, s, c->dhist, c->hist_cap, 1,
+            LAUNCH(launch_cg_update<double>(c, c->aslm, x, r, p, Ap, nullptr, nullptr, s, c->dhist, c->hist_cap, 1,
                                          st));
             rep->lhs_applications_f64 += 1;
             ts = read_status(c, s, &k, &done, st);
@@ -276,10 +288,10 @@ static tr_status solve_fp64(tr_ctx *c, const tr_solve_opts *o, const double *b, 
             if (done) break;
             ts = invprec(c, r, z, imax, itol, &inner, &dapps);
             if (ts != TR_OK) return ts;
-            TRY(launch_dot<double, double>(c, c->aslm, z, r, c->red_out + 1, st));
-            k_set_beta<<<1, 1, 0, st>>>(s, c->red_out + 1);
+            LAUNCH(launch_dot<double, double>(c, c->aslm, z, r, c->red_out + 1, st));
+            k_set_beta<<<1, 1, 0, st>>>(s, c->red_out + 1); ++c->launches;
             TRY(cudaGetLastError());
-            TRY(launch_cg_direction<double>(c, c->aslm, p, z, s, st));
+            LAUNCH(launch_cg_direction<double>(c, c->aslm, p, z, s, st));
         }
         rep->inner_iterations = inner;
         rep->diag_applications = dapps;
@@ -310,7 +322,7 @@ static tr_status solve_mixed(tr_ctx *c, const tr_solve_opts *o, const double *b,
     if (ts != TR_OK) return ts;
     TRY(cudaMemsetAsync(x, 0, sizeof(double) * c->nP * c->aslm, st));
     TRY(cudaMemsetAsync(Ax, 0, sizeof(double) * c->nP * c->aslm, st));
-    TRY(launch_residual(c, bb_src, Ax, r64, so, st));  // r = b, scale = ||b||
+    LAUNCH(launch_residual(c, bb_src, Ax, r64, so, st));  // r = b, scale = ||b||
     double bnorm = 0.0;
     ts = read_double(c, &so->scale, &bnorm, st);
     if (ts != TR_OK) return ts;
@@ -321,10 +333,10 @@ static tr_status solve_mixed(tr_ctx *c, const tr_solve_opts *o, const double *b,
     int total = 0, outer = 0, hist_used = 0;
     bool converged = (rn < target);
     while (!converged && outer < max_outer && total < (o->max_iter > 0 ? o->max_iter : 1 << 30)) {
-        TRY(launch_to_f32(c, r64, r, so, st));
+        LAUNCH(launch_to_f32(c, r64, r, so, st));
         ts = init_scalars(c, si, inner_tol, inner_max, st);
         if (ts != TR_OK) return ts;
-        TRY(launch_cg_start<float>(c, c->aslm32, r, d, r, z, p, dinv, si, st));
+        LAUNCH(launch_cg_start<float>(c, c->aslm32, r, d, r, z, p, dinv, si, st));
         int k = 0, done = 0;
         int slot = dinv ? 3 : 2;
         ts = run_cg<float>(c, slot, c->op32, c->aslm32, d, r, p, Ap, z, dinv, si, nullptr, 0, o->use_graph, &k,
@@ -332,10 +344,10 @@ static tr_status solve_mixed(tr_ctx *c, const tr_solve_opts *o, const double *b,
         if (ts != TR_OK) return ts;
         total += k;
         rep->lhs_applications_f32 += k;
-        TRY(launch_correct(c, x, d, so, st));
-        TRY(launch_lhs<double>(c, c->op64, x, Ax, 0, nullptr, nullptr, nullptr, st));
+        LAUNCH(launch_correct(c, x, d, so, st));
+        LAUNCH(launch_lhs<double>(c, c->op64, x, Ax, 0, nullptr, nullptr, nullptr, st));
         rep->lhs_applications_f64 += 1;
-        TRY(launch_residual(c, bb_src, Ax, r64, so, st));
+        LAUNCH(launch_residual(c, bb_src, Ax, r64, so, st));
         ts = read_double(c, &so->scale, &rn, st);
         if (ts != TR_OK) return ts;
         if (o->history && hist_used < o->history_len) o->history[hist_used++] = rn;
@@ -360,6 +372,7 @@ static tr_status solve_mixed(tr_ctx *c, const tr_solve_opts *o, const double *b,
 tr_status solve(tr_ctx *c, const tr_solve_opts *o, const double *b_in, double *f, tr_solve_report *rep) {
     cudaStream_t st = stream_of(c);
     std::memset(rep, 0, sizeof(*rep));
+    const int64_t launches0 = c->launches;
     tr_status ts = ensure_workspace(c, std::max(o->max_iter, 1));
     if (ts != TR_OK) return ts;
     cudaEvent_t e0, e1;
@@ -368,7 +381,7 @@ tr_status solve(tr_ctx *c, const tr_solve_opts *o, const double *b_in, double *f
     TRY(cudaEventRecord(e0, st));
     double *b = c->w64[5];
     if (b_in) TRY(cudaMemcpyAsync(b, b_in, sizeof(double) * c->nP * c->aslm, cudaMemcpyDeviceToDevice, st));
-    else TRY(launch_rhs(c, b, st));
+    else LAUNCH(launch_rhs(c, b, st));
     double *x = c->w64[0];
     if (o->mode == TR_MODE_MIXED) ts = solve_mixed(c, o, b, x, rep);
     else ts = solve_fp64(c, o, b, x, rep);
@@ -377,8 +390,8 @@ tr_status solve(tr_ctx *c, const tr_solve_opts *o, const double *b_in, double *f
     if (o->mode != TR_MODE_MIXED) {
         // true FP64 residual of the returned solution
         CgScalars *sr = c->cg + 2;
-        TRY(launch_lhs<double>(c, c->op64, x, c->w64[3], 0, nullptr, nullptr, nullptr, st));
-        TRY(launch_residual(c, b, c->w64[3], c->w64[1], sr, st));
+        LAUNCH(launch_lhs<double>(c, c->op64, x, c->w64[3], 0, nullptr, nullptr, nullptr, st));
+        LAUNCH(launch_residual(c, b, c->w64[3], c->w64[1], sr, st));
         tr_status rs = read_double(c, &sr->scale, &rep->final_residual, st);
         if (rs != TR_OK) return rs;
         if (o->history && o->history_len > 0) {
@@ -392,6 +405,7 @@ tr_status solve(tr_ctx *c, const tr_solve_opts *o, const double *b_in, double *f
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, e0, e1);
     rep->device_ms = ms;
+    rep->kernel_launches = c->launches - launches0;
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (solve_status != TR_OK) return solve_status;

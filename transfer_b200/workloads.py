@@ -1,0 +1,90 @@
+"""Standard synthetic problems (no public dataset is involved; all meshes are
+generated, seeded).
+
+  config1      unit cube, 16^3 Kuhn hexahedra (24,576 tets), interior jitter
+               +-0.2h, kappa = 1, Ip = 1 inside r < 0.25 about the centre,
+               vacuum, maxk = 1 (harmonics up to l = 2; 26-point Lebedev
+               precision).  Small enough for the reference's own run.
+  milne_slab   box [0,1]^2 x [0,20], 8 x 8 x 160 Kuhn hexahedra (61,440
+               tets), jitter +-0.15h, kappa = 1, no internal source,
+               isotropic inflow I = 1 through z = 20, vacuum elsewhere,
+               maxk = 3 (l <= 6; the 86-point set: the reference's rule
+               choice 4 maxk + 2 cannot reach the 110-point set).
+  cube64       unit cube, 64^3 Kuhn hexahedra (1,572,864 tets), kappa per
+               tet = exp(0.5 g), g a unit Gaussian random field with
+               correlation length 0.1 (random-Fourier-feature sample),
+               Ip = 1 in a 0.05-radius ball at (0.2, 0.5, 0.5), maxk = 5
+               (l <= 10; 194-point precision).
+Each returns (MeshData, AngularData, Physics or None, description dict).
+"""
+import numpy as np
+
+from .core import AngularData, MeshData, Physics
+from ._lib import TR_BC_INCIDENT, TR_BC_VACUUM
+
+SEED = 20261203
+
+
+def config1(maxk=1, n=16):
+    md = MeshData.kuhn((n, n, n), jitter=0.2, seed=SEED, kappa=[0.0, 1.0, 1.0], Ip=[0.0, 1.0, 0.0],
+                       region_kind=1, region_arg=(0.5, 0.5, 0.5, 0.25))
+    desc = dict(workload="config1", mesh=f"{n}^3 Kuhn cube, jitter 0.2h", maxk=maxk,
+                physics="kappa=1, Ip=1 in r<0.25, vacuum")
+    return md, AngularData(maxk), None, desc
+
+
+def milne_slab(maxk=3, n=(8, 8, 160), depth=20.0, incident=1.0):
+    md = MeshData.kuhn(n, box=(0.0, 1.0, 0.0, 1.0, 0.0, depth), jitter=0.15, seed=SEED, kappa=[0.0, 1.0],
+                       Ip=[0.0, 0.0])
+    side = md.face_side
+    bc = np.where(side == 5, TR_BC_INCIDENT, TR_BC_VACUUM).astype(np.int32)
+    inc = np.where(side == 5, float(incident), 0.0)
+    phys = Physics(face_bc=bc, face_incident=inc)
+    desc = dict(workload="milne_slab", mesh=f"{n[0]}x{n[1]}x{n[2]} Kuhn slab [0,1]^2x[0,{depth:g}], jitter 0.15h",
+                maxk=maxk, physics=f"kappa=1, no scattering, isotropic inflow I={incident:g} at z={depth:g}, "
+                                   "vacuum elsewhere")
+    return md, AngularData(maxk), phys, desc
+
+
+def gaussian_random_field(points, corr_len=0.1, modes=512, seed=SEED):
+    """Unit-variance Gaussian field with covariance exp(-r^2 / (2 l^2)),
+    sampled as sqrt(2/M) sum cos(k.x + phi), k ~ N(0, I / l^2)."""
+    rng = np.random.default_rng(seed)
+    k = rng.standard_normal((modes, 3)) / corr_len
+    phi = rng.uniform(0.0, 2.0 * np.pi, modes)
+    out = np.zeros(len(points))
+    for c in range(0, modes, 64):
+        out += np.cos(points @ k[c:c + 64].T + phi[c:c + 64]).sum(axis=1)
+    return out * np.sqrt(2.0 / modes)
+
+
+def cube64(maxk=5, n=64):
+    base = MeshData.kuhn((n, n, n), jitter=0.2, seed=SEED, kappa=[0.0, 1.0], Ip=[0.0, 0.0])
+    tets = base.mesh["p"]
+    cent = base.coords[tets].mean(axis=1)
+    kappa_t = np.exp(0.5 * gaussian_random_field(cent))
+    hot = ((cent - np.array([0.2, 0.5, 0.5])) ** 2).sum(axis=1) < 0.05 ** 2
+    nT = len(tets)
+    kappa = np.concatenate([[0.0], kappa_t])
+    Ip = np.concatenate([[0.0], hot.astype(np.float64)])
+    md = MeshData.from_tets(base.coords, tets, np.arange(1, nT + 1, dtype=np.int32), kappa, Ip)
+    desc = dict(workload="cube64", mesh=f"{n}^3 Kuhn cube, jitter 0.2h", maxk=maxk,
+                physics="kappa=exp(0.5 GRF(l=0.1)) per tet, Ip=1 in r<0.05 at (0.2,0.5,0.5), vacuum")
+    return md, AngularData(maxk), None, desc
+
+
+WORKLOADS = {"config1": config1, "milne_slab": milne_slab, "cube64": cube64}
+
+
+def algorithmic_work(md, ad, real_bytes=8):
+    """Per operator application: bytes and flops as counted for the roofline:
+    read f and write A f (2 * real_bytes per vertex and harmonic), 4 vertex
+    indices + kappa per tet (24 B), 3 coordinates per vertex (24 B), 3
+    indices per boundary face (12 B); 108 flops per tet and harmonic, the
+    angular contraction 2 nnz(omega) per vertex and the boundary term
+    6 slm^2 per boundary face."""
+    slm = ad.slm
+    nnz = int((np.abs(ad.omega) > 1e-14 * np.abs(ad.omega).max()).sum())
+    byt = 2 * real_bytes * md.nP * slm + 24 * md.nT + 24 * md.nP + 12 * md.nF
+    flops = 108 * md.nT * slm + 2 * nnz * md.nP + 6 * md.nF * slm * slm
+    return byt, flops
