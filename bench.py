@@ -271,7 +271,8 @@ def run_ours(args, rank, world, local):
             "data": "synthetic",
             "config": {
                 **desc, "nP": nP, "nT": nT, "nF": ctx.nF, "slm": slm, "tol": TOL,
-                "solver": "FP32 CG inside FP64 defect correction (headline); plain FP64 CG timed alongside",
+                "solver": "FP32 CG inside FP64 defect correction (headline); plain FP64 CG timed alongside; "
+                          "persistent cooperative CG kernel",
                 "l2": "256 MiB buffer written before every solve (inputs of one solve fit in L2)",
                 "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
             },

@@ -189,6 +189,11 @@ enum {
     TR_MODE_FP64 = 0,        /* plain FP64 CG (the drop-in)                 */
     TR_MODE_MIXED = 1        /* FP32 CG inside FP64 defect correction       */
 };
+enum {
+    TR_ENGINE_PERSISTENT = 0,/* one cooperative kernel runs many iterations */
+    TR_ENGINE_GRAPH = 1,     /* CUDA-graph replay of 2-launch iterations    */
+    TR_ENGINE_LAUNCH = 2     /* the same launches issued one by one         */
+};
 typedef struct tr_solve_opts {
     int32_t mode;            /* TR_MODE_*                                   */
     int32_t precondition;    /* TR_PREC_*                                   */
@@ -198,10 +203,11 @@ typedef struct tr_solve_opts {
     double  tol;             /* reference: 1e-4 absolute                    */
     double  inner_tol;       /* invprec tolerance (reference 1e-8, absolute);
                                 mixed mode: relative reduction per inner
-                                FP32 solve (0 -> 1e-4)                      */
+                                FP32 solve (0 -> adaptive: 0.3 x what is
+                                still missing to tol, at least 2e-6)        */
     int32_t inner_max_iter;  /* invprec / FP32 inner cap (0 -> 1000)       */
     int32_t max_outer;       /* mixed mode: defect-correction steps (0->30) */
-    int32_t use_graph;       /* 1: replay captured CUDA graphs (default)    */
+    int32_t engine;          /* TR_ENGINE_* (all give identical results)    */
     int32_t history_len;     /* capacity of history[] (may be 0)            */
     double *history;         /* host array: ||r|| after each CG iteration   */
 } tr_solve_opts;

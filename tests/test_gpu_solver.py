@@ -38,9 +38,10 @@ def test_cg_matches_reference_program(cuda, name):
     assert rep.converged and rep.iterations == len(ks)
     assert abs(hist[len(ks) - 1] / r["residual"][-1] - 1) < 1e-6
     U, T = ctx.computeMoments(f)
-    assert rel_err(host(U), r["U"]) < 1e-7
-    W = ctx.computeFlux(T)
-    assert rel_err(host(W).reshape(-1), r["W"]) < 1e-6
+    # C1's stop ||r|| < 1e-4 is a 3% relative residual: looser agreement
+    assert rel_err(host(U), r["U"]) < (1e-6 if name == "c1_k1" else 1e-7)
+    W = ctx.computeFlux(T)   # W differentiates T: amplifies the spread (C1: ~1e-5)
+    assert rel_err(host(W).reshape(-1), r["W"]) < (1e-4 if name == "c1_k1" else 1e-6)
 
 
 def test_cg_with_reference_preconditioner(cuda):
@@ -93,14 +94,29 @@ def test_mixed_precision_defect_correction(cuda, prec):
     assert rel_err(host(ctx.computeMoments(f2)[0]), O.moments(fo)[0]) < 1e-9
 
 
-def test_graph_replay_is_bitwise_equal_to_direct_launches(cuda):
+def test_engines_agree(cuda):
+    """Graph replay and direct launches run the same kernels: bitwise equal.
+    The persistent kernel sums its reductions over a different block
+    partition: equal iteration counts (+-1) and rounding-level agreement."""
     md, ad = c1_mesh(), golden_angular(1)
     ctx = tr.CudaContext(0, md, ad)
-    f1, r1 = ctx.solve(tol=1e-10, relative=1, use_graph=1)
-    f2, r2 = ctx.solve(tol=1e-10, relative=1, use_graph=0)
-    f3, r3 = ctx.solve(tol=1e-10, relative=1, use_graph=1)
+    f1, r1 = ctx.solve(tol=1e-10, relative=1, engine=tr.TR_ENGINE_GRAPH)
+    f2, r2 = ctx.solve(tol=1e-10, relative=1, engine=tr.TR_ENGINE_LAUNCH)
+    f3, r3 = ctx.solve(tol=1e-10, relative=1, engine=tr.TR_ENGINE_GRAPH)
     assert r1.iterations == r2.iterations == r3.iterations
     assert torch.equal(f1, f2) and torch.equal(f1, f3)
+    f4, r4 = ctx.solve(tol=1e-10, relative=1, engine=tr.TR_ENGINE_PERSISTENT)
+    f5, r5 = ctx.solve(tol=1e-10, relative=1, engine=tr.TR_ENGINE_PERSISTENT)
+    assert torch.equal(f4, f5) and r4.iterations == r5.iterations
+    assert abs(r4.iterations - r1.iterations) <= 1
+    assert rel_err(host(f4), host(f1)) < 1e-9
+    for prec in (tr.TR_PREC_JACOBI,):
+        fa, ra = ctx.solve(tol=1e-10, relative=1, precondition=prec, engine=tr.TR_ENGINE_GRAPH)
+        fb, rb = ctx.solve(tol=1e-10, relative=1, precondition=prec, engine=tr.TR_ENGINE_PERSISTENT)
+        assert abs(ra.iterations - rb.iterations) <= 1 and rel_err(host(fb), host(fa)) < 1e-9
+    fm, rm = ctx.solve(mode=tr.TR_MODE_MIXED, tol=1e-10, relative=1, engine=tr.TR_ENGINE_GRAPH)
+    fn, rn = ctx.solve(mode=tr.TR_MODE_MIXED, tol=1e-10, relative=1, engine=tr.TR_ENGINE_PERSISTENT)
+    assert rm.converged and rn.converged and rel_err(host(fn), host(fm)) < 1e-8
 
 
 def test_host_buffers_and_explicit_rhs(cuda):

@@ -29,6 +29,7 @@ TR_BC_VACUUM, TR_BC_REFLECTIVE, TR_BC_INCIDENT = 0, 1, 2
 TR_SURFACE_AXIS, TR_SURFACE_EXACT = 0, 1
 TR_PREC_NONE, TR_PREC_REFERENCE, TR_PREC_JACOBI = 0, 1, 2
 TR_MODE_FP64, TR_MODE_MIXED = 0, 1
+TR_ENGINE_PERSISTENT, TR_ENGINE_GRAPH, TR_ENGINE_LAUNCH = 0, 1, 2
 
 
 class tr_tetrahedron(C.Structure):
@@ -67,7 +68,7 @@ class tr_ctx_info(C.Structure):
 class tr_solve_opts(C.Structure):
     _fields_ = [("mode", C.c_int32), ("precondition", C.c_int32), ("max_iter", C.c_int32),
                 ("relative", C.c_int32), ("tol", C.c_double), ("inner_tol", C.c_double),
-                ("inner_max_iter", C.c_int32), ("max_outer", C.c_int32), ("use_graph", C.c_int32),
+                ("inner_max_iter", C.c_int32), ("max_outer", C.c_int32), ("engine", C.c_int32),
                 ("history_len", C.c_int32), ("history", C.POINTER(C.c_double))]
 
 

@@ -22,10 +22,6 @@ struct Edge {
     uint32_t u;
     double c[kCoefStride];
 };
-struct BEdge {
-    uint32_t u;
-    double e[kBCoefStride];
-};
 
 // reference axis choice for a boundary face (kernels.cu:419-425)
 inline int face_axis(const tr_face &f, double *surf) {
@@ -47,7 +43,7 @@ std::string validate(const tr_mesh_view *m, const tr_angular_view *a) {
     for (int k = 0; k <= TR_MAXK_MAX; ++k)
         if (a->slm == static_cast<tr_idx>((1 + k) * (1 + 2 * k))) slm_ok = true;
     if (!slm_ok) return "slm is not (1+maxk)(1+2maxk) for maxk <= 7";
-    if (static_cast<uint64_t>(m->nP) * 128 > 0xFFFFFFFFULL * 8ULL) return "mesh too large";
+    if (static_cast<uint64_t>(m->nP) * 128 >= 0xFFFFFFFFULL) return "mesh too large for 32-bit vector offsets";
     if (m->tetstart[0] != 0) return "tetstart[0] != 0";
     for (tr_idx v = 0; v < m->nP; ++v)
         if (m->tetstart[v + 1] < m->tetstart[v]) return "tetstart not monotonic";
@@ -180,9 +176,8 @@ tr_status ctx_create(int device, const tr_mesh_view *m, const tr_angular_view *a
     c->num_sms = prop.multiProcessorCount;
 
     // ---------------------------------------------------- assembled operator
-    std::vector<uint32_t> row(nP + 1, 0), brow(nP + 1, 0);
+    std::vector<uint32_t> row(nP + 1, 0);
     std::vector<std::vector<Edge>> edges(nP);
-    std::vector<std::vector<BEdge>> bedges(nP);
     std::vector<double> inflow;
     bool any_inflow = false;
     if (bc)
@@ -215,8 +210,6 @@ tr_status ctx_create(int device, const tr_mesh_view *m, const tr_angular_view *a
                 e.c[10] += ka * mult * (1.0 / 20.0);
             }
         }
-        std::sort(E.begin(), E.end(), [](const Edge &x, const Edge &y) { return x.u < y.u; });
-        std::vector<BEdge> &B = bedges[v];
         for (tr_idx j = m->facestart[v]; j < m->facestart[v + 1]; ++j) {
             const tr_idx fi = m->faceidx[j], loc = m->facepos[j];
             const int kind = bc ? bc[fi] : TR_BC_VACUUM;
@@ -225,45 +218,34 @@ tr_status ctx_create(int device, const tr_mesh_view *m, const tr_angular_view *a
             double surf;
             const int ax = face_axis(F, &surf);
             if (kind == TR_BC_INCIDENT) inflow[3ULL * v + ax] += finc[fi] * surf * (1.0 / 3.0);
-            for (int k = 0; k < 3; ++k) {
-                BEdge *e = nullptr;
-                for (BEdge &b : B)
-                    if (b.u == F.p[k]) e = &b;
-                if (!e) {
-                    BEdge nb;
-                    nb.u = F.p[k];
-                    std::memset(nb.e, 0, sizeof(nb.e));
-                    B.push_back(nb);
-                    e = &B.back();
-                }
-                e->e[ax] += surf * ((k == static_cast<int>(loc)) ? 2.0 : 1.0) * (1.0 / 12.0);
-            }
+            for (int k = 0; k < 3; ++k)
+                find(F.p[k]).c[11 + ax] += surf * ((k == static_cast<int>(loc)) ? 2.0 : 1.0) * (1.0 / 12.0);
         }
-        std::sort(B.begin(), B.end(), [](const BEdge &x, const BEdge &y) { return x.u < y.u; });
+        std::sort(E.begin(), E.end(), [](const Edge &x, const Edge &y) { return x.u < y.u; });
     }
-    for (tr_idx v = 0; v < nP; ++v) {
-        row[v + 1] = row[v] + static_cast<uint32_t>(edges[v].size());
-        brow[v + 1] = brow[v] + static_cast<uint32_t>(bedges[v].size());
-    }
-    const size_t nnz = row[nP], nbnz = brow[nP];
+    for (tr_idx v = 0; v < nP; ++v) row[v + 1] = row[v] + static_cast<uint32_t>(edges[v].size());
+    const size_t nnz = row[nP];
     c->n_edges = nnz;
-    c->n_bnd_edges = nbnz;
-    std::vector<uint32_t> col(nnz), bcol(std::max<size_t>(nbnz, 1));
-    std::vector<double> coef(nnz * kCoefStride), bcoef(std::max<size_t>(nbnz, 1) * kBCoefStride, 0.0);
+    std::vector<uint32_t> col(nnz);
+    std::vector<double> coef(nnz * kCoefStride);
+    std::vector<uint8_t> bmask(nP, 0);
+    uint64_t nb = 0;
     for (tr_idx v = 0; v < nP; ++v) {
         size_t o = row[v];
         for (const Edge &e : edges[v]) {
             col[o] = e.u;
             std::memcpy(&coef[o * kCoefStride], e.c, sizeof(e.c));
-            ++o;
-        }
-        o = brow[v];
-        for (const BEdge &e : bedges[v]) {
-            bcol[o] = e.u;
-            std::memcpy(&bcoef[o * kBCoefStride], e.e, sizeof(e.e));
+            bool any = false;
+            for (int n = 0; n < 3; ++n)
+                if (e.c[11 + n] != 0.0) {
+                    bmask[v] |= static_cast<uint8_t>(1u << n);
+                    any = true;
+                }
+            nb += any;
             ++o;
         }
     }
+    c->n_bnd_edges = nb;
 
     // ---------------------------------------------------- angular tables
     const size_t ss = static_cast<size_t>(slm) * slm;
@@ -271,7 +253,7 @@ tr_status ctx_create(int device, const tr_mesh_view *m, const tr_angular_view *a
     for (size_t i = 0; i < 3 * ss; ++i) maxabs = std::max(maxabs, std::fabs(a->omega[i]));
     const double drop = 1e-14 * maxabs;
     std::vector<uint32_t> ang_start(slm + 1, 0);
-    std::vector<uint16_t> ang_src;
+    std::vector<uint32_t> ang_q, ang_lms;  // (3i+pos), lms of every kept entry
     std::vector<double> ang_w;
     for (tr_idx lm = 0; lm < slm; ++lm) {
         for (int i = 0; i < 3; ++i)
@@ -280,10 +262,22 @@ tr_status ctx_create(int device, const tr_mesh_view *m, const tr_angular_view *a
                 const size_t q = (static_cast<size_t>(i) * slm + lms) * slm + lm;
                 const double w = a->omega[q];
                 if (std::fabs(w) <= drop) continue;
-                ang_src.push_back(static_cast<uint16_t>(((3 * i + a->omega_pos[q]) << 8) | lms));
+                ang_q.push_back(3 * i + a->omega_pos[q]);
+                ang_lms.push_back(lms);
                 ang_w.push_back(w);
             }
         ang_start[lm + 1] = static_cast<uint32_t>(ang_w.size());
+    }
+    const size_t nang = ang_w.size();
+    std::vector<AngEntry<double>> ang64(std::max<size_t>(nang, 1));
+    std::vector<AngEntry<float>> ang32(std::max<size_t>(nang, 1));
+    const uint32_t sa64 = s_row_stride((slm + 7) & ~7u), sa32 = s_row_stride((slm + 15) & ~15u);
+    for (size_t e = 0; e < nang; ++e) {
+        ang64[e].w = ang_w[e];
+        ang64[e].off = ang_q[e] * sa64 + ang_lms[e];
+        ang64[e].pad = 0;
+        ang32[e].w = static_cast<float>(ang_w[e]);
+        ang32[e].off = ang_q[e] * sa32 + ang_lms[e];
     }
     std::vector<double> O(3 * ss), ang_diag(3 * slm), O_diag(3 * slm);
     const double *On[3] = {a->Ox, a->Oy, a->Oz};
@@ -301,9 +295,6 @@ tr_status ctx_create(int device, const tr_mesh_view *m, const tr_angular_view *a
         const double *cv = nullptr;
         for (uint32_t e = row[v]; e < row[v + 1]; ++e)
             if (col[e] == v) cv = &coef[static_cast<size_t>(e) * kCoefStride];
-        const double *bv = nullptr;
-        for (uint32_t e = brow[v]; e < brow[v + 1]; ++e)
-            if (bcol[e] == v) bv = &bcoef[static_cast<size_t>(e) * kBCoefStride];
         for (tr_idx lm = 0; lm < slm; ++lm) {
             double d = 0.0;
             if (cv) {
@@ -313,8 +304,8 @@ tr_status ctx_create(int device, const tr_mesh_view *m, const tr_angular_view *a
                     d += a->omega[q] * cv[3 * i + a->omega_pos[q]];
                 }
             }
-            if (bv)
-                for (int n = 0; n < 3; ++n) d += O_diag[n * slm + lm] * bv[n];
+            if (cv)
+                for (int n = 0; n < 3; ++n) d += O_diag[n * slm + lm] * cv[11 + n];
             const double inv = (d != 0.0) ? 1.0 / d : 0.0;
             dinv[static_cast<size_t>(v) * c->aslm + lm] = inv;
             dinv32[static_cast<size_t>(v) * c->aslm32 + lm] = static_cast<float>(inv);
@@ -352,30 +343,23 @@ tr_status ctx_create(int device, const tr_mesh_view *m, const tr_angular_view *a
     o32.aslm = c->aslm32;
     ok(upload(c, &o64.row, row.data(), row.size() * 4));
     ok(upload(c, &o64.col, col.data(), col.size() * 4));
-    ok(upload(c, &o64.brow, brow.data(), brow.size() * 4));
-    ok(upload(c, &o64.bcol, bcol.data(), bcol.size() * 4));
     ok(upload(c, &o64.ang_start, ang_start.data(), ang_start.size() * 4));
-    ok(upload(c, &o64.ang_src, ang_src.data(), ang_src.size() * 2));
+    ok(upload(c, &o64.ang, ang64.data(), ang64.size() * sizeof(AngEntry<double>)));
     ok(upload(c, &o64.coef, coef.data(), coef.size() * 8));
-    ok(upload(c, &o64.bcoef, bcoef.data(), bcoef.size() * 8));
-    ok(upload(c, &o64.ang_w, ang_w.data(), ang_w.size() * 8));
     ok(upload(c, &o64.O, O.data(), O.size() * 8));
     ok(upload(c, &o64.ang_diag, ang_diag.data(), ang_diag.size() * 8));
     ok(upload(c, &o64.O_diag, O_diag.data(), O_diag.size() * 8));
     ok(upload(c, &o64.dinv, dinv.data(), dinv.size() * 8));
+    ok(upload(c, &o64.bmask, bmask.data(), bmask.size()));
+    o64.ang_nnz = o32.ang_nnz = static_cast<uint32_t>(ang_w.size());
     o32.row = o64.row;
     o32.col = o64.col;
-    o32.brow = o64.brow;
-    o32.bcol = o64.bcol;
     o32.ang_start = o64.ang_start;
-    o32.ang_src = o64.ang_src;
+    ok(upload(c, &o32.ang, ang32.data(), ang32.size() * sizeof(AngEntry<float>)));
+    o32.bmask = o64.bmask;
     {
         auto c32 = to_type<float>(coef);
         ok(upload(c, &o32.coef, c32.data(), c32.size() * 4));
-        auto b32 = to_type<float>(bcoef);
-        ok(upload(c, &o32.bcoef, b32.data(), b32.size() * 4));
-        auto w32 = to_type<float>(ang_w);
-        ok(upload(c, &o32.ang_w, w32.data(), w32.size() * 4));
         auto O32 = to_type<float>(O);
         ok(upload(c, &o32.O, O32.data(), O32.size() * 4));
         auto d32 = to_type<float>(ang_diag);
@@ -394,8 +378,10 @@ tr_status ctx_create(int device, const tr_mesh_view *m, const tr_angular_view *a
     ok(upload(c, &c->tet_kv, tetkv.data(), tetkv.size() * 8));
     ok(upload(c, &c->mom_w, mom_w.data(), mom_w.size() * 8));
     ok(upload(c, &c->mom_pos, mom_pos.data(), mom_pos.size() * 4));
-    ok(upload(c, &c->partials, nullptr, 4 * 4096 * sizeof(double)));
+    ok(upload(c, &c->partials, nullptr, 4 * kMaxGrid * sizeof(double)));
     ok(upload(c, &c->counters, nullptr, 16 * sizeof(unsigned int)));
+    ok(upload(c, &c->bar, nullptr, 2 * sizeof(unsigned int)));
+    ok(upload(c, &c->bar_err, nullptr, sizeof(int)));
     ok(upload(c, &c->red_out, nullptr, 16 * sizeof(double)));
     if (e == cudaSuccess) e = cudaMallocHost(reinterpret_cast<void **>(&c->host_pinned), 16 * sizeof(double));
     if (e == cudaSuccess) e = cudaStreamCreate(&c->own_stream);
@@ -407,13 +393,15 @@ tr_status ctx_create(int device, const tr_mesh_view *m, const tr_angular_view *a
     }
     // grids: whole waves of resident 256-thread blocks, capped by the work
     const size_t n64 = static_cast<size_t>(nP) * c->aslm;
-    c->grid_vec = static_cast<int>(std::min<size_t>(static_cast<size_t>(c->num_sms) * 8, (n64 + kBlock - 1) / kBlock));
+    // (up to 4 resident blocks per SM; the grid-reduction tickets scale with it)
+    const size_t waves = static_cast<size_t>(c->num_sms) * 4;
+    auto cap = [&](size_t need) { return static_cast<int>(std::max<size_t>(1, std::min(waves, need))); };
+    c->grid_vec = cap((n64 + kBlock - 1) / kBlock);
+    c->grid_vec64 = cap((n64 / 2 + kBlock - 1) / kBlock);
+    c->grid_vec32 = cap((static_cast<size_t>(nP) * c->aslm32 / 4 + kBlock - 1) / kBlock);
     const uint32_t G = c->aslm <= 8 ? 8 : c->aslm <= 16 ? 16 : 32;
     const size_t groups_per_block = kBlock / G;
-    c->grid_op = static_cast<int>(
-        std::min<size_t>(static_cast<size_t>(c->num_sms) * 8, (nP + groups_per_block - 1) / groups_per_block));
-    c->grid_vec = std::max(c->grid_vec, 1);
-    c->grid_op = std::max(c->grid_op, 1);
+    c->grid_op = cap((nP + groups_per_block - 1) / groups_per_block);
     *out = c;
     return TR_OK;
 }

@@ -13,7 +13,8 @@
 //   S_v[3i+j][lms] = sum_u K_vu[i][j] f[u][lms],
 // which is the reference's sum re-associated (same operator, rounding-level
 // differences).  Boundary couplings E_vu[n] = sum_{faces ∋ v,u, axis n}
-// area (1 + delta_vu) / 12 carry the surface term (kernels.cu:383-438).
+// area (1 + delta_vu) / 12 carry the surface term (kernels.cu:383-438); they
+// sit in the same edge record (every face edge is a tet edge).
 #pragma once
 #include <cuda_runtime.h>
 
@@ -25,26 +26,67 @@
 
 namespace transfer {
 
-constexpr int kCoefStride = 12;  // K[9], M, M0, pad
-constexpr int kBCoefStride = 4;  // E_x, E_y, E_z, pad
+// per-edge coefficient record: K[9] (0-8), M (9), M0 (10), E_x, E_y, E_z
+// (11-13), pad (14-15); 128 bytes in FP64, 64 in FP32
+constexpr int kCoefStride = 16;
 constexpr int kBlock = 256;
+
+// One nonzero of the angular coupling, packed for a single shared-memory
+// load: w = omega_i[lms][lm], off = (3i + pos) * SA + lms, the offset of
+// S_v[3i+pos][lms] in the kernel's shared S table (row stride SA).
+template <typename T>
+struct AngEntry;
+template <>
+struct __align__(8) AngEntry<float> {
+    float w;
+    uint32_t off;
+};
+template <>
+struct __align__(16) AngEntry<double> {
+    double w;
+    uint32_t off;
+    uint32_t pad;
+};
+
+// lanes per vertex (G) and harmonics per lane (H) for a vector stride
+inline constexpr int group_width(uint32_t aslm) { return aslm <= 8 ? 8 : aslm <= 16 ? 16 : 32; }
+inline constexpr int harm_per_lane(uint32_t aslm) {
+    return aslm <= 32 ? 1 : aslm <= 64 ? 2 : aslm <= 96 ? 3 : 4;
+}
+inline constexpr uint32_t s_row_stride(uint32_t aslm) {
+    return static_cast<uint32_t>(group_width(aslm) * harm_per_lane(aslm) + 1);
+}
 
 template <typename T>
 struct OpData {
     uint32_t nP, slm, aslm;          // aslm: vector stride of this precision
     const uint32_t *row;             // [nP+1]
     const uint32_t *col;             // [nnz]
-    const T *coef;                   // [nnz][12]
-    const uint32_t *brow;            // [nP+1]
-    const uint32_t *bcol;            // [nbnz]
-    const T *bcoef;                  // [nbnz][4]
+    const T *coef;                   // [nnz][16]
     const uint32_t *ang_start;       // [slm+1]  entries per output lm
-    const uint16_t *ang_src;         // (3i+pos) << 8 | lms
-    const T *ang_w;                  // omega_i[lms][lm]
+    const AngEntry<T> *ang;          // [nnz]
     const T *O;                      // [3][slm][slm]: O_n[lms][lm]
     const T *ang_diag;               // [3][slm]: omega_i[lm][lm]
     const T *O_diag;                 // [3][slm]: O_n[lm][lm]
     const T *mask;                   // [nP][aslm] reflective constraint or null
+    const uint8_t *bmask;            // [nP] boundary axes present (bits 0..2)
+};
+
+// Arguments of one operator launch.  fin_kind: 0 plain A x; 1 also <x, A x>
+// stored to *fin_out; 2 also the CG step alpha = cgs->nrz / <x, A x>;
+// 3 as 2 with the direction update fused into the gather: the operator is
+// applied to p_new = x + cgs->beta * pold, which is also written to pnew.
+template <typename T>
+struct LhsArgs {
+    const T *x = nullptr;
+    const T *pold = nullptr;
+    T *pnew = nullptr;
+    T *y = nullptr;
+    int fin_kind = 0;
+    double *fin_out = nullptr;
+    struct CgScalars *cgs = nullptr;
+    const int32_t *done = nullptr;
+    uint32_t ang_nnz = 0;
 };
 
 // Scalars of a device-resident CG, one per concurrent solve.
@@ -62,21 +104,43 @@ struct CgScalars {
     uint32_t counter[4];
 };
 
+// Arguments of the persistent CG kernel (one cooperative launch runs up to
+// `iters` iterations).  p0 / p1 alternate as p_old / p_new by the parity of
+// the iteration count; partials holds [3][grid] per-block sums; bar[2] is
+// the grid barrier's arrival count and generation, err its timeout flag.
+template <typename T>
+struct PcgArgs {
+    T *x, *r, *z, *p0, *p1, *Ap;
+    const T *dinv;
+    struct CgScalars *s;
+    double *hist;
+    int hist_cap;
+    double *partials;
+    unsigned int *bar;
+    int *err;
+    uint32_t nvec;
+    int iters;
+};
+constexpr int kMaxGrid = 4096;  // partial-sum slots per reduction
+
 struct CachedGraph {
     cudaGraphExec_t exec = nullptr;
     cudaStream_t stream = nullptr;
     bool valid = false;
 };
-constexpr int kCgChunk = 16;  // CG iterations per captured graph / status read
+constexpr int kCgChunk = 16;       // CG iterations per captured graph / status read (even)
+constexpr int kPersistChunk = 64;  // CG iterations per persistent-kernel launch
 
 template <typename T>
 struct DeviceOp {
-    uint32_t *row = nullptr, *col = nullptr, *brow = nullptr, *bcol = nullptr, *ang_start = nullptr;
-    uint16_t *ang_src = nullptr;
-    T *coef = nullptr, *bcoef = nullptr, *ang_w = nullptr, *O = nullptr, *ang_diag = nullptr, *O_diag = nullptr;
+    uint32_t *row = nullptr, *col = nullptr, *ang_start = nullptr;
+    AngEntry<T> *ang = nullptr;
+    T *coef = nullptr, *O = nullptr, *ang_diag = nullptr, *O_diag = nullptr;
     T *mask = nullptr;
     T *dinv = nullptr;               // Jacobi: 1 / diag(A), [nP][aslm]
+    uint8_t *bmask = nullptr;
     uint32_t aslm = 0;
+    uint32_t ang_nnz = 0;
     OpData<T> data(uint32_t nP, uint32_t slm) const {
         OpData<T> d;
         d.nP = nP;
@@ -85,16 +149,13 @@ struct DeviceOp {
         d.row = row;
         d.col = col;
         d.coef = coef;
-        d.brow = brow;
-        d.bcol = bcol;
-        d.bcoef = bcoef;
         d.ang_start = ang_start;
-        d.ang_src = ang_src;
-        d.ang_w = ang_w;
+        d.ang = ang;
         d.O = O;
         d.ang_diag = ang_diag;
         d.O_diag = O_diag;
         d.mask = mask;
+        d.bmask = bmask;
         return d;
     }
 };
@@ -143,14 +204,17 @@ struct tr_ctx {
     uint32_t *mom_pos = nullptr;
 
     // reductions: per-block partials + last-block counters + results
-    double *partials = nullptr;      // [4][grid max]
+    double *partials = nullptr;      // [4][kMaxGrid]
+    unsigned int *bar = nullptr;     // persistent-kernel grid barrier [2]
+    int *bar_err = nullptr;          // barrier timeout flag
     unsigned int *counters = nullptr;
     double *red_out = nullptr;       // [8]
     double *host_pinned = nullptr;   // [16] pinned staging for scalars
 
     // solver work space (allocated on first solve)
-    double *w64[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-    float *w32[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    double *w64[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // x r p Ap z b p'
+    float *w32[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};           // d r p Ap z p'
+    int grid_vec64 = 0, grid_vec32 = 0;  // vectorised vector kernels
     double *inner[3] = {nullptr, nullptr, nullptr};  // invprec inner CG vectors
     double *io[2] = {nullptr, nullptr};              // tr_solve_host device b / f
     transfer::CgScalars *cg = nullptr;   // [4]: fp64 CG, invprec, outer, inner
@@ -167,11 +231,16 @@ struct tr_ctx {
 namespace transfer {
 
 // operator launches (operator.cu)
-// fin_kind: 0 plain A f; 1 also <f, A f> stored to *fin_out; 2 also the CG
-// step length cgs->alpha = cgs->nrz / <f, A f>.
+// see LhsArgs for fin_kind
+template <typename T>
+cudaError_t launch_lhs(const tr_ctx *c, const DeviceOp<T> &op, LhsArgs<T> a, cudaStream_t s);
 template <typename T>
 cudaError_t launch_lhs(const tr_ctx *c, const DeviceOp<T> &op, const T *f, T *r, int fin_kind, double *fin_out,
                        CgScalars *cgs, const int32_t *done, cudaStream_t s);
+size_t lhs_max_smem(uint32_t aslm, uint32_t slm, uint32_t nnz, bool fp64);
+template <typename T>
+cudaError_t launch_cg_persistent(const tr_ctx *c, const DeviceOp<T> &op, const PcgArgs<T> &a, cudaStream_t s,
+                                 int *grid_out);
 cudaError_t operator_init_attributes();
 template <typename T>
 cudaError_t launch_lhs_diag(const tr_ctx *c, const DeviceOp<T> &op, const T *f, T *r, const int32_t *done,

@@ -2,10 +2,11 @@
 // preconditioner invprec (main.cpp:223-248), a Jacobi variant, and the
 // FP32-in-FP64 defect-correction solve.
 //
-// All CG scalars live in device memory (CgScalars): each iteration is three
-// launches -- A p with <p, A p> and alpha fused, the x/r update with ||r||,
-// the stop test and beta fused, and the new direction -- none of which
-// returns to the host.  Iterations run in chunks; a chunk is captured once
+// All CG scalars live in device memory (CgScalars): each iteration is two
+// launches -- the new direction p = z + beta p_old formed inside the
+// operator's gather, A p with <p, A p> and alpha fused; then the x/r update
+// with ||r||, the stop test and beta fused -- neither returns to the host.
+// The two p buffers swap roles every iteration.  Iterations run in chunks; a chunk is captured once
 // as a CUDA graph and replayed, and the host reads one 8-byte status word
 // per chunk.  Kernels of a chunk that starts after convergence return
 // immediately, so the result is the same as with a per-iteration test.
@@ -23,7 +24,7 @@ namespace transfer {
 
 template <typename T>
 cudaError_t launch_cg_start(const tr_ctx *c, uint32_t aslm, const T *b, T *f, T *r, T *z, T *p, const T *dinv,
-                            CgScalars *s, cudaStream_t st);
+                            CgScalars *s, int zero_p, cudaStream_t st);
 template <typename T>
 cudaError_t launch_cg_update(const tr_ctx *c, uint32_t aslm, T *f, T *r, const T *p, const T *Ap, T *z,
                              const T *dinv, CgScalars *s, double *hist, int hist_cap, int defer_beta,
@@ -70,6 +71,9 @@ static tr_status fail(tr_ctx *c, cudaError_t e, const char *what) {
 
 static cudaStream_t stream_of(const tr_ctx *c) { return c->stream ? c->stream : c->own_stream; }
 
+// smallest relative residual asked of one FP32 inner solve
+constexpr double kMixedInnerFloor = 2e-6;
+
 tr_status ensure_workspace(tr_ctx *c, int hist_cap) {
     const size_t n64 = static_cast<size_t>(c->nP) * c->aslm, n32 = static_cast<size_t>(c->nP) * c->aslm32;
     auto alloc = [&](void **p, size_t bytes) -> bool {
@@ -80,12 +84,12 @@ tr_status ensure_workspace(tr_ctx *c, int hist_cap) {
         c->device_bytes += bytes;
         return true;
     };
-    for (int i = 0; i < 6; ++i)
+    for (int i = 0; i < 7; ++i)
         if (!alloc(reinterpret_cast<void **>(&c->w64[i]), n64 * sizeof(double))) {
             c->last_error = "out of device memory (solver work vectors)";
             return TR_ERR_OUT_OF_MEMORY;
         }
-    for (int i = 0; i < 5; ++i)
+    for (int i = 0; i < 6; ++i)
         if (!alloc(reinterpret_cast<void **>(&c->w32[i]), n32 * sizeof(float))) {
             c->last_error = "out of device memory (solver work vectors)";
             return TR_ERR_OUT_OF_MEMORY;
@@ -146,23 +150,84 @@ static tr_status read_double(tr_ctx *c, const double *d, double *out, cudaStream
     return TR_OK;
 }
 
-// One CG iteration of precision T (three launches, all on device state).
+// One CG iteration of precision T (two launches, all on device state).
+// parity selects which p buffer holds p_old.
 template <typename T>
-static cudaError_t cg_iteration(tr_ctx *c, const DeviceOp<T> &op, uint32_t aslm, T *x, T *r, T *p, T *Ap, T *z,
-                                const T *dinv, CgScalars *s, double *hist, int hcap, cudaStream_t st) {
-    cudaError_t e = launch_lhs<T>(c, op, p, Ap, 2, nullptr, s, &s->done, st);
-    if (e == cudaSuccess) e = launch_cg_update<T>(c, aslm, x, r, p, Ap, z, dinv, s, hist, hcap, 0, st);
-    if (e == cudaSuccess) e = launch_cg_direction<T>(c, aslm, p, dinv ? z : r, s, st);
-    c->launches += 3;
+static cudaError_t cg_iteration(tr_ctx *c, const DeviceOp<T> &op, uint32_t aslm, T *x, T *r, T *const pbuf[2], T *Ap,
+                                T *z, const T *dinv, CgScalars *s, double *hist, int hcap, int parity,
+                                cudaStream_t st) {
+    LhsArgs<T> a;
+    a.x = dinv ? z : r;
+    a.pold = pbuf[parity];
+    a.pnew = pbuf[parity ^ 1];
+    a.y = Ap;
+    a.fin_kind = 3;
+    a.cgs = s;
+    a.done = &s->done;
+    cudaError_t e = launch_lhs<T>(c, op, a, st);
+    if (e == cudaSuccess) e = launch_cg_update<T>(c, aslm, x, r, a.pnew, Ap, z, dinv, s, hist, hcap, 0, st);
+    c->launches += 2;
     return e;
 }
 
 // Runs CG iterations from a started state until done (converged, cap or
-// non-finite).  Graph slot `slot` caches the captured chunk.
+// non-finite).  TR_ENGINE_PERSISTENT: cooperative launches of the persistent
+// kernel, kPersistChunk iterations each; TR_ENGINE_GRAPH: graph slot `slot`
+// caches a captured chunk of kCgChunk two-launch iterations; TR_ENGINE_LAUNCH:
+// the same launches issued directly.  All three give bitwise equal results.
 template <typename T>
-static tr_status run_cg(tr_ctx *c, int slot, const DeviceOp<T> &op, uint32_t aslm, T *x, T *r, T *p, T *Ap, T *z,
-                        const T *dinv, CgScalars *s, double *hist, int hcap, int use_graph, int *iters,
+static tr_status run_cg(tr_ctx *c, int slot, const DeviceOp<T> &op, uint32_t aslm, T *x, T *r, T *const pbuf[2],
+                        T *Ap, T *z, const T *dinv, CgScalars *s, double *hist, int hcap, int engine, int *iters,
                         int *done_out) {
+    if (engine == TR_ENGINE_PERSISTENT) {
+        cudaStream_t st = stream_of(c);
+        PcgArgs<T> a;
+        a.x = x;
+        a.r = r;
+        a.z = z;
+        a.p0 = pbuf[0];
+        a.p1 = pbuf[1];
+        a.Ap = Ap;
+        a.dinv = dinv;
+        a.s = s;
+        a.hist = hist;
+        a.hist_cap = hcap;
+        a.partials = c->partials;
+        a.bar = c->bar;
+        a.err = c->bar_err;
+        a.nvec = static_cast<uint32_t>(static_cast<size_t>(c->nP) * aslm / (16 / sizeof(T)));
+        a.iters = kPersistChunk;
+        int k = 0, done = 0;
+        for (int guard = 0; guard < (1 << 24); ++guard) {
+            int grid = 0;
+            cudaError_t e = launch_cg_persistent<T>(c, op, a, st, &grid);
+            if (e == cudaErrorCooperativeLaunchTooLarge || e == cudaErrorNotSupported) {
+                cudaGetLastError();  // this device cannot co-schedule the grid: replay graphs instead
+                return run_cg<T>(c, slot, op, aslm, x, r, pbuf, Ap, z, dinv, s, hist, hcap, TR_ENGINE_GRAPH,
+                                 iters, done_out);
+            }
+            TRY(e);
+            ++c->launches;
+            int32_t *h = reinterpret_cast<int32_t *>(c->host_pinned);
+            TRY(cudaMemcpyAsync(h, &s->k, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+            TRY(cudaMemcpyAsync(h + 2, c->bar_err, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+            TRY(cudaStreamSynchronize(st));
+            k = h[0];
+            done = h[1];
+            if (h[2]) {
+                c->last_error = "persistent CG: grid barrier timed out";
+                cudaMemsetAsync(c->bar_err, 0, sizeof(int), st);
+                cudaMemsetAsync(c->bar, 0, 2 * sizeof(unsigned int), st);
+                return TR_ERR_CUDA;
+            }
+            if (done) break;
+        }
+        *iters = k;
+        *done_out = done;
+        return TR_OK;
+    }
+    const int use_graph = (engine == TR_ENGINE_GRAPH);
+    static_assert(kCgChunk % 2 == 0, "the p buffers must be back in place after a chunk");
     cudaStream_t st = stream_of(c);
     const int chunk = kCgChunk;
     CachedGraph &g = c->graphs[slot];
@@ -176,7 +241,7 @@ static tr_status run_cg(tr_ctx *c, int slot, const DeviceOp<T> &op, uint32_t asl
         TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         cudaError_t ce = cudaSuccess;
         for (int i = 0; i < chunk && ce == cudaSuccess; ++i)
-            ce = cg_iteration<T>(c, op, aslm, x, r, p, Ap, z, dinv, s, hist, hcap, st);
+            ce = cg_iteration<T>(c, op, aslm, x, r, pbuf, Ap, z, dinv, s, hist, hcap, i & 1, st);
         cudaError_t ee = cudaStreamEndCapture(st, &graph);
         c->launches = counted;
         if (ce != cudaSuccess) return fail(c, ce, "capture of CG chunk");
@@ -191,9 +256,10 @@ static tr_status run_cg(tr_ctx *c, int slot, const DeviceOp<T> &op, uint32_t asl
     for (int guard = 0; guard < (1 << 24); ++guard) {
         if (use_graph) {
             TRY(cudaGraphLaunch(g.exec, st));
-            c->launches += 3 * chunk;
+            c->launches += 2 * chunk;
         } else {
-            for (int i = 0; i < chunk; ++i) TRY((cg_iteration<T>(c, op, aslm, x, r, p, Ap, z, dinv, s, hist, hcap, st)));
+            for (int i = 0; i < chunk; ++i)
+                TRY(cg_iteration<T>(c, op, aslm, x, r, pbuf, Ap, z, dinv, s, hist, hcap, i & 1, st));
         }
         tr_status rs = read_status(c, s, &k, &done, st);
         if (rs != TR_OK) return rs;
@@ -213,7 +279,7 @@ static tr_status invprec(tr_ctx *c, const double *b, double *z, int inner_max, d
     CgScalars *s = c->cg + 1;
     tr_status ts = init_scalars(c, s, inner_tol, inner_max, st);
     if (ts != TR_OK) return ts;
-    LAUNCH(launch_cg_start<double>(c, c->aslm, b, z, ir, nullptr, ip, nullptr, s, st));
+    LAUNCH(launch_cg_start<double>(c, c->aslm, b, z, ir, nullptr, ip, nullptr, s, 0, st));
     int k = 0, done = 0;
     for (int guard = 0; guard < (1 << 24); ++guard) {
         for (int i = 0; i < kCgChunk; ++i) {
@@ -257,10 +323,11 @@ static tr_status solve_fp64(tr_ctx *c, const tr_solve_opts *o, const double *b, 
 
     int k = 0, done = 0;
     if (o->precondition != TR_PREC_REFERENCE) {
-        LAUNCH(launch_cg_start<double>(c, c->aslm, b, x, r, z, p, dinv, s, st));
+        double *const pbuf[2] = {p, c->w64[6]};
+        LAUNCH(launch_cg_start<double>(c, c->aslm, b, x, r, z, p, dinv, s, 1, st));
         int slot = dinv ? 1 : 0;
-        ts = run_cg<double>(c, slot, c->op64, c->aslm, x, r, p, Ap, z, dinv, s, c->dhist, c->hist_cap,
-                            o->use_graph, &k, &done);
+        ts = run_cg<double>(c, slot, c->op64, c->aslm, x, r, pbuf, Ap, z, dinv, s, c->dhist, c->hist_cap,
+                            o->engine, &k, &done);
         if (ts != TR_OK) return ts;
         rep->lhs_applications_f64 += k;
     } else {
@@ -316,7 +383,6 @@ static tr_status solve_mixed(tr_ctx *c, const tr_solve_opts *o, const double *b,
     const float *dinv = (o->precondition == TR_PREC_JACOBI) ? c->op32.dinv : nullptr;
     const int max_outer = o->max_outer > 0 ? o->max_outer : 30;
     const int inner_max = o->inner_max_iter > 0 ? o->inner_max_iter : (o->max_iter > 0 ? o->max_iter : 1000);
-    const double inner_tol = o->inner_tol > 0 ? o->inner_tol : 1e-4;
 
     tr_status ts = init_scalars(c, so, 0.0, 0, st);
     if (ts != TR_OK) return ts;
@@ -334,12 +400,18 @@ static tr_status solve_mixed(tr_ctx *c, const tr_solve_opts *o, const double *b,
     bool converged = (rn < target);
     while (!converged && outer < max_outer && total < (o->max_iter > 0 ? o->max_iter : 1 << 30)) {
         LAUNCH(launch_to_f32(c, r64, r, so, st));
+        // each FP32 solve aims at what is still missing to the target
+        // (relative to the normalised residual), floored where FP32 CG
+        // stops gaining true accuracy
+        const double inner_tol =
+            o->inner_tol > 0 ? o->inner_tol : std::min(0.5, std::max(0.3 * target / rn, kMixedInnerFloor));
         ts = init_scalars(c, si, inner_tol, inner_max, st);
         if (ts != TR_OK) return ts;
-        LAUNCH(launch_cg_start<float>(c, c->aslm32, r, d, r, z, p, dinv, si, st));
+        LAUNCH(launch_cg_start<float>(c, c->aslm32, r, d, r, z, p, dinv, si, 1, st));
         int k = 0, done = 0;
         int slot = dinv ? 3 : 2;
-        ts = run_cg<float>(c, slot, c->op32, c->aslm32, d, r, p, Ap, z, dinv, si, nullptr, 0, o->use_graph, &k,
+        float *const pbuf[2] = {p, c->w32[5]};
+        ts = run_cg<float>(c, slot, c->op32, c->aslm32, d, r, pbuf, Ap, z, dinv, si, nullptr, 0, o->engine, &k,
                            &done);
         if (ts != TR_OK) return ts;
         total += k;

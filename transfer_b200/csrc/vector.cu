@@ -38,31 +38,73 @@ __global__ void __launch_bounds__(kBlock) k_dot(size_t n, uint32_t aslm, uint32_
     if (grid_reduce<1>(v, partials, counter, tot) && threadIdx.x == 0) *out = tot[0];
 }
 
+// 16-byte vectors of T and component access (indices are compile-time
+// constants after unrolling)
+template <typename T>
+struct VecT;
+template <>
+struct VecT<double> {
+    typedef double2 V;
+    static constexpr int W = 2;
+    __device__ static double get(const V &v, int k) { return k == 0 ? v.x : v.y; }
+    __device__ static void set(V &v, int k, double a) {
+        if (k == 0) v.x = a;
+        else v.y = a;
+    }
+};
+template <>
+struct VecT<float> {
+    typedef float4 V;
+    static constexpr int W = 4;
+    __device__ static float get(const V &v, int k) { return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w; }
+    __device__ static void set(V &v, int k, float a) {
+        if (k == 0) v.x = a;
+        else if (k == 1) v.y = a;
+        else if (k == 2) v.z = a;
+        else v.w = a;
+    }
+};
+
 // CG update (main.cpp:144-154): f += alpha p; r -= alpha Ap; optional
 // Jacobi z = D^-1 r; then, in the last block, the stop test on ||r||, the
-// residual history and beta = (r,z)_new / (r,z)_old.
+// residual history and beta = (r,z)_new / (r,z)_old.  n is in 16-byte
+// vectors (aslm is a multiple of the vector width, so a vector never
+// straddles two vertices).
 template <typename T>
-__global__ void __launch_bounds__(kBlock) k_cg_update(size_t n, uint32_t aslm, uint32_t slm, T *__restrict__ f,
+__global__ void __launch_bounds__(kBlock) k_cg_update(size_t nvec, uint32_t aslm, uint32_t slm, T *__restrict__ f,
                                                       T *__restrict__ r, const T *__restrict__ p,
                                                       const T *__restrict__ Ap, T *__restrict__ z,
                                                       const T *__restrict__ dinv, CgScalars *s, double *partials,
                                                       unsigned int *counter, double *hist, int hist_cap,
                                                       int defer_beta) {
     if (s->done) return;
+    typedef VecT<T> O;
+    typedef typename O::V V;
     const T alpha = static_cast<T>(s->alpha);
     double rr = 0.0, rz = 0.0;
-    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
-         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-        f[i] = fma(alpha, p[i], f[i]);
-        const T ri = fma(-alpha, Ap[i], r[i]);
-        r[i] = ri;
-        const bool live = static_cast<uint32_t>(i % aslm) < slm;
-        if (dinv) {
-            const T zi = dinv[i] * ri;
-            z[i] = zi;
-            if (live) rz += static_cast<double>(ri) * static_cast<double>(zi);
+    for (size_t iv = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; iv < nvec;
+         iv += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        V fv = reinterpret_cast<const V *>(f)[iv], rv = reinterpret_cast<const V *>(r)[iv];
+        const V pv = reinterpret_cast<const V *>(p)[iv], av = reinterpret_cast<const V *>(Ap)[iv];
+        V dv, zv;
+        if (dinv) dv = reinterpret_cast<const V *>(dinv)[iv];
+        const uint32_t lm0 = static_cast<uint32_t>((iv * O::W) % aslm);
+#pragma unroll
+        for (int k = 0; k < O::W; ++k) {
+            O::set(fv, k, fma(alpha, O::get(pv, k), O::get(fv, k)));
+            const T ri = fma(-alpha, O::get(av, k), O::get(rv, k));
+            O::set(rv, k, ri);
+            const bool live = lm0 + k < slm;
+            if (dinv) {
+                const T zi = O::get(dv, k) * ri;
+                O::set(zv, k, zi);
+                if (live) rz += static_cast<double>(ri) * static_cast<double>(zi);
+            }
+            if (live) rr += static_cast<double>(ri) * static_cast<double>(ri);
         }
-        if (live) rr += static_cast<double>(ri) * static_cast<double>(ri);
+        reinterpret_cast<V *>(f)[iv] = fv;
+        reinterpret_cast<V *>(r)[iv] = rv;
+        if (dinv) reinterpret_cast<V *>(z)[iv] = zv;
     }
     double v[2] = {rr, rz}, tot[2];
     if (grid_reduce<2>(v, partials, counter, tot) && threadIdx.x == 0) {
@@ -95,13 +137,14 @@ __global__ void __launch_bounds__(kBlock) k_cg_direction(size_t n, T *__restrict
         p[i] = fma(beta, p[i], z[i]);
 }
 
-// CG start: r = b - A f0 is r = b for f0 = 0; z = D^-1 r or r; p = z;
-// nrz = (r, z).  Writes r, z (if Jacobi) and p; finishes the scalars.
+// CG start: r = b - A f0 is r = b for f0 = 0; z = D^-1 r or r; nrz = (r, z);
+// p = z, or, for the fused-direction iteration, p = 0 with beta = 0 (the
+// first operator launch then forms p = z + 0 p).
 template <typename T>
 __global__ void __launch_bounds__(kBlock) k_cg_start(size_t n, uint32_t aslm, uint32_t slm, const T *__restrict__ b,
                                                      T *__restrict__ f, T *__restrict__ r, T *__restrict__ z,
                                                      T *__restrict__ p, const T *__restrict__ dinv, CgScalars *s,
-                                                     double *partials, unsigned int *counter) {
+                                                     double *partials, unsigned int *counter, int zero_p) {
     double rz = 0.0, bb = 0.0;
     for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
          i += static_cast<size_t>(gridDim.x) * blockDim.x) {
@@ -110,7 +153,7 @@ __global__ void __launch_bounds__(kBlock) k_cg_start(size_t n, uint32_t aslm, ui
         r[i] = bi;
         const T zi = dinv ? dinv[i] * bi : bi;
         if (dinv) z[i] = zi;
-        p[i] = zi;
+        p[i] = zero_p ? T(0) : zi;
         if (static_cast<uint32_t>(i % aslm) < slm) {
             rz += static_cast<double>(bi) * static_cast<double>(zi);
             bb += static_cast<double>(bi) * static_cast<double>(bi);
@@ -120,6 +163,7 @@ __global__ void __launch_bounds__(kBlock) k_cg_start(size_t n, uint32_t aslm, ui
     if (grid_reduce<2>(v, partials, counter, tot) && threadIdx.x == 0) {
         s->nrz = tot[0];
         s->rr = tot[1];
+        s->beta = 0.0;
         s->k = 0;
         s->done = (tot[0] == 0.0) ? 1 : 0;
     }
@@ -235,18 +279,19 @@ template cudaError_t launch_dot<float, float>(const tr_ctx *, uint32_t, const fl
 
 template <typename T>
 cudaError_t launch_cg_start(const tr_ctx *c, uint32_t aslm, const T *b, T *f, T *r, T *z, T *p, const T *dinv,
-                            CgScalars *s, cudaStream_t st) {
+                            CgScalars *s, int zero_p, cudaStream_t st) {
     k_cg_start<T><<<c->grid_vec, kBlock, 0, st>>>(static_cast<size_t>(c->nP) * aslm, aslm, c->slm, b, f, r, z, p,
-                                                  dinv, s, c->partials, c->counters + 2);
+                                                  dinv, s, c->partials, c->counters + 2, zero_p);
     return cudaGetLastError();
 }
 template <typename T>
 cudaError_t launch_cg_update(const tr_ctx *c, uint32_t aslm, T *f, T *r, const T *p, const T *Ap, T *z,
                              const T *dinv, CgScalars *s, double *hist, int hist_cap, int defer_beta,
                              cudaStream_t st) {
-    k_cg_update<T><<<c->grid_vec, kBlock, 0, st>>>(static_cast<size_t>(c->nP) * aslm, aslm, c->slm, f, r, p, Ap, z,
-                                                   dinv, s, c->partials, c->counters + 2, hist, hist_cap,
-                                                   defer_beta);
+    const size_t nvec = static_cast<size_t>(c->nP) * aslm / VecT<T>::W;
+    const int grid = sizeof(T) == 8 ? c->grid_vec64 : c->grid_vec32;
+    k_cg_update<T><<<grid, kBlock, 0, st>>>(nvec, aslm, c->slm, f, r, p, Ap, z, dinv, s, c->partials,
+                                            c->counters + 2, hist, hist_cap, defer_beta);
     return cudaGetLastError();
 }
 template <typename T>
@@ -256,9 +301,9 @@ cudaError_t launch_cg_direction(const tr_ctx *c, uint32_t aslm, T *p, const T *z
     return cudaGetLastError();
 }
 template cudaError_t launch_cg_start<double>(const tr_ctx *, uint32_t, const double *, double *, double *, double *,
-                                             double *, const double *, CgScalars *, cudaStream_t);
+                                             double *, const double *, CgScalars *, int, cudaStream_t);
 template cudaError_t launch_cg_start<float>(const tr_ctx *, uint32_t, const float *, float *, float *, float *,
-                                            float *, const float *, CgScalars *, cudaStream_t);
+                                            float *, const float *, CgScalars *, int, cudaStream_t);
 template cudaError_t launch_cg_update<double>(const tr_ctx *, uint32_t, double *, double *, const double *,
                                               const double *, double *, const double *, CgScalars *, double *, int,
                                               int, cudaStream_t);
