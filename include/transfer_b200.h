@@ -145,6 +145,13 @@ tr_status tr_ctx_create_ex(int device, const tr_mesh_view *mesh,
                            const tr_physics_view *phys, tr_ctx **out);
 tr_status tr_ctx_destroy(tr_ctx *ctx);
 tr_status tr_ctx_info_get(const tr_ctx *ctx, tr_ctx_info *info);
+/* Operator kernel family (no reference counterpart; results agree to
+ * rounding): TR_OPERATOR_TENSOR computes each vertex's edge sums as a small
+ * dense product on the tensor cores (FP32: split-TF32, FP64: DMMA);
+ * TR_OPERATOR_SIMT accumulates them with FMA instructions.  A new context
+ * uses TENSOR for FP64 and SIMT for FP32; this call sets both precisions. */
+enum { TR_OPERATOR_SIMT = 0, TR_OPERATOR_TENSOR = 1 };
+tr_status tr_ctx_set_operator(tr_ctx *ctx, int kind);
 /* cudaStream_t passed as void*; NULL selects the context's own stream. */
 tr_status tr_ctx_set_stream(tr_ctx *ctx, void *stream);
 const char *tr_last_error(const tr_ctx *ctx);

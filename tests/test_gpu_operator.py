@@ -31,10 +31,15 @@ def setup(md, ad, **phys):
     return ctx, O
 
 
+KINDS = [tr.TR_OPERATOR_TENSOR, tr.TR_OPERATOR_SIMT]
+
+
+@pytest.mark.parametrize("kind", KINDS)
 @pytest.mark.parametrize("maxk", range(8))
-def test_lhs_matches_oracle(cuda, maxk):
+def test_lhs_matches_oracle(cuda, maxk, kind):
     md, ad = small_mesh(), golden_angular(maxk)
     ctx, O = setup(md, ad)
+    ctx.set_operator(kind)
     f = random_vector(md.nP, ad.slm, ctx.aslm, seed=maxk)
     Af = ctx.allocVector()
     ctx.computeLhs(dev(f), Af)
@@ -43,9 +48,11 @@ def test_lhs_matches_oracle(cuda, maxk):
     assert np.all(host(Af).reshape(md.nP, -1)[:, ad.slm:] == 0)
 
 
-def test_lhs_config1_matches_oracle(cuda):
+@pytest.mark.parametrize("kind", KINDS)
+def test_lhs_config1_matches_oracle(cuda, kind):
     md, ad = c1_mesh(), golden_angular(1)
     ctx, O = setup(md, ad)
+    ctx.set_operator(kind)
     assert (ctx.nP, ctx.nT, ctx.nF) == (4913, 24576, 3072)
     f = random_vector(md.nP, ad.slm, ctx.aslm, seed=5)
     Af = ctx.allocVector()
@@ -108,10 +115,12 @@ def test_reductions_are_deterministic(cuda):
     assert torch.equal(Af1, Af2)
 
 
-@pytest.mark.parametrize("maxk", [1, 3, 5])
-def test_f32_entry_points(cuda, maxk):
+@pytest.mark.parametrize("kind", KINDS)
+@pytest.mark.parametrize("maxk", [1, 3, 5, 7])
+def test_f32_entry_points(cuda, maxk, kind):
     md, ad = small_mesh(), golden_angular(maxk)
     ctx, O = setup(md, ad)
+    ctx.set_operator(kind)
     f = random_vector(md.nP, ad.slm, ctx.aslm, seed=20 + maxk)
     f32 = repad(f, md.nP, ad.slm, ctx.aslm, ctx.aslm_f32).astype(np.float32)
     Af = ctx.allocVector(torch.float32)

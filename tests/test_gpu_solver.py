@@ -117,6 +117,12 @@ def test_engines_agree(cuda):
     fm, rm = ctx.solve(mode=tr.TR_MODE_MIXED, tol=1e-10, relative=1, engine=tr.TR_ENGINE_GRAPH)
     fn, rn = ctx.solve(mode=tr.TR_MODE_MIXED, tol=1e-10, relative=1, engine=tr.TR_ENGINE_PERSISTENT)
     assert rm.converged and rn.converged and rel_err(host(fn), host(fm)) < 1e-8
+    # the SIMT operator family gives the same solutions
+    ctx.set_operator(tr.TR_OPERATOR_SIMT)
+    fs, rs = ctx.solve(tol=1e-10, relative=1, engine=tr.TR_ENGINE_PERSISTENT)
+    assert abs(rs.iterations - r4.iterations) <= 1 and rel_err(host(fs), host(f4)) < 1e-9
+    fs2, rs2 = ctx.solve(mode=tr.TR_MODE_MIXED, tol=1e-10, relative=1)
+    assert rs2.converged and rel_err(host(fs2), host(fm)) < 1e-8
 
 
 def test_host_buffers_and_explicit_rhs(cuda):

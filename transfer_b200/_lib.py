@@ -30,6 +30,7 @@ TR_SURFACE_AXIS, TR_SURFACE_EXACT = 0, 1
 TR_PREC_NONE, TR_PREC_REFERENCE, TR_PREC_JACOBI = 0, 1, 2
 TR_MODE_FP64, TR_MODE_MIXED = 0, 1
 TR_ENGINE_PERSISTENT, TR_ENGINE_GRAPH, TR_ENGINE_LAUNCH = 0, 1, 2
+TR_OPERATOR_SIMT, TR_OPERATOR_TENSOR = 0, 1
 
 
 class tr_tetrahedron(C.Structure):
@@ -105,6 +106,7 @@ PROTOTYPES = [
                              C.POINTER(tr_physics_view), C.POINTER(P)]),
     ("tr_ctx_destroy", S, [P]),
     ("tr_ctx_info_get", S, [P, C.POINTER(tr_ctx_info)]),
+    ("tr_ctx_set_operator", S, [P, I]),
     ("tr_ctx_set_stream", S, [P, P]),
     ("tr_compute_lhs", S, [P, P, P]),
     ("tr_compute_lhs_diag", S, [P, P, P]),

@@ -425,6 +425,10 @@ class CudaContext:
                                    C.byref(extra), C.byref(steps)))
         return lmax.value, extra.value, steps.value
 
+    def set_operator(self, kind):
+        """TR_OPERATOR_TENSOR (default) or TR_OPERATOR_SIMT."""
+        self._c(lib.tr_ctx_set_operator(self._h, int(kind)))
+
     def set_stream(self, stream):
         self._c(lib.tr_ctx_set_stream(self._h, _ptr(stream) if stream is not None else None))
 

@@ -148,6 +148,15 @@ tr_status tr_ctx_info_get(const tr_ctx *c, tr_ctx_info *info) {
     return TR_OK;
 }
 
+tr_status tr_ctx_set_operator(tr_ctx *c, int kind) {
+    CHECK_CTX(c);
+    if (kind != TR_OPERATOR_SIMT && kind != TR_OPERATOR_TENSOR)
+        return set_err(c, TR_ERR_INVALID_ARG, "operator kind must be TR_OPERATOR_SIMT or TR_OPERATOR_TENSOR");
+    c->op64.kind = c->op32.kind = kind;
+    for (auto &g : c->graphs) g.valid = false;  // captured launches name the old kernels
+    return TR_OK;
+}
+
 tr_status tr_ctx_set_stream(tr_ctx *c, void *stream) {
     CHECK_CTX(c);
     c->stream = static_cast<cudaStream_t>(stream);

@@ -20,6 +20,7 @@ namespace {
 
 struct Edge {
     uint32_t u;
+    double k9[9];             // K[i][j] before symmetrisation
     double c[kCoefStride];
 };
 
@@ -193,6 +194,7 @@ tr_status ctx_create(int device, const tr_mesh_view *m, const tr_angular_view *a
                 if (e.u == u) return e;
             Edge ne;
             ne.u = u;
+            std::memset(ne.k9, 0, sizeof(ne.k9));
             std::memset(ne.c, 0, sizeof(ne.c));
             E.push_back(ne);
             return E.back();
@@ -204,10 +206,10 @@ tr_status ctx_create(int device, const tr_mesh_view *m, const tr_angular_view *a
             for (int k = 0; k < 4; ++k) {
                 Edge &e = find(T.p[k]);
                 for (int i = 0; i < 3; ++i)
-                    for (int jj = 0; jj < 3; ++jj) e.c[3 * i + jj] += T.s[loc][i] / kv * (1.0 / 9.0) * T.s[k][jj];
+                    for (int jj = 0; jj < 3; ++jj) e.k9[3 * i + jj] += T.s[loc][i] / kv * (1.0 / 9.0) * T.s[k][jj];
                 const double mult = (k == static_cast<int>(loc)) ? 2.0 : 1.0;
-                e.c[9] += kv * mult * (1.0 / 20.0);
-                e.c[10] += ka * mult * (1.0 / 20.0);
+                e.c[kRowM] += kv * mult * (1.0 / 20.0);
+                e.c[kRowM0] += ka * mult * (1.0 / 20.0);
             }
         }
         for (tr_idx j = m->facestart[v]; j < m->facestart[v + 1]; ++j) {
@@ -219,7 +221,15 @@ tr_status ctx_create(int device, const tr_mesh_view *m, const tr_angular_view *a
             const int ax = face_axis(F, &surf);
             if (kind == TR_BC_INCIDENT) inflow[3ULL * v + ax] += finc[fi] * surf * (1.0 / 3.0);
             for (int k = 0; k < 3; ++k)
-                find(F.p[k]).c[11 + ax] += surf * ((k == static_cast<int>(loc)) ? 2.0 : 1.0) * (1.0 / 12.0);
+                find(F.p[k]).c[kRowE + ax] += surf * ((k == static_cast<int>(loc)) ? 2.0 : 1.0) * (1.0 / 12.0);
+        }
+        for (Edge &e : E) {  // symmetric stiffness rows
+            e.c[0] = e.k9[0];
+            e.c[1] = e.k9[4];
+            e.c[2] = e.k9[8];
+            e.c[3] = e.k9[1] + e.k9[3];
+            e.c[4] = e.k9[2] + e.k9[6];
+            e.c[5] = e.k9[5] + e.k9[7];
         }
         std::sort(E.begin(), E.end(), [](const Edge &x, const Edge &y) { return x.u < y.u; });
     }
@@ -237,7 +247,7 @@ tr_status ctx_create(int device, const tr_mesh_view *m, const tr_angular_view *a
             std::memcpy(&coef[o * kCoefStride], e.c, sizeof(e.c));
             bool any = false;
             for (int n = 0; n < 3; ++n)
-                if (e.c[11 + n] != 0.0) {
+                if (e.c[kRowE + n] != 0.0) {
                     bmask[v] |= static_cast<uint8_t>(1u << n);
                     any = true;
                 }
@@ -252,33 +262,47 @@ tr_status ctx_create(int device, const tr_mesh_view *m, const tr_angular_view *a
     double maxabs = 0.0;
     for (size_t i = 0; i < 3 * ss; ++i) maxabs = std::max(maxabs, std::fabs(a->omega[i]));
     const double drop = 1e-14 * maxabs;
-    std::vector<uint32_t> ang_start(slm + 1, 0);
-    std::vector<uint32_t> ang_q, ang_lms;  // (3i+pos), lms of every kept entry
-    std::vector<double> ang_w;
+    // per harmonic lm: sum_q,lms W[q][lms] S_sym[q][lms], merging (i,j) and
+    // (j,i) into the symmetric row q (kernels.cu:276-282 reads
+    // omega[i][lms][lm] and omega_pos[i][lms][lm])
+    auto sym_row = [](int i, int j) { return i == j ? i : (i + j == 1 ? 3 : (i + j == 2 ? 4 : 5)); };
+    std::vector<std::vector<std::pair<uint32_t, double>>> lists(slm);  // (q * 256 + lms, w)
+    uint32_t ckmax = 0;
     for (tr_idx lm = 0; lm < slm; ++lm) {
+        std::vector<double> wsum(kSymRows * slm, 0.0);
+        std::vector<char> used(kSymRows * slm, 0);
         for (int i = 0; i < 3; ++i)
             for (tr_idx lms = 0; lms < slm; ++lms) {
-                // kernels.cu:276-282 reads omega[i][lms][lm] and omega_pos[i][lms][lm]
                 const size_t q = (static_cast<size_t>(i) * slm + lms) * slm + lm;
                 const double w = a->omega[q];
                 if (std::fabs(w) <= drop) continue;
-                ang_q.push_back(3 * i + a->omega_pos[q]);
-                ang_lms.push_back(lms);
-                ang_w.push_back(w);
+                const int r = sym_row(i, static_cast<int>(a->omega_pos[q]));
+                wsum[r * slm + lms] += (r < 3) ? w : 0.5 * w;  // S_sym = S_ij + S_ji
+                used[r * slm + lms] = 1;
             }
-        ang_start[lm + 1] = static_cast<uint32_t>(ang_w.size());
+        for (int r = 0; r < kSymRows; ++r)
+            for (tr_idx lms = 0; lms < slm; ++lms)
+                if (used[r * slm + lms]) lists[lm].push_back({static_cast<uint32_t>(r * 256 + lms), wsum[r * slm + lms]});
+        ckmax = std::max<uint32_t>(ckmax, static_cast<uint32_t>(lists[lm].size()));
     }
-    const size_t nang = ang_w.size();
-    std::vector<AngEntry<double>> ang64(std::max<size_t>(nang, 1));
-    std::vector<AngEntry<float>> ang32(std::max<size_t>(nang, 1));
+    const uint32_t aslm_max = std::max((slm + 7) & ~7u, (slm + 15) & ~15u);
+    const uint32_t cls = (aslm_max + 31) & ~31u;
     const uint32_t sa64 = s_row_stride((slm + 7) & ~7u), sa32 = s_row_stride((slm + 15) & ~15u);
-    for (size_t e = 0; e < nang; ++e) {
-        ang64[e].w = ang_w[e];
-        ang64[e].off = ang_q[e] * sa64 + ang_lms[e];
-        ang64[e].pad = 0;
-        ang32[e].w = static_cast<float>(ang_w[e]);
-        ang32[e].off = ang_q[e] * sa32 + ang_lms[e];
-    }
+    const uint32_t satc = (slm + 7) / 8 * 8 + 1;
+    const size_t ncon = std::max<size_t>(static_cast<size_t>(ckmax) * cls, 1);
+    std::vector<double> cw64(ncon, 0.0);
+    std::vector<float> cw32(ncon, 0.0f);
+    std::vector<uint16_t> co64(ncon, 0), co32(ncon, 0), cotc(ncon, 0);
+    for (tr_idx lm = 0; lm < slm; ++lm)
+        for (size_t k = 0; k < lists[lm].size(); ++k) {
+            const uint32_t r = lists[lm][k].first >> 8, lms = lists[lm][k].first & 255u;
+            const size_t o = k * cls + lm;
+            cw64[o] = lists[lm][k].second;
+            cw32[o] = static_cast<float>(lists[lm][k].second);
+            co64[o] = static_cast<uint16_t>(r * sa64 + lms);
+            co32[o] = static_cast<uint16_t>(r * sa32 + lms);
+            cotc[o] = static_cast<uint16_t>(r * satc + lms);
+        }
     std::vector<double> O(3 * ss), ang_diag(3 * slm), O_diag(3 * slm);
     const double *On[3] = {a->Ox, a->Oy, a->Oz};
     for (int n = 0; n < 3; ++n) {
@@ -298,14 +322,14 @@ tr_status ctx_create(int device, const tr_mesh_view *m, const tr_angular_view *a
         for (tr_idx lm = 0; lm < slm; ++lm) {
             double d = 0.0;
             if (cv) {
-                d += (lm == 0) ? cv[10] : cv[9];
-                for (int i = 0; i < 3; ++i) {
+                d += (lm == 0) ? cv[kRowM0] : cv[kRowM];
+                for (int i = 0; i < 3; ++i) {  // omega_pos[i][lm][lm] = i: the K_ii rows
                     const size_t q = (static_cast<size_t>(i) * slm + lm) * slm + lm;
-                    d += a->omega[q] * cv[3 * i + a->omega_pos[q]];
+                    d += a->omega[q] * cv[i];
                 }
             }
             if (cv)
-                for (int n = 0; n < 3; ++n) d += O_diag[n * slm + lm] * cv[11 + n];
+                for (int n = 0; n < 3; ++n) d += O_diag[n * slm + lm] * cv[kRowE + n];
             const double inv = (d != 0.0) ? 1.0 / d : 0.0;
             dinv[static_cast<size_t>(v) * c->aslm + lm] = inv;
             dinv32[static_cast<size_t>(v) * c->aslm32 + lm] = static_cast<float>(inv);
@@ -341,21 +365,27 @@ tr_status ctx_create(int device, const tr_mesh_view *m, const tr_angular_view *a
     DeviceOp<float> &o32 = c->op32;
     o64.aslm = c->aslm;
     o32.aslm = c->aslm32;
+    o64.kind = TR_OPERATOR_TENSOR;  // DMMA edge sums: fastest FP64 form measured
+    o32.kind = TR_OPERATOR_SIMT;    // FMA edge sums: split-TF32 needs 3 products
     ok(upload(c, &o64.row, row.data(), row.size() * 4));
     ok(upload(c, &o64.col, col.data(), col.size() * 4));
-    ok(upload(c, &o64.ang_start, ang_start.data(), ang_start.size() * 4));
-    ok(upload(c, &o64.ang, ang64.data(), ang64.size() * sizeof(AngEntry<double>)));
+    o64.ckmax = o32.ckmax = ckmax;
+    o64.cls = o32.cls = cls;
+    ok(upload(c, &o64.cw, cw64.data(), cw64.size() * 8));
+    ok(upload(c, &o32.cw, cw32.data(), cw32.size() * 4));
+    ok(upload(c, &o64.co, co64.data(), co64.size() * 2));
+    ok(upload(c, &o32.co, co32.data(), co32.size() * 2));
+    ok(upload(c, &o64.co_tc, cotc.data(), cotc.size() * 2));
+    o32.co_tc = o64.co_tc;
     ok(upload(c, &o64.coef, coef.data(), coef.size() * 8));
     ok(upload(c, &o64.O, O.data(), O.size() * 8));
     ok(upload(c, &o64.ang_diag, ang_diag.data(), ang_diag.size() * 8));
     ok(upload(c, &o64.O_diag, O_diag.data(), O_diag.size() * 8));
     ok(upload(c, &o64.dinv, dinv.data(), dinv.size() * 8));
     ok(upload(c, &o64.bmask, bmask.data(), bmask.size()));
-    o64.ang_nnz = o32.ang_nnz = static_cast<uint32_t>(ang_w.size());
+    o64.ang_nnz = o32.ang_nnz = static_cast<uint32_t>(ncon);
     o32.row = o64.row;
     o32.col = o64.col;
-    o32.ang_start = o64.ang_start;
-    ok(upload(c, &o32.ang, ang32.data(), ang32.size() * sizeof(AngEntry<float>)));
     o32.bmask = o64.bmask;
     {
         auto c32 = to_type<float>(coef);

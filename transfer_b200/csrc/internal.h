@@ -26,28 +26,21 @@
 
 namespace transfer {
 
-// per-edge coefficient record: K[9] (0-8), M (9), M0 (10), E_x, E_y, E_z
-// (11-13), pad (14-15); 128 bytes in FP64, 64 in FP32
+// Per-edge coefficient record (16 values; 128 bytes in FP64, 64 in FP32):
+//   0-5   the symmetric stiffness sums K_xx, K_yy, K_zz, K_xy+K_yx,
+//         K_xz+K_zx, K_yz+K_zy  (the angular weights satisfy
+//         omega_ij = omega_ji, so only S_ij + S_ji enters the operator)
+//   6, 7  M, M0 (mass; M0 for l = 0)
+//   8-10  E_x, E_y, E_z (boundary)      11-15 zero
 constexpr int kCoefStride = 16;
+constexpr int kSymRows = 6, kRowM = 6, kRowM0 = 7, kRowE = 8;
 constexpr int kBlock = 256;
 
-// One nonzero of the angular coupling, packed for a single shared-memory
-// load: w = omega_i[lms][lm], off = (3i + pos) * SA + lms, the offset of
-// S_v[3i+pos][lms] in the kernel's shared S table (row stride SA).
-template <typename T>
-struct AngEntry;
-template <>
-struct __align__(8) AngEntry<float> {
-    float w;
-    uint32_t off;
-};
-template <>
-struct __align__(16) AngEntry<double> {
-    double w;
-    uint32_t off;
-    uint32_t pad;
-};
-
+// The angular coupling out[lm] = sum_k cw[k][lm] * S[co[k][lm]] is stored
+// lane-major: entry k of every harmonic lm is contiguous (cw[k * cls + lm]),
+// lists padded to the longest one (ckmax) with zero weights, so each step
+// of the contraction is one coalesced, conflict-free load per table.  co is
+// the offset q * SA + lms of S_sym[q][lms] in the kernel's S table.
 // lanes per vertex (G) and harmonics per lane (H) for a vector stride
 inline constexpr int group_width(uint32_t aslm) { return aslm <= 8 ? 8 : aslm <= 16 ? 16 : 32; }
 inline constexpr int harm_per_lane(uint32_t aslm) {
@@ -63,8 +56,10 @@ struct OpData {
     const uint32_t *row;             // [nP+1]
     const uint32_t *col;             // [nnz]
     const T *coef;                   // [nnz][16]
-    const uint32_t *ang_start;       // [slm+1]  entries per output lm
-    const AngEntry<T> *ang;          // [nnz]
+    uint32_t ckmax, cls;             // contraction: entries per lm, lane stride
+    const T *cw;                     // [ckmax][cls] weights
+    const uint16_t *co;              // [ckmax][cls] offsets, SIMT S table
+    const uint16_t *co_tc;           // [ckmax][cls] offsets, tensor-core C table
     const T *O;                      // [3][slm][slm]: O_n[lms][lm]
     const T *ang_diag;               // [3][slm]: omega_i[lm][lm]
     const T *O_diag;                 // [3][slm]: O_n[lm][lm]
@@ -133,14 +128,17 @@ constexpr int kPersistChunk = 64;  // CG iterations per persistent-kernel launch
 
 template <typename T>
 struct DeviceOp {
-    uint32_t *row = nullptr, *col = nullptr, *ang_start = nullptr;
-    AngEntry<T> *ang = nullptr;
+    uint32_t *row = nullptr, *col = nullptr;
+    uint32_t ckmax = 0, cls = 0;
+    T *cw = nullptr;
+    uint16_t *co = nullptr, *co_tc = nullptr;
     T *coef = nullptr, *O = nullptr, *ang_diag = nullptr, *O_diag = nullptr;
     T *mask = nullptr;
     T *dinv = nullptr;               // Jacobi: 1 / diag(A), [nP][aslm]
     uint8_t *bmask = nullptr;
     uint32_t aslm = 0;
-    uint32_t ang_nnz = 0;
+    uint32_t ang_nnz = 0;            // ckmax * cls
+    int kind = TR_OPERATOR_TENSOR;   // TR_OPERATOR_*
     OpData<T> data(uint32_t nP, uint32_t slm) const {
         OpData<T> d;
         d.nP = nP;
@@ -149,8 +147,11 @@ struct DeviceOp {
         d.row = row;
         d.col = col;
         d.coef = coef;
-        d.ang_start = ang_start;
-        d.ang = ang;
+        d.ckmax = ckmax;
+        d.cls = cls;
+        d.cw = cw;
+        d.co = co;
+        d.co_tc = co_tc;
         d.O = O;
         d.ang_diag = ang_diag;
         d.O_diag = O_diag;
@@ -237,7 +238,6 @@ cudaError_t launch_lhs(const tr_ctx *c, const DeviceOp<T> &op, LhsArgs<T> a, cud
 template <typename T>
 cudaError_t launch_lhs(const tr_ctx *c, const DeviceOp<T> &op, const T *f, T *r, int fin_kind, double *fin_out,
                        CgScalars *cgs, const int32_t *done, cudaStream_t s);
-size_t lhs_max_smem(uint32_t aslm, uint32_t slm, uint32_t nnz, bool fp64);
 template <typename T>
 cudaError_t launch_cg_persistent(const tr_ctx *c, const DeviceOp<T> &op, const PcgArgs<T> &a, cudaStream_t s,
                                  int *grid_out);

@@ -85,15 +85,16 @@ __host__ __device__ constexpr int batch_of(int H) { return H <= 2 ? 4 : 2; }
 
 __host__ __device__ inline size_t align16(size_t b) { return (b + 15) & ~size_t(15); }
 
+// bytes of the staged contraction tables (weights + offsets)
 template <typename T>
-__host__ __device__ inline size_t ang_smem_bytes(uint32_t nnz) {
-    return align16(nnz * sizeof(AngEntry<T>));
+__host__ __device__ inline size_t ang_smem_bytes(uint32_t ncon) {
+    return align16(ncon * sizeof(T)) + align16(ncon * sizeof(uint16_t));
 }
 // per-group shared slab: staged edge coefficients + the S / B table,
 // rounded to 16 bytes so every slab (and its vector stores) stays aligned
 template <int G, int H, typename T>
 __host__ __device__ constexpr size_t group_smem_elems() {
-    return (G * kCoefStride + 9 * (G * H + 1) + (16 / sizeof(T)) - 1) / (16 / sizeof(T)) * (16 / sizeof(T));
+    return (G * kCoefStride + kSymRows * (G * H + 1) + (16 / sizeof(T)) - 1) / (16 / sizeof(T)) * (16 / sizeof(T));
 }
 
 // loads of vectors that other blocks of the same launch may have written
@@ -125,7 +126,8 @@ __device__ __forceinline__ void gather_row(const T *__restrict__ f, const T *__r
 // when small, the three half-range tables O_n.
 template <typename T>
 struct Staged {
-    const AngEntry<T> *ang;
+    const T *cw;          // contraction weights  [ckmax][cls]
+    const uint16_t *co;   // contraction offsets  [ckmax][cls]
     const T *O;
     size_t bytes;
 };
@@ -134,15 +136,23 @@ __host__ __device__ inline size_t O_smem_bytes(uint32_t slm) {
     return align16(3 * static_cast<size_t>(slm) * slm * sizeof(T));
 }
 
+// flags: 1 stage the contraction tables, 2 stage O, 4 use the tensor-core
+// (C table) offsets
 template <typename T>
 __device__ __forceinline__ Staged<T> stage_tables(const OpData<T> &d, unsigned char *smem, int flags) {
-    Staged<T> st{d.ang, d.O, 0};
-    const uint32_t nnz = d.ang_start[d.slm];
+    const uint16_t *co = (flags & 4) ? d.co_tc : d.co;
+    Staged<T> st{d.cw, co, d.O, 0};
+    const uint32_t ncon = d.ckmax * d.cls;
     if (flags & 1) {
-        AngEntry<T> *se = reinterpret_cast<AngEntry<T> *>(smem);
-        for (uint32_t i = threadIdx.x; i < nnz; i += blockDim.x) se[i] = d.ang[i];
-        st.ang = se;
-        st.bytes = ang_smem_bytes<T>(nnz);
+        T *sw = reinterpret_cast<T *>(smem);
+        uint16_t *so = reinterpret_cast<uint16_t *>(smem + align16(ncon * sizeof(T)));
+        for (uint32_t i = threadIdx.x; i < ncon; i += blockDim.x) {
+            sw[i] = __ldg(d.cw + i);
+            so[i] = __ldg(co + i);
+        }
+        st.cw = sw;
+        st.co = so;
+        st.bytes = ang_smem_bytes<T>(ncon);
     }
     if (flags & 2) {
         T *so = reinterpret_cast<T *>(smem + st.bytes);
@@ -151,35 +161,49 @@ __device__ __forceinline__ Staged<T> stage_tables(const OpData<T> &d, unsigned c
         st.O = so;
         st.bytes += O_smem_bytes<T>(d.slm);
     }
-    if (flags) __syncthreads();
+    if (flags & 3) __syncthreads();
     return st;
 }
 
-// the 14 coefficients of one staged edge record (vector shared loads)
+// out += sum_k cw[k][lm] * S[co[k][lm]]  (lane-major tables: coalesced)
 template <typename T>
-__device__ __forceinline__ void load_coef(const T *c, T (&k)[14]);
+__device__ __forceinline__ T contract(const Staged<T> &tab, const T *S, uint32_t lm, uint32_t kmax, uint32_t ls,
+                                      T acc0) {
+    const T *w = tab.cw + lm;
+    const uint16_t *o = tab.co + lm;
+    T acc1 = T(0), acc2 = T(0), acc3 = T(0);
+    uint32_t k = 0;
+    for (; k + 3 < kmax; k += 4) {
+        acc0 = fma(w[k * ls], S[o[k * ls]], acc0);
+        acc1 = fma(w[(k + 1) * ls], S[o[(k + 1) * ls]], acc1);
+        acc2 = fma(w[(k + 2) * ls], S[o[(k + 2) * ls]], acc2);
+        acc3 = fma(w[(k + 3) * ls], S[o[(k + 3) * ls]], acc3);
+    }
+    for (; k < kmax; ++k) acc0 = fma(w[k * ls], S[o[k * ls]], acc0);
+    return (acc0 + acc2) + (acc1 + acc3);
+}
+
+// the 11 used coefficients of one staged edge record (vector shared loads)
+template <typename T>
+__device__ __forceinline__ void load_coef(const T *c, T (&k)[12]);
 template <>
-__device__ __forceinline__ void load_coef<float>(const float *c, float (&k)[14]) {
+__device__ __forceinline__ void load_coef<float>(const float *c, float (&k)[12]) {
     const float4 a = reinterpret_cast<const float4 *>(c)[0], b = reinterpret_cast<const float4 *>(c)[1],
-                 e = reinterpret_cast<const float4 *>(c)[2], g = reinterpret_cast<const float4 *>(c)[3];
-    k[0] = a.x; k[1] = a.y; k[2] = a.z; k[3] = a.w; k[4] = b.x; k[5] = b.y; k[6] = b.z;
-    k[7] = b.w; k[8] = e.x; k[9] = e.y; k[10] = e.z; k[11] = e.w; k[12] = g.x; k[13] = g.y;
+                 e = reinterpret_cast<const float4 *>(c)[2];
+    k[0] = a.x; k[1] = a.y; k[2] = a.z; k[3] = a.w; k[4] = b.x; k[5] = b.y;
+    k[6] = b.z; k[7] = b.w; k[8] = e.x; k[9] = e.y; k[10] = e.z; k[11] = e.w;
 }
 template <>
-__device__ __forceinline__ void load_coef<double>(const double *c, double (&k)[14]) {
+__device__ __forceinline__ void load_coef<double>(const double *c, double (&k)[12]) {
     const double2 *v = reinterpret_cast<const double2 *>(c);
 #pragma unroll
-    for (int i = 0; i < 7; ++i) {
+    for (int i = 0; i < 6; ++i) {
         const double2 t = v[i];
         k[2 * i] = t.x;
         k[2 * i + 1] = t.y;
     }
 }
 
-// A x over the vertices of this block (grid-stride by vertex groups);
-// returns this thread's share of <x, A x> (DOT) -- x = f, or, with FUSEP,
-// x = f + beta pold, written to pnew.  smem_groups: the block's per-group
-// slabs (after the staged tables).
 template <int G, int H, typename T, bool DOT, bool FUSEP, bool COH = false>
 __device__ __forceinline__ double lhs_vertices(const OpData<T> &d, const Staged<T> &tab, unsigned char *smem_groups,
                                                const T *__restrict__ f, const T *__restrict__ pold,
@@ -197,12 +221,12 @@ __device__ __forceinline__ double lhs_vertices(const OpData<T> &d, const Staged<
 
     for (uint32_t v = blockIdx.x * gpb + threadIdx.x / G; v < d.nP; v += ng) {
         const uint32_t axes = __ldg(d.bmask + v);
-        T mass[H], S[9][H], B[3][H];
+        T mass[H], S[kSymRows][H], B[3][H];
 #pragma unroll
         for (int h = 0; h < H; ++h) {
             mass[h] = B[0][h] = B[1][h] = B[2][h] = T(0);
 #pragma unroll
-            for (int q = 0; q < 9; ++q) S[q][h] = T(0);
+            for (int q = 0; q < kSymRows; ++q) S[q][h] = T(0);
         }
         const uint32_t e0 = __ldg(d.row + v), e1 = __ldg(d.row + v + 1);
         for (uint32_t base = e0; base < e1; base += G) {
@@ -218,21 +242,21 @@ __device__ __forceinline__ double lhs_vertices(const OpData<T> &d, const Staged<
             }
             tile.sync();
             auto accumulate = [&](const T *cp, const T(&x)[H]) {
-                T c[14];
+                T c[12];
                 load_coef<T>(cp, c);
 #pragma unroll
                 for (int h = 0; h < H; ++h) {
                     const uint32_t lm = lane + G * h;
-                    mass[h] = fma(lm == 0 ? c[10] : c[9], x[h], mass[h]);
+                    mass[h] = fma(lm == 0 ? c[kRowM0] : c[kRowM], x[h], mass[h]);
 #pragma unroll
-                    for (int q = 0; q < 9; ++q) S[q][h] = fma(c[q], x[h], S[q][h]);
+                    for (int q = 0; q < kSymRows; ++q) S[q][h] = fma(c[q], x[h], S[q][h]);
                 }
                 if (axes) {
 #pragma unroll
                     for (int h = 0; h < H; ++h) {
-                        B[0][h] = fma(c[11], x[h], B[0][h]);
-                        B[1][h] = fma(c[12], x[h], B[1][h]);
-                        B[2][h] = fma(c[13], x[h], B[2][h]);
+                        B[0][h] = fma(c[kRowE], x[h], B[0][h]);
+                        B[1][h] = fma(c[kRowE + 1], x[h], B[1][h]);
+                        B[2][h] = fma(c[kRowE + 2], x[h], B[2][h]);
                     }
                 }
             };
@@ -252,31 +276,17 @@ __device__ __forceinline__ double lhs_vertices(const OpData<T> &d, const Staged<
             }
             tile.sync();
         }
-        // angular coupling through shared memory (two partial sums)
+        // angular coupling through shared memory
 #pragma unroll
         for (int h = 0; h < H; ++h)
 #pragma unroll
-            for (int q = 0; q < 9; ++q) sm[q * SA + lane + G * h] = S[q][h];
+            for (int q = 0; q < kSymRows; ++q) sm[q * SA + lane + G * h] = S[q][h];
         tile.sync();
         T out[H];
 #pragma unroll
         for (int h = 0; h < H; ++h) {
             const uint32_t lm = lane + G * h;
-            T acc0 = T(0), acc1 = T(0);
-            if (lm < slm) {
-                const uint32_t a1 = __ldg(d.ang_start + lm + 1);
-                uint32_t a = __ldg(d.ang_start + lm);
-                for (; a + 1 < a1; a += 2) {
-                    const AngEntry<T> p0 = tab.ang[a], p1 = tab.ang[a + 1];
-                    acc0 = fma(p0.w, sm[p0.off], acc0);
-                    acc1 = fma(p1.w, sm[p1.off], acc1);
-                }
-                if (a < a1) {
-                    const AngEntry<T> p0 = tab.ang[a];
-                    acc0 = fma(p0.w, sm[p0.off], acc0);
-                }
-            }
-            out[h] = mass[h] + (acc0 + acc1);
+            out[h] = (lm < d.cls) ? contract<T>(tab, sm, lm, d.ckmax, d.cls, mass[h]) : mass[h];
         }
         // half-range boundary term from the per-axis sums B_n
         if (axes) {
@@ -323,12 +333,261 @@ __device__ __forceinline__ double lhs_vertices(const OpData<T> &d, const Staged<
     return dacc;
 }
 
-// register budget: FP64 128 registers (2 resident blocks), FP32 80 (3
-// blocks); one block per SM for FP64 with H > 2 harmonics per lane
-#define TR_LHS_MINBLOCKS(T, H) (sizeof(T) == 8 ? ((H) > 2 ? 1 : 2) : ((H) > 1 ? 2 : 3))
 
-template <int G, int H, typename T, bool DOT, bool FUSEP, class Fin>
-__global__ void __launch_bounds__(kBlock, TR_LHS_MINBLOCKS(T, H)) k_lhs(
+// ------------------------------------------------------ tensor-core path
+// Per vertex v, everything the edge loop accumulates is one small dense
+// product: with rows q = K[9], M, M0, E_x, E_y, E_z (the 14 coefficients of
+// an edge record, padded to 16) and columns lm,
+//   C_v[q][lm] = sum_{edges e of v} coef[e][q] * x[u_e][lm],
+// i.e. C_v (16 x 8NT) = A_v (16 x edges) X_v (edges x 8NT), where A_v^T is
+// the vertex's run of edge records and X_v its gathered neighbour rows.  One
+// warp computes it with mma.sync: FP32 as split-TF32 (3 products per tile,
+// a ~ a_hi + a_lo with a_hi, a_lo TF32; the lo*lo term is dropped) on
+// m16n8k8 tiles, FP64 exactly on m8n8k4 DMMA tiles.  C goes to shared memory
+// and the epilogue (lane = harmonic) takes the mass term from rows 9 / 10,
+// the spatial sums S from rows 0-8 for the angular contraction and the
+// per-axis boundary sums from rows 11-13.
+__device__ __forceinline__ uint32_t tf32_bits(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ void split_tf32(float x, uint32_t &hi, uint32_t &lo) {
+    hi = tf32_bits(x);
+    lo = tf32_bits(x - __uint_as_float(hi));
+}
+// D = A B + D for one m16n8k8 tile (A row-major, B column-major fragments)
+__device__ __forceinline__ void mma_tf32(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+// D = A B + D for one m8n8k4 FP64 tile
+__device__ __forceinline__ void mma_f64(double &c0, double &c1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
+template <int NT>
+struct TcShape {
+    static constexpr int SA = NT * 8 + 1;  // row stride of the per-warp C table
+};
+
+// x_u[lm] for one harmonic (0 outside the valid range)
+template <typename T, bool FUSEP, bool COH>
+__device__ __forceinline__ T gather_one(const T *__restrict__ f, const T *__restrict__ pold, T beta, uint32_t u,
+                                        uint32_t aslm, uint32_t lm, bool ok) {
+    if (!ok) return T(0);
+    T x = ldv<COH>(f + u * aslm + lm);
+    if (FUSEP) x = fma(beta, ldv<COH>(pold + u * aslm + lm), x);
+    return x;
+}
+
+template <int NT, typename T, bool DOT, bool FUSEP, bool COH = false>
+__device__ __forceinline__ double lhs_vertices_tc(const OpData<T> &d, const Staged<T> &tab, unsigned char *smem_warps,
+                                                  const T *__restrict__ f, const T *__restrict__ pold,
+                                                  T *__restrict__ pnew, T *__restrict__ r, const T beta) {
+    constexpr int SA = TcShape<NT>::SA;
+    const uint32_t slm = d.slm, aslm = d.aslm;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    T *sm = reinterpret_cast<T *>(smem_warps) + warp * 16 * SA;
+    const uint32_t wpb = kBlock / 32;
+    const uint32_t nw = gridDim.x * wpb;
+    double dacc = 0.0;
+
+    for (uint32_t v = blockIdx.x * wpb + warp; v < d.nP; v += nw) {
+        const uint32_t axes = __ldg(d.bmask + v);
+        const uint32_t e0 = __ldg(d.row + v), e1 = __ldg(d.row + v + 1);
+        if constexpr (sizeof(T) == 4) {
+            float acc[NT][4];
+#pragma unroll
+            for (int n = 0; n < NT; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.0f;
+            // one k-step of 8 edges: A = coefficient rows, B = gathered rows
+            auto kstep = [&](const float (&a)[4], const float (&xa)[NT], const float (&xb)[NT]) {
+                uint32_t ahi[4], alo[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) split_tf32(a[i], ahi[i], alo[i]);
+#pragma unroll
+                for (int n = 0; n < NT; ++n) {
+                    uint32_t b0h, b0l, b1h, b1l;
+                    split_tf32(xa[n], b0h, b0l);
+                    split_tf32(xb[n], b1h, b1l);
+                    mma_tf32(acc[n], alo, b0h, b1h);
+                    mma_tf32(acc[n], ahi, b0l, b1l);
+                    mma_tf32(acc[n], ahi, b0h, b1h);
+                }
+            };
+            auto load_step = [&](uint32_t base, float (&a)[4], uint32_t &ua, uint32_t &ub, bool &va, bool &vb) {
+                const uint32_t ea = base + t, eb = base + t + 4;
+                va = ea < e1;
+                vb = eb < e1;
+                const float *ca = d.coef + static_cast<size_t>(va ? ea : e0) * kCoefStride;
+                const float *cb = d.coef + static_cast<size_t>(vb ? eb : e0) * kCoefStride;
+                a[0] = va ? __ldg(ca + g) : 0.0f;
+                a[1] = va ? __ldg(ca + g + 8) : 0.0f;
+                a[2] = vb ? __ldg(cb + g) : 0.0f;
+                a[3] = vb ? __ldg(cb + g + 8) : 0.0f;
+                ua = va ? __ldg(d.col + ea) : 0u;
+                ub = vb ? __ldg(d.col + eb) : 0u;
+            };
+            // the first 16 edges: all indices and coefficients first, then all
+            // row gathers, then the MMAs -- two latency stages per vertex
+            {
+                float a0[4], a1[4];
+                uint32_t ua0, ub0, ua1, ub1;
+                bool va0, vb0, va1, vb1;
+                load_step(e0, a0, ua0, ub0, va0, vb0);
+                load_step(e0 + 8, a1, ua1, ub1, va1, vb1);
+                float xa0[NT], xb0[NT], xa1[NT], xb1[NT];
+#pragma unroll
+                for (int n = 0; n < NT; ++n) {
+                    const uint32_t lm = n * 8 + g;
+                    const bool in = lm < slm;
+                    xa0[n] = gather_one<float, FUSEP, COH>(f, pold, beta, ua0, aslm, lm, va0 && in);
+                    xb0[n] = gather_one<float, FUSEP, COH>(f, pold, beta, ub0, aslm, lm, vb0 && in);
+                    xa1[n] = gather_one<float, FUSEP, COH>(f, pold, beta, ua1, aslm, lm, va1 && in);
+                    xb1[n] = gather_one<float, FUSEP, COH>(f, pold, beta, ub1, aslm, lm, vb1 && in);
+                }
+                kstep(a0, xa0, xb0);
+                if (e0 + 8 < e1) kstep(a1, xa1, xb1);
+            }
+            for (uint32_t base = e0 + 16; base < e1; base += 8) {  // vertices with > 16 edges
+                float a[4];
+                uint32_t ua, ub;
+                bool va, vb;
+                load_step(base, a, ua, ub, va, vb);
+                float xa[NT], xb[NT];
+#pragma unroll
+                for (int n = 0; n < NT; ++n) {
+                    const uint32_t lm = n * 8 + g;
+                    xa[n] = gather_one<float, FUSEP, COH>(f, pold, beta, ua, aslm, lm, va && lm < slm);
+                    xb[n] = gather_one<float, FUSEP, COH>(f, pold, beta, ub, aslm, lm, vb && lm < slm);
+                }
+                kstep(a, xa, xb);
+            }
+#pragma unroll
+            for (int n = 0; n < NT; ++n) {
+                sm[g * SA + n * 8 + 2 * t] = acc[n][0];
+                sm[g * SA + n * 8 + 2 * t + 1] = acc[n][1];
+                sm[(g + 8) * SA + n * 8 + 2 * t] = acc[n][2];
+                sm[(g + 8) * SA + n * 8 + 2 * t + 1] = acc[n][3];
+            }
+        } else {
+            double acc[2][NT][2];
+#pragma unroll
+            for (int n = 0; n < NT; ++n) acc[0][n][0] = acc[0][n][1] = acc[1][n][0] = acc[1][n][1] = 0.0;
+            // edges in k-steps of 4; batches of KB k-steps load everything
+            // (indices, coefficients, then rows) before their MMAs
+            constexpr int KB = NT <= 4 ? 4 : 2;
+            for (uint32_t base = e0; base < e1; base += 4 * KB) {
+                uint32_t ua[KB];
+                bool va[KB];
+                double alo[KB], ahi[KB];
+#pragma unroll
+                for (int k = 0; k < KB; ++k) {
+                    const uint32_t ea = base + 4 * k + t;
+                    va[k] = ea < e1;
+                    const double *ca = d.coef + static_cast<size_t>(va[k] ? ea : e0) * kCoefStride;
+                    alo[k] = va[k] ? __ldg(ca + g) : 0.0;
+                    ahi[k] = (va[k] && axes) ? __ldg(ca + g + 8) : 0.0;
+                    ua[k] = va[k] ? __ldg(d.col + ea) : 0u;
+                }
+                double xa[KB][NT];
+#pragma unroll
+                for (int k = 0; k < KB; ++k)
+#pragma unroll
+                    for (int n = 0; n < NT; ++n) {
+                        const uint32_t lm = n * 8 + g;
+                        xa[k][n] = gather_one<double, FUSEP, COH>(f, pold, beta, ua[k], aslm, lm, va[k] && lm < slm);
+                    }
+#pragma unroll
+                for (int k = 0; k < KB; ++k)
+#pragma unroll
+                    for (int n = 0; n < NT; ++n) mma_f64(acc[0][n][0], acc[0][n][1], alo[k], xa[k][n]);
+                if (axes)  // rows 8-15: the boundary sums (warp-uniform)
+#pragma unroll
+                    for (int k = 0; k < KB; ++k)
+#pragma unroll
+                        for (int n = 0; n < NT; ++n) mma_f64(acc[1][n][0], acc[1][n][1], ahi[k], xa[k][n]);
+            }
+#pragma unroll
+            for (int n = 0; n < NT; ++n) {
+                sm[g * SA + n * 8 + 2 * t] = acc[0][n][0];
+                sm[g * SA + n * 8 + 2 * t + 1] = acc[0][n][1];
+                sm[(g + 8) * SA + n * 8 + 2 * t] = acc[1][n][0];
+                sm[(g + 8) * SA + n * 8 + 2 * t + 1] = acc[1][n][1];
+            }
+        }
+        __syncwarp();
+        // epilogue: lane = harmonic
+        T *rv = r + static_cast<size_t>(v) * aslm;
+        for (uint32_t lm = lane; lm < aslm; lm += 32) {
+            T out = T(0);
+            if (lm < slm) {
+                T acc0 = contract<T>(tab, sm, lm, d.ckmax, d.cls, sm[(lm == 0 ? kRowM0 : kRowM) * SA + lm]);
+                T acc1 = T(0);
+                if (axes) {
+                    for (int n = 0; n < 3; ++n) {
+                        if (!(axes & (1u << n))) continue;
+                        const T *On = tab.O + static_cast<size_t>(n) * slm * slm + lm;
+                        const T *Bn = sm + (kRowE + n) * SA;
+                        uint32_t lms = 0;
+                        for (; lms + 1 < slm; lms += 2) {
+                            acc0 = fma(On[lms * slm], Bn[lms], acc0);
+                            acc1 = fma(On[(lms + 1) * slm], Bn[lms + 1], acc1);
+                        }
+                        if (lms < slm) acc0 = fma(On[lms * slm], Bn[lms], acc0);
+                    }
+                }
+                out = acc0 + acc1;
+            }
+            rv[lm] = out;
+            if (DOT || FUSEP) {
+                const T xv = gather_one<T, FUSEP, COH>(f, pold, beta, v, aslm, lm, lm < slm);
+                if (FUSEP) pnew[static_cast<size_t>(v) * aslm + lm] = xv;
+                if (DOT) dacc += static_cast<double>(xv) * static_cast<double>(out);
+            }
+        }
+        __syncwarp();
+    }
+    return dacc;
+}
+
+// ------------------------------------------------------------- policies
+// An operator policy supplies the per-block vertex loop and its shared
+// memory: SimtOp (groups of G lanes, H harmonics per lane, FMA pipes) or
+// TcOp (one warp per vertex, NT n-tiles, tensor pipes).
+template <int G, int H, typename T>
+struct SimtOp {
+    static constexpr int kMinBlocks = sizeof(T) == 8 ? (H > 2 ? 1 : 2) : (H > 1 ? 2 : 3);
+    static constexpr int kLanes = G;
+    static constexpr bool kTc = false;
+    static size_t slab_bytes() { return (kBlock / G) * group_smem_elems<G, H, T>() * sizeof(T); }
+    template <bool DOT, bool FUSEP, bool COH>
+    __device__ static double run(const OpData<T> &d, const Staged<T> &tab, unsigned char *slabs, const T *f,
+                                 const T *pold, T *pnew, T *r, T beta) {
+        return lhs_vertices<G, H, T, DOT, FUSEP, COH>(d, tab, slabs, f, pold, pnew, r, beta);
+    }
+};
+template <int NT, typename T>
+struct TcOp {
+    static constexpr int kMinBlocks = NT > 6 ? 1 : 2;  // up to 128 registers: loads in flight over occupancy
+    static constexpr int kLanes = 32;
+    static constexpr bool kTc = true;
+    static size_t slab_bytes() { return align16((kBlock / 32) * 16 * TcShape<NT>::SA * sizeof(T)); }
+    template <bool DOT, bool FUSEP, bool COH>
+    __device__ static double run(const OpData<T> &d, const Staged<T> &tab, unsigned char *slabs, const T *f,
+                                 const T *pold, T *pnew, T *r, T beta) {
+        return lhs_vertices_tc<NT, T, DOT, FUSEP, COH>(d, tab, slabs, f, pold, pnew, r, beta);
+    }
+};
+
+template <class Op, typename T, bool DOT, bool FUSEP, class Fin>
+__global__ void __launch_bounds__(kBlock, Op::kMinBlocks) k_lhs(
     const OpData<T> d, const T *__restrict__ f, const T *__restrict__ pold, T *__restrict__ pnew,
     T *__restrict__ r, double *partials, unsigned int *counter, Fin fin, const int32_t *__restrict__ done,
     const CgScalars *__restrict__ cgs, int stage_flags) {
@@ -336,8 +595,7 @@ __global__ void __launch_bounds__(kBlock, TR_LHS_MINBLOCKS(T, H)) k_lhs(
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const Staged<T> tab = stage_tables<T>(d, smem_raw, stage_flags);
     const T beta = FUSEP ? static_cast<T>(cgs->beta) : T(0);
-    const double dacc =
-        lhs_vertices<G, H, T, DOT, FUSEP>(d, tab, smem_raw + tab.bytes, f, pold, pnew, r, beta);
+    const double dacc = Op::template run<DOT, FUSEP, false>(d, tab, smem_raw + tab.bytes, f, pold, pnew, r, beta);
     if (DOT) {
         double vv[1] = {dacc}, tot[1];
         if (grid_reduce<1>(vv, partials, counter, tot) && threadIdx.x == 0) fin(tot[0]);
@@ -361,8 +619,8 @@ __global__ void __launch_bounds__(kBlock) k_lhs_diag(const OpData<T> d, const T 
         for (uint32_t e = __ldg(d.row + v); e < e1; ++e) {
             const uint32_t u = __ldg(d.col + e);
             const T *c = d.coef + static_cast<size_t>(e) * kCoefStride;
-            const T K0 = __ldg(c), K4 = __ldg(c + 4), K8 = __ldg(c + 8), M = __ldg(c + 9), M0 = __ldg(c + 10);
-            const T E0 = __ldg(c + 11), E1 = __ldg(c + 12), E2 = __ldg(c + 13);
+            const T K0 = __ldg(c), K4 = __ldg(c + 1), K8 = __ldg(c + 2), M = __ldg(c + kRowM), M0 = __ldg(c + kRowM0);
+            const T E0 = __ldg(c + kRowE), E1 = __ldg(c + kRowE + 1), E2 = __ldg(c + kRowE + 2);
             T x[H];
             gather_row<G, H, T, false>(f, nullptr, T(0), u, aslm, slm, lane, x);
 #pragma unroll
@@ -452,8 +710,8 @@ __device__ __forceinline__ void sum_partials(const double *partials, double (&to
 // ||r||^2 and (r, z); after a second barrier every block takes the stop
 // test and beta.  The scalars never leave the device; block 0 mirrors them
 // (and the residual history) into CgScalars for the host.
-template <int G, int H, typename T, bool JAC>
-__global__ void __launch_bounds__(kBlock, TR_LHS_MINBLOCKS(T, H))
+template <class Op, typename T, bool JAC>
+__global__ void __launch_bounds__(kBlock, Op::kMinBlocks)
     k_cg_persistent(const OpData<T> d, const PcgArgs<T> a, int stage_flags) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double sh[32];
@@ -472,8 +730,8 @@ __global__ void __launch_bounds__(kBlock, TR_LHS_MINBLOCKS(T, H))
         const T *pold = parity ? a.p1 : a.p0;
         T *pnew = parity ? a.p0 : a.p1;
         // phase A: p = z + beta p_old, A p, <p, A p>
-        const double dacc = lhs_vertices<G, H, T, true, true, true>(d, tab, smem_raw + tab.bytes, JAC ? a.z : a.r,
-                                                                    pold, pnew, a.Ap, static_cast<T>(beta));
+        const double dacc = Op::template run<true, true, true>(d, tab, smem_raw + tab.bytes, JAC ? a.z : a.r, pold,
+                                                               pnew, a.Ap, static_cast<T>(beta));
         const double bs = block_sum(dacc, sh);
         if (threadIdx.x == 0) a.partials[blockIdx.x] = bs;
         if (!grid_barrier(a.bar, a.bar + 1, a.err)) return;
@@ -566,53 +824,77 @@ __global__ void __launch_bounds__(kBlock) k_rhs(const RhsData d, T *__restrict__
 constexpr size_t kAngSmemBudget = 64 * 1024;
 constexpr size_t kOSmemBudget = 40 * 1024;
 
-template <typename T>
+template <class Op, typename T>
 static int stage_flags(uint32_t slm, uint32_t nnz) {
-    return (ang_smem_bytes<T>(nnz) <= kAngSmemBudget ? 1 : 0) | (O_smem_bytes<T>(slm) <= kOSmemBudget ? 2 : 0);
+    return (ang_smem_bytes<T>(nnz) <= kAngSmemBudget ? 1 : 0) | (O_smem_bytes<T>(slm) <= kOSmemBudget ? 2 : 0) |
+           (Op::kTc ? 4 : 0);
 }
-template <int G, int H, typename T>
+template <class Op, typename T>
 static size_t lhs_smem(uint32_t slm, uint32_t nnz) {
-    const int fl = stage_flags<T>(slm, nnz);
-    return ((fl & 1) ? ang_smem_bytes<T>(nnz) : 0) + ((fl & 2) ? O_smem_bytes<T>(slm) : 0) +
-           (kBlock / G) * group_smem_elems<G, H, T>() * sizeof(T);
+    const int fl = stage_flags<Op, T>(slm, nnz);
+    return ((fl & 1) ? ang_smem_bytes<T>(nnz) : 0) + ((fl & 2) ? O_smem_bytes<T>(slm) : 0) + Op::slab_bytes();
 }
 
-template <int G, int H, typename T, bool DOT, bool FUSEP, class Fin>
-static cudaError_t launch_one(const tr_ctx *c, const OpData<T> &d, const LhsArgs<T> &a, Fin fin, cudaStream_t s) {
-    const size_t smem = lhs_smem<G, H, T>(d.slm, a.ang_nnz);
-    auto kern = k_lhs<G, H, T, DOT, FUSEP, Fin>;
-    static size_t opted = 0;  // dynamic shared memory granted so far (per instantiation)
+template <class K>
+static cudaError_t opt_in_smem(K kern, size_t smem, size_t &opted) {
     if (smem > 48 * 1024 && smem > opted) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
         if (e != cudaSuccess) return e;
         opted = smem;
     }
-    kern<<<c->grid_op, kBlock, smem, s>>>(d, a.x, a.pold, a.pnew, a.y, c->partials, c->counters, fin, a.done, a.cgs,
-                                          stage_flags<T>(d.slm, a.ang_nnz));
-    return cudaGetLastError();
+    return cudaSuccess;
 }
 
-template <int G, int H, typename T>
-static cudaError_t launch_lhs_gh(const tr_ctx *c, const OpData<T> &d, const LhsArgs<T> &a, cudaStream_t s) {
-    switch (a.fin_kind) {
-    case 0: return launch_one<G, H, T, false, false>(c, d, a, FinNone(), s);
-    case 1: return launch_one<G, H, T, true, false>(c, d, a, FinStore{a.fin_out}, s);
-    case 2: return launch_one<G, H, T, true, false>(c, d, a, FinAlpha{a.cgs}, s);
-    default: return launch_one<G, H, T, true, true>(c, d, a, FinAlpha{a.cgs}, s);
+// Calls fn(Op()) with the operator policy of this context and precision:
+// SIMT groups (G, H) from the vector stride, or tensor-core tiles NT from slm.
+template <typename T, class F>
+static cudaError_t with_op(const DeviceOp<T> &op, uint32_t slm, F &&fn) {
+    if (op.kind == TR_OPERATOR_TENSOR) {
+        const uint32_t nt = (slm + 7) / 8;
+        if (nt <= 1) return fn(TcOp<1, T>());
+        if (nt <= 2) return fn(TcOp<2, T>());
+        if (nt <= 4) return fn(TcOp<4, T>());
+        if (nt <= 6) return fn(TcOp<6, T>());
+        if (nt <= 9) return fn(TcOp<9, T>());
+        if (nt <= 12) return fn(TcOp<12, T>());
+        return fn(TcOp<15, T>());
     }
+    const uint32_t as = op.aslm;
+    if (as <= 8) return fn(SimtOp<8, 1, T>());
+    if (as <= 16) return fn(SimtOp<16, 1, T>());
+    if (as <= 32) return fn(SimtOp<32, 1, T>());
+    if (as <= 64) return fn(SimtOp<32, 2, T>());
+    if (as <= 96) return fn(SimtOp<32, 3, T>());
+    return fn(SimtOp<32, 4, T>());
+}
+
+template <class Op, typename T, bool DOT, bool FUSEP, class Fin>
+static cudaError_t launch_one(const tr_ctx *c, const OpData<T> &d, const LhsArgs<T> &a, Fin fin, cudaStream_t s) {
+    const size_t smem = lhs_smem<Op, T>(d.slm, a.ang_nnz);
+    auto kern = k_lhs<Op, T, DOT, FUSEP, Fin>;
+    static size_t opted = 0;  // dynamic shared memory granted so far (per instantiation)
+    cudaError_t e = opt_in_smem(kern, smem, opted);
+    if (e != cudaSuccess) return e;
+    const int gpb = kBlock / Op::kLanes;
+    const int grid = std::max(1, std::min(c->num_sms * 4, static_cast<int>((d.nP + gpb - 1) / gpb)));
+    kern<<<grid, kBlock, smem, s>>>(d, a.x, a.pold, a.pnew, a.y, c->partials, c->counters, fin, a.done, a.cgs,
+                                    stage_flags<Op, T>(d.slm, a.ang_nnz));
+    return cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t launch_lhs(const tr_ctx *c, const DeviceOp<T> &op, LhsArgs<T> a, cudaStream_t s) {
     const OpData<T> d = op.data(c->nP, c->slm);
     a.ang_nnz = op.ang_nnz;
-    const uint32_t as = op.aslm;
-    if (as <= 8) return launch_lhs_gh<8, 1, T>(c, d, a, s);
-    if (as <= 16) return launch_lhs_gh<16, 1, T>(c, d, a, s);
-    if (as <= 32) return launch_lhs_gh<32, 1, T>(c, d, a, s);
-    if (as <= 64) return launch_lhs_gh<32, 2, T>(c, d, a, s);
-    if (as <= 96) return launch_lhs_gh<32, 3, T>(c, d, a, s);
-    return launch_lhs_gh<32, 4, T>(c, d, a, s);
+    return with_op<T>(op, c->slm, [&](auto tag) -> cudaError_t {
+        typedef decltype(tag) Op;
+        switch (a.fin_kind) {
+        case 0: return launch_one<Op, T, false, false>(c, d, a, FinNone(), s);
+        case 1: return launch_one<Op, T, true, false>(c, d, a, FinStore{a.fin_out}, s);
+        case 2: return launch_one<Op, T, true, false>(c, d, a, FinAlpha{a.cgs}, s);
+        default: return launch_one<Op, T, true, true>(c, d, a, FinAlpha{a.cgs}, s);
+        }
+    });
 }
 
 template <typename T>
@@ -643,27 +925,24 @@ cudaError_t launch_lhs_diag(const tr_ctx *c, const DeviceOp<T> &op, const T *f, 
     return cudaGetLastError();
 }
 
-template <int G, int H, typename T, bool JAC>
-static cudaError_t launch_pcg_gh(const tr_ctx *c, const OpData<T> &d, const PcgArgs<T> &a, uint32_t nnz,
-                                 cudaStream_t s, int *grid_out) {
-    auto kern = k_cg_persistent<G, H, T, JAC>;
-    const size_t smem = lhs_smem<G, H, T>(d.slm, nnz);
+template <class Op, typename T, bool JAC>
+static cudaError_t launch_pcg(const tr_ctx *c, const OpData<T> &d, const PcgArgs<T> &a, uint32_t nnz, cudaStream_t s,
+                              int *grid_out) {
+    auto kern = k_cg_persistent<Op, T, JAC>;
+    const size_t smem = lhs_smem<Op, T>(d.slm, nnz);
     static size_t opted = 0;
-    if (smem > 48 * 1024 && smem > opted) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-        if (e != cudaSuccess) return e;
-        opted = smem;
-    }
+    cudaError_t e = opt_in_smem(kern, smem, opted);
+    if (e != cudaSuccess) return e;
     int per_sm = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorCooperativeLaunchTooLarge;
     // enough blocks for the vertices, at most one wave of resident blocks
-    const int gpb = kBlock / G;
+    const int gpb = kBlock / Op::kLanes;
     const int need = static_cast<int>((d.nP + gpb - 1) / gpb);
     const int grid = std::max(1, std::min(per_sm * c->num_sms, std::min(need, kMaxGrid)));
     *grid_out = grid;
-    int flags = stage_flags<T>(d.slm, nnz);
+    int flags = stage_flags<Op, T>(d.slm, nnz);
     OpData<T> dd = d;
     PcgArgs<T> aa = a;
     void *args[] = {&dd, &aa, &flags};
@@ -674,18 +953,13 @@ template <typename T>
 cudaError_t launch_cg_persistent(const tr_ctx *c, const DeviceOp<T> &op, const PcgArgs<T> &a, cudaStream_t s,
                                  int *grid_out) {
     const OpData<T> d = op.data(c->nP, c->slm);
-    const uint32_t as = op.aslm, nnz = op.ang_nnz;
+    const uint32_t nnz = op.ang_nnz;
     const bool jac = a.dinv != nullptr;
-#define TR_PCG(G, H)                                                                                   \
-    return jac ? launch_pcg_gh<G, H, T, true>(c, d, a, nnz, s, grid_out)                              \
-               : launch_pcg_gh<G, H, T, false>(c, d, a, nnz, s, grid_out)
-    if (as <= 8) TR_PCG(8, 1);
-    if (as <= 16) TR_PCG(16, 1);
-    if (as <= 32) TR_PCG(32, 1);
-    if (as <= 64) TR_PCG(32, 2);
-    if (as <= 96) TR_PCG(32, 3);
-    TR_PCG(32, 4);
-#undef TR_PCG
+    return with_op<T>(op, c->slm, [&](auto tag) -> cudaError_t {
+        typedef decltype(tag) Op;
+        return jac ? launch_pcg<Op, T, true>(c, d, a, nnz, s, grid_out)
+                   : launch_pcg<Op, T, false>(c, d, a, nnz, s, grid_out);
+    });
 }
 template cudaError_t launch_cg_persistent<double>(const tr_ctx *, const DeviceOp<double> &, const PcgArgs<double> &,
                                                   cudaStream_t, int *);
@@ -714,20 +988,6 @@ cudaError_t launch_rhs_f32(const tr_ctx *c, float *b, cudaStream_t s) {
 }
 
 cudaError_t operator_init_attributes() { return cudaSuccess; }
-
-// largest dynamic shared memory the operator needs for this context
-size_t lhs_max_smem(uint32_t aslm, uint32_t slm, uint32_t nnz, bool fp64) {
-    auto pick = [&](auto tag) -> size_t {
-        typedef decltype(tag) T;
-        if (aslm <= 8) return lhs_smem<8, 1, T>(slm, nnz);
-        if (aslm <= 16) return lhs_smem<16, 1, T>(slm, nnz);
-        if (aslm <= 32) return lhs_smem<32, 1, T>(slm, nnz);
-        if (aslm <= 64) return lhs_smem<32, 2, T>(slm, nnz);
-        if (aslm <= 96) return lhs_smem<32, 3, T>(slm, nnz);
-        return lhs_smem<32, 4, T>(slm, nnz);
-    };
-    return fp64 ? pick(double()) : pick(float());
-}
 
 template cudaError_t launch_lhs<double>(const tr_ctx *, const DeviceOp<double> &, LhsArgs<double>, cudaStream_t);
 template cudaError_t launch_lhs<float>(const tr_ctx *, const DeviceOp<float> &, LhsArgs<float>, cudaStream_t);
