@@ -117,6 +117,27 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
+# DRAM bytes (read + write) of one persistent-kernel launch from an ncu capture
+# of that launch, per CG iteration, by workload (0 iterations: none captured)
+NCU_TRAFFIC_PER_ITERATION = {}
+
+
+def operator_policy(tensor, slm, aslm, real):
+    """Name of the operator policy the library selects (operator.cu with_op)."""
+    if tensor:
+        nt = (slm + 7) // 8
+        nt = next(n for n in (1, 2, 4, 6, 9, 12, 15) if nt <= n or n == 15)
+        return f"TcOp<{nt},{real}>"
+    g, h = next((g, h) for a, g, h in ((8, 8, 1), (16, 16, 1), (32, 32, 1), (64, 32, 2), (96, 32, 3), (1 << 30, 32, 4))
+                if aslm <= a)
+    return f"SimtOp<{g},{h},{real}>"
+
+
+def traffic_per_launch(workload, iters_per_launch):
+    t = NCU_TRAFFIC_PER_ITERATION.get(workload)
+    return None if t is None else t * iters_per_launch
+
+
 # ----------------------------------------------------------------- CPU arm
 def cpu_sample(workload, iters, steps=1):
     """FP64 oracle CG iterations on the workload (all host threads);
@@ -254,6 +275,16 @@ def run_ours(args, rank, world, local):
         bytes64, _ = W.algorithmic_work(md, ad, real_bytes=8)
         ach32 = bytes32 / (ms32.value * 1e-3) / 1e9
         ach64 = bytes64 / (ms64.value * 1e-3) / 1e9
+        # dominant kernel of the timed region: the persistent FP32 CG kernel,
+        # timed by CUDA events around each of its launches inside the solves
+        it_bytes, it_flops = W.cg_iteration_work(md, ad, real_bytes=4)
+        cg_ms = sum(r.cg_kernel_ms for r in reps_mixed)
+        cg_launches = sum(r.cg_kernel_launches for r in reps_mixed)
+        cg_iters = sum(r.iterations for r in reps_mixed)
+        solve_ms = sum(r.device_ms for r in reps_mixed)
+        ach_cg = cg_iters * it_bytes / (cg_ms * 1e-3) / 1e9
+        pol32 = operator_policy(False, slm, ctx.aslm_f32, "float")   # context defaults: FP32 SIMT,
+        pol64 = operator_policy(True, slm, ctx.aslm, "double")       # FP64 tensor cores
         it_mixed = statistics.mean(r.iterations for r in reps_mixed)
         it_fp64 = statistics.mean(r.iterations for r in reps_fp64)
         line = {
@@ -287,13 +318,24 @@ def run_ours(args, rank, world, local):
             "e2e": {"value": world * u_e2e / (t_e2e * 1e-3), "unit": UNIT,
                     "h2d_bytes_per_step": 8 * ctx.N(), "d2h_bytes_per_step": 8 * ctx.N()},
             "gpu_launches": int(l_mixed),
-            "roofline": {"bound": "hbm", "achieved": ach32, "peak": peak, "unit": "GB/s", "frac": ach32 / peak,
-                         "traffic": None, "peak_source": peak_kind,
-                         "kernel": "k_lhs<float> (FP32 operator, the inner-solve matvec)",
-                         "us_per_launch": 1e3 * ms32.value, "algorithmic_bytes": bytes32,
-                         "algorithmic_gflop": flops / 1e9, "gflops": flops / (ms32.value * 1e-3) / 1e9,
-                         "fp64_kernel": {"us_per_launch": 1e3 * ms64.value, "achieved": ach64,
-                                         "gflops": flops / (ms64.value * 1e-3) / 1e9}},
+            "roofline": {"bound": "hbm", "achieved": ach_cg, "peak": peak, "unit": "GB/s", "frac": ach_cg / peak,
+                         "traffic": traffic_per_launch(args.workload, cg_iters / cg_launches),
+                         "peak_source": peak_kind,
+                         "kernel": f"k_cg_persistent<{pol32}> (FP32 CG iterations of the mixed solve)",
+                         "us_per_launch": 1e3 * cg_ms / cg_launches,
+                         "iterations_per_launch": cg_iters / cg_launches,
+                         "algorithmic_bytes_per_launch": it_bytes * cg_iters / cg_launches,
+                         "algorithmic_bytes_per_iteration": it_bytes,
+                         "share_of_solve_device_time": cg_ms / solve_ms,
+                         "gflops": cg_iters * it_flops / (cg_ms * 1e-3) / 1e9,
+                         "operator_alone": {
+                             "fp32": {"kernel": f"k_lhs<{pol32}>", "us_per_launch": 1e3 * ms32.value,
+                                      "algorithmic_bytes": bytes32, "achieved_gbs": ach32,
+                                      "gflops": flops / (ms32.value * 1e-3) / 1e9},
+                             "fp64": {"kernel": f"k_lhs<{pol64}>", "us_per_launch": 1e3 * ms64.value,
+                                      "algorithmic_bytes": bytes64, "achieved_gbs": ach64,
+                                      "gflops": flops / (ms64.value * 1e-3) / 1e9},
+                             "algorithmic_gflop": flops / 1e9}},
             "clocks": clocks,
         }
         if world == 1 and not args.no_cpu_baseline:

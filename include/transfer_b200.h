@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define TR_ABI_VERSION 1
+#define TR_ABI_VERSION 2
 
 /* Vertex / element index type (util.h:6 `typedef uint32_t idx`). */
 typedef uint32_t tr_idx;
@@ -234,6 +234,10 @@ typedef struct tr_solve_report {
     double  device_ms;           /* device time of the solve (CUDA events)    */
     int64_t kernel_launches;     /* kernels of this library launched (graph
                                     nodes counted one by one)               */
+    double  cg_kernel_ms;        /* device time of the CG-iteration launches
+                                    (persistent kernels or graph replays),
+                                    CUDA events around each                 */
+    int64_t cg_kernel_launches;  /* those launches                           */
 } tr_solve_report;
 
 void tr_solve_opts_default(tr_solve_opts *opts);   /* reference settings */
@@ -250,7 +254,8 @@ tr_status tr_solve_host(tr_ctx *ctx, const tr_solve_opts *opts,
 /* Measurement helper (no reference counterpart): launches the operator
  * (precision 64: tr_compute_lhs, 32: tr_compute_lhs_f32) `iters` times back
  * to back on the context stream from x into y (device vectors of that
- * precision) and returns the mean device time per launch from CUDA events. */
+ * precision), after 3 untimed launches, and returns the mean device time
+ * per launch from CUDA events. */
 tr_status tr_bench_lhs(tr_ctx *ctx, int precision, const void *x, void *y,
                        int iters, double *ms_per_launch);
 

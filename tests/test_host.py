@@ -41,7 +41,7 @@ def test_record_layouts_match_reference():
 
 
 def test_abi_version_and_status_strings():
-    assert tr.lib.tr_abi_version() == 1
+    assert tr.lib.tr_abi_version() == tr._lib.ABI_VERSION == 2
     assert tr.lib.tr_status_string(0) == b"ok"
     assert tr.lib.tr_status_string(3) == b"not converged"
 

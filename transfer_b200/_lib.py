@@ -11,6 +11,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libtransfer_b200.so")
 
 tr_idx = C.c_uint32
+ABI_VERSION = 2  # TR_ABI_VERSION of the header these structures mirror
 
 # status codes (tr_status)
 TR_OK = 0
@@ -78,7 +79,8 @@ class tr_solve_report(C.Structure):
                 ("outer_steps", C.c_int32), ("lhs_applications_f64", C.c_int64),
                 ("lhs_applications_f32", C.c_int64), ("diag_applications", C.c_int64),
                 ("initial_residual", C.c_double), ("final_residual", C.c_double),
-                ("rhs_norm", C.c_double), ("device_ms", C.c_double), ("kernel_launches", C.c_int64)]
+                ("rhs_norm", C.c_double), ("device_ms", C.c_double), ("kernel_launches", C.c_int64),
+                ("cg_kernel_ms", C.c_double), ("cg_kernel_launches", C.c_int64)]
 
 
 class tr_region_params(C.Structure):
@@ -171,6 +173,9 @@ def load(path=LIB_PATH):
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
+    if lib.tr_abi_version() != ABI_VERSION:
+        raise ImportError(f"{path} has ABI version {lib.tr_abi_version()}, this binding expects {ABI_VERSION}: "
+                          "rebuild it with `make -C transfer_b200/csrc`")
     return lib
 
 

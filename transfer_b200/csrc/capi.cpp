@@ -322,13 +322,18 @@ tr_status tr_bench_lhs(tr_ctx *c, int precision, const void *x, void *y, int ite
     tr_status s = check_cuda(c, cudaEventCreate(&e0), "event");
     if (s != TR_OK) return s;
     cudaEventCreate(&e1);
-    cudaEventRecord(e0, st);
+    auto launch = [&]() {
+        return precision == 64 ? launch_lhs<double>(c, c->op64, static_cast<const double *>(x),
+                                                    static_cast<double *>(y), 0, nullptr, nullptr, nullptr, st)
+                               : launch_lhs<float>(c, c->op32, static_cast<const float *>(x), static_cast<float *>(y),
+                                                   0, nullptr, nullptr, nullptr, st);
+    };
+    // untimed warm-up: the first launch of a kernel loads its module
     cudaError_t e = cudaSuccess;
-    for (int i = 0; i < iters && e == cudaSuccess; ++i)
-        e = precision == 64 ? launch_lhs<double>(c, c->op64, static_cast<const double *>(x), static_cast<double *>(y),
-                                                 0, nullptr, nullptr, nullptr, st)
-                            : launch_lhs<float>(c, c->op32, static_cast<const float *>(x), static_cast<float *>(y), 0,
-                                                nullptr, nullptr, nullptr, st);
+    for (int i = 0; i < 3 && e == cudaSuccess; ++i) e = launch();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaEventRecord(e0, st);
+    for (int i = 0; i < iters && e == cudaSuccess; ++i) e = launch();
     cudaEventRecord(e1, st);
     s = check_cuda(c, e, "bench launch");
     if (s == TR_OK) s = check_cuda(c, cudaEventSynchronize(e1), "bench sync");

@@ -110,6 +110,8 @@ void ctx_free(tr_ctx *c) {
     if (c->host_pinned) cudaFreeHost(c->host_pinned);
     if (c->stage_in) cudaFreeHost(c->stage_in);
     if (c->stage_out) cudaFreeHost(c->stage_out);
+    for (cudaEvent_t e : c->ev)
+        if (e) cudaEventDestroy(e);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
 }
@@ -378,7 +380,13 @@ tr_status ctx_create(int device, const tr_mesh_view *m, const tr_angular_view *a
     ok(upload(c, &o64.co_tc, cotc.data(), cotc.size() * 2));
     o32.co_tc = o64.co_tc;
     ok(upload(c, &o64.coef, coef.data(), coef.size() * 8));
-    ok(upload(c, &o64.O, O.data(), O.size() * 8));
+    // operator copy of O_n, rows lms padded to the lane stride cls
+    std::vector<double> Opad(3 * static_cast<size_t>(slm) * cls, 0.0);
+    for (int n = 0; n < 3; ++n)
+        for (tr_idx lms = 0; lms < slm; ++lms)
+            for (tr_idx lm = 0; lm < slm; ++lm)
+                Opad[(static_cast<size_t>(n) * slm + lms) * cls + lm] = On[n][static_cast<size_t>(lms) * slm + lm];
+    ok(upload(c, &o64.O, Opad.data(), Opad.size() * 8));
     ok(upload(c, &o64.ang_diag, ang_diag.data(), ang_diag.size() * 8));
     ok(upload(c, &o64.O_diag, O_diag.data(), O_diag.size() * 8));
     ok(upload(c, &o64.dinv, dinv.data(), dinv.size() * 8));
@@ -390,7 +398,7 @@ tr_status ctx_create(int device, const tr_mesh_view *m, const tr_angular_view *a
     {
         auto c32 = to_type<float>(coef);
         ok(upload(c, &o32.coef, c32.data(), c32.size() * 4));
-        auto O32 = to_type<float>(O);
+        auto O32 = to_type<float>(Opad);
         ok(upload(c, &o32.O, O32.data(), O32.size() * 4));
         auto d32 = to_type<float>(ang_diag);
         ok(upload(c, &o32.ang_diag, d32.data(), d32.size() * 4));

@@ -60,7 +60,7 @@ struct OpData {
     const T *cw;                     // [ckmax][cls] weights
     const uint16_t *co;              // [ckmax][cls] offsets, SIMT S table
     const uint16_t *co_tc;           // [ckmax][cls] offsets, tensor-core C table
-    const T *O;                      // [3][slm][slm]: O_n[lms][lm]
+    const T *O;                      // [3][slm][cls]: O_n[lms][lm], rows padded to cls
     const T *ang_diag;               // [3][slm]: omega_i[lm][lm]
     const T *O_diag;                 // [3][slm]: O_n[lm][lm]
     const T *mask;                   // [nP][aslm] reflective constraint or null
@@ -227,6 +227,9 @@ struct tr_ctx {
 
     std::vector<void *> allocations;
     int64_t launches = 0;            // kernels launched (for solve reports)
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // solve [0,1], CG launches [2,3]
+    double cg_ms = 0.0;              // device time of the CG-iteration launches of a solve
+    int64_t cg_launches = 0;         // those launches (persistent kernels or graph replays)
 };
 
 namespace transfer {

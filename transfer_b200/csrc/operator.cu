@@ -132,8 +132,8 @@ struct Staged {
     size_t bytes;
 };
 template <typename T>
-__host__ __device__ inline size_t O_smem_bytes(uint32_t slm) {
-    return align16(3 * static_cast<size_t>(slm) * slm * sizeof(T));
+__host__ __device__ inline size_t O_smem_bytes(uint32_t slm, uint32_t cls) {
+    return align16(3 * static_cast<size_t>(slm) * cls * sizeof(T));
 }
 
 // flags: 1 stage the contraction tables, 2 stage O, 4 use the tensor-core
@@ -156,10 +156,10 @@ __device__ __forceinline__ Staged<T> stage_tables(const OpData<T> &d, unsigned c
     }
     if (flags & 2) {
         T *so = reinterpret_cast<T *>(smem + st.bytes);
-        const uint32_t n = 3 * d.slm * d.slm;
+        const uint32_t n = 3 * d.slm * d.cls;
         for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) so[i] = __ldg(d.O + i);
         st.O = so;
-        st.bytes += O_smem_bytes<T>(d.slm);
+        st.bytes += O_smem_bytes<T>(d.slm, d.cls);
     }
     if (flags & 3) __syncthreads();
     return st;
@@ -180,6 +180,22 @@ __device__ __forceinline__ T contract(const Staged<T> &tab, const T *S, uint32_t
         acc3 = fma(w[(k + 3) * ls], S[o[(k + 3) * ls]], acc3);
     }
     for (; k < kmax; ++k) acc0 = fma(w[k * ls], S[o[k * ls]], acc0);
+    return (acc0 + acc2) + (acc1 + acc3);
+}
+
+// the same with the lane stride LS of the tables known at compile time
+template <typename T, int LS>
+__device__ __forceinline__ T contract_ls(const T *__restrict__ w, const uint16_t *__restrict__ o, const T *S,
+                                         uint32_t kmax, T acc0) {
+    T acc1 = T(0), acc2 = T(0), acc3 = T(0);
+    uint32_t k = 0;
+    for (; k + 3 < kmax; k += 4, w += 4 * LS, o += 4 * LS) {
+        acc0 = fma(w[0], S[o[0]], acc0);
+        acc1 = fma(w[LS], S[o[LS]], acc1);
+        acc2 = fma(w[2 * LS], S[o[2 * LS]], acc2);
+        acc3 = fma(w[3 * LS], S[o[3 * LS]], acc3);
+    }
+    for (; k < kmax; ++k, w += LS, o += LS) acc0 = fma(w[0], S[o[0]], acc0);
     return (acc0 + acc2) + (acc1 + acc3);
 }
 
@@ -210,6 +226,7 @@ __device__ __forceinline__ double lhs_vertices(const OpData<T> &d, const Staged<
                                                T *__restrict__ pnew, T *__restrict__ r, const T beta) {
     constexpr int SA = G * H + 1;  // padded row of the shared S / B tables
     constexpr int NB = batch_of(H);
+    constexpr int LS = G * H < 32 ? 32 : G * H;  // lane stride of the tables (== d.cls, checked at launch)
     const uint32_t slm = d.slm, aslm = d.aslm;
     T *scoef = reinterpret_cast<T *>(smem_groups) + (threadIdx.x / G) * group_smem_elems<G, H, T>();
     T *sm = scoef + G * kCoefStride;
@@ -286,7 +303,7 @@ __device__ __forceinline__ double lhs_vertices(const OpData<T> &d, const Staged<
 #pragma unroll
         for (int h = 0; h < H; ++h) {
             const uint32_t lm = lane + G * h;
-            out[h] = (lm < d.cls) ? contract<T>(tab, sm, lm, d.ckmax, d.cls, mass[h]) : mass[h];
+            out[h] = contract_ls<T, LS>(tab.cw + lm, tab.co + lm, sm, d.ckmax, mass[h]);
         }
         // half-range boundary term from the per-axis sums B_n
         if (axes) {
@@ -300,19 +317,21 @@ __device__ __forceinline__ double lhs_vertices(const OpData<T> &d, const Staged<
             for (int h = 0; h < H; ++h) {
                 const uint32_t lm = lane + G * h;
                 if (lm < slm) {
-                    T acc0 = T(0), acc1 = T(0);
+                    T acc0 = T(0), acc1 = T(0), acc2 = T(0), acc3 = T(0);
                     for (int n = 0; n < 3; ++n) {
                         if (!(axes & (1u << n))) continue;
-                        const T *On = tab.O + static_cast<size_t>(n) * slm * slm + lm;
+                        const T *On = tab.O + static_cast<size_t>(n) * slm * LS + lm;
                         const T *Bn = sm + n * SA;
                         uint32_t lms = 0;
-                        for (; lms + 1 < slm; lms += 2) {
-                            acc0 = fma(On[lms * slm], Bn[lms], acc0);
-                            acc1 = fma(On[(lms + 1) * slm], Bn[lms + 1], acc1);
+                        for (; lms + 3 < slm; lms += 4, On += 4 * LS) {
+                            acc0 = fma(On[0], Bn[lms], acc0);
+                            acc1 = fma(On[LS], Bn[lms + 1], acc1);
+                            acc2 = fma(On[2 * LS], Bn[lms + 2], acc2);
+                            acc3 = fma(On[3 * LS], Bn[lms + 3], acc3);
                         }
-                        if (lms < slm) acc0 = fma(On[lms * slm], Bn[lms], acc0);
+                        for (; lms < slm; ++lms, On += LS) acc0 = fma(On[0], Bn[lms], acc0);
                     }
-                    out[h] += acc0 + acc1;
+                    out[h] += (acc0 + acc2) + (acc1 + acc3);
                 }
             }
         }
@@ -533,14 +552,15 @@ __device__ __forceinline__ double lhs_vertices_tc(const OpData<T> &d, const Stag
                 if (axes) {
                     for (int n = 0; n < 3; ++n) {
                         if (!(axes & (1u << n))) continue;
-                        const T *On = tab.O + static_cast<size_t>(n) * slm * slm + lm;
+                        const T *On = tab.O + static_cast<size_t>(n) * slm * d.cls + lm;
                         const T *Bn = sm + (kRowE + n) * SA;
+                        const uint32_t ls = d.cls;
                         uint32_t lms = 0;
                         for (; lms + 1 < slm; lms += 2) {
-                            acc0 = fma(On[lms * slm], Bn[lms], acc0);
-                            acc1 = fma(On[(lms + 1) * slm], Bn[lms + 1], acc1);
+                            acc0 = fma(On[lms * ls], Bn[lms], acc0);
+                            acc1 = fma(On[(lms + 1) * ls], Bn[lms + 1], acc1);
                         }
-                        if (lms < slm) acc0 = fma(On[lms * slm], Bn[lms], acc0);
+                        if (lms < slm) acc0 = fma(On[lms * ls], Bn[lms], acc0);
                     }
                 }
                 out = acc0 + acc1;
@@ -561,10 +581,16 @@ __device__ __forceinline__ double lhs_vertices_tc(const OpData<T> &d, const Stag
 // An operator policy supplies the per-block vertex loop and its shared
 // memory: SimtOp (groups of G lanes, H harmonics per lane, FMA pipes) or
 // TcOp (one warp per vertex, NT n-tiles, tensor pipes).
+// resident blocks per SM the FP32 single-harmonic SIMT kernels are compiled
+// for (register cap 65536 / (256 * blocks))
+#ifndef TR_SIMT_F32_MINBLOCKS
+#define TR_SIMT_F32_MINBLOCKS 3
+#endif
 template <int G, int H, typename T>
 struct SimtOp {
-    static constexpr int kMinBlocks = sizeof(T) == 8 ? (H > 2 ? 1 : 2) : (H > 1 ? 2 : 3);
+    static constexpr int kMinBlocks = sizeof(T) == 8 ? (H > 2 ? 1 : 2) : (H > 1 ? 2 : TR_SIMT_F32_MINBLOCKS);
     static constexpr int kLanes = G;
+    static constexpr uint32_t kLS = G * H < 32 ? 32 : G * H;  // lane stride of the contraction tables
     static constexpr bool kTc = false;
     static size_t slab_bytes() { return (kBlock / G) * group_smem_elems<G, H, T>() * sizeof(T); }
     template <bool DOT, bool FUSEP, bool COH>
@@ -577,6 +603,7 @@ template <int NT, typename T>
 struct TcOp {
     static constexpr int kMinBlocks = NT > 6 ? 1 : 2;  // up to 128 registers: loads in flight over occupancy
     static constexpr int kLanes = 32;
+    static constexpr uint32_t kLS = 0;  // any lane stride
     static constexpr bool kTc = true;
     static size_t slab_bytes() { return align16((kBlock / 32) * 16 * TcShape<NT>::SA * sizeof(T)); }
     template <bool DOT, bool FUSEP, bool COH>
@@ -825,18 +852,28 @@ constexpr size_t kAngSmemBudget = 64 * 1024;
 constexpr size_t kOSmemBudget = 40 * 1024;
 
 template <class Op, typename T>
-static int stage_flags(uint32_t slm, uint32_t nnz) {
-    return (ang_smem_bytes<T>(nnz) <= kAngSmemBudget ? 1 : 0) | (O_smem_bytes<T>(slm) <= kOSmemBudget ? 2 : 0) |
+static int stage_flags(uint32_t slm, uint32_t cls, uint32_t nnz) {
+    return (ang_smem_bytes<T>(nnz) <= kAngSmemBudget ? 1 : 0) | (O_smem_bytes<T>(slm, cls) <= kOSmemBudget ? 2 : 0) |
            (Op::kTc ? 4 : 0);
 }
 template <class Op, typename T>
-static size_t lhs_smem(uint32_t slm, uint32_t nnz) {
-    const int fl = stage_flags<Op, T>(slm, nnz);
-    return ((fl & 1) ? ang_smem_bytes<T>(nnz) : 0) + ((fl & 2) ? O_smem_bytes<T>(slm) : 0) + Op::slab_bytes();
+static size_t lhs_smem(uint32_t slm, uint32_t cls, uint32_t nnz) {
+    const int fl = stage_flags<Op, T>(slm, cls, nnz);
+    return ((fl & 1) ? ang_smem_bytes<T>(nnz) : 0) + ((fl & 2) ? O_smem_bytes<T>(slm, cls) : 0) + Op::slab_bytes();
 }
 
+// preferred shared-memory carveout (percent of the unified L1/shared array)
+// of the operator kernels; negative leaves the driver's choice
+#ifndef TR_SMEM_CARVEOUT
+#define TR_SMEM_CARVEOUT -1
+#endif
 template <class K>
 static cudaError_t opt_in_smem(K kern, size_t smem, size_t &opted) {
+    if (TR_SMEM_CARVEOUT >= 0 && opted == 0) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, TR_SMEM_CARVEOUT);
+        if (e != cudaSuccess) return e;
+        opted = 1;
+    }
     if (smem > 48 * 1024 && smem > opted) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
         if (e != cudaSuccess) return e;
@@ -870,7 +907,8 @@ static cudaError_t with_op(const DeviceOp<T> &op, uint32_t slm, F &&fn) {
 
 template <class Op, typename T, bool DOT, bool FUSEP, class Fin>
 static cudaError_t launch_one(const tr_ctx *c, const OpData<T> &d, const LhsArgs<T> &a, Fin fin, cudaStream_t s) {
-    const size_t smem = lhs_smem<Op, T>(d.slm, a.ang_nnz);
+    if (Op::kLS && d.cls != Op::kLS) return cudaErrorInvalidValue;  // tables built for another lane stride
+    const size_t smem = lhs_smem<Op, T>(d.slm, d.cls, a.ang_nnz);
     auto kern = k_lhs<Op, T, DOT, FUSEP, Fin>;
     static size_t opted = 0;  // dynamic shared memory granted so far (per instantiation)
     cudaError_t e = opt_in_smem(kern, smem, opted);
@@ -878,7 +916,7 @@ static cudaError_t launch_one(const tr_ctx *c, const OpData<T> &d, const LhsArgs
     const int gpb = kBlock / Op::kLanes;
     const int grid = std::max(1, std::min(c->num_sms * 4, static_cast<int>((d.nP + gpb - 1) / gpb)));
     kern<<<grid, kBlock, smem, s>>>(d, a.x, a.pold, a.pnew, a.y, c->partials, c->counters, fin, a.done, a.cgs,
-                                    stage_flags<Op, T>(d.slm, a.ang_nnz));
+                                    stage_flags<Op, T>(d.slm, d.cls, a.ang_nnz));
     return cudaGetLastError();
 }
 
@@ -928,8 +966,9 @@ cudaError_t launch_lhs_diag(const tr_ctx *c, const DeviceOp<T> &op, const T *f, 
 template <class Op, typename T, bool JAC>
 static cudaError_t launch_pcg(const tr_ctx *c, const OpData<T> &d, const PcgArgs<T> &a, uint32_t nnz, cudaStream_t s,
                               int *grid_out) {
+    if (Op::kLS && d.cls != Op::kLS) return cudaErrorInvalidValue;
     auto kern = k_cg_persistent<Op, T, JAC>;
-    const size_t smem = lhs_smem<Op, T>(d.slm, nnz);
+    const size_t smem = lhs_smem<Op, T>(d.slm, d.cls, nnz);
     static size_t opted = 0;
     cudaError_t e = opt_in_smem(kern, smem, opted);
     if (e != cudaSuccess) return e;
@@ -942,7 +981,7 @@ static cudaError_t launch_pcg(const tr_ctx *c, const OpData<T> &d, const PcgArgs
     const int need = static_cast<int>((d.nP + gpb - 1) / gpb);
     const int grid = std::max(1, std::min(per_sm * c->num_sms, std::min(need, kMaxGrid)));
     *grid_out = grid;
-    int flags = stage_flags<Op, T>(d.slm, nnz);
+    int flags = stage_flags<Op, T>(d.slm, d.cls, nnz);
     OpData<T> dd = d;
     PcgArgs<T> aa = a;
     void *args[] = {&dd, &aa, &flags};

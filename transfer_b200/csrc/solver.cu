@@ -150,6 +150,13 @@ static tr_status read_double(tr_ctx *c, const double *d, double *out, cudaStream
     return TR_OK;
 }
 
+// adds the device time between ev[2] and ev[3] (both complete) to cg_ms
+static void add_cg_time(tr_ctx *c) {
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]) == cudaSuccess) c->cg_ms += ms;
+    ++c->cg_launches;
+}
+
 // One CG iteration of precision T (two launches, all on device state).
 // parity selects which p buffer holds p_old.
 template <typename T>
@@ -200,6 +207,7 @@ static tr_status run_cg(tr_ctx *c, int slot, const DeviceOp<T> &op, uint32_t asl
         int k = 0, done = 0;
         for (int guard = 0; guard < (1 << 24); ++guard) {
             int grid = 0;
+            TRY(cudaEventRecord(c->ev[2], st));
             cudaError_t e = launch_cg_persistent<T>(c, op, a, st, &grid);
             if (e == cudaErrorCooperativeLaunchTooLarge || e == cudaErrorNotSupported) {
                 cudaGetLastError();  // this device cannot co-schedule the grid: replay graphs instead
@@ -207,6 +215,7 @@ static tr_status run_cg(tr_ctx *c, int slot, const DeviceOp<T> &op, uint32_t asl
                                  iters, done_out);
             }
             TRY(e);
+            TRY(cudaEventRecord(c->ev[3], st));
             ++c->launches;
             int32_t *h = reinterpret_cast<int32_t *>(c->host_pinned);
             TRY(cudaMemcpyAsync(h, &s->k, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
@@ -214,6 +223,7 @@ static tr_status run_cg(tr_ctx *c, int slot, const DeviceOp<T> &op, uint32_t asl
             TRY(cudaStreamSynchronize(st));
             k = h[0];
             done = h[1];
+            add_cg_time(c);
             if (h[2]) {
                 c->last_error = "persistent CG: grid barrier timed out";
                 cudaMemsetAsync(c->bar_err, 0, sizeof(int), st);
@@ -254,6 +264,7 @@ static tr_status run_cg(tr_ctx *c, int slot, const DeviceOp<T> &op, uint32_t asl
     }
     int k = 0, done = 0;
     for (int guard = 0; guard < (1 << 24); ++guard) {
+        TRY(cudaEventRecord(c->ev[2], st));
         if (use_graph) {
             TRY(cudaGraphLaunch(g.exec, st));
             c->launches += 2 * chunk;
@@ -261,8 +272,10 @@ static tr_status run_cg(tr_ctx *c, int slot, const DeviceOp<T> &op, uint32_t asl
             for (int i = 0; i < chunk; ++i)
                 TRY(cg_iteration<T>(c, op, aslm, x, r, pbuf, Ap, z, dinv, s, hist, hcap, i & 1, st));
         }
+        TRY(cudaEventRecord(c->ev[3], st));
         tr_status rs = read_status(c, s, &k, &done, st);
         if (rs != TR_OK) return rs;
+        add_cg_time(c);
         if (done) break;
     }
     *iters = k;
@@ -447,9 +460,11 @@ tr_status solve(tr_ctx *c, const tr_solve_opts *o, const double *b_in, double *f
     const int64_t launches0 = c->launches;
     tr_status ts = ensure_workspace(c, std::max(o->max_iter, 1));
     if (ts != TR_OK) return ts;
-    cudaEvent_t e0, e1;
-    TRY(cudaEventCreate(&e0));
-    TRY(cudaEventCreate(&e1));
+    for (cudaEvent_t &e : c->ev)
+        if (!e) TRY(cudaEventCreate(&e));
+    c->cg_ms = 0.0;
+    c->cg_launches = 0;
+    cudaEvent_t e0 = c->ev[0], e1 = c->ev[1];
     TRY(cudaEventRecord(e0, st));
     double *b = c->w64[5];
     if (b_in) TRY(cudaMemcpyAsync(b, b_in, sizeof(double) * c->nP * c->aslm, cudaMemcpyDeviceToDevice, st));
@@ -478,8 +493,8 @@ tr_status solve(tr_ctx *c, const tr_solve_opts *o, const double *b_in, double *f
     cudaEventElapsedTime(&ms, e0, e1);
     rep->device_ms = ms;
     rep->kernel_launches = c->launches - launches0;
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    rep->cg_kernel_ms = c->cg_ms;
+    rep->cg_kernel_launches = c->cg_launches;
     if (solve_status != TR_OK) return solve_status;
     if (!rep->converged) {
         c->last_error = "solver reached its iteration limit before the tolerance";

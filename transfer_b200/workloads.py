@@ -88,3 +88,13 @@ def algorithmic_work(md, ad, real_bytes=8):
     byt = 2 * real_bytes * md.nP * slm + 24 * md.nT + 24 * md.nP + 12 * md.nF
     flops = 108 * md.nT * slm + 2 * nnz * md.nP + 6 * md.nF * slm * slm
     return byt, flops
+
+
+def cg_iteration_work(md, ad, real_bytes=8):
+    """Per CG iteration: the operator application (algorithmic_work) plus the
+    vector traffic of the iteration (main.cpp:139-158): x += alpha p (3 vector
+    passes), r -= alpha Ap (3), p = z + beta p (3) and Ap read once more for
+    <p, Ap> (1), ten passes of real_bytes * nP * slm; 2 flops per entry and
+    pass-pair (10 nP slm)."""
+    byt, flops = algorithmic_work(md, ad, real_bytes)
+    return byt + 10 * real_bytes * md.nP * ad.slm, flops + 10 * md.nP * ad.slm
