@@ -179,6 +179,26 @@ tr_status tr_mul_add_prod(tr_ctx *ctx, double *x, double wx,
 tr_status tr_norm(tr_ctx *ctx, const double *x, double *out);
 tr_status tr_dot(tr_ctx *ctx, const double *x, const double *y, double *out);
 
+/* tr_dot without a context and without allocating (no counterpart in the
+ * reference).  For callers that may not call cudaMalloc here: a host whose
+ * memory pool owns all device memory, a loop where cudaMalloc/cudaFree would
+ * synchronise the device, or a caller without a tr_ctx (creating one
+ * allocates).  x, y: FP64 device vectors [nP][aslm] on the current device;
+ * the sum runs over lm < slm.  out: ONE double of device memory, written by
+ * a kernel queued on `stream` (cudaStream_t as void*, NULL = legacy default
+ * stream); the call returns without waiting for it.  Limit: nP * aslm <=
+ * 33,554,432 entries, else TR_ERR_INVALID_ARG (message in
+ * tr_last_error(NULL)).  Its scratch is one static device array of about
+ * 16 KiB per GPU, shared by all calls: calls that overlap on the GPU race
+ * and must be ordered by the caller.  The first call on a device looks up
+ * that array's device address (set-up work), so make it before any stream
+ * capture on that device.  Summation order depends only on nP * aslm, so the
+ * bits do not depend on the GPU; they may differ from tr_dot's in the last
+ * places. */
+tr_status tr_dot_noalloc(const double *x, const double *y, uint32_t nP,
+                         uint32_t aslm, uint32_t slm, double *out,
+                         void *stream);
+
 /* FP32 variants (the reference's default REAL=float build): vectors with
  * aslm_f32 padding, operator tables rounded to float once at creation. */
 tr_status tr_compute_lhs_f32(tr_ctx *ctx, const float *f, float *Af);

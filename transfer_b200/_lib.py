@@ -119,6 +119,7 @@ PROTOTYPES = [
     ("tr_mul_add_prod", S, [P, P, D, P, D]),
     ("tr_norm", S, [P, P, C.POINTER(D)]),
     ("tr_dot", S, [P, P, P, C.POINTER(D)]),
+    ("tr_dot_noalloc", S, [P, P, C.c_uint32, C.c_uint32, C.c_uint32, P, P]),
     ("tr_compute_lhs_f32", S, [P, P, P]),
     ("tr_compute_lhs_diag_f32", S, [P, P, P]),
     ("tr_compute_rhs_f32", S, [P, P]),

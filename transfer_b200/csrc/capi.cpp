@@ -33,6 +33,11 @@ static tr_status set_err(tr_ctx *c, tr_status st, const std::string &msg) {
     g_last_error = msg;
     return st;
 }
+namespace transfer {
+// records a failure that belongs to no context (tr_last_error(NULL))
+tr_status set_global_error(tr_status st, const std::string &msg) { return set_err(nullptr, st, msg); }
+}  // namespace transfer
+
 static cudaStream_t stream_of(const tr_ctx *c) { return c->stream ? c->stream : c->own_stream; }
 
 static tr_status check_cuda(tr_ctx *c, cudaError_t e, const char *what) {
