@@ -181,6 +181,20 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+# ----------------------------------------------------------------- replicas
+def aggregate_replicas(times_ms, updates, dist=None, device="cpu"):
+    """Whole-job figures of N independent replicas: each time is the slowest
+    rank's (max over ranks), each update count the sum over ranks.  dist is
+    torch.distributed (initialised) or None for one process."""
+    import torch
+    t = torch.tensor([float(x) for x in times_ms], dtype=torch.float64, device=device)
+    u = torch.tensor([float(x) for x in updates], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(u, op=dist.ReduceOp.SUM)
+    return [float(x) for x in t.cpu()], [float(x) for x in u.cpu()]
+
+
 # ----------------------------------------------------------------- GPU arm
 def run_ours(args, rank, world, local):
     import numpy as np
@@ -264,10 +278,8 @@ def run_ours(args, rank, world, local):
     tr.check(tr.lib.tr_bench_lhs(ctx._h, 32, x32.data_ptr(), y32.data_ptr(), 200, C.byref(ms32)), ctx._h)
     tr.check(tr.lib.tr_bench_lhs(ctx._h, 64, x64.data_ptr(), y64.data_ptr(), 200, C.byref(ms64)), ctx._h)
 
-    vals = torch.tensor([t_mixed, t_fp64, t_e2e], dtype=torch.float64, device=f"cuda:{local}")
-    if pg:
-        pg.all_reduce(vals, op=pg.ReduceOp.MAX)
-    t_mixed, t_fp64, t_e2e = [float(x) for x in vals.cpu()]
+    (t_mixed, t_fp64, t_e2e), (u_mixed, u_fp64, u_e2e) = aggregate_replicas(
+        [t_mixed, t_fp64, t_e2e], [u_mixed, u_fp64, u_e2e], pg, f"cuda:{local}")
 
     if rank == 0:
         peak, peak_kind = load_peaks()
@@ -289,7 +301,7 @@ def run_ours(args, rank, world, local):
         it_fp64 = statistics.mean(r.iterations for r in reps_fp64)
         line = {
             "metric": METRIC,
-            "value": world * u_mixed / (t_mixed * 1e-3),
+            "value": u_mixed / (t_mixed * 1e-3),
             "unit": UNIT,
             "n_gpus": world,
             "steps": args.steps,
@@ -309,13 +321,13 @@ def run_ours(args, rank, world, local):
             },
             "time_to_solution_ms": {"mixed": t_mixed / args.steps, "fp64": t_fp64 / args.steps,
                                     "speedup_mixed_vs_fp64": t_fp64 / t_mixed},
-            "fp64": {"value": world * u_fp64 / (t_fp64 * 1e-3), "unit": UNIT, "iterations": it_fp64},
+            "fp64": {"value": u_fp64 / (t_fp64 * 1e-3), "unit": UNIT, "iterations": it_fp64},
             "iterations": {"mixed_fp32_cg": it_mixed,
                            "mixed_outer": statistics.mean(r.outer_steps for r in reps_mixed),
                            "fp64_cg": it_fp64},
             "final_relative_residual": {"mixed": max(r.final_residual / r.rhs_norm for r in reps_mixed),
                                         "fp64": max(r.final_residual / r.rhs_norm for r in reps_fp64)},
-            "e2e": {"value": world * u_e2e / (t_e2e * 1e-3), "unit": UNIT,
+            "e2e": {"value": u_e2e / (t_e2e * 1e-3), "unit": UNIT,
                     "h2d_bytes_per_step": 8 * ctx.N(), "d2h_bytes_per_step": 8 * ctx.N()},
             "gpu_launches": int(l_mixed),
             "roofline": {"bound": "hbm", "achieved": ach_cg, "peak": peak, "unit": "GB/s", "frac": ach_cg / peak,
