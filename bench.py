@@ -117,9 +117,11 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
-# DRAM bytes (read + write) of one persistent-kernel launch from an ncu capture
-# of that launch, per CG iteration, by workload (0 iterations: none captured)
-NCU_TRAFFIC_PER_ITERATION = {}
+# DRAM bytes (read + write) of one launch of the persistent FP32 CG kernel,
+# from one ncu capture of that launch (profiles/k_cg_persistent_simt_f32_milne_slab.md);
+# the iteration working set is L2-resident, so this is first-touch traffic
+# and does not grow with the iterations of the launch
+NCU_TRAFFIC_PER_LAUNCH = {"milne_slab": 16.880640e6 + 0.595712e6}
 
 
 def operator_policy(tensor, slm, aslm, real):
@@ -133,9 +135,8 @@ def operator_policy(tensor, slm, aslm, real):
     return f"SimtOp<{g},{h},{real}>"
 
 
-def traffic_per_launch(workload, iters_per_launch):
-    t = NCU_TRAFFIC_PER_ITERATION.get(workload)
-    return None if t is None else t * iters_per_launch
+def traffic_per_launch(workload):
+    return NCU_TRAFFIC_PER_LAUNCH.get(workload)
 
 
 # ----------------------------------------------------------------- CPU arm
@@ -331,7 +332,7 @@ def run_ours(args, rank, world, local):
                     "h2d_bytes_per_step": 8 * ctx.N(), "d2h_bytes_per_step": 8 * ctx.N()},
             "gpu_launches": int(l_mixed),
             "roofline": {"bound": "hbm", "achieved": ach_cg, "peak": peak, "unit": "GB/s", "frac": ach_cg / peak,
-                         "traffic": traffic_per_launch(args.workload, cg_iters / cg_launches),
+                         "traffic": traffic_per_launch(args.workload),
                          "peak_source": peak_kind,
                          "kernel": f"k_cg_persistent<{pol32}> (FP32 CG iterations of the mixed solve)",
                          "us_per_launch": 1e3 * cg_ms / cg_launches,
