@@ -101,8 +101,9 @@ struct CgScalars {
 
 // Arguments of the persistent CG kernel (one cooperative launch runs up to
 // `iters` iterations).  p0 / p1 alternate as p_old / p_new by the parity of
-// the iteration count; partials holds [3][grid] per-block sums; bar[2] is
-// the grid barrier's arrival count and generation, err its timeout flag.
+// the iteration count; partials holds [3][grid] per-block sums; bar[0] is
+// the grid barrier's monotone arrival count (zeroed before every launch),
+// err its timeout flag.
 template <typename T>
 struct PcgArgs {
     T *x, *r, *z, *p0, *p1, *Ap;

@@ -97,11 +97,14 @@ __host__ __device__ constexpr size_t group_smem_elems() {
     return (G * kCoefStride + kSymRows * (G * H + 1) + (16 / sizeof(T)) - 1) / (16 / sizeof(T)) * (16 / sizeof(T));
 }
 
-// loads of vectors that other blocks of the same launch may have written
-// (persistent kernel) bypass the non-coherent read-only path: L2 only
+// Loads of vectors that other blocks of the same launch may have written
+// (persistent kernel) avoid the non-coherent read-only path (ld.global.nc
+// requires data that no thread writes during the kernel) and use ordinary
+// cached loads (ld.global.ca); they only read data written before the last
+// grid barrier, whose fences order those writes before these loads.
 template <bool COH, typename T>
 __device__ __forceinline__ T ldv(const T *p) {
-    return COH ? __ldcg(p) : __ldg(p);
+    return COH ? __ldca(p) : __ldg(p);
 }
 
 // x_u = f[u] (plain) or z[u] + beta p_old[u] (fused CG direction)
@@ -232,7 +235,7 @@ __device__ __forceinline__ double lhs_vertices(const OpData<T> &d, const Staged<
     T *sm = scoef + G * kCoefStride;
     cg::thread_block_tile<G> tile = cg::tiled_partition<G>(cg::this_thread_block());
     const int lane = threadIdx.x % G;
-    const uint32_t gpb = kBlock / G;
+    const uint32_t gpb = blockDim.x / G;
     const uint32_t ng = gridDim.x * gpb;
     double dacc = 0.0;
 
@@ -414,7 +417,7 @@ __device__ __forceinline__ double lhs_vertices_tc(const OpData<T> &d, const Stag
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int g = lane >> 2, t = lane & 3;
     T *sm = reinterpret_cast<T *>(smem_warps) + warp * 16 * SA;
-    const uint32_t wpb = kBlock / 32;
+    const uint32_t wpb = blockDim.x / 32;
     const uint32_t nw = gridDim.x * wpb;
     double dacc = 0.0;
 
@@ -592,7 +595,9 @@ struct SimtOp {
     static constexpr int kLanes = G;
     static constexpr uint32_t kLS = G * H < 32 ? 32 : G * H;  // lane stride of the contraction tables
     static constexpr bool kTc = false;
-    static size_t slab_bytes() { return (kBlock / G) * group_smem_elems<G, H, T>() * sizeof(T); }
+    // the persistent CG kernel runs all resident threads of an SM as one block
+    static constexpr int kPersistThreads = kBlock * kMinBlocks > 1024 ? 1024 : kBlock * kMinBlocks;
+    static size_t slab_bytes(int threads) { return (threads / G) * group_smem_elems<G, H, T>() * sizeof(T); }
     template <bool DOT, bool FUSEP, bool COH>
     __device__ static double run(const OpData<T> &d, const Staged<T> &tab, unsigned char *slabs, const T *f,
                                  const T *pold, T *pnew, T *r, T beta) {
@@ -605,7 +610,8 @@ struct TcOp {
     static constexpr int kLanes = 32;
     static constexpr uint32_t kLS = 0;  // any lane stride
     static constexpr bool kTc = true;
-    static size_t slab_bytes() { return align16((kBlock / 32) * 16 * TcShape<NT>::SA * sizeof(T)); }
+    static constexpr int kPersistThreads = kBlock * kMinBlocks > 1024 ? 1024 : kBlock * kMinBlocks;
+    static size_t slab_bytes(int threads) { return align16((threads / 32) * 16 * TcShape<NT>::SA * sizeof(T)); }
     template <bool DOT, bool FUSEP, bool COH>
     __device__ static double run(const OpData<T> &d, const Staged<T> &tab, unsigned char *slabs, const T *f,
                                  const T *pold, T *pnew, T *r, T beta) {
@@ -680,33 +686,32 @@ __global__ void __launch_bounds__(kBlock) k_lhs_diag(const OpData<T> d, const T 
 }
 
 // ------------------------------------------------------- persistent CG
-// Bounded sense-reversing grid barrier for a co-resident (cooperatively
-// launched) grid.  Gives up after kBarrierPolls polls, or as soon as another
-// block has given up: sets *err and returns false.
+// Bounded grid barrier for a co-resident (cooperatively launched) grid.
+// *count is a monotone arrival counter that the host zeroes before every
+// launch; barrier number n of the launch completes when it reaches
+// n * gridDim.x (`target` carries that per block).  One fire-and-forget add
+// per block and a poll: the critical path is one fence, one add and one
+// load.  Gives up after kBarrierPolls polls, or as soon as another block
+// has given up: sets *err and returns false.
 constexpr unsigned int kBarrierPolls = 1u << 24;
-__device__ __forceinline__ bool grid_barrier(unsigned int *count, unsigned int *gen, int *err) {
+__device__ __forceinline__ bool grid_barrier(unsigned int *count, int *err, unsigned int &target) {
     __shared__ int ok;
     __syncthreads();
+    target += gridDim.x;
     if (threadIdx.x == 0) {
         ok = 1;
-        const unsigned int g = atomicAdd(gen, 0u);
-        __threadfence();
-        if (atomicAdd(count, 1u) == gridDim.x - 1) {
-            atomicExch(count, 0u);
-            __threadfence();
-            atomicAdd(gen, 1u);
-        } else {
-            unsigned int polls = 0;
-            while (*reinterpret_cast<volatile unsigned int *>(gen) == g) {
-                if (++polls > kBarrierPolls || *reinterpret_cast<volatile int *>(err)) {
-                    atomicExch(err, 1);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(40);
+        __threadfence();  // this block's writes before its arrival
+        atomicAdd(count, 1u);
+        unsigned int polls = 0;
+        while (*reinterpret_cast<volatile unsigned int *>(count) < target) {
+            if (++polls > kBarrierPolls || *reinterpret_cast<volatile int *>(err)) {
+                atomicExch(err, 1);
+                ok = 0;
+                break;
             }
+            __nanosleep(32);
         }
-        __threadfence();
+        __threadfence();  // the other blocks' writes before this block's reads
     }
     __syncthreads();
     return ok != 0;
@@ -738,12 +743,13 @@ __device__ __forceinline__ void sum_partials(const double *partials, double (&to
 // test and beta.  The scalars never leave the device; block 0 mirrors them
 // (and the residual history) into CgScalars for the host.
 template <class Op, typename T, bool JAC>
-__global__ void __launch_bounds__(kBlock, Op::kMinBlocks)
+__global__ void __launch_bounds__(Op::kPersistThreads, 1)
     k_cg_persistent(const OpData<T> d, const PcgArgs<T> a, int stage_flags) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ double sh[32];
     const Staged<T> tab = stage_tables<T>(d, smem_raw, stage_flags);
     CgScalars *s = a.s;
+    unsigned int target = 0;  // grid_barrier arrival target
     int k = __ldcg(&s->k);
     if (__ldcg(&s->done)) return;
     const int maxit = s->maxit;
@@ -761,7 +767,7 @@ __global__ void __launch_bounds__(kBlock, Op::kMinBlocks)
                                                                pnew, a.Ap, static_cast<T>(beta));
         const double bs = block_sum(dacc, sh);
         if (threadIdx.x == 0) a.partials[blockIdx.x] = bs;
-        if (!grid_barrier(a.bar, a.bar + 1, a.err)) return;
+        if (!grid_barrier(a.bar, a.err, target)) return;
         double t1[1];
         sum_partials<1>(a.partials, t1);
         const double alpha_d = nrz / t1[0];
@@ -798,7 +804,7 @@ __global__ void __launch_bounds__(kBlock, Op::kMinBlocks)
             a.partials[gridDim.x + blockIdx.x] = brr;
             a.partials[2 * gridDim.x + blockIdx.x] = brz;
         }
-        if (!grid_barrier(a.bar, a.bar + 1, a.err)) return;
+        if (!grid_barrier(a.bar, a.err, target)) return;
         double t2[2];
         sum_partials<2>(a.partials + gridDim.x, t2);
         const double nr = sqrt(t2[0]);
@@ -857,9 +863,10 @@ static int stage_flags(uint32_t slm, uint32_t cls, uint32_t nnz) {
            (Op::kTc ? 4 : 0);
 }
 template <class Op, typename T>
-static size_t lhs_smem(uint32_t slm, uint32_t cls, uint32_t nnz) {
+static size_t lhs_smem(uint32_t slm, uint32_t cls, uint32_t nnz, int threads) {
     const int fl = stage_flags<Op, T>(slm, cls, nnz);
-    return ((fl & 1) ? ang_smem_bytes<T>(nnz) : 0) + ((fl & 2) ? O_smem_bytes<T>(slm, cls) : 0) + Op::slab_bytes();
+    return ((fl & 1) ? ang_smem_bytes<T>(nnz) : 0) + ((fl & 2) ? O_smem_bytes<T>(slm, cls) : 0) +
+           Op::slab_bytes(threads);
 }
 
 // preferred shared-memory carveout (percent of the unified L1/shared array)
@@ -908,13 +915,22 @@ static cudaError_t with_op(const DeviceOp<T> &op, uint32_t slm, F &&fn) {
 template <class Op, typename T, bool DOT, bool FUSEP, class Fin>
 static cudaError_t launch_one(const tr_ctx *c, const OpData<T> &d, const LhsArgs<T> &a, Fin fin, cudaStream_t s) {
     if (Op::kLS && d.cls != Op::kLS) return cudaErrorInvalidValue;  // tables built for another lane stride
-    const size_t smem = lhs_smem<Op, T>(d.slm, d.cls, a.ang_nnz);
+    const size_t smem = lhs_smem<Op, T>(d.slm, d.cls, a.ang_nnz, kBlock);
     auto kern = k_lhs<Op, T, DOT, FUSEP, Fin>;
     static size_t opted = 0;  // dynamic shared memory granted so far (per instantiation)
     cudaError_t e = opt_in_smem(kern, smem, opted);
     if (e != cudaSuccess) return e;
+    // one wave of resident blocks (a partial second wave would idle most SMs)
+    static int per_sm = 0;
+    static size_t per_sm_smem = 0;
+    if (per_sm == 0 || per_sm_smem != smem) {
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, smem);
+        if (e != cudaSuccess) return e;
+        per_sm = std::max(per_sm, 1);
+        per_sm_smem = smem;
+    }
     const int gpb = kBlock / Op::kLanes;
-    const int grid = std::max(1, std::min(c->num_sms * 4, static_cast<int>((d.nP + gpb - 1) / gpb)));
+    const int grid = std::max(1, std::min(c->num_sms * per_sm, static_cast<int>((d.nP + gpb - 1) / gpb)));
     kern<<<grid, kBlock, smem, s>>>(d, a.x, a.pold, a.pnew, a.y, c->partials, c->counters, fin, a.done, a.cgs,
                                     stage_flags<Op, T>(d.slm, d.cls, a.ang_nnz));
     return cudaGetLastError();
@@ -968,16 +984,17 @@ static cudaError_t launch_pcg(const tr_ctx *c, const OpData<T> &d, const PcgArgs
                               int *grid_out) {
     if (Op::kLS && d.cls != Op::kLS) return cudaErrorInvalidValue;
     auto kern = k_cg_persistent<Op, T, JAC>;
-    const size_t smem = lhs_smem<Op, T>(d.slm, d.cls, nnz);
+    constexpr int threads = Op::kPersistThreads;
+    const size_t smem = lhs_smem<Op, T>(d.slm, d.cls, nnz, threads);
     static size_t opted = 0;
     cudaError_t e = opt_in_smem(kern, smem, opted);
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kBlock, smem);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorCooperativeLaunchTooLarge;
     // enough blocks for the vertices, at most one wave of resident blocks
-    const int gpb = kBlock / Op::kLanes;
+    const int gpb = threads / Op::kLanes;
     const int need = static_cast<int>((d.nP + gpb - 1) / gpb);
     const int grid = std::max(1, std::min(per_sm * c->num_sms, std::min(need, kMaxGrid)));
     *grid_out = grid;
@@ -985,7 +1002,7 @@ static cudaError_t launch_pcg(const tr_ctx *c, const OpData<T> &d, const PcgArgs
     OpData<T> dd = d;
     PcgArgs<T> aa = a;
     void *args[] = {&dd, &aa, &flags};
-    return cudaLaunchCooperativeKernel(reinterpret_cast<void *>(kern), grid, kBlock, args, smem, s);
+    return cudaLaunchCooperativeKernel(reinterpret_cast<void *>(kern), grid, threads, args, smem, s);
 }
 
 template <typename T>

@@ -207,6 +207,7 @@ static tr_status run_cg(tr_ctx *c, int slot, const DeviceOp<T> &op, uint32_t asl
         int k = 0, done = 0;
         for (int guard = 0; guard < (1 << 24); ++guard) {
             int grid = 0;
+            TRY(cudaMemsetAsync(c->bar, 0, sizeof(unsigned int), st));  // grid_barrier's arrival count
             TRY(cudaEventRecord(c->ev[2], st));
             cudaError_t e = launch_cg_persistent<T>(c, op, a, st, &grid);
             if (e == cudaErrorCooperativeLaunchTooLarge || e == cudaErrorNotSupported) {
