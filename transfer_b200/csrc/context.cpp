@@ -294,15 +294,17 @@ tr_status ctx_create(int device, const tr_mesh_view *m, const tr_angular_view *a
     const size_t ncon = std::max<size_t>(static_cast<size_t>(ckmax) * cls, 1);
     std::vector<double> cw64(ncon, 0.0);
     std::vector<float> cw32(ncon, 0.0f);
-    std::vector<uint16_t> co64(ncon, 0), co32(ncon, 0), cotc(ncon, 0);
+    std::vector<CEnt<double>> ce64(ncon, CEnt<double>{0.0, 0});
+    std::vector<CEnt<float>> ce32(ncon, CEnt<float>{0.0f, 0});
+    std::vector<uint16_t> cotc(ncon, 0);
     for (tr_idx lm = 0; lm < slm; ++lm)
         for (size_t k = 0; k < lists[lm].size(); ++k) {
             const uint32_t r = lists[lm][k].first >> 8, lms = lists[lm][k].first & 255u;
             const size_t o = k * cls + lm;
             cw64[o] = lists[lm][k].second;
             cw32[o] = static_cast<float>(lists[lm][k].second);
-            co64[o] = static_cast<uint16_t>(r * sa64 + lms);
-            co32[o] = static_cast<uint16_t>(r * sa32 + lms);
+            ce64[o] = CEnt<double>{lists[lm][k].second, r * sa64 + lms};
+            ce32[o] = CEnt<float>{static_cast<float>(lists[lm][k].second), r * sa32 + lms};
             cotc[o] = static_cast<uint16_t>(r * satc + lms);
         }
     std::vector<double> O(3 * ss), ang_diag(3 * slm), O_diag(3 * slm);
@@ -375,8 +377,8 @@ tr_status ctx_create(int device, const tr_mesh_view *m, const tr_angular_view *a
     o64.cls = o32.cls = cls;
     ok(upload(c, &o64.cw, cw64.data(), cw64.size() * 8));
     ok(upload(c, &o32.cw, cw32.data(), cw32.size() * 4));
-    ok(upload(c, &o64.co, co64.data(), co64.size() * 2));
-    ok(upload(c, &o32.co, co32.data(), co32.size() * 2));
+    ok(upload(c, &o64.ce, ce64.data(), ce64.size() * sizeof(CEnt<double>)));
+    ok(upload(c, &o32.ce, ce32.data(), ce32.size() * sizeof(CEnt<float>)));
     ok(upload(c, &o64.co_tc, cotc.data(), cotc.size() * 2));
     o32.co_tc = o64.co_tc;
     ok(upload(c, &o64.coef, coef.data(), coef.size() * 8));

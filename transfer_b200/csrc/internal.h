@@ -36,11 +36,19 @@ constexpr int kCoefStride = 16;
 constexpr int kSymRows = 6, kRowM = 6, kRowM0 = 7, kRowE = 8;
 constexpr int kBlock = 256;
 
-// The angular coupling out[lm] = sum_k cw[k][lm] * S[co[k][lm]] is stored
-// lane-major: entry k of every harmonic lm is contiguous (cw[k * cls + lm]),
+// The angular coupling out[lm] = sum_k w[k][lm] * S[o[k][lm]] is stored
+// lane-major: entry k of every harmonic lm is contiguous ([k * cls + lm]),
 // lists padded to the longest one (ckmax) with zero weights, so each step
-// of the contraction is one coalesced, conflict-free load per table.  co is
-// the offset q * SA + lms of S_sym[q][lms] in the kernel's S table.
+// of the contraction is one coalesced, conflict-free load.  o is the offset
+// q * SA + lms of S_sym[q][lms] in the kernel's S table.  The SIMT kernels
+// read (w, o) pairs (CEnt, one vector load per step); the tensor-core
+// kernels read the weights cw and their C-table offsets co_tc.
+template <typename T>
+struct alignas(2 * sizeof(T)) CEnt {
+    T w;
+    uint32_t o;
+};
+static_assert(sizeof(CEnt<float>) == 8 && sizeof(CEnt<double>) == 16, "contraction entry layout");
 // lanes per vertex (G) and harmonics per lane (H) for a vector stride
 inline constexpr int group_width(uint32_t aslm) { return aslm <= 8 ? 8 : aslm <= 16 ? 16 : 32; }
 inline constexpr int harm_per_lane(uint32_t aslm) {
@@ -57,8 +65,8 @@ struct OpData {
     const uint32_t *col;             // [nnz]
     const T *coef;                   // [nnz][16]
     uint32_t ckmax, cls;             // contraction: entries per lm, lane stride
+    const CEnt<T> *ce;               // [ckmax][cls] (weight, SIMT S-table offset)
     const T *cw;                     // [ckmax][cls] weights
-    const uint16_t *co;              // [ckmax][cls] offsets, SIMT S table
     const uint16_t *co_tc;           // [ckmax][cls] offsets, tensor-core C table
     const T *O;                      // [3][slm][cls]: O_n[lms][lm], rows padded to cls
     const T *ang_diag;               // [3][slm]: omega_i[lm][lm]
@@ -131,8 +139,9 @@ template <typename T>
 struct DeviceOp {
     uint32_t *row = nullptr, *col = nullptr;
     uint32_t ckmax = 0, cls = 0;
+    CEnt<T> *ce = nullptr;
     T *cw = nullptr;
-    uint16_t *co = nullptr, *co_tc = nullptr;
+    uint16_t *co_tc = nullptr;
     T *coef = nullptr, *O = nullptr, *ang_diag = nullptr, *O_diag = nullptr;
     T *mask = nullptr;
     T *dinv = nullptr;               // Jacobi: 1 / diag(A), [nP][aslm]
@@ -150,8 +159,8 @@ struct DeviceOp {
         d.coef = coef;
         d.ckmax = ckmax;
         d.cls = cls;
+        d.ce = ce;
         d.cw = cw;
-        d.co = co;
         d.co_tc = co_tc;
         d.O = O;
         d.ang_diag = ang_diag;

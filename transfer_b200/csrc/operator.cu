@@ -81,14 +81,19 @@ struct FinAlpha {  // CG step length alpha = (r,z) / (p, A p)
     __device__ void operator()(double pAp) const { s->alpha = s->nrz / pAp; }
 };
 
-__host__ __device__ constexpr int batch_of(int H) { return H <= 2 ? 4 : 2; }
+// neighbour rows gathered at once per lane (loads in flight)
+#ifndef TR_GATHER_BATCH1
+#define TR_GATHER_BATCH1 4
+#endif
+__host__ __device__ constexpr int batch_of(int H) { return H == 1 ? TR_GATHER_BATCH1 : H == 2 ? 4 : 2; }
 
 __host__ __device__ inline size_t align16(size_t b) { return (b + 15) & ~size_t(15); }
 
-// bytes of the staged contraction tables (weights + offsets)
+// bytes of the staged contraction tables: (weight, offset) pairs for the
+// SIMT kernels, weights + C-table offsets for the tensor-core ones
 template <typename T>
-__host__ __device__ inline size_t ang_smem_bytes(uint32_t ncon) {
-    return align16(ncon * sizeof(T)) + align16(ncon * sizeof(uint16_t));
+__host__ __device__ inline size_t ang_smem_bytes(uint32_t ncon, bool tc) {
+    return tc ? align16(ncon * sizeof(T)) + align16(ncon * sizeof(uint16_t)) : align16(ncon * sizeof(CEnt<T>));
 }
 // per-group shared slab: staged edge coefficients + the S / B table,
 // rounded to 16 bytes so every slab (and its vector stores) stays aligned
@@ -129,8 +134,9 @@ __device__ __forceinline__ void gather_row(const T *__restrict__ f, const T *__r
 // when small, the three half-range tables O_n.
 template <typename T>
 struct Staged {
-    const T *cw;          // contraction weights  [ckmax][cls]
-    const uint16_t *co;   // contraction offsets  [ckmax][cls]
+    const CEnt<T> *ce;    // SIMT contraction entries [ckmax][cls]
+    const T *cw;          // tensor-core contraction weights [ckmax][cls]
+    const uint16_t *co;   // tensor-core C-table offsets [ckmax][cls]
     const T *O;
     size_t bytes;
 };
@@ -143,19 +149,31 @@ __host__ __device__ inline size_t O_smem_bytes(uint32_t slm, uint32_t cls) {
 // (C table) offsets
 template <typename T>
 __device__ __forceinline__ Staged<T> stage_tables(const OpData<T> &d, unsigned char *smem, int flags) {
-    const uint16_t *co = (flags & 4) ? d.co_tc : d.co;
-    Staged<T> st{d.cw, co, d.O, 0};
+    const bool tc = (flags & 4) != 0;
+    Staged<T> st{d.ce, d.cw, d.co_tc, d.O, 0};
     const uint32_t ncon = d.ckmax * d.cls;
-    if (flags & 1) {
+    if ((flags & 1) && tc) {
         T *sw = reinterpret_cast<T *>(smem);
         uint16_t *so = reinterpret_cast<uint16_t *>(smem + align16(ncon * sizeof(T)));
         for (uint32_t i = threadIdx.x; i < ncon; i += blockDim.x) {
             sw[i] = __ldg(d.cw + i);
-            so[i] = __ldg(co + i);
+            so[i] = __ldg(d.co_tc + i);
         }
         st.cw = sw;
         st.co = so;
-        st.bytes = ang_smem_bytes<T>(ncon);
+        st.bytes = ang_smem_bytes<T>(ncon, true);
+    } else if (flags & 1) {
+        typedef typename Vec16<T>::type V;  // one entry is 8 (FP32) or 16 (FP64) bytes
+        CEnt<T> *se = reinterpret_cast<CEnt<T> *>(smem);
+        if (sizeof(CEnt<T>) == 16) {
+            for (uint32_t i = threadIdx.x; i < ncon; i += blockDim.x)
+                reinterpret_cast<V *>(se)[i] = __ldg(reinterpret_cast<const V *>(d.ce) + i);
+        } else {
+            for (uint32_t i = threadIdx.x; i < ncon; i += blockDim.x)
+                reinterpret_cast<uint2 *>(se)[i] = __ldg(reinterpret_cast<const uint2 *>(d.ce) + i);
+        }
+        st.ce = se;
+        st.bytes = ang_smem_bytes<T>(ncon, false);
     }
     if (flags & 2) {
         T *so = reinterpret_cast<T *>(smem + st.bytes);
@@ -186,19 +204,22 @@ __device__ __forceinline__ T contract(const Staged<T> &tab, const T *S, uint32_t
     return (acc0 + acc2) + (acc1 + acc3);
 }
 
-// the same with the lane stride LS of the tables known at compile time
+// the SIMT form: (weight, offset) entries at a compile-time lane stride LS
 template <typename T, int LS>
-__device__ __forceinline__ T contract_ls(const T *__restrict__ w, const uint16_t *__restrict__ o, const T *S,
-                                         uint32_t kmax, T acc0) {
+__device__ __forceinline__ T contract_ls(const CEnt<T> *__restrict__ e, const T *S, uint32_t kmax, T acc0) {
     T acc1 = T(0), acc2 = T(0), acc3 = T(0);
     uint32_t k = 0;
-    for (; k + 3 < kmax; k += 4, w += 4 * LS, o += 4 * LS) {
-        acc0 = fma(w[0], S[o[0]], acc0);
-        acc1 = fma(w[LS], S[o[LS]], acc1);
-        acc2 = fma(w[2 * LS], S[o[2 * LS]], acc2);
-        acc3 = fma(w[3 * LS], S[o[3 * LS]], acc3);
+    for (; k + 3 < kmax; k += 4, e += 4 * LS) {
+        const CEnt<T> e0 = e[0], e1 = e[LS], e2 = e[2 * LS], e3 = e[3 * LS];
+        acc0 = fma(e0.w, S[e0.o], acc0);
+        acc1 = fma(e1.w, S[e1.o], acc1);
+        acc2 = fma(e2.w, S[e2.o], acc2);
+        acc3 = fma(e3.w, S[e3.o], acc3);
     }
-    for (; k < kmax; ++k, w += LS, o += LS) acc0 = fma(w[0], S[o[0]], acc0);
+    for (; k < kmax; ++k, e += LS) {
+        const CEnt<T> e0 = e[0];
+        acc0 = fma(e0.w, S[e0.o], acc0);
+    }
     return (acc0 + acc2) + (acc1 + acc3);
 }
 
@@ -223,6 +244,73 @@ __device__ __forceinline__ void load_coef<double>(const double *c, double (&k)[1
     }
 }
 
+// Edge-loop accumulators of one harmonic lm: the six symmetric stiffness
+// sums S_q, the mass term and the three boundary sums B_n.
+//   FP64: the mass row is chosen per lane (M0 for lm = 0, M otherwise).
+//   FP32: the sums are float2 pairs updated by paired FMAs (__ffma2_rn,
+//   FFMA2 on sm_100: one instruction, two independent round-to-nearest
+//   FMAs), and the mass pair (M, M0) is accumulated for every lane, the
+//   lane choosing its half at the end.  Same products, same order, same
+//   rounding as scalar FMAs.
+template <typename T>
+struct EdgeAcc;
+template <>
+struct EdgeAcc<double> {
+    typedef double Coef[12];
+    double S_[kSymRows], m_, B_[3];
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int q = 0; q < kSymRows; ++q) S_[q] = 0.0;
+        m_ = B_[0] = B_[1] = B_[2] = 0.0;
+    }
+    __device__ static __forceinline__ void load(const double *cp, Coef &c) { load_coef<double>(cp, c); }
+    __device__ __forceinline__ void add(const Coef &c, double x, bool l0) {
+        m_ = fma(l0 ? c[kRowM0] : c[kRowM], x, m_);
+#pragma unroll
+        for (int q = 0; q < kSymRows; ++q) S_[q] = fma(c[q], x, S_[q]);
+    }
+    __device__ __forceinline__ void add_bnd(const Coef &c, double x) {
+#pragma unroll
+        for (int n = 0; n < 3; ++n) B_[n] = fma(c[kRowE + n], x, B_[n]);
+    }
+    __device__ __forceinline__ double S(int q) const { return S_[q]; }
+    __device__ __forceinline__ double mass(bool) const { return m_; }
+    __device__ __forceinline__ double B(int n) const { return B_[n]; }
+};
+template <>
+struct EdgeAcc<float> {
+    typedef float4 Coef[3];  // records 0-11: K (6), M, M0, E (3), pad
+    float2 s01_, s23_, s45_, mm_, e01_;
+    float e2_;
+    __device__ __forceinline__ void zero() {
+        s01_ = s23_ = s45_ = mm_ = e01_ = make_float2(0.0f, 0.0f);
+        e2_ = 0.0f;
+    }
+    __device__ static __forceinline__ void load(const float *cp, Coef &c) {
+        const float4 *v = reinterpret_cast<const float4 *>(cp);
+        c[0] = v[0];
+        c[1] = v[1];
+        c[2] = v[2];
+    }
+    __device__ __forceinline__ void add(const Coef &c, float x, bool) {
+        const float2 xx = make_float2(x, x);
+        s01_ = __ffma2_rn(make_float2(c[0].x, c[0].y), xx, s01_);
+        s23_ = __ffma2_rn(make_float2(c[0].z, c[0].w), xx, s23_);
+        s45_ = __ffma2_rn(make_float2(c[1].x, c[1].y), xx, s45_);
+        mm_ = __ffma2_rn(make_float2(c[1].z, c[1].w), xx, mm_);
+    }
+    __device__ __forceinline__ void add_bnd(const Coef &c, float x) {
+        e01_ = __ffma2_rn(make_float2(c[2].x, c[2].y), make_float2(x, x), e01_);
+        e2_ = fmaf(c[2].z, x, e2_);
+    }
+    __device__ __forceinline__ float S(int q) const {
+        return q == 0 ? s01_.x : q == 1 ? s01_.y : q == 2 ? s23_.x : q == 3 ? s23_.y : q == 4 ? s45_.x : s45_.y;
+    }
+    __device__ __forceinline__ float mass(bool l0) const { return l0 ? mm_.y : mm_.x; }
+    __device__ __forceinline__ float B(int n) const { return n == 0 ? e01_.x : n == 1 ? e01_.y : e2_; }
+};
+static_assert(kRowM == 6 && kRowM0 == 7 && kRowE == 8 && kSymRows == 6, "EdgeAcc<float> pairs the record rows");
+
 template <int G, int H, typename T, bool DOT, bool FUSEP, bool COH = false>
 __device__ __forceinline__ double lhs_vertices(const OpData<T> &d, const Staged<T> &tab, unsigned char *smem_groups,
                                                const T *__restrict__ f, const T *__restrict__ pold,
@@ -241,13 +329,9 @@ __device__ __forceinline__ double lhs_vertices(const OpData<T> &d, const Staged<
 
     for (uint32_t v = blockIdx.x * gpb + threadIdx.x / G; v < d.nP; v += ng) {
         const uint32_t axes = __ldg(d.bmask + v);
-        T mass[H], S[kSymRows][H], B[3][H];
+        EdgeAcc<T> acc[H];
 #pragma unroll
-        for (int h = 0; h < H; ++h) {
-            mass[h] = B[0][h] = B[1][h] = B[2][h] = T(0);
-#pragma unroll
-            for (int q = 0; q < kSymRows; ++q) S[q][h] = T(0);
-        }
+        for (int h = 0; h < H; ++h) acc[h].zero();
         const uint32_t e0 = __ldg(d.row + v), e1 = __ldg(d.row + v + 1);
         for (uint32_t base = e0; base < e1; base += G) {
             const int cnt = min(static_cast<int>(e1 - base), G);
@@ -262,22 +346,13 @@ __device__ __forceinline__ double lhs_vertices(const OpData<T> &d, const Staged<
             }
             tile.sync();
             auto accumulate = [&](const T *cp, const T(&x)[H]) {
-                T c[12];
-                load_coef<T>(cp, c);
+                typename EdgeAcc<T>::Coef c;
+                EdgeAcc<T>::load(cp, c);
 #pragma unroll
-                for (int h = 0; h < H; ++h) {
-                    const uint32_t lm = lane + G * h;
-                    mass[h] = fma(lm == 0 ? c[kRowM0] : c[kRowM], x[h], mass[h]);
-#pragma unroll
-                    for (int q = 0; q < kSymRows; ++q) S[q][h] = fma(c[q], x[h], S[q][h]);
-                }
+                for (int h = 0; h < H; ++h) acc[h].add(c, x[h], lane + G * h == 0);
                 if (axes) {
 #pragma unroll
-                    for (int h = 0; h < H; ++h) {
-                        B[0][h] = fma(c[kRowE], x[h], B[0][h]);
-                        B[1][h] = fma(c[kRowE + 1], x[h], B[1][h]);
-                        B[2][h] = fma(c[kRowE + 2], x[h], B[2][h]);
-                    }
+                    for (int h = 0; h < H; ++h) acc[h].add_bnd(c, x[h]);
                 }
             };
             int jj = 0;
@@ -300,13 +375,13 @@ __device__ __forceinline__ double lhs_vertices(const OpData<T> &d, const Staged<
 #pragma unroll
         for (int h = 0; h < H; ++h)
 #pragma unroll
-            for (int q = 0; q < kSymRows; ++q) sm[q * SA + lane + G * h] = S[q][h];
+            for (int q = 0; q < kSymRows; ++q) sm[q * SA + lane + G * h] = acc[h].S(q);
         tile.sync();
         T out[H];
 #pragma unroll
         for (int h = 0; h < H; ++h) {
             const uint32_t lm = lane + G * h;
-            out[h] = contract_ls<T, LS>(tab.cw + lm, tab.co + lm, sm, d.ckmax, mass[h]);
+            out[h] = contract_ls<T, LS>(tab.ce + lm, sm, d.ckmax, acc[h].mass(lm == 0));
         }
         // half-range boundary term from the per-axis sums B_n
         if (axes) {
@@ -314,7 +389,7 @@ __device__ __forceinline__ double lhs_vertices(const OpData<T> &d, const Staged<
 #pragma unroll
             for (int h = 0; h < H; ++h)
 #pragma unroll
-                for (int n = 0; n < 3; ++n) sm[n * SA + lane + G * h] = B[n][h];
+                for (int n = 0; n < 3; ++n) sm[n * SA + lane + G * h] = acc[h].B(n);
             tile.sync();
 #pragma unroll
             for (int h = 0; h < H; ++h) {
@@ -859,13 +934,13 @@ constexpr size_t kOSmemBudget = 40 * 1024;
 
 template <class Op, typename T>
 static int stage_flags(uint32_t slm, uint32_t cls, uint32_t nnz) {
-    return (ang_smem_bytes<T>(nnz) <= kAngSmemBudget ? 1 : 0) | (O_smem_bytes<T>(slm, cls) <= kOSmemBudget ? 2 : 0) |
-           (Op::kTc ? 4 : 0);
+    return (ang_smem_bytes<T>(nnz, Op::kTc) <= kAngSmemBudget ? 1 : 0) |
+           (O_smem_bytes<T>(slm, cls) <= kOSmemBudget ? 2 : 0) | (Op::kTc ? 4 : 0);
 }
 template <class Op, typename T>
 static size_t lhs_smem(uint32_t slm, uint32_t cls, uint32_t nnz, int threads) {
     const int fl = stage_flags<Op, T>(slm, cls, nnz);
-    return ((fl & 1) ? ang_smem_bytes<T>(nnz) : 0) + ((fl & 2) ? O_smem_bytes<T>(slm, cls) : 0) +
+    return ((fl & 1) ? ang_smem_bytes<T>(nnz, Op::kTc) : 0) + ((fl & 2) ? O_smem_bytes<T>(slm, cls) : 0) +
            Op::slab_bytes(threads);
 }
 
