@@ -99,9 +99,11 @@ __host__ __device__ inline size_t ang_smem_bytes(uint32_t ncon, bool tc) {
 // rounded to 16 bytes so every slab (and its vector stores) stays aligned
 template <int G, int H, typename T>
 __host__ __device__ constexpr size_t group_smem_elems() {
-    return (G * kCoefStride + kSymRows * (G * H + 1) + (16 / sizeof(T)) - 1) / (16 / sizeof(T)) * (16 / sizeof(T));
+    // two edge-record buffers [2][G][kCoefStride], two neighbour-index
+    // buffers [2][G] (uint32), the S / B table [kSymRows][G*H+1]
+    return (2 * G * kCoefStride + (2 * G * 4 + sizeof(T) - 1) / sizeof(T) + kSymRows * (G * H + 1) +
+            (16 / sizeof(T)) - 1) / (16 / sizeof(T)) * (16 / sizeof(T));
 }
-
 // Loads of vectors that other blocks of the same launch may have written
 // (persistent kernel) avoid the non-coherent read-only path (ld.global.nc
 // requires data that no thread writes during the kernel) and use ordinary
@@ -311,6 +313,38 @@ struct EdgeAcc<float> {
 };
 static_assert(kRowM == 6 && kRowM0 == 7 && kRowE == 8 && kSymRows == 6, "EdgeAcc<float> pairs the record rows");
 
+// Asynchronous global -> shared copies (cp.async, no registers held while
+// in flight): a group queues the next vertex's neighbour indices and edge
+// records while it still works on the current vertex.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(smem))),
+                 "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async4(void *smem, const void *gmem) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(smem))),
+                 "l"(gmem)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// queue the edges [base, base + cnt) of a vertex into one staging buffer:
+// lane l < cnt copies edge base + l (its neighbour index and 16-value record)
+template <typename T>
+__device__ __forceinline__ void stage_edges_async(const OpData<T> &d, uint32_t base, int cnt, int lane, T *scoef,
+                                                  uint32_t *scol) {
+    if (lane < cnt) {
+        cp_async4(scol + lane, d.col + base + lane);
+        const T *src = d.coef + static_cast<size_t>(base + lane) * kCoefStride;
+        T *dst = scoef + lane * kCoefStride;
+#pragma unroll
+        for (int q = 0; q < kCoefStride * static_cast<int>(sizeof(T)) / 16; ++q)
+            cp_async16(dst + q * (16 / sizeof(T)), src + q * (16 / sizeof(T)));
+    }
+    cp_async_commit();
+}
+
 template <int G, int H, typename T, bool DOT, bool FUSEP, bool COH = false>
 __device__ __forceinline__ double lhs_vertices(const OpData<T> &d, const Staged<T> &tab, unsigned char *smem_groups,
                                                const T *__restrict__ f, const T *__restrict__ pold,
@@ -319,32 +353,58 @@ __device__ __forceinline__ double lhs_vertices(const OpData<T> &d, const Staged<
     constexpr int NB = batch_of(H);
     constexpr int LS = G * H < 32 ? 32 : G * H;  // lane stride of the tables (== d.cls, checked at launch)
     const uint32_t slm = d.slm, aslm = d.aslm;
-    T *scoef = reinterpret_cast<T *>(smem_groups) + (threadIdx.x / G) * group_smem_elems<G, H, T>();
-    T *sm = scoef + G * kCoefStride;
+    T *slab = reinterpret_cast<T *>(smem_groups) + (threadIdx.x / G) * group_smem_elems<G, H, T>();
+    uint32_t *scolbuf = reinterpret_cast<uint32_t *>(slab + 2 * G * kCoefStride);  // [2][G]
+    T *sm = slab + 2 * G * kCoefStride + (2 * G * 4 + sizeof(T) - 1) / sizeof(T);
     cg::thread_block_tile<G> tile = cg::tiled_partition<G>(cg::this_thread_block());
     const int lane = threadIdx.x % G;
     const uint32_t gpb = blockDim.x / G;
-    const uint32_t ng = gridDim.x * gpb;
     double dacc = 0.0;
 
-    for (uint32_t v = blockIdx.x * gpb + threadIdx.x / G; v < d.nP; v += ng) {
+    // Each block owns a contiguous range of vertices (neighbouring rows are
+    // shared in L1); its groups take the range's vertices one at a time from
+    // a shared counter, so a group that drew cheap vertices draws more.
+    __shared__ unsigned int s_next;
+    const uint32_t per_block = (d.nP + gridDim.x - 1) / gridDim.x;
+    const uint32_t vb0 = min(d.nP, blockIdx.x * per_block), vb1 = min(d.nP, vb0 + per_block);
+    if (threadIdx.x == 0) s_next = gpb;
+    __syncthreads();
+
+    // software pipeline over this group's vertices: the first chunk of edges
+    // of its next vertex is queued (cp.async) before the current vertex's
+    // angular coupling runs
+    uint32_t v = vb0 + threadIdx.x / G;
+    uint32_t e0 = 0, e1 = 0;
+    int cur = 0;
+    if (v < vb1) {
+        e0 = __ldg(d.row + v);
+        e1 = __ldg(d.row + v + 1);
+        stage_edges_async<T>(d, e0, min(static_cast<int>(e1 - e0), G), lane, slab, scolbuf);
+    }
+    while (v < vb1) {
+        uint32_t vn = 0;
+        if (lane == 0) vn = vb0 + atomicAdd(&s_next, 1u);
+        vn = tile.shfl(vn, 0);
+        uint32_t e0n = 0, e1n = 0;
+        if (vn < vb1) {  // consumed after this vertex's edge loop
+            e0n = __ldg(d.row + vn);
+            e1n = __ldg(d.row + vn + 1);
+        }
         const uint32_t axes = __ldg(d.bmask + v);
         EdgeAcc<T> acc[H];
 #pragma unroll
         for (int h = 0; h < H; ++h) acc[h].zero();
-        const uint32_t e0 = __ldg(d.row + v), e1 = __ldg(d.row + v + 1);
+        T *scoef = slab + cur * G * kCoefStride;
+        uint32_t *scol = scolbuf + cur * G;
         for (uint32_t base = e0; base < e1; base += G) {
             const int cnt = min(static_cast<int>(e1 - base), G);
-            uint32_t ul = 0;
-            if (lane < cnt) {
-                ul = __ldg(d.col + base + lane);
-                typedef typename Vec16<T>::type V;
-                const V *src = reinterpret_cast<const V *>(d.coef + static_cast<size_t>(base + lane) * kCoefStride);
-                V *dst = reinterpret_cast<V *>(scoef + lane * kCoefStride);
-#pragma unroll
-                for (int q = 0; q < kCoefStride / Vec16<T>::n; ++q) dst[q] = __ldg(src + q);
+            if (base != e0) {  // further chunks of a vertex with more than G edges
+                tile.sync();
+                stage_edges_async<T>(d, base, cnt, lane, scoef, scol);
             }
+            cp_async_wait_all();
             tile.sync();
+            const uint32_t ul = scol[lane];
             auto accumulate = [&](const T *cp, const T(&x)[H]) {
                 typename EdgeAcc<T>::Coef c;
                 EdgeAcc<T>::load(cp, c);
@@ -369,8 +429,16 @@ __device__ __forceinline__ double lhs_vertices(const OpData<T> &d, const Staged<
                 gather_row<G, H, T, FUSEP, COH>(f, pold, beta, tile.shfl(ul, jj), aslm, slm, lane, x);
                 accumulate(scoef + jj * kCoefStride, x);
             }
-            tile.sync();
         }
+        // queue the next vertex's first chunk into the other buffer; it lands
+        // while this vertex's angular coupling runs
+        cur ^= 1;
+        if (vn < vb1)
+            stage_edges_async<T>(d, e0n, min(static_cast<int>(e1n - e0n), G), lane, slab + cur * G * kCoefStride,
+                                 scolbuf + cur * G);
+        e0 = e0n;
+        e1 = e1n;
+        tile.sync();
         // angular coupling through shared memory
 #pragma unroll
         for (int h = 0; h < H; ++h)
@@ -426,6 +494,7 @@ __device__ __forceinline__ double lhs_vertices(const OpData<T> &d, const Staged<
             }
             if (DOT && lm < slm) dacc += static_cast<double>(xv[h]) * static_cast<double>(out[h]);
         }
+        v = vn;
     }
     return dacc;
 }
