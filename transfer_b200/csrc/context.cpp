@@ -369,8 +369,11 @@ tr_status ctx_create(int device, const tr_mesh_view *m, const tr_angular_view *a
     DeviceOp<float> &o32 = c->op32;
     o64.aslm = c->aslm;
     o32.aslm = c->aslm32;
-    o64.kind = TR_OPERATOR_TENSOR;  // DMMA edge sums: fastest FP64 form measured
-    o32.kind = TR_OPERATOR_SIMT;    // FMA edge sums: split-TF32 needs 3 products
+    // the fastest solves measured on B200: FP64 DMMA edge sums, FP32 FMA edge
+    // sums (split-TF32 tensor-core sums drop the lo*lo product, which costs
+    // the mixed solve more inner iterations than the faster operator saves)
+    o64.kind = TR_OPERATOR_TENSOR;
+    o32.kind = TR_OPERATOR_SIMT;
     ok(upload(c, &o64.row, row.data(), row.size() * 4));
     ok(upload(c, &o64.col, col.data(), col.size() * 4));
     o64.ckmax = o32.ckmax = ckmax;

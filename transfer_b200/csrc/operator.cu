@@ -557,6 +557,11 @@ __device__ __forceinline__ double lhs_vertices_tc(const OpData<T> &d, const Stag
                                                   const T *__restrict__ f, const T *__restrict__ pold,
                                                   T *__restrict__ pnew, T *__restrict__ r, const T beta) {
     constexpr int SA = TcShape<NT>::SA;
+    // wide rows are done in column passes of at most 4 n-tiles, so the
+    // accumulators and gathered fragments of one pass stay in registers at
+    // several resident blocks per SM
+    constexpr int kPasses = (NT + 3) / 4;
+    constexpr int NTH = (NT + kPasses - 1) / kPasses;
     const uint32_t slm = d.slm, aslm = d.aslm;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int g = lane >> 2, t = lane & 3;
@@ -569,16 +574,19 @@ __device__ __forceinline__ double lhs_vertices_tc(const OpData<T> &d, const Stag
         const uint32_t axes = __ldg(d.bmask + v);
         const uint32_t e0 = __ldg(d.row + v), e1 = __ldg(d.row + v + 1);
         if constexpr (sizeof(T) == 4) {
-            float acc[NT][4];
+          for (int pass = 0; pass < kPasses; ++pass) {
+            const int n0 = pass * NTH;  // first n-tile of this column pass
+            float acc[NTH][4];
 #pragma unroll
-            for (int n = 0; n < NT; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.0f;
+            for (int n = 0; n < NTH; ++n) acc[n][0] = acc[n][1] = acc[n][2] = acc[n][3] = 0.0f;
             // one k-step of 8 edges: A = coefficient rows, B = gathered rows
-            auto kstep = [&](const float (&a)[4], const float (&xa)[NT], const float (&xb)[NT]) {
+            auto kstep = [&](const float (&a)[4], const float (&xa)[NTH], const float (&xb)[NTH]) {
                 uint32_t ahi[4], alo[4];
 #pragma unroll
                 for (int i = 0; i < 4; ++i) split_tf32(a[i], ahi[i], alo[i]);
 #pragma unroll
-                for (int n = 0; n < NT; ++n) {
+                for (int n = 0; n < NTH; ++n) {
+                    if (n0 + n >= NT) break;
                     uint32_t b0h, b0l, b1h, b1l;
                     split_tf32(xa[n], b0h, b0l);
                     split_tf32(xb[n], b1h, b1l);
@@ -608,10 +616,10 @@ __device__ __forceinline__ double lhs_vertices_tc(const OpData<T> &d, const Stag
                 bool va0, vb0, va1, vb1;
                 load_step(e0, a0, ua0, ub0, va0, vb0);
                 load_step(e0 + 8, a1, ua1, ub1, va1, vb1);
-                float xa0[NT], xb0[NT], xa1[NT], xb1[NT];
+                float xa0[NTH], xb0[NTH], xa1[NTH], xb1[NTH];
 #pragma unroll
-                for (int n = 0; n < NT; ++n) {
-                    const uint32_t lm = n * 8 + g;
+                for (int n = 0; n < NTH; ++n) {
+                    const uint32_t lm = (n0 + n) * 8 + g;
                     const bool in = lm < slm;
                     xa0[n] = gather_one<float, FUSEP, COH>(f, pold, beta, ua0, aslm, lm, va0 && in);
                     xb0[n] = gather_one<float, FUSEP, COH>(f, pold, beta, ub0, aslm, lm, vb0 && in);
@@ -626,29 +634,34 @@ __device__ __forceinline__ double lhs_vertices_tc(const OpData<T> &d, const Stag
                 uint32_t ua, ub;
                 bool va, vb;
                 load_step(base, a, ua, ub, va, vb);
-                float xa[NT], xb[NT];
+                float xa[NTH], xb[NTH];
 #pragma unroll
-                for (int n = 0; n < NT; ++n) {
-                    const uint32_t lm = n * 8 + g;
+                for (int n = 0; n < NTH; ++n) {
+                    const uint32_t lm = (n0 + n) * 8 + g;
                     xa[n] = gather_one<float, FUSEP, COH>(f, pold, beta, ua, aslm, lm, va && lm < slm);
                     xb[n] = gather_one<float, FUSEP, COH>(f, pold, beta, ub, aslm, lm, vb && lm < slm);
                 }
                 kstep(a, xa, xb);
             }
 #pragma unroll
-            for (int n = 0; n < NT; ++n) {
-                sm[g * SA + n * 8 + 2 * t] = acc[n][0];
-                sm[g * SA + n * 8 + 2 * t + 1] = acc[n][1];
-                sm[(g + 8) * SA + n * 8 + 2 * t] = acc[n][2];
-                sm[(g + 8) * SA + n * 8 + 2 * t + 1] = acc[n][3];
+            for (int n = 0; n < NTH; ++n) {
+                if (n0 + n >= NT) break;
+                const int c = (n0 + n) * 8 + 2 * t;
+                sm[g * SA + c] = acc[n][0];
+                sm[g * SA + c + 1] = acc[n][1];
+                sm[(g + 8) * SA + c] = acc[n][2];
+                sm[(g + 8) * SA + c + 1] = acc[n][3];
             }
+          }
         } else {
-            double acc[2][NT][2];
+          for (int pass = 0; pass < kPasses; ++pass) {
+            const int n0 = pass * NTH;  // first n-tile of this column pass
+            double acc[2][NTH][2];
 #pragma unroll
-            for (int n = 0; n < NT; ++n) acc[0][n][0] = acc[0][n][1] = acc[1][n][0] = acc[1][n][1] = 0.0;
+            for (int n = 0; n < NTH; ++n) acc[0][n][0] = acc[0][n][1] = acc[1][n][0] = acc[1][n][1] = 0.0;
             // edges in k-steps of 4; batches of KB k-steps load everything
             // (indices, coefficients, then rows) before their MMAs
-            constexpr int KB = NT <= 4 ? 4 : 2;
+            constexpr int KB = NTH <= 4 ? 4 : 2;
             for (uint32_t base = e0; base < e1; base += 4 * KB) {
                 uint32_t ua[KB];
                 bool va[KB];
@@ -662,31 +675,36 @@ __device__ __forceinline__ double lhs_vertices_tc(const OpData<T> &d, const Stag
                     ahi[k] = (va[k] && axes) ? __ldg(ca + g + 8) : 0.0;
                     ua[k] = va[k] ? __ldg(d.col + ea) : 0u;
                 }
-                double xa[KB][NT];
+                double xa[KB][NTH];
 #pragma unroll
                 for (int k = 0; k < KB; ++k)
 #pragma unroll
-                    for (int n = 0; n < NT; ++n) {
-                        const uint32_t lm = n * 8 + g;
+                    for (int n = 0; n < NTH; ++n) {
+                        const uint32_t lm = (n0 + n) * 8 + g;
                         xa[k][n] = gather_one<double, FUSEP, COH>(f, pold, beta, ua[k], aslm, lm, va[k] && lm < slm);
                     }
 #pragma unroll
                 for (int k = 0; k < KB; ++k)
 #pragma unroll
-                    for (int n = 0; n < NT; ++n) mma_f64(acc[0][n][0], acc[0][n][1], alo[k], xa[k][n]);
+                    for (int n = 0; n < NTH; ++n)
+                        if (n0 + n < NT) mma_f64(acc[0][n][0], acc[0][n][1], alo[k], xa[k][n]);
                 if (axes)  // rows 8-15: the boundary sums (warp-uniform)
 #pragma unroll
                     for (int k = 0; k < KB; ++k)
 #pragma unroll
-                        for (int n = 0; n < NT; ++n) mma_f64(acc[1][n][0], acc[1][n][1], ahi[k], xa[k][n]);
+                        for (int n = 0; n < NTH; ++n)
+                            if (n0 + n < NT) mma_f64(acc[1][n][0], acc[1][n][1], ahi[k], xa[k][n]);
             }
 #pragma unroll
-            for (int n = 0; n < NT; ++n) {
-                sm[g * SA + n * 8 + 2 * t] = acc[0][n][0];
-                sm[g * SA + n * 8 + 2 * t + 1] = acc[0][n][1];
-                sm[(g + 8) * SA + n * 8 + 2 * t] = acc[1][n][0];
-                sm[(g + 8) * SA + n * 8 + 2 * t + 1] = acc[1][n][1];
+            for (int n = 0; n < NTH; ++n) {
+                if (n0 + n >= NT) break;
+                const int c = (n0 + n) * 8 + 2 * t;
+                sm[g * SA + c] = acc[0][n][0];
+                sm[g * SA + c + 1] = acc[0][n][1];
+                sm[(g + 8) * SA + c] = acc[1][n][0];
+                sm[(g + 8) * SA + c + 1] = acc[1][n][1];
             }
+          }
         }
         __syncwarp();
         // epilogue: lane = harmonic
@@ -750,7 +768,7 @@ struct SimtOp {
 };
 template <int NT, typename T>
 struct TcOp {
-    static constexpr int kMinBlocks = NT > 6 ? 1 : 2;  // up to 128 registers: loads in flight over occupancy
+    static constexpr int kMinBlocks = 2;  // up to 128 registers (column passes of <= 4 n-tiles)
     static constexpr int kLanes = 32;
     static constexpr uint32_t kLS = 0;  // any lane stride
     static constexpr bool kTc = true;
