@@ -250,6 +250,13 @@ def run_ours(args, rank, world, local):
     t_mixed, u_mixed, l_mixed, reps_mixed, f_mixed = timed(mixed, args.steps)
     clocks = sampler.stop()
     t_fp64, u_fp64, l_fp64, reps_fp64, _ = timed(fp64, args.steps)
+    # the same two solves with the Jacobi preconditioner (fewer iterations,
+    # slightly dearer ones); reported beside the headline
+    jac = dict(precondition=tr.TR_PREC_JACOBI)
+    ctx.solve(**mixed, **jac)
+    ctx.solve(**fp64, **jac)
+    t_mixed_j, _, _, reps_mixed_j, _ = timed({**mixed, **jac}, args.steps)
+    t_fp64_j, _, _, reps_fp64_j, _ = timed({**fp64, **jac}, args.steps)
     # end to end through the C ABI with host buffers (pinned staging inside)
     b = ctx.allocVector()
     ctx.computeRhs(b)
@@ -279,8 +286,8 @@ def run_ours(args, rank, world, local):
     tr.check(tr.lib.tr_bench_lhs(ctx._h, 32, x32.data_ptr(), y32.data_ptr(), 200, C.byref(ms32)), ctx._h)
     tr.check(tr.lib.tr_bench_lhs(ctx._h, 64, x64.data_ptr(), y64.data_ptr(), 200, C.byref(ms64)), ctx._h)
 
-    (t_mixed, t_fp64, t_e2e), (u_mixed, u_fp64, u_e2e) = aggregate_replicas(
-        [t_mixed, t_fp64, t_e2e], [u_mixed, u_fp64, u_e2e], pg, f"cuda:{local}")
+    (t_mixed, t_fp64, t_e2e, t_mixed_j, t_fp64_j), (u_mixed, u_fp64, u_e2e) = aggregate_replicas(
+        [t_mixed, t_fp64, t_e2e, t_mixed_j, t_fp64_j], [u_mixed, u_fp64, u_e2e], pg, f"cuda:{local}")
 
     if rank == 0:
         peak, peak_kind = load_peaks()
@@ -322,6 +329,10 @@ def run_ours(args, rank, world, local):
             },
             "time_to_solution_ms": {"mixed": t_mixed / args.steps, "fp64": t_fp64 / args.steps,
                                     "speedup_mixed_vs_fp64": t_fp64 / t_mixed},
+            "time_to_solution_ms_jacobi": {
+                "mixed": t_mixed_j / args.steps, "fp64": t_fp64_j / args.steps,
+                "iterations_mixed_fp32_cg": statistics.mean(r.iterations for r in reps_mixed_j),
+                "iterations_fp64_cg": statistics.mean(r.iterations for r in reps_fp64_j)},
             "fp64": {"value": u_fp64 / (t_fp64 * 1e-3), "unit": UNIT, "iterations": it_fp64},
             "iterations": {"mixed_fp32_cg": it_mixed,
                            "mixed_outer": statistics.mean(r.outer_steps for r in reps_mixed),

@@ -290,6 +290,34 @@ tr_status ctx_create(int device, const tr_mesh_view *m, const tr_angular_view *a
     const uint32_t aslm_max = std::max((slm + 7) & ~7u, (slm + 15) & ~15u);
     const uint32_t cls = (aslm_max + 31) & ~31u;
     const uint32_t sa64 = s_row_stride((slm + 7) & ~7u), sa32 = s_row_stride((slm + 15) & ~15u);
+    // Step k of the contraction has every lane lm read one S-table word; the
+    // entries of each harmonic are ordered so that, step by step, the lanes
+    // of a warp hit distinct shared-memory banks (FP32 S table: bank = word
+    // offset mod 32).  Greedy over the lanes of each 32-lane group.
+    {
+        std::vector<std::vector<std::pair<uint32_t, double>>> rem(slm);
+        for (tr_idx lm = 0; lm < slm; ++lm) rem[lm].swap(lists[lm]);
+        for (uint32_t k = 0; k < ckmax; ++k)
+            for (tr_idx g0 = 0; g0 < slm; g0 += 32) {
+                uint32_t used = 0;
+                for (tr_idx lm = g0; lm < std::min<tr_idx>(slm, g0 + 32); ++lm) {
+                    auto &r = rem[lm];
+                    if (r.empty()) continue;
+                    size_t pick = 0;
+                    for (size_t i = 0; i < r.size(); ++i) {
+                        const uint32_t word = (r[i].first >> 8) * sa32 + (r[i].first & 255u);
+                        if (!(used & (1u << (word % 32)))) {
+                            pick = i;
+                            break;
+                        }
+                    }
+                    const uint32_t word = (r[pick].first >> 8) * sa32 + (r[pick].first & 255u);
+                    used |= 1u << (word % 32);
+                    lists[lm].push_back(r[pick]);
+                    r.erase(r.begin() + static_cast<std::ptrdiff_t>(pick));
+                }
+            }
+    }
     const uint32_t satc = (slm + 7) / 8 * 8 + 1;
     const size_t ncon = std::max<size_t>(static_cast<size_t>(ckmax) * cls, 1);
     std::vector<double> cw64(ncon, 0.0);

@@ -374,23 +374,29 @@ __device__ __forceinline__ double lhs_vertices(const OpData<T> &d, const Staged<
     // of its next vertex is queued (cp.async) before the current vertex's
     // angular coupling runs
     uint32_t v = vb0 + threadIdx.x / G;
-    uint32_t e0 = 0, e1 = 0;
+    uint32_t e0 = 0, e1 = 0, axes = 0;
     int cur = 0;
     if (v < vb1) {
         e0 = __ldg(d.row + v);
         e1 = __ldg(d.row + v + 1);
+        axes = __ldg(d.bmask + v);
         stage_edges_async<T>(d, e0, min(static_cast<int>(e1 - e0), G), lane, slab, scolbuf);
     }
     while (v < vb1) {
         uint32_t vn = 0;
         if (lane == 0) vn = vb0 + atomicAdd(&s_next, 1u);
         vn = tile.shfl(vn, 0);
-        uint32_t e0n = 0, e1n = 0;
-        if (vn < vb1) {  // consumed after this vertex's edge loop
+        // loads whose results are used only later in this step are issued
+        // first: the next vertex's edge range and boundary axes, and this
+        // vertex's own row (for <x, A x> and the stored direction)
+        uint32_t e0n = 0, e1n = 0, axesn = 0;
+        if (vn < vb1) {
             e0n = __ldg(d.row + vn);
             e1n = __ldg(d.row + vn + 1);
+            axesn = __ldg(d.bmask + vn);
         }
-        const uint32_t axes = __ldg(d.bmask + v);
+        T xv[H];
+        if (DOT || FUSEP) gather_row<G, H, T, FUSEP, COH>(f, pold, beta, v, aslm, slm, lane, xv);
         EdgeAcc<T> acc[H];
 #pragma unroll
         for (int h = 0; h < H; ++h) acc[h].zero();
@@ -438,6 +444,8 @@ __device__ __forceinline__ double lhs_vertices(const OpData<T> &d, const Staged<
                                  scolbuf + cur * G);
         e0 = e0n;
         e1 = e1n;
+        const uint32_t axes_v = axes;
+        axes = axesn;
         tile.sync();
         // angular coupling through shared memory
 #pragma unroll
@@ -452,7 +460,7 @@ __device__ __forceinline__ double lhs_vertices(const OpData<T> &d, const Staged<
             out[h] = contract_ls<T, LS>(tab.ce + lm, sm, d.ckmax, acc[h].mass(lm == 0));
         }
         // half-range boundary term from the per-axis sums B_n
-        if (axes) {
+        if (axes_v) {
             tile.sync();
 #pragma unroll
             for (int h = 0; h < H; ++h)
@@ -465,7 +473,7 @@ __device__ __forceinline__ double lhs_vertices(const OpData<T> &d, const Staged<
                 if (lm < slm) {
                     T acc0 = T(0), acc1 = T(0), acc2 = T(0), acc3 = T(0);
                     for (int n = 0; n < 3; ++n) {
-                        if (!(axes & (1u << n))) continue;
+                        if (!(axes_v & (1u << n))) continue;
                         const T *On = tab.O + static_cast<size_t>(n) * slm * LS + lm;
                         const T *Bn = sm + n * SA;
                         uint32_t lms = 0;
@@ -483,8 +491,6 @@ __device__ __forceinline__ double lhs_vertices(const OpData<T> &d, const Staged<
         }
         tile.sync();
         T *rv = r + static_cast<size_t>(v) * aslm;
-        T xv[H];
-        if (DOT || FUSEP) gather_row<G, H, T, FUSEP, COH>(f, pold, beta, v, aslm, slm, lane, xv);
 #pragma unroll
         for (int h = 0; h < H; ++h) {
             const uint32_t lm = lane + G * h;
