@@ -219,7 +219,15 @@ enum {
 enum {
     TR_ENGINE_PERSISTENT = 0,/* one cooperative kernel runs many iterations */
     TR_ENGINE_GRAPH = 1,     /* CUDA-graph replay of 2-launch iterations    */
-    TR_ENGINE_LAUNCH = 2     /* the same launches issued one by one         */
+    TR_ENGINE_LAUNCH = 2,    /* the same launches issued one by one         */
+    TR_ENGINE_PERSISTENT_SR = 3 /* mixed mode: the FP32 inner solves run
+                                single-reduction CG (Chronopoulos-Gear: one
+                                grid barrier per iteration) in one
+                                cooperative kernel; same iterates in exact
+                                arithmetic, different rounding.  FP64 mode
+                                and the tensor-core FP32 operator run
+                                TR_ENGINE_PERSISTENT.  No reference
+                                counterpart.                                */
 };
 typedef struct tr_solve_opts {
     int32_t mode;            /* TR_MODE_*                                   */
@@ -234,7 +242,7 @@ typedef struct tr_solve_opts {
                                 still missing to tol, at least 2e-6)        */
     int32_t inner_max_iter;  /* invprec / FP32 inner cap (0 -> 1000)       */
     int32_t max_outer;       /* mixed mode: defect-correction steps (0->30) */
-    int32_t engine;          /* TR_ENGINE_* (all give identical results)    */
+    int32_t engine;          /* TR_ENGINE_* (0-2 give identical results)    */
     int32_t history_len;     /* capacity of history[] (may be 0)            */
     double *history;         /* host array: ||r|| after each CG iteration   */
 } tr_solve_opts;

@@ -94,6 +94,27 @@ def test_mixed_precision_defect_correction(cuda, prec):
     assert rel_err(host(ctx.computeMoments(f2)[0]), O.moments(fo)[0]) < 1e-9
 
 
+@pytest.mark.parametrize("prec", [tr.TR_PREC_NONE, tr.TR_PREC_JACOBI])
+@pytest.mark.parametrize("mesh", ["c1", "small"])
+def test_single_reduction_inner_cg(cuda, prec, mesh):
+    """TR_ENGINE_PERSISTENT_SR (Chronopoulos-Gear inner FP32 CG): the same
+    FP64 solution as the two-reduction inner CG to the solve's accuracy,
+    with a comparable number of inner iterations, reproducible run to run."""
+    md, ad = (c1_mesh(), golden_angular(1)) if mesh == "c1" else (small_mesh(), golden_angular(3))
+    ctx, O = tr.CudaContext(0, md, ad), op.Oracle(md, ad)
+    kw = dict(mode=tr.TR_MODE_MIXED, tol=1e-10, relative=1, precondition=prec, max_iter=20000)
+    fa, ra = ctx.solve(engine=tr.TR_ENGINE_PERSISTENT, **kw)
+    fb, rb = ctx.solve(engine=tr.TR_ENGINE_PERSISTENT_SR, **kw)
+    fc, rc = ctx.solve(engine=tr.TR_ENGINE_PERSISTENT_SR, **kw)
+    assert ra.converged and rb.converged
+    assert rb.final_residual / rb.rhs_norm < 1e-10
+    assert torch.equal(fb, fc) and rb.iterations == rc.iterations
+    assert abs(rb.iterations - ra.iterations) <= max(3, ra.iterations // 10)
+    assert rel_err(host(fb), host(fa)) < 1e-8
+    fo, _ = O.cg(tol=1e-12, relative=1, max_iter=5000)
+    assert rel_err(host(ctx.computeMoments(fb)[0]), O.moments(fo)[0]) < 1e-9
+
+
 def test_engines_agree(cuda):
     """Graph replay and direct launches run the same kernels: bitwise equal.
     The persistent kernel sums its reductions over a different block

@@ -6,7 +6,7 @@ kernels for sm_100a behind a C ABI (include/transfer_b200.h).  This package
 is the Python binding of that library; it has no CPU fallback.
 """
 from ._lib import (TR_BC_INCIDENT, TR_BC_REFLECTIVE, TR_BC_VACUUM, TR_ENGINE_GRAPH, TR_ENGINE_LAUNCH,  # noqa: F401
-                   TR_ENGINE_PERSISTENT, TR_MODE_FP64, TR_MODE_MIXED, TR_PREC_JACOBI, TR_PREC_NONE,
+                   TR_ENGINE_PERSISTENT, TR_ENGINE_PERSISTENT_SR, TR_MODE_FP64, TR_MODE_MIXED, TR_PREC_JACOBI, TR_PREC_NONE,
                    TR_PREC_REFERENCE, TR_OPERATOR_SIMT, TR_OPERATOR_TENSOR, LIB_PATH, TransferError, check, lib)
 from .core import (FACE_DTYPE, TET_DTYPE, AngularData, Config, CudaContext, MeshData, Physics,  # noqa: F401
                    solve_options, trieig)

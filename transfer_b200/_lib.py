@@ -30,7 +30,7 @@ TR_BC_VACUUM, TR_BC_REFLECTIVE, TR_BC_INCIDENT = 0, 1, 2
 TR_SURFACE_AXIS, TR_SURFACE_EXACT = 0, 1
 TR_PREC_NONE, TR_PREC_REFERENCE, TR_PREC_JACOBI = 0, 1, 2
 TR_MODE_FP64, TR_MODE_MIXED = 0, 1
-TR_ENGINE_PERSISTENT, TR_ENGINE_GRAPH, TR_ENGINE_LAUNCH = 0, 1, 2
+TR_ENGINE_PERSISTENT, TR_ENGINE_GRAPH, TR_ENGINE_LAUNCH, TR_ENGINE_PERSISTENT_SR = 0, 1, 2, 3
 TR_OPERATOR_SIMT, TR_OPERATOR_TENSOR = 0, 1
 
 

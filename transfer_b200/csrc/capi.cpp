@@ -255,7 +255,7 @@ static tr_status check_opts(tr_ctx *c, const tr_solve_opts *o) {
     if (!o) return set_err(c, TR_ERR_INVALID_ARG, "null options");
     if (o->mode != TR_MODE_FP64 && o->mode != TR_MODE_MIXED) return set_err(c, TR_ERR_INVALID_ARG, "bad mode");
     if (o->precondition < 0 || o->precondition > 2) return set_err(c, TR_ERR_INVALID_ARG, "bad precondition");
-    if (o->engine < 0 || o->engine > 2) return set_err(c, TR_ERR_INVALID_ARG, "bad engine");
+    if (o->engine < 0 || o->engine > 3) return set_err(c, TR_ERR_INVALID_ARG, "bad engine");
     if (o->mode == TR_MODE_MIXED && o->precondition == TR_PREC_REFERENCE)
         return set_err(c, TR_ERR_UNSUPPORTED, "mixed mode supports precondition 0 or 2");
     if (!(o->tol >= 0.0) || o->max_iter < 0 || o->history_len < 0 || (o->history_len > 0 && !o->history))

@@ -104,6 +104,7 @@ struct CgScalars {
     int32_t done;    // 0 running, 1 converged, 2 iteration cap, 3 non-finite
     int32_t maxit;
     int32_t prec;    // 0 none, 2 jacobi
+    int32_t phase;   // single-reduction CG: steps done (step 0 forms w_0 = A u_0)
     uint32_t counter[4];
 };
 
@@ -126,6 +127,23 @@ struct PcgArgs {
     int iters;
 };
 constexpr int kMaxGrid = 4096;  // partial-sum slots per reduction
+
+// Arguments of the persistent single-reduction CG kernel (operator.cu
+// k_sr_persistent): r, w, s double buffered by step parity; partials holds
+// [2][3][grid] per-block sums (parity-buffered: one barrier per step).
+template <typename T>
+struct SrArgs {
+    T *x, *p;
+    T *R[2], *W[2], *S[2];
+    const T *dinv;
+    struct CgScalars *s;
+    double *hist;
+    int hist_cap;
+    double *partials;
+    unsigned int *bar;
+    int *err;
+    int iters;
+};
 
 struct CachedGraph {
     cudaGraphExec_t exec = nullptr;
@@ -224,7 +242,7 @@ struct tr_ctx {
 
     // solver work space (allocated on first solve)
     double *w64[7] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // x r p Ap z b p'
-    float *w32[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};           // d r p Ap z p'
+    float *w32[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};  // d r p Ap z p' s0 s1
     int grid_vec64 = 0, grid_vec32 = 0;  // vectorised vector kernels
     double *inner[3] = {nullptr, nullptr, nullptr};  // invprec inner CG vectors
     double *io[2] = {nullptr, nullptr};              // tr_solve_host device b / f
@@ -254,6 +272,8 @@ cudaError_t launch_lhs(const tr_ctx *c, const DeviceOp<T> &op, const T *f, T *r,
 template <typename T>
 cudaError_t launch_cg_persistent(const tr_ctx *c, const DeviceOp<T> &op, const PcgArgs<T> &a, cudaStream_t s,
                                  int *grid_out);
+template <typename T>
+cudaError_t launch_sr_persistent(const tr_ctx *c, const DeviceOp<T> &op, const SrArgs<T> &a, cudaStream_t s);
 cudaError_t operator_init_attributes();
 template <typename T>
 cudaError_t launch_lhs_diag(const tr_ctx *c, const DeviceOp<T> &op, const T *f, T *r, const int32_t *done,

@@ -345,10 +345,152 @@ __device__ __forceinline__ void stage_edges_async(const OpData<T> &d, uint32_t b
     cp_async_commit();
 }
 
-template <int G, int H, typename T, bool DOT, bool FUSEP, bool COH = false>
-__device__ __forceinline__ double lhs_vertices(const OpData<T> &d, const Staged<T> &tab, unsigned char *smem_groups,
-                                               const T *__restrict__ f, const T *__restrict__ pold,
-                                               T *__restrict__ pnew, T *__restrict__ r, const T beta) {
+// ---- what the SIMT vertex loop reads and what its owner step writes
+// Src::row(u, lane, x): the input row of neighbour u.  Out::load(v, lane)
+// fetches what the owner step of vertex v needs (issued early), Out::store
+// writes the results of v from its operator row `out` and adds Out::NV
+// partial sums.
+
+// plain operator input (x_u = f[u]) or CG's fused direction (z[u] + beta p_old[u])
+template <int G, int H, typename T, bool FUSEP, bool COH>
+struct SrcDir {
+    const T *f, *pold;
+    T beta;
+    uint32_t aslm, slm;
+    __device__ __forceinline__ void row(uint32_t u, int lane, T (&x)[H]) const {
+        gather_row<G, H, T, FUSEP, COH>(f, pold, beta, u, aslm, slm, lane, x);
+    }
+};
+// A x stored in r; with FUSEP the direction row is stored in pnew; with DOT
+// the partial sum <x, A x>
+template <int G, int H, typename T, bool DOT, bool FUSEP, bool COH>
+struct OutStd {
+    static constexpr int NV = 1;
+    const T *f, *pold;
+    T *pnew, *r;
+    T beta;
+    uint32_t aslm, slm;
+    struct Pre {
+        T xv[H];
+    };
+    __device__ __forceinline__ Pre load(uint32_t v, int lane) const {
+        Pre p;
+        if (DOT || FUSEP) gather_row<G, H, T, FUSEP, COH>(f, pold, beta, v, aslm, slm, lane, p.xv);
+        return p;
+    }
+    __device__ __forceinline__ void store(uint32_t v, int lane, const T (&out)[H], const Pre &p,
+                                          double (&acc)[NV]) const {
+        T *rv = r + static_cast<size_t>(v) * aslm;
+#pragma unroll
+        for (int h = 0; h < H; ++h) {
+            const uint32_t lm = lane + G * h;
+            if (lm < aslm) {
+                rv[lm] = (lm < slm) ? out[h] : T(0);
+                if (FUSEP) pnew[static_cast<size_t>(v) * aslm + lm] = p.xv[h];
+            }
+            if (DOT && lm < slm) acc[0] += static_cast<double>(p.xv[h]) * static_cast<double>(out[h]);
+        }
+    }
+};
+
+// Single-reduction CG (Chronopoulos & Gear, J. Comput. Appl. Math. 25 (1989))
+// with preconditioner M (identity or Jacobi).  Step j reads r_{j-1},
+// w_{j-1} = A u_{j-1}, s_{j-2} and the scalars alpha_{j-1}, beta_{j-1}, and
+// in one pass over the operator forms
+//   s_{j-1} = w_{j-1} + beta s_{j-2},  p_{j-1} = u_{j-1} + beta p_{j-2},
+//   x_j = x_{j-1} + alpha p_{j-1},     r_j = r_{j-1} - alpha s_{j-1},
+//   u_j = M r_j,  w_j = A u_j,  and (r_j, u_j), (w_j, u_j), (r_j, r_j):
+// the neighbours' u_j are formed on the fly from their r, w, s rows, so the
+// two reductions of a CG step meet at one grid barrier.  r, w, s are double
+// buffered (read j-1, write j); p and x are only touched by their owner.
+template <typename T>
+struct SrStep {
+    const T *r, *w, *s;  // r_{j-1}, w_{j-1}, s_{j-2}
+    T *rn, *wn, *sn;     // r_j, w_j, s_{j-1}
+    T *p, *x;            // p_{j-2} -> p_{j-1}, x_{j-1} -> x_j
+    const T *dinv;       // Jacobi, or null
+    T alpha, beta;       // alpha_{j-1}, beta_{j-1}
+};
+// u_j from the step-(j-1) rows; the owner forms the same value with the same operations
+template <typename T, bool JAC>
+__device__ __forceinline__ T sr_u(T r, T w, T s, T dv, T alpha, T beta, T &s1, T &r1) {
+    s1 = fma(beta, s, w);
+    r1 = fma(-alpha, s1, r);
+    return JAC ? dv * r1 : r1;
+}
+template <int G, int H, typename T, bool JAC>
+struct SrcSr {
+    SrStep<T> st;
+    uint32_t aslm, slm;
+    __device__ __forceinline__ void row(uint32_t u, int lane, T (&x)[H]) const {
+        const size_t o = static_cast<size_t>(u) * aslm;
+#pragma unroll
+        for (int h = 0; h < H; ++h) {
+            const uint32_t lm = lane + G * h;
+            if (lm < slm) {
+                const T dv = JAC ? ldv<false>(st.dinv + o + lm) : T(1);
+                T s1, r1;
+                x[h] = sr_u<T, JAC>(ldv<true>(st.r + o + lm), ldv<true>(st.w + o + lm), ldv<true>(st.s + o + lm), dv,
+                                    st.alpha, st.beta, s1, r1);
+            } else {
+                x[h] = T(0);
+            }
+        }
+    }
+};
+template <int G, int H, typename T, bool JAC>
+struct OutSr {
+    static constexpr int NV = 3;  // (r_j, u_j), (w_j, u_j), (r_j, r_j)
+    SrStep<T> st;
+    uint32_t aslm, slm;
+    struct Pre {
+        T r[H], w[H], s[H], p[H], x[H], dv[H];
+    };
+    __device__ __forceinline__ Pre load(uint32_t v, int lane) const {
+        Pre q;
+        const size_t o = static_cast<size_t>(v) * aslm;
+#pragma unroll
+        for (int h = 0; h < H; ++h) {
+            const uint32_t lm = lane + G * h;
+            const bool in = lm < aslm;
+            q.r[h] = in ? ldv<true>(st.r + o + lm) : T(0);
+            q.w[h] = in ? ldv<true>(st.w + o + lm) : T(0);
+            q.s[h] = in ? ldv<true>(st.s + o + lm) : T(0);
+            q.p[h] = in ? st.p[o + lm] : T(0);
+            q.x[h] = in ? st.x[o + lm] : T(0);
+            q.dv[h] = (JAC && in) ? ldv<false>(st.dinv + o + lm) : T(1);
+        }
+        return q;
+    }
+    __device__ __forceinline__ void store(uint32_t v, int lane, const T (&out)[H], const Pre &q,
+                                          double (&acc)[NV]) const {
+        const size_t o = static_cast<size_t>(v) * aslm;
+#pragma unroll
+        for (int h = 0; h < H; ++h) {
+            const uint32_t lm = lane + G * h;
+            if (lm >= aslm) continue;
+            T s1, r1;
+            const T uj = sr_u<T, JAC>(q.r[h], q.w[h], q.s[h], q.dv[h], st.alpha, st.beta, s1, r1);
+            const T u0 = JAC ? q.dv[h] * q.r[h] : q.r[h];     // u_{j-1}
+            const T p1 = fma(st.beta, q.p[h], u0);            // p_{j-1}
+            const T wj = (lm < slm) ? out[h] : T(0);
+            st.sn[o + lm] = s1;
+            st.p[o + lm] = p1;
+            st.x[o + lm] = fma(st.alpha, p1, q.x[h]);
+            st.rn[o + lm] = r1;
+            st.wn[o + lm] = wj;
+            if (lm < slm) {
+                acc[0] += static_cast<double>(r1) * static_cast<double>(uj);
+                acc[1] += static_cast<double>(wj) * static_cast<double>(uj);
+                acc[2] += static_cast<double>(r1) * static_cast<double>(r1);
+            }
+        }
+    }
+};
+
+template <int G, int H, typename T, class Src, class Out>
+__device__ __forceinline__ void simt_vertices(const OpData<T> &d, const Staged<T> &tab, unsigned char *smem_groups,
+                                              const Src &src, const Out &fin, double (&dacc)[Out::NV]) {
     constexpr int SA = G * H + 1;  // padded row of the shared S / B tables
     constexpr int NB = batch_of(H);
     constexpr int LS = G * H < 32 ? 32 : G * H;  // lane stride of the tables (== d.cls, checked at launch)
@@ -359,7 +501,8 @@ __device__ __forceinline__ double lhs_vertices(const OpData<T> &d, const Staged<
     cg::thread_block_tile<G> tile = cg::tiled_partition<G>(cg::this_thread_block());
     const int lane = threadIdx.x % G;
     const uint32_t gpb = blockDim.x / G;
-    double dacc = 0.0;
+#pragma unroll
+    for (int q = 0; q < Out::NV; ++q) dacc[q] = 0.0;
 
     // Each block owns a contiguous range of vertices (neighbouring rows are
     // shared in L1); its groups take the range's vertices one at a time from
@@ -395,8 +538,7 @@ __device__ __forceinline__ double lhs_vertices(const OpData<T> &d, const Staged<
             e1n = __ldg(d.row + vn + 1);
             axesn = __ldg(d.bmask + vn);
         }
-        T xv[H];
-        if (DOT || FUSEP) gather_row<G, H, T, FUSEP, COH>(f, pold, beta, v, aslm, slm, lane, xv);
+        const typename Out::Pre pre = fin.load(v, lane);
         EdgeAcc<T> acc[H];
 #pragma unroll
         for (int h = 0; h < H; ++h) acc[h].zero();
@@ -426,13 +568,13 @@ __device__ __forceinline__ double lhs_vertices(const OpData<T> &d, const Staged<
                 T x[NB][H];
 #pragma unroll
                 for (int b = 0; b < NB; ++b)
-                    gather_row<G, H, T, FUSEP, COH>(f, pold, beta, tile.shfl(ul, jj + b), aslm, slm, lane, x[b]);
+                    src.row(tile.shfl(ul, jj + b), lane, x[b]);
 #pragma unroll
                 for (int b = 0; b < NB; ++b) accumulate(scoef + (jj + b) * kCoefStride, x[b]);
             }
             for (; jj < cnt; ++jj) {
                 T x[H];
-                gather_row<G, H, T, FUSEP, COH>(f, pold, beta, tile.shfl(ul, jj), aslm, slm, lane, x);
+                src.row(tile.shfl(ul, jj), lane, x);
                 accumulate(scoef + jj * kCoefStride, x);
             }
         }
@@ -490,19 +632,20 @@ __device__ __forceinline__ double lhs_vertices(const OpData<T> &d, const Staged<
             }
         }
         tile.sync();
-        T *rv = r + static_cast<size_t>(v) * aslm;
-#pragma unroll
-        for (int h = 0; h < H; ++h) {
-            const uint32_t lm = lane + G * h;
-            if (lm < aslm) {
-                rv[lm] = (lm < slm) ? out[h] : T(0);
-                if (FUSEP) pnew[static_cast<size_t>(v) * aslm + lm] = xv[h];
-            }
-            if (DOT && lm < slm) dacc += static_cast<double>(xv[h]) * static_cast<double>(out[h]);
-        }
+        fin.store(v, lane, out, pre, dacc);
         v = vn;
     }
-    return dacc;
+}
+
+template <int G, int H, typename T, bool DOT, bool FUSEP, bool COH = false>
+__device__ __forceinline__ double lhs_vertices(const OpData<T> &d, const Staged<T> &tab, unsigned char *smem_groups,
+                                               const T *__restrict__ f, const T *__restrict__ pold,
+                                               T *__restrict__ pnew, T *__restrict__ r, const T beta) {
+    const SrcDir<G, H, T, FUSEP, COH> src{f, pold, beta, d.aslm, d.slm};
+    const OutStd<G, H, T, DOT, FUSEP, COH> fin{f, pold, pnew, r, beta, d.aslm, d.slm};
+    double acc[1];
+    simt_vertices<G, H, T>(d, tab, smem_groups, src, fin, acc);
+    return acc[0];
 }
 
 
@@ -771,6 +914,13 @@ struct SimtOp {
                                  const T *pold, T *pnew, T *r, T beta) {
         return lhs_vertices<G, H, T, DOT, FUSEP, COH>(d, tab, slabs, f, pold, pnew, r, beta);
     }
+    template <bool JAC>
+    __device__ static void run_sr(const OpData<T> &d, const Staged<T> &tab, unsigned char *slabs, const SrStep<T> &st,
+                                  double (&dots)[3]) {
+        const SrcSr<G, H, T, JAC> src{st, d.aslm, d.slm};
+        const OutSr<G, H, T, JAC> fin{st, d.aslm, d.slm};
+        simt_vertices<G, H, T>(d, tab, slabs, src, fin, dots);
+    }
 };
 template <int NT, typename T>
 struct TcOp {
@@ -999,6 +1149,87 @@ __global__ void __launch_bounds__(Op::kPersistThreads, 1)
     }
 }
 
+// Single-reduction CG (see SrStep) for up to a.iters steps in one
+// cooperative launch: per step one operator pass with the owner updates,
+// one grid barrier, then every block derives
+//   step 0:  beta_0 = 0, alpha_0 = gamma_0 / delta_0
+//   step j:  beta_j = gamma_j / gamma_{j-1},
+//            alpha_j = gamma_j / (delta_j - beta_j gamma_j / alpha_{j-1})
+// from gamma_j = (r_j, u_j), delta_j = (w_j, u_j) and stops on ||r_j||
+// (rho_j = (r_j, r_j)) like the two-reduction kernel.  After step j the
+// solve has made j CG iterations and x holds x_j.
+template <class Op, typename T, bool JAC>
+__global__ void __launch_bounds__(Op::kPersistThreads, 1)
+    k_sr_persistent(const OpData<T> d, const SrArgs<T> a, int stage_flags) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ double sh[32];
+    const Staged<T> tab = stage_tables<T>(d, smem_raw, stage_flags);
+    CgScalars *s = a.s;
+    unsigned int target = 0;  // grid_barrier arrival target
+    if (__ldcg(&s->done)) return;
+    int j = __ldcg(&s->phase);
+    const int maxit = s->maxit;
+    const double tol = s->tol;
+    double gamma_prev = __ldcg(&s->nrz), alpha_prev = __ldcg(&s->alpha), beta_prev = __ldcg(&s->beta);
+    for (int it = 0; it < a.iters; ++it) {
+        const int par = j & 1;
+        SrStep<T> st;
+        st.r = a.R[par ^ 1];
+        st.w = a.W[par ^ 1];
+        st.s = a.S[par];
+        st.rn = a.R[par];
+        st.wn = a.W[par];
+        st.sn = a.S[par ^ 1];
+        st.p = a.p;
+        st.x = a.x;
+        st.dinv = a.dinv;
+        st.alpha = static_cast<T>(alpha_prev);
+        st.beta = static_cast<T>(beta_prev);
+        double dots[3];
+        Op::template run_sr<JAC>(d, tab, smem_raw + tab.bytes, st, dots);
+        double *part = a.partials + static_cast<size_t>(par) * 3 * gridDim.x;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            const double bq = block_sum(dots[q], sh);
+            if (threadIdx.x == 0) part[q * gridDim.x + blockIdx.x] = bq;
+        }
+        if (!grid_barrier(a.bar, a.err, target)) return;
+        double t[3];
+        sum_partials<3>(part, t);
+        const double gamma = t[0], delta = t[1], nr = sqrt(t[2]);
+        double alpha = alpha_prev, beta = beta_prev;
+        int dn = 0;
+        if (!isfinite(nr) || !isfinite(gamma) || !isfinite(delta)) dn = 3;
+        else if (nr < tol) dn = 1;
+        else if (j >= maxit) dn = 2;
+        else {
+            if (j == 0) {
+                beta = 0.0;
+                alpha = gamma / delta;
+            } else {
+                beta = gamma / gamma_prev;
+                alpha = gamma / (delta - beta * gamma / alpha_prev);
+            }
+            if (!isfinite(alpha) || !isfinite(beta)) dn = 3;
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            if (a.hist && j >= 1 && j - 1 < a.hist_cap) a.hist[j - 1] = nr;
+            s->alpha = alpha;
+            s->beta = beta;
+            s->nrz = gamma;
+            s->rr = t[2];
+            s->k = j;
+            s->phase = j + 1;
+            s->done = dn;
+        }
+        gamma_prev = gamma;
+        alpha_prev = alpha;
+        beta_prev = beta;
+        ++j;
+        if (dn) break;
+    }
+}
+
 // rightHandSide (kernels.cu:135-165): b[v][0] = sum_t kappa_volume I_p / 4 in
 // the vertex's tet order; inflow faces add I A/3 <|Omega_n| Y_lm>.
 template <typename T>
@@ -1189,6 +1420,48 @@ template cudaError_t launch_cg_persistent<double>(const tr_ctx *, const DeviceOp
                                                   cudaStream_t, int *);
 template cudaError_t launch_cg_persistent<float>(const tr_ctx *, const DeviceOp<float> &, const PcgArgs<float> &,
                                                  cudaStream_t, int *);
+
+template <class Op, typename T, bool JAC>
+static cudaError_t launch_sr(const tr_ctx *c, const OpData<T> &d, const SrArgs<T> &a, uint32_t nnz, cudaStream_t s) {
+    if (Op::kLS && d.cls != Op::kLS) return cudaErrorInvalidValue;
+    constexpr int threads = Op::kPersistThreads;
+    auto kern = k_sr_persistent<Op, T, JAC>;
+    const size_t smem = lhs_smem<Op, T>(d.slm, d.cls, nnz, threads);
+    static size_t opted = 0;
+    cudaError_t e = opt_in_smem(kern, smem, opted);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+    if (e != cudaSuccess) return e;
+    if (per_sm < 1) return cudaErrorCooperativeLaunchTooLarge;
+    const int gpb = threads / Op::kLanes;
+    const int need = static_cast<int>((d.nP + gpb - 1) / gpb);
+    const int grid = std::max(1, std::min(per_sm * c->num_sms, std::min(need, kMaxGrid / 2)));
+    int flags = stage_flags<Op, T>(d.slm, d.cls, nnz);
+    OpData<T> dd = d;
+    SrArgs<T> aa = a;
+    void *args[] = {&dd, &aa, &flags};
+    return cudaLaunchCooperativeKernel(reinterpret_cast<void *>(kern), grid, threads, args, smem, s);
+}
+
+// the SIMT operator policies only (TR_OPERATOR_SIMT)
+template <typename T>
+cudaError_t launch_sr_persistent(const tr_ctx *c, const DeviceOp<T> &op, const SrArgs<T> &a, cudaStream_t s) {
+    if (op.kind != TR_OPERATOR_SIMT) return cudaErrorNotSupported;
+    const OpData<T> d = op.data(c->nP, c->slm);
+    const uint32_t nnz = op.ang_nnz;
+    const bool jac = a.dinv != nullptr;
+    return with_op<T>(op, c->slm, [&](auto tag) -> cudaError_t {
+        typedef decltype(tag) Op;
+        if constexpr (Op::kTc) {
+            return cudaErrorNotSupported;
+        } else {
+            return jac ? launch_sr<Op, T, true>(c, d, a, nnz, s) : launch_sr<Op, T, false>(c, d, a, nnz, s);
+        }
+    });
+}
+template cudaError_t launch_sr_persistent<float>(const tr_ctx *, const DeviceOp<float> &, const SrArgs<float> &,
+                                                 cudaStream_t);
 
 static RhsData rhs_data(const tr_ctx *c) {
     RhsData d;

@@ -89,7 +89,7 @@ tr_status ensure_workspace(tr_ctx *c, int hist_cap) {
             c->last_error = "out of device memory (solver work vectors)";
             return TR_ERR_OUT_OF_MEMORY;
         }
-    for (int i = 0; i < 6; ++i)
+    for (int i = 0; i < 8; ++i)
         if (!alloc(reinterpret_cast<void **>(&c->w32[i]), n32 * sizeof(float))) {
             c->last_error = "out of device memory (solver work vectors)";
             return TR_ERR_OUT_OF_MEMORY;
@@ -284,6 +284,46 @@ static tr_status run_cg(tr_ctx *c, int slot, const DeviceOp<T> &op, uint32_t asl
     return TR_OK;
 }
 
+// the engine of the two-reduction CG loops (TR_ENGINE_PERSISTENT_SR only
+// changes the FP32 inner solves of the mixed mode)
+static int base_engine(int engine) { return engine == TR_ENGINE_PERSISTENT_SR ? TR_ENGINE_PERSISTENT : engine; }
+
+// Single-reduction CG steps (k_sr_persistent) from a started state until
+// done; the same launch / status-read loop as the persistent engine.
+template <typename T>
+static tr_status run_sr(tr_ctx *c, const DeviceOp<T> &op, SrArgs<T> a, int *iters, int *done_out) {
+    cudaStream_t st = stream_of(c);
+    a.partials = c->partials;
+    a.bar = c->bar;
+    a.err = c->bar_err;
+    a.iters = kPersistChunk;
+    int k = 0, done = 0;
+    for (int guard = 0; guard < (1 << 24); ++guard) {
+        TRY(cudaMemsetAsync(c->bar, 0, sizeof(unsigned int), st));  // grid_barrier's arrival count
+        TRY(cudaEventRecord(c->ev[2], st));
+        TRY(launch_sr_persistent<T>(c, op, a, st));
+        TRY(cudaEventRecord(c->ev[3], st));
+        ++c->launches;
+        int32_t *h = reinterpret_cast<int32_t *>(c->host_pinned);
+        TRY(cudaMemcpyAsync(h, &a.s->k, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        TRY(cudaMemcpyAsync(h + 2, c->bar_err, sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+        TRY(cudaStreamSynchronize(st));
+        k = h[0];
+        done = h[1];
+        add_cg_time(c);
+        if (h[2]) {
+            c->last_error = "single-reduction CG: grid barrier timed out";
+            cudaMemsetAsync(c->bar_err, 0, sizeof(int), st);
+            cudaMemsetAsync(c->bar, 0, 2 * sizeof(unsigned int), st);
+            return TR_ERR_CUDA;
+        }
+        if (done) break;
+    }
+    *iters = k;
+    *done_out = done;
+    return TR_OK;
+}
+
 // invprec (main.cpp:223-248): z = approximately D^-1 r by an inner CG on
 // computeLhsDiag from z = 0 to ||r_inner|| < inner_tol (absolute).
 static tr_status invprec(tr_ctx *c, const double *b, double *z, int inner_max, double inner_tol, int *inner_k,
@@ -341,7 +381,7 @@ static tr_status solve_fp64(tr_ctx *c, const tr_solve_opts *o, const double *b, 
         LAUNCH(launch_cg_start<double>(c, c->aslm, b, x, r, z, p, dinv, s, 1, st));
         int slot = dinv ? 1 : 0;
         ts = run_cg<double>(c, slot, c->op64, c->aslm, x, r, pbuf, Ap, z, dinv, s, c->dhist, c->hist_cap,
-                            o->engine, &k, &done);
+                            base_engine(o->engine), &k, &done);
         if (ts != TR_OK) return ts;
         rep->lhs_applications_f64 += k;
     } else {
@@ -396,6 +436,8 @@ static tr_status solve_mixed(tr_ctx *c, const tr_solve_opts *o, const double *b,
     const double *bb_src = b;
     const float *dinv = (o->precondition == TR_PREC_JACOBI) ? c->op32.dinv : nullptr;
     const int max_outer = o->max_outer > 0 ? o->max_outer : 30;
+    // single-reduction inner CG: the SIMT FP32 operator only
+    const bool single_reduction = o->engine == TR_ENGINE_PERSISTENT_SR && c->op32.kind == TR_OPERATOR_SIMT;
     const int inner_max = o->inner_max_iter > 0 ? o->inner_max_iter : (o->max_iter > 0 ? o->max_iter : 1000);
 
     tr_status ts = init_scalars(c, so, 0.0, 0, st);
@@ -421,12 +463,36 @@ static tr_status solve_mixed(tr_ctx *c, const tr_solve_opts *o, const double *b,
             o->inner_tol > 0 ? o->inner_tol : std::min(0.5, std::max(0.3 * target / rn, kMixedInnerFloor));
         ts = init_scalars(c, si, inner_tol, inner_max, st);
         if (ts != TR_OK) return ts;
-        LAUNCH(launch_cg_start<float>(c, c->aslm32, r, d, r, z, p, dinv, si, 1, st));
         int k = 0, done = 0;
-        int slot = dinv ? 3 : 2;
-        float *const pbuf[2] = {p, c->w32[5]};
-        ts = run_cg<float>(c, slot, c->op32, c->aslm32, d, r, pbuf, Ap, z, dinv, si, nullptr, 0, o->engine, &k,
-                           &done);
+        if (single_reduction) {
+            // step 0 reads r_{-1} = r (the FP32 residual) and zero w_{-1},
+            // s_{-2}, p_{-2}, x_{-1}
+            const size_t bytes = sizeof(float) * c->nP * c->aslm32;
+            SrArgs<float> a;
+            a.x = d;
+            a.p = p;
+            a.R[0] = z;
+            a.R[1] = r;
+            a.W[0] = Ap;
+            a.W[1] = c->w32[5];
+            a.S[0] = c->w32[6];
+            a.S[1] = c->w32[7];
+            a.dinv = dinv;
+            a.s = si;
+            a.hist = nullptr;
+            a.hist_cap = 0;
+            TRY(cudaMemsetAsync(a.x, 0, bytes, st));
+            TRY(cudaMemsetAsync(a.p, 0, bytes, st));
+            TRY(cudaMemsetAsync(a.W[1], 0, bytes, st));
+            TRY(cudaMemsetAsync(a.S[0], 0, bytes, st));
+            ts = run_sr<float>(c, c->op32, a, &k, &done);
+        } else {
+            LAUNCH(launch_cg_start<float>(c, c->aslm32, r, d, r, z, p, dinv, si, 1, st));
+            int slot = dinv ? 3 : 2;
+            float *const pbuf[2] = {p, c->w32[5]};
+            ts = run_cg<float>(c, slot, c->op32, c->aslm32, d, r, pbuf, Ap, z, dinv, si, nullptr, 0, base_engine(o->engine), &k,
+                               &done);
+        }
         if (ts != TR_OK) return ts;
         total += k;
         rep->lhs_applications_f32 += k;
