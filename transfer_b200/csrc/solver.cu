@@ -36,6 +36,8 @@ cudaError_t launch_residual(const tr_ctx *c, const double *b, const double *Ax, 
                             cudaStream_t st);
 cudaError_t launch_to_f32(const tr_ctx *c, const double *r64, float *r32, const CgScalars *s, cudaStream_t st);
 cudaError_t launch_correct(const tr_ctx *c, double *x, const float *d32, const CgScalars *s, cudaStream_t st);
+cudaError_t launch_cg_reliable(const tr_ctx *c, float *f, const float *r, float *z, const float *dinv, CgScalars *s,
+                               double ratio, cudaStream_t st);
 
 // alpha = nrz / *dot (invprec's inner CG, whose operator launch has no fused dot)
 __global__ void k_set_alpha(CgScalars *s, const double *dot) {
@@ -73,6 +75,10 @@ static cudaStream_t stream_of(const tr_ctx *c) { return c->stream ? c->stream : 
 
 // smallest relative residual asked of one FP32 inner solve
 constexpr double kMixedInnerFloor = 2e-6;
+#ifndef TR_RELIABLE_DELTA
+#define TR_RELIABLE_DELTA 1e-3
+#endif
+constexpr double kReliableDelta = TR_RELIABLE_DELTA;
 
 tr_status ensure_workspace(tr_ctx *c, int hist_cap) {
     const size_t n64 = static_cast<size_t>(c->nP) * c->aslm, n32 = static_cast<size_t>(c->nP) * c->aslm32;
@@ -454,17 +460,30 @@ static tr_status solve_mixed(tr_ctx *c, const tr_solve_opts *o, const double *b,
     double rn = bnorm;
     int total = 0, outer = 0, hist_used = 0;
     bool converged = (rn < target);
+    // The two-reduction FP32 CG runs with reliable updates: after each
+    // defect correction it continues with its last direction instead of
+    // restarting, so the Krylov space built so far is kept (the FP32 CG
+    // runs in the frame of the normalised residual; frame_scale is that
+    // frame's ||r64||).  The single-reduction engine restarts each time.
+    bool started = false, restart = true;
+    int k_run = 0;
+    double frame_scale = rn, leg_tol = 0.0;
     while (!converged && outer < max_outer && total < (o->max_iter > 0 ? o->max_iter : 1 << 30)) {
         LAUNCH(launch_to_f32(c, r64, r, so, st));
         // each FP32 solve aims at what is still missing to the target
         // (relative to the normalised residual), floored where FP32 CG
         // stops gaining true accuracy
+        // (the continued CG updates reliably every kReliableDelta of residual
+        // reduction: longer FP32 legs let the recursive residual drift from
+        // the true one, which a continued direction cannot absorb)
         const double inner_tol =
-            o->inner_tol > 0 ? o->inner_tol : std::min(0.5, std::max(0.3 * target / rn, kMixedInnerFloor));
-        ts = init_scalars(c, si, inner_tol, inner_max, st);
-        if (ts != TR_OK) return ts;
+            o->inner_tol > 0 ? o->inner_tol
+                             : std::min(0.5, std::max(0.3 * target / rn,
+                                                      single_reduction ? kMixedInnerFloor : kReliableDelta));
         int k = 0, done = 0;
         if (single_reduction) {
+            ts = init_scalars(c, si, inner_tol, inner_max, st);
+            if (ts != TR_OK) return ts;
             // step 0 reads r_{-1} = r (the FP32 residual) and zero w_{-1},
             // s_{-2}, p_{-2}, x_{-1}
             const size_t bytes = sizeof(float) * c->nP * c->aslm32;
@@ -487,11 +506,35 @@ static tr_status solve_mixed(tr_ctx *c, const tr_solve_opts *o, const double *b,
             TRY(cudaMemsetAsync(a.S[0], 0, bytes, st));
             ts = run_sr<float>(c, c->op32, a, &k, &done);
         } else {
-            LAUNCH(launch_cg_start<float>(c, c->aslm32, r, d, r, z, p, dinv, si, 1, st));
+            if (restart) {
+                ts = init_scalars(c, si, inner_tol, inner_max, st);
+                if (ts != TR_OK) return ts;
+                LAUNCH(launch_cg_start<float>(c, c->aslm32, r, d, r, z, p, dinv, si, 1, st));
+                started = true;
+                k_run = 0;
+            } else {
+                // new stop rule for this leg, then the reliable update
+                CgScalars h;
+                h.tol = inner_tol;
+                h.maxit = k_run + inner_max;
+                TRY(cudaMemcpyAsync(&si->tol, &h.tol, sizeof(double), cudaMemcpyHostToDevice, st));
+                TRY(cudaMemcpyAsync(&si->maxit, &h.maxit, sizeof(int32_t), cudaMemcpyHostToDevice, st));
+                LAUNCH(launch_cg_reliable(c, d, r, z, dinv, si, rn / frame_scale, st));
+                // the graph and launch engines take p_old from buffer 0 at the
+                // start of a leg (the persistent kernel from buffer k & 1)
+                if (k_run & 1)
+                    TRY(cudaMemcpyAsync(p, c->w32[5], sizeof(float) * c->nP * c->aslm32, cudaMemcpyDeviceToDevice,
+                                        st));
+            }
+            frame_scale = rn;
             int slot = dinv ? 3 : 2;
             float *const pbuf[2] = {p, c->w32[5]};
-            ts = run_cg<float>(c, slot, c->op32, c->aslm32, d, r, pbuf, Ap, z, dinv, si, nullptr, 0, base_engine(o->engine), &k,
-                               &done);
+            int kc = 0;
+            ts = run_cg<float>(c, slot, c->op32, c->aslm32, d, r, pbuf, Ap, z, dinv, si, nullptr, 0,
+                               base_engine(o->engine), &kc, &done);
+            k = kc - k_run;  // iterations of this leg
+            k_run = kc;
+            leg_tol = inner_tol;
         }
         if (ts != TR_OK) return ts;
         total += k;
@@ -509,6 +552,10 @@ static tr_status solve_mixed(tr_ctx *c, const tr_solve_opts *o, const double *b,
             return TR_ERR_NAN;
         }
         converged = rn < target;
+        // continue the Krylov space only while the FP32 recursion tracks the
+        // true residual; if the leg's true residual missed its goal by more
+        // than 10x, the next leg restarts from p = 0
+        if (started && !single_reduction) restart = !(rn <= 10.0 * leg_tol * frame_scale) || done == 2;
         if (done == 3) {
             c->last_error = "FP32 inner CG produced a non-finite residual";
             return TR_ERR_NAN;

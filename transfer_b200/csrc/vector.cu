@@ -169,6 +169,37 @@ __global__ void __launch_bounds__(kBlock) k_cg_start(size_t n, uint32_t aslm, ui
     }
 }
 
+// Reliable update of the FP32 CG of the mixed mode (after x64 += scale d and
+// an FP64 residual): r holds the new true residual in its new scale; the
+// correction d restarts at 0, z = D^-1 r (or r), and the CG continues with
+// its last direction p: beta = (r, z)_new / (r, z)_old * ratio, where ratio
+// = new scale / old scale carries p into the new scale (see solve_mixed).
+template <typename T>
+__global__ void __launch_bounds__(kBlock) k_cg_reliable(size_t n, uint32_t aslm, uint32_t slm, T *__restrict__ f,
+                                                        const T *__restrict__ r, T *__restrict__ z,
+                                                        const T *__restrict__ dinv, CgScalars *s, double ratio,
+                                                        double *partials, unsigned int *counter) {
+    double rz = 0.0, rr = 0.0;
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const T ri = r[i];
+        f[i] = T(0);
+        const T zi = dinv ? dinv[i] * ri : ri;
+        if (dinv) z[i] = zi;
+        if (static_cast<uint32_t>(i % aslm) < slm) {
+            rz += static_cast<double>(ri) * static_cast<double>(zi);
+            rr += static_cast<double>(ri) * static_cast<double>(ri);
+        }
+    }
+    double v[2] = {rz, rr}, tot[2];
+    if (grid_reduce<2>(v, partials, counter, tot) && threadIdx.x == 0) {
+        s->beta = (s->nrz != 0.0) ? tot[0] / s->nrz * ratio : 0.0;
+        s->nrz = tot[0];
+        s->rr = tot[1];
+        s->done = (tot[0] == 0.0) ? 1 : 0;
+    }
+}
+
 // Defect correction: r = b - Ax in FP64 with ||r||^2 -> s->rr, s->scale.
 __global__ void __launch_bounds__(kBlock) k_residual(size_t n, uint32_t aslm, uint32_t slm,
                                                      const double *__restrict__ b, const double *__restrict__ Ax,
@@ -323,6 +354,12 @@ cudaError_t launch_residual(const tr_ctx *c, const double *b, const double *Ax, 
 }
 cudaError_t launch_to_f32(const tr_ctx *c, const double *r64, float *r32, const CgScalars *s, cudaStream_t st) {
     k_to_f32<<<c->grid_vec, kBlock, 0, st>>>(c->nP, c->slm, c->aslm, c->aslm32, r64, r32, s);
+    return cudaGetLastError();
+}
+cudaError_t launch_cg_reliable(const tr_ctx *c, float *f, const float *r, float *z, const float *dinv, CgScalars *s,
+                               double ratio, cudaStream_t st) {
+    k_cg_reliable<float><<<c->grid_vec, kBlock, 0, st>>>(static_cast<size_t>(c->nP) * c->aslm32, c->aslm32, c->slm,
+                                                         f, r, z, dinv, s, ratio, c->partials, c->counters + 2);
     return cudaGetLastError();
 }
 cudaError_t launch_correct(const tr_ctx *c, double *x, const float *d32, const CgScalars *s, cudaStream_t st) {
