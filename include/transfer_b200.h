@@ -287,6 +287,14 @@ tr_status tr_solve_host(tr_ctx *ctx, const tr_solve_opts *opts,
 tr_status tr_bench_lhs(tr_ctx *ctx, int precision, const void *x, void *y,
                        int iters, double *ms_per_launch);
 
+/* Self-test of the bounded grid barrier of the persistent CG kernels (no
+ * reference counterpart): a cooperative grid of one block per SM on `device`
+ * runs `rounds` barriers; if skip_block >= 0 that block never arrives, and
+ * the others must give up after max_polls (<= 2^24) polls each.
+ * *timed_out = 1 when the barrier gave up (the device stays usable). */
+tr_status tr_selftest_grid_barrier(int device, int skip_block, int rounds,
+                                   unsigned int max_polls, int *timed_out);
+
 /* ---- post-processing (MeshData::ComputeMoments / ComputeFlux,
  *      MeshData.cpp:96-136), on the device ----------------------------- */
 /* U[nP] = 4 pi I_00 ; T[3][3][nP] = 4 pi sum_lm omega_i[lm][0] I_lm. */

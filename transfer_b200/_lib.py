@@ -128,6 +128,7 @@ PROTOTYPES = [
     ("tr_solve", S, [P, C.POINTER(tr_solve_opts), P, P, C.POINTER(tr_solve_report)]),
     ("tr_solve_host", S, [P, C.POINTER(tr_solve_opts), P, P, C.POINTER(tr_solve_report)]),
     ("tr_bench_lhs", S, [P, I, P, P, I, C.POINTER(D)]),
+    ("tr_selftest_grid_barrier", S, [I, I, I, C.c_uint, C.POINTER(I)]),
     ("tr_compute_moments", S, [P, P, P, P]),
     ("tr_compute_flux", S, [P, P, P]),
     ("tr_eig_lanczos", S, [P, P, P, P, I, C.POINTER(D), C.POINTER(D), C.POINTER(I)]),

@@ -350,6 +350,37 @@ tr_status tr_bench_lhs(tr_ctx *c, int precision, const void *x, void *y, int ite
     return s;
 }
 
+// ------------------------------------------------------------- self-test
+tr_status tr_selftest_grid_barrier(int device, int skip_block, int rounds, unsigned int max_polls, int *timed_out) {
+    if (!timed_out || rounds < 1 || max_polls < 1 || max_polls > (1u << 24))
+        return set_err(nullptr, TR_ERR_INVALID_ARG, "tr_selftest_grid_barrier: bad arguments");
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+        cudaGetLastError();
+        return set_err(nullptr, TR_ERR_NO_DEVICE, "tr_selftest_grid_barrier: no such CUDA device");
+    }
+    int prev = 0;
+    cudaGetDevice(&prev);
+    tr_status st = check_cuda(nullptr, cudaSetDevice(device), "cudaSetDevice");
+    if (st != TR_OK) return st;
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    unsigned int *count = nullptr;
+    st = check_cuda(nullptr, cudaMalloc(reinterpret_cast<void **>(&count), 256), "cudaMalloc");
+    if (st == TR_OK) st = check_cuda(nullptr, cudaMemset(count, 0, 256), "cudaMemset");
+    int *err = reinterpret_cast<int *>(count + 32);
+    if (st == TR_OK)
+        st = check_cuda(nullptr, launch_barrier_selftest(sms, count, err, skip_block, rounds, max_polls, 0),
+                        "barrier self-test launch");
+    if (st == TR_OK) st = check_cuda(nullptr, cudaDeviceSynchronize(), "barrier self-test");
+    int h = 0;
+    if (st == TR_OK) st = check_cuda(nullptr, cudaMemcpy(&h, err, sizeof(int), cudaMemcpyDeviceToHost), "copy");
+    if (count) cudaFree(count);
+    cudaSetDevice(prev);
+    *timed_out = h;
+    return st;
+}
+
 // --------------------------------------------------------------- moments
 tr_status tr_compute_moments(tr_ctx *c, const double *f, double *U, double *T) {
     CHECK_CTX(c);

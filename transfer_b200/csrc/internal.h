@@ -274,6 +274,9 @@ cudaError_t launch_cg_persistent(const tr_ctx *c, const DeviceOp<T> &op, const P
                                  int *grid_out);
 template <typename T>
 cudaError_t launch_sr_persistent(const tr_ctx *c, const DeviceOp<T> &op, const SrArgs<T> &a, cudaStream_t s);
+// bounded grid barrier self-test (operator.cu)
+cudaError_t launch_barrier_selftest(int blocks, unsigned int *count, int *err, int skip, int rounds,
+                                    unsigned int max_polls, cudaStream_t s);
 cudaError_t operator_init_attributes();
 template <typename T>
 cudaError_t launch_lhs_diag(const tr_ctx *c, const DeviceOp<T> &op, const T *f, T *r, const int32_t *done,

@@ -1012,7 +1012,8 @@ __global__ void __launch_bounds__(kBlock) k_lhs_diag(const OpData<T> d, const T 
 // load.  Gives up after kBarrierPolls polls, or as soon as another block
 // has given up: sets *err and returns false.
 constexpr unsigned int kBarrierPolls = 1u << 24;
-__device__ __forceinline__ bool grid_barrier(unsigned int *count, int *err, unsigned int &target) {
+__device__ __forceinline__ bool grid_barrier(unsigned int *count, int *err, unsigned int &target,
+                                             unsigned int max_polls = kBarrierPolls) {
     __shared__ int ok;
     __syncthreads();
     target += gridDim.x;
@@ -1022,7 +1023,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned int *count, int *err, unsi
         atomicAdd(count, 1u);
         unsigned int polls = 0;
         while (*reinterpret_cast<volatile unsigned int *>(count) < target) {
-            if (++polls > kBarrierPolls || *reinterpret_cast<volatile int *>(err)) {
+            if (++polls > max_polls || *reinterpret_cast<volatile int *>(err)) {
                 atomicExch(err, 1);
                 ok = 0;
                 break;
@@ -1033,6 +1034,21 @@ __device__ __forceinline__ bool grid_barrier(unsigned int *count, int *err, unsi
     }
     __syncthreads();
     return ok != 0;
+}
+
+// Self-test of the bounded barrier: `rounds` barriers over the grid; block
+// `skip` (if >= 0) never arrives, so the others must give up after
+// max_polls polls and report through *err instead of waiting forever.
+__global__ void k_barrier_selftest(unsigned int *count, int *err, int skip, int rounds, unsigned int max_polls) {
+    unsigned int target = 0;
+    if (static_cast<int>(blockIdx.x) == skip) return;
+    for (int i = 0; i < rounds; ++i)
+        if (!grid_barrier(count, err, target, max_polls)) return;
+}
+cudaError_t launch_barrier_selftest(int blocks, unsigned int *count, int *err, int skip, int rounds,
+                                    unsigned int max_polls, cudaStream_t s) {
+    void *args[] = {&count, &err, &skip, &rounds, &max_polls};
+    return cudaLaunchCooperativeKernel(reinterpret_cast<void *>(k_barrier_selftest), blocks, 128, args, 0, s);
 }
 
 // Totals of per-block partials [NV][gridDim.x], summed by every block in the
