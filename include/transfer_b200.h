@@ -312,6 +312,103 @@ tr_status tr_eig_lanczos(tr_ctx *ctx, double *v, double *v0, double *w,
  * b[0..n-2]) by Newton on the characteristic polynomial (trieig). */
 double tr_trieig(const double *a, const double *b, int n);
 
+/* ---- discrete-ordinates sweep (no counterpart in the reference) --------
+ *
+ * The reference solves only the even-parity spherical-harmonics system
+ * above.  This is the upwind transport sweep over the SAME problem data: the
+ * `tetrahedron` records (outward face area normals s, kappa_volume = sigma_t
+ * V, I_p = Planck intensity B) and boundary `face` records of tr_mesh_view,
+ * with tr_physics_view's kappa_abs_volume (sigma_a V; sigma_s = sigma_t -
+ * sigma_a scatters isotropically), face_bc and face_incident.  Angles are an
+ * ordinate set (directions + weights summing to 1).
+ *
+ * Discretisation: linear discontinuous finite elements on each tetrahedron
+ * (values at its 4 vertices), upwind between cells.  The unknowns of the
+ * outer iteration are the scalar flux J[nT][4] (mean intensity at each
+ * cell's vertices, J = sum_q w_q psi_q) and the extra vector B[n_extra]:
+ * the inflow through reflective faces ([n_reflective][nq][4]) and through
+ * faces where a dependency cycle was cut ([n_lag][4]).  All vectors are
+ * FP64 DEVICE pointers. */
+typedef struct tr_sweep tr_sweep;
+typedef struct tr_ordinates_view {
+    uint32_t nq;
+    const double *x, *y, *z;   /* unit directions       */
+    const double *w;           /* weights, sum 1         */
+} tr_ordinates_view;
+typedef struct tr_sweep_info {
+    uint32_t nT, nF, nq;
+    uint64_t n_extra;          /* length of B                              */
+    uint32_t n_reflective;     /* reflective boundary faces                */
+    uint32_t n_lag;            /* faces lagged to break dependency cycles  */
+    uint32_t max_levels;       /* longest per-ordinate dependency chain    */
+    uint32_t forced_levels;    /* levels started by cutting a cycle        */
+    uint64_t device_bytes;
+    int device;
+} tr_sweep_info;
+enum { TR_SWEEP_GMRES = 0, TR_SWEEP_SOURCE_ITERATION = 1 };
+typedef struct tr_sweep_opts {
+    int32_t method;            /* TR_SWEEP_*                                */
+    int32_t mode;              /* TR_MODE_FP64, or TR_MODE_MIXED: FP32
+                                  sweeps inside FP64 defect correction      */
+    double  tol;               /* GMRES: ||b - (I - T) x|| / ||b||;
+                                  source iteration: relative change        */
+    int32_t max_iter;          /* sweeps of the iteration (Krylov steps)   */
+    int32_t restart;           /* GMRES restart length, 1..64              */
+    double  inner_tol;         /* mixed: FP32 solve reduction (0: adaptive)*/
+    int32_t max_outer;         /* mixed: defect-correction steps           */
+} tr_sweep_opts;
+typedef struct tr_sweep_report {
+    int32_t converged;
+    int32_t iterations;        /* Krylov steps (or source iterations)      */
+    int32_t outer_steps;       /* mixed mode defect-correction steps       */
+    int64_t sweeps_f32, sweeps_f64;
+    double  residual;          /* final relative residual, FP64            */
+    double  rhs_norm;
+    double  device_ms;
+    int64_t kernel_launches;
+} tr_sweep_report;
+
+/* Gauss-Legendre (n_polar in cos theta) x uniform azimuth (n_azim, at
+ * (k + 1/2) 2 pi / n_azim) ordinates, n_polar * n_azim points, weights
+ * summing to 1; mirror-symmetric in x, y, z for even n_azim. */
+tr_status tr_ordinates_product(int n_polar, int n_azim, double *x, double *y, double *z, double *w);
+/* Builds the device geometry (face adjacency, consistent face normals) and
+ * the per-ordinate dependency levels (on the device). */
+tr_status tr_sweep_create(int device, const tr_mesh_view *mesh, const tr_physics_view *phys,
+                          const tr_ordinates_view *ord, tr_sweep **out);
+tr_status tr_sweep_destroy(tr_sweep *s);
+const char *tr_sweep_last_error(const tr_sweep *s);
+tr_status tr_sweep_info_get(const tr_sweep *s, tr_sweep_info *info);
+/* level[q * nT + c]: dependency level of cell c in ordinate q (host array). */
+tr_status tr_sweep_levels(tr_sweep *s, int32_t *level);
+/* One sweep of all ordinates in FP32 (precision 32) or FP64 (64) from the
+ * scattering source of J_in and the inflow B_in (NULL = 0); with_ext adds
+ * emission and the incident boundary inflow.  J_out: scalar flux of the
+ * result; B_out: the resulting reflective / lagged inflow (either NULL). */
+tr_status tr_sweep_apply(tr_sweep *s, int precision, const double *J_in, const double *B_in, int with_ext,
+                         double *J_out, double *B_out);
+/* psi of the last sweep as FP64, device [nq][nT][4]. */
+tr_status tr_sweep_psi(tr_sweep *s, double *psi);
+/* Angular moments of the last sweep's psi: mom[m][nT][4] = sum_q w_q
+ * Y_m(Omega_q) psi_q for m < nmom <= 16 (l <= 3, m index l^2 + l + mm,
+ * real harmonics of tr_spherical_value, Y_00 = 1). */
+tr_status tr_sweep_moments(tr_sweep *s, int nmom, double *mom);
+/* FP64 energy balance of the last sweep given its inputs J_in, B_in and its
+ * scalar flux J_out:  out = {emitted, absorbed, escaped, incoming,
+ * reflective_net} with emitted + incoming = absorbed + escaped +
+ * reflective_net (absorbed = sigma_t V mean J_out - sigma_s V mean J_in; at
+ * convergence sigma_a V mean J).  Units: mean intensity x area. */
+tr_status tr_sweep_balance(tr_sweep *s, const double *J_in, const double *B_in, const double *J_out,
+                           double out[5]);
+void tr_sweep_opts_default(tr_sweep_opts *opts);
+/* Solves J = S(J, B) (scattering source iteration fixed point) by GMRES on
+ * (I - T) x = S(0) or by source iteration; J [nT][4], B [n_extra] device
+ * outputs (B may be NULL). */
+tr_status tr_sweep_solve(tr_sweep *s, const tr_sweep_opts *opts, double *J, double *B, tr_sweep_report *rep);
+/* Measurement helper: mean device time of one sweep with sources (3
+ * untimed sweeps first). */
+tr_status tr_sweep_bench(tr_sweep *s, int precision, int iters, double *ms_per_sweep);
+
 /* ---- host problem data (C++ host code behind the C ABI) ---------------- */
 /* AngularData(maxk) (AngularData.cpp:9-67): tables for the even harmonics
  * l = 0,2,..,2maxk; slm = (1+maxk)(1+2maxk). */

@@ -61,6 +61,15 @@ def _load():
         "oracle_trieig": (D, [P, P, U32]),
         "oracle_eigest": (D, [P, P, P, C.c_int, P, P]),
         "oracle_expint_en": (D, [C.c_int, D]),
+        "oracle_sweep_create": (P, [P, U32, P, P, P, P, P]),
+        "oracle_sweep_destroy": (None, [P]),
+        "oracle_sweep_info": (None, [P, P]),
+        "oracle_sweep_levels": (None, [P, P]),
+        "oracle_sweep_apply": (None, [P, P, P, C.c_int, P, P, P]),
+        "oracle_sweep_solve": (C.c_int, [P, C.c_int, D, C.c_int, C.c_int, P, P, P, P]),
+        "oracle_sweep_balance": (None, [P, P, P, P, P]),
+        "oracle_sweep_moments": (None, [P, P, C.c_int, P]),
+        "oracle_ordinates_product": (None, [C.c_int, C.c_int, P, P, P, P]),
         "oracle_num_threads": (C.c_int, []),
         "oracle_set_num_threads": (None, [C.c_int]),
     }
@@ -194,3 +203,79 @@ def trieig(a, b):
     a = np.ascontiguousarray(a, dtype=np.float64)
     b = np.ascontiguousarray(b, dtype=np.float64)
     return lib.oracle_trieig(_p(a), _p(b), len(a))
+
+
+class or_sweep_mesh(C.Structure):
+    _fields_ = [("nT", C.c_uint32), ("nF", C.c_uint32), ("mesh", C.c_void_p), ("bnd", C.c_void_p),
+                ("kappa_abs_volume", C.c_void_p), ("face_bc", C.c_void_p), ("face_incident", C.c_void_p)]
+
+
+def ordinates_product(n_polar, n_azim):
+    """Gauss-Legendre (mu) x uniform azimuth ordinates; returns (x, y, z, w)."""
+    n = n_polar * n_azim
+    x, y, z, w = (np.zeros(n) for _ in range(4))
+    lib.oracle_ordinates_product(n_polar, n_azim, _p(x), _p(y), _p(z), _p(w))
+    return x, y, z, w
+
+
+class SweepOracle:
+    """FP64 CPU restatement of the linear-discontinuous discrete-ordinates
+    sweep (oracle/sweep_oracle.h) bound to a MeshData and an ordinate set."""
+
+    def __init__(self, md, ordinates, kappa_abs_volume=None, face_bc=None, face_incident=None):
+        self.md = md
+        self.ox, self.oy, self.oz, self.w = (np.ascontiguousarray(a, dtype=np.float64) for a in ordinates)
+        self.nq, self.nT = len(self.w), int(md.nT)
+        self.kav = None if kappa_abs_volume is None else np.ascontiguousarray(kappa_abs_volume, dtype=np.float64)
+        self.fbc = None if face_bc is None else np.ascontiguousarray(face_bc, dtype=np.int32)
+        self.finc = None if face_incident is None else np.ascontiguousarray(face_incident, dtype=np.float64)
+        m = or_sweep_mesh(md.nT, md.nF, _p(md.mesh), _p(md.bnd) if md.nF else None, _p(self.kav), _p(self.fbc),
+                          _p(self.finc))
+        err = C.c_char_p()
+        self.h = lib.oracle_sweep_create(C.byref(m), self.nq, _p(self.ox), _p(self.oy), _p(self.oz), _p(self.w),
+                                         C.byref(err))
+        if not self.h:
+            raise ValueError(err.value.decode())
+        info = np.zeros(6, dtype=np.int64)
+        lib.oracle_sweep_info(self.h, _p(info))
+        self.nB, self.n_reflective, self.n_lag, self.max_levels, self.forced, self.n_interior = (int(v) for v in info)
+
+    def levels(self):
+        lv = np.zeros(self.nq * self.nT, dtype=np.int32)
+        lib.oracle_sweep_levels(self.h, _p(lv))
+        return lv.reshape(self.nq, self.nT)
+
+    def apply(self, J=None, B=None, with_ext=1, want_psi=False):
+        Jo, Bo = np.zeros(4 * self.nT), np.zeros(max(self.nB, 1))
+        psi = np.zeros(4 * self.nq * self.nT) if want_psi else None
+        Ji = None if J is None else np.ascontiguousarray(J, dtype=np.float64).reshape(-1)
+        Bi = None if B is None else np.ascontiguousarray(B, dtype=np.float64).reshape(-1)
+        lib.oracle_sweep_apply(self.h, _p(Ji), _p(Bi), int(with_ext), _p(Jo), _p(Bo), _p(psi))
+        out = (Jo.reshape(self.nT, 4), Bo[:self.nB])
+        return out + ((psi.reshape(self.nq, self.nT, 4),) if want_psi else ())
+
+    def solve(self, method=1, tol=1e-10, max_iter=500, restart=30):
+        J, B = np.zeros(4 * self.nT), np.zeros(max(self.nB, 1))
+        it, res = C.c_int(), C.c_double()
+        rc = lib.oracle_sweep_solve(self.h, int(method), float(tol), int(max_iter), int(restart), _p(J), _p(B),
+                                    C.byref(it), C.byref(res))
+        return J.reshape(self.nT, 4), B[:self.nB], dict(converged=rc == 0, iterations=it.value, residual=res.value)
+
+    def balance(self, J_in, B_in, psi):
+        out = np.zeros(5)
+        Ji = None if J_in is None else np.ascontiguousarray(J_in, dtype=np.float64).reshape(-1)
+        Bi = None if B_in is None else np.ascontiguousarray(B_in, dtype=np.float64).reshape(-1)
+        lib.oracle_sweep_balance(self.h, _p(Ji), _p(Bi), _p(np.ascontiguousarray(psi, dtype=np.float64).reshape(-1)),
+                                 _p(out))
+        return dict(emitted=out[0], absorbed=out[1], escaped=out[2], incoming=out[3], reflective_net=out[4])
+
+    def moments(self, psi, nmom=16):
+        mom = np.zeros(nmom * 4 * self.nT)
+        lib.oracle_sweep_moments(self.h, _p(np.ascontiguousarray(psi, dtype=np.float64).reshape(-1)), int(nmom),
+                                 _p(mom))
+        return mom.reshape(nmom, self.nT, 4)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib.oracle_sweep_destroy(self.h)
+            self.h = None

@@ -32,6 +32,7 @@ TR_PREC_NONE, TR_PREC_REFERENCE, TR_PREC_JACOBI = 0, 1, 2
 TR_MODE_FP64, TR_MODE_MIXED = 0, 1
 TR_ENGINE_PERSISTENT, TR_ENGINE_GRAPH, TR_ENGINE_LAUNCH, TR_ENGINE_PERSISTENT_SR = 0, 1, 2, 3
 TR_OPERATOR_SIMT, TR_OPERATOR_TENSOR = 0, 1
+TR_SWEEP_GMRES, TR_SWEEP_SOURCE_ITERATION = 0, 1
 
 
 class tr_tetrahedron(C.Structure):
@@ -91,6 +92,27 @@ class tr_kuhn_params(C.Structure):
     _fields_ = [("n", C.c_int32 * 3), ("box", C.c_double * 6), ("jitter", C.c_double),
                 ("seed", C.c_uint64), ("region_kind", C.c_int32), ("region_arg", C.c_double * 4),
                 ("ball", C.c_int32), ("ball_center", C.c_double * 3), ("ball_radius", C.c_double)]
+
+
+class tr_ordinates_view(C.Structure):
+    _fields_ = [("nq", C.c_uint32), ("x", C.c_void_p), ("y", C.c_void_p), ("z", C.c_void_p), ("w", C.c_void_p)]
+
+
+class tr_sweep_info(C.Structure):
+    _fields_ = [("nT", C.c_uint32), ("nF", C.c_uint32), ("nq", C.c_uint32), ("n_extra", C.c_uint64),
+                ("n_reflective", C.c_uint32), ("n_lag", C.c_uint32), ("max_levels", C.c_uint32),
+                ("forced_levels", C.c_uint32), ("device_bytes", C.c_uint64), ("device", C.c_int)]
+
+
+class tr_sweep_opts(C.Structure):
+    _fields_ = [("method", C.c_int32), ("mode", C.c_int32), ("tol", C.c_double), ("max_iter", C.c_int32),
+                ("restart", C.c_int32), ("inner_tol", C.c_double), ("max_outer", C.c_int32)]
+
+
+class tr_sweep_report(C.Structure):
+    _fields_ = [("converged", C.c_int32), ("iterations", C.c_int32), ("outer_steps", C.c_int32),
+                ("sweeps_f32", C.c_int64), ("sweeps_f64", C.c_int64), ("residual", C.c_double),
+                ("rhs_norm", C.c_double), ("device_ms", C.c_double), ("kernel_launches", C.c_int64)]
 
 
 P = C.c_void_p
@@ -154,6 +176,20 @@ PROTOTYPES = [
     ("tr_meshdata_kappa_abs_volume", P, [P]),
     ("tr_meshdata_face_side", P, [P]),
     ("tr_meshdata_destroy", None, [P]),
+    ("tr_ordinates_product", S, [I, I, P, P, P, P]),
+    ("tr_sweep_create", S, [I, C.POINTER(tr_mesh_view), C.POINTER(tr_physics_view), C.POINTER(tr_ordinates_view),
+                            C.POINTER(P)]),
+    ("tr_sweep_destroy", S, [P]),
+    ("tr_sweep_last_error", C.c_char_p, [P]),
+    ("tr_sweep_info_get", S, [P, C.POINTER(tr_sweep_info)]),
+    ("tr_sweep_levels", S, [P, P]),
+    ("tr_sweep_apply", S, [P, I, P, P, I, P, P]),
+    ("tr_sweep_psi", S, [P, P]),
+    ("tr_sweep_moments", S, [P, I, P]),
+    ("tr_sweep_balance", S, [P, P, P, P, P]),
+    ("tr_sweep_opts_default", None, [C.POINTER(tr_sweep_opts)]),
+    ("tr_sweep_solve", S, [P, C.POINTER(tr_sweep_opts), P, P, C.POINTER(tr_sweep_report)]),
+    ("tr_sweep_bench", S, [P, I, I, C.POINTER(D)]),
 ]
 
 

@@ -1,0 +1,1695 @@
+// Discrete-ordinates transport sweep on the reference's tetrahedral problem
+// data (no counterpart in the reference, whose solver is the even-parity
+// spherical-harmonics operator of kernels.cu).  The sweep reads the same
+// `tetrahedron` records (MeshData.cpp:56-76: outward face area normals s,
+// kappa_volume = sigma_t V, I_p = B) and boundary `face` records.
+//
+// Discretisation: linear discontinuous finite elements per tetrahedron and
+// ordinate, upwind coupling across faces; per (cell, ordinate) the 4x4
+// system
+//   L_ij  = a_j/12 + sigma_t V (1+d_ij)/20 + (1+d_ij)/12 sum_{k in, k!=i,j} a_k
+//   rhs_i = sigma_s V/20 (J_i + sum_j J_j) + sigma_a V B/4
+//           + sum_{k in, k!=i} a_k/12 (T_k + psi_up_{k,i}),
+// a_k = -Omega.s_k (> 0 on inflow faces), T_k the sum of the three upwind
+// traces on face k, solved by Gaussian elimination without pivoting (the
+// symmetric part of L is positive definite).  J = sum_q w_q psi_q.
+//
+// Device layout (one GPU; SoA, cell-major):
+//   s [nT][12] (face normals; a shared face stores exactly negated normals,
+//   so both sides agree on which one is upwind), sigma_t V, sigma_s V,
+//   sigma_a V B / 4 [nT], neighbours nbr [nT][4] (>= 0 cell, < 0 boundary
+//   face -(f+1)), vertex maps across faces packed 2 bits per (face, vertex).
+//   psi [nq][nT][4] (FP32 or FP64), task records [nq][nT] (uint4, below).
+//
+// Schedule, built once on the device (k_sched_build, one block per
+// ordinate): Kahn levels over the upwind graph; when a level comes out
+// empty while cells remain, the smallest unscheduled cell forms a level of
+// its own and its inflow from unscheduled cells is lagged (read from the
+// extra-unknown vector B, which the Krylov solver carries).
+//   task[q][p] = { cell | inflow_mask << 28, up[3] } in level order, up[i]
+//   the source of the i-th inflow face (ascending local face index): the
+//   upstream cell's position p' in this ordinate's order, kLagBit | slot,
+//   or kNone for a boundary face.
+//
+// Sweep (k_sweep, one block per ordinate): levels in order, a block
+// barrier between levels; each cell's solution goes to psi and to a
+// shared-memory ring indexed by position, from which downstream cells of
+// the next levels read their upwind traces (global psi for older ones).
+// Blocks never wait on one another, so a sweep has no inter-block waits.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/transfer_b200.h"
+#include "reduce.cuh"
+
+namespace transfer {
+tr_status set_global_error(tr_status st, const std::string &msg);
+}
+
+namespace transfer {
+namespace sweep {
+
+constexpr uint32_t kNone = 0xFFFFFFFFu;
+constexpr uint32_t kLagBit = 0x80000000u;
+constexpr uint32_t kCellMask = 0x0FFFFFFFu;
+constexpr int kSchedThreads = 1024;
+constexpr int kSweepThreads = 256;
+constexpr int kRingBytes = 64 * 1024;
+constexpr int kRedGrid = 296;            // 2 x 148 SMs
+constexpr uint32_t kMaxLag = 1u << 22;   // lagged (cycle-breaking) faces over all ordinates
+constexpr int kMaxRestart = 64;
+constexpr int kMaxMoments = 16;
+
+template <typename T>
+struct Vec4;
+template <>
+struct Vec4<float> {
+    using type = float4;
+};
+template <>
+struct Vec4<double> {
+    using type = double4;
+};
+
+template <typename T>
+__device__ __forceinline__ T comp(const typename Vec4<T>::type &v, uint32_t i) {
+    return i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w;
+}
+
+template <typename T>
+struct Geom {
+    const T *s;          // [nT][12]
+    const T *stv;        // sigma_t V
+    const T *ssv;        // sigma_s V
+    const T *ext;        // sigma_a V B / 4
+    const int32_t *nbr;  // [nT][4]
+    const uint32_t *map; // [nT]
+    const int32_t *fbc;  // [nF]
+    const T *finc;       // [nF]
+    const int32_t *rslot;// [nF]
+    const uint32_t *rinv;// [nrefl][nq] incoming ordinate mirrored onto q, or kNone
+};
+
+struct Sched {
+    const uint4 *task;     // [nq][nT]
+    const uint32_t *lvl;   // [nq][lstride]
+    const uint32_t *nlev;  // [nq]
+    uint32_t lstride;
+};
+
+template <typename T>
+struct SweepArgs {
+    uint32_t nT, nq;
+    const T *ox, *oy, *oz;
+    const T *J;        // [nT][4] or null (zero)
+    const T *Bin;      // extra unknowns or null (zero)
+    T *Bout;           // reflective outflow (mirrored), or null
+    T *psi;            // [nq][nT][4]
+    int with_ext;
+    uint64_t lag_base; // offset of the lag slots in B
+};
+
+// ---- schedule -------------------------------------------------------------
+struct SchedBuild {
+    uint32_t nT, nq;
+    const double *s;
+    const int32_t *nbr;
+    const double *ox, *oy, *oz;
+    int32_t *indeg;     // [nq][nT]
+    uint32_t *order;    // [nq][nT]
+    uint32_t *pos;      // [nq][nT]
+    uint8_t *mask;      // [nq][nT] inflow faces
+    uint8_t *lagm;      // [nq][nT] lagged faces
+    uint32_t *lvl;      // [nq][nT + 1]
+    uint32_t *nlev;     // [nq]
+    uint32_t *nforced;  // [nq]
+};
+
+// Omega . s without contraction, in the order ((x + y) + z): the sign
+// decisions must be those of the FP64 oracle and antisymmetric across a face.
+__device__ __forceinline__ double odot_rn(double ox, double oy, double oz, const double *s) {
+    return __dadd_rn(__dadd_rn(__dmul_rn(ox, s[0]), __dmul_rn(oy, s[1])), __dmul_rn(oz, s[2]));
+}
+
+__global__ void __launch_bounds__(kSchedThreads) k_sched_build(SchedBuild b) {
+    __shared__ uint32_t s_n, s_min;
+    const uint32_t q = blockIdx.x, nT = b.nT;
+    const double ox = b.ox[q], oy = b.oy[q], oz = b.oz[q];
+    int32_t *indeg = b.indeg + (size_t)q * nT;
+    uint32_t *order = b.order + (size_t)q * nT, *pos = b.pos + (size_t)q * nT, *lvl = b.lvl + (size_t)q * (nT + 1);
+    uint8_t *mask = b.mask + (size_t)q * nT, *lagm = b.lagm + (size_t)q * nT;
+    for (uint32_t c = threadIdx.x; c < nT; c += blockDim.x) {
+        uint32_t m = 0;
+        int d = 0;
+        for (int k = 0; k < 4; ++k) {
+            double dd = odot_rn(ox, oy, oz, b.s + 12 * (size_t)c + 3 * k);
+            if (dd < 0.0) {
+                m |= 1u << k;
+                if (b.nbr[4 * (size_t)c + k] >= 0) ++d;
+            }
+        }
+        mask[c] = static_cast<uint8_t>(m);
+        lagm[c] = 0;
+        indeg[c] = d;
+        pos[c] = kNone;
+    }
+    if (threadIdx.x == 0) s_n = 0;
+    __syncthreads();
+    for (uint32_t c = threadIdx.x; c < nT; c += blockDim.x)
+        if (indeg[c] == 0) {
+            uint32_t p = atomicAdd(&s_n, 1u);
+            order[p] = c;
+            pos[c] = p;
+        }
+    uint32_t head = 0, minrem = 0, forced = 0;
+    for (uint32_t L = 0;; ++L) {
+        __syncthreads();
+        uint32_t n = s_n;
+        __syncthreads();
+        if (head == n) {
+            if (n == nT) {
+                if (threadIdx.x == 0) {
+                    lvl[L] = nT;
+                    b.nlev[q] = L;
+                    b.nforced[q] = forced;
+                }
+                return;
+            }
+            // stalled on a cycle: the smallest unscheduled cell forms a level
+            if (threadIdx.x == 0) s_min = nT;
+            __syncthreads();
+            for (uint32_t c = minrem + threadIdx.x; c < nT; c += blockDim.x)
+                if (pos[c] == kNone) {
+                    atomicMin(&s_min, c);
+                    break;
+                }
+            __syncthreads();
+            const uint32_t c = s_min;
+            minrem = c;
+            ++forced;
+            if (threadIdx.x == 0) {
+                uint32_t lg = 0;
+                for (int k = 0; k < 4; ++k) {
+                    int32_t u = b.nbr[4 * (size_t)c + k];
+                    if (u >= 0 && (mask[c] >> k & 1u) && pos[u] == kNone) lg |= 1u << k;
+                }
+                lagm[c] = static_cast<uint8_t>(lg);
+                indeg[c] = -(1 << 20);
+                order[n] = c;
+                pos[c] = n;
+                s_n = n + 1;
+            }
+            __syncthreads();
+            n = n + 1;
+        }
+        if (threadIdx.x == 0) lvl[L] = head;
+        for (uint32_t i = head + threadIdx.x; i < n; i += blockDim.x) {
+            const uint32_t c = order[i];
+            for (int k = 0; k < 4; ++k) {
+                const int32_t d = b.nbr[4 * (size_t)c + k];
+                if (d < 0) continue;
+                if (!(odot_rn(ox, oy, oz, b.s + 12 * (size_t)c + 3 * k) > 0.0)) continue;
+                if (atomicSub(&indeg[d], 1) == 1) {
+                    uint32_t p = atomicAdd(&s_n, 1u);
+                    order[p] = static_cast<uint32_t>(d);
+                    pos[d] = p;
+                }
+            }
+        }
+        head = n;
+    }
+}
+
+// lagged faces -> list of keys ((q * nT + c) * 4 + k)
+__global__ void k_lag_collect(uint32_t nT, uint32_t nq, const uint8_t *lagm, unsigned long long *keys,
+                              unsigned int *count) {
+    const uint64_t n = (uint64_t)nT * nq;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t m = lagm[i];
+        for (int k = 0; k < 4; ++k)
+            if (m >> k & 1u) {
+                unsigned int slot = atomicAdd(count, 1u);
+                if (slot < kMaxLag) keys[slot] = i * 4 + k;
+            }
+    }
+}
+
+__global__ void k_records(uint32_t nT, uint32_t nq, const uint32_t *order, const uint32_t *pos, const uint8_t *mask,
+                          const uint8_t *lagm, const int32_t *nbr, const unsigned long long *lag_keys, uint32_t nlag,
+                          uint4 *task) {
+    const uint64_t n = (uint64_t)nT * nq;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t q = static_cast<uint32_t>(i / nT);
+        const uint32_t c = order[i];
+        const uint64_t qc = (uint64_t)q * nT + c;
+        const uint32_t m = mask[qc], lg = lagm[qc];
+        uint32_t up[3] = {0u, 0u, 0u};
+        int t = 0;
+        for (int k = 0; k < 4; ++k) {
+            if (!(m >> k & 1u)) continue;
+            const int32_t nb = nbr[4 * (size_t)c + k];
+            uint32_t code;
+            if (nb < 0) {
+                code = kNone;
+            } else if (lg >> k & 1u) {
+                const unsigned long long key = qc * 4 + k;
+                uint32_t lo = 0, hi = nlag;  // lag keys sorted ascending
+                while (lo < hi) {
+                    uint32_t mid = (lo + hi) >> 1;
+                    if (lag_keys[mid] < key) lo = mid + 1;
+                    else hi = mid;
+                }
+                code = kLagBit | lo;
+            } else {
+                code = pos[(size_t)q * nT + nb];
+            }
+            if (t < 3) up[t] = code;
+            ++t;
+        }
+        task[i] = make_uint4(c | (m << 28), up[0], up[1], up[2]);
+    }
+}
+
+// ---- the sweep --------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ void load_s(const T *s, T (&v)[12]);
+template <>
+__device__ __forceinline__ void load_s<float>(const float *s, float (&v)[12]) {
+    const float4 *p = reinterpret_cast<const float4 *>(s);
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        float4 t = __ldg(p + i);
+        v[4 * i] = t.x;
+        v[4 * i + 1] = t.y;
+        v[4 * i + 2] = t.z;
+        v[4 * i + 3] = t.w;
+    }
+}
+template <>
+__device__ __forceinline__ void load_s<double>(const double *s, double (&v)[12]) {
+    const double2 *p = reinterpret_cast<const double2 *>(s);
+#pragma unroll
+    for (int i = 0; i < 6; ++i) {
+        double2 t = __ldg(p + i);
+        v[2 * i] = t.x;
+        v[2 * i + 1] = t.y;
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ typename Vec4<T>::type load_v4(const T *p);
+template <>
+__device__ __forceinline__ float4 load_v4<float>(const float *p) {
+    return *reinterpret_cast<const float4 *>(p);
+}
+template <>
+__device__ __forceinline__ double4 load_v4<double>(const double *p) {
+    const double2 *q = reinterpret_cast<const double2 *>(p);
+    double2 a = q[0], b = q[1];
+    return make_double4(a.x, a.y, b.x, b.y);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, SweepArgs<T> a) {
+    using V = typename Vec4<T>::type;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    V *ring = reinterpret_cast<V *>(smem_raw);
+    constexpr uint32_t R = kRingBytes / sizeof(V);
+    const uint32_t q = blockIdx.x, nT = a.nT, nq = a.nq;
+    const T ox = a.ox[q], oy = a.oy[q], oz = a.oz[q];
+    const uint4 *task = sc.task + (size_t)q * nT;
+    const uint32_t *lvl = sc.lvl + (size_t)q * sc.lstride;
+    const uint32_t nl = sc.nlev[q];
+    T *psi = a.psi + (size_t)q * nT * 4;
+    const T c12 = T(1) / T(12), c20 = T(1) / T(20);
+    for (uint32_t L = 0; L < nl; ++L) {
+        const uint32_t s0 = lvl[L], e0 = lvl[L + 1];
+        for (uint32_t p = s0 + threadIdx.x; p < e0; p += blockDim.x) {
+            const uint4 rec = __ldg(task + p);
+            const uint32_t c = rec.x & kCellMask, mask = rec.x >> 28;
+            T sv[12];
+            load_s<T>(g.s + 12 * (size_t)c, sv);
+            T av[4], al[4], Ain = T(0);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                av[k] = -(ox * sv[3 * k] + oy * sv[3 * k + 1] + oz * sv[3 * k + 2]);
+                al[k] = (mask >> k & 1u) ? av[k] : T(0);
+                Ain += al[k];
+            }
+            const T stv = __ldg(g.stv + c), ssv = __ldg(g.ssv + c);
+            const T ext = a.with_ext ? __ldg(g.ext + c) : T(0);
+            T Jc[4] = {T(0), T(0), T(0), T(0)};
+            if (a.J) {
+                V j4 = load_v4<T>(a.J + 4 * (size_t)c);
+                Jc[0] = j4.x;
+                Jc[1] = j4.y;
+                Jc[2] = j4.z;
+                Jc[3] = j4.w;
+            }
+            const T Js = Jc[0] + Jc[1] + Jc[2] + Jc[3];
+            T Lm[4][4], r[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const T face = (i == j) ? T(2) * (Ain - al[i]) : (Ain - al[i] - al[j]);
+                    Lm[i][j] = av[j] * c12 + stv * (i == j ? T(2) : T(1)) * c20 + face * c12;
+                }
+                r[i] = ssv * c20 * (Jc[i] + Js) + ext;
+            }
+            const uint32_t mp = __ldg(g.map + c);
+            uint32_t ups[3] = {rec.y, rec.z, rec.w};
+            int t = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (!(mask >> k & 1u)) continue;
+                const uint32_t code = ups[t < 3 ? t : 2];
+                ++t;
+                T up[4] = {T(0), T(0), T(0), T(0)};
+                if (code == kNone) {
+                    const int32_t f = -__ldg(g.nbr + 4 * (size_t)c + k) - 1;
+                    const int32_t bc = __ldg(g.fbc + f);
+                    if (bc == TR_BC_REFLECTIVE) {
+                        if (a.Bin) {
+                            const T *bp = a.Bin + ((size_t)__ldg(g.rslot + f) * nq + q) * 4;
+#pragma unroll
+                            for (int j = 0; j < 4; ++j) up[j] = bp[j];
+                        }
+                    } else if (bc == TR_BC_INCIDENT && a.with_ext) {
+                        const T v = __ldg(g.finc + f);
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) up[j] = v;
+                    }
+                } else if (code & kLagBit) {
+                    if (a.Bin) {
+                        const T *bp = a.Bin + a.lag_base + 4 * (size_t)(code & ~kLagBit);
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) up[j] = bp[j];
+                    }
+                } else {
+                    V v;
+                    if (code + R >= e0) {
+                        v = ring[code % R];
+                    } else {
+                        const int32_t nb = __ldg(g.nbr + 4 * (size_t)c + k);
+                        v = load_v4<T>(psi + 4 * (size_t)nb);
+                    }
+#pragma unroll
+                    for (int j = 0; j < 4; ++j) up[j] = comp<T>(v, (mp >> (2 * (4 * k + j))) & 3u);
+                }
+                up[k] = T(0);
+                const T Tk = up[0] + up[1] + up[2] + up[3];
+                const T ak = av[k] * c12;
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+                    if (i != k) r[i] += ak * (Tk + up[i]);
+            }
+            // Gaussian elimination without pivoting
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const T inv = T(1) / Lm[k][k];
+#pragma unroll
+                for (int i = k + 1; i < 4; ++i) {
+                    const T f = Lm[i][k] * inv;
+#pragma unroll
+                    for (int j = k + 1; j < 4; ++j) Lm[i][j] -= f * Lm[k][j];
+                    r[i] -= f * r[k];
+                }
+            }
+            T o[4];
+#pragma unroll
+            for (int i = 3; i >= 0; --i) {
+                T v = r[i];
+#pragma unroll
+                for (int j = i + 1; j < 4; ++j) v -= Lm[i][j] * o[j];
+                o[i] = v / Lm[i][i];
+            }
+            V out;
+            out.x = o[0];
+            out.y = o[1];
+            out.z = o[2];
+            out.w = o[3];
+            if constexpr (sizeof(T) == 4) {
+                *reinterpret_cast<float4 *>(psi + 4 * (size_t)c) = out;
+            } else {
+                double2 *dst = reinterpret_cast<double2 *>(psi + 4 * (size_t)c);
+                dst[0] = make_double2(o[0], o[1]);
+                dst[1] = make_double2(o[2], o[3]);
+            }
+            ring[p % R] = out;
+            if (a.Bout && mask != 0xFu) {
+                // outflow through reflective faces feeds the mirrored ordinate's inflow
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    if (mask >> k & 1u) continue;
+                    const int32_t nb = __ldg(g.nbr + 4 * (size_t)c + k);
+                    if (nb >= 0) continue;
+                    const int32_t f = -nb - 1;
+                    if (__ldg(g.fbc + f) != TR_BC_REFLECTIVE) continue;
+                    const int32_t sl = __ldg(g.rslot + f);
+                    const uint32_t qin = __ldg(g.rinv + (size_t)sl * nq + q);
+                    if (qin == kNone) continue;
+                    T *bp = a.Bout + ((size_t)sl * nq + qin) * 4;
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+                        if (j != k) bp[j] = o[j];
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// B_out lag slots: the upstream trace of this sweep
+template <typename T>
+__global__ void k_lag_out(uint32_t nT, uint32_t nlag, const unsigned long long *keys, const int32_t *nbr,
+                          const uint32_t *map, const T *psi, T *Bout_lag) {
+    for (uint32_t l = blockIdx.x * blockDim.x + threadIdx.x; l < nlag; l += gridDim.x * blockDim.x) {
+        const unsigned long long key = keys[l];
+        const uint32_t k = static_cast<uint32_t>(key & 3u);
+        const uint64_t qc = key >> 2;
+        const uint32_t q = static_cast<uint32_t>(qc / nT), c = static_cast<uint32_t>(qc % nT);
+        const int32_t u = nbr[4 * (size_t)c + k];
+        const uint32_t mp = map[c];
+        for (int j = 0; j < 4; ++j)
+            Bout_lag[4 * (size_t)l + j] =
+                (j == (int)k) ? T(0) : psi[((size_t)q * nT + u) * 4 + ((mp >> (2 * (4 * k + j))) & 3u)];
+    }
+}
+
+// J[c][j] = sum_q w_q psi_q[c][j], FP64 accumulation in ordinate order
+template <typename T>
+__global__ void k_scalar_flux(uint32_t nT, uint32_t nq, const double *w, const T *psi, double *J) {
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nT; c += gridDim.x * blockDim.x) {
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+        for (uint32_t q = 0; q < nq; ++q) {
+            const typename Vec4<T>::type v = load_v4<T>(psi + ((size_t)q * nT + c) * 4);
+            const double wq = __ldg(w + q);
+            a0 += wq * static_cast<double>(v.x);
+            a1 += wq * static_cast<double>(v.y);
+            a2 += wq * static_cast<double>(v.z);
+            a3 += wq * static_cast<double>(v.w);
+        }
+        double2 *dst = reinterpret_cast<double2 *>(J + 4 * (size_t)c);
+        dst[0] = make_double2(a0, a1);
+        dst[1] = make_double2(a2, a3);
+    }
+}
+
+// moments mom[m][c][j] = sum_q W[m][q] psi_q[c][j], W = w_q Y_m(Omega_q)
+template <typename T, int NM>
+__global__ void k_moments_simt(uint32_t nT, uint32_t nq, const double *W, const T *psi, double *mom) {
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nT; c += gridDim.x * blockDim.x) {
+        double acc[NM][4];
+#pragma unroll
+        for (int m = 0; m < NM; ++m) acc[m][0] = acc[m][1] = acc[m][2] = acc[m][3] = 0.0;
+        for (uint32_t q = 0; q < nq; ++q) {
+            const typename Vec4<T>::type v = load_v4<T>(psi + ((size_t)q * nT + c) * 4);
+#pragma unroll
+            for (int m = 0; m < NM; ++m) {
+                const double wq = __ldg(W + (size_t)m * nq + q);
+                acc[m][0] += wq * static_cast<double>(v.x);
+                acc[m][1] += wq * static_cast<double>(v.y);
+                acc[m][2] += wq * static_cast<double>(v.z);
+                acc[m][3] += wq * static_cast<double>(v.w);
+            }
+        }
+#pragma unroll
+        for (int m = 0; m < NM; ++m)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) mom[(size_t)m * 4 * nT + 4 * (size_t)c + j] = acc[m][j];
+    }
+}
+
+// Moments of FP32 psi on the tensor cores in split TF32 (3 products, FP32
+// accumulation): D[r][n] = sum_q A[r][q] W[n][q] with A[r][q] = psi[q][r]
+// (r = 4c + j over the M = 4 nT vertex values), N = 16 harmonics (l <= 3).
+// One warp per 16 rows, mma.sync m16n8k8 tf32; A fragments straight from
+// global memory (lanes of equal k read 8 consecutive rows: whole 32-byte
+// sectors), W split into TF32 hi/lo parts in shared memory.
+__device__ __forceinline__ uint32_t to_tf32(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+constexpr int kMomWarps = 4;
+__global__ void __launch_bounds__(32 * kMomWarps) k_moments_tf32x3(uint32_t M, uint32_t nq, uint32_t nqp,
+                                                                  const double *W, const float *psi, int nmom,
+                                                                  double *mom) {
+    extern __shared__ uint32_t wsh[];  // [2][16][nqp]: hi, lo
+    for (uint32_t i = threadIdx.x; i < 16 * nqp; i += blockDim.x) {
+        const uint32_t n = i / nqp, q = i % nqp;
+        const float w = q < nq ? static_cast<float>(W[static_cast<size_t>(n) * nq + q]) : 0.0f;
+        const uint32_t hi = to_tf32(w);
+        wsh[i] = hi;
+        wsh[16 * nqp + i] = to_tf32(w - __uint_as_float(hi));
+    }
+    __syncthreads();
+    const uint32_t lane = threadIdx.x & 31u, g = lane >> 2, t = lane & 3u;
+    const uint64_t r0 = (static_cast<uint64_t>(blockIdx.x) * kMomWarps + (threadIdx.x >> 5)) * 16;
+    if (r0 >= M) return;
+    const bool ok0 = r0 + g < M, ok1 = r0 + g + 8 < M;
+    float d[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+    for (uint32_t k0 = 0; k0 < nq; k0 += 8) {
+        const uint32_t ka = k0 + t, kb = k0 + t + 4;
+        float av[4];
+        av[0] = (ka < nq && ok0) ? __ldg(psi + static_cast<uint64_t>(ka) * M + r0 + g) : 0.0f;
+        av[1] = (ka < nq && ok1) ? __ldg(psi + static_cast<uint64_t>(ka) * M + r0 + g + 8) : 0.0f;
+        av[2] = (kb < nq && ok0) ? __ldg(psi + static_cast<uint64_t>(kb) * M + r0 + g) : 0.0f;
+        av[3] = (kb < nq && ok1) ? __ldg(psi + static_cast<uint64_t>(kb) * M + r0 + g + 8) : 0.0f;
+        uint32_t ahi[4], alo[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            ahi[i] = to_tf32(av[i]);
+            alo[i] = to_tf32(av[i] - __uint_as_float(ahi[i]));
+        }
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt) {
+            const uint32_t n = nt * 8 + g;
+            const uint32_t bh0 = wsh[n * nqp + ka], bh1 = wsh[n * nqp + kb];
+            const uint32_t bl0 = wsh[16 * nqp + n * nqp + ka], bl1 = wsh[16 * nqp + n * nqp + kb];
+            mma_tf32(d[nt], alo, bh0, bh1);   // small products first
+            mma_tf32(d[nt], ahi, bl0, bl1);
+            mma_tf32(d[nt], ahi, bh0, bh1);
+        }
+    }
+#pragma unroll
+    for (int nt = 0; nt < 2; ++nt) {
+        const int n0 = nt * 8 + 2 * static_cast<int>(t);
+        if (ok0) {
+            if (n0 < nmom) mom[static_cast<uint64_t>(n0) * M + r0 + g] = d[nt][0];
+            if (n0 + 1 < nmom) mom[static_cast<uint64_t>(n0 + 1) * M + r0 + g] = d[nt][1];
+        }
+        if (ok1) {
+            if (n0 < nmom) mom[static_cast<uint64_t>(n0) * M + r0 + g + 8] = d[nt][2];
+            if (n0 + 1 < nmom) mom[static_cast<uint64_t>(n0 + 1) * M + r0 + g + 8] = d[nt][3];
+        }
+    }
+}
+
+// ---- FP64 vector kernels of the Krylov solver --------------------------------
+__global__ void k_to_f32(uint64_t n, const double *x, float *y) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        y[i] = static_cast<float>(x[i]);
+}
+__global__ void k_to_f64(uint64_t n, const float *x, double *y) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        y[i] = static_cast<double>(x[i]);
+}
+// y = alpha * x + beta * y (x may alias y)
+__global__ void k_axpby(uint64_t n, double alpha, const double *x, double beta, double *y) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        y[i] = alpha * x[i] + beta * y[i];
+}
+// out[i] = <V_i, w> for i < k; V rows of length n with stride ld
+__global__ void k_multidot(uint64_t n, int k, const double *V, uint64_t ld, const double *w, double *partials,
+                           unsigned int *counter, double *out) {
+    __shared__ double sh[32];
+    __shared__ bool am_last;
+    for (int i = 0; i < k; ++i) {
+        double acc = 0.0;
+        const double *v = V + (uint64_t)i * ld;
+        for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n; t += (uint64_t)gridDim.x * blockDim.x)
+            acc += v[t] * w[t];
+        double s = block_sum(acc, sh);
+        if (threadIdx.x == 0) partials[(uint64_t)i * gridDim.x + blockIdx.x] = s;
+    }
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) am_last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    __syncthreads();
+    if (!am_last) return;
+    __threadfence();
+    for (int i = 0; i < k; ++i) {
+        double acc = 0.0;
+        for (unsigned int b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+            acc += __ldcg(partials + (uint64_t)i * gridDim.x + b);
+        double s = block_sum(acc, sh);
+        if (threadIdx.x == 0) out[i] = s;
+    }
+    if (threadIdx.x == 0) *counter = 0u;
+}
+// w -= sum_i h[i] V_i
+__global__ void k_gs_update(uint64_t n, int k, const double *V, uint64_t ld, const double *h, double *w) {
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n; t += (uint64_t)gridDim.x * blockDim.x) {
+        double acc = w[t];
+        for (int i = 0; i < k; ++i) acc -= h[i] * V[(uint64_t)i * ld + t];
+        w[t] = acc;
+    }
+}
+// x += sum_i y[i] V_i
+__global__ void k_combine(uint64_t n, int k, const double *V, uint64_t ld, const double *y, double *x) {
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n; t += (uint64_t)gridDim.x * blockDim.x) {
+        double acc = x[t];
+        for (int i = 0; i < k; ++i) acc += y[i] * V[(uint64_t)i * ld + t];
+        x[t] = acc;
+    }
+}
+
+// ---- energy balance (FP64, deterministic) ------------------------------------
+struct BalanceArgs {
+    uint32_t nT, nq, nbf;
+    const double *s, *stv, *ssv, *ext, *w, *ox, *oy, *oz, *finc;
+    const int32_t *fbc, *rslot;
+    const uint32_t *bcell;   // [nbf] owner cell*4 + local face
+    const uint32_t *bface;   // [nbf] face id
+    const double *Jin, *Jout, *Bin;
+};
+template <typename T>
+__global__ void k_balance(BalanceArgs b, const T *psi, double *partials, unsigned int *counter, double *out) {
+    double v[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x, nth = gridDim.x * blockDim.x;
+    for (uint32_t c = tid; c < b.nT; c += nth) {
+        double ji = 0.0, jo = 0.0;
+        for (int j = 0; j < 4; ++j) {
+            if (b.Jin) ji += b.Jin[4 * (size_t)c + j];
+            jo += b.Jout[4 * (size_t)c + j];
+        }
+        v[0] += 4.0 * b.ext[c];
+        v[1] += 0.25 * (b.stv[c] * jo - b.ssv[c] * ji);
+    }
+    for (uint32_t i = tid; i < b.nbf; i += nth) {
+        const uint32_t ck = b.bcell[i], c = ck >> 2, k = ck & 3u, f = b.bface[i];
+        const double *sk = b.s + 12 * (size_t)c + 3 * k;
+        const int32_t bc = b.fbc[f];
+        for (uint32_t q = 0; q < b.nq; ++q) {
+            const double d = odot_rn(b.ox[q], b.oy[q], b.oz[q], sk);
+            if (d > 0.0) {
+                const T *pp = psi + ((size_t)q * b.nT + c) * 4;
+                double m = 0.0;
+                for (uint32_t j = 0; j < 4; ++j)
+                    if (j != k) m += static_cast<double>(pp[j]);
+                m /= 3.0;
+                if (bc == TR_BC_REFLECTIVE) v[4] += b.w[q] * d * m;
+                else v[2] += b.w[q] * d * m;
+            } else if (d < 0.0) {
+                if (bc == TR_BC_INCIDENT) {
+                    v[3] += b.w[q] * (-d) * b.finc[f];
+                } else if (bc == TR_BC_REFLECTIVE && b.Bin) {
+                    const double *bp = b.Bin + ((size_t)b.rslot[f] * b.nq + q) * 4;
+                    double m = 0.0;
+                    for (uint32_t j = 0; j < 4; ++j)
+                        if (j != k) m += bp[j];
+                    v[4] -= b.w[q] * (-d) * m / 3.0;
+                }
+            }
+        }
+    }
+    double tot[5];
+    if (grid_reduce<5>(v, partials, counter, tot) && threadIdx.x == 0)
+        for (int i = 0; i < 5; ++i) out[i] = tot[i];
+}
+
+}  // namespace sweep
+}  // namespace transfer
+
+using namespace transfer;
+using namespace transfer::sweep;
+
+// ============================================================================
+// the context
+// ============================================================================
+struct tr_sweep {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string last_error;
+    uint32_t nT = 0, nF = 0, nq = 0, nrefl = 0, nlag = 0, maxlev = 0, forced = 0, lstride = 0, nbf = 0;
+    uint64_t nB = 0, nJ = 0, device_bytes = 0;
+    int num_sms = 0;
+    // geometry and physics
+    double *s64 = nullptr, *stv64 = nullptr, *ssv64 = nullptr, *ext64 = nullptr, *finc64 = nullptr;
+    float *s32 = nullptr, *stv32 = nullptr, *ssv32 = nullptr, *ext32 = nullptr, *finc32 = nullptr;
+    int32_t *nbr = nullptr, *fbc = nullptr, *rslot = nullptr;
+    uint32_t *map = nullptr, *rinv = nullptr, *bcell = nullptr, *bface = nullptr;
+    double *o64[4] = {nullptr, nullptr, nullptr, nullptr};  // x y z w
+    float *o32[3] = {nullptr, nullptr, nullptr};
+    double *Wm = nullptr;          // [16][nq] w_q Y_m(Omega_q)
+    // schedule
+    uint4 *task = nullptr;
+    uint32_t *lvl = nullptr, *nlev = nullptr;
+    unsigned long long *lag_keys = nullptr;
+    // state
+    double *psi64 = nullptr;
+    float *psi32 = nullptr;
+    int last_prec = 0;             // precision of the last sweep (0: none)
+    float *J32 = nullptr, *Bi32 = nullptr, *Bo32 = nullptr;
+    double *partials = nullptr, *red = nullptr;
+    unsigned int *counter = nullptr;
+    // Krylov work space (allocated on first solve)
+    double *kv = nullptr;          // [kMaxRestart + 1][n] basis
+    double *kb = nullptr, *kx = nullptr, *kr = nullptr, *kt = nullptr, *kd = nullptr, *kh = nullptr;
+    int kv_m = 0;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    std::vector<void *> allocs;
+    int64_t sweeps32 = 0, sweeps64 = 0, launches = 0;
+};
+
+static tr_status sw_err(tr_sweep *s, tr_status st, const std::string &m) {
+    if (s) s->last_error = m;
+    return transfer::set_global_error(st, m);
+}
+static tr_status sw_cuda(tr_sweep *s, cudaError_t e, const char *what) {
+    if (e == cudaSuccess) return TR_OK;
+    return sw_err(s, TR_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+template <typename T>
+static cudaError_t sw_alloc(tr_sweep *s, T **p, size_t count) {
+    size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    cudaError_t e = cudaMalloc(reinterpret_cast<void **>(p), bytes);
+    if (e != cudaSuccess) return e;
+    s->allocs.push_back(*p);
+    s->device_bytes += bytes;
+    return cudaSuccess;
+}
+template <typename T>
+static cudaError_t sw_upload(tr_sweep *s, T **p, const std::vector<T> &h) {
+    cudaError_t e = sw_alloc(s, p, h.size());
+    if (e != cudaSuccess) return e;
+    if (h.empty()) return cudaSuccess;
+    return cudaMemcpy(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+static void sw_free(tr_sweep *s) {
+    if (!s) return;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    for (void *p : s->allocs) cudaFree(p);
+    for (auto &e : s->ev)
+        if (e) cudaEventDestroy(e);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    cudaSetDevice(prev);
+    delete s;
+}
+
+static inline int grid_for(const tr_sweep *s, uint64_t n, int block = 256) {
+    uint64_t g = (n + block - 1) / block;
+    uint64_t cap = static_cast<uint64_t>(s->num_sms) * 8;
+    return static_cast<int>(std::max<uint64_t>(1, std::min(g, cap)));
+}
+
+// ---- host set-up --------------------------------------------------------------
+namespace {
+struct FaceKey {
+    uint32_t v[3];
+    uint32_t cell, k;
+    bool operator<(const FaceKey &o) const {
+        for (int i = 0; i < 3; ++i)
+            if (v[i] != o.v[i]) return v[i] < o.v[i];
+        if (cell != o.cell) return cell < o.cell;
+        return k < o.k;
+    }
+    bool same(const FaceKey &o) const { return v[0] == o.v[0] && v[1] == o.v[1] && v[2] == o.v[2]; }
+};
+void sort3(uint32_t *v) {
+    if (v[0] > v[1]) std::swap(v[0], v[1]);
+    if (v[1] > v[2]) std::swap(v[1], v[2]);
+    if (v[0] > v[1]) std::swap(v[0], v[1]);
+}
+}  // namespace
+
+static tr_status sweep_setup(tr_sweep *S, const tr_mesh_view *m, const tr_physics_view *ph,
+                             const tr_ordinates_view *o) {
+    const uint32_t nT = m->nT, nF = m->nF, nq = o->nq;
+    S->nT = nT;
+    S->nF = nF;
+    S->nq = nq;
+    S->nJ = 4ull * nT;
+    std::vector<double> s(12ull * nT), stv(nT), ssv(nT), ext(nT);
+    for (uint32_t c = 0; c < nT; ++c) {
+        const tr_tetrahedron &t = m->mesh[c];
+        std::memcpy(&s[12ull * c], t.s, sizeof(double) * 12);
+        const double sav = (ph && ph->kappa_abs_volume) ? ph->kappa_abs_volume[c] : t.kappa_volume;
+        if (!(t.kappa_volume > 0.0) || sav < 0.0 || sav > t.kappa_volume * (1.0 + 1e-12))
+            return sw_err(S, TR_ERR_MESH, "sweep: need kappa_volume > 0 and 0 <= sigma_a V <= sigma_t V");
+        stv[c] = t.kappa_volume;
+        ssv[c] = t.kappa_volume - sav;
+        ext[c] = sav * t.I_p / 4.0;
+    }
+    std::vector<int32_t> fbc(nF + 1, TR_BC_VACUUM);
+    std::vector<double> finc(nF + 1, 0.0);
+    for (uint32_t f = 0; f < nF; ++f) {
+        if (ph && ph->face_bc) fbc[f] = ph->face_bc[f];
+        if (ph && ph->face_incident) finc[f] = ph->face_incident[f];
+        if (fbc[f] < 0 || fbc[f] > 2) return sw_err(S, TR_ERR_INVALID_ARG, "sweep: face_bc must be 0, 1 or 2");
+    }
+    // adjacency by sorted vertex triples
+    std::vector<FaceKey> keys(4ull * nT);
+    for (uint32_t c = 0; c < nT; ++c)
+        for (uint32_t k = 0; k < 4; ++k) {
+            FaceKey &e = keys[4ull * c + k];
+            int n = 0;
+            for (int j = 0; j < 4; ++j)
+                if (j != (int)k) e.v[n++] = m->mesh[c].p[j];
+            sort3(e.v);
+            e.cell = c;
+            e.k = k;
+        }
+    std::sort(keys.begin(), keys.end());
+    std::vector<FaceKey> bkeys(nF);
+    for (uint32_t f = 0; f < nF; ++f) {
+        std::memcpy(bkeys[f].v, m->bnd[f].p, sizeof(uint32_t) * 3);
+        sort3(bkeys[f].v);
+        bkeys[f].cell = f;
+        bkeys[f].k = 0;
+    }
+    std::sort(bkeys.begin(), bkeys.end());
+    std::vector<int32_t> nbr(4ull * nT, 0);
+    std::vector<uint32_t> map(nT, 0u), bcell, bface;
+    for (size_t i = 0; i < keys.size();) {
+        if (i + 1 < keys.size() && keys[i].same(keys[i + 1])) {
+            if (i + 2 < keys.size() && keys[i].same(keys[i + 2]))
+                return sw_err(S, TR_ERR_MESH, "sweep: a face is shared by more than two tetrahedra");
+            const uint32_t a = keys[i].cell, ka = keys[i].k, b = keys[i + 1].cell, kb = keys[i + 1].k;
+            nbr[4ull * a + ka] = static_cast<int32_t>(b);
+            nbr[4ull * b + kb] = static_cast<int32_t>(a);
+            for (int d = 0; d < 3; ++d) s[12ull * b + 3 * kb + d] = -s[12ull * a + 3 * ka + d];
+            for (uint32_t j = 0; j < 4; ++j) {
+                if (j != ka)
+                    for (uint32_t jj = 0; jj < 4; ++jj)
+                        if (m->mesh[b].p[jj] == m->mesh[a].p[j]) map[a] |= jj << (2 * (4 * ka + j));
+                if (j != kb)
+                    for (uint32_t jj = 0; jj < 4; ++jj)
+                        if (m->mesh[a].p[jj] == m->mesh[b].p[j]) map[b] |= jj << (2 * (4 * kb + j));
+            }
+            i += 2;
+        } else {
+            auto it = std::lower_bound(bkeys.begin(), bkeys.end(), keys[i],
+                                       [](const FaceKey &x, const FaceKey &y) {
+                                           for (int d = 0; d < 3; ++d)
+                                               if (x.v[d] != y.v[d]) return x.v[d] < y.v[d];
+                                           return false;
+                                       });
+            if (it == bkeys.end() || !it->same(keys[i]))
+                return sw_err(S, TR_ERR_MESH, "sweep: a tetrahedron face is neither shared nor a boundary face");
+            nbr[4ull * keys[i].cell + keys[i].k] = -static_cast<int32_t>(it->cell) - 1;
+            bcell.push_back(keys[i].cell * 4 + keys[i].k);
+            bface.push_back(it->cell);
+            i += 1;
+        }
+    }
+    S->nbf = static_cast<uint32_t>(bcell.size());
+    // reflective faces: slots and mirrored ordinates (incoming q_in -> outgoing q_out;
+    // stored inverted: rinv[slot][q_out] = q_in)
+    std::vector<int32_t> rslot(nF + 1, -1);
+    uint32_t nrefl = 0;
+    for (uint32_t f = 0; f < nF; ++f)
+        if (fbc[f] == TR_BC_REFLECTIVE) rslot[f] = static_cast<int32_t>(nrefl++);
+    S->nrefl = nrefl;
+    std::vector<uint32_t> rinv(static_cast<size_t>(nrefl) * nq + 1, kNone);
+    for (uint32_t i = 0; i < S->nbf; ++i) {
+        const uint32_t c = bcell[i] >> 2, k = bcell[i] & 3u, f = bface[i];
+        if (rslot[f] < 0) continue;
+        const double *sk = &s[12ull * c + 3 * k];
+        const double a = std::sqrt(sk[0] * sk[0] + sk[1] * sk[1] + sk[2] * sk[2]);
+        const double n[3] = {sk[0] / a, sk[1] / a, sk[2] / a};
+        for (uint32_t q = 0; q < nq; ++q) {
+            if (!(o->x[q] * sk[0] + o->y[q] * sk[1] + o->z[q] * sk[2] < 0.0)) continue;
+            const double on = o->x[q] * n[0] + o->y[q] * n[1] + o->z[q] * n[2];
+            const double r[3] = {o->x[q] - 2 * on * n[0], o->y[q] - 2 * on * n[1], o->z[q] - 2 * on * n[2]};
+            uint32_t best = 0;
+            double bd = 1e300;
+            for (uint32_t p = 0; p < nq; ++p) {
+                const double d = (o->x[p] - r[0]) * (o->x[p] - r[0]) + (o->y[p] - r[1]) * (o->y[p] - r[1]) +
+                                 (o->z[p] - r[2]) * (o->z[p] - r[2]);
+                if (d < bd) {
+                    bd = d;
+                    best = p;
+                }
+            }
+            if (bd > 1e-16)
+                return sw_err(S, TR_ERR_INVALID_ARG,
+                              "sweep: a reflective face mirrors an ordinate onto a direction outside the set");
+            rinv[static_cast<size_t>(rslot[f]) * nq + best] = q;
+        }
+    }
+    // ordinates, moment weights
+    std::vector<double> ox(o->x, o->x + nq), oy(o->y, o->y + nq), oz(o->z, o->z + nq), w(o->w, o->w + nq);
+    std::vector<float> ox32(nq), oy32(nq), oz32(nq);
+    for (uint32_t q = 0; q < nq; ++q) {
+        ox32[q] = static_cast<float>(ox[q]);
+        oy32[q] = static_cast<float>(oy[q]);
+        oz32[q] = static_cast<float>(oz[q]);
+    }
+    std::vector<double> Wm(static_cast<size_t>(kMaxMoments) * nq);
+    for (int l = 0, mm = 0; l <= 3; ++l)
+        for (int mq = -l; mq <= l; ++mq, ++mm)
+            for (uint32_t q = 0; q < nq; ++q)
+                Wm[static_cast<size_t>(mm) * nq + q] = w[q] * tr_spherical_value(l, mq, ox[q], oy[q], oz[q]);
+    auto f32 = [](const std::vector<double> &v) {
+        std::vector<float> r(v.size());
+        for (size_t i = 0; i < v.size(); ++i) r[i] = static_cast<float>(v[i]);
+        return r;
+    };
+    cudaError_t e = cudaSuccess;
+#define UP(ptr, vec)                                         \
+    if (e == cudaSuccess) e = sw_upload(S, &S->ptr, vec);
+    UP(s64, s) UP(stv64, stv) UP(ssv64, ssv) UP(ext64, ext) UP(finc64, finc)
+    UP(s32, f32(s)) UP(stv32, f32(stv)) UP(ssv32, f32(ssv)) UP(ext32, f32(ext)) UP(finc32, f32(finc))
+    UP(nbr, nbr) UP(fbc, fbc) UP(rslot, rslot) UP(map, map) UP(rinv, rinv) UP(bcell, bcell) UP(bface, bface)
+    UP(o64[0], ox) UP(o64[1], oy) UP(o64[2], oz) UP(o64[3], w) UP(o32[0], ox32) UP(o32[1], oy32) UP(o32[2], oz32)
+    UP(Wm, Wm)
+#undef UP
+    if (e != cudaSuccess) return sw_cuda(S, e, "sweep: upload");
+    // ---- schedule on the device
+    SchedBuild b;
+    b.nT = nT;
+    b.nq = nq;
+    b.s = S->s64;
+    b.nbr = S->nbr;
+    b.ox = S->o64[0];
+    b.oy = S->o64[1];
+    b.oz = S->o64[2];
+    int32_t *indeg = nullptr;
+    uint32_t *order = nullptr, *pos = nullptr, *lvl_tmp = nullptr, *nforced = nullptr;
+    uint8_t *mask = nullptr, *lagm = nullptr;
+    unsigned long long *lag_tmp = nullptr;
+    unsigned int *lag_count = nullptr;
+    const size_t nqT = static_cast<size_t>(nq) * nT;
+    auto tmp_alloc = [&](void **p, size_t bytes) {
+        if (e == cudaSuccess) e = cudaMalloc(p, std::max<size_t>(bytes, 16));
+    };
+    tmp_alloc(reinterpret_cast<void **>(&indeg), nqT * 4);
+    tmp_alloc(reinterpret_cast<void **>(&order), nqT * 4);
+    tmp_alloc(reinterpret_cast<void **>(&pos), nqT * 4);
+    tmp_alloc(reinterpret_cast<void **>(&mask), nqT);
+    tmp_alloc(reinterpret_cast<void **>(&lagm), nqT);
+    tmp_alloc(reinterpret_cast<void **>(&lvl_tmp), static_cast<size_t>(nq) * (nT + 1) * 4);
+    tmp_alloc(reinterpret_cast<void **>(&nforced), static_cast<size_t>(nq) * 4);
+    tmp_alloc(reinterpret_cast<void **>(&lag_tmp), static_cast<size_t>(kMaxLag) * 8);
+    tmp_alloc(reinterpret_cast<void **>(&lag_count), 4);
+    if (e == cudaSuccess) e = sw_alloc(S, &S->nlev, nq);
+    if (e == cudaSuccess) e = sw_alloc(S, &S->task, nqT);
+    tr_status st = TR_OK;
+    std::vector<uint32_t> nlev_h(nq), nforced_h(nq);
+    uint32_t nlag = 0;
+    if (e == cudaSuccess) {
+        b.indeg = indeg;
+        b.order = order;
+        b.pos = pos;
+        b.mask = mask;
+        b.lagm = lagm;
+        b.lvl = lvl_tmp;
+        b.nlev = S->nlev;
+        b.nforced = nforced;
+        k_sched_build<<<nq, kSchedThreads, 0, S->stream>>>(b);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemsetAsync(lag_count, 0, 4, S->stream);
+    if (e == cudaSuccess) {
+        k_lag_collect<<<grid_for(S, nqT), 256, 0, S->stream>>>(nT, nq, lagm, lag_tmp, lag_count);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&nlag, lag_count, 4, cudaMemcpyDeviceToHost, S->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(nlev_h.data(), S->nlev, 4ull * nq, cudaMemcpyDeviceToHost, S->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(nforced_h.data(), nforced, 4ull * nq, cudaMemcpyDeviceToHost, S->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(S->stream);
+    if (e == cudaSuccess && nlag > kMaxLag) st = sw_err(S, TR_ERR_UNSUPPORTED, "sweep: too many cyclic dependencies");
+    std::vector<unsigned long long> lag_h(nlag);
+    if (e == cudaSuccess && st == TR_OK && nlag) {
+        e = cudaMemcpy(lag_h.data(), lag_tmp, 8ull * nlag, cudaMemcpyDeviceToHost);
+        std::sort(lag_h.begin(), lag_h.end());
+    }
+    if (e == cudaSuccess && st == TR_OK) e = sw_upload(S, &S->lag_keys, lag_h);
+    S->nlag = nlag;
+    uint32_t maxlev = 0, forced = 0;
+    for (uint32_t q = 0; q < nq; ++q) {
+        maxlev = std::max(maxlev, nlev_h[q]);
+        forced += nforced_h[q];
+    }
+    S->maxlev = maxlev;
+    S->forced = forced;
+    S->lstride = maxlev + 1;
+    if (e == cudaSuccess && st == TR_OK) {
+        k_records<<<grid_for(S, nqT), 256, 0, S->stream>>>(nT, nq, order, pos, mask, lagm, S->nbr, S->lag_keys, nlag,
+                                                           S->task);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && st == TR_OK) e = sw_alloc(S, &S->lvl, static_cast<size_t>(nq) * S->lstride);
+    if (e == cudaSuccess && st == TR_OK) {
+        // compact the level pointers to [nq][lstride]; levels past nlev[q] are empty
+        std::vector<uint32_t> lv(static_cast<size_t>(nq) * (nT + 1)), lc(static_cast<size_t>(nq) * S->lstride);
+        e = cudaMemcpy(lv.data(), lvl_tmp, lv.size() * 4, cudaMemcpyDeviceToHost);
+        for (uint32_t q = 0; q < nq && e == cudaSuccess; ++q)
+            for (uint32_t L = 0; L < S->lstride; ++L)
+                lc[static_cast<size_t>(q) * S->lstride + L] = L <= nlev_h[q] ? lv[static_cast<size_t>(q) * (nT + 1) + L] : nT;
+        if (e == cudaSuccess) e = cudaMemcpy(S->lvl, lc.data(), lc.size() * 4, cudaMemcpyHostToDevice);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(S->stream);
+    for (void *p : {(void *)indeg, (void *)order, (void *)pos, (void *)mask, (void *)lagm, (void *)lvl_tmp,
+                    (void *)nforced, (void *)lag_tmp, (void *)lag_count})
+        if (p) cudaFree(p);
+    if (st != TR_OK) return st;
+    if (e != cudaSuccess) return sw_cuda(S, e, "sweep: schedule");
+    S->nB = static_cast<uint64_t>(nrefl) * nq * 4 + 4ull * nlag;
+    // reductions
+    if (e == cudaSuccess) e = sw_alloc(S, &S->partials, 64ull * kRedGrid);
+    if (e == cudaSuccess) e = sw_alloc(S, &S->red, 256);
+    if (e == cudaSuccess) e = sw_alloc(S, &S->counter, 4);
+    if (e == cudaSuccess) e = cudaMemset(S->counter, 0, 16);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_sweep<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRingBytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_sweep<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRingBytes);
+    if (e == cudaSuccess) e = cudaEventCreate(&S->ev[0]);
+    if (e == cudaSuccess) e = cudaEventCreate(&S->ev[1]);
+    if (e != cudaSuccess) return sw_cuda(S, e, "sweep: allocation");
+    return TR_OK;
+}
+
+// ---- one sweep ------------------------------------------------------------------
+static cudaError_t ensure_psi(tr_sweep *S, int prec) {
+    const size_t n = 4ull * S->nT * S->nq;
+    cudaError_t e = cudaSuccess;
+    if (prec == 64 && !S->psi64) e = sw_alloc(S, &S->psi64, n);
+    if (prec == 32 && !S->psi32) {
+        e = sw_alloc(S, &S->psi32, n);
+        if (e == cudaSuccess) e = sw_alloc(S, &S->J32, S->nJ);
+        if (e == cudaSuccess) e = sw_alloc(S, &S->Bi32, S->nB);
+        if (e == cudaSuccess) e = sw_alloc(S, &S->Bo32, S->nB);
+    }
+    return e;
+}
+
+template <typename T>
+static Geom<T> geom_of(const tr_sweep *S) {
+    Geom<T> g;
+    if constexpr (sizeof(T) == 8) {
+        g.s = S->s64;
+        g.stv = S->stv64;
+        g.ssv = S->ssv64;
+        g.ext = S->ext64;
+        g.finc = S->finc64;
+    } else {
+        g.s = S->s32;
+        g.stv = S->stv32;
+        g.ssv = S->ssv32;
+        g.ext = S->ext32;
+        g.finc = S->finc32;
+    }
+    g.nbr = S->nbr;
+    g.map = S->map;
+    g.fbc = S->fbc;
+    g.rslot = S->rslot;
+    g.rinv = S->rinv;
+    return g;
+}
+
+// Queues one sweep: J_in, B_in FP64 (null = 0) -> J_out, B_out FP64 (null = skip).
+static cudaError_t sweep_enqueue(tr_sweep *S, int prec, const double *J_in, const double *B_in, int with_ext,
+                                 double *J_out, double *B_out) {
+    cudaError_t e = ensure_psi(S, prec);
+    if (e != cudaSuccess) return e;
+    cudaStream_t st = S->stream;
+    Sched sc{S->task, S->lvl, S->nlev, S->lstride};
+    const size_t smem = kRingBytes;
+    if (prec == 64) {
+        SweepArgs<double> a;
+        a.nT = S->nT;
+        a.nq = S->nq;
+        a.ox = S->o64[0];
+        a.oy = S->o64[1];
+        a.oz = S->o64[2];
+        a.J = J_in;
+        a.Bin = B_in;
+        a.Bout = B_out;
+        a.psi = S->psi64;
+        a.with_ext = with_ext;
+        a.lag_base = static_cast<uint64_t>(S->nrefl) * S->nq * 4;
+        if (B_out && S->nB) {
+            e = cudaMemsetAsync(B_out, 0, S->nB * 8, st);
+            if (e != cudaSuccess) return e;
+        }
+        k_sweep<double><<<S->nq, kSweepThreads, smem, st>>>(geom_of<double>(S), sc, a);
+        ++S->launches;
+        if (B_out && S->nlag) {
+            k_lag_out<double><<<grid_for(S, S->nlag), 256, 0, st>>>(S->nT, S->nlag, S->lag_keys, S->nbr, S->map,
+                                                                   S->psi64, B_out + a.lag_base);
+            ++S->launches;
+        }
+        if (J_out) {
+            k_scalar_flux<double><<<grid_for(S, S->nT), 256, 0, st>>>(S->nT, S->nq, S->o64[3], S->psi64, J_out);
+            ++S->launches;
+        }
+        ++S->sweeps64;
+    } else {
+        if (J_in) {
+            k_to_f32<<<grid_for(S, S->nJ), 256, 0, st>>>(S->nJ, J_in, S->J32);
+            ++S->launches;
+        }
+        if (B_in && S->nB) {
+            k_to_f32<<<grid_for(S, S->nB), 256, 0, st>>>(S->nB, B_in, S->Bi32);
+            ++S->launches;
+        }
+        SweepArgs<float> a;
+        a.nT = S->nT;
+        a.nq = S->nq;
+        a.ox = S->o32[0];
+        a.oy = S->o32[1];
+        a.oz = S->o32[2];
+        a.J = J_in ? S->J32 : nullptr;
+        a.Bin = (B_in && S->nB) ? S->Bi32 : nullptr;
+        a.Bout = (B_out && S->nB) ? S->Bo32 : nullptr;
+        a.psi = S->psi32;
+        a.with_ext = with_ext;
+        a.lag_base = static_cast<uint64_t>(S->nrefl) * S->nq * 4;
+        if (a.Bout) {
+            e = cudaMemsetAsync(S->Bo32, 0, S->nB * 4, st);
+            if (e != cudaSuccess) return e;
+        }
+        k_sweep<float><<<S->nq, kSweepThreads, smem, st>>>(geom_of<float>(S), sc, a);
+        ++S->launches;
+        if (a.Bout && S->nlag) {
+            k_lag_out<float><<<grid_for(S, S->nlag), 256, 0, st>>>(S->nT, S->nlag, S->lag_keys, S->nbr, S->map,
+                                                                  S->psi32, S->Bo32 + a.lag_base);
+            ++S->launches;
+        }
+        if (a.Bout) {
+            k_to_f64<<<grid_for(S, S->nB), 256, 0, st>>>(S->nB, S->Bo32, B_out);
+            ++S->launches;
+        }
+        if (J_out) {
+            k_scalar_flux<float><<<grid_for(S, S->nT), 256, 0, st>>>(S->nT, S->nq, S->o64[3], S->psi32, J_out);
+            ++S->launches;
+        }
+        ++S->sweeps32;
+    }
+    S->last_prec = prec;
+    return cudaGetLastError();
+}
+
+// ---- Krylov solver ------------------------------------------------------------
+static cudaError_t krylov_alloc(tr_sweep *S, int m) {
+    if (S->kv && S->kv_m >= m) return cudaSuccess;
+    const uint64_t n = S->nJ + S->nB;
+    cudaError_t e = sw_alloc(S, &S->kv, n * (m + 1));
+    if (e == cudaSuccess && !S->kb) e = sw_alloc(S, &S->kb, n);
+    if (e == cudaSuccess && !S->kx) e = sw_alloc(S, &S->kx, n);
+    if (e == cudaSuccess && !S->kr) e = sw_alloc(S, &S->kr, n);
+    if (e == cudaSuccess && !S->kt) e = sw_alloc(S, &S->kt, n);
+    if (e == cudaSuccess && !S->kd) e = sw_alloc(S, &S->kd, n);
+    if (e == cudaSuccess && !S->kh) e = sw_alloc(S, &S->kh, 2 * (kMaxRestart + 2));
+    if (e == cudaSuccess) S->kv_m = m;
+    return e;
+}
+
+// y = (I - T) x with T the sweep of precision prec without external sources
+static cudaError_t op_apply(tr_sweep *S, int prec, const double *x, double *y) {
+    const uint64_t n = S->nJ + S->nB;
+    cudaError_t e = sweep_enqueue(S, prec, x, S->nB ? x + S->nJ : nullptr, 0, y, S->nB ? y + S->nJ : nullptr);
+    if (e != cudaSuccess) return e;
+    k_axpby<<<grid_for(S, n), 256, 0, S->stream>>>(n, 1.0, x, -1.0, y);
+    ++S->launches;
+    return cudaGetLastError();
+}
+
+static cudaError_t dots(tr_sweep *S, int k, const double *V, uint64_t ld, const double *w, double *dev_out,
+                        double *host_out) {
+    const uint64_t n = S->nJ + S->nB;
+    k_multidot<<<kRedGrid, 256, 0, S->stream>>>(n, k, V, ld, w, S->partials, S->counter, dev_out);
+    ++S->launches;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || !host_out) return e;
+    e = cudaMemcpyAsync(host_out, dev_out, sizeof(double) * k, cudaMemcpyDeviceToHost, S->stream);
+    if (e != cudaSuccess) return e;
+    return cudaStreamSynchronize(S->stream);
+}
+static cudaError_t vnorm(tr_sweep *S, const double *x, double *out) {
+    double v = 0.0;
+    cudaError_t e = dots(S, 1, x, 0, x, S->red, &v);
+    *out = std::sqrt(v);
+    return e;
+}
+
+// GMRES(m) on (I - T_prec) x = b, x updated in place (device vectors).
+// Stops at ||b - (I - T) x|| <= rtol * bref (the recursion estimate,
+// confirmed by a true residual at the end of a cycle).
+static cudaError_t gmres(tr_sweep *S, int prec, const double *b, double *x, int m, double rtol, double bref,
+                         int max_it, int *its, double *res_out) {
+    const uint64_t n = S->nJ + S->nB;
+    cudaError_t e = krylov_alloc(S, m);
+    if (e != cudaSuccess) return e;
+    cudaStream_t st = S->stream;
+    std::vector<double> H(static_cast<size_t>(m + 1) * m), cs(m), sn(m), g(m + 1), y(m), h(m + 1);
+    double res = 1.0;
+    int it = 0;
+    const int gr = grid_for(S, n);
+    while (it < max_it) {
+        // r = b - (I - T) x  into V_0
+        e = op_apply(S, prec, x, S->kv);
+        if (e != cudaSuccess) return e;
+        k_axpby<<<gr, 256, 0, st>>>(n, 1.0, b, -1.0, S->kv);
+        ++S->launches;
+        double beta = 0.0;
+        if ((e = vnorm(S, S->kv, &beta)) != cudaSuccess) return e;
+        res = beta / bref;
+        if (res <= rtol || beta == 0.0) break;
+        k_axpby<<<gr, 256, 0, st>>>(n, 0.0, S->kv, 1.0 / beta, S->kv);
+        ++S->launches;
+        std::fill(H.begin(), H.end(), 0.0);
+        std::fill(g.begin(), g.end(), 0.0);
+        g[0] = beta;
+        int j = 0;
+        for (; j < m && it < max_it; ++j) {
+            double *w = S->kv + static_cast<uint64_t>(j + 1) * n;
+            if ((e = op_apply(S, prec, S->kv + static_cast<uint64_t>(j) * n, w)) != cudaSuccess) return e;
+            ++it;
+            for (int pass = 0; pass < 2; ++pass) {  // classical Gram-Schmidt, twice
+                if ((e = dots(S, j + 1, S->kv, n, w, S->kh, h.data())) != cudaSuccess) return e;
+                k_gs_update<<<gr, 256, 0, st>>>(n, j + 1, S->kv, n, S->kh, w);
+                ++S->launches;
+                for (int i = 0; i <= j; ++i) H[static_cast<size_t>(i) * m + j] += h[i];
+            }
+            double hn = 0.0;
+            if ((e = vnorm(S, w, &hn)) != cudaSuccess) return e;
+            H[static_cast<size_t>(j + 1) * m + j] = hn;
+            if (hn > 0.0) {
+                k_axpby<<<gr, 256, 0, st>>>(n, 0.0, w, 1.0 / hn, w);
+                ++S->launches;
+            }
+            for (int i = 0; i < j; ++i) {
+                const double t0 = cs[i] * H[static_cast<size_t>(i) * m + j] + sn[i] * H[static_cast<size_t>(i + 1) * m + j];
+                H[static_cast<size_t>(i + 1) * m + j] =
+                    -sn[i] * H[static_cast<size_t>(i) * m + j] + cs[i] * H[static_cast<size_t>(i + 1) * m + j];
+                H[static_cast<size_t>(i) * m + j] = t0;
+            }
+            const double h0 = H[static_cast<size_t>(j) * m + j], h1 = H[static_cast<size_t>(j + 1) * m + j];
+            const double rr = std::sqrt(h0 * h0 + h1 * h1);
+            cs[j] = h0 / rr;
+            sn[j] = h1 / rr;
+            H[static_cast<size_t>(j) * m + j] = rr;
+            H[static_cast<size_t>(j + 1) * m + j] = 0.0;
+            g[j + 1] = -sn[j] * g[j];
+            g[j] = cs[j] * g[j];
+            res = std::fabs(g[j + 1]) / bref;
+            if (res <= rtol) {
+                ++j;
+                break;
+            }
+        }
+        for (int i = j - 1; i >= 0; --i) {
+            double v = g[i];
+            for (int k = i + 1; k < j; ++k) v -= H[static_cast<size_t>(i) * m + k] * y[k];
+            y[i] = v / H[static_cast<size_t>(i) * m + i];
+        }
+        e = cudaMemcpyAsync(S->kh, y.data(), sizeof(double) * j, cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return e;
+        k_combine<<<gr, 256, 0, st>>>(n, j, S->kv, n, S->kh, x);
+        ++S->launches;
+        if (res <= rtol) {  // confirm with the true residual
+            if ((e = op_apply(S, prec, x, S->kt)) != cudaSuccess) return e;
+            k_axpby<<<gr, 256, 0, st>>>(n, 1.0, b, -1.0, S->kt);
+            ++S->launches;
+            double tr = 0.0;
+            if ((e = vnorm(S, S->kt, &tr)) != cudaSuccess) return e;
+            res = tr / bref;
+            if (res <= rtol) break;
+        }
+    }
+    *its = it;
+    *res_out = res;
+    return cudaSuccess;
+}
+
+// ============================================================================
+// C ABI
+// ============================================================================
+#define SW_CHECK(s)                                                                      \
+    do {                                                                                 \
+        if (!(s)) return transfer::set_global_error(TR_ERR_INVALID_ARG, "null sweep");   \
+        if (cudaSetDevice((s)->device) != cudaSuccess)                                   \
+            return sw_err((s), TR_ERR_CUDA, "cudaSetDevice failed");                     \
+    } while (0)
+
+extern "C" {
+
+tr_status tr_ordinates_product(int n_polar, int n_azim, double *x, double *y, double *z, double *w) {
+    if (n_polar < 1 || n_azim < 1 || !x || !y || !z || !w)
+        return transfer::set_global_error(TR_ERR_INVALID_ARG, "tr_ordinates_product: bad arguments");
+    std::vector<double> mu(n_polar), wm(n_polar);
+    for (int i = 0; i < n_polar; ++i) {  // Gauss-Legendre nodes by Newton on P_n
+        double t = std::cos(M_PI * (i + 0.75) / (n_polar + 0.5)), dp = 1.0;
+        for (int it = 0; it < 100; ++it) {
+            double p0 = 1.0, p1 = t;
+            for (int l = 2; l <= n_polar; ++l) {
+                const double p2 = ((2.0 * l - 1.0) * t * p1 - (l - 1.0) * p0) / l;
+                p0 = p1;
+                p1 = p2;
+            }
+            dp = n_polar * (t * p1 - p0) / (t * t - 1.0);
+            const double dt = p1 / dp;
+            t -= dt;
+            if (std::fabs(dt) < 1e-16) break;
+        }
+        mu[i] = t;
+        wm[i] = 2.0 / ((1.0 - t * t) * dp * dp);
+    }
+    int q = 0;
+    for (int i = 0; i < n_polar; ++i) {
+        const double st = std::sqrt(1.0 - mu[i] * mu[i]);
+        for (int k = 0; k < n_azim; ++k, ++q) {
+            const double phi = (k + 0.5) * 2.0 * M_PI / n_azim;
+            x[q] = st * std::cos(phi);
+            y[q] = st * std::sin(phi);
+            z[q] = mu[i];
+            w[q] = 0.5 * wm[i] / n_azim;
+        }
+    }
+    return TR_OK;
+}
+
+tr_status tr_sweep_create(int device, const tr_mesh_view *mesh, const tr_physics_view *phys,
+                          const tr_ordinates_view *ord, tr_sweep **out) {
+    if (!mesh || !ord || !out || !mesh->mesh || (mesh->nF && !mesh->bnd) || !ord->x || !ord->y || !ord->z || !ord->w)
+        return transfer::set_global_error(TR_ERR_INVALID_ARG, "tr_sweep_create: null argument");
+    *out = nullptr;
+    if (mesh->nT == 0 || mesh->nT > kCellMask || ord->nq == 0 || ord->nq > 65535)
+        return transfer::set_global_error(TR_ERR_INVALID_ARG, "tr_sweep_create: need 0 < nT < 2^28, 0 < nq < 65536");
+    if (static_cast<uint64_t>(mesh->nT) * ord->nq >= (1ull << 31))
+        return transfer::set_global_error(TR_ERR_INVALID_ARG, "tr_sweep_create: nT * nq must stay below 2^31");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return transfer::set_global_error(TR_ERR_NO_DEVICE, "tr_sweep_create: no CUDA device");
+    if (device < 0 || device >= ndev) return transfer::set_global_error(TR_ERR_INVALID_ARG, "tr_sweep_create: bad device");
+    tr_sweep *S = new (std::nothrow) tr_sweep();
+    if (!S) return transfer::set_global_error(TR_ERR_OUT_OF_MEMORY, "tr_sweep_create: host allocation");
+    S->device = device;
+    if (cudaSetDevice(device) != cudaSuccess) {
+        delete S;
+        return transfer::set_global_error(TR_ERR_CUDA, "cudaSetDevice failed");
+    }
+    cudaDeviceGetAttribute(&S->num_sms, cudaDevAttrMultiProcessorCount, device);
+    if (cudaStreamCreateWithFlags(&S->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete S;
+        return transfer::set_global_error(TR_ERR_CUDA, "tr_sweep_create: stream");
+    }
+    tr_status st = sweep_setup(S, mesh, phys, ord);
+    if (st != TR_OK) {
+        std::string msg = S->last_error;
+        sw_free(S);
+        return transfer::set_global_error(st, msg);
+    }
+    *out = S;
+    return TR_OK;
+}
+
+tr_status tr_sweep_destroy(tr_sweep *s) {
+    sw_free(s);
+    return TR_OK;
+}
+
+const char *tr_sweep_last_error(const tr_sweep *s) { return s ? s->last_error.c_str() : ""; }
+
+tr_status tr_sweep_info_get(const tr_sweep *s, tr_sweep_info *info) {
+    if (!s || !info) return transfer::set_global_error(TR_ERR_INVALID_ARG, "tr_sweep_info_get: null argument");
+    info->nT = s->nT;
+    info->nF = s->nF;
+    info->nq = s->nq;
+    info->n_extra = s->nB;
+    info->n_reflective = s->nrefl;
+    info->n_lag = s->nlag;
+    info->max_levels = s->maxlev;
+    info->forced_levels = s->forced;
+    info->device_bytes = s->device_bytes;
+    info->device = s->device;
+    return TR_OK;
+}
+
+tr_status tr_sweep_levels(tr_sweep *s, int32_t *level) {
+    SW_CHECK(s);
+    if (!level) return sw_err(s, TR_ERR_INVALID_ARG, "tr_sweep_levels: null output");
+    const size_t nqT = static_cast<size_t>(s->nq) * s->nT;
+    std::vector<uint4> task(nqT);
+    std::vector<uint32_t> lvl(static_cast<size_t>(s->nq) * s->lstride), nlev(s->nq);
+    cudaError_t e = cudaMemcpy(task.data(), s->task, nqT * sizeof(uint4), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(lvl.data(), s->lvl, lvl.size() * 4, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(nlev.data(), s->nlev, nlev.size() * 4, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return sw_cuda(s, e, "tr_sweep_levels");
+    for (uint32_t q = 0; q < s->nq; ++q)
+        for (uint32_t L = 0; L < nlev[q]; ++L)
+            for (uint32_t p = lvl[static_cast<size_t>(q) * s->lstride + L]; p < lvl[static_cast<size_t>(q) * s->lstride + L + 1]; ++p)
+                level[static_cast<size_t>(q) * s->nT + (task[static_cast<size_t>(q) * s->nT + p].x & kCellMask)] =
+                    static_cast<int32_t>(L);
+    return TR_OK;
+}
+
+tr_status tr_sweep_apply(tr_sweep *s, int precision, const double *J_in, const double *B_in, int with_ext,
+                         double *J_out, double *B_out) {
+    SW_CHECK(s);
+    if (precision != 32 && precision != 64) return sw_err(s, TR_ERR_INVALID_ARG, "precision must be 32 or 64");
+    cudaError_t e = sweep_enqueue(s, precision, J_in, s->nB ? B_in : nullptr, with_ext, J_out, s->nB ? B_out : nullptr);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    return sw_cuda(s, e, "tr_sweep_apply");
+}
+
+tr_status tr_sweep_psi(tr_sweep *s, double *psi) {
+    SW_CHECK(s);
+    if (!psi) return sw_err(s, TR_ERR_INVALID_ARG, "tr_sweep_psi: null output");
+    if (!s->last_prec) return sw_err(s, TR_ERR_INVALID_ARG, "tr_sweep_psi: no sweep has run");
+    const uint64_t n = 4ull * s->nT * s->nq;
+    cudaError_t e;
+    if (s->last_prec == 64) {
+        e = cudaMemcpyAsync(psi, s->psi64, n * 8, cudaMemcpyDeviceToDevice, s->stream);
+    } else {
+        k_to_f64<<<grid_for(s, n), 256, 0, s->stream>>>(n, s->psi32, psi);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    return sw_cuda(s, e, "tr_sweep_psi");
+}
+
+tr_status tr_sweep_moments(tr_sweep *s, int nmom, double *mom) {
+    SW_CHECK(s);
+    if (!mom || nmom < 1 || nmom > kMaxMoments)
+        return sw_err(s, TR_ERR_INVALID_ARG, "tr_sweep_moments: need 1 <= nmom <= 16 and an output");
+    if (!s->last_prec) return sw_err(s, TR_ERR_INVALID_ARG, "tr_sweep_moments: no sweep has run");
+    cudaError_t e = cudaSuccess;
+    const uint32_t nqp8 = (s->nq + 7) / 8 * 8;
+    if (s->last_prec == 32 && 2ull * 16 * nqp8 * sizeof(uint32_t) <= 48 * 1024) {  // nq <= 384
+        const uint32_t M = 4 * s->nT, nqp = nqp8;
+        const uint64_t warps = (M + 15) / 16;
+        const int blocks = static_cast<int>((warps + kMomWarps - 1) / kMomWarps);
+        const size_t smem = 2ull * 16 * nqp * sizeof(uint32_t);
+        k_moments_tf32x3<<<blocks, 32 * kMomWarps, smem, s->stream>>>(M, s->nq, nqp, s->Wm, s->psi32, nmom, mom);
+        e = cudaGetLastError();
+        ++s->launches;
+    } else {
+        // FP64 (and FP32 with more than 384 ordinates): FP64 accumulation over
+        // complete l bands (1, 4, 9 or 16 moments); extra bands go to scratch
+        const int gr = grid_for(s, s->nT, 128);
+        const int nb = nmom <= 1 ? 1 : nmom <= 4 ? 4 : nmom <= 9 ? 9 : 16;
+        double *out = mom, *tmp = nullptr;
+        if (nb != nmom) {
+            e = cudaMalloc(&tmp, sizeof(double) * nb * 4ull * s->nT);
+            out = tmp;
+        }
+        if (e == cudaSuccess && s->last_prec == 64) {
+            if (nb == 1) k_moments_simt<double, 1><<<gr, 128, 0, s->stream>>>(s->nT, s->nq, s->Wm, s->psi64, out);
+            else if (nb == 4) k_moments_simt<double, 4><<<gr, 128, 0, s->stream>>>(s->nT, s->nq, s->Wm, s->psi64, out);
+            else if (nb == 9) k_moments_simt<double, 9><<<gr, 128, 0, s->stream>>>(s->nT, s->nq, s->Wm, s->psi64, out);
+            else k_moments_simt<double, 16><<<gr, 128, 0, s->stream>>>(s->nT, s->nq, s->Wm, s->psi64, out);
+            e = cudaGetLastError();
+            ++s->launches;
+        } else if (e == cudaSuccess) {
+            if (nb == 1) k_moments_simt<float, 1><<<gr, 128, 0, s->stream>>>(s->nT, s->nq, s->Wm, s->psi32, out);
+            else if (nb == 4) k_moments_simt<float, 4><<<gr, 128, 0, s->stream>>>(s->nT, s->nq, s->Wm, s->psi32, out);
+            else if (nb == 9) k_moments_simt<float, 9><<<gr, 128, 0, s->stream>>>(s->nT, s->nq, s->Wm, s->psi32, out);
+            else k_moments_simt<float, 16><<<gr, 128, 0, s->stream>>>(s->nT, s->nq, s->Wm, s->psi32, out);
+            e = cudaGetLastError();
+            ++s->launches;
+        }
+        if (e == cudaSuccess && tmp)
+            e = cudaMemcpyAsync(mom, tmp, sizeof(double) * nmom * 4ull * s->nT, cudaMemcpyDeviceToDevice, s->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+        if (tmp) cudaFree(tmp);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    return sw_cuda(s, e, "tr_sweep_moments");
+}
+
+tr_status tr_sweep_balance(tr_sweep *s, const double *J_in, const double *B_in, const double *J_out,
+                           double out[5]) {
+    SW_CHECK(s);
+    if (!J_out || !out) return sw_err(s, TR_ERR_INVALID_ARG, "tr_sweep_balance: null argument");
+    if (!s->last_prec) return sw_err(s, TR_ERR_INVALID_ARG, "tr_sweep_balance: no sweep has run");
+    BalanceArgs b;
+    b.nT = s->nT;
+    b.nq = s->nq;
+    b.nbf = s->nbf;
+    b.s = s->s64;
+    b.stv = s->stv64;
+    b.ssv = s->ssv64;
+    b.ext = s->ext64;
+    b.w = s->o64[3];
+    b.ox = s->o64[0];
+    b.oy = s->o64[1];
+    b.oz = s->o64[2];
+    b.finc = s->finc64;
+    b.fbc = s->fbc;
+    b.rslot = s->rslot;
+    b.bcell = s->bcell;
+    b.bface = s->bface;
+    b.Jin = J_in;
+    b.Jout = J_out;
+    b.Bin = s->nB ? B_in : nullptr;
+    if (s->last_prec == 64)
+        k_balance<double><<<kRedGrid, 256, 0, s->stream>>>(b, s->psi64, s->partials, s->counter, s->red);
+    else
+        k_balance<float><<<kRedGrid, 256, 0, s->stream>>>(b, s->psi32, s->partials, s->counter, s->red);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, s->red, 5 * sizeof(double), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    return sw_cuda(s, e, "tr_sweep_balance");
+}
+
+void tr_sweep_opts_default(tr_sweep_opts *o) {
+    if (!o) return;
+    o->method = TR_SWEEP_GMRES;
+    o->mode = TR_MODE_FP64;
+    o->tol = 1e-8;
+    o->max_iter = 1000;
+    o->restart = 30;
+    o->inner_tol = 0.0;
+    o->max_outer = 30;
+}
+
+tr_status tr_sweep_solve(tr_sweep *s, const tr_sweep_opts *opts, double *J, double *B, tr_sweep_report *rep) {
+    SW_CHECK(s);
+    if (!J) return sw_err(s, TR_ERR_INVALID_ARG, "tr_sweep_solve: null J");
+    tr_sweep_opts o;
+    tr_sweep_opts_default(&o);
+    if (opts) o = *opts;
+    if (o.restart < 1 || o.restart > kMaxRestart) return sw_err(s, TR_ERR_INVALID_ARG, "restart must be 1..64");
+    if (o.mode != TR_MODE_FP64 && o.mode != TR_MODE_MIXED) return sw_err(s, TR_ERR_INVALID_ARG, "bad mode");
+    if (o.method != TR_SWEEP_GMRES && o.method != TR_SWEEP_SOURCE_ITERATION)
+        return sw_err(s, TR_ERR_INVALID_ARG, "bad method");
+    const uint64_t n = s->nJ + s->nB;
+    cudaError_t e = krylov_alloc(s, o.restart);
+    if (e != cudaSuccess) return sw_cuda(s, e, "tr_sweep_solve: allocation");
+    cudaStream_t st = s->stream;
+    const int64_t s32_0 = s->sweeps32, s64_0 = s->sweeps64, l0 = s->launches;
+    cudaEventRecord(s->ev[0], st);
+    // b = S_64(0) with sources; x = 0
+    e = sweep_enqueue(s, 64, nullptr, nullptr, 1, s->kb, s->nB ? s->kb + s->nJ : nullptr);
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->kx, 0, n * 8, st);
+    double bn = 0.0;
+    if (e == cudaSuccess) e = vnorm(s, s->kb, &bn);
+    int its = 0, outer = 0;
+    double res = 0.0;
+    bool conv = false;
+    const int gr = grid_for(s, n);
+    if (e == cudaSuccess && bn == 0.0) conv = true;
+    if (e == cudaSuccess && !conv) {
+        if (o.method == TR_SWEEP_SOURCE_ITERATION) {
+            // x <- S(x) with sources, in the mode's sweep precision; change measured in FP64
+            const int prec = o.mode == TR_MODE_MIXED ? 32 : 64;
+            e = cudaMemcpyAsync(s->kx, s->kb, n * 8, cudaMemcpyDeviceToDevice, st);
+            while (e == cudaSuccess && its < o.max_iter) {
+                e = sweep_enqueue(s, prec, s->kx, s->nB ? s->kx + s->nJ : nullptr, 1, s->kt,
+                                  s->nB ? s->kt + s->nJ : nullptr);
+                ++its;
+                if (e != cudaSuccess) break;
+                k_axpby<<<gr, 256, 0, st>>>(n, 1.0, s->kt, -1.0, s->kx);  // kx = kt - kx
+                ++s->launches;
+                double dn = 0.0, tn = 0.0;
+                if ((e = vnorm(s, s->kx, &dn)) != cudaSuccess) break;
+                if ((e = vnorm(s, s->kt, &tn)) != cudaSuccess) break;
+                e = cudaMemcpyAsync(s->kx, s->kt, n * 8, cudaMemcpyDeviceToDevice, st);
+                res = tn > 0.0 ? dn / tn : 0.0;
+                if (res < o.tol) {
+                    conv = true;
+                    break;
+                }
+            }
+        } else if (o.mode == TR_MODE_FP64) {
+            e = gmres(s, 64, s->kb, s->kx, o.restart, o.tol, bn, o.max_iter, &its, &res);
+            conv = e == cudaSuccess && res <= o.tol;
+        } else {
+            // FP32 sweeps inside FP64 defect correction: r = b - (I - T_64) x;
+            // (I - T_32) d = r by GMRES; x += d
+            e = cudaMemcpyAsync(s->kr, s->kb, n * 8, cudaMemcpyDeviceToDevice, st);
+            double rn = bn;
+            while (e == cudaSuccess && outer < o.max_outer && its < o.max_iter) {
+                ++outer;
+                double want = o.inner_tol > 0.0 ? o.inner_tol : std::max(2e-6, 0.3 * o.tol * bn / rn);
+                want = std::min(want, 0.5);
+                e = cudaMemsetAsync(s->kd, 0, n * 8, st);
+                int it_in = 0;
+                double res_in = 0.0;
+                if (e == cudaSuccess) {
+                    // the correction accumulates in kd; its right-hand side is kr
+                    e = gmres(s, 32, s->kr, s->kd, o.restart, want, rn, o.max_iter - its, &it_in, &res_in);
+                }
+                its += it_in;
+                if (e != cudaSuccess) break;
+                k_axpby<<<gr, 256, 0, st>>>(n, 1.0, s->kd, 1.0, s->kx);
+                ++s->launches;
+                if ((e = op_apply(s, 64, s->kx, s->kr)) != cudaSuccess) break;
+                k_axpby<<<gr, 256, 0, st>>>(n, 1.0, s->kb, -1.0, s->kr);
+                ++s->launches;
+                if ((e = vnorm(s, s->kr, &rn)) != cudaSuccess) break;
+                res = rn / bn;
+                if (res <= o.tol) {
+                    conv = true;
+                    break;
+                }
+            }
+        }
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(J, s->kx, s->nJ * 8, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess && B && s->nB) e = cudaMemcpyAsync(B, s->kx + s->nJ, s->nB * 8, cudaMemcpyDeviceToDevice, st);
+    cudaEventRecord(s->ev[1], st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return sw_cuda(s, e, "tr_sweep_solve");
+    if (rep) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, s->ev[0], s->ev[1]);
+        rep->converged = conv ? 1 : 0;
+        rep->iterations = its;
+        rep->outer_steps = outer;
+        rep->sweeps_f32 = s->sweeps32 - s32_0;
+        rep->sweeps_f64 = s->sweeps64 - s64_0;
+        rep->residual = res;
+        rep->rhs_norm = bn;
+        rep->device_ms = ms;
+        rep->kernel_launches = s->launches - l0;
+    }
+    if (!conv) return sw_err(s, TR_ERR_NOT_CONVERGED, "tr_sweep_solve: not converged");
+    return TR_OK;
+}
+
+tr_status tr_sweep_bench(tr_sweep *s, int precision, int iters, double *ms_per_sweep) {
+    SW_CHECK(s);
+    if ((precision != 32 && precision != 64) || iters < 1 || !ms_per_sweep)
+        return sw_err(s, TR_ERR_INVALID_ARG, "tr_sweep_bench: bad arguments");
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < 3 && e == cudaSuccess; ++i) e = sweep_enqueue(s, precision, nullptr, nullptr, 1, nullptr, nullptr);
+    if (e == cudaSuccess) e = cudaEventRecord(s->ev[0], s->stream);
+    for (int i = 0; i < iters && e == cudaSuccess; ++i)
+        e = sweep_enqueue(s, precision, nullptr, nullptr, 1, nullptr, nullptr);
+    if (e == cudaSuccess) e = cudaEventRecord(s->ev[1], s->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(s->ev[1]);
+    if (e != cudaSuccess) return sw_cuda(s, e, "tr_sweep_bench");
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, s->ev[0], s->ev[1]);
+    *ms_per_sweep = ms / iters;
+    return TR_OK;
+}
+
+}  // extern "C"

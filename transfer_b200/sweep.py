@@ -1,0 +1,124 @@
+"""Discrete-ordinates transport sweep over the reference's problem data.
+
+``Sweep(device, MeshData, ordinates, physics)`` binds the C ABI's tr_sweep
+(include/transfer_b200.h): the linear-discontinuous upwind sweep over the
+`tetrahedron` / `face` records of MeshData (MeshData.h:13-32), with isotropic
+scattering (``Physics.kappa_abs_volume``), vacuum / reflective / incident
+faces (``Physics.face_bc``, ``face_incident``), GMRES or source iteration
+over the scattering source, FP64 or FP32-in-FP64 defect correction.  The
+reference has no sweep of its own.  Device vectors are torch CUDA tensors
+(torch is only the allocator); every computation runs in libtransfer_b200.so.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as L
+from ._lib import check, lib
+from .core import _ptr
+
+
+def ordinates_product(n_polar, n_azim):
+    """Gauss-Legendre (cos theta) x uniform azimuth ordinates: (x, y, z, w)."""
+    n = int(n_polar) * int(n_azim)
+    x, y, z, w = (np.zeros(n) for _ in range(4))
+    check(lib.tr_ordinates_product(int(n_polar), int(n_azim), _ptr(x), _ptr(y), _ptr(z), _ptr(w)))
+    return x, y, z, w
+
+
+class SweepReport(dict):
+    __getattr__ = dict.__getitem__
+
+
+class Sweep:
+    """Sweep(device, md, ordinates=(x, y, z, w), physics=None)."""
+
+    def __init__(self, device, md, ordinates, physics=None):
+        import torch  # device-memory plumbing only
+        self._torch = torch
+        self.ordinates = tuple(np.ascontiguousarray(a, dtype=np.float64) for a in ordinates)
+        self._keep = (md, physics, self.ordinates)
+        ov = L.tr_ordinates_view()
+        ov.nq = len(self.ordinates[3])
+        ov.x, ov.y, ov.z, ov.w = (_ptr(a) for a in self.ordinates)
+        mv = md.view()
+        pv = physics.view() if physics is not None else None
+        h = C.c_void_p()
+        check(lib.tr_sweep_create(int(device), C.byref(mv), C.byref(pv) if pv is not None else None, C.byref(ov),
+                                  C.byref(h)))
+        self._h = h
+        info = L.tr_sweep_info()
+        check(lib.tr_sweep_info_get(h, C.byref(info)))
+        self.nT, self.nF, self.nq = info.nT, info.nF, info.nq
+        self.n_extra, self.n_reflective, self.n_lag = info.n_extra, info.n_reflective, info.n_lag
+        self.max_levels, self.forced_levels, self.device_bytes = info.max_levels, info.forced_levels, info.device_bytes
+        self.device = device
+
+    def _c(self, st):
+        if st != L.TR_OK:
+            msg = lib.tr_sweep_last_error(self._h)
+            raise L.TransferError(st, msg.decode() if msg else lib.tr_status_string(st).decode())
+        return st
+
+    def _dev(self, n, dtype=None):
+        t = self._torch
+        return t.zeros(max(int(n), 1), dtype=dtype or t.float64, device=f"cuda:{self.device}")
+
+    def vector_J(self):
+        return self._dev(4 * self.nT)
+
+    def vector_B(self):
+        return self._dev(self.n_extra)
+
+    def levels(self):
+        lv = np.zeros(self.nq * self.nT, dtype=np.int32)
+        self._c(lib.tr_sweep_levels(self._h, _ptr(lv)))
+        return lv.reshape(self.nq, self.nT)
+
+    def apply(self, J=None, B=None, with_ext=True, precision=64):
+        """One sweep; returns (J_out [nT,4], B_out [n_extra]) as device tensors."""
+        Jo, Bo = self.vector_J(), self.vector_B()
+        self._c(lib.tr_sweep_apply(self._h, int(precision), _ptr(J), _ptr(B), int(bool(with_ext)), _ptr(Jo),
+                                   _ptr(Bo)))
+        return Jo.view(self.nT, 4), Bo[:self.n_extra]
+
+    def psi(self):
+        out = self._dev(4 * self.nq * self.nT)
+        self._c(lib.tr_sweep_psi(self._h, _ptr(out)))
+        return out.view(self.nq, self.nT, 4)
+
+    def moments(self, nmom=16):
+        out = self._dev(nmom * 4 * self.nT)
+        self._c(lib.tr_sweep_moments(self._h, int(nmom), _ptr(out)))
+        return out.view(nmom, self.nT, 4)
+
+    def balance(self, J_in, B_in, J_out):
+        out = (C.c_double * 5)()
+        self._c(lib.tr_sweep_balance(self._h, _ptr(J_in), _ptr(B_in), _ptr(J_out), out))
+        return dict(emitted=out[0], absorbed=out[1], escaped=out[2], incoming=out[3], reflective_net=out[4])
+
+    def solve(self, raise_on_error=True, **kw):
+        """Returns (J [nT,4], B [n_extra], report)."""
+        o = L.tr_sweep_opts()
+        lib.tr_sweep_opts_default(C.byref(o))
+        for k, v in kw.items():
+            if not hasattr(o, k):
+                raise KeyError(k)
+            setattr(o, k, v)
+        J, B = self.vector_J(), self.vector_B()
+        rep = L.tr_sweep_report()
+        st = lib.tr_sweep_solve(self._h, C.byref(o), _ptr(J), _ptr(B), C.byref(rep))
+        report = SweepReport({f: getattr(rep, f) for f, _ in L.tr_sweep_report._fields_})
+        if st != L.TR_OK and (raise_on_error or st != L.TR_ERR_NOT_CONVERGED):
+            self._c(st)
+        return J.view(self.nT, 4), B[:self.n_extra], report
+
+    def bench(self, precision=32, iters=20):
+        ms = C.c_double()
+        self._c(lib.tr_sweep_bench(self._h, int(precision), int(iters), C.byref(ms)))
+        return ms.value
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib.tr_sweep_destroy(self._h)
+            self._h = None
