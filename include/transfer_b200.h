@@ -405,6 +405,24 @@ void tr_sweep_opts_default(tr_sweep_opts *opts);
  * (I - T) x = S(0) or by source iteration; J [nT][4], B [n_extra] device
  * outputs (B may be NULL). */
 tr_status tr_sweep_solve(tr_sweep *s, const tr_sweep_opts *opts, double *J, double *B, tr_sweep_report *rep);
+/* Outflow of the last sweep through the boundary faces with face_mask[f]
+ * != 0 (HOST array [nF]): F = sum_q w_q sum_f max(Omega_q.s_f, 0) mean_f psi_q
+ * (mean intensity x area), FP64. */
+tr_status tr_sweep_outflow(tr_sweep *s, const int32_t *face_mask, double *F);
+/* Adjoint gradient of F (the outflow through a face set) with respect to
+ * each cell's absorption and scattering coefficients sigma_a, sigma_s
+ * (sigma_t = sigma_a + sigma_s, volumes fixed).  `adj` is the adjoint
+ * problem: a sweep over the same mesh and coefficients with the ordinates
+ * reversed (-Omega_q, same order and weights), no emission (I_p = 0),
+ * unit isotropic inflow (TR_BC_INCIDENT, 1) on F's faces and vacuum
+ * elsewhere -- the transpose of the upwind sweep is the sweep in the
+ * reversed direction.  J, B: the converged forward solution; J_adj: the
+ * converged adjoint scalar flux (tr_sweep_solve on adj).  Only the scalar
+ * fluxes are kept between the solves: both angular fluxes are recomputed
+ * here by one sweep each (precision 32 or 64).  Outputs: device [nT].
+ * Faces must be vacuum or incident (no reflective faces, no cut cycles). */
+tr_status tr_sweep_gradient(tr_sweep *fwd, tr_sweep *adj, int precision, const double *J, const double *B,
+                            const double *J_adj, double *dF_dsigma_a, double *dF_dsigma_s);
 /* Measurement helper: mean device time of one sweep with sources (3
  * untimed sweeps first). */
 tr_status tr_sweep_bench(tr_sweep *s, int precision, int iters, double *ms_per_sweep);

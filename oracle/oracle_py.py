@@ -70,6 +70,7 @@ def _load():
         "oracle_sweep_balance": (None, [P, P, P, P, P]),
         "oracle_sweep_moments": (None, [P, P, C.c_int, P]),
         "oracle_ordinates_product": (None, [C.c_int, C.c_int, P, P, P, P]),
+        "oracle_sweep_outflow": (D, [P, P, P]),
         "oracle_num_threads": (C.c_int, []),
         "oracle_set_num_threads": (None, [C.c_int]),
     }
@@ -269,6 +270,10 @@ class SweepOracle:
                                  _p(out))
         return dict(emitted=out[0], absorbed=out[1], escaped=out[2], incoming=out[3], reflective_net=out[4])
 
+    def outflow(self, psi, face_mask):
+        m = np.ascontiguousarray(face_mask, dtype=np.int32)
+        return lib.oracle_sweep_outflow(self.h, _p(np.ascontiguousarray(psi, dtype=np.float64).reshape(-1)), _p(m))
+
     def moments(self, psi, nmom=16):
         mom = np.zeros(nmom * 4 * self.nT)
         lib.oracle_sweep_moments(self.h, _p(np.ascontiguousarray(psi, dtype=np.float64).reshape(-1)), int(nmom),
@@ -279,3 +284,45 @@ class SweepOracle:
         if getattr(self, "h", None):
             lib.oracle_sweep_destroy(self.h)
             self.h = None
+
+
+def tet_volumes(md):
+    """V from the face area normals: |det(s_1, s_2, s_3)| = 9 V^2 / 2."""
+    s = md.mesh["s"]
+    return np.sqrt(np.abs(np.linalg.det(s[:, 1:4, :])) / 4.5)
+
+
+def sweep_adjoint_gradient(md, ordinates, kappa_abs_volume, face_bc, face_incident, face_mask, tol=1e-13):
+    """FP64 reference for the adjoint gradient of the outflow F through
+    face_mask's faces with respect to each cell's sigma_a and sigma_s:
+    forward and adjoint (reversed ordinates, unit inflow on the functional's
+    faces, no emission) solves by the oracle, then per cell
+      G = sum_q w_q mu_q^T M psi_q,  M = (1 + d_ij)/20,
+      dF/dsigma_a = V (B/4) sum_i Phi_i - V G,  dF/dsigma_s = V Phi^T M J - V G.
+    Returns (F, dsa, dss)."""
+    x, y, z, w = (np.asarray(a, dtype=np.float64) for a in ordinates)
+    Of = SweepOracle(md, (x, y, z, w), kappa_abs_volume=kappa_abs_volume, face_bc=face_bc,
+                     face_incident=face_incident)
+    J, B, info = Of.solve(method=1, tol=tol)
+    _, _, psi = Of.apply(J, B, want_psi=True)
+    F = Of.outflow(psi, face_mask)
+    mesh = md.mesh.copy()
+    mesh["I_p"] = 0.0
+
+    class _Adj:  # the adjoint problem's mesh: same arrays, no emission
+        pass
+    ma = _Adj()
+    ma.nT, ma.nF, ma.mesh, ma.bnd = md.nT, md.nF, mesh, md.bnd
+    mask = np.asarray(face_mask) != 0
+    Oa = SweepOracle(ma, (-x, -y, -z, w), kappa_abs_volume=kappa_abs_volume,
+                     face_bc=np.where(mask, 2, 0).astype(np.int32), face_incident=mask.astype(np.float64))
+    Ja, _, _ = Oa.solve(method=1, tol=tol)
+    _, _, mu = Oa.apply(Ja, None, want_psi=True)
+    G = np.einsum("q,qcj,qcj->c", w, mu, psi) + np.einsum("q,qc,qc->c", w, mu.sum(axis=2), psi.sum(axis=2))
+    G /= 20.0
+    V = tet_volumes(md)
+    Bp = md.mesh["I_p"]
+    PJ = ((Ja * J).sum(axis=1) + Ja.sum(axis=1) * J.sum(axis=1)) / 20.0
+    dsa = V * (Bp / 4.0 * Ja.sum(axis=1) - G)
+    dss = V * (PJ - G)
+    return F, dsa, dss

@@ -657,3 +657,21 @@ void oracle_sweep_moments(const or_sweep *S, const double *psi, int nmom, double
             }
     free(Y);
 }
+
+double oracle_sweep_outflow(const or_sweep *S, const double *psi, const int32_t *face_mask) {
+    uint32_t nT = S->nT, nq = S->nq;
+    double F = 0.0;
+    for (uint32_t c = 0; c < nT; c++)
+        for (int k = 0; k < 4; k++) {
+            int64_t nb = S->nbr[4 * c + k];
+            if (nb >= 0 || !face_mask[-nb - 1]) continue;
+            for (uint32_t q = 0; q < nq; q++) {
+                double d = odots(S, q, c, k), m = 0.0;
+                if (!(d > 0.0)) continue;
+                for (int j = 0; j < 4; j++)
+                    if (j != k) m += psi[4 * ((size_t)q * nT + c) + j];
+                F += S->w[q] * d * m / 3.0;
+            }
+        }
+    return F;
+}

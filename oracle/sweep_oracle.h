@@ -96,6 +96,10 @@ void oracle_sweep_balance(const or_sweep *s, const double *J_in, const double *B
  * (Y_00 = 1). */
 void oracle_sweep_moments(const or_sweep *s, const double *psi, int nmom, double *mom);
 
+/* Outflow through the boundary faces with face_mask[f] != 0:
+ * sum_q w_q sum_f max(Omega_q.s_f, 0) mean_f psi_q. */
+double oracle_sweep_outflow(const or_sweep *s, const double *psi, const int32_t *face_mask);
+
 /* Product ordinate set: Gauss-Legendre in mu (n_polar) x uniform azimuth
  * (n_azim, phi_k = (k + 1/2) 2 pi / n_azim), weights summing to 1. */
 void oracle_ordinates_product(int n_polar, int n_azim, double *x, double *y, double *z, double *w);

@@ -57,3 +57,32 @@ def e2_slab_exact(x, a):
     inside = 0.5 * ((1.0 - expn(2, np.maximum(x, 0))) + (1.0 - expn(2, np.maximum(a - x, 0))))
     outside = 0.5 * (expn(2, np.maximum(x - a, 0)) - expn(2, np.maximum(x, 0)))
     return np.where(x < a, inside, outside)
+
+
+def adjoint_box(n=(4, 3, 3), jitter=0.2):
+    """Vacuum box with a scattering, emitting sphere (sigma_t 2, albedo 0.6,
+    B = 1) in a thinner scattering medium (sigma_t 0.5, albedo 0.3, B = 0.1)
+    and isotropic inflow 0.5 through x = 0; the functional is the outflow
+    through the faces at x = 1."""
+    md = tr.MeshData.kuhn(n, jitter=jitter, seed=SEED, kappa=[0.0, 2.0, 0.5], Ip=[0.0, 1.0, 0.1],
+                          albedo=[0.0, 0.6, 0.3], region_kind=1, region_arg=(0.5, 0.5, 0.5, 0.3))
+    side = md.face_side
+    bc = np.where(side == 0, tr.TR_BC_INCIDENT, tr.TR_BC_VACUUM).astype(np.int32)
+    ph = tr.Physics(kappa_abs_volume=md.kappa_abs_volume, face_bc=bc, face_incident=np.where(side == 0, 0.5, 0.0))
+    return md, ph, (side == 1).astype(np.int32)
+
+
+def perturbed(md, ph, cell, d_sigma_a=0.0, d_sigma_s=0.0):
+    """The problem with cell's sigma_a / sigma_s changed (volume fixed)."""
+    import oracle_py as op
+    V = op.tet_volumes(md)[cell]
+    mesh = md.mesh.copy()
+    mesh["kappa_volume"][cell] += (d_sigma_a + d_sigma_s) * V
+    kav = ph.kappa_abs_volume.copy()
+    kav[cell] += d_sigma_a * V
+
+    class _M:
+        pass
+    m = _M()
+    m.nT, m.nF, m.mesh, m.bnd = md.nT, md.nF, mesh, md.bnd
+    return m, kav

@@ -152,3 +152,25 @@ def test_bad_arguments_are_rejected(cuda):
     x, y, z, w = tr.ordinates_product(2, 5)
     with pytest.raises(tr.TransferError):
         tr.Sweep(0, md, (x, y, z, w), ph)
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_adjoint_gradient_matches_oracle(cuda, precision):
+    from sweep_cases import adjoint_box
+    md, ph, mask = adjoint_box()
+    ords = tr.ordinates_product(4, 8)
+    mode = tr.TR_MODE_FP64 if precision == 64 else tr.TR_MODE_MIXED
+    F, dsa, dss, rep, rep_a = tr.adjoint_gradient(0, md, ords, ph, mask, precision=precision, mode=mode, tol=1e-11)
+    Fo, dsa_o, dss_o = op.sweep_adjoint_gradient(md, ords, ph.kappa_abs_volume, ph.face_bc, ph.face_incident, mask)
+    assert rep.converged and rep_a.converged
+    assert abs(F - Fo) < 1e-10 * abs(Fo)
+    tol = 1e-9 if precision == 64 else 2e-5
+    assert rel_err(host(dsa), dsa_o) < tol
+    assert rel_err(host(dss), dss_o) < tol
+
+
+def test_adjoint_gradient_rejects_reflective_faces(cuda):
+    md, ph = scattering_box(n=(2, 2, 2))
+    ords = tr.ordinates_product(2, 4)
+    with pytest.raises(tr.TransferError):
+        tr.adjoint_gradient(0, md, ords, ph, (md.face_side == 1).astype(np.int32))

@@ -136,3 +136,26 @@ def test_moments_l0_is_scalar_flux():
     x, y, z, w = S.ox, S.oy, S.oz, S.w
     Fx = np.einsum("q,q,qcj->cj", w, x, psi)
     assert np.abs(mom[3] - np.sqrt(3) * Fx).max() < 1e-13
+
+
+def test_adjoint_gradient_matches_central_differences():
+    from sweep_cases import adjoint_box, perturbed
+    md, ph, mask = adjoint_box()
+    ords = op.ordinates_product(4, 8)
+    F, dsa, dss = op.sweep_adjoint_gradient(md, ords, ph.kappa_abs_volume, ph.face_bc, ph.face_incident, mask)
+    rng = np.random.default_rng(7)
+    for c in rng.choice(md.nT, 6, replace=False):
+        for which in ("a", "s"):
+            sig = (ph.kappa_abs_volume[c] if which == "a" else md.mesh["kappa_volume"][c] - ph.kappa_abs_volume[c])
+            h = 1e-4 * sig / op.tet_volumes(md)[c]
+            Fs = []
+            for sgn in (1, -1):
+                kw = {"d_sigma_a": sgn * h} if which == "a" else {"d_sigma_s": sgn * h}
+                m, kav = perturbed(md, ph, c, **kw)
+                O = op.SweepOracle(m, ords, kappa_abs_volume=kav, face_bc=ph.face_bc, face_incident=ph.face_incident)
+                J, B, info = O.solve(method=1, tol=1e-13)
+                _, _, psi = O.apply(J, B, want_psi=True)
+                Fs.append(O.outflow(psi, mask))
+            fd = (Fs[0] - Fs[1]) / (2 * h)
+            g = dsa[c] if which == "a" else dss[c]
+            assert abs(g - fd) < 1e-6 * max(abs(fd), 1e-3 * abs(F)), (c, which, g, fd)

@@ -600,6 +600,60 @@ __global__ void __launch_bounds__(32 * kMomWarps) k_moments_tf32x3(uint32_t M, u
     }
 }
 
+// Adjoint gradient of a boundary functional F (outflow through a set of
+// faces).  With mu_q the adjoint angular flux (the sweep in the reversed
+// ordinate -Omega_q, unit isotropic inflow on the functional's faces, no
+// volume source) and Phi = sum_q w_q mu_q its scalar flux, per cell
+//   G     = sum_q w_q mu_q^T M psi_q,          M = (1 + d_ij) / 20,
+//   dF/dsigma_a = V (B/4) sum_i Phi_i - V G,
+//   dF/dsigma_s = V Phi^T M J       - V G     (sigma_t = sigma_a + sigma_s).
+template <typename T>
+__global__ void k_gradient(uint32_t nT, uint32_t nq, const double *w, const T *psi, const T *mu, const double *J,
+                           const double *Phi, const double *vol, const double *Bp, double *dsa, double *dss) {
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nT; c += gridDim.x * blockDim.x) {
+        double G = 0.0;
+        for (uint32_t q = 0; q < nq; ++q) {
+            const typename Vec4<T>::type p = load_v4<T>(psi + ((size_t)q * nT + c) * 4);
+            const typename Vec4<T>::type m = load_v4<T>(mu + ((size_t)q * nT + c) * 4);
+            const double pp[4] = {(double)p.x, (double)p.y, (double)p.z, (double)p.w};
+            const double mm[4] = {(double)m.x, (double)m.y, (double)m.z, (double)m.w};
+            const double dot = mm[0] * pp[0] + mm[1] * pp[1] + mm[2] * pp[2] + mm[3] * pp[3];
+            const double sum = (mm[0] + mm[1] + mm[2] + mm[3]) * (pp[0] + pp[1] + pp[2] + pp[3]);
+            G += w[q] * (dot + sum) / 20.0;
+        }
+        const double *jc = J + 4 * (size_t)c, *fc = Phi + 4 * (size_t)c;
+        const double pj = (fc[0] * jc[0] + fc[1] * jc[1] + fc[2] * jc[2] + fc[3] * jc[3] +
+                           (fc[0] + fc[1] + fc[2] + fc[3]) * (jc[0] + jc[1] + jc[2] + jc[3])) / 20.0;
+        const double V = vol[c];
+        dsa[c] = V * (Bp[c] / 4.0 * (fc[0] + fc[1] + fc[2] + fc[3]) - G);
+        dss[c] = V * (pj - G);
+    }
+}
+
+// sum_q w_q sum_{masked boundary faces, Omega.s > 0} (Omega.s) mean_face(psi_q)
+template <typename T>
+__global__ void k_outflow(uint32_t nT, uint32_t nq, uint32_t nbf, const uint32_t *bcell, const uint32_t *bface,
+                          const uint8_t *fmask, const double *s, const double *ox, const double *oy, const double *oz,
+                          const double *w, const T *psi, double *partials, unsigned int *counter, double *out) {
+    double v[1] = {0.0};
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nbf; i += gridDim.x * blockDim.x) {
+        if (!fmask[bface[i]]) continue;
+        const uint32_t c = bcell[i] >> 2, k = bcell[i] & 3u;
+        const double *sk = s + 12 * (size_t)c + 3 * k;
+        for (uint32_t q = 0; q < nq; ++q) {
+            const double d = odot_rn(ox[q], oy[q], oz[q], sk);
+            if (!(d > 0.0)) continue;
+            const T *pp = psi + ((size_t)q * nT + c) * 4;
+            double m = 0.0;
+            for (uint32_t j = 0; j < 4; ++j)
+                if (j != k) m += static_cast<double>(pp[j]);
+            v[0] += w[q] * d * m / 3.0;
+        }
+    }
+    double tot[1];
+    if (grid_reduce<1>(v, partials, counter, tot) && threadIdx.x == 0) out[0] = tot[0];
+}
+
 // ---- FP64 vector kernels of the Krylov solver --------------------------------
 __global__ void k_to_f32(uint64_t n, const double *x, float *y) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
@@ -737,6 +791,8 @@ struct tr_sweep {
     double *o64[4] = {nullptr, nullptr, nullptr, nullptr};  // x y z w
     float *o32[3] = {nullptr, nullptr, nullptr};
     double *Wm = nullptr;          // [16][nq] w_q Y_m(Omega_q)
+    double *vol64 = nullptr, *B64 = nullptr;  // cell volume, Planck intensity
+    std::vector<double> ord_host;  // x, y, z, w of the ordinates
     // schedule
     uint4 *task = nullptr;
     uint32_t *lvl = nullptr, *nlev = nullptr;
@@ -830,10 +886,16 @@ static tr_status sweep_setup(tr_sweep *S, const tr_mesh_view *m, const tr_physic
     S->nF = nF;
     S->nq = nq;
     S->nJ = 4ull * nT;
-    std::vector<double> s(12ull * nT), stv(nT), ssv(nT), ext(nT);
+    std::vector<double> s(12ull * nT), stv(nT), ssv(nT), ext(nT), vol(nT), bpl(nT);
     for (uint32_t c = 0; c < nT; ++c) {
         const tr_tetrahedron &t = m->mesh[c];
         std::memcpy(&s[12ull * c], t.s, sizeof(double) * 12);
+        // |det(s_1, s_2, s_3)| = 9 V^2 / 2 for the face area normals of a tetrahedron
+        const double *a = t.s[1], *b2 = t.s[2], *c3 = t.s[3];
+        const double det = a[0] * (b2[1] * c3[2] - b2[2] * c3[1]) - a[1] * (b2[0] * c3[2] - b2[2] * c3[0]) +
+                           a[2] * (b2[0] * c3[1] - b2[1] * c3[0]);
+        vol[c] = std::sqrt(std::fabs(det) / 4.5);
+        bpl[c] = t.I_p;
         const double sav = (ph && ph->kappa_abs_volume) ? ph->kappa_abs_volume[c] : t.kappa_volume;
         if (!(t.kappa_volume > 0.0) || sav < 0.0 || sav > t.kappa_volume * (1.0 + 1e-12))
             return sw_err(S, TR_ERR_MESH, "sweep: need kappa_volume > 0 and 0 <= sigma_a V <= sigma_t V");
@@ -963,8 +1025,12 @@ static tr_status sweep_setup(tr_sweep *S, const tr_mesh_view *m, const tr_physic
     UP(s32, f32(s)) UP(stv32, f32(stv)) UP(ssv32, f32(ssv)) UP(ext32, f32(ext)) UP(finc32, f32(finc))
     UP(nbr, nbr) UP(fbc, fbc) UP(rslot, rslot) UP(map, map) UP(rinv, rinv) UP(bcell, bcell) UP(bface, bface)
     UP(o64[0], ox) UP(o64[1], oy) UP(o64[2], oz) UP(o64[3], w) UP(o32[0], ox32) UP(o32[1], oy32) UP(o32[2], oz32)
-    UP(Wm, Wm)
+    UP(Wm, Wm) UP(vol64, vol) UP(B64, bpl)
 #undef UP
+    S->ord_host.assign(o->x, o->x + nq);
+    S->ord_host.insert(S->ord_host.end(), o->y, o->y + nq);
+    S->ord_host.insert(S->ord_host.end(), o->z, o->z + nq);
+    S->ord_host.insert(S->ord_host.end(), o->w, o->w + nq);
     if (e != cudaSuccess) return sw_cuda(S, e, "sweep: upload");
     // ---- schedule on the device
     SchedBuild b;
@@ -1672,6 +1738,67 @@ tr_status tr_sweep_solve(tr_sweep *s, const tr_sweep_opts *opts, double *J, doub
     }
     if (!conv) return sw_err(s, TR_ERR_NOT_CONVERGED, "tr_sweep_solve: not converged");
     return TR_OK;
+}
+
+tr_status tr_sweep_outflow(tr_sweep *s, const int32_t *face_mask, double *F) {
+    SW_CHECK(s);
+    if (!face_mask || !F) return sw_err(s, TR_ERR_INVALID_ARG, "tr_sweep_outflow: null argument");
+    if (!s->last_prec) return sw_err(s, TR_ERR_INVALID_ARG, "tr_sweep_outflow: no sweep has run");
+    std::vector<uint8_t> m(s->nF + 1, 0);
+    for (uint32_t f = 0; f < s->nF; ++f) m[f] = face_mask[f] != 0;
+    uint8_t *dm = nullptr;
+    cudaError_t e = cudaMalloc(&dm, m.size());
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dm, m.data(), m.size(), cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess) {
+        if (s->last_prec == 64)
+            k_outflow<double><<<kRedGrid, 256, 0, s->stream>>>(s->nT, s->nq, s->nbf, s->bcell, s->bface, dm, s->s64,
+                                                               s->o64[0], s->o64[1], s->o64[2], s->o64[3], s->psi64,
+                                                               s->partials, s->counter, s->red);
+        else
+            k_outflow<float><<<kRedGrid, 256, 0, s->stream>>>(s->nT, s->nq, s->nbf, s->bcell, s->bface, dm, s->s64,
+                                                              s->o64[0], s->o64[1], s->o64[2], s->o64[3], s->psi32,
+                                                              s->partials, s->counter, s->red);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(F, s->red, sizeof(double), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (dm) cudaFree(dm);
+    return sw_cuda(s, e, "tr_sweep_outflow");
+}
+
+tr_status tr_sweep_gradient(tr_sweep *fwd, tr_sweep *adj, int precision, const double *J, const double *B,
+                            const double *J_adj, double *dF_dsigma_a, double *dF_dsigma_s) {
+    SW_CHECK(fwd);
+    if (!adj || !J || !J_adj || !dF_dsigma_a || !dF_dsigma_s)
+        return sw_err(fwd, TR_ERR_INVALID_ARG, "tr_sweep_gradient: null argument");
+    if (precision != 32 && precision != 64) return sw_err(fwd, TR_ERR_INVALID_ARG, "precision must be 32 or 64");
+    if (adj->device != fwd->device || adj->nT != fwd->nT || adj->nq != fwd->nq)
+        return sw_err(fwd, TR_ERR_INVALID_ARG, "tr_sweep_gradient: adjoint sweep of another problem");
+    const uint32_t nq = fwd->nq;
+    for (uint32_t q = 0; q < nq; ++q)
+        for (int d = 0; d < 3; ++d)
+            if (adj->ord_host[d * nq + q] != -fwd->ord_host[d * nq + q])
+                return sw_err(fwd, TR_ERR_INVALID_ARG, "tr_sweep_gradient: the adjoint ordinates must be -Omega_q");
+    if (fwd->nrefl || fwd->nlag || adj->nrefl || adj->nlag)
+        return sw_err(fwd, TR_ERR_UNSUPPORTED,
+                      "tr_sweep_gradient: reflective faces and cut dependency cycles are not supported");
+    // forward angular flux recomputed from the converged (checkpointed) J, B;
+    // adjoint angular flux from the adjoint scalar flux
+    cudaError_t e = sweep_enqueue(fwd, precision, J, B, 1, nullptr, nullptr);
+    if (e == cudaSuccess) e = sweep_enqueue(adj, precision, J_adj, nullptr, 1, nullptr, nullptr);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(adj->stream);
+    if (e == cudaSuccess) {
+        const int gr = grid_for(fwd, fwd->nT);
+        if (precision == 64)
+            k_gradient<double><<<gr, 256, 0, fwd->stream>>>(fwd->nT, nq, fwd->o64[3], fwd->psi64, adj->psi64, J, J_adj,
+                                                            fwd->vol64, fwd->B64, dF_dsigma_a, dF_dsigma_s);
+        else
+            k_gradient<float><<<gr, 256, 0, fwd->stream>>>(fwd->nT, nq, fwd->o64[3], fwd->psi32, adj->psi32, J, J_adj,
+                                                           fwd->vol64, fwd->B64, dF_dsigma_a, dF_dsigma_s);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(fwd->stream);
+    return sw_cuda(fwd, e, "tr_sweep_gradient");
 }
 
 tr_status tr_sweep_bench(tr_sweep *s, int precision, int iters, double *ms_per_sweep) {

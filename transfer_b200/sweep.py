@@ -113,6 +113,13 @@ class Sweep:
             self._c(st)
         return J.view(self.nT, 4), B[:self.n_extra], report
 
+    def outflow(self, face_mask):
+        """Outflow of the last sweep through the faces with face_mask != 0."""
+        m = np.ascontiguousarray(face_mask, dtype=np.int32)
+        F = C.c_double()
+        self._c(lib.tr_sweep_outflow(self._h, _ptr(m), C.byref(F)))
+        return F.value
+
     def bench(self, precision=32, iters=20):
         ms = C.c_double()
         self._c(lib.tr_sweep_bench(self._h, int(precision), int(iters), C.byref(ms)))
@@ -122,3 +129,37 @@ class Sweep:
         if getattr(self, "_h", None):
             lib.tr_sweep_destroy(self._h)
             self._h = None
+
+
+def adjoint_problem(md, physics, face_mask):
+    """The adjoint of the outflow functional through face_mask's faces: the
+    same mesh and coefficients without emission, unit isotropic inflow on
+    those faces, vacuum elsewhere (the sweep runs in reversed ordinates)."""
+    from .core import MeshData, Physics
+    mesh = md.mesh.copy()
+    mesh["I_p"] = 0.0
+    md_adj = MeshData.from_arrays(tetstart=md.tetstart, tetidx=md.tetidx, tetpos=md.tetpos, facestart=md.facestart,
+                                  faceidx=md.faceidx, facepos=md.facepos, mesh=mesh, bnd=md.bnd, coords=md.coords,
+                                  regions=md.regions, kappa_abs_volume=md.kappa_abs_volume, face_side=md.face_side)
+    mask = np.asarray(face_mask) != 0
+    bc = np.where(mask, L.TR_BC_INCIDENT, L.TR_BC_VACUUM).astype(np.int32)
+    kav = None if physics is None else physics.kappa_abs_volume
+    return md_adj, Physics(kappa_abs_volume=kav, face_bc=bc, face_incident=mask.astype(np.float64))
+
+
+def adjoint_gradient(device, md, ordinates, physics, face_mask, precision=64, mode=L.TR_MODE_FP64, tol=1e-10,
+                     restart=30, fwd=None):
+    """Outflow F through face_mask's faces and its gradient with respect to
+    every cell's sigma_a and sigma_s.  Returns (F, dF/dsigma_a, dF/dsigma_s,
+    forward report, adjoint report); the gradients are device tensors [nT]."""
+    x, y, z, w = (np.ascontiguousarray(a, dtype=np.float64) for a in ordinates)
+    fwd = fwd or Sweep(device, md, (x, y, z, w), physics)
+    md_adj, ph_adj = adjoint_problem(md, physics, face_mask)
+    adj = Sweep(device, md_adj, (-x, -y, -z, w), ph_adj)
+    J, B, rep = fwd.solve(mode=mode, tol=tol, restart=restart)
+    Ja, _, rep_a = adj.solve(mode=mode, tol=tol, restart=restart)
+    fwd.apply(J, B, precision=64)
+    F = fwd.outflow(face_mask)
+    dsa, dss = fwd._dev(fwd.nT), fwd._dev(fwd.nT)
+    fwd._c(lib.tr_sweep_gradient(fwd._h, adj._h, int(precision), _ptr(J), _ptr(B), _ptr(Ja), _ptr(dsa), _ptr(dss)))
+    return F, dsa[:fwd.nT], dss[:fwd.nT], rep, rep_a
