@@ -326,9 +326,11 @@ double tr_trieig(const double *a, const double *b, int n);
  * (values at its 4 vertices), upwind between cells.  The unknowns of the
  * outer iteration are the scalar flux J[nT][4] (mean intensity at each
  * cell's vertices, J = sum_q w_q psi_q) and the extra vector B[n_extra]:
- * the inflow through reflective faces ([n_reflective][nq][4]) and through
- * faces where a dependency cycle was cut ([n_lag][4]).  All vectors are
- * FP64 DEVICE pointers. */
+ * the inflow through reflective faces (4 values for each pair of a
+ * reflective face and an ordinate entering through it, in (face, ordinate)
+ * order) and through faces where a dependency cycle was cut ([n_lag][4]).
+ * All vectors are FP64 DEVICE pointers, 16-byte aligned (TR_ERR_INVALID_ARG
+ * otherwise). */
 typedef struct tr_sweep tr_sweep;
 typedef struct tr_ordinates_view {
     uint32_t nq;
@@ -354,7 +356,8 @@ typedef struct tr_sweep_opts {
                                   source iteration: relative change        */
     int32_t max_iter;          /* sweeps of the iteration (Krylov steps)   */
     int32_t restart;           /* GMRES restart length, 1..64              */
-    double  inner_tol;         /* mixed: FP32 solve reduction (0: adaptive)*/
+    double  inner_tol;         /* mixed: FP32 solve reduction (0: adaptive,
+                                  0.3 x what is missing, at least 1e-4)    */
     int32_t max_outer;         /* mixed: defect-correction steps           */
 } tr_sweep_opts;
 typedef struct tr_sweep_report {

@@ -26,6 +26,8 @@ struct or_sweep {
     int64_t *rslot;     /* [nF] reflective slot or -1 */
     uint32_t nrefl;
     uint32_t *rmap;     /* [nrefl][nq] mirrored ordinate of an incoming q (NONE if outgoing) */
+    uint32_t *rent;     /* [nrefl][nq] B entry of an incoming q (NONE if outgoing) */
+    uint32_t nent;      /* reflective B entries: (slot, incoming q) in that order */
     double *ox, *oy, *oz, *w;
     /* schedule */
     uint32_t *order;    /* [nq][nT] */
@@ -246,6 +248,9 @@ or_sweep *oracle_sweep_create(const or_sweep_mesh *m, uint32_t nq, const double 
                 S->rmap[(size_t)S->rslot[f] * nq + q] = best;
             }
         }
+    S->rent = (uint32_t *)malloc(sizeof(uint32_t) * ((size_t)S->nrefl * nq + 1));
+    S->nent = 0;
+    for (size_t i = 0; i < (size_t)S->nrefl * nq; i++) S->rent[i] = S->rmap[i] == NONE ? NONE : S->nent++;
     build_schedule(S);
     return S;
 }
@@ -253,7 +258,7 @@ or_sweep *oracle_sweep_create(const or_sweep_mesh *m, uint32_t nq, const double 
 void oracle_sweep_destroy(or_sweep *S) {
     if (!S) return;
     free(S->s); free(S->stv); free(S->sav); free(S->B); free(S->nbr); free(S->map);
-    free(S->bc); free(S->inc); free(S->rslot); free(S->rmap);
+    free(S->bc); free(S->inc); free(S->rslot); free(S->rmap); free(S->rent);
     free(S->ox); free(S->oy); free(S->oz); free(S->w);
     free(S->order); free(S->level); free(S->lagbase); free(S->lag_qck);
     free(S);
@@ -351,7 +356,8 @@ static void build_schedule(or_sweep *S) {
     free(lagged);
 }
 
-static inline uint64_t blen(const or_sweep *S) { return (uint64_t)S->nrefl * S->nq * 4 + (uint64_t)S->nlag * 4; }
+static inline uint64_t lagbase(const or_sweep *S) { return 4 * (uint64_t)S->nent; }
+static inline uint64_t blen(const or_sweep *S) { return lagbase(S) + (uint64_t)S->nlag * 4; }
 
 void oracle_sweep_info(const or_sweep *S, int64_t info[6]) {
     info[0] = (int64_t)blen(S);
@@ -400,7 +406,7 @@ static void solve_cell(const or_sweep *S, uint32_t q, uint32_t c, const double *
         int64_t nb = S->nbr[4 * c + k];
         uint32_t lag = S->lagbase[4 * ((size_t)q * S->nT + c) + k];
         if (lag != NONE) {
-            uint64_t base = (uint64_t)S->nrefl * S->nq * 4 + 4 * (uint64_t)lag;
+            uint64_t base = lagbase(S) + 4 * (uint64_t)lag;
             for (int j = 0; j < 4; j++)
                 if (j != k) up[j] = B_in ? B_in[base + j] : 0.0;
         } else if (nb >= 0) {
@@ -409,7 +415,7 @@ static void solve_cell(const or_sweep *S, uint32_t q, uint32_t c, const double *
         } else {
             uint32_t f = (uint32_t)(-nb - 1);
             if (S->bc[f] == 1) {
-                uint64_t base = ((uint64_t)S->rslot[f] * S->nq + q) * 4;
+                uint64_t base = 4 * (uint64_t)S->rent[(size_t)S->rslot[f] * S->nq + q];
                 for (int j = 0; j < 4; j++)
                     if (j != k) up[j] = B_in ? B_in[base + j] : 0.0;
             } else if (S->bc[f] == 2 && with_ext) {
@@ -471,10 +477,12 @@ void oracle_sweep_apply(const or_sweep *S, const double *J_in, const double *B_i
                     uint32_t p = S->rmap[(size_t)S->rslot[f] * nq + q];
                     if (p == NONE) continue;
                     for (int j = 0; j < 4; j++)
-                        if (j != k) B_out[((uint64_t)S->rslot[f] * nq + q) * 4 + j] = psi[4 * ((size_t)p * nT + c) + j];
+                        if (j != k)
+                            B_out[4 * (uint64_t)S->rent[(size_t)S->rslot[f] * nq + q] + j] =
+                                psi[4 * ((size_t)p * nT + c) + j];
                 }
             }
-        uint64_t base = (uint64_t)S->nrefl * nq * 4;
+        uint64_t base = lagbase(S);
         for (uint32_t l = 0; l < S->nlag; l++) {
             uint32_t q = S->lag_qck[3 * l], c = S->lag_qck[3 * l + 1], k = S->lag_qck[3 * l + 2];
             int64_t u = S->nbr[4 * c + k];
@@ -625,7 +633,7 @@ void oracle_sweep_balance(const or_sweep *S, const double *J_in, const double *B
                     if (S->bc[f] == 2) {
                         in += S->w[q] * (-d) * S->inc[f];
                     } else if (S->bc[f] == 1 && B_in) {
-                        uint64_t base = ((uint64_t)S->rslot[f] * nq + q) * 4;
+                        uint64_t base = 4 * (uint64_t)S->rent[(size_t)S->rslot[f] * nq + q];
                         for (int j = 0; j < 4; j++)
                             if (j != k) m += B_in[base + j];
                         refl -= S->w[q] * (-d) * m / 3.0;

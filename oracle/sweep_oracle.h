@@ -36,7 +36,8 @@
  * empty while cells remain, the smallest-index remaining cell forms the next
  * level alone and its inflow from unfinished cells is "lagged" (read from
  * the extra-unknown vector B).  Lag slots are numbered in (q, cell, face)
- * order.  B = [reflective inflow: n_reflective_faces x nq x 4][lag: n_lag x 4].
+ * order.  B = [reflective inflow: one entry of 4 values per (reflective
+ * face, incoming ordinate), in (face, ordinate) order][lag: n_lag x 4].
  */
 #ifndef SWEEP_ORACLE_H
 #define SWEEP_ORACLE_H

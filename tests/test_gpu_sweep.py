@@ -148,10 +148,15 @@ def test_bad_arguments_are_rejected(cuda):
         S.apply(precision=16)
     with pytest.raises(tr.TransferError):
         S.solve(restart=0)
-    # a reflective face with an ordinate set that is not mirror symmetric
-    x, y, z, w = tr.ordinates_product(2, 5)
+    # reflective x faces with an ordinate set that is not mirror symmetric in x
+    # (an odd number of azimuths)
+    bc = np.where(md.face_side <= 1, tr.TR_BC_REFLECTIVE, tr.TR_BC_VACUUM).astype(np.int32)
     with pytest.raises(tr.TransferError):
-        tr.Sweep(0, md, (x, y, z, w), ph)
+        tr.Sweep(0, md, tr.ordinates_product(2, 5), tr.Physics(face_bc=bc))
+    # a misaligned device vector
+    J = torch.zeros(4 * md.nT + 2, dtype=torch.float64, device="cuda")
+    with pytest.raises(tr.TransferError):
+        S.apply(J[1:1 + 4 * md.nT])
 
 
 @pytest.mark.parametrize("precision", [64, 32])

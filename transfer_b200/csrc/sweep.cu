@@ -58,9 +58,10 @@ namespace sweep {
 constexpr uint32_t kNone = 0xFFFFFFFFu;
 constexpr uint32_t kLagBit = 0x80000000u;
 constexpr uint32_t kCellMask = 0x0FFFFFFFu;
+constexpr uint32_t kBndBit = 0x40000000u;    // boundary face: kind in bits 28-29, value index below
+constexpr uint32_t kBndIndex = 0x0FFFFFFFu;
 constexpr int kSchedThreads = 1024;
 constexpr int kSweepThreads = 256;
-constexpr int kRingBytes = 64 * 1024;
 constexpr int kRedGrid = 296;            // 2 x 148 SMs
 constexpr uint32_t kMaxLag = 1u << 22;   // lagged (cycle-breaking) faces over all ordinates
 constexpr int kMaxRestart = 64;
@@ -93,7 +94,6 @@ struct Geom {
     const int32_t *fbc;  // [nF]
     const T *finc;       // [nF]
     const int32_t *rslot;// [nF]
-    const uint32_t *rinv;// [nrefl][nq] incoming ordinate mirrored onto q, or kNone
 };
 
 struct Sched {
@@ -101,6 +101,12 @@ struct Sched {
     const uint32_t *lvl;   // [nq][lstride]
     const uint32_t *nlev;  // [nq]
     uint32_t lstride;
+    // cells whose four faces are all inflow (only an inverted element, whose
+    // shared-face normals disagree with its own, can have them): the source
+    // of face 3, sorted by key q * nT + position
+    const unsigned long long *f4_keys;
+    const uint32_t *f4_codes;
+    uint32_t n_f4;
 };
 
 template <typename T>
@@ -241,8 +247,9 @@ __global__ void k_lag_collect(uint32_t nT, uint32_t nq, const uint8_t *lagm, uns
 }
 
 __global__ void k_records(uint32_t nT, uint32_t nq, const uint32_t *order, const uint32_t *pos, const uint8_t *mask,
-                          const uint8_t *lagm, const int32_t *nbr, const unsigned long long *lag_keys, uint32_t nlag,
-                          uint4 *task) {
+                          const uint8_t *lagm, const int32_t *nbr, const int32_t *fbc, const int32_t *rslot,
+                          const uint32_t *rent, const unsigned long long *lag_keys, uint32_t nlag, uint4 *task,
+                          unsigned long long *f4_keys, uint32_t *f4_codes, unsigned int *f4_count) {
     const uint64_t n = (uint64_t)nT * nq;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t q = static_cast<uint32_t>(i / nT);
@@ -255,8 +262,12 @@ __global__ void k_records(uint32_t nT, uint32_t nq, const uint32_t *order, const
             if (!(m >> k & 1u)) continue;
             const int32_t nb = nbr[4 * (size_t)c + k];
             uint32_t code;
-            if (nb < 0) {
-                code = kNone;
+            if (nb < 0) {  // boundary: kind and the index of its inflow value
+                const int32_t f = -nb - 1;
+                const uint32_t bc = static_cast<uint32_t>(fbc[f]);
+                const uint32_t idx = bc == TR_BC_REFLECTIVE ? rent[static_cast<size_t>(rslot[f]) * nq + q]
+                                                            : static_cast<uint32_t>(f);
+                code = kBndBit | (bc << 28) | idx;
             } else if (lg >> k & 1u) {
                 const unsigned long long key = qc * 4 + k;
                 uint32_t lo = 0, hi = nlag;  // lag keys sorted ascending
@@ -269,7 +280,15 @@ __global__ void k_records(uint32_t nT, uint32_t nq, const uint32_t *order, const
             } else {
                 code = pos[(size_t)q * nT + nb];
             }
-            if (t < 3) up[t] = code;
+            if (t < 3) {
+                up[t] = code;
+            } else {
+                const unsigned int slot = atomicAdd(f4_count, 1u);
+                if (slot < kMaxLag) {
+                    f4_keys[slot] = i;
+                    f4_codes[slot] = code;
+                }
+            }
             ++t;
         }
         task[i] = make_uint4(c | (m << 28), up[0], up[1], up[2]);
@@ -315,42 +334,195 @@ __device__ __forceinline__ double4 load_v4<double>(const double *p) {
     return make_double4(a.x, a.y, b.x, b.y);
 }
 
+// Per-thread staging of one task's inputs in shared memory.  Everything a
+// task reads that does not depend on this sweep's results -- face normals,
+// coefficients, scalar-flux source, vertex map, and the inflow values of its
+// boundary and lagged faces -- is copied with cp.async one task ahead
+// (task records two tasks ahead, in registers), so that a level costs the
+// arithmetic of its cells, a shared-memory read of the upwind traces and a
+// block barrier instead of a chain of dependent global loads.
+template <typename T>
+struct alignas(16) Slot {
+    T s[12];
+    T J[4];
+    T bv[3][4];      // inflow values of boundary / lagged faces, by inflow order
+    T coef[4];       // sigma_t V, sigma_s V, sigma_a V B / 4, -
+    uint32_t map, pad[3];
+};
+template <typename T>
+constexpr int ring_bytes() { return sizeof(T) == 4 ? 64 * 1024 : 40 * 1024; }
+template <typename T>
+constexpr size_t sweep_smem() { return ring_bytes<T>() + 2ull * kSweepThreads * sizeof(Slot<T>); }
+
+__device__ __forceinline__ void cp_async16(void *dst, const void *src) {
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src));
+}
+template <int N>
+__device__ __forceinline__ void cp_async_small(void *dst, const void *src) {
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;" ::"r"(d), "l"(src), "n"(N));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N)); }
+// `bytes` (a multiple of 16) from global to shared
+__device__ __forceinline__ void cp_async_bytes(void *dst, const void *src, int bytes) {
+    for (int o = 0; o < bytes; o += 16)
+        cp_async16(static_cast<char *>(dst) + o, static_cast<const char *>(src) + o);
+}
+
+template <typename T>
+__device__ __forceinline__ void stage_task(Slot<T> &sl, const uint4 rec, const Geom<T> &g, const SweepArgs<T> &a) {
+    const uint32_t c = rec.x & kCellMask, mask = rec.x >> 28;
+    cp_async_bytes(sl.s, g.s + 12 * (size_t)c, 12 * sizeof(T));
+    if (a.J) cp_async_bytes(sl.J, a.J + 4 * (size_t)c, 4 * sizeof(T));
+    cp_async_small<sizeof(T)>(&sl.coef[0], g.stv + c);
+    cp_async_small<sizeof(T)>(&sl.coef[1], g.ssv + c);
+    if (a.with_ext) cp_async_small<sizeof(T)>(&sl.coef[2], g.ext + c);
+    cp_async_small<4>(&sl.map, g.map + c);
+    int t = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (!(mask >> k & 1u) || t >= 3) continue;
+        const uint32_t code = t == 0 ? rec.y : t == 1 ? rec.z : rec.w;
+        if (code & kLagBit) {
+            if (a.Bin) cp_async_bytes(sl.bv[t], a.Bin + a.lag_base + 4 * (size_t)(code & ~kLagBit), 4 * sizeof(T));
+        } else if (code & kBndBit) {
+            const uint32_t type = (code >> 28) & 3u, idx = code & kBndIndex;
+            if (type == TR_BC_REFLECTIVE && a.Bin)
+                cp_async_bytes(sl.bv[t], a.Bin + 4 * (size_t)idx, 4 * sizeof(T));
+            else if (type == TR_BC_INCIDENT && a.with_ext)
+                cp_async_small<sizeof(T)>(&sl.bv[t][0], g.finc + idx);
+        }
+        ++t;
+    }
+}
+
+// position of this thread's next task after (L, p), looking up to 4 levels
+// ahead (L is advanced to its level); kNone if none
+__device__ __forceinline__ uint32_t next_task(uint32_t &L, uint32_t p, const uint32_t *lvl, uint32_t nl) {
+    if (p == kNone) return kNone;
+    if (p + blockDim.x < __ldg(lvl + L + 1)) return p + blockDim.x;
+    for (uint32_t d = 1; d <= 4 && L + d < nl; ++d) {
+        const uint32_t s1 = __ldg(lvl + L + d), e1 = __ldg(lvl + L + d + 1);
+        if (s1 + threadIdx.x < e1) {
+            L += d;
+            return s1 + threadIdx.x;
+        }
+    }
+    return kNone;
+}
+
+// upwind trace of one inflow face from its source code
+template <typename T>
+__device__ __forceinline__ void inflow_values(uint32_t code, const T *staged, bool staged_ok, const Geom<T> &g,
+                                              const SweepArgs<T> &a, const typename Vec4<T>::type *ring,
+                                              uint32_t R, uint32_t e0, const T *psi, uint32_t c, int k, uint32_t mp,
+                                              T (&up)[4]) {
+    if (code & kLagBit) {
+        if (a.Bin) {
+            const T *bp = staged_ok ? staged : a.Bin + a.lag_base + 4 * (size_t)(code & ~kLagBit);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) up[j] = bp[j];
+        }
+    } else if (code & kBndBit) {
+        const uint32_t type = (code >> 28) & 3u, idx = code & kBndIndex;
+        if (type == TR_BC_REFLECTIVE && a.Bin) {
+            const T *bp = staged_ok ? staged : a.Bin + 4 * (size_t)idx;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) up[j] = bp[j];
+        } else if (type == TR_BC_INCIDENT && a.with_ext) {
+            const T v = staged_ok ? staged[0] : __ldg(g.finc + idx);
+#pragma unroll
+            for (int j = 0; j < 4; ++j) up[j] = v;
+        }
+    } else {
+        typename Vec4<T>::type v;
+        if (code + R >= e0) {
+            v = ring[code % R];
+        } else {
+            const int32_t nb = __ldg(g.nbr + 4 * (size_t)c + k);
+            v = load_v4<T>(psi + 4 * (size_t)nb);
+        }
+#pragma unroll
+        for (int j = 0; j < 4; ++j) up[j] = comp<T>(v, (mp >> (2 * (4 * k + j))) & 3u);
+    }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, SweepArgs<T> a) {
     using V = typename Vec4<T>::type;
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr uint32_t R = ring_bytes<T>() / sizeof(V);
     V *ring = reinterpret_cast<V *>(smem_raw);
-    constexpr uint32_t R = kRingBytes / sizeof(V);
-    const uint32_t q = blockIdx.x, nT = a.nT, nq = a.nq;
+    Slot<T> *slots = reinterpret_cast<Slot<T> *>(smem_raw + ring_bytes<T>()) + 2 * threadIdx.x;
+    const uint32_t q = blockIdx.x, nT = a.nT;
     const T ox = a.ox[q], oy = a.oy[q], oz = a.oz[q];
     const uint4 *task = sc.task + (size_t)q * nT;
     const uint32_t *lvl = sc.lvl + (size_t)q * sc.lstride;
     const uint32_t nl = sc.nlev[q];
     T *psi = a.psi + (size_t)q * nT * 4;
     const T c12 = T(1) / T(12), c20 = T(1) / T(20);
+
+    // pipeline: the staged task (position pst, slot `cur`, record r_cur) and
+    // the position / record of the task after it (p1 at level L1, r1)
+    uint32_t pst = kNone, L1 = 0;
+    for (uint32_t d = 0; d < 5 && d < nl; ++d)
+        if (__ldg(lvl + d) + threadIdx.x < __ldg(lvl + d + 1)) {
+            pst = __ldg(lvl + d) + threadIdx.x;
+            L1 = d;
+            break;
+        }
+    int cur = 0;
+    uint4 r_cur = make_uint4(0, 0, 0, 0), r1 = make_uint4(0, 0, 0, 0);
+    uint32_t p1 = kNone;
+    if (pst != kNone) {
+        r_cur = __ldg(task + pst);
+        stage_task<T>(slots[cur], r_cur, g, a);
+        p1 = next_task(L1, pst, lvl, nl);
+        if (p1 != kNone) r1 = __ldg(task + p1);
+    }
+    cp_async_commit();
+
     for (uint32_t L = 0; L < nl; ++L) {
-        const uint32_t s0 = lvl[L], e0 = lvl[L + 1];
+        const uint32_t s0 = __ldg(lvl + L), e0 = __ldg(lvl + L + 1);
         for (uint32_t p = s0 + threadIdx.x; p < e0; p += blockDim.x) {
-            const uint4 rec = __ldg(task + p);
+            if (p != pst) {  // not staged ahead: fetch now
+                cp_async_wait<0>();
+                r_cur = __ldg(task + p);
+                stage_task<T>(slots[cur], r_cur, g, a);
+                cp_async_commit();
+                pst = p;
+                L1 = L;
+                p1 = next_task(L1, p, lvl, nl);
+                if (p1 != kNone) r1 = __ldg(task + p1);
+            }
+            // stage the next task, load the record after it
+            uint32_t L2 = L1, p2 = kNone;
+            uint4 r2 = make_uint4(0, 0, 0, 0);
+            if (p1 != kNone) {
+                stage_task<T>(slots[cur ^ 1], r1, g, a);
+                p2 = next_task(L2, p1, lvl, nl);
+                if (p2 != kNone) r2 = __ldg(task + p2);
+            }
+            cp_async_commit();
+            cp_async_wait<1>();  // this task's group has landed
+            const Slot<T> &sl = slots[cur];
+            const uint4 rec = r_cur;
             const uint32_t c = rec.x & kCellMask, mask = rec.x >> 28;
-            T sv[12];
-            load_s<T>(g.s + 12 * (size_t)c, sv);
             T av[4], al[4], Ain = T(0);
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                av[k] = -(ox * sv[3 * k] + oy * sv[3 * k + 1] + oz * sv[3 * k + 2]);
+                av[k] = -(ox * sl.s[3 * k] + oy * sl.s[3 * k + 1] + oz * sl.s[3 * k + 2]);
                 al[k] = (mask >> k & 1u) ? av[k] : T(0);
                 Ain += al[k];
             }
-            const T stv = __ldg(g.stv + c), ssv = __ldg(g.ssv + c);
-            const T ext = a.with_ext ? __ldg(g.ext + c) : T(0);
+            const T stv = sl.coef[0], ssv = sl.coef[1], ext = a.with_ext ? sl.coef[2] : T(0);
             T Jc[4] = {T(0), T(0), T(0), T(0)};
             if (a.J) {
-                V j4 = load_v4<T>(a.J + 4 * (size_t)c);
-                Jc[0] = j4.x;
-                Jc[1] = j4.y;
-                Jc[2] = j4.z;
-                Jc[3] = j4.w;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) Jc[j] = sl.J[j];
             }
             const T Js = Jc[0] + Jc[1] + Jc[2] + Jc[3];
             T Lm[4][4], r[4];
@@ -363,46 +535,28 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, Sw
                 }
                 r[i] = ssv * c20 * (Jc[i] + Js) + ext;
             }
-            const uint32_t mp = __ldg(g.map + c);
-            uint32_t ups[3] = {rec.y, rec.z, rec.w};
+            const uint32_t mp = sl.map;
             int t = 0;
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 if (!(mask >> k & 1u)) continue;
-                const uint32_t code = ups[t < 3 ? t : 2];
-                ++t;
                 T up[4] = {T(0), T(0), T(0), T(0)};
-                if (code == kNone) {
-                    const int32_t f = -__ldg(g.nbr + 4 * (size_t)c + k) - 1;
-                    const int32_t bc = __ldg(g.fbc + f);
-                    if (bc == TR_BC_REFLECTIVE) {
-                        if (a.Bin) {
-                            const T *bp = a.Bin + ((size_t)__ldg(g.rslot + f) * nq + q) * 4;
-#pragma unroll
-                            for (int j = 0; j < 4; ++j) up[j] = bp[j];
-                        }
-                    } else if (bc == TR_BC_INCIDENT && a.with_ext) {
-                        const T v = __ldg(g.finc + f);
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) up[j] = v;
-                    }
-                } else if (code & kLagBit) {
-                    if (a.Bin) {
-                        const T *bp = a.Bin + a.lag_base + 4 * (size_t)(code & ~kLagBit);
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) up[j] = bp[j];
-                    }
+                if (t < 3) {
+                    const uint32_t code = t == 0 ? rec.y : t == 1 ? rec.z : rec.w;
+                    inflow_values<T>(code, sl.bv[t], true, g, a, ring, R, e0, psi, c, k, mp, up);
                 } else {
-                    V v;
-                    if (code + R >= e0) {
-                        v = ring[code % R];
-                    } else {
-                        const int32_t nb = __ldg(g.nbr + 4 * (size_t)c + k);
-                        v = load_v4<T>(psi + 4 * (size_t)nb);
+                    // the fourth inflow face of an inverted element: its source from the side table
+                    const unsigned long long key = (unsigned long long)q * nT + p;
+                    uint32_t lo = 0, hi = sc.n_f4;
+                    while (lo < hi) {
+                        const uint32_t mid = (lo + hi) >> 1;
+                        if (sc.f4_keys[mid] < key) lo = mid + 1;
+                        else hi = mid;
                     }
-#pragma unroll
-                    for (int j = 0; j < 4; ++j) up[j] = comp<T>(v, (mp >> (2 * (4 * k + j))) & 3u);
+                    if (lo < sc.n_f4 && sc.f4_keys[lo] == key)
+                        inflow_values<T>(sc.f4_codes[lo], nullptr, false, g, a, ring, R, e0, psi, c, k, mp, up);
                 }
+                ++t;
                 up[k] = T(0);
                 const T Tk = up[0] + up[1] + up[2] + up[3];
                 const T ak = av[k] * c12;
@@ -443,26 +597,39 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, Sw
                 dst[1] = make_double2(o[2], o[3]);
             }
             ring[p % R] = out;
-            if (a.Bout && mask != 0xFu) {
-                // outflow through reflective faces feeds the mirrored ordinate's inflow
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    if (mask >> k & 1u) continue;
-                    const int32_t nb = __ldg(g.nbr + 4 * (size_t)c + k);
-                    if (nb >= 0) continue;
-                    const int32_t f = -nb - 1;
-                    if (__ldg(g.fbc + f) != TR_BC_REFLECTIVE) continue;
-                    const int32_t sl = __ldg(g.rslot + f);
-                    const uint32_t qin = __ldg(g.rinv + (size_t)sl * nq + q);
-                    if (qin == kNone) continue;
-                    T *bp = a.Bout + ((size_t)sl * nq + qin) * 4;
-#pragma unroll
-                    for (int j = 0; j < 4; ++j)
-                        if (j != k) bp[j] = o[j];
-                }
-            }
+            // advance the pipeline
+            cur ^= 1;
+            pst = p1;
+            r_cur = r1;
+            p1 = p2;
+            L1 = L2;
+            r1 = r2;
         }
         __syncthreads();
+    }
+    cp_async_wait<0>();
+}
+
+// B_out of the reflective faces: the inflow of each (face, incoming q)
+// entry is the outflow of the mirrored ordinate at the same face (same
+// vertex values; the face's opposite vertex left zero)
+template <typename T>
+__global__ void k_reflect_out(uint32_t nT, uint32_t nent, const uint32_t *ent_cell, const uint32_t *ent_qout,
+                              const T *psi, T *Bout) {
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < nent; e += gridDim.x * blockDim.x) {
+        const uint32_t ck = ent_cell[e], c = ck >> 2, k = ck & 3u;
+        typename Vec4<T>::type v = load_v4<T>(psi + ((size_t)ent_qout[e] * nT + c) * 4);
+        if (k == 0) v.x = T(0);
+        if (k == 1) v.y = T(0);
+        if (k == 2) v.z = T(0);
+        if (k == 3) v.w = T(0);
+        if constexpr (sizeof(T) == 4) {
+            *reinterpret_cast<float4 *>(Bout + 4 * (size_t)e) = v;
+        } else {
+            double2 *dst = reinterpret_cast<double2 *>(Bout + 4 * (size_t)e);
+            dst[0] = make_double2(v.x, v.y);
+            dst[1] = make_double2(v.z, v.w);
+        }
     }
 }
 
@@ -718,6 +885,7 @@ struct BalanceArgs {
     uint32_t nT, nq, nbf;
     const double *s, *stv, *ssv, *ext, *w, *ox, *oy, *oz, *finc;
     const int32_t *fbc, *rslot;
+    const uint32_t *rent;    // [nrefl][nq] B entry of an incoming ordinate
     const uint32_t *bcell;   // [nbf] owner cell*4 + local face
     const uint32_t *bface;   // [nbf] face id
     const double *Jin, *Jout, *Bin;
@@ -753,7 +921,7 @@ __global__ void k_balance(BalanceArgs b, const T *psi, double *partials, unsigne
                 if (bc == TR_BC_INCIDENT) {
                     v[3] += b.w[q] * (-d) * b.finc[f];
                 } else if (bc == TR_BC_REFLECTIVE && b.Bin) {
-                    const double *bp = b.Bin + ((size_t)b.rslot[f] * b.nq + q) * 4;
+                    const double *bp = b.Bin + 4 * (size_t)b.rent[(size_t)b.rslot[f] * b.nq + q];
                     double m = 0.0;
                     for (uint32_t j = 0; j < 4; ++j)
                         if (j != k) m += bp[j];
@@ -787,7 +955,11 @@ struct tr_sweep {
     double *s64 = nullptr, *stv64 = nullptr, *ssv64 = nullptr, *ext64 = nullptr, *finc64 = nullptr;
     float *s32 = nullptr, *stv32 = nullptr, *ssv32 = nullptr, *ext32 = nullptr, *finc32 = nullptr;
     int32_t *nbr = nullptr, *fbc = nullptr, *rslot = nullptr;
-    uint32_t *map = nullptr, *rinv = nullptr, *bcell = nullptr, *bface = nullptr;
+    uint32_t *map = nullptr, *bcell = nullptr, *bface = nullptr;
+    uint32_t *rent = nullptr;      // [nrefl][nq] B entry of an incoming ordinate, or kNone
+    uint32_t *ent_cell = nullptr;  // [nent] owner cell * 4 + local face of a reflective B entry
+    uint32_t *ent_qout = nullptr;  // [nent] the mirrored outgoing ordinate
+    uint32_t nent = 0;
     double *o64[4] = {nullptr, nullptr, nullptr, nullptr};  // x y z w
     float *o32[3] = {nullptr, nullptr, nullptr};
     double *Wm = nullptr;          // [16][nq] w_q Y_m(Omega_q)
@@ -797,6 +969,9 @@ struct tr_sweep {
     uint4 *task = nullptr;
     uint32_t *lvl = nullptr, *nlev = nullptr;
     unsigned long long *lag_keys = nullptr;
+    unsigned long long *f4_keys = nullptr;
+    uint32_t *f4_codes = nullptr;
+    uint32_t n_f4 = 0;
     // state
     double *psi64 = nullptr;
     float *psi32 = nullptr;
@@ -966,17 +1141,18 @@ static tr_status sweep_setup(tr_sweep *S, const tr_mesh_view *m, const tr_physic
         }
     }
     S->nbf = static_cast<uint32_t>(bcell.size());
-    // reflective faces: slots and mirrored ordinates (incoming q_in -> outgoing q_out;
-    // stored inverted: rinv[slot][q_out] = q_in)
+    // reflective faces: slots, and for each (slot, incoming q_in) the mirrored
+    // outgoing ordinate q_out; the B entries are those pairs in (slot, q) order
     std::vector<int32_t> rslot(nF + 1, -1);
     uint32_t nrefl = 0;
     for (uint32_t f = 0; f < nF; ++f)
         if (fbc[f] == TR_BC_REFLECTIVE) rslot[f] = static_cast<int32_t>(nrefl++);
     S->nrefl = nrefl;
-    std::vector<uint32_t> rinv(static_cast<size_t>(nrefl) * nq + 1, kNone);
+    std::vector<uint32_t> rmap(static_cast<size_t>(nrefl) * nq + 1, kNone), rcell(nrefl + 1, 0u);
     for (uint32_t i = 0; i < S->nbf; ++i) {
         const uint32_t c = bcell[i] >> 2, k = bcell[i] & 3u, f = bface[i];
         if (rslot[f] < 0) continue;
+        rcell[rslot[f]] = c * 4 + k;
         const double *sk = &s[12ull * c + 3 * k];
         const double a = std::sqrt(sk[0] * sk[0] + sk[1] * sk[1] + sk[2] * sk[2]);
         const double n[3] = {sk[0] / a, sk[1] / a, sk[2] / a};
@@ -997,9 +1173,17 @@ static tr_status sweep_setup(tr_sweep *S, const tr_mesh_view *m, const tr_physic
             if (bd > 1e-16)
                 return sw_err(S, TR_ERR_INVALID_ARG,
                               "sweep: a reflective face mirrors an ordinate onto a direction outside the set");
-            rinv[static_cast<size_t>(rslot[f]) * nq + best] = q;
+            rmap[static_cast<size_t>(rslot[f]) * nq + q] = best;
         }
     }
+    std::vector<uint32_t> rent(static_cast<size_t>(nrefl) * nq + 1, kNone), ent_cell, ent_qout;
+    for (size_t i = 0; i < static_cast<size_t>(nrefl) * nq; ++i)
+        if (rmap[i] != kNone) {
+            rent[i] = static_cast<uint32_t>(ent_cell.size());
+            ent_cell.push_back(rcell[i / nq]);
+            ent_qout.push_back(rmap[i]);
+        }
+    S->nent = static_cast<uint32_t>(ent_cell.size());
     // ordinates, moment weights
     std::vector<double> ox(o->x, o->x + nq), oy(o->y, o->y + nq), oz(o->z, o->z + nq), w(o->w, o->w + nq);
     std::vector<float> ox32(nq), oy32(nq), oz32(nq);
@@ -1023,7 +1207,7 @@ static tr_status sweep_setup(tr_sweep *S, const tr_mesh_view *m, const tr_physic
     if (e == cudaSuccess) e = sw_upload(S, &S->ptr, vec);
     UP(s64, s) UP(stv64, stv) UP(ssv64, ssv) UP(ext64, ext) UP(finc64, finc)
     UP(s32, f32(s)) UP(stv32, f32(stv)) UP(ssv32, f32(ssv)) UP(ext32, f32(ext)) UP(finc32, f32(finc))
-    UP(nbr, nbr) UP(fbc, fbc) UP(rslot, rslot) UP(map, map) UP(rinv, rinv) UP(bcell, bcell) UP(bface, bface)
+    UP(nbr, nbr) UP(fbc, fbc) UP(rslot, rslot) UP(map, map) UP(rent, rent) UP(ent_cell, ent_cell) UP(ent_qout, ent_qout) UP(bcell, bcell) UP(bface, bface)
     UP(o64[0], ox) UP(o64[1], oy) UP(o64[2], oz) UP(o64[3], w) UP(o32[0], ox32) UP(o32[1], oy32) UP(o32[2], oz32)
     UP(Wm, Wm) UP(vol64, vol) UP(B64, bpl)
 #undef UP
@@ -1102,11 +1286,45 @@ static tr_status sweep_setup(tr_sweep *S, const tr_mesh_view *m, const tr_physic
     S->maxlev = maxlev;
     S->forced = forced;
     S->lstride = maxlev + 1;
+    unsigned long long *f4k_tmp = nullptr;
+    uint32_t *f4c_tmp = nullptr;
+    unsigned int *f4_count = nullptr;
+    tmp_alloc(reinterpret_cast<void **>(&f4k_tmp), static_cast<size_t>(kMaxLag) * 8);
+    tmp_alloc(reinterpret_cast<void **>(&f4c_tmp), static_cast<size_t>(kMaxLag) * 4);
+    tmp_alloc(reinterpret_cast<void **>(&f4_count), 4);
+    if (e == cudaSuccess) e = cudaMemsetAsync(f4_count, 0, 4, S->stream);
     if (e == cudaSuccess && st == TR_OK) {
-        k_records<<<grid_for(S, nqT), 256, 0, S->stream>>>(nT, nq, order, pos, mask, lagm, S->nbr, S->lag_keys, nlag,
-                                                           S->task);
+        k_records<<<grid_for(S, nqT), 256, 0, S->stream>>>(nT, nq, order, pos, mask, lagm, S->nbr, S->fbc, S->rslot,
+                                                           S->rent, S->lag_keys, nlag, S->task, f4k_tmp, f4c_tmp,
+                                                           f4_count);
         e = cudaGetLastError();
     }
+    // cells with four inflow faces: their face-3 sources, sorted by (ordinate, position)
+    uint32_t n_f4 = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&n_f4, f4_count, 4, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && n_f4 > kMaxLag && st == TR_OK)
+        st = sw_err(S, TR_ERR_UNSUPPORTED, "sweep: too many inverted elements");
+    if (e == cudaSuccess && st == TR_OK) {
+        std::vector<unsigned long long> fk(n_f4);
+        std::vector<uint32_t> fc(n_f4), idx(n_f4);
+        if (n_f4) {
+            e = cudaMemcpy(fk.data(), f4k_tmp, 8ull * n_f4, cudaMemcpyDeviceToHost);
+            if (e == cudaSuccess) e = cudaMemcpy(fc.data(), f4c_tmp, 4ull * n_f4, cudaMemcpyDeviceToHost);
+        }
+        for (uint32_t i = 0; i < n_f4; ++i) idx[i] = i;
+        std::sort(idx.begin(), idx.end(), [&](uint32_t x, uint32_t y) { return fk[x] < fk[y]; });
+        std::vector<unsigned long long> sk(n_f4);
+        std::vector<uint32_t> scodes(n_f4);
+        for (uint32_t i = 0; i < n_f4; ++i) {
+            sk[i] = fk[idx[i]];
+            scodes[i] = fc[idx[i]];
+        }
+        if (e == cudaSuccess) e = sw_upload(S, &S->f4_keys, sk);
+        if (e == cudaSuccess) e = sw_upload(S, &S->f4_codes, scodes);
+        S->n_f4 = n_f4;
+    }
+    for (void *p : {(void *)f4k_tmp, (void *)f4c_tmp, (void *)f4_count})
+        if (p) cudaFree(p);
     if (e == cudaSuccess && st == TR_OK) e = sw_alloc(S, &S->lvl, static_cast<size_t>(nq) * S->lstride);
     if (e == cudaSuccess && st == TR_OK) {
         // compact the level pointers to [nq][lstride]; levels past nlev[q] are empty
@@ -1123,16 +1341,18 @@ static tr_status sweep_setup(tr_sweep *S, const tr_mesh_view *m, const tr_physic
         if (p) cudaFree(p);
     if (st != TR_OK) return st;
     if (e != cudaSuccess) return sw_cuda(S, e, "sweep: schedule");
-    S->nB = static_cast<uint64_t>(nrefl) * nq * 4 + 4ull * nlag;
+    S->nB = 4ull * S->nent + 4ull * nlag;
     // reductions
     if (e == cudaSuccess) e = sw_alloc(S, &S->partials, 64ull * kRedGrid);
     if (e == cudaSuccess) e = sw_alloc(S, &S->red, 256);
     if (e == cudaSuccess) e = sw_alloc(S, &S->counter, 4);
     if (e == cudaSuccess) e = cudaMemset(S->counter, 0, 16);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_sweep<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRingBytes);
+        e = cudaFuncSetAttribute(k_sweep<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(sweep_smem<double>()));
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_sweep<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, kRingBytes);
+        e = cudaFuncSetAttribute(k_sweep<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(sweep_smem<float>()));
     if (e == cudaSuccess) e = cudaEventCreate(&S->ev[0]);
     if (e == cudaSuccess) e = cudaEventCreate(&S->ev[1]);
     if (e != cudaSuccess) return sw_cuda(S, e, "sweep: allocation");
@@ -1173,43 +1393,55 @@ static Geom<T> geom_of(const tr_sweep *S) {
     g.map = S->map;
     g.fbc = S->fbc;
     g.rslot = S->rslot;
-    g.rinv = S->rinv;
     return g;
 }
 
 // Queues one sweep: J_in, B_in FP64 (null = 0) -> J_out, B_out FP64 (null = skip).
+template <typename T>
+static cudaError_t sweep_launch(tr_sweep *S, const T *J, const T *Bin, int with_ext, T *psi, T *Bout) {
+    cudaStream_t st = S->stream;
+    Sched sc{S->task, S->lvl, S->nlev, S->lstride, S->f4_keys, S->f4_codes, S->n_f4};
+    SweepArgs<T> a;
+    a.nT = S->nT;
+    a.nq = S->nq;
+    if constexpr (sizeof(T) == 8) {
+        a.ox = S->o64[0];
+        a.oy = S->o64[1];
+        a.oz = S->o64[2];
+    } else {
+        a.ox = S->o32[0];
+        a.oy = S->o32[1];
+        a.oz = S->o32[2];
+    }
+    a.J = J;
+    a.Bin = Bin;
+    a.Bout = nullptr;
+    a.psi = psi;
+    a.with_ext = with_ext;
+    a.lag_base = 4ull * S->nent;
+    k_sweep<T><<<S->nq, kSweepThreads, sweep_smem<T>(), st>>>(geom_of<T>(S), sc, a);
+    ++S->launches;
+    if (Bout && S->nent) {
+        k_reflect_out<T><<<grid_for(S, S->nent), 256, 0, st>>>(S->nT, S->nent, S->ent_cell, S->ent_qout, psi, Bout);
+        ++S->launches;
+    }
+    if (Bout && S->nlag) {
+        k_lag_out<T><<<grid_for(S, S->nlag), 256, 0, st>>>(S->nT, S->nlag, S->lag_keys, S->nbr, S->map, psi,
+                                                          Bout + a.lag_base);
+        ++S->launches;
+    }
+    return cudaGetLastError();
+}
+
 static cudaError_t sweep_enqueue(tr_sweep *S, int prec, const double *J_in, const double *B_in, int with_ext,
                                  double *J_out, double *B_out) {
     cudaError_t e = ensure_psi(S, prec);
     if (e != cudaSuccess) return e;
     cudaStream_t st = S->stream;
-    Sched sc{S->task, S->lvl, S->nlev, S->lstride};
-    const size_t smem = kRingBytes;
+    if (!S->nB) B_in = B_out = nullptr;
     if (prec == 64) {
-        SweepArgs<double> a;
-        a.nT = S->nT;
-        a.nq = S->nq;
-        a.ox = S->o64[0];
-        a.oy = S->o64[1];
-        a.oz = S->o64[2];
-        a.J = J_in;
-        a.Bin = B_in;
-        a.Bout = B_out;
-        a.psi = S->psi64;
-        a.with_ext = with_ext;
-        a.lag_base = static_cast<uint64_t>(S->nrefl) * S->nq * 4;
-        if (B_out && S->nB) {
-            e = cudaMemsetAsync(B_out, 0, S->nB * 8, st);
-            if (e != cudaSuccess) return e;
-        }
-        k_sweep<double><<<S->nq, kSweepThreads, smem, st>>>(geom_of<double>(S), sc, a);
-        ++S->launches;
-        if (B_out && S->nlag) {
-            k_lag_out<double><<<grid_for(S, S->nlag), 256, 0, st>>>(S->nT, S->nlag, S->lag_keys, S->nbr, S->map,
-                                                                   S->psi64, B_out + a.lag_base);
-            ++S->launches;
-        }
-        if (J_out) {
+        e = sweep_launch<double>(S, J_in, B_in, with_ext, S->psi64, B_out);
+        if (e == cudaSuccess && J_out) {
             k_scalar_flux<double><<<grid_for(S, S->nT), 256, 0, st>>>(S->nT, S->nq, S->o64[3], S->psi64, J_out);
             ++S->launches;
         }
@@ -1219,44 +1451,24 @@ static cudaError_t sweep_enqueue(tr_sweep *S, int prec, const double *J_in, cons
             k_to_f32<<<grid_for(S, S->nJ), 256, 0, st>>>(S->nJ, J_in, S->J32);
             ++S->launches;
         }
-        if (B_in && S->nB) {
+        if (B_in) {
             k_to_f32<<<grid_for(S, S->nB), 256, 0, st>>>(S->nB, B_in, S->Bi32);
             ++S->launches;
         }
-        SweepArgs<float> a;
-        a.nT = S->nT;
-        a.nq = S->nq;
-        a.ox = S->o32[0];
-        a.oy = S->o32[1];
-        a.oz = S->o32[2];
-        a.J = J_in ? S->J32 : nullptr;
-        a.Bin = (B_in && S->nB) ? S->Bi32 : nullptr;
-        a.Bout = (B_out && S->nB) ? S->Bo32 : nullptr;
-        a.psi = S->psi32;
-        a.with_ext = with_ext;
-        a.lag_base = static_cast<uint64_t>(S->nrefl) * S->nq * 4;
-        if (a.Bout) {
-            e = cudaMemsetAsync(S->Bo32, 0, S->nB * 4, st);
-            if (e != cudaSuccess) return e;
-        }
-        k_sweep<float><<<S->nq, kSweepThreads, smem, st>>>(geom_of<float>(S), sc, a);
-        ++S->launches;
-        if (a.Bout && S->nlag) {
-            k_lag_out<float><<<grid_for(S, S->nlag), 256, 0, st>>>(S->nT, S->nlag, S->lag_keys, S->nbr, S->map,
-                                                                  S->psi32, S->Bo32 + a.lag_base);
-            ++S->launches;
-        }
-        if (a.Bout) {
+        e = sweep_launch<float>(S, J_in ? S->J32 : nullptr, B_in ? S->Bi32 : nullptr, with_ext, S->psi32,
+                                B_out ? S->Bo32 : nullptr);
+        if (e == cudaSuccess && B_out) {
             k_to_f64<<<grid_for(S, S->nB), 256, 0, st>>>(S->nB, S->Bo32, B_out);
             ++S->launches;
         }
-        if (J_out) {
+        if (e == cudaSuccess && J_out) {
             k_scalar_flux<float><<<grid_for(S, S->nT), 256, 0, st>>>(S->nT, S->nq, S->o64[3], S->psi32, J_out);
             ++S->launches;
         }
         ++S->sweeps32;
     }
     S->last_prec = prec;
+    if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
 
@@ -1515,10 +1727,14 @@ tr_status tr_sweep_levels(tr_sweep *s, int32_t *level) {
     return TR_OK;
 }
 
+static bool aligned16(const void *p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
 tr_status tr_sweep_apply(tr_sweep *s, int precision, const double *J_in, const double *B_in, int with_ext,
                          double *J_out, double *B_out) {
     SW_CHECK(s);
     if (precision != 32 && precision != 64) return sw_err(s, TR_ERR_INVALID_ARG, "precision must be 32 or 64");
+    if (!aligned16(J_in) || !aligned16(B_in) || !aligned16(J_out) || !aligned16(B_out))
+        return sw_err(s, TR_ERR_INVALID_ARG, "tr_sweep_apply: device vectors must be 16-byte aligned");
     cudaError_t e = sweep_enqueue(s, precision, J_in, s->nB ? B_in : nullptr, with_ext, J_out, s->nB ? B_out : nullptr);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
     return sw_cuda(s, e, "tr_sweep_apply");
@@ -1609,6 +1825,7 @@ tr_status tr_sweep_balance(tr_sweep *s, const double *J_in, const double *B_in, 
     b.finc = s->finc64;
     b.fbc = s->fbc;
     b.rslot = s->rslot;
+    b.rent = s->rent;
     b.bcell = s->bcell;
     b.bface = s->bface;
     b.Jin = J_in;
@@ -1693,7 +1910,9 @@ tr_status tr_sweep_solve(tr_sweep *s, const tr_sweep_opts *opts, double *J, doub
             double rn = bn;
             while (e == cudaSuccess && outer < o.max_outer && its < o.max_iter) {
                 ++outer;
-                double want = o.inner_tol > 0.0 ? o.inner_tol : std::max(2e-6, 0.3 * o.tol * bn / rn);
+                // inner reduction: what is still missing to tol (x 0.3), but no
+                // deeper than 1e-4, which FP32 sweeps reach reliably
+                double want = o.inner_tol > 0.0 ? o.inner_tol : std::max(1e-4, 0.3 * o.tol * bn / rn);
                 want = std::min(want, 0.5);
                 e = cudaMemsetAsync(s->kd, 0, n * 8, st);
                 int it_in = 0;
@@ -1772,6 +1991,8 @@ tr_status tr_sweep_gradient(tr_sweep *fwd, tr_sweep *adj, int precision, const d
     if (!adj || !J || !J_adj || !dF_dsigma_a || !dF_dsigma_s)
         return sw_err(fwd, TR_ERR_INVALID_ARG, "tr_sweep_gradient: null argument");
     if (precision != 32 && precision != 64) return sw_err(fwd, TR_ERR_INVALID_ARG, "precision must be 32 or 64");
+    if (!aligned16(J) || !aligned16(B) || !aligned16(J_adj))
+        return sw_err(fwd, TR_ERR_INVALID_ARG, "tr_sweep_gradient: device vectors must be 16-byte aligned");
     if (adj->device != fwd->device || adj->nT != fwd->nT || adj->nq != fwd->nq)
         return sw_err(fwd, TR_ERR_INVALID_ARG, "tr_sweep_gradient: adjoint sweep of another problem");
     const uint32_t nq = fwd->nq;

@@ -76,6 +76,40 @@ def cube64(maxk=5, n=64):
 WORKLOADS = {"config1": config1, "milne_slab": milne_slab, "cube64": cube64}
 
 
+def milne_sweep(n=(8, 8, 160), depth=20.0, albedo=0.999, incident=1.0, n_polar=8, n_azim=14):
+    """The Milne-type slab for the discrete-ordinates sweep: 8 x 8 x 160 Kuhn
+    hexahedra on [0,1]^2 x [0,20] (61,440 tets, jitter +-0.15h), sigma_t = 1
+    with isotropic scattering of albedo 0.999, reflective x / y faces (an
+    infinite slab), vacuum at z = 0, isotropic inflow I = 1 at z = 20.
+    Ordinates: 8 Gauss-Legendre cosines x 14 azimuths = 112 directions, the
+    mirror-symmetric product set nearest the 110-point Lebedev set.
+    Returns (MeshData, Physics, ordinates, description)."""
+    from ._lib import TR_BC_REFLECTIVE
+    from .sweep import ordinates_product
+    md = MeshData.kuhn(n, box=(0.0, 1.0, 0.0, 1.0, 0.0, depth), jitter=0.15, seed=SEED, kappa=[0.0, 1.0],
+                       Ip=[0.0, 0.0], albedo=[0.0, albedo])
+    side = md.face_side
+    bc = np.full(md.nF, TR_BC_VACUUM, dtype=np.int32)
+    bc[side <= 3] = TR_BC_REFLECTIVE
+    bc[side == 5] = TR_BC_INCIDENT
+    phys = Physics(kappa_abs_volume=md.kappa_abs_volume, face_bc=bc, face_incident=np.where(side == 5, incident, 0.0))
+    ords = ordinates_product(n_polar, n_azim)
+    desc = dict(workload="milne_sweep", mesh=f"{n[0]}x{n[1]}x{n[2]} Kuhn slab [0,1]^2x[0,{depth:g}], jitter 0.15h",
+                ordinates=f"{n_polar}x{n_azim} Gauss-Legendre x azimuth product set ({n_polar * n_azim})",
+                physics=f"sigma_t=1, isotropic scattering albedo {albedo:g}, reflective x/y, vacuum z=0, "
+                        f"isotropic inflow I={incident:g} at z={depth:g}")
+    return md, phys, ords, desc
+
+
+def sweep_work(nT, nq, real_bytes=4):
+    """Algorithmic work of one sweep of all ordinates: per (cell, ordinate)
+    the task record (16 B) and vertex map (4 B), face normals and
+    coefficients (15 reals) and the scalar-flux source (4 reals) are read
+    and psi (4 reals) is written; about 220 flops for the 4x4 system and its
+    solve."""
+    return nq * nT * (16 + 4 + real_bytes * (15 + 4 + 4)), 220 * nq * nT
+
+
 def algorithmic_work(md, ad, real_bytes=8):
     """Per operator application: bytes and flops as counted for the roofline:
     read f and write A f (2 * real_bytes per vertex and harmonic), 4 vertex
