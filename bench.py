@@ -44,6 +44,7 @@ def parse_args():
     p.add_argument("--workload", default="milne_slab")
     p.add_argument("--cpu-iters", type=int, default=0, help="CG iterations per CPU-baseline sample (0: auto)")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-sweep", action="store_true", help="skip the discrete-ordinates sweep section")
     return p.parse_args()
 
 
@@ -194,6 +195,70 @@ def aggregate_replicas(times_ms, updates, dist=None, device="cpu"):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.all_reduce(u, op=dist.ReduceOp.SUM)
     return [float(x) for x in t.cpu()], [float(x) for x in u.cpu()]
+
+
+# ----------------------------------------------------------------- sweep
+def sweep_section(local, flush, peak, want_cpu):
+    """The discrete-ordinates sweep on the Milne slab (workloads.milne_sweep):
+    one sweep of all ordinates timed alone (FP32 and FP64), and solves of the
+    scattering problem to the FP64 relative residual TOL, FP64 GMRES against
+    FP32 sweeps in FP64 defect correction; the FP64 energy balance of the
+    mixed solution and its difference from the FP64 one."""
+    import torch
+    import transfer_b200 as tr
+    from transfer_b200 import workloads as W
+    md, ph, ords, desc = W.milne_sweep()
+    S = tr.Sweep(local, md, ords, ph)
+    nT, nq = S.nT, S.nq
+    ms = {p: S.bench(p, 20) for p in (32, 64)}
+    out = {"config": {**desc, "nT": nT, "nq": nq, "max_levels": S.max_levels, "n_extra": S.n_extra,
+                      "tol": TOL, "solver": "GMRES(40) over the scattering source and reflective inflow"},
+           "unit": "cell-ordinate updates/s (nT * nq per sweep)"}
+    for p in (32, 64):
+        byt, flops = W.sweep_work(nT, nq, real_bytes=p // 8)
+        out[f"sweep_fp{p}"] = {"ms": ms[p], "value": nT * nq / (ms[p] * 1e-3),
+                               "algorithmic_gbs": byt / (ms[p] * 1e-3) / 1e9,
+                               "frac_of_hbm": byt / (ms[p] * 1e-3) / 1e9 / peak,
+                               "gflops": flops / (ms[p] * 1e-3) / 1e9,
+                               "us_per_level": 1e3 * ms[p] / S.max_levels}
+    sols = {}
+    for name, mode in (("fp64", tr.TR_MODE_FP64), ("mixed", tr.TR_MODE_MIXED)):
+        S.solve(mode=mode, tol=TOL, restart=40, max_iter=5000)   # warm-up
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        J, B, rep = S.solve(mode=mode, tol=TOL, restart=40, max_iter=5000)
+        e1.record()
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1)
+        sweeps = rep.sweeps_f32 + rep.sweeps_f64
+        sols[name] = (J, B)
+        out[f"solve_{name}"] = {"ms": t, "converged": bool(rep.converged), "iterations": rep.iterations,
+                                "outer_steps": rep.outer_steps, "sweeps_f32": rep.sweeps_f32,
+                                "sweeps_f64": rep.sweeps_f64, "residual": rep.residual,
+                                "value": sweeps * nT * nq / (t * 1e-3)}
+    out["speedup_mixed_vs_fp64"] = out["solve_fp64"]["ms"] / out["solve_mixed"]["ms"]
+    J, B = sols["mixed"]
+    Jo, _ = S.apply(J, B, precision=64)
+    b = S.balance(J, B, Jo)
+    out["balance_mixed"] = {**b, "relative_imbalance": (b["emitted"] + b["incoming"] - b["absorbed"] - b["escaped"]
+                                                        - b["reflective_net"]) / b["incoming"]}
+    Jf = sols["fp64"][0]
+    out["mixed_vs_fp64_J"] = float(((J - Jf).abs().max() / Jf.abs().max()).item())
+    if want_cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle_py as op
+        O = op.SweepOracle(md, ords, kappa_abs_volume=ph.kappa_abs_volume, face_bc=ph.face_bc,
+                           face_incident=ph.face_incident)
+        t0 = time.perf_counter()
+        n = 3
+        for _ in range(n):
+            O.apply()
+        secs = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": n * nT * nq / secs, "unit": out["unit"], "cores": op.lib.oracle_num_threads(),
+                               "kind": "port", "sample": f"{n} FP64 sweeps of the CPU restatement ({secs:.1f} s)"}
+    return out
 
 
 # ----------------------------------------------------------------- GPU arm
@@ -362,6 +427,8 @@ def run_ours(args, rank, world, local):
                              "algorithmic_gflop": flops / 1e9}},
             "clocks": clocks,
         }
+        if not args.no_sweep:
+            line["sweep"] = sweep_section(local, flush, peak, world == 1 and not args.no_cpu_baseline)
         if world == 1 and not args.no_cpu_baseline:
             iters = args.cpu_iters or auto_cpu_iters(args.workload)
             v, threads, secs, n = cpu_sample(args.workload, iters)

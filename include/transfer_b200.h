@@ -351,19 +351,23 @@ enum { TR_SWEEP_GMRES = 0, TR_SWEEP_SOURCE_ITERATION = 1 };
 typedef struct tr_sweep_opts {
     int32_t method;            /* TR_SWEEP_*                                */
     int32_t mode;              /* TR_MODE_FP64, or TR_MODE_MIXED: FP32
-                                  sweeps inside FP64 defect correction      */
-    double  tol;               /* GMRES: ||b - (I - T) x|| / ||b||;
+                                  sweeps inside FP64 defect correction
+                                  (each GMRES cycle starts from the FP64
+                                  residual, its Krylov steps sweep in FP32) */
+    double  tol;               /* GMRES: ||b - (I - T) x|| / ||b||, FP64;
                                   source iteration: relative change        */
     int32_t max_iter;          /* sweeps of the iteration (Krylov steps)   */
     int32_t restart;           /* GMRES restart length, 1..64              */
-    double  inner_tol;         /* mixed: FP32 solve reduction (0: adaptive,
-                                  0.3 x what is missing, at least 1e-4)    */
-    int32_t max_outer;         /* mixed: defect-correction steps           */
+    double  inner_tol;         /* GMRES: end a cycle early once it reduced
+                                  its residual by this factor, then restart
+                                  from the true residual (0: never)        */
+    int32_t max_outer;         /* unused; kept for layout                   */
 } tr_sweep_opts;
 typedef struct tr_sweep_report {
     int32_t converged;
     int32_t iterations;        /* Krylov steps (or source iterations)      */
-    int32_t outer_steps;       /* mixed mode defect-correction steps       */
+    int32_t outer_steps;       /* mixed mode: GMRES cycles (each from an
+                                  FP64 residual)                           */
     int64_t sweeps_f32, sweeps_f64;
     double  residual;          /* final relative residual, FP64            */
     double  rhs_norm;

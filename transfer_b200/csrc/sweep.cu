@@ -981,7 +981,7 @@ struct tr_sweep {
     unsigned int *counter = nullptr;
     // Krylov work space (allocated on first solve)
     double *kv = nullptr;          // [kMaxRestart + 1][n] basis
-    double *kb = nullptr, *kx = nullptr, *kr = nullptr, *kt = nullptr, *kd = nullptr, *kh = nullptr;
+    double *kb = nullptr, *kx = nullptr, *kt = nullptr, *kh = nullptr;
     int kv_m = 0;
     cudaEvent_t ev[2] = {nullptr, nullptr};
     std::vector<void *> allocs;
@@ -1479,9 +1479,7 @@ static cudaError_t krylov_alloc(tr_sweep *S, int m) {
     cudaError_t e = sw_alloc(S, &S->kv, n * (m + 1));
     if (e == cudaSuccess && !S->kb) e = sw_alloc(S, &S->kb, n);
     if (e == cudaSuccess && !S->kx) e = sw_alloc(S, &S->kx, n);
-    if (e == cudaSuccess && !S->kr) e = sw_alloc(S, &S->kr, n);
     if (e == cudaSuccess && !S->kt) e = sw_alloc(S, &S->kt, n);
-    if (e == cudaSuccess && !S->kd) e = sw_alloc(S, &S->kd, n);
     if (e == cudaSuccess && !S->kh) e = sw_alloc(S, &S->kh, 2 * (kMaxRestart + 2));
     if (e == cudaSuccess) S->kv_m = m;
     return e;
@@ -1518,24 +1516,28 @@ static cudaError_t vnorm(tr_sweep *S, const double *x, double *out) {
 // GMRES(m) on (I - T_prec) x = b, x updated in place (device vectors).
 // Stops at ||b - (I - T) x|| <= rtol * bref (the recursion estimate,
 // confirmed by a true residual at the end of a cycle).
-static cudaError_t gmres(tr_sweep *S, int prec, const double *b, double *x, int m, double rtol, double bref,
-                         int max_it, int *its, double *res_out) {
+static cudaError_t gmres(tr_sweep *S, int prec, int prec_res, const double *b, double *x, int m, double rtol,
+                         double bref, double cycle_tol, int max_it, int *its, double *res_out, int *cycles_out) {
     const uint64_t n = S->nJ + S->nB;
     cudaError_t e = krylov_alloc(S, m);
     if (e != cudaSuccess) return e;
     cudaStream_t st = S->stream;
     std::vector<double> H(static_cast<size_t>(m + 1) * m), cs(m), sn(m), g(m + 1), y(m), h(m + 1);
-    double res = 1.0;
-    int it = 0;
+    double res = 1.0, beta = 0.0;
+    int it = 0, cycles = 0;
+    bool have_r = false;  // V_0 already holds the true residual (from a failed confirmation)
     const int gr = grid_for(S, n);
     while (it < max_it) {
-        // r = b - (I - T) x  into V_0
-        e = op_apply(S, prec, x, S->kv);
-        if (e != cudaSuccess) return e;
-        k_axpby<<<gr, 256, 0, st>>>(n, 1.0, b, -1.0, S->kv);
-        ++S->launches;
-        double beta = 0.0;
-        if ((e = vnorm(S, S->kv, &beta)) != cudaSuccess) return e;
+        // r = b - (I - T) x  into V_0, the operator in the residual precision
+        ++cycles;
+        if (!have_r) {
+            e = op_apply(S, prec_res, x, S->kv);
+            if (e != cudaSuccess) return e;
+            k_axpby<<<gr, 256, 0, st>>>(n, 1.0, b, -1.0, S->kv);
+            ++S->launches;
+            if ((e = vnorm(S, S->kv, &beta)) != cudaSuccess) return e;
+        }
+        have_r = false;
         res = beta / bref;
         if (res <= rtol || beta == 0.0) break;
         k_axpby<<<gr, 256, 0, st>>>(n, 0.0, S->kv, 1.0 / beta, S->kv);
@@ -1576,7 +1578,7 @@ static cudaError_t gmres(tr_sweep *S, int prec, const double *b, double *x, int 
             g[j + 1] = -sn[j] * g[j];
             g[j] = cs[j] * g[j];
             res = std::fabs(g[j + 1]) / bref;
-            if (res <= rtol) {
+            if (res <= rtol || (cycle_tol > 0.0 && std::fabs(g[j + 1]) <= cycle_tol * beta)) {
                 ++j;
                 break;
             }
@@ -1590,18 +1592,19 @@ static cudaError_t gmres(tr_sweep *S, int prec, const double *b, double *x, int 
         if (e != cudaSuccess) return e;
         k_combine<<<gr, 256, 0, st>>>(n, j, S->kv, n, S->kh, x);
         ++S->launches;
-        if (res <= rtol) {  // confirm with the true residual
-            if ((e = op_apply(S, prec, x, S->kt)) != cudaSuccess) return e;
-            k_axpby<<<gr, 256, 0, st>>>(n, 1.0, b, -1.0, S->kt);
+        if (res <= rtol || cycle_tol > 0.0) {  // the true residual: confirm, or start the next cycle from it
+            if ((e = op_apply(S, prec_res, x, S->kv)) != cudaSuccess) return e;
+            k_axpby<<<gr, 256, 0, st>>>(n, 1.0, b, -1.0, S->kv);
             ++S->launches;
-            double tr = 0.0;
-            if ((e = vnorm(S, S->kt, &tr)) != cudaSuccess) return e;
-            res = tr / bref;
+            if ((e = vnorm(S, S->kv, &beta)) != cudaSuccess) return e;
+            res = beta / bref;
             if (res <= rtol) break;
+            have_r = true;
         }
     }
     *its = it;
     *res_out = res;
+    if (cycles_out) *cycles_out = cycles;
     return cudaSuccess;
 }
 
@@ -1901,40 +1904,16 @@ tr_status tr_sweep_solve(tr_sweep *s, const tr_sweep_opts *opts, double *J, doub
                 }
             }
         } else if (o.mode == TR_MODE_FP64) {
-            e = gmres(s, 64, s->kb, s->kx, o.restart, o.tol, bn, o.max_iter, &its, &res);
+            e = gmres(s, 64, 64, s->kb, s->kx, o.restart, o.tol, bn, 0.0, o.max_iter, &its, &res, nullptr);
             conv = e == cudaSuccess && res <= o.tol;
         } else {
-            // FP32 sweeps inside FP64 defect correction: r = b - (I - T_64) x;
-            // (I - T_32) d = r by GMRES; x += d
-            e = cudaMemcpyAsync(s->kr, s->kb, n * 8, cudaMemcpyDeviceToDevice, st);
-            double rn = bn;
-            while (e == cudaSuccess && outer < o.max_outer && its < o.max_iter) {
-                ++outer;
-                // inner reduction: what is still missing to tol (x 0.3), but no
-                // deeper than 1e-4, which FP32 sweeps reach reliably
-                double want = o.inner_tol > 0.0 ? o.inner_tol : std::max(1e-4, 0.3 * o.tol * bn / rn);
-                want = std::min(want, 0.5);
-                e = cudaMemsetAsync(s->kd, 0, n * 8, st);
-                int it_in = 0;
-                double res_in = 0.0;
-                if (e == cudaSuccess) {
-                    // the correction accumulates in kd; its right-hand side is kr
-                    e = gmres(s, 32, s->kr, s->kd, o.restart, want, rn, o.max_iter - its, &it_in, &res_in);
-                }
-                its += it_in;
-                if (e != cudaSuccess) break;
-                k_axpby<<<gr, 256, 0, st>>>(n, 1.0, s->kd, 1.0, s->kx);
-                ++s->launches;
-                if ((e = op_apply(s, 64, s->kx, s->kr)) != cudaSuccess) break;
-                k_axpby<<<gr, 256, 0, st>>>(n, 1.0, s->kb, -1.0, s->kr);
-                ++s->launches;
-                if ((e = vnorm(s, s->kr, &rn)) != cudaSuccess) break;
-                res = rn / bn;
-                if (res <= o.tol) {
-                    conv = true;
-                    break;
-                }
-            }
+            // FP32 sweeps inside FP64 defect correction: each GMRES cycle starts
+            // from the FP64 residual r = b - (I - T_64) x (one FP64 sweep) and
+            // builds its Krylov space with FP32 sweeps; the correction is added
+            // to x in FP64.  A cycle ends at its restart length, at the target,
+            // or (inner_tol > 0) once it has reduced its residual by inner_tol.
+            e = gmres(s, 32, 64, s->kb, s->kx, o.restart, o.tol, bn, o.inner_tol, o.max_iter, &its, &res, &outer);
+            conv = e == cudaSuccess && res <= o.tol;
         }
     }
     if (e == cudaSuccess) e = cudaMemcpyAsync(J, s->kx, s->nJ * 8, cudaMemcpyDeviceToDevice, st);
