@@ -448,7 +448,10 @@ double tr_spherical_value(int l, int m, double x, double y, double z);
 /* HemiQuad(mindegree) (HemiQuad.cpp:265-286) / LebedevQuad(mindegree)
  * (LebedevQuad.cpp:6269-6277): returns the rule's number of points and, if
  * cap >= that number, fills x, y, z, w (weights sum to 1).  Returns -1 for
- * an unsupported degree. */
+ * an unsupported degree.  The Lebedev rules are generated from their
+ * defining equations instead of stored tables, up to 194 points (precision
+ * 23; the first call for a rule solves it, a few seconds for 194 points);
+ * the points may come in another order than the reference's tables. */
 int tr_hemiquad(int mindegree, double *x, double *y, double *z, double *w, int cap);
 int tr_lebedev(int mindegree, double *x, double *y, double *z, double *w, int cap);
 

@@ -100,6 +100,35 @@ def test_hemiquad_matches_reference(deg):
     assert abs(ours[3].sum() - 1.0) < 1e-14
 
 
+def _sorted_rule(r):
+    r = np.asarray(r)
+    idx = np.lexsort((r[2].round(9), r[1].round(9), r[0].round(9)))
+    return r[:, idx]
+
+
+@pytest.mark.parametrize("deg", [2, 6, 10, 14, 17, 18, 22])
+def test_lebedev_matches_reference(deg):
+    """The generated rules are the reference's LebedevQuad point sets
+    (LebedevQuad.cpp) up to the order of the points."""
+    g = golden("quadrature.npz")[f"lebedev_{deg}"]
+    ours = rule(tr.lib.tr_lebedev, deg)
+    assert ours.shape == g.shape
+    assert np.abs(_sorted_rule(ours) - _sorted_rule(g)).max() < 1e-11
+    assert abs(ours[3].sum() - 1.0) < 1e-14
+    # exact for the real harmonics up to the rule's precision
+    prec = {6: 3, 26: 7, 50: 11, 86: 15, 110: 17, 146: 19, 194: 23}[g.shape[1]]
+    x, y, z, w = ours
+    for l in range(1, prec + 1):
+        for m in range(-l, l + 1):
+            v = np.array([tr.lib.tr_spherical_value(l, m, a, b, c) for a, b, c in zip(x, y, z)])
+            assert abs((w * v).sum()) < 1e-12
+
+
+@pytest.mark.parametrize("deg", [26, 29, 30])
+def test_lebedev_beyond_generated_rules_is_refused(deg):
+    assert tr.lib.tr_lebedev(deg, None, None, None, None, 0) == -1
+
+
 def test_trieig_matches_reference():
     g = golden("misc.npz")
     o = 0

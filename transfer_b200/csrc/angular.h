@@ -46,11 +46,12 @@ struct HemiQuad {
 
 // Lebedev rule of algebraic precision >= mindegree (LebedevQuad.cpp:6269-6277):
 // the smallest of the tabulated octahedral rules whose precision reaches
-// mindegree; weights sum to 1.  See lebedev.cpp for how the rules are
-// obtained.
+// mindegree; weights sum to 1.  The rules (up to 194 points) are generated
+// from their defining equations (lebedev.cpp); throws for larger ones.
 struct LebedevQuad {
-    int order;
+    int order = 0;
     std::vector<double> x, y, z, w;
+    LebedevQuad() {}
     explicit LebedevQuad(int mindegree);
 };
 // Number of points of the Lebedev rule with precision >= prec, or -1

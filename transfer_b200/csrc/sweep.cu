@@ -11,7 +11,7 @@
 //   rhs_i = sigma_s V/20 (J_i + sum_j J_j) + sigma_a V B/4
 //           + sum_{k in, k!=i} a_k/12 (T_k + psi_up_{k,i}),
 // a_k = -Omega.s_k (> 0 on inflow faces), T_k the sum of the three upwind
-// traces on face k, solved by Gaussian elimination without pivoting (the
+// traces on face k, solved by the adjugate formula (solve4; the
 // symmetric part of L is positive definite).  J = sum_q w_q psi_q.
 //
 // Device layout (one GPU; SoA, cell-major):
@@ -386,14 +386,25 @@ __device__ __forceinline__ void stage_task(Slot<T> &sl, const uint4 rec, const G
     for (int k = 0; k < 4; ++k) {
         if (!(mask >> k & 1u) || t >= 3) continue;
         const uint32_t code = t == 0 ? rec.y : t == 1 ? rec.z : rec.w;
+        // every non-interior inflow face gets its 4 values staged (zeros where none)
         if (code & kLagBit) {
-            if (a.Bin) cp_async_bytes(sl.bv[t], a.Bin + a.lag_base + 4 * (size_t)(code & ~kLagBit), 4 * sizeof(T));
+            if (a.Bin) {
+                cp_async_bytes(sl.bv[t], a.Bin + a.lag_base + 4 * (size_t)(code & ~kLagBit), 4 * sizeof(T));
+            } else {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) sl.bv[t][j] = T(0);
+            }
         } else if (code & kBndBit) {
             const uint32_t type = (code >> 28) & 3u, idx = code & kBndIndex;
-            if (type == TR_BC_REFLECTIVE && a.Bin)
+            if (type == TR_BC_REFLECTIVE && a.Bin) {
                 cp_async_bytes(sl.bv[t], a.Bin + 4 * (size_t)idx, 4 * sizeof(T));
-            else if (type == TR_BC_INCIDENT && a.with_ext)
-                cp_async_small<sizeof(T)>(&sl.bv[t][0], g.finc + idx);
+            } else if (type == TR_BC_INCIDENT && a.with_ext) {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) cp_async_small<sizeof(T)>(&sl.bv[t][j], g.finc + idx);
+            } else {
+#pragma unroll
+                for (int j = 0; j < 4; ++j) sl.bv[t][j] = T(0);
+            }
         }
         ++t;
     }
@@ -448,6 +459,33 @@ __device__ __forceinline__ void inflow_values(uint32_t code, const T *staged, bo
 #pragma unroll
         for (int j = 0; j < 4; ++j) up[j] = comp<T>(v, (mp >> (2 * (4 * k + j))) & 3u);
     }
+}
+
+// x = L^-1 r for one cell by the adjugate (2x2 minors of rows 0-1 and 2-3,
+// one division): a short dependency chain with much independent work, where
+// Gaussian elimination would chain four pivots and eight divisions.  The
+// matrices are well conditioned (positive definite symmetric part).
+template <typename T>
+__device__ __forceinline__ void solve4(const T (&a)[4][4], const T (&r)[4], T (&x)[4]) {
+    const T s0 = a[0][0] * a[1][1] - a[1][0] * a[0][1], s1 = a[0][0] * a[1][2] - a[1][0] * a[0][2];
+    const T s2 = a[0][0] * a[1][3] - a[1][0] * a[0][3], s3 = a[0][1] * a[1][2] - a[1][1] * a[0][2];
+    const T s4 = a[0][1] * a[1][3] - a[1][1] * a[0][3], s5 = a[0][2] * a[1][3] - a[1][2] * a[0][3];
+    const T c5 = a[2][2] * a[3][3] - a[3][2] * a[2][3], c4 = a[2][1] * a[3][3] - a[3][1] * a[2][3];
+    const T c3 = a[2][1] * a[3][2] - a[3][1] * a[2][2], c2 = a[2][0] * a[3][3] - a[3][0] * a[2][3];
+    const T c1 = a[2][0] * a[3][2] - a[3][0] * a[2][2], c0 = a[2][0] * a[3][1] - a[3][0] * a[2][1];
+    const T det = s0 * c5 - s1 * c4 + s2 * c3 + s3 * c2 - s4 * c1 + s5 * c0;
+    const T b[4][4] = {
+        {a[1][1] * c5 - a[1][2] * c4 + a[1][3] * c3, -a[0][1] * c5 + a[0][2] * c4 - a[0][3] * c3,
+         a[3][1] * s5 - a[3][2] * s4 + a[3][3] * s3, -a[2][1] * s5 + a[2][2] * s4 - a[2][3] * s3},
+        {-a[1][0] * c5 + a[1][2] * c2 - a[1][3] * c1, a[0][0] * c5 - a[0][2] * c2 + a[0][3] * c1,
+         -a[3][0] * s5 + a[3][2] * s2 - a[3][3] * s1, a[2][0] * s5 - a[2][2] * s2 + a[2][3] * s1},
+        {a[1][0] * c4 - a[1][1] * c2 + a[1][3] * c0, -a[0][0] * c4 + a[0][1] * c2 - a[0][3] * c0,
+         a[3][0] * s4 - a[3][1] * s2 + a[3][3] * s0, -a[2][0] * s4 + a[2][1] * s2 - a[2][3] * s0},
+        {-a[1][0] * c3 + a[1][1] * c1 - a[1][2] * c0, a[0][0] * c3 - a[0][1] * c1 + a[0][2] * c0,
+         -a[3][0] * s3 + a[3][1] * s1 - a[3][2] * s0, a[2][0] * s3 - a[2][1] * s1 + a[2][2] * s0}};
+    const T inv = T(1) / det;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) x[i] = (b[i][0] * r[0] + b[i][1] * r[1] + b[i][2] * r[2] + b[i][3] * r[3]) * inv;
 }
 
 template <typename T>
@@ -536,6 +574,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, Sw
                 r[i] = ssv * c20 * (Jc[i] + Js) + ext;
             }
             const uint32_t mp = sl.map;
+            const T *ring_s = reinterpret_cast<const T *>(ring);
             int t = 0;
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
@@ -543,7 +582,18 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, Sw
                 T up[4] = {T(0), T(0), T(0), T(0)};
                 if (t < 3) {
                     const uint32_t code = t == 0 ? rec.y : t == 1 ? rec.z : rec.w;
-                    inflow_values<T>(code, sl.bv[t], true, g, a, ring, R, e0, psi, c, k, mp, up);
+                    if (code & (kLagBit | kBndBit)) {
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) up[j] = sl.bv[t][j];
+                    } else if (code + R >= e0) {  // upwind trace from the ring
+                        const T *src = ring_s + 4 * (size_t)(code % R);
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) up[j] = src[(mp >> (2 * (4 * k + j))) & 3u];
+                    } else {                      // older than the ring: global psi
+                        const T *src = psi + 4 * (size_t)__ldg(g.nbr + 4 * (size_t)c + k);
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) up[j] = src[(mp >> (2 * (4 * k + j))) & 3u];
+                    }
                 } else {
                     // the fourth inflow face of an inverted element: its source from the side table
                     const unsigned long long key = (unsigned long long)q * nT + p;
@@ -564,26 +614,8 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, Sw
                 for (int i = 0; i < 4; ++i)
                     if (i != k) r[i] += ak * (Tk + up[i]);
             }
-            // Gaussian elimination without pivoting
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const T inv = T(1) / Lm[k][k];
-#pragma unroll
-                for (int i = k + 1; i < 4; ++i) {
-                    const T f = Lm[i][k] * inv;
-#pragma unroll
-                    for (int j = k + 1; j < 4; ++j) Lm[i][j] -= f * Lm[k][j];
-                    r[i] -= f * r[k];
-                }
-            }
             T o[4];
-#pragma unroll
-            for (int i = 3; i >= 0; --i) {
-                T v = r[i];
-#pragma unroll
-                for (int j = i + 1; j < 4; ++j) v -= Lm[i][j] * o[j];
-                o[i] = v / Lm[i][i];
-            }
+            solve4<T>(Lm, r, o);
             V out;
             out.x = o[0];
             out.y = o[1];
@@ -1301,6 +1333,8 @@ static tr_status sweep_setup(tr_sweep *S, const tr_mesh_view *m, const tr_physic
     }
     // cells with four inflow faces: their face-3 sources, sorted by (ordinate, position)
     uint32_t n_f4 = 0;
+    // the context stream does not synchronise with the legacy stream of cudaMemcpy
+    if (e == cudaSuccess) e = cudaStreamSynchronize(S->stream);
     if (e == cudaSuccess) e = cudaMemcpy(&n_f4, f4_count, 4, cudaMemcpyDeviceToHost);
     if (e == cudaSuccess && n_f4 > kMaxLag && st == TR_OK)
         st = sw_err(S, TR_ERR_UNSUPPORTED, "sweep: too many inverted elements");
