@@ -171,7 +171,12 @@ void eval(const Problem &pr, const std::vector<int> &kinds, const std::vector<do
         }
         pi += np;
     }
-    for (int e = 0; e < ne; ++e) F[e] -= pr.target[e];
+    // rows scaled by 1 / target, so that every equation counts to relative precision
+    for (int e = 0; e < ne; ++e) {
+        F[e] = F[e] / pr.target[e] - 1.0;
+        if (J)
+            for (int k = 0; k < nv; ++k) (*J)[static_cast<size_t>(e) * nv + k] /= pr.target[e];
+    }
 }
 
 // solves (A) x = b, A n x n (copied), partial pivoting; false if singular
@@ -482,8 +487,8 @@ bool generate(const OrbitSpec &sp, LebedevQuad &q) {
         std::vector<double> F;
         eval(pr, kinds, v, F, nullptr);
         double worst = 0.0;
-        for (size_t e = 0; e < F.size(); ++e) worst = std::fmax(worst, std::fabs(F[e]) / pr.target[e]);
-        if (worst > 1e-13) continue;
+        for (size_t e = 0; e < F.size(); ++e) worst = std::fmax(worst, std::fabs(F[e]));
+        if (worst > 1e-14) continue;
         q.x.clear();
         q.y.clear();
         q.z.clear();

@@ -89,6 +89,7 @@ struct Geom {
     const T *stv;        // sigma_t V
     const T *ssv;        // sigma_s V
     const T *ext;        // sigma_a V B / 4
+    const T *coef;       // [nT][4]: sigma_t V, sigma_s V, sigma_a V B / 4, 0
     const int32_t *nbr;  // [nT][4]
     const uint32_t *map; // [nT]
     const int32_t *fbc;  // [nF]
@@ -341,18 +342,30 @@ __device__ __forceinline__ double4 load_v4<double>(const double *p) {
 // (task records two tasks ahead, in registers), so that a level costs the
 // arithmetic of its cells, a shared-memory read of the upwind traces and a
 // block barrier instead of a chain of dependent global loads.
+// The two staging slots of each thread are stored field by field in
+// 16-byte units, unit-major across the block's threads, so a warp's reads
+// of one field are contiguous (no bank conflicts).  Per slot: normals s (12
+// reals), source J (4), inflow values bv of up to three non-interior faces
+// (3 x 4), coefficients (sigma_t V, sigma_s V, sigma_a V B / 4, -) and the
+// vertex map.
 template <typename T>
-struct alignas(16) Slot {
-    T s[12];
-    T J[4];
-    T bv[3][4];      // inflow values of boundary / lagged faces, by inflow order
-    T coef[4];       // sigma_t V, sigma_s V, sigma_a V B / 4, -
-    uint32_t map, pad[3];
+struct Slots {
+    static constexpr int kR = 16 / sizeof(T);          // reals per unit
+    static constexpr int kS = 0, kJ = 12 / kR, kBv = kJ + 4 / kR, kCoef = kBv + 12 / kR, kMap = kCoef + 4 / kR;
+    static constexpr int kUnits = kMap + 1;
+    unsigned char *base;
+    __device__ __forceinline__ T *unit(int slot, int u) const {
+        return reinterpret_cast<T *>(base + ((static_cast<size_t>(slot) * kUnits + u) * kSweepThreads + threadIdx.x) * 16);
+    }
+    __device__ __forceinline__ T &el(int slot, int u0, int e) const { return unit(slot, u0 + e / kR)[e % kR]; }
+    __device__ __forceinline__ uint32_t &map(int slot) const {
+        return *reinterpret_cast<uint32_t *>(unit(slot, kMap));
+    }
 };
 template <typename T>
 constexpr int ring_bytes() { return sizeof(T) == 4 ? 64 * 1024 : 40 * 1024; }
 template <typename T>
-constexpr size_t sweep_smem() { return ring_bytes<T>() + 2ull * kSweepThreads * sizeof(Slot<T>); }
+constexpr size_t sweep_smem() { return ring_bytes<T>() + 2ull * Slots<T>::kUnits * kSweepThreads * 16; }
 
 __device__ __forceinline__ void cp_async16(void *dst, const void *src) {
     const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
@@ -373,38 +386,46 @@ __device__ __forceinline__ void cp_async_bytes(void *dst, const void *src, int b
 }
 
 template <typename T>
-__device__ __forceinline__ void stage_task(Slot<T> &sl, const uint4 rec, const Geom<T> &g, const SweepArgs<T> &a) {
+__device__ __forceinline__ void stage_task(const Slots<T> &S, int slot, const uint4 rec, const Geom<T> &g,
+                                           const SweepArgs<T> &a) {
+    using Sl = Slots<T>;
     const uint32_t c = rec.x & kCellMask, mask = rec.x >> 28;
-    cp_async_bytes(sl.s, g.s + 12 * (size_t)c, 12 * sizeof(T));
-    if (a.J) cp_async_bytes(sl.J, a.J + 4 * (size_t)c, 4 * sizeof(T));
-    cp_async_small<sizeof(T)>(&sl.coef[0], g.stv + c);
-    cp_async_small<sizeof(T)>(&sl.coef[1], g.ssv + c);
-    if (a.with_ext) cp_async_small<sizeof(T)>(&sl.coef[2], g.ext + c);
-    cp_async_small<4>(&sl.map, g.map + c);
+    for (int u = 0; u < 12 / Sl::kR; ++u) cp_async16(S.unit(slot, Sl::kS + u), g.s + 12 * (size_t)c + u * Sl::kR);
+    if (a.J)
+        for (int u = 0; u < 4 / Sl::kR; ++u) cp_async16(S.unit(slot, Sl::kJ + u), a.J + 4 * (size_t)c + u * Sl::kR);
+    for (int u = 0; u < 4 / Sl::kR; ++u) cp_async16(S.unit(slot, Sl::kCoef + u), g.coef + 4 * (size_t)c + u * Sl::kR);
+    cp_async_small<4>(&S.map(slot), g.map + c);
     int t = 0;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         if (!(mask >> k & 1u) || t >= 3) continue;
         const uint32_t code = t == 0 ? rec.y : t == 1 ? rec.z : rec.w;
+        const int u0 = Sl::kBv + t * (4 / Sl::kR);
         // every non-interior inflow face gets its 4 values staged (zeros where none)
+        const T *src = nullptr;
+        bool bcast = false;
         if (code & kLagBit) {
-            if (a.Bin) {
-                cp_async_bytes(sl.bv[t], a.Bin + a.lag_base + 4 * (size_t)(code & ~kLagBit), 4 * sizeof(T));
-            } else {
-#pragma unroll
-                for (int j = 0; j < 4; ++j) sl.bv[t][j] = T(0);
-            }
+            if (a.Bin) src = a.Bin + a.lag_base + 4 * (size_t)(code & ~kLagBit);
         } else if (code & kBndBit) {
             const uint32_t type = (code >> 28) & 3u, idx = code & kBndIndex;
             if (type == TR_BC_REFLECTIVE && a.Bin) {
-                cp_async_bytes(sl.bv[t], a.Bin + 4 * (size_t)idx, 4 * sizeof(T));
+                src = a.Bin + 4 * (size_t)idx;
             } else if (type == TR_BC_INCIDENT && a.with_ext) {
-#pragma unroll
-                for (int j = 0; j < 4; ++j) cp_async_small<sizeof(T)>(&sl.bv[t][j], g.finc + idx);
-            } else {
-#pragma unroll
-                for (int j = 0; j < 4; ++j) sl.bv[t][j] = T(0);
+                src = g.finc + idx;
+                bcast = true;
             }
+        } else {
+            ++t;
+            continue;
+        }
+        if (src && !bcast) {
+            for (int u = 0; u < 4 / Sl::kR; ++u) cp_async16(S.unit(slot, u0 + u), src + u * Sl::kR);
+        } else if (src) {
+#pragma unroll
+            for (int e = 0; e < 4; ++e) cp_async_small<sizeof(T)>(&S.el(slot, u0, e), src);
+        } else {
+#pragma unroll
+            for (int e = 0; e < 4; ++e) S.el(slot, u0, e) = T(0);
         }
         ++t;
     }
@@ -494,7 +515,8 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, Sw
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr uint32_t R = ring_bytes<T>() / sizeof(V);
     V *ring = reinterpret_cast<V *>(smem_raw);
-    Slot<T> *slots = reinterpret_cast<Slot<T> *>(smem_raw + ring_bytes<T>()) + 2 * threadIdx.x;
+    const Slots<T> SL{smem_raw + ring_bytes<T>()};
+    using Sl = Slots<T>;
     const uint32_t q = blockIdx.x, nT = a.nT;
     const T ox = a.ox[q], oy = a.oy[q], oz = a.oz[q];
     const uint4 *task = sc.task + (size_t)q * nT;
@@ -517,7 +539,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, Sw
     uint32_t p1 = kNone;
     if (pst != kNone) {
         r_cur = __ldg(task + pst);
-        stage_task<T>(slots[cur], r_cur, g, a);
+        stage_task<T>(SL, cur, r_cur, g, a);
         p1 = next_task(L1, pst, lvl, nl);
         if (p1 != kNone) r1 = __ldg(task + p1);
     }
@@ -529,7 +551,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, Sw
             if (p != pst) {  // not staged ahead: fetch now
                 cp_async_wait<0>();
                 r_cur = __ldg(task + p);
-                stage_task<T>(slots[cur], r_cur, g, a);
+                stage_task<T>(SL, cur, r_cur, g, a);
                 cp_async_commit();
                 pst = p;
                 L1 = L;
@@ -540,27 +562,28 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, Sw
             uint32_t L2 = L1, p2 = kNone;
             uint4 r2 = make_uint4(0, 0, 0, 0);
             if (p1 != kNone) {
-                stage_task<T>(slots[cur ^ 1], r1, g, a);
+                stage_task<T>(SL, cur ^ 1, r1, g, a);
                 p2 = next_task(L2, p1, lvl, nl);
                 if (p2 != kNone) r2 = __ldg(task + p2);
             }
             cp_async_commit();
             cp_async_wait<1>();  // this task's group has landed
-            const Slot<T> &sl = slots[cur];
             const uint4 rec = r_cur;
             const uint32_t c = rec.x & kCellMask, mask = rec.x >> 28;
             T av[4], al[4], Ain = T(0);
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                av[k] = -(ox * sl.s[3 * k] + oy * sl.s[3 * k + 1] + oz * sl.s[3 * k + 2]);
+                av[k] = -(ox * SL.el(cur, Sl::kS, 3 * k) + oy * SL.el(cur, Sl::kS, 3 * k + 1) +
+                          oz * SL.el(cur, Sl::kS, 3 * k + 2));
                 al[k] = (mask >> k & 1u) ? av[k] : T(0);
                 Ain += al[k];
             }
-            const T stv = sl.coef[0], ssv = sl.coef[1], ext = a.with_ext ? sl.coef[2] : T(0);
+            const T stv = SL.el(cur, Sl::kCoef, 0), ssv = SL.el(cur, Sl::kCoef, 1);
+            const T ext = a.with_ext ? SL.el(cur, Sl::kCoef, 2) : T(0);
             T Jc[4] = {T(0), T(0), T(0), T(0)};
             if (a.J) {
 #pragma unroll
-                for (int j = 0; j < 4; ++j) Jc[j] = sl.J[j];
+                for (int j = 0; j < 4; ++j) Jc[j] = SL.el(cur, Sl::kJ, j);
             }
             const T Js = Jc[0] + Jc[1] + Jc[2] + Jc[3];
             T Lm[4][4], r[4];
@@ -573,7 +596,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, Sw
                 }
                 r[i] = ssv * c20 * (Jc[i] + Js) + ext;
             }
-            const uint32_t mp = sl.map;
+            const uint32_t mp = SL.map(cur);
             const T *ring_s = reinterpret_cast<const T *>(ring);
             int t = 0;
 #pragma unroll
@@ -584,7 +607,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, Sw
                     const uint32_t code = t == 0 ? rec.y : t == 1 ? rec.z : rec.w;
                     if (code & (kLagBit | kBndBit)) {
 #pragma unroll
-                        for (int j = 0; j < 4; ++j) up[j] = sl.bv[t][j];
+                        for (int j = 0; j < 4; ++j) up[j] = SL.el(cur, Sl::kBv + t * (4 / Sl::kR), j);
                     } else if (code + R >= e0) {  // upwind trace from the ring
                         const T *src = ring_s + 4 * (size_t)(code % R);
 #pragma unroll
@@ -985,6 +1008,8 @@ struct tr_sweep {
     int num_sms = 0;
     // geometry and physics
     double *s64 = nullptr, *stv64 = nullptr, *ssv64 = nullptr, *ext64 = nullptr, *finc64 = nullptr;
+    double *coef64 = nullptr;  // [nT][4] sigma_t V, sigma_s V, sigma_a V B / 4, 0
+    float *coef32 = nullptr;
     float *s32 = nullptr, *stv32 = nullptr, *ssv32 = nullptr, *ext32 = nullptr, *finc32 = nullptr;
     int32_t *nbr = nullptr, *fbc = nullptr, *rslot = nullptr;
     uint32_t *map = nullptr, *bcell = nullptr, *bface = nullptr;
@@ -1237,7 +1262,13 @@ static tr_status sweep_setup(tr_sweep *S, const tr_mesh_view *m, const tr_physic
     cudaError_t e = cudaSuccess;
 #define UP(ptr, vec)                                         \
     if (e == cudaSuccess) e = sw_upload(S, &S->ptr, vec);
-    UP(s64, s) UP(stv64, stv) UP(ssv64, ssv) UP(ext64, ext) UP(finc64, finc)
+    std::vector<double> coef(4ull * nT, 0.0);
+    for (uint32_t c = 0; c < nT; ++c) {
+        coef[4ull * c] = stv[c];
+        coef[4ull * c + 1] = ssv[c];
+        coef[4ull * c + 2] = ext[c];
+    }
+    UP(s64, s) UP(stv64, stv) UP(ssv64, ssv) UP(ext64, ext) UP(finc64, finc) UP(coef64, coef) UP(coef32, f32(coef))
     UP(s32, f32(s)) UP(stv32, f32(stv)) UP(ssv32, f32(ssv)) UP(ext32, f32(ext)) UP(finc32, f32(finc))
     UP(nbr, nbr) UP(fbc, fbc) UP(rslot, rslot) UP(map, map) UP(rent, rent) UP(ent_cell, ent_cell) UP(ent_qout, ent_qout) UP(bcell, bcell) UP(bface, bface)
     UP(o64[0], ox) UP(o64[1], oy) UP(o64[2], oz) UP(o64[3], w) UP(o32[0], ox32) UP(o32[1], oy32) UP(o32[2], oz32)
@@ -1377,7 +1408,7 @@ static tr_status sweep_setup(tr_sweep *S, const tr_mesh_view *m, const tr_physic
     if (e != cudaSuccess) return sw_cuda(S, e, "sweep: schedule");
     S->nB = 4ull * S->nent + 4ull * nlag;
     // reductions
-    if (e == cudaSuccess) e = sw_alloc(S, &S->partials, 64ull * kRedGrid);
+    if (e == cudaSuccess) e = sw_alloc(S, &S->partials, (kMaxRestart + 2ull) * kRedGrid);
     if (e == cudaSuccess) e = sw_alloc(S, &S->red, 256);
     if (e == cudaSuccess) e = sw_alloc(S, &S->counter, 4);
     if (e == cudaSuccess) e = cudaMemset(S->counter, 0, 16);
@@ -1413,12 +1444,14 @@ static Geom<T> geom_of(const tr_sweep *S) {
     if constexpr (sizeof(T) == 8) {
         g.s = S->s64;
         g.stv = S->stv64;
+        g.coef = S->coef64;
         g.ssv = S->ssv64;
         g.ext = S->ext64;
         g.finc = S->finc64;
     } else {
         g.s = S->s32;
         g.stv = S->stv32;
+        g.coef = S->coef32;
         g.ssv = S->ssv32;
         g.ext = S->ext32;
         g.finc = S->finc32;
@@ -1584,14 +1617,23 @@ static cudaError_t gmres(tr_sweep *S, int prec, int prec_res, const double *b, d
             double *w = S->kv + static_cast<uint64_t>(j + 1) * n;
             if ((e = op_apply(S, prec, S->kv + static_cast<uint64_t>(j) * n, w)) != cudaSuccess) return e;
             ++it;
-            for (int pass = 0; pass < 2; ++pass) {  // classical Gram-Schmidt, twice
+            // classical Gram-Schmidt; the first pass also gives ||w||^2 (w is
+            // basis row j + 1), and a second pass runs only when the first
+            // cancelled most of w (Daniel-Gragg-Kaufman-Stewart criterion)
+            if ((e = dots(S, j + 2, S->kv, n, w, S->kh, h.data())) != cudaSuccess) return e;
+            const double w0 = std::sqrt(std::fmax(h[j + 1], 0.0));
+            k_gs_update<<<gr, 256, 0, st>>>(n, j + 1, S->kv, n, S->kh, w);
+            ++S->launches;
+            for (int i = 0; i <= j; ++i) H[static_cast<size_t>(i) * m + j] += h[i];
+            double hn = 0.0;
+            if ((e = vnorm(S, w, &hn)) != cudaSuccess) return e;
+            if (hn < 0.7 * w0) {
                 if ((e = dots(S, j + 1, S->kv, n, w, S->kh, h.data())) != cudaSuccess) return e;
                 k_gs_update<<<gr, 256, 0, st>>>(n, j + 1, S->kv, n, S->kh, w);
                 ++S->launches;
                 for (int i = 0; i <= j; ++i) H[static_cast<size_t>(i) * m + j] += h[i];
+                if ((e = vnorm(S, w, &hn)) != cudaSuccess) return e;
             }
-            double hn = 0.0;
-            if ((e = vnorm(S, w, &hn)) != cudaSuccess) return e;
             H[static_cast<size_t>(j + 1) * m + j] = hn;
             if (hn > 0.0) {
                 k_axpby<<<gr, 256, 0, st>>>(n, 0.0, w, 1.0 / hn, w);
