@@ -12,6 +12,12 @@ plain FP64 CG (the drop-in) is timed in the same run.  A cell-ordinate
 update is one (tetrahedron, harmonic) pair of one operator application:
 nT * slm per application, FP32 and FP64 applications both counted.
 
+The line's "sweep" object measures the discrete-ordinates sweep on the
+Milne slab (scattering albedo 0.999, 112 ordinates): one sweep alone (FP32
+and FP64), GMRES solves to the same FP64 residual (FP64 and FP32 sweeps in
+FP64 defect correction), the FP64 energy balance and the CPU restatement's
+sweep rate (--no-sweep skips it).
+
 --gpus N runs N independent replicas (one process per GPU under torchrun):
 the solve does not shard (one GPU per problem), value = total updates of
 all ranks / the slowest rank's time.  --impl reference times the FP64 CPU

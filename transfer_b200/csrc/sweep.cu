@@ -890,18 +890,29 @@ __global__ void k_axpby(uint64_t n, double alpha, const double *x, double beta, 
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
         y[i] = alpha * x[i] + beta * y[i];
 }
-// out[i] = <V_i, w> for i < k; V rows of length n with stride ld
+// out[i] = <V_i, w> for i < k; V rows of length n with stride ld.  Eight
+// rows per pass over w (w is read k/8 times, each V row once), one partial
+// per block and row, summed in a fixed order by the last block.
 __global__ void k_multidot(uint64_t n, int k, const double *V, uint64_t ld, const double *w, double *partials,
                            unsigned int *counter, double *out) {
     __shared__ double sh[32];
     __shared__ bool am_last;
-    for (int i = 0; i < k; ++i) {
-        double acc = 0.0;
-        const double *v = V + (uint64_t)i * ld;
-        for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n; t += (uint64_t)gridDim.x * blockDim.x)
-            acc += v[t] * w[t];
-        double s = block_sum(acc, sh);
-        if (threadIdx.x == 0) partials[(uint64_t)i * gridDim.x + blockIdx.x] = s;
+    const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x, nth = (uint64_t)gridDim.x * blockDim.x;
+    for (int i0 = 0; i0 < k; i0 += 8) {
+        const int m = k - i0 < 8 ? k - i0 : 8;
+        double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        for (uint64_t t = tid; t < n; t += nth) {
+            const double wt = w[t];
+#pragma unroll
+            for (int ii = 0; ii < 8; ++ii)
+                if (ii < m) acc[ii] += V[(uint64_t)(i0 + ii) * ld + t] * wt;
+        }
+#pragma unroll
+        for (int ii = 0; ii < 8; ++ii) {
+            if (ii >= m) break;
+            const double sum = block_sum(acc[ii], sh);
+            if (threadIdx.x == 0) partials[(uint64_t)(i0 + ii) * gridDim.x + blockIdx.x] = sum;
+        }
     }
     __threadfence();
     __syncthreads();
@@ -913,8 +924,8 @@ __global__ void k_multidot(uint64_t n, int k, const double *V, uint64_t ld, cons
         double acc = 0.0;
         for (unsigned int b = threadIdx.x; b < gridDim.x; b += blockDim.x)
             acc += __ldcg(partials + (uint64_t)i * gridDim.x + b);
-        double s = block_sum(acc, sh);
-        if (threadIdx.x == 0) out[i] = s;
+        double sum = block_sum(acc, sh);
+        if (threadIdx.x == 0) out[i] = sum;
     }
     if (threadIdx.x == 0) *counter = 0u;
 }
