@@ -351,21 +351,37 @@ __device__ __forceinline__ double4 load_v4<double>(const double *p) {
 template <typename T>
 struct Slots {
     static constexpr int kR = 16 / sizeof(T);          // reals per unit
-    static constexpr int kS = 0, kJ = 12 / kR, kBv = kJ + 4 / kR, kCoef = kBv + 12 / kR, kMap = kCoef + 4 / kR;
-    static constexpr int kUnits = kMap + 1;
+    static constexpr int kS = 0, kJ = 12 / kR, kBv = kJ + 4 / kR, kCoef = kBv + 12 / kR;
+    static constexpr int kUnits = kCoef + 4 / kR;
     unsigned char *base;
     __device__ __forceinline__ T *unit(int slot, int u) const {
         return reinterpret_cast<T *>(base + ((static_cast<size_t>(slot) * kUnits + u) * kSweepThreads + threadIdx.x) * 16);
     }
     __device__ __forceinline__ T &el(int slot, int u0, int e) const { return unit(slot, u0 + e / kR)[e % kR]; }
-    __device__ __forceinline__ uint32_t &map(int slot) const {
-        return *reinterpret_cast<uint32_t *>(unit(slot, kMap));
+    // N reals of consecutive units from u0 into registers (16-byte shared loads)
+    template <int N>
+    __device__ __forceinline__ void load(int slot, int u0, T (&out)[N]) const {
+        const unsigned char *b = reinterpret_cast<const unsigned char *>(unit(slot, u0));
+#pragma unroll
+        for (int i = 0; i < N / kR; ++i) {
+            const uint4 v = *reinterpret_cast<const uint4 *>(b + static_cast<size_t>(i) * kSweepThreads * 16);
+            memcpy(&out[i * kR], &v, 16);
+        }
+    }
+    // the vertex map travels in the low 32 bits of the fourth coefficient
+    __device__ __forceinline__ uint32_t map(int slot) const {
+        return *reinterpret_cast<const uint32_t *>(&el(slot, kCoef, 3));
     }
 };
 template <typename T>
 constexpr int ring_bytes() { return sizeof(T) == 4 ? 64 * 1024 : 40 * 1024; }
+// level pointers of the block's ordinate, staged in shared memory when
+// there are at most kLevelCap levels (else read from global memory)
+constexpr uint32_t kLevelCap = 4096;
 template <typename T>
-constexpr size_t sweep_smem() { return ring_bytes<T>() + 2ull * Slots<T>::kUnits * kSweepThreads * 16; }
+constexpr size_t slots_bytes() { return 2ull * Slots<T>::kUnits * kSweepThreads * 16; }
+template <typename T>
+constexpr size_t sweep_smem() { return ring_bytes<T>() + slots_bytes<T>() + 4ull * (kLevelCap + 1); }
 
 __device__ __forceinline__ void cp_async16(void *dst, const void *src) {
     const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
@@ -394,7 +410,6 @@ __device__ __forceinline__ void stage_task(const Slots<T> &S, int slot, const ui
     if (a.J)
         for (int u = 0; u < 4 / Sl::kR; ++u) cp_async16(S.unit(slot, Sl::kJ + u), a.J + 4 * (size_t)c + u * Sl::kR);
     for (int u = 0; u < 4 / Sl::kR; ++u) cp_async16(S.unit(slot, Sl::kCoef + u), g.coef + 4 * (size_t)c + u * Sl::kR);
-    cp_async_small<4>(&S.map(slot), g.map + c);
     int t = 0;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -432,12 +447,13 @@ __device__ __forceinline__ void stage_task(const Slots<T> &S, int slot, const ui
 }
 
 // position of this thread's next task after (L, p), looking up to 4 levels
-// ahead (L is advanced to its level); kNone if none
+// ahead (L is advanced to its level); kNone if none.  lvl: the level
+// pointers in shared memory, or in global memory for very many levels
 __device__ __forceinline__ uint32_t next_task(uint32_t &L, uint32_t p, const uint32_t *lvl, uint32_t nl) {
     if (p == kNone) return kNone;
-    if (p + blockDim.x < __ldg(lvl + L + 1)) return p + blockDim.x;
+    if (p + blockDim.x < lvl[L + 1]) return p + blockDim.x;
     for (uint32_t d = 1; d <= 4 && L + d < nl; ++d) {
-        const uint32_t s1 = __ldg(lvl + L + d), e1 = __ldg(lvl + L + d + 1);
+        const uint32_t s1 = lvl[L + d], e1 = lvl[L + d + 1];
         if (s1 + threadIdx.x < e1) {
             L += d;
             return s1 + threadIdx.x;
@@ -520,8 +536,14 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, Sw
     const uint32_t q = blockIdx.x, nT = a.nT;
     const T ox = a.ox[q], oy = a.oy[q], oz = a.oz[q];
     const uint4 *task = sc.task + (size_t)q * nT;
-    const uint32_t *lvl = sc.lvl + (size_t)q * sc.lstride;
     const uint32_t nl = sc.nlev[q];
+    const uint32_t *lvl = sc.lvl + (size_t)q * sc.lstride;
+    if (nl <= kLevelCap) {
+        uint32_t *lv = reinterpret_cast<uint32_t *>(smem_raw + ring_bytes<T>() + slots_bytes<T>());
+        for (uint32_t L = threadIdx.x; L <= nl; L += blockDim.x) lv[L] = __ldg(lvl + L);
+        __syncthreads();
+        lvl = lv;
+    }
     T *psi = a.psi + (size_t)q * nT * 4;
     const T c12 = T(1) / T(12), c20 = T(1) / T(20);
 
@@ -529,8 +551,8 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, Sw
     // the position / record of the task after it (p1 at level L1, r1)
     uint32_t pst = kNone, L1 = 0;
     for (uint32_t d = 0; d < 5 && d < nl; ++d)
-        if (__ldg(lvl + d) + threadIdx.x < __ldg(lvl + d + 1)) {
-            pst = __ldg(lvl + d) + threadIdx.x;
+        if (lvl[d] + threadIdx.x < lvl[d + 1]) {
+            pst = lvl[d] + threadIdx.x;
             L1 = d;
             break;
         }
@@ -546,7 +568,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, Sw
     cp_async_commit();
 
     for (uint32_t L = 0; L < nl; ++L) {
-        const uint32_t s0 = __ldg(lvl + L), e0 = __ldg(lvl + L + 1);
+        const uint32_t s0 = lvl[L], e0 = lvl[L + 1];
         for (uint32_t p = s0 + threadIdx.x; p < e0; p += blockDim.x) {
             if (p != pst) {  // not staged ahead: fetch now
                 cp_async_wait<0>();
@@ -570,20 +592,23 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, Sw
             cp_async_wait<1>();  // this task's group has landed
             const uint4 rec = r_cur;
             const uint32_t c = rec.x & kCellMask, mask = rec.x >> 28;
+            T sv[12], cf[4];
+            SL.template load<12>(cur, Sl::kS, sv);
+            SL.template load<4>(cur, Sl::kCoef, cf);
             T av[4], al[4], Ain = T(0);
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                av[k] = -(ox * SL.el(cur, Sl::kS, 3 * k) + oy * SL.el(cur, Sl::kS, 3 * k + 1) +
-                          oz * SL.el(cur, Sl::kS, 3 * k + 2));
+                av[k] = -(ox * sv[3 * k] + oy * sv[3 * k + 1] + oz * sv[3 * k + 2]);
                 al[k] = (mask >> k & 1u) ? av[k] : T(0);
                 Ain += al[k];
             }
-            const T stv = SL.el(cur, Sl::kCoef, 0), ssv = SL.el(cur, Sl::kCoef, 1);
-            const T ext = a.with_ext ? SL.el(cur, Sl::kCoef, 2) : T(0);
+            const T stv = cf[0], ssv = cf[1];
+            const T ext = a.with_ext ? cf[2] : T(0);
             T Jc[4] = {T(0), T(0), T(0), T(0)};
             if (a.J) {
 #pragma unroll
-                for (int j = 0; j < 4; ++j) Jc[j] = SL.el(cur, Sl::kJ, j);
+                for (int j = 0; j < 4; ++j) Jc[j] = T(0);
+                SL.template load<4>(cur, Sl::kJ, Jc);
             }
             const T Js = Jc[0] + Jc[1] + Jc[2] + Jc[3];
             T Lm[4][4], r[4];
@@ -596,7 +621,8 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, Sw
                 }
                 r[i] = ssv * c20 * (Jc[i] + Js) + ext;
             }
-            const uint32_t mp = SL.map(cur);
+            uint32_t mp;
+            memcpy(&mp, &cf[3], sizeof(uint32_t));  // the vertex map rides in the fourth coefficient
             const T *ring_s = reinterpret_cast<const T *>(ring);
             int t = 0;
 #pragma unroll
@@ -607,7 +633,8 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, Sw
                     const uint32_t code = t == 0 ? rec.y : t == 1 ? rec.z : rec.w;
                     if (code & (kLagBit | kBndBit)) {
 #pragma unroll
-                        for (int j = 0; j < 4; ++j) up[j] = SL.el(cur, Sl::kBv + t * (4 / Sl::kR), j);
+                        for (int j = 0; j < 4; ++j) up[j] = T(0);
+                        SL.template load<4>(cur, Sl::kBv + t * (4 / Sl::kR), up);
                     } else if (code + R >= e0) {  // upwind trace from the ring
                         const T *src = ring_s + 4 * (size_t)(code % R);
 #pragma unroll
@@ -1273,13 +1300,21 @@ static tr_status sweep_setup(tr_sweep *S, const tr_mesh_view *m, const tr_physic
     cudaError_t e = cudaSuccess;
 #define UP(ptr, vec)                                         \
     if (e == cudaSuccess) e = sw_upload(S, &S->ptr, vec);
+    // per-cell coefficient record: sigma_t V, sigma_s V, sigma_a V B / 4 and the
+    // vertex map in the low 32 bits of the fourth value (copied, never computed on)
     std::vector<double> coef(4ull * nT, 0.0);
+    std::vector<float> coef_f(4ull * nT, 0.0f);
     for (uint32_t c = 0; c < nT; ++c) {
         coef[4ull * c] = stv[c];
         coef[4ull * c + 1] = ssv[c];
         coef[4ull * c + 2] = ext[c];
+        std::memcpy(&coef[4ull * c + 3], &map[c], sizeof(uint32_t));
+        coef_f[4ull * c] = static_cast<float>(stv[c]);
+        coef_f[4ull * c + 1] = static_cast<float>(ssv[c]);
+        coef_f[4ull * c + 2] = static_cast<float>(ext[c]);
+        std::memcpy(&coef_f[4ull * c + 3], &map[c], sizeof(uint32_t));
     }
-    UP(s64, s) UP(stv64, stv) UP(ssv64, ssv) UP(ext64, ext) UP(finc64, finc) UP(coef64, coef) UP(coef32, f32(coef))
+    UP(s64, s) UP(stv64, stv) UP(ssv64, ssv) UP(ext64, ext) UP(finc64, finc) UP(coef64, coef) UP(coef32, coef_f)
     UP(s32, f32(s)) UP(stv32, f32(stv)) UP(ssv32, f32(ssv)) UP(ext32, f32(ext)) UP(finc32, f32(finc))
     UP(nbr, nbr) UP(fbc, fbc) UP(rslot, rslot) UP(map, map) UP(rent, rent) UP(ent_cell, ent_cell) UP(ent_qout, ent_qout) UP(bcell, bcell) UP(bface, bface)
     UP(o64[0], ox) UP(o64[1], oy) UP(o64[2], oz) UP(o64[3], w) UP(o32[0], ox32) UP(o32[1], oy32) UP(o32[2], oz32)

@@ -164,32 +164,3 @@ def adjoint_gradient(device, md, ordinates, physics, face_mask, precision=64, mo
     fwd._c(lib.tr_sweep_gradient(fwd._h, adj._h, int(precision), _ptr(J), _ptr(B), _ptr(Ja), _ptr(dsa), _ptr(dss)))
     return F, dsa[:fwd.nT], dss[:fwd.nT], rep, rep_a
 
-
-def _main():
-    """python -m transfer_b200.sweep [--precision 32|64] [--sweeps N]: N sweeps
-    of the Milne slab (workloads.milne_sweep) with a scattering source, and
-    the mean device time of one sweep."""
-    import argparse
-
-    import torch
-
-    from . import workloads as W
-    ap = argparse.ArgumentParser(description=_main.__doc__)
-    ap.add_argument("--precision", type=int, default=32, choices=(32, 64))
-    ap.add_argument("--sweeps", type=int, default=3)
-    args = ap.parse_args()
-    md, ph, ords, desc = W.milne_sweep()
-    S = Sweep(0, md, ords, ph)
-    J = torch.rand(4 * S.nT, dtype=torch.float64, device="cuda:0")
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(args.sweeps):
-        S.apply(J, None, precision=args.precision)
-    e1.record()
-    torch.cuda.synchronize()
-    print(f"{desc['workload']}: nT {S.nT}, nq {S.nq}, {S.max_levels} levels; FP{args.precision} sweep "
-          f"{e0.elapsed_time(e1) / args.sweeps:.3f} ms (host-timed, includes the API call)")
-
-
-if __name__ == "__main__":
-    _main()
