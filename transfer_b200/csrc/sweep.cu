@@ -63,6 +63,7 @@ constexpr uint32_t kBndIndex = 0x0FFFFFFFu;
 constexpr int kSchedThreads = 1024;
 constexpr int kSweepThreads = 256;
 constexpr int kRedGrid = 296;            // 2 x 148 SMs
+constexpr int kDotGrid = 1184;           // 8 x 148 SMs: the multi-dot is HBM-bound
 constexpr uint32_t kMaxLag = 1u << 22;   // lagged (cycle-breaking) faces over all ordinates
 constexpr int kMaxRestart = 64;
 constexpr int kMaxMoments = 16;
@@ -335,51 +336,43 @@ __device__ __forceinline__ double4 load_v4<double>(const double *p) {
     return make_double4(a.x, a.y, b.x, b.y);
 }
 
-// Per-thread staging of one task's inputs in shared memory.  Everything a
-// task reads that does not depend on this sweep's results -- face normals,
-// coefficients, scalar-flux source, vertex map, and the inflow values of its
-// boundary and lagged faces -- is copied with cp.async one task ahead
-// (task records two tasks ahead, in registers), so that a level costs the
-// arithmetic of its cells, a shared-memory read of the upwind traces and a
-// block barrier instead of a chain of dependent global loads.
-// The two staging slots of each thread are stored field by field in
-// 16-byte units, unit-major across the block's threads, so a warp's reads
-// of one field are contiguous (no bank conflicts).  Per slot: normals s (12
-// reals), source J (4), inflow values bv of up to three non-interior faces
-// (3 x 4), coefficients (sigma_t V, sigma_s V, sigma_a V B / 4, -) and the
-// vertex map.
+// Staging of the tasks' inputs in shared memory.  Everything a task reads
+// that does not depend on this sweep's results -- its record, face normals,
+// coefficients and vertex map, scalar-flux source and the inflow values of
+// its boundary and lagged faces -- is copied into a slot indexed by the
+// task's position.  Positions are processed in chunks of up to 256 (a level,
+// or a part of a long one); while one chunk is computed, the slots of the next
+// are filled with cp.async by threads shifted by half a block -- on the
+// typical level of fewer than 128 cells, threads that compute nothing -- and
+// the copies are waited for before the chunk barrier.  The computing threads
+// thus only do arithmetic, shared-memory reads and the barrier.
+constexpr uint32_t kSlots = 2 * kSweepThreads;  // two chunks of positions in flight
 template <typename T>
 struct Slots {
-    static constexpr int kR = 16 / sizeof(T);          // reals per unit
-    static constexpr int kS = 0, kJ = 12 / kR, kBv = kJ + 4 / kR, kCoef = kBv + 12 / kR;
+    static constexpr int kR = 16 / sizeof(T);          // reals per 16-byte unit
+    static constexpr int kRec = 0, kS = 1, kJ = kS + 12 / kR, kBv = kJ + 4 / kR, kCoef = kBv + 12 / kR;
     static constexpr int kUnits = kCoef + 4 / kR;
     unsigned char *base;
-    __device__ __forceinline__ T *unit(int slot, int u) const {
-        return reinterpret_cast<T *>(base + ((static_cast<size_t>(slot) * kUnits + u) * kSweepThreads + threadIdx.x) * 16);
+    __device__ __forceinline__ unsigned char *unit(uint32_t slot, int u) const {
+        return base + (static_cast<size_t>(u) * kSlots + slot) * 16;
     }
-    __device__ __forceinline__ T &el(int slot, int u0, int e) const { return unit(slot, u0 + e / kR)[e % kR]; }
     // N reals of consecutive units from u0 into registers (16-byte shared loads)
     template <int N>
-    __device__ __forceinline__ void load(int slot, int u0, T (&out)[N]) const {
-        const unsigned char *b = reinterpret_cast<const unsigned char *>(unit(slot, u0));
+    __device__ __forceinline__ void load(uint32_t slot, int u0, T (&out)[N]) const {
 #pragma unroll
         for (int i = 0; i < N / kR; ++i) {
-            const uint4 v = *reinterpret_cast<const uint4 *>(b + static_cast<size_t>(i) * kSweepThreads * 16);
+            const uint4 v = *reinterpret_cast<const uint4 *>(unit(slot, u0 + i));
             memcpy(&out[i * kR], &v, 16);
         }
     }
-    // the vertex map travels in the low 32 bits of the fourth coefficient
-    __device__ __forceinline__ uint32_t map(int slot) const {
-        return *reinterpret_cast<const uint32_t *>(&el(slot, kCoef, 3));
-    }
 };
-template <typename T>
-constexpr int ring_bytes() { return sizeof(T) == 4 ? 64 * 1024 : 40 * 1024; }
 // level pointers of the block's ordinate, staged in shared memory when
 // there are at most kLevelCap levels (else read from global memory)
 constexpr uint32_t kLevelCap = 4096;
 template <typename T>
-constexpr size_t slots_bytes() { return 2ull * Slots<T>::kUnits * kSweepThreads * 16; }
+constexpr int ring_bytes() { return sizeof(T) == 4 ? 64 * 1024 : 32 * 1024; }
+template <typename T>
+constexpr size_t slots_bytes() { return static_cast<size_t>(Slots<T>::kUnits) * kSlots * 16; }
 template <typename T>
 constexpr size_t sweep_smem() { return ring_bytes<T>() + slots_bytes<T>() + 4ull * (kLevelCap + 1); }
 
@@ -395,28 +388,31 @@ __device__ __forceinline__ void cp_async_small(void *dst, const void *src) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N)); }
-// `bytes` (a multiple of 16) from global to shared
-__device__ __forceinline__ void cp_async_bytes(void *dst, const void *src, int bytes) {
-    for (int o = 0; o < bytes; o += 16)
-        cp_async16(static_cast<char *>(dst) + o, static_cast<const char *>(src) + o);
-}
 
+// fills the slot of position p (record, normals, source, coefficients and
+// the inflow values of non-interior faces, zeros where there are none)
 template <typename T>
-__device__ __forceinline__ void stage_task(const Slots<T> &S, int slot, const uint4 rec, const Geom<T> &g,
+__device__ __forceinline__ void stage_task(const Slots<T> &S, uint32_t p, const uint4 *task, const Geom<T> &g,
                                            const SweepArgs<T> &a) {
     using Sl = Slots<T>;
+    const uint32_t sl = p % kSlots;
+    const uint4 rec = __ldg(task + p);
+    *reinterpret_cast<uint4 *>(S.unit(sl, Sl::kRec)) = rec;
     const uint32_t c = rec.x & kCellMask, mask = rec.x >> 28;
-    for (int u = 0; u < 12 / Sl::kR; ++u) cp_async16(S.unit(slot, Sl::kS + u), g.s + 12 * (size_t)c + u * Sl::kR);
-    if (a.J)
-        for (int u = 0; u < 4 / Sl::kR; ++u) cp_async16(S.unit(slot, Sl::kJ + u), a.J + 4 * (size_t)c + u * Sl::kR);
-    for (int u = 0; u < 4 / Sl::kR; ++u) cp_async16(S.unit(slot, Sl::kCoef + u), g.coef + 4 * (size_t)c + u * Sl::kR);
+#pragma unroll
+    for (int u = 0; u < 12 / Sl::kR; ++u) cp_async16(S.unit(sl, Sl::kS + u), g.s + 12 * (size_t)c + u * Sl::kR);
+    if (a.J) {
+#pragma unroll
+        for (int u = 0; u < 4 / Sl::kR; ++u) cp_async16(S.unit(sl, Sl::kJ + u), a.J + 4 * (size_t)c + u * Sl::kR);
+    }
+#pragma unroll
+    for (int u = 0; u < 4 / Sl::kR; ++u) cp_async16(S.unit(sl, Sl::kCoef + u), g.coef + 4 * (size_t)c + u * Sl::kR);
     int t = 0;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
         if (!(mask >> k & 1u) || t >= 3) continue;
         const uint32_t code = t == 0 ? rec.y : t == 1 ? rec.z : rec.w;
         const int u0 = Sl::kBv + t * (4 / Sl::kR);
-        // every non-interior inflow face gets its 4 values staged (zeros where none)
         const T *src = nullptr;
         bool bcast = false;
         if (code & kLagBit) {
@@ -434,32 +430,44 @@ __device__ __forceinline__ void stage_task(const Slots<T> &S, int slot, const ui
             continue;
         }
         if (src && !bcast) {
-            for (int u = 0; u < 4 / Sl::kR; ++u) cp_async16(S.unit(slot, u0 + u), src + u * Sl::kR);
+#pragma unroll
+            for (int u = 0; u < 4 / Sl::kR; ++u) cp_async16(S.unit(sl, u0 + u), src + u * Sl::kR);
         } else if (src) {
 #pragma unroll
-            for (int e = 0; e < 4; ++e) cp_async_small<sizeof(T)>(&S.el(slot, u0, e), src);
+            for (int e = 0; e < 4; ++e)
+                cp_async_small<sizeof(T)>(S.unit(sl, u0 + e / Sl::kR) + (e % Sl::kR) * sizeof(T), src);
         } else {
 #pragma unroll
-            for (int e = 0; e < 4; ++e) S.el(slot, u0, e) = T(0);
+            for (int u = 0; u < 4 / Sl::kR; ++u) *reinterpret_cast<uint4 *>(S.unit(sl, u0 + u)) = make_uint4(0, 0, 0, 0);
         }
         ++t;
     }
 }
 
-// position of this thread's next task after (L, p), looking up to 4 levels
-// ahead (L is advanced to its level); kNone if none.  lvl: the level
-// pointers in shared memory, or in global memory for very many levels
-__device__ __forceinline__ uint32_t next_task(uint32_t &L, uint32_t p, const uint32_t *lvl, uint32_t nl) {
-    if (p == kNone) return kNone;
-    if (p + blockDim.x < lvl[L + 1]) return p + blockDim.x;
-    for (uint32_t d = 1; d <= 4 && L + d < nl; ++d) {
-        const uint32_t s1 = lvl[L + d], e1 = lvl[L + d + 1];
-        if (s1 + threadIdx.x < e1) {
-            L += d;
-            return s1 + threadIdx.x;
-        }
+// the chunk after [c0, ...) of level L: the rest of the level, or the next
+// level; false when none
+__device__ __forceinline__ bool next_chunk(uint32_t &L, uint32_t &c0, const uint32_t *lvl, uint32_t nl) {
+    if (c0 + kSweepThreads < lvl[L + 1]) {
+        c0 += kSweepThreads;
+        return true;
     }
-    return kNone;
+    if (L + 1 < nl) {
+        ++L;
+        c0 = lvl[L];
+        return true;
+    }
+    return false;
+}
+
+// stages the chunk [c0, min(c0 + 256, end of level L)) from threads shifted
+// by half a block
+template <typename T>
+__device__ __forceinline__ void stage_chunk(const Slots<T> &S, uint32_t L, uint32_t c0, const uint32_t *lvl,
+                                            const uint4 *task, const Geom<T> &g, const SweepArgs<T> &a) {
+    const uint32_t e = min(c0 + kSweepThreads, lvl[L + 1]);
+    const uint32_t p = c0 + ((threadIdx.x + kSweepThreads / 2) % kSweepThreads);
+    if (p < e) stage_task<T>(S, p, task, g, a);
+    cp_async_commit();
 }
 
 // upwind trace of one inflow face from its source code
@@ -528,11 +536,11 @@ __device__ __forceinline__ void solve4(const T (&a)[4][4], const T (&r)[4], T (&
 template <typename T>
 __global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, SweepArgs<T> a) {
     using V = typename Vec4<T>::type;
+    using Sl = Slots<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr uint32_t R = ring_bytes<T>() / sizeof(V);
     V *ring = reinterpret_cast<V *>(smem_raw);
     const Slots<T> SL{smem_raw + ring_bytes<T>()};
-    using Sl = Slots<T>;
     const uint32_t q = blockIdx.x, nT = a.nT;
     const T ox = a.ox[q], oy = a.oy[q], oz = a.oz[q];
     const uint4 *task = sc.task + (size_t)q * nT;
@@ -544,57 +552,27 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, Sw
         __syncthreads();
         lvl = lv;
     }
+    if (nl == 0) return;
     T *psi = a.psi + (size_t)q * nT * 4;
     const T c12 = T(1) / T(12), c20 = T(1) / T(20);
 
-    // pipeline: the staged task (position pst, slot `cur`, record r_cur) and
-    // the position / record of the task after it (p1 at level L1, r1)
-    uint32_t pst = kNone, L1 = 0;
-    for (uint32_t d = 0; d < 5 && d < nl; ++d)
-        if (lvl[d] + threadIdx.x < lvl[d + 1]) {
-            pst = lvl[d] + threadIdx.x;
-            L1 = d;
-            break;
-        }
-    int cur = 0;
-    uint4 r_cur = make_uint4(0, 0, 0, 0), r1 = make_uint4(0, 0, 0, 0);
-    uint32_t p1 = kNone;
-    if (pst != kNone) {
-        r_cur = __ldg(task + pst);
-        stage_task<T>(SL, cur, r_cur, g, a);
-        p1 = next_task(L1, pst, lvl, nl);
-        if (p1 != kNone) r1 = __ldg(task + p1);
-    }
-    cp_async_commit();
-
-    for (uint32_t L = 0; L < nl; ++L) {
-        const uint32_t s0 = lvl[L], e0 = lvl[L + 1];
-        for (uint32_t p = s0 + threadIdx.x; p < e0; p += blockDim.x) {
-            if (p != pst) {  // not staged ahead: fetch now
-                cp_async_wait<0>();
-                r_cur = __ldg(task + p);
-                stage_task<T>(SL, cur, r_cur, g, a);
-                cp_async_commit();
-                pst = p;
-                L1 = L;
-                p1 = next_task(L1, p, lvl, nl);
-                if (p1 != kNone) r1 = __ldg(task + p1);
-            }
-            // stage the next task, load the record after it
-            uint32_t L2 = L1, p2 = kNone;
-            uint4 r2 = make_uint4(0, 0, 0, 0);
-            if (p1 != kNone) {
-                stage_task<T>(SL, cur ^ 1, r1, g, a);
-                p2 = next_task(L2, p1, lvl, nl);
-                if (p2 != kNone) r2 = __ldg(task + p2);
-            }
-            cp_async_commit();
-            cp_async_wait<1>();  // this task's group has landed
-            const uint4 rec = r_cur;
+    uint32_t L = 0, c0 = lvl[0];
+    stage_chunk<T>(SL, L, c0, lvl, task, g, a);
+    cp_async_wait<0>();
+    __syncthreads();
+    for (;;) {
+        const uint32_t e0 = min(c0 + kSweepThreads, lvl[L + 1]);  // this chunk is [c0, e0)
+        uint32_t nL = L, nc0 = c0;
+        const bool more = next_chunk(nL, nc0, lvl, nl);
+        if (more) stage_chunk<T>(SL, nL, nc0, lvl, task, g, a);
+        const uint32_t p = c0 + threadIdx.x;
+        if (p < e0) {
+            const uint32_t sl = p % kSlots;
+            const uint4 rec = *reinterpret_cast<const uint4 *>(SL.unit(sl, Sl::kRec));
             const uint32_t c = rec.x & kCellMask, mask = rec.x >> 28;
             T sv[12], cf[4];
-            SL.template load<12>(cur, Sl::kS, sv);
-            SL.template load<4>(cur, Sl::kCoef, cf);
+            SL.template load<12>(sl, Sl::kS, sv);
+            SL.template load<4>(sl, Sl::kCoef, cf);
             T av[4], al[4], Ain = T(0);
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
@@ -605,11 +583,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, Sw
             const T stv = cf[0], ssv = cf[1];
             const T ext = a.with_ext ? cf[2] : T(0);
             T Jc[4] = {T(0), T(0), T(0), T(0)};
-            if (a.J) {
-#pragma unroll
-                for (int j = 0; j < 4; ++j) Jc[j] = T(0);
-                SL.template load<4>(cur, Sl::kJ, Jc);
-            }
+            if (a.J) SL.template load<4>(sl, Sl::kJ, Jc);
             const T Js = Jc[0] + Jc[1] + Jc[2] + Jc[3];
             T Lm[4][4], r[4];
 #pragma unroll
@@ -632,9 +606,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, Sw
                 if (t < 3) {
                     const uint32_t code = t == 0 ? rec.y : t == 1 ? rec.z : rec.w;
                     if (code & (kLagBit | kBndBit)) {
-#pragma unroll
-                        for (int j = 0; j < 4; ++j) up[j] = T(0);
-                        SL.template load<4>(cur, Sl::kBv + t * (4 / Sl::kR), up);
+                        SL.template load<4>(sl, Sl::kBv + t * (4 / Sl::kR), up);
                     } else if (code + R >= e0) {  // upwind trace from the ring
                         const T *src = ring_s + 4 * (size_t)(code % R);
 #pragma unroll
@@ -679,17 +651,13 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, Sw
                 dst[1] = make_double2(o[2], o[3]);
             }
             ring[p % R] = out;
-            // advance the pipeline
-            cur ^= 1;
-            pst = p1;
-            r_cur = r1;
-            p1 = p2;
-            L1 = L2;
-            r1 = r2;
         }
+        cp_async_wait<0>();
         __syncthreads();
+        if (!more) break;
+        L = nL;
+        c0 = nc0;
     }
-    cp_async_wait<0>();
 }
 
 // B_out of the reflective faces: the inflow of each (face, incoming q)
@@ -1454,7 +1422,7 @@ static tr_status sweep_setup(tr_sweep *S, const tr_mesh_view *m, const tr_physic
     if (e != cudaSuccess) return sw_cuda(S, e, "sweep: schedule");
     S->nB = 4ull * S->nent + 4ull * nlag;
     // reductions
-    if (e == cudaSuccess) e = sw_alloc(S, &S->partials, (kMaxRestart + 2ull) * kRedGrid);
+    if (e == cudaSuccess) e = sw_alloc(S, &S->partials, (kMaxRestart + 2ull) * kDotGrid);
     if (e == cudaSuccess) e = sw_alloc(S, &S->red, 256);
     if (e == cudaSuccess) e = sw_alloc(S, &S->counter, 4);
     if (e == cudaSuccess) e = cudaMemset(S->counter, 0, 16);
@@ -1611,7 +1579,7 @@ static cudaError_t op_apply(tr_sweep *S, int prec, const double *x, double *y) {
 static cudaError_t dots(tr_sweep *S, int k, const double *V, uint64_t ld, const double *w, double *dev_out,
                         double *host_out) {
     const uint64_t n = S->nJ + S->nB;
-    k_multidot<<<kRedGrid, 256, 0, S->stream>>>(n, k, V, ld, w, S->partials, S->counter, dev_out);
+    k_multidot<<<kDotGrid, 256, 0, S->stream>>>(n, k, V, ld, w, S->partials, S->counter, dev_out);
     ++S->launches;
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess || !host_out) return e;
