@@ -31,11 +31,14 @@
 //   upstream cell's position p' in this ordinate's order, kLagBit | slot,
 //   or kNone for a boundary face.
 //
-// Sweep (k_sweep, one block per ordinate): levels in order, a block
-// barrier between levels; each cell's solution goes to psi and to a
-// shared-memory ring indexed by position, from which downstream cells of
-// the next levels read their upwind traces (global psi for older ones).
-// Blocks never wait on one another, so a sweep has no inter-block waits.
+// Sweep (k_sweep, one block per ordinate): positions in chunks (a level, or
+// 256 cells of a longer one), a block barrier between chunks; each cell's
+// solution goes to psi and to a shared-memory ring indexed by position, from
+// which downstream cells of later levels read their upwind traces (global
+// psi for older ones).  The inputs of the next chunk are staged in shared
+// memory by the threads shifted by half a block while the current chunk is
+// computed.  Blocks never wait on one another, so a sweep has no
+// inter-block waits.
 #include <cuda_runtime.h>
 
 #include <algorithm>
