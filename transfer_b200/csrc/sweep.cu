@@ -29,7 +29,8 @@
 //   task[q][p] = { cell | inflow_mask << 28, up[3] } in level order, up[i]
 //   the source of the i-th inflow face (ascending local face index): the
 //   upstream cell's position p' in this ordinate's order, kLagBit | slot,
-//   or kNone for a boundary face.
+//   or for a boundary face kBndBit | kind << 28 | the index of its inflow
+//   value (the reflective B entry, or the face for incident inflow).
 //
 // Sweep (k_sweep, one block per ordinate): positions in chunks (a level, or
 // 256 cells of a longer one), a block barrier between chunks; each cell's
