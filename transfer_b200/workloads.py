@@ -108,3 +108,28 @@ def sweep_work(nT, nq, real_bytes=4):
     the scalar-flux source (4 reals) are read once; about 220 flops per
     (cell, ordinate) for the 4x4 system and its solve."""
     return nq * nT * (16 + 4 * real_bytes) + nT * 20 * real_bytes, 220 * nq * nT
+
+
+
+def algorithmic_work(md, ad, real_bytes=8):
+    """Per operator application: bytes and flops as counted for the roofline:
+    read f and write A f (2 * real_bytes per vertex and harmonic), 4 vertex
+    indices + kappa per tet (24 B), 3 coordinates per vertex (24 B), 3
+    indices per boundary face (12 B); 108 flops per tet and harmonic, the
+    angular contraction 2 nnz(omega) per vertex and the boundary term
+    6 slm^2 per boundary face."""
+    slm = ad.slm
+    nnz = int((np.abs(ad.omega) > 1e-14 * np.abs(ad.omega).max()).sum())
+    byt = 2 * real_bytes * md.nP * slm + 24 * md.nT + 24 * md.nP + 12 * md.nF
+    flops = 108 * md.nT * slm + 2 * nnz * md.nP + 6 * md.nF * slm * slm
+    return byt, flops
+
+
+def cg_iteration_work(md, ad, real_bytes=8):
+    """Per CG iteration: the operator application (algorithmic_work) plus the
+    vector traffic of the iteration (main.cpp:139-158): x += alpha p (3 vector
+    passes), r -= alpha Ap (3), p = z + beta p (3) and Ap read once more for
+    <p, Ap> (1), ten passes of real_bytes * nP * slm; 2 flops per entry and
+    pass-pair (10 nP slm)."""
+    byt, flops = algorithmic_work(md, ad, real_bytes)
+    return byt + 10 * real_bytes * md.nP * ad.slm, flops + 10 * md.nP * ad.slm
