@@ -505,6 +505,31 @@ const double  *tr_meshdata_kappa_abs_volume(const tr_meshdata *md);
 const int32_t *tr_meshdata_face_side(const tr_meshdata *md);
 void tr_meshdata_destroy(tr_meshdata *md);
 
+/* Mesh I/O in place of the reference's meshProcessor library (MeshData.cpp:10
+ * reads the meshfile of radiation.cfg, main.cpp:209-216 saves the solution
+ * with saveVtk).  tr_meshdata_read_vol reads a Netgen ".vol" mesh: points,
+ * volumeelements (region = matnr; the first four vertices of each element)
+ * and surfaceelements / surfaceelementsgi, whose bcnr is kept per boundary
+ * face (tr_meshdata_face_bcnr, -1 where a face has no surface element; NULL
+ * for meshes not read from .vol). */
+tr_status tr_meshdata_read_vol(const char *path, const tr_region_params *rp, tr_meshdata **out);
+const int32_t *tr_meshdata_face_bcnr(const tr_meshdata *md);
+/* Legacy VTK unstructured grid (binary, big-endian reals of real_bytes 4 or
+ * 8) with the mesh and the given fields, as saveVtk writes "W%v" cell vectors
+ * and "U%sT%t..." point scalars / symmetric tensors.  Field data are
+ * component-major: data[c * n + i] for component c of point / cell i; a
+ * TR_VTK_TENSOR gives the 6 components xx xy xz yy yz zz. */
+enum { TR_VTK_POINT = 0, TR_VTK_CELL = 1 };
+enum { TR_VTK_SCALAR = 0, TR_VTK_VECTOR = 1, TR_VTK_TENSOR = 2 };
+typedef struct tr_vtk_field {
+    const char *name;
+    int32_t location;          /* TR_VTK_POINT or TR_VTK_CELL */
+    int32_t kind;              /* TR_VTK_SCALAR (1), VECTOR (3), TENSOR (6)  */
+    const double *data;        /* host, component-major                     */
+} tr_vtk_field;
+tr_status tr_vtk_write(const char *path, const tr_meshdata *md, int real_bytes, int nfields,
+                       const tr_vtk_field *fields);
+
 #ifdef __cplusplus
 }
 #endif

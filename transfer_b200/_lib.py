@@ -33,6 +33,8 @@ TR_MODE_FP64, TR_MODE_MIXED = 0, 1
 TR_ENGINE_PERSISTENT, TR_ENGINE_GRAPH, TR_ENGINE_LAUNCH, TR_ENGINE_PERSISTENT_SR = 0, 1, 2, 3
 TR_OPERATOR_SIMT, TR_OPERATOR_TENSOR = 0, 1
 TR_SWEEP_GMRES, TR_SWEEP_SOURCE_ITERATION = 0, 1
+TR_VTK_POINT, TR_VTK_CELL = 0, 1
+TR_VTK_SCALAR, TR_VTK_VECTOR, TR_VTK_TENSOR = 0, 1, 2
 
 
 class tr_tetrahedron(C.Structure):
@@ -109,6 +111,10 @@ class tr_sweep_opts(C.Structure):
                 ("restart", C.c_int32), ("inner_tol", C.c_double), ("max_outer", C.c_int32)]
 
 
+class tr_vtk_field(C.Structure):
+    _fields_ = [("name", C.c_char_p), ("location", C.c_int32), ("kind", C.c_int32), ("data", C.c_void_p)]
+
+
 class tr_sweep_report(C.Structure):
     _fields_ = [("converged", C.c_int32), ("iterations", C.c_int32), ("outer_steps", C.c_int32),
                 ("sweeps_f32", C.c_int64), ("sweeps_f64", C.c_int64), ("residual", C.c_double),
@@ -176,6 +182,9 @@ PROTOTYPES = [
     ("tr_meshdata_kappa_abs_volume", P, [P]),
     ("tr_meshdata_face_side", P, [P]),
     ("tr_meshdata_destroy", None, [P]),
+    ("tr_meshdata_read_vol", S, [C.c_char_p, C.POINTER(tr_region_params), C.POINTER(P)]),
+    ("tr_meshdata_face_bcnr", P, [P]),
+    ("tr_vtk_write", S, [C.c_char_p, P, I, I, P]),
     ("tr_ordinates_product", S, [I, I, P, P, P, P]),
     ("tr_sweep_create", S, [I, C.POINTER(tr_mesh_view), C.POINTER(tr_physics_view), C.POINTER(tr_ordinates_view),
                             C.POINTER(P)]),

@@ -201,6 +201,36 @@ class MeshData:
         return cls._from_handle(h)
 
     @classmethod
+    def read_vol(cls, path, kappa, Ip, albedo=None):
+        """Netgen .vol mesh (the reference's meshfile format); region of a
+        tetrahedron = its matnr; face_bcnr = the bc number of each boundary
+        face's surface element (-1 if none)."""
+        rp, keep = cls._rp(kappa, Ip, albedo)
+        h = C.c_void_p()
+        check(lib.tr_meshdata_read_vol(str(path).encode(), C.byref(rp), C.byref(h)))
+        md = cls._from_handle(h)
+        fb = lib.tr_meshdata_face_bcnr(h)
+        md.face_bcnr = _carr(fb, np.int32, md.nF) if fb else None
+        return md
+
+    def write_vtk(self, path, point_fields=None, cell_fields=None, real_bytes=8):
+        """Legacy VTK of the mesh with fields, as the reference's saveVtk
+        (main.cpp:209-216): each field is an array [n] (scalar), [3, n]
+        (vector) or [6, n] (symmetric tensor xx xy xz yy yz zz)."""
+        if not getattr(self, "_h", None):
+            raise ValueError("write_vtk needs a MeshData built by this library (kuhn, from_tets, read_vol)")
+        fields, keep = [], []
+        for loc, group in ((L.TR_VTK_POINT, point_fields or {}), (L.TR_VTK_CELL, cell_fields or {})):
+            for name, arr in group.items():
+                a = np.ascontiguousarray(arr, dtype=np.float64)
+                ncomp = 1 if a.ndim == 1 else a.shape[0]
+                kind = {1: L.TR_VTK_SCALAR, 3: L.TR_VTK_VECTOR, 6: L.TR_VTK_TENSOR}[ncomp]
+                keep.append(a)
+                fields.append(L.tr_vtk_field(name.encode(), loc, kind, a.ctypes.data))
+        arr_t = (L.tr_vtk_field * max(len(fields), 1))(*fields)
+        check(lib.tr_vtk_write(str(path).encode(), self._h, int(real_bytes), len(fields), arr_t))
+
+    @classmethod
     def _from_handle(cls, h):
         md = cls()
         md._h = h

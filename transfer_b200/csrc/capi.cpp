@@ -660,4 +660,36 @@ const int32_t *tr_meshdata_face_side(const tr_meshdata *md) {
 }
 void tr_meshdata_destroy(tr_meshdata *md) { delete md; }
 
+tr_status tr_meshdata_read_vol(const char *path, const tr_region_params *rp, tr_meshdata **out) {
+    if (!path || !rp || !rp->kappa || !rp->Ip || !out || rp->nreg < 1)
+        return set_err(nullptr, TR_ERR_INVALID_ARG, "null or empty argument");
+    try {
+        tr_meshdata *m = new tr_meshdata();
+        try {
+            m->md = MeshData::read_vol(path, region_params(rp));
+        } catch (...) {
+            delete m;
+            throw;
+        }
+        *out = m;
+    } catch (const std::exception &e) {
+        return set_err(nullptr, TR_ERR_IO, e.what());
+    }
+    return TR_OK;
+}
+const int32_t *tr_meshdata_face_bcnr(const tr_meshdata *md) {
+    return (md && !md->md.face_bcnr.empty()) ? md->md.face_bcnr.data() : nullptr;
+}
+tr_status tr_vtk_write(const char *path, const tr_meshdata *md, int real_bytes, int nfields,
+                       const tr_vtk_field *fields) {
+    if (!path || !md || nfields < 0 || (nfields > 0 && !fields))
+        return set_err(nullptr, TR_ERR_INVALID_ARG, "null argument");
+    try {
+        write_vtk(path, md->md, real_bytes, nfields, fields);
+    } catch (const std::exception &e) {
+        return set_err(nullptr, TR_ERR_IO, e.what());
+    }
+    return TR_OK;
+}
+
 }  // extern "C"

@@ -313,6 +313,8 @@ MeshData::MeshData(const Config &cfg) {
         std::istringstream ra(cfg.get_string("region_arg", "0 0 0 0"));
         ra >> kp.region_arg[0] >> kp.region_arg[1] >> kp.region_arg[2] >> kp.region_arg[3];
         *this = kuhn(kp, rp);
+    } else if (fn.size() > 4 && fn.compare(fn.size() - 4, 4, ".vol") == 0) {
+        *this = read_vol(fn, rp);
     } else {
         *this = read_tmesh(fn, rp);
     }

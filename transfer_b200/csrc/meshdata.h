@@ -51,13 +51,14 @@ struct MeshData {
     std::vector<int32_t> region;            // [nT]
     std::vector<double> kappa_abs_volume;   // [nT] or empty (no scattering)
     std::vector<int32_t> face_side;         // [nF] box side 0..5 or -1
+    std::vector<int32_t> face_bcnr;         // [nF] bc number of a .vol surface element, -1 if none
 
     MeshData() {}
-    // MeshData(const Config &) (MeshData.cpp:9): meshfile is either a
-    // plain-text mesh ("*.tmesh") or a Kuhn box spec
-    // "kuhn:nx,ny,nz:x0,x1,y0,y1,z0,z1:jitter:seed"; regions of a Kuhn box
-    // come from the additive keys region_kind (uniform|sphere|halfspace) and
-    // region_arg (4 numbers).
+    // MeshData(const Config &) (MeshData.cpp:9): meshfile is a Netgen mesh
+    // ("*.vol", the reference's format), a plain-text mesh ("*.tmesh") or a
+    // Kuhn box spec "kuhn:nx,ny,nz:x0,x1,y0,y1,z0,z1:jitter:seed"; regions of
+    // a Kuhn box come from the additive keys region_kind
+    // (uniform|sphere|halfspace) and region_arg (4 numbers).
     explicit MeshData(const Config &cfg);
 
     static MeshData from_tets(tr_idx nP, const double *xyz, tr_idx nT, const tr_idx *tets,
@@ -65,6 +66,7 @@ struct MeshData {
                               const int32_t *vertex_side_mask = nullptr);
     static MeshData kuhn(const KuhnParams &kp, const RegionParams &rp);
     static MeshData read_tmesh(const std::string &path, const RegionParams &rp);
+    static MeshData read_vol(const std::string &path, const RegionParams &rp);  // meshio.cpp
 
     tr_mesh_view view() const;
 };
@@ -81,5 +83,8 @@ struct SplitMix64 {
     }
     double uniform() { return static_cast<double>(next() >> 11) * (1.0 / 9007199254740992.0); }
 };
+
+// legacy VTK writer (meshio.cpp)
+void write_vtk(const std::string &path, const MeshData &md, int real_bytes, int nfields, const tr_vtk_field *fields);
 
 }  // namespace transfer
