@@ -208,13 +208,14 @@ def sweep_section(local, flush, peak, want_cpu):
     """The discrete-ordinates sweep on the Milne slab (workloads.milne_sweep):
     one sweep of all ordinates timed alone (FP32 and FP64), and solves of the
     scattering problem to the FP64 relative residual TOL, FP64 GMRES against
-    FP32 sweeps in FP64 defect correction; the FP64 energy balance of the
+    FP32 sweeps in FP64 defect correction, each also as flexible GMRES with
+    the diffusion synthetic acceleration; the FP64 energy balance of the
     mixed solution and its difference from the FP64 one."""
     import torch
     import transfer_b200 as tr
     from transfer_b200 import workloads as W
     md, ph, ords, desc = W.milne_sweep()
-    S = tr.Sweep(local, md, ords, ph)
+    S = tr.Sweep(local, md, ords, ph, dsa=True)
     nT, nq = S.nT, S.nq
     ms = {p: S.bench(p, 20) for p in (32, 64)}
     out = {"config": {**desc, "nT": nT, "nq": nq, "max_levels": S.max_levels, "n_extra": S.n_extra,
@@ -228,13 +229,16 @@ def sweep_section(local, flush, peak, want_cpu):
                                "gflops": flops / (ms[p] * 1e-3) / 1e9,
                                "us_per_level": 1e3 * ms[p] / S.max_levels}
     sols = {}
-    for name, mode in (("fp64", tr.TR_MODE_FP64), ("mixed", tr.TR_MODE_MIXED)):
-        S.solve(mode=mode, tol=TOL, restart=40, max_iter=5000)   # warm-up
+    DSA = tr._lib.TR_SWEEP_PREC_DSA
+    for name, mode, prec in (("fp64", tr.TR_MODE_FP64, 0), ("mixed", tr.TR_MODE_MIXED, 0),
+                             ("fp64_dsa", tr.TR_MODE_FP64, DSA), ("mixed_dsa", tr.TR_MODE_MIXED, DSA)):
+        kw = dict(mode=mode, tol=TOL, restart=40, max_iter=5000, precondition=prec, precond_tol=1e-2)
+        S.solve(**kw)   # warm-up
         flush.fill_(1.0)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
-        J, B, rep = S.solve(mode=mode, tol=TOL, restart=40, max_iter=5000)
+        J, B, rep = S.solve(**kw)
         e1.record()
         torch.cuda.synchronize()
         t = e0.elapsed_time(e1)
@@ -244,7 +248,14 @@ def sweep_section(local, flush, peak, want_cpu):
                                 "outer_steps": rep.outer_steps, "sweeps_f32": rep.sweeps_f32,
                                 "sweeps_f64": rep.sweeps_f64, "residual": rep.residual,
                                 "value": sweeps * nT * nq / (t * 1e-3)}
+        if prec:
+            out[f"solve_{name}"].update(diffusion_solves=rep.precond_solves,
+                                        diffusion_cg_iterations=rep.precond_iterations, precond_tol=1e-2)
     out["speedup_mixed_vs_fp64"] = out["solve_fp64"]["ms"] / out["solve_mixed"]["ms"]
+    out["speedup_dsa_vs_fp64"] = out["solve_fp64"]["ms"] / min(out["solve_fp64_dsa"]["ms"],
+                                                               out["solve_mixed_dsa"]["ms"])
+    out["dsa_vs_fp64_J"] = float(((sols["fp64_dsa"][0] - sols["fp64"][0]).abs().max()
+                                  / sols["fp64"][0].abs().max()).item())
     J, B = sols["mixed"]
     Jo, _ = S.apply(J, B, precision=64)
     b = S.balance(J, B, Jo)

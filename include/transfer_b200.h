@@ -348,6 +348,14 @@ typedef struct tr_sweep_info {
     int device;
 } tr_sweep_info;
 enum { TR_SWEEP_GMRES = 0, TR_SWEEP_SOURCE_ITERATION = 1 };
+/* Diffusion synthetic acceleration (TR_SWEEP_PREC_DSA, after
+ * tr_sweep_enable_dsa): GMRES becomes flexible GMRES right-preconditioned by
+ * P^-1 y = y + C sigma_s y, and source iteration adds C sigma_s (S(x) - x)
+ * to each iterate, where C solves the P1 diffusion problem -div(1 / (3
+ * sigma_t)) grad f + sigma_a f = g with Marshak faces (vacuum and incident)
+ * and zero current (reflective) -- the even-parity operator with l = 0 only,
+ * continuous linear elements on the vertices, by FP64 Jacobi CG. */
+enum { TR_SWEEP_PREC_NONE = 0, TR_SWEEP_PREC_DSA = 1 };
 typedef struct tr_sweep_opts {
     int32_t method;            /* TR_SWEEP_*                                */
     int32_t mode;              /* TR_MODE_FP64, or TR_MODE_MIXED: FP32
@@ -362,6 +370,9 @@ typedef struct tr_sweep_opts {
                                   its residual by this factor, then restart
                                   from the true residual (0: never)        */
     int32_t max_outer;         /* unused; kept for layout                   */
+    int32_t precondition;      /* TR_SWEEP_PREC_*                           */
+    double  precond_tol;       /* DSA: relative tolerance of each diffusion
+                                  solve (FP64 Jacobi CG), in (0, 1)        */
 } tr_sweep_opts;
 typedef struct tr_sweep_report {
     int32_t converged;
@@ -372,7 +383,10 @@ typedef struct tr_sweep_report {
     double  residual;          /* final relative residual, FP64            */
     double  rhs_norm;
     double  device_ms;
-    int64_t kernel_launches;
+    int64_t kernel_launches;   /* sweep kernels; the diffusion solves' own
+                                  launches are not counted here            */
+    int32_t precond_solves;    /* diffusion solves (DSA)                   */
+    int32_t precond_iterations;/* their CG iterations summed               */
 } tr_sweep_report;
 
 /* Gauss-Legendre (n_polar in cos theta) x uniform azimuth (n_azim, at
@@ -412,6 +426,11 @@ void tr_sweep_opts_default(tr_sweep_opts *opts);
  * (I - T) x = S(0) or by source iteration; J [nT][4], B [n_extra] device
  * outputs (B may be NULL). */
 tr_status tr_sweep_solve(tr_sweep *s, const tr_sweep_opts *opts, double *J, double *B, tr_sweep_report *rep);
+/* Prepares the diffusion operator for TR_SWEEP_PREC_DSA from the mesh and
+ * physics the sweep was created with (the vertex -> cell and vertex -> face
+ * tables of the mesh view are used): an even-parity context with l = 0 on
+ * the same device, with the reflective faces left out of its face list. */
+tr_status tr_sweep_enable_dsa(tr_sweep *s, const tr_mesh_view *mesh, const tr_physics_view *phys);
 /* Outflow of the last sweep through the boundary faces with face_mask[f]
  * != 0 (HOST array [nF]): F = sum_q w_q sum_f max(Omega_q.s_f, 0) mean_f psi_q
  * (mean intensity x area), FP64. */

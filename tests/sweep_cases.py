@@ -36,6 +36,17 @@ def scattering_box(n=(5, 4, 6), jitter=0.2, albedo=0.6, incident=0.7):
     return md, tr.Physics(kappa_abs_volume=md.kappa_abs_volume, face_bc=bc, face_incident=inc)
 
 
+def diffusive_box(n=(6, 6, 6), sigma_t=10.0, albedo=0.995):
+    """Optically thick, nearly conservative unit cube (cells about sigma_t / n
+    mean free paths across), B = 1, reflective y faces and vacuum elsewhere:
+    the regime where unaccelerated iterations stall and the diffusion
+    correction pays."""
+    md = tr.MeshData.kuhn(n, jitter=0.2, seed=SEED, kappa=[0.0, sigma_t, sigma_t], Ip=[0.0, 1.0, 1.0],
+                          albedo=[0.0, albedo, albedo], region_kind=1, region_arg=(0.5, 0.5, 0.5, 0.3))
+    bc = np.where((md.face_side == 2) | (md.face_side == 3), tr.TR_BC_REFLECTIVE, tr.TR_BC_VACUUM).astype(np.int32)
+    return md, tr.Physics(kappa_abs_volume=md.kappa_abs_volume, face_bc=bc, face_incident=np.zeros(md.nF))
+
+
 def tangled_cube():
     """6^3 Kuhn cube jittered by +-0.36h: some tetrahedra overlap, and the
     upwind graphs of many ordinates have cycles.  Not a physical mesh (no

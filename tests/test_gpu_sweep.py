@@ -14,7 +14,7 @@ import torch
 import oracle_py as op
 import transfer_b200 as tr
 from common import rel_err
-from sweep_cases import absorbing_slab, e2_slab_exact, scattering_box, tangled_cube, vertex_x
+from sweep_cases import absorbing_slab, diffusive_box, e2_slab_exact, scattering_box, tangled_cube, vertex_x
 
 pytestmark = pytest.mark.gpu
 
@@ -130,6 +130,52 @@ def test_mixed_precision_solve(cuda):
     Jout, _ = S.apply(J, B)
     b = S.balance(J, B, Jout)
     assert abs(b["emitted"] + b["incoming"] - b["absorbed"] - b["escaped"]) < 1e-8 * b["emitted"]
+
+
+def test_dsa_gmres_matches_oracle(cuda):
+    """Flexible GMRES with the diffusion correction reaches the oracle's
+    fixed point in fewer Krylov steps, one diffusion solve per step."""
+    md, ph = diffusive_box()
+    ords = op.ordinates_product(4, 8)
+    S = tr.Sweep(0, md, ords, ph, dsa=True)
+    O = op.SweepOracle(md, ords, kappa_abs_volume=ph.kappa_abs_volume, face_bc=ph.face_bc,
+                       face_incident=ph.face_incident)
+    Jo, Bo, info = O.solve(method=1, tol=1e-11)
+    J0, B0, r0 = S.solve(tol=1e-10, max_iter=2000)
+    J1, B1, r1 = S.solve(tol=1e-10, precondition=tr._lib.TR_SWEEP_PREC_DSA)
+    assert info["converged"] and r0.converged and r1.converged
+    assert r1.residual <= 1e-10 and r1.precond_solves == r1.iterations and r1.precond_iterations > 0
+    assert r1.iterations < r0.iterations / 2, (r1.iterations, r0.iterations)
+    assert rel_err(host(J1), Jo) < 1e-8 and rel_err(host(B1), Bo) < 1e-8
+    assert r0.precond_solves == 0
+
+
+def test_dsa_mixed_and_source_iteration(cuda):
+    md, ph = diffusive_box(n=(4, 4, 4))
+    ords = op.ordinates_product(4, 8)
+    S = tr.Sweep(0, md, ords, ph, dsa=True)
+    Jg, _, rg = S.solve(tol=1e-11)
+    Jm, _, rm = S.solve(mode=tr.TR_MODE_MIXED, tol=1e-9, precondition=tr._lib.TR_SWEEP_PREC_DSA)
+    assert rm.converged and rm.residual <= 1e-9 and rm.sweeps_f32 > rm.sweeps_f64
+    assert rel_err(host(Jm), host(Jg)) < 1e-7
+    SI = tr._lib.TR_SWEEP_SOURCE_ITERATION
+    _, _, rs0 = S.solve(method=SI, tol=1e-9, max_iter=100, raise_on_error=False)
+    Js, _, rs = S.solve(method=SI, tol=1e-9, max_iter=400, precondition=tr._lib.TR_SWEEP_PREC_DSA,
+                        precond_tol=1e-6)
+    assert rs.converged and not rs0.converged and rs.iterations < 100
+    assert rel_err(host(Js), host(Jg)) < 1e-6
+
+
+def test_dsa_needs_enable(cuda):
+    md, ph = diffusive_box(n=(2, 2, 2))
+    S = tr.Sweep(0, md, tr.ordinates_product(2, 4), ph)
+    with pytest.raises(tr.TransferError):
+        S.solve(precondition=tr._lib.TR_SWEEP_PREC_DSA)
+    S2 = tr.Sweep(0, md, tr.ordinates_product(2, 4), ph, dsa=True)
+    with pytest.raises(tr.TransferError):
+        S2.solve(precondition=tr._lib.TR_SWEEP_PREC_DSA, precond_tol=0.0)
+    with pytest.raises(tr.TransferError):
+        S2.solve(precondition=7)
 
 
 def test_absorbing_slab_matches_e2_on_gpu(cuda):

@@ -33,6 +33,7 @@ TR_MODE_FP64, TR_MODE_MIXED = 0, 1
 TR_ENGINE_PERSISTENT, TR_ENGINE_GRAPH, TR_ENGINE_LAUNCH, TR_ENGINE_PERSISTENT_SR = 0, 1, 2, 3
 TR_OPERATOR_SIMT, TR_OPERATOR_TENSOR = 0, 1
 TR_SWEEP_GMRES, TR_SWEEP_SOURCE_ITERATION = 0, 1
+TR_SWEEP_PREC_NONE, TR_SWEEP_PREC_DSA = 0, 1
 TR_VTK_POINT, TR_VTK_CELL = 0, 1
 TR_VTK_SCALAR, TR_VTK_VECTOR, TR_VTK_TENSOR = 0, 1, 2
 
@@ -108,7 +109,8 @@ class tr_sweep_info(C.Structure):
 
 class tr_sweep_opts(C.Structure):
     _fields_ = [("method", C.c_int32), ("mode", C.c_int32), ("tol", C.c_double), ("max_iter", C.c_int32),
-                ("restart", C.c_int32), ("inner_tol", C.c_double), ("max_outer", C.c_int32)]
+                ("restart", C.c_int32), ("inner_tol", C.c_double), ("max_outer", C.c_int32),
+                ("precondition", C.c_int32), ("precond_tol", C.c_double)]
 
 
 class tr_vtk_field(C.Structure):
@@ -118,7 +120,8 @@ class tr_vtk_field(C.Structure):
 class tr_sweep_report(C.Structure):
     _fields_ = [("converged", C.c_int32), ("iterations", C.c_int32), ("outer_steps", C.c_int32),
                 ("sweeps_f32", C.c_int64), ("sweeps_f64", C.c_int64), ("residual", C.c_double),
-                ("rhs_norm", C.c_double), ("device_ms", C.c_double), ("kernel_launches", C.c_int64)]
+                ("rhs_norm", C.c_double), ("device_ms", C.c_double), ("kernel_launches", C.c_int64),
+                ("precond_solves", C.c_int32), ("precond_iterations", C.c_int32)]
 
 
 P = C.c_void_p
@@ -198,6 +201,7 @@ PROTOTYPES = [
     ("tr_sweep_balance", S, [P, P, P, P, P]),
     ("tr_sweep_opts_default", None, [C.POINTER(tr_sweep_opts)]),
     ("tr_sweep_solve", S, [P, C.POINTER(tr_sweep_opts), P, P, C.POINTER(tr_sweep_report)]),
+    ("tr_sweep_enable_dsa", S, [P, C.POINTER(tr_mesh_view), C.POINTER(tr_physics_view)]),
     ("tr_sweep_outflow", S, [P, P, C.POINTER(D)]),
     ("tr_sweep_gradient", S, [P, P, I, P, P, P, P, P]),
     ("tr_sweep_bench", S, [P, I, I, C.POINTER(D)]),

@@ -875,6 +875,58 @@ __global__ void k_outflow(uint32_t nT, uint32_t nq, uint32_t nbf, const uint32_t
     if (grid_reduce<1>(v, partials, counter, tot) && threadIdx.x == 0) out[0] = tot[0];
 }
 
+// ---- diffusion synthetic acceleration ----------------------------------------
+// The diffusion correction of the scalar flux: b_v = sum over the cells c at
+// vertex v (local vertex j) of int_c sigma_s y lambda_j = sigma_s V/20 (y_j +
+// sum_i y_i), on the even-parity operator's vertex layout [nP][aslm] (l = 0).
+__global__ void k_dsa_rhs(uint32_t nP, uint32_t aslm, const uint32_t *vc_start, const uint32_t *vc_cj,
+                          const double *ssv, const double *y, double *b) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < nP; v += gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (uint32_t i = vc_start[v]; i < vc_start[v + 1]; ++i) {
+            const uint32_t cj = vc_cj[i], c = cj >> 2, j = cj & 3u;
+            const double *yc = y + 4 * (size_t)c;
+            acc += ssv[c] / 20.0 * (yc[j] + yc[0] + yc[1] + yc[2] + yc[3]);
+        }
+        for (uint32_t l = 0; l < aslm; ++l) b[(size_t)v * aslm + l] = l == 0 ? acc : 0.0;
+    }
+}
+// z = y + the correction f carried to every unknown: J[c][j] += f[vertex(c,
+// j)], and each inflow value of B (reflective entry or lagged face, indexed by
+// its cell's local vertex j, zero at the face's own index k) += f[vertex(c,
+// j)] -- near the diffusion limit the error of the angular flux is isotropic
+__global__ void k_dsa_prolong(uint32_t nT, uint32_t nent, uint64_t nB, uint32_t aslm, const uint4 *cell_p,
+                              const uint32_t *ent_cell, const unsigned long long *lag_keys, const double *f,
+                              const double *y, double *z) {
+    const uint64_t n = 4ull * nT + nB;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        double v = y[i];
+        uint32_t c, j, k = 4;
+        if (i < 4ull * nT) {
+            c = static_cast<uint32_t>(i >> 2);
+            j = static_cast<uint32_t>(i & 3u);
+        } else {
+            const uint64_t b = i - 4ull * nT, e = b >> 2;
+            j = static_cast<uint32_t>(b & 3u);
+            if (e < nent) {
+                const uint32_t ck = ent_cell[e];
+                c = ck >> 2;
+                k = ck & 3u;
+            } else {
+                const unsigned long long key = lag_keys[e - nent];
+                c = static_cast<uint32_t>((key >> 2) % nT);
+                k = static_cast<uint32_t>(key & 3u);
+            }
+        }
+        if (j != k) {
+            const uint4 p = cell_p[c];
+            const uint32_t vert = j == 0 ? p.x : j == 1 ? p.y : j == 2 ? p.z : p.w;
+            v += f[(size_t)vert * aslm];
+        }
+        z[i] = v;
+    }
+}
+
 // ---- FP64 vector kernels of the Krylov solver --------------------------------
 __global__ void k_to_f32(uint64_t n, const double *x, float *y) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
@@ -1051,6 +1103,18 @@ struct tr_sweep {
     double *kb = nullptr, *kx = nullptr, *kt = nullptr, *kh = nullptr;
     int kv_m = 0;
     cudaEvent_t ev[2] = {nullptr, nullptr};
+    // diffusion synthetic acceleration (tr_sweep_enable_dsa): the even-parity
+    // operator with l = 0 only on the same mesh, vertex -> (cell, local vertex)
+    // CSR, cell vertices, the diffusion right-hand side and solution
+    tr_ctx *dsa = nullptr;
+    uint32_t nP = 0, dsa_aslm = 0;
+    uint32_t *vc_start = nullptr, *vc_cj = nullptr;
+    uint4 *cell_p = nullptr;
+    double *dsa_b = nullptr, *dsa_f = nullptr;
+    double *kz = nullptr;          // flexible GMRES: preconditioned basis [kMaxRestart + 1][n]
+    int kz_m = 0;
+    int64_t dsa_solves = 0, dsa_iterations = 0;
+    std::string prec_error;
     std::vector<void *> allocs;
     int64_t sweeps32 = 0, sweeps64 = 0, launches = 0;
 };
@@ -1087,6 +1151,7 @@ static void sw_free(tr_sweep *s) {
     cudaGetDevice(&prev);
     cudaSetDevice(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
+    if (s->dsa) tr_ctx_destroy(s->dsa);
     for (void *p : s->allocs) cudaFree(p);
     for (auto &e : s->ev)
         if (e) cudaEventDestroy(e);
@@ -1598,14 +1663,64 @@ static cudaError_t vnorm(tr_sweep *S, const double *x, double *out) {
     return e;
 }
 
+// Diffusion correction f = C sigma_s y into S->dsa_f: C solves the P1
+// diffusion problem (the l = 0 even-parity operator: sigma_a mass, 1 / (3
+// sigma_t) stiffness, Marshak faces) by FP64 Jacobi CG to tol relative to the
+// right-hand side; a zero right-hand side gives f = 0 without a solve.
+static cudaError_t dsa_solve(tr_sweep *S, const double *y, double tol) {
+    cudaStream_t st = S->stream;
+    const uint64_t np = static_cast<uint64_t>(S->nP) * S->dsa_aslm;
+    k_dsa_rhs<<<grid_for(S, S->nP), 256, 0, st>>>(S->nP, S->dsa_aslm, S->vc_start, S->vc_cj, S->ssv64, y, S->dsa_b);
+    k_multidot<<<kDotGrid, 256, 0, st>>>(np, 1, S->dsa_b, 0, S->dsa_b, S->partials, S->counter, S->red);
+    S->launches += 2;
+    double bb = 0.0;
+    cudaError_t e = cudaMemcpyAsync(&bb, S->red, sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return e;
+    if (!(bb > 0.0)) return cudaMemsetAsync(S->dsa_f, 0, np * sizeof(double), st);
+    tr_solve_opts o;
+    tr_solve_opts_default(&o);
+    o.mode = TR_MODE_FP64;
+    o.precondition = TR_PREC_JACOBI;
+    o.relative = 0;
+    o.tol = tol * std::sqrt(bb);
+    o.max_iter = 10000;
+    tr_solve_report rep;
+    const tr_status ts = tr_solve(S->dsa, &o, S->dsa_b, S->dsa_f, &rep);
+    ++S->dsa_solves;
+    S->dsa_iterations += rep.iterations;
+    if (ts != TR_OK && ts != TR_ERR_NOT_CONVERGED) {
+        S->prec_error = std::string("diffusion solve: ") + tr_last_error(S->dsa);
+        return cudaErrorUnknown;
+    }
+    return cudaSuccess;
+}
+// z = base + the correction f on every unknown (k_dsa_prolong)
+static cudaError_t dsa_prolong(tr_sweep *S, const double *base, double *z) {
+    const uint64_t n = S->nJ + S->nB;
+    k_dsa_prolong<<<grid_for(S, n), 256, 0, S->stream>>>(S->nT, S->nent, S->nB, S->dsa_aslm, S->cell_p, S->ent_cell,
+                                                         S->lag_keys, S->dsa_f, base, z);
+    ++S->launches;
+    return cudaGetLastError();
+}
+
 // GMRES(m) on (I - T_prec) x = b, x updated in place (device vectors).
 // Stops at ||b - (I - T) x|| <= rtol * bref (the recursion estimate,
-// confirmed by a true residual at the end of a cycle).
+// confirmed by a true residual at the end of a cycle).  With dsa_tol > 0 it
+// is right-preconditioned by the diffusion correction P^-1 y = y + C sigma_s y
+// in its flexible form (the inexact inner solve varies from step to step, so
+// the preconditioned basis Z is kept and x += Z y).
 static cudaError_t gmres(tr_sweep *S, int prec, int prec_res, const double *b, double *x, int m, double rtol,
-                         double bref, double cycle_tol, int max_it, int *its, double *res_out, int *cycles_out) {
+                         double bref, double cycle_tol, int max_it, int *its, double *res_out, int *cycles_out,
+                         double dsa_tol = 0.0) {
     const uint64_t n = S->nJ + S->nB;
     cudaError_t e = krylov_alloc(S, m);
     if (e != cudaSuccess) return e;
+    const bool flex = dsa_tol > 0.0;
+    if (flex && (!S->kz || S->kz_m < m)) {
+        if ((e = sw_alloc(S, &S->kz, n * (m + 1))) != cudaSuccess) return e;
+        S->kz_m = m;
+    }
     cudaStream_t st = S->stream;
     std::vector<double> H(static_cast<size_t>(m + 1) * m), cs(m), sn(m), g(m + 1), y(m), h(m + 1);
     double res = 1.0, beta = 0.0;
@@ -1633,7 +1748,14 @@ static cudaError_t gmres(tr_sweep *S, int prec, int prec_res, const double *b, d
         int j = 0;
         for (; j < m && it < max_it; ++j) {
             double *w = S->kv + static_cast<uint64_t>(j + 1) * n;
-            if ((e = op_apply(S, prec, S->kv + static_cast<uint64_t>(j) * n, w)) != cudaSuccess) return e;
+            const double *vj = S->kv + static_cast<uint64_t>(j) * n;
+            if (flex) {
+                double *zj = S->kz + static_cast<uint64_t>(j) * n;
+                if ((e = dsa_solve(S, vj, dsa_tol)) != cudaSuccess) return e;
+                if ((e = dsa_prolong(S, vj, zj)) != cudaSuccess) return e;
+                vj = zj;
+            }
+            if ((e = op_apply(S, prec, vj, w)) != cudaSuccess) return e;
             ++it;
             // classical Gram-Schmidt; the first pass also gives ||w||^2 (w is
             // basis row j + 1), and a second pass runs only when the first
@@ -1684,7 +1806,7 @@ static cudaError_t gmres(tr_sweep *S, int prec, int prec_res, const double *b, d
         }
         e = cudaMemcpyAsync(S->kh, y.data(), sizeof(double) * j, cudaMemcpyHostToDevice, st);
         if (e != cudaSuccess) return e;
-        k_combine<<<gr, 256, 0, st>>>(n, j, S->kv, n, S->kh, x);
+        k_combine<<<gr, 256, 0, st>>>(n, j, flex ? S->kz : S->kv, n, S->kh, x);
         ++S->launches;
         if (res <= rtol || cycle_tol > 0.0) {  // the true residual: confirm, or start the next cycle from it
             if ((e = op_apply(S, prec_res, x, S->kv)) != cudaSuccess) return e;
@@ -1947,6 +2069,98 @@ void tr_sweep_opts_default(tr_sweep_opts *o) {
     o->restart = 30;
     o->inner_tol = 0.0;
     o->max_outer = 30;
+    o->precondition = TR_SWEEP_PREC_NONE;
+    o->precond_tol = 1e-3;
+}
+
+tr_status tr_sweep_enable_dsa(tr_sweep *s, const tr_mesh_view *mesh, const tr_physics_view *phys) {
+    SW_CHECK(s);
+    if (!mesh || !mesh->mesh || !mesh->tetstart || !mesh->tetidx || !mesh->tetpos)
+        return sw_err(s, TR_ERR_INVALID_ARG, "tr_sweep_enable_dsa: incomplete mesh view");
+    if (mesh->nT != s->nT || mesh->nF != s->nF)
+        return sw_err(s, TR_ERR_INVALID_ARG, "tr_sweep_enable_dsa: mesh differs from the sweep's");
+    if (s->dsa) return TR_OK;
+    const uint32_t nP = mesh->nP, nT = mesh->nT;
+    if (mesh->nF && (!mesh->bnd || !mesh->facestart || !mesh->faceidx || !mesh->facepos))
+        return sw_err(s, TR_ERR_INVALID_ARG, "tr_sweep_enable_dsa: incomplete face arrays");
+    if (mesh->tetstart[0] != 0 || mesh->tetstart[nP] != 4ull * nT)
+        return sw_err(s, TR_ERR_MESH, "tr_sweep_enable_dsa: vertex -> cell table does not cover 4 nT entries");
+    std::vector<uint32_t> vstart(mesh->tetstart, mesh->tetstart + nP + 1), vcj(4ull * nT);
+    for (uint32_t v = 0; v < nP; ++v) {
+        if (vstart[v + 1] < vstart[v]) return sw_err(s, TR_ERR_MESH, "tr_sweep_enable_dsa: tetstart decreases");
+        for (uint32_t i = vstart[v]; i < vstart[v + 1]; ++i) {
+            const uint32_t c = mesh->tetidx[i], j = mesh->tetpos[i];
+            if (c >= nT || j > 3 || mesh->mesh[c].p[j] != v)
+                return sw_err(s, TR_ERR_MESH, "tr_sweep_enable_dsa: inconsistent vertex -> cell table");
+            vcj[i] = 4 * c + j;
+        }
+    }
+    std::vector<uint4> cp(nT);
+    for (uint32_t c = 0; c < nT; ++c) {
+        const tr_idx *p = mesh->mesh[c].p;
+        if (p[0] >= nP || p[1] >= nP || p[2] >= nP || p[3] >= nP)
+            return sw_err(s, TR_ERR_MESH, "tr_sweep_enable_dsa: vertex index out of range");
+        cp[c] = make_uint4(p[0], p[1], p[2], p[3]);
+    }
+    cudaSetDevice(s->device);
+    tr_angular *ang = nullptr;
+    tr_status st = tr_angular_create(0, &ang);
+    if (st != TR_OK) return sw_err(s, st, "tr_sweep_enable_dsa: angular tables");
+    tr_angular_view av;
+    tr_angular_view_get(ang, &av);
+    // Vacuum and incident faces carry the operator's l = 0 surface term, 1/2
+    // of its face measure |s_x + s_y + s_z| (the face area on the axis-aligned
+    // faces of a box), a Marshak condition for the homogeneous correction.
+    // Reflective faces (zero current) carry none: they are left out of the
+    // diffusion context's face list.
+    const int32_t *bc = phys ? phys->face_bc : nullptr;
+    std::vector<tr_face> fkeep;
+    std::vector<tr_idx> fnew(mesh->nF, ~0u), fstart(nP + 1, 0), fidx, fpos;
+    for (uint32_t f = 0; f < mesh->nF; ++f)
+        if (!bc || bc[f] != TR_BC_REFLECTIVE) {
+            fnew[f] = static_cast<tr_idx>(fkeep.size());
+            fkeep.push_back(mesh->bnd[f]);
+        }
+    for (uint32_t v = 0; v < nP && mesh->nF; ++v) {
+        for (tr_idx i = mesh->facestart[v]; i < mesh->facestart[v + 1]; ++i) {
+            const tr_idx f = mesh->faceidx[i];
+            if (f >= mesh->nF) {
+                tr_angular_destroy(ang);
+                return sw_err(s, TR_ERR_MESH, "tr_sweep_enable_dsa: face index out of range");
+            }
+            if (fnew[f] == ~0u) continue;
+            fidx.push_back(fnew[f]);
+            fpos.push_back(mesh->facepos[i]);
+        }
+        fstart[v + 1] = static_cast<tr_idx>(fidx.size());
+    }
+    tr_mesh_view mv = *mesh;
+    mv.nF = static_cast<tr_idx>(fkeep.size());
+    mv.bnd = fkeep.data();
+    mv.facestart = fstart.data();
+    mv.faceidx = fidx.data();
+    mv.facepos = fpos.data();
+    const tr_physics_view pv = {phys ? phys->kappa_abs_volume : nullptr, nullptr, nullptr, TR_SURFACE_AXIS};
+    tr_ctx *ctx = nullptr;
+    st = tr_ctx_create_ex(s->device, &mv, &av, &pv, &ctx);
+    tr_angular_destroy(ang);
+    if (st != TR_OK) return sw_err(s, st, std::string("tr_sweep_enable_dsa: ") + tr_last_error(nullptr));
+    tr_ctx_info info;
+    tr_ctx_info_get(ctx, &info);
+    s->dsa = ctx;
+    s->nP = nP;
+    s->dsa_aslm = info.aslm;
+    cudaError_t e = sw_upload(s, &s->vc_start, vstart);
+    if (e == cudaSuccess) e = sw_upload(s, &s->vc_cj, vcj);
+    if (e == cudaSuccess) e = sw_upload(s, &s->cell_p, cp);
+    if (e == cudaSuccess) e = sw_alloc(s, &s->dsa_b, static_cast<size_t>(nP) * info.aslm);
+    if (e == cudaSuccess) e = sw_alloc(s, &s->dsa_f, static_cast<size_t>(nP) * info.aslm);
+    if (e != cudaSuccess) {
+        tr_ctx_destroy(s->dsa);
+        s->dsa = nullptr;
+        return sw_cuda(s, e, "tr_sweep_enable_dsa");
+    }
+    return TR_OK;
 }
 
 tr_status tr_sweep_solve(tr_sweep *s, const tr_sweep_opts *opts, double *J, double *B, tr_sweep_report *rep) {
@@ -1959,11 +2173,20 @@ tr_status tr_sweep_solve(tr_sweep *s, const tr_sweep_opts *opts, double *J, doub
     if (o.mode != TR_MODE_FP64 && o.mode != TR_MODE_MIXED) return sw_err(s, TR_ERR_INVALID_ARG, "bad mode");
     if (o.method != TR_SWEEP_GMRES && o.method != TR_SWEEP_SOURCE_ITERATION)
         return sw_err(s, TR_ERR_INVALID_ARG, "bad method");
+    if (o.precondition != TR_SWEEP_PREC_NONE && o.precondition != TR_SWEEP_PREC_DSA)
+        return sw_err(s, TR_ERR_INVALID_ARG, "bad precondition");
+    const bool dsa = o.precondition == TR_SWEEP_PREC_DSA;
+    if (dsa && !s->dsa) return sw_err(s, TR_ERR_INVALID_ARG, "precondition DSA needs tr_sweep_enable_dsa");
+    if (dsa && !(o.precond_tol > 0.0 && o.precond_tol < 1.0))
+        return sw_err(s, TR_ERR_INVALID_ARG, "precond_tol must be in (0, 1)");
+    const double dsa_tol = dsa ? o.precond_tol : 0.0;
+    s->prec_error.clear();
     const uint64_t n = s->nJ + s->nB;
     cudaError_t e = krylov_alloc(s, o.restart);
     if (e != cudaSuccess) return sw_cuda(s, e, "tr_sweep_solve: allocation");
     cudaStream_t st = s->stream;
     const int64_t s32_0 = s->sweeps32, s64_0 = s->sweeps64, l0 = s->launches;
+    const int64_t d0 = s->dsa_solves, di0 = s->dsa_iterations;
     cudaEventRecord(s->ev[0], st);
     // b = S_64(0) with sources; x = 0
     e = sweep_enqueue(s, 64, nullptr, nullptr, 1, s->kb, s->nB ? s->kb + s->nJ : nullptr);
@@ -1990,7 +2213,17 @@ tr_status tr_sweep_solve(tr_sweep *s, const tr_sweep_opts *opts, double *J, doub
                 double dn = 0.0, tn = 0.0;
                 if ((e = vnorm(s, s->kx, &dn)) != cudaSuccess) break;
                 if ((e = vnorm(s, s->kt, &tn)) != cudaSuccess) break;
-                e = cudaMemcpyAsync(s->kx, s->kt, n * 8, cudaMemcpyDeviceToDevice, st);
+                if (!std::isfinite(dn) || !std::isfinite(tn)) {  // diverged: not converged
+                    res = dn;
+                    break;
+                }
+                if (dsa) {
+                    // x <- S(x) + C sigma_s (S(x) - x): the diffusion estimate of the error
+                    if ((e = dsa_solve(s, s->kx, dsa_tol)) != cudaSuccess) break;
+                    e = dsa_prolong(s, s->kt, s->kx);
+                } else {
+                    e = cudaMemcpyAsync(s->kx, s->kt, n * 8, cudaMemcpyDeviceToDevice, st);
+                }
                 res = tn > 0.0 ? dn / tn : 0.0;
                 if (res < o.tol) {
                     conv = true;
@@ -1998,7 +2231,7 @@ tr_status tr_sweep_solve(tr_sweep *s, const tr_sweep_opts *opts, double *J, doub
                 }
             }
         } else if (o.mode == TR_MODE_FP64) {
-            e = gmres(s, 64, 64, s->kb, s->kx, o.restart, o.tol, bn, 0.0, o.max_iter, &its, &res, nullptr);
+            e = gmres(s, 64, 64, s->kb, s->kx, o.restart, o.tol, bn, 0.0, o.max_iter, &its, &res, nullptr, dsa_tol);
             conv = e == cudaSuccess && res <= o.tol;
         } else {
             // FP32 sweeps inside FP64 defect correction: each GMRES cycle starts
@@ -2006,7 +2239,8 @@ tr_status tr_sweep_solve(tr_sweep *s, const tr_sweep_opts *opts, double *J, doub
             // builds its Krylov space with FP32 sweeps; the correction is added
             // to x in FP64.  A cycle ends at its restart length, at the target,
             // or (inner_tol > 0) once it has reduced its residual by inner_tol.
-            e = gmres(s, 32, 64, s->kb, s->kx, o.restart, o.tol, bn, o.inner_tol, o.max_iter, &its, &res, &outer);
+            e = gmres(s, 32, 64, s->kb, s->kx, o.restart, o.tol, bn, o.inner_tol, o.max_iter, &its, &res, &outer,
+                      dsa_tol);
             conv = e == cudaSuccess && res <= o.tol;
         }
     }
@@ -2014,6 +2248,10 @@ tr_status tr_sweep_solve(tr_sweep *s, const tr_sweep_opts *opts, double *J, doub
     if (e == cudaSuccess && B && s->nB) e = cudaMemcpyAsync(B, s->kx + s->nJ, s->nB * 8, cudaMemcpyDeviceToDevice, st);
     cudaEventRecord(s->ev[1], st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e == cudaErrorUnknown && !s->prec_error.empty()) {
+        cudaStreamSynchronize(st);
+        return sw_err(s, TR_ERR_CUDA, "tr_sweep_solve: " + s->prec_error);
+    }
     if (e != cudaSuccess) return sw_cuda(s, e, "tr_sweep_solve");
     if (rep) {
         float ms = 0.0f;
@@ -2027,6 +2265,8 @@ tr_status tr_sweep_solve(tr_sweep *s, const tr_sweep_opts *opts, double *J, doub
         rep->rhs_norm = bn;
         rep->device_ms = ms;
         rep->kernel_launches = s->launches - l0;
+        rep->precond_solves = static_cast<int32_t>(s->dsa_solves - d0);
+        rep->precond_iterations = static_cast<int32_t>(s->dsa_iterations - di0);
     }
     if (!conv) return sw_err(s, TR_ERR_NOT_CONVERGED, "tr_sweep_solve: not converged");
     return TR_OK;

@@ -31,9 +31,12 @@ class SweepReport(dict):
 
 
 class Sweep:
-    """Sweep(device, md, ordinates=(x, y, z, w), physics=None)."""
+    """Sweep(device, md, ordinates=(x, y, z, w), physics=None, dsa=False).
 
-    def __init__(self, device, md, ordinates, physics=None):
+    dsa=True prepares the diffusion operator for solve(precondition=
+    TR_SWEEP_PREC_DSA) (tr_sweep_enable_dsa)."""
+
+    def __init__(self, device, md, ordinates, physics=None, dsa=False):
         import torch  # device-memory plumbing only
         self._torch = torch
         self.ordinates = tuple(np.ascontiguousarray(a, dtype=np.float64) for a in ordinates)
@@ -53,6 +56,8 @@ class Sweep:
         self.n_extra, self.n_reflective, self.n_lag = info.n_extra, info.n_reflective, info.n_lag
         self.max_levels, self.forced_levels, self.device_bytes = info.max_levels, info.forced_levels, info.device_bytes
         self.device = device
+        if dsa:
+            self._c(lib.tr_sweep_enable_dsa(h, C.byref(mv), C.byref(pv) if pv is not None else None))
 
     def _c(self, st):
         if st != L.TR_OK:
