@@ -356,6 +356,14 @@ enum { TR_SWEEP_GMRES = 0, TR_SWEEP_SOURCE_ITERATION = 1 };
  * and zero current (reflective) -- the even-parity operator with l = 0 only,
  * continuous linear elements on the vertices, by FP64 Jacobi CG. */
 enum { TR_SWEEP_PREC_NONE = 0, TR_SWEEP_PREC_DSA = 1 };
+/* Where the diffusion CG runs.  CLUSTER: the assembled matrix (ELL) in one
+ * thread-block cluster of 16 (or 8) CTAs with hardware cluster barriers, no
+ * host round trip per solve, preconditioned by Jacobi plus an aggregation
+ * coarse space (16 row blocks per CTA); meshes up to 2^18 vertices.  EVEN_PARITY: the
+ * even-parity operator with l = 0 (tr_solve on its own context; its face
+ * term uses the operator's face measure |s_x + s_y + s_z|, equal to the area
+ * on axis-aligned faces).  AUTO: CLUSTER where available. */
+enum { TR_SWEEP_DSA_AUTO = 0, TR_SWEEP_DSA_CLUSTER = 1, TR_SWEEP_DSA_EVEN_PARITY = 2 };
 typedef struct tr_sweep_opts {
     int32_t method;            /* TR_SWEEP_*                                */
     int32_t mode;              /* TR_MODE_FP64, or TR_MODE_MIXED: FP32
@@ -373,6 +381,7 @@ typedef struct tr_sweep_opts {
     int32_t precondition;      /* TR_SWEEP_PREC_*                           */
     double  precond_tol;       /* DSA: relative tolerance of each diffusion
                                   solve (FP64 Jacobi CG), in (0, 1)        */
+    int32_t precond_engine;    /* TR_SWEEP_DSA_*                            */
 } tr_sweep_opts;
 typedef struct tr_sweep_report {
     int32_t converged;

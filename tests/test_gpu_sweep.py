@@ -132,9 +132,13 @@ def test_mixed_precision_solve(cuda):
     assert abs(b["emitted"] + b["incoming"] - b["absorbed"] - b["escaped"]) < 1e-8 * b["emitted"]
 
 
-def test_dsa_gmres_matches_oracle(cuda):
+@pytest.mark.parametrize("engine", ["cluster", "even_parity"])
+def test_dsa_gmres_matches_oracle(cuda, engine):
     """Flexible GMRES with the diffusion correction reaches the oracle's
-    fixed point in fewer Krylov steps, one diffusion solve per step."""
+    fixed point in fewer Krylov steps, one diffusion solve per step, with the
+    diffusion CG in one thread-block cluster or on the even-parity context
+    (the same diffusion matrix on this box, whose faces are axis-aligned)."""
+    L = tr._lib
     md, ph = diffusive_box()
     ords = op.ordinates_product(4, 8)
     S = tr.Sweep(0, md, ords, ph, dsa=True)
@@ -142,12 +146,29 @@ def test_dsa_gmres_matches_oracle(cuda):
                        face_incident=ph.face_incident)
     Jo, Bo, info = O.solve(method=1, tol=1e-11)
     J0, B0, r0 = S.solve(tol=1e-10, max_iter=2000)
-    J1, B1, r1 = S.solve(tol=1e-10, precondition=tr._lib.TR_SWEEP_PREC_DSA)
+    eng = L.TR_SWEEP_DSA_CLUSTER if engine == "cluster" else L.TR_SWEEP_DSA_EVEN_PARITY
+    J1, B1, r1 = S.solve(tol=1e-10, precondition=L.TR_SWEEP_PREC_DSA, precond_engine=eng, precond_tol=1e-3)
     assert info["converged"] and r0.converged and r1.converged
     assert r1.residual <= 1e-10 and r1.precond_solves == r1.iterations and r1.precond_iterations > 0
     assert r1.iterations < r0.iterations / 2, (r1.iterations, r0.iterations)
     assert rel_err(host(J1), Jo) < 1e-8 and rel_err(host(B1), Bo) < 1e-8
     assert r0.precond_solves == 0
+
+
+def test_dsa_engines_agree(cuda):
+    """Both diffusion engines solve the same system to 1e-6: the same Krylov
+    steps; the cluster engine's two-level CG (aggregation coarse space) needs
+    fewer CG iterations than the even-parity context's Jacobi CG."""
+    L = tr._lib
+    md, ph = diffusive_box(n=(5, 5, 5))
+    S = tr.Sweep(0, md, op.ordinates_product(4, 8), ph, dsa=True)
+    kw = dict(tol=1e-10, precondition=L.TR_SWEEP_PREC_DSA, precond_tol=1e-6)
+    Jc, _, rc = S.solve(precond_engine=L.TR_SWEEP_DSA_CLUSTER, **kw)
+    Je, _, re = S.solve(precond_engine=L.TR_SWEEP_DSA_EVEN_PARITY, **kw)
+    assert rc.converged and re.converged
+    assert abs(rc.iterations - re.iterations) <= 1
+    assert 0 < rc.precond_iterations < re.precond_iterations
+    assert rel_err(host(Jc), host(Je)) < 1e-8
 
 
 def test_dsa_mixed_and_source_iteration(cuda):
@@ -176,6 +197,8 @@ def test_dsa_needs_enable(cuda):
         S2.solve(precondition=tr._lib.TR_SWEEP_PREC_DSA, precond_tol=0.0)
     with pytest.raises(tr.TransferError):
         S2.solve(precondition=7)
+    with pytest.raises(tr.TransferError):
+        S2.solve(precondition=tr._lib.TR_SWEEP_PREC_DSA, precond_engine=5)
 
 
 def test_absorbing_slab_matches_e2_on_gpu(cuda):

@@ -34,6 +34,7 @@ TR_ENGINE_PERSISTENT, TR_ENGINE_GRAPH, TR_ENGINE_LAUNCH, TR_ENGINE_PERSISTENT_SR
 TR_OPERATOR_SIMT, TR_OPERATOR_TENSOR = 0, 1
 TR_SWEEP_GMRES, TR_SWEEP_SOURCE_ITERATION = 0, 1
 TR_SWEEP_PREC_NONE, TR_SWEEP_PREC_DSA = 0, 1
+TR_SWEEP_DSA_AUTO, TR_SWEEP_DSA_CLUSTER, TR_SWEEP_DSA_EVEN_PARITY = 0, 1, 2
 TR_VTK_POINT, TR_VTK_CELL = 0, 1
 TR_VTK_SCALAR, TR_VTK_VECTOR, TR_VTK_TENSOR = 0, 1, 2
 
@@ -110,7 +111,7 @@ class tr_sweep_info(C.Structure):
 class tr_sweep_opts(C.Structure):
     _fields_ = [("method", C.c_int32), ("mode", C.c_int32), ("tol", C.c_double), ("max_iter", C.c_int32),
                 ("restart", C.c_int32), ("inner_tol", C.c_double), ("max_outer", C.c_int32),
-                ("precondition", C.c_int32), ("precond_tol", C.c_double)]
+                ("precondition", C.c_int32), ("precond_tol", C.c_double), ("precond_engine", C.c_int32)]
 
 
 class tr_vtk_field(C.Structure):

@@ -40,6 +40,7 @@
 // memory by the threads shifted by half a block while the current chunk is
 // computed.  Blocks never wait on one another, so a sweep has no
 // inter-block waits.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -927,6 +928,214 @@ __global__ void k_dsa_prolong(uint32_t nT, uint32_t nent, uint64_t nB, uint32_t 
     }
 }
 
+// Two-level preconditioned CG on the assembled diffusion matrix (ELL, column
+// major: val/col[j * n + i] for row i, padded with zeros on the diagonal)
+// run by ONE thread-block cluster.  Rows are split evenly over its CTAs
+// (CTA k: rows [k per, (k + 1) per)), and each CTA's rows into kDsaAgg
+// contiguous aggregates; the preconditioner is additive two-level,
+//   z = D^-1 r + P A_c^-1 P^T r,   A_c = P^T K P  (P: aggregate indicator),
+// with A_c^-1 precomputed on the host (nr kDsaAgg square, L2-resident).
+// Vectors live in global memory (L2-resident at these sizes); each
+// iteration synchronises with four hardware cluster barriers, three of
+// which carry dot products or aggregate sums through distributed shared
+// memory.  Every CTA sums the CTAs' values in rank order, so all of them see
+// bit-identical scalars and take the same branch: the loop needs no grid
+// barrier and no spin.  Stops at ||r|| <= tol ||b|| or maxit.
+namespace cgr = cooperative_groups;
+constexpr int kDsaThreads = 1024;
+constexpr int kDsaAgg = 16;                        // aggregates per CTA
+constexpr int kDsaMaxCluster = 16;
+constexpr uint32_t kDsaClusterMaxRows = 1u << 18;  // larger problems use the even-parity context
+struct DsaCg {
+    uint32_t n, w;
+    const uint32_t *col;
+    const double *val, *dinv, *b;
+    const double *ainv;          // [nc][nc], nc = cluster size * kDsaAgg
+    double *x, *r, *p, *q;
+    double tol;
+    int maxit;
+    unsigned long long *stats;   // [0] CG iterations, [1] solves, [2] non-finite stops
+};
+struct DsaShared {
+    double slots[2][2];          // dot products: ring of two, rewritten only two barriers later
+    double agg[1 + kDsaAgg];     // ||r||^2 partial and this CTA's aggregate sums of r
+    double rc[kDsaMaxCluster * kDsaAgg];  // every aggregate sum, gathered
+    double e[kDsaAgg];           // coarse correction of this CTA's aggregates
+    double2 wsum[kDsaThreads / 32];
+    double2 bcast;
+};
+__device__ __forceinline__ double dsa_warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;  // lane 0
+}
+// sum of (v0, v1) over the cluster, identical bits in every CTA
+__device__ __forceinline__ double2 dsa_cluster_sum(cgr::cluster_group &cl, double v0, double v1, double *slot,
+                                                   DsaShared &sh) {
+    v0 = dsa_warp_sum(v0);
+    v1 = dsa_warp_sum(v1);
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    if (lane == 0) sh.wsum[warp] = make_double2(v0, v1);
+    __syncthreads();
+    if (warp == 0) {
+        const double2 t = lane < (blockDim.x >> 5) ? sh.wsum[lane] : make_double2(0.0, 0.0);
+        const double a0 = dsa_warp_sum(t.x), a1 = dsa_warp_sum(t.y);
+        if (lane == 0) {
+            slot[0] = a0;
+            slot[1] = a1;
+        }
+    }
+    cl.sync();
+    if (warp == 0) {
+        double a0 = 0.0, a1 = 0.0;
+        if (lane < cl.num_blocks()) {
+            const double *rs = cl.map_shared_rank(slot, static_cast<int>(lane));
+            a0 = rs[0];
+            a1 = rs[1];
+        }
+        a0 = dsa_warp_sum(a0);
+        a1 = dsa_warp_sum(a1);
+        if (lane == 0) sh.bcast = make_double2(a0, a1);
+    }
+    __syncthreads();
+    return sh.bcast;
+}
+// first row of local aggregate g (g = 0..kDsaAgg) of the rows [r0, r1)
+__device__ __forceinline__ uint32_t dsa_agg_bound(uint32_t r0, uint32_t r1, int g) {
+    return r0 + static_cast<uint32_t>((static_cast<uint64_t>(r1 - r0) * g) / kDsaAgg);
+}
+// ||r||^2 over the cluster and every aggregate sum of r (into sh.rc); r of
+// this CTA's rows was written by this CTA before the call
+__device__ double dsa_exchange(cgr::cluster_group &cl, const DsaCg &a, uint32_t r0, uint32_t r1, double rr,
+                               DsaShared &sh) {
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    rr = dsa_warp_sum(rr);
+    if (lane == 0) sh.wsum[warp] = make_double2(rr, 0.0);
+    __syncthreads();  // also orders this CTA's writes of r before the sums below
+    if (warp < kDsaAgg) {
+        const uint32_t g0 = dsa_agg_bound(r0, r1, warp), g1 = dsa_agg_bound(r0, r1, warp + 1);
+        double sum = 0.0;
+        for (uint32_t i = g0 + lane; i < g1; i += 32) sum += a.r[i];
+        sum = dsa_warp_sum(sum);
+        if (lane == 0) sh.agg[1 + warp] = sum;
+    } else if (warp == kDsaAgg) {
+        const double t = dsa_warp_sum(lane < (blockDim.x >> 5) ? sh.wsum[lane].x : 0.0);
+        if (lane == 0) sh.agg[0] = t;
+    }
+    cl.sync();
+    const unsigned nr = cl.num_blocks();
+    for (unsigned t = threadIdx.x; t < nr * kDsaAgg; t += blockDim.x) {
+        const double *rs = cl.map_shared_rank(sh.agg, static_cast<int>(t / kDsaAgg));
+        sh.rc[t] = rs[1 + t % kDsaAgg];
+    }
+    if (warp == 0) {
+        double v = 0.0;
+        if (lane < nr) v = cl.map_shared_rank(sh.agg, static_cast<int>(lane))[0];
+        v = dsa_warp_sum(v);
+        if (lane == 0) sh.bcast = make_double2(v, 0.0);
+    }
+    __syncthreads();
+    return sh.bcast.x;
+}
+// z = D^-1 r + e[aggregate] into q (own rows); returns the local part of r.z
+__device__ double dsa_precondition(cgr::cluster_group &cl, const DsaCg &a, uint32_t r0, uint32_t r1,
+                                   DsaShared &sh) {
+    const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const unsigned nc = cl.num_blocks() * kDsaAgg, rank = cl.block_rank();
+    if (warp < kDsaAgg) {
+        const double *row = a.ainv + (size_t)(rank * kDsaAgg + warp) * nc;
+        double v = 0.0;
+        for (unsigned b = lane; b < nc; b += 32) v += __ldg(row + b) * sh.rc[b];
+        v = dsa_warp_sum(v);
+        if (lane == 0) sh.e[warp] = v;
+    }
+    __syncthreads();
+    double rz = 0.0;
+    for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+        int g = 0;
+        while (g + 1 < kDsaAgg && i >= dsa_agg_bound(r0, r1, g + 1)) ++g;
+        const double ri = a.r[i], zi = __ldg(a.dinv + i) * ri + sh.e[g];
+        a.q[i] = zi;
+        rz += ri * zi;
+    }
+    return rz;
+}
+__global__ void __launch_bounds__(kDsaThreads, 1) k_dsa_cg(const __grid_constant__ DsaCg a) {
+    cgr::cluster_group cl = cgr::this_cluster();
+    __shared__ DsaShared sh;
+    const uint32_t nr = cl.num_blocks(), rank = cl.block_rank();
+    const uint32_t per = (a.n + nr - 1) / nr;
+    const uint32_t r0 = min(a.n, rank * per), r1 = min(a.n, r0 + per);
+    int sl = 0;
+    double l0 = 0.0;
+    for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+        const double bi = __ldg(a.b + i);
+        a.x[i] = 0.0;
+        a.r[i] = bi;
+        l0 += bi * bi;
+    }
+    const double bb = dsa_exchange(cl, a, r0, r1, l0, sh);
+    const double tol = a.tol * sqrt(bb);
+    int k = 0, bad = 0;
+    if (bb > 0.0 && isfinite(bb)) {
+        // z_0 into q, p_0 = z_0
+        double2 t = dsa_cluster_sum(cl, dsa_precondition(cl, a, r0, r1, sh), 0.0, sh.slots[sl], sh);
+        sl ^= 1;
+        double rz = t.x;
+        for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) a.p[i] = a.q[i];
+        cl.sync();  // p of every CTA visible before the product
+        while (k < a.maxit) {
+            l0 = 0.0;
+            for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+                double acc = 0.0;
+                uint32_t j = 0;
+                for (; j + 4 <= a.w; j += 4) {
+                    const size_t e = (size_t)j * a.n + i, n = a.n;
+                    const uint32_t c0 = __ldg(a.col + e), c1 = __ldg(a.col + e + n), c2 = __ldg(a.col + e + 2 * n),
+                                   c3 = __ldg(a.col + e + 3 * n);
+                    const double v0 = __ldg(a.val + e), v1 = __ldg(a.val + e + n), v2 = __ldg(a.val + e + 2 * n),
+                                 v3 = __ldg(a.val + e + 3 * n);
+                    acc += v0 * a.p[c0] + v1 * a.p[c1] + v2 * a.p[c2] + v3 * a.p[c3];
+                }
+                for (; j < a.w; ++j) {
+                    const size_t e = (size_t)j * a.n + i;
+                    acc += __ldg(a.val + e) * a.p[__ldg(a.col + e)];
+                }
+                a.q[i] = acc;
+                l0 += a.p[i] * acc;
+            }
+            t = dsa_cluster_sum(cl, l0, 0.0, sh.slots[sl], sh);
+            sl ^= 1;
+            const double alpha = rz / t.x;
+            l0 = 0.0;
+            for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+                a.x[i] += alpha * a.p[i];
+                const double ri = a.r[i] - alpha * a.q[i];
+                a.r[i] = ri;
+                l0 += ri * ri;
+            }
+            const double rr = dsa_exchange(cl, a, r0, r1, l0, sh);
+            ++k;
+            if (!isfinite(rr) || !isfinite(alpha)) {
+                bad = 1;
+                break;
+            }
+            if (sqrt(rr) <= tol) break;
+            t = dsa_cluster_sum(cl, dsa_precondition(cl, a, r0, r1, sh), 0.0, sh.slots[sl], sh);
+            sl ^= 1;
+            const double beta = t.x / rz;
+            rz = t.x;
+            for (uint32_t i = r0 + threadIdx.x; i < r1; i += blockDim.x) a.p[i] = a.q[i] + beta * a.p[i];
+            cl.sync();  // p of every CTA visible before the next product
+        }
+    }
+    cl.sync();  // no CTA leaves while another may still read its shared memory
+    if (rank == 0 && threadIdx.x == 0) {
+        atomicAdd(a.stats, static_cast<unsigned long long>(k));
+        atomicAdd(a.stats + 1, 1ull);
+        if (bad) atomicAdd(a.stats + 2, 1ull);
+    }
+}
+
 // ---- FP64 vector kernels of the Krylov solver --------------------------------
 __global__ void k_to_f32(uint64_t n, const double *x, float *y) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
@@ -1111,6 +1320,14 @@ struct tr_sweep {
     uint32_t *vc_start = nullptr, *vc_cj = nullptr;
     uint4 *cell_p = nullptr;
     double *dsa_b = nullptr, *dsa_f = nullptr;
+    // the assembled diffusion matrix for the one-cluster CG (k_dsa_cg)
+    int dsa_cluster = 0;           // CTAs of the cluster (0: the path is unavailable)
+    uint32_t ell_w = 0;
+    uint32_t *ell_col = nullptr;
+    double *ell_val = nullptr, *dsa_dinv = nullptr;
+    double *dsa_ainv = nullptr;    // inverse of the aggregated matrix [nc][nc]
+    double *dsa_vec = nullptr;     // b, x, r, p, q  [5][nP]
+    unsigned long long *dsa_stats = nullptr;
     double *kz = nullptr;          // flexible GMRES: preconditioned basis [kMaxRestart + 1][n]
     int kz_m = 0;
     int64_t dsa_solves = 0, dsa_iterations = 0;
@@ -1663,12 +1880,52 @@ static cudaError_t vnorm(tr_sweep *S, const double *x, double *out) {
     return e;
 }
 
-// Diffusion correction f = C sigma_s y into S->dsa_f: C solves the P1
-// diffusion problem (the l = 0 even-parity operator: sigma_a mass, 1 / (3
-// sigma_t) stiffness, Marshak faces) by FP64 Jacobi CG to tol relative to the
-// right-hand side; a zero right-hand side gives f = 0 without a solve.
-static cudaError_t dsa_solve(tr_sweep *S, const double *y, double tol) {
+// Diffusion correction f = C sigma_s y: C solves the P1 diffusion problem
+// (sigma_a mass, 1 / (3 sigma_t) stiffness, Marshak faces) by FP64 Jacobi CG
+// to tol relative to the right-hand side.  cluster: the assembled matrix in
+// one thread-block cluster (k_dsa_cg, no host synchronisation); otherwise the
+// even-parity context with l = 0 (tr_solve), where a zero right-hand side
+// gives f = 0 without a solve.  The result: dsa_f_of(S, cluster).
+static inline const double *dsa_f_of(const tr_sweep *S, bool cluster) {
+    return cluster ? S->dsa_vec + S->nP : S->dsa_f;
+}
+static cudaError_t dsa_solve(tr_sweep *S, const double *y, double tol, bool cluster, int maxit) {
     cudaStream_t st = S->stream;
+    if (cluster) {
+        const uint32_t n = S->nP;
+        k_dsa_rhs<<<grid_for(S, n), 256, 0, st>>>(n, 1, S->vc_start, S->vc_cj, S->ssv64, y, S->dsa_vec);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(S->dsa_cluster);
+        cfg.blockDim = dim3(kDsaThreads);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = st;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = S->dsa_cluster;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        DsaCg a;
+        a.n = n;
+        a.w = S->ell_w;
+        a.col = S->ell_col;
+        a.val = S->ell_val;
+        a.dinv = S->dsa_dinv;
+        a.ainv = S->dsa_ainv;
+        a.b = S->dsa_vec;
+        a.x = S->dsa_vec + n;
+        a.r = S->dsa_vec + 2ull * n;
+        a.p = S->dsa_vec + 3ull * n;
+        a.q = S->dsa_vec + 4ull * n;
+        a.tol = tol;
+        a.maxit = maxit;
+        a.stats = S->dsa_stats;
+        S->launches += 2;
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        return cudaLaunchKernelEx(&cfg, k_dsa_cg, a);
+    }
     const uint64_t np = static_cast<uint64_t>(S->nP) * S->dsa_aslm;
     k_dsa_rhs<<<grid_for(S, S->nP), 256, 0, st>>>(S->nP, S->dsa_aslm, S->vc_start, S->vc_cj, S->ssv64, y, S->dsa_b);
     k_multidot<<<kDotGrid, 256, 0, st>>>(np, 1, S->dsa_b, 0, S->dsa_b, S->partials, S->counter, S->red);
@@ -1684,7 +1941,7 @@ static cudaError_t dsa_solve(tr_sweep *S, const double *y, double tol) {
     o.precondition = TR_PREC_JACOBI;
     o.relative = 0;
     o.tol = tol * std::sqrt(bb);
-    o.max_iter = 10000;
+    o.max_iter = maxit;
     tr_solve_report rep;
     const tr_status ts = tr_solve(S->dsa, &o, S->dsa_b, S->dsa_f, &rep);
     ++S->dsa_solves;
@@ -1696,27 +1953,34 @@ static cudaError_t dsa_solve(tr_sweep *S, const double *y, double tol) {
     return cudaSuccess;
 }
 // z = base + the correction f on every unknown (k_dsa_prolong)
-static cudaError_t dsa_prolong(tr_sweep *S, const double *base, double *z) {
+static cudaError_t dsa_prolong(tr_sweep *S, const double *base, double *z, bool cluster) {
     const uint64_t n = S->nJ + S->nB;
-    k_dsa_prolong<<<grid_for(S, n), 256, 0, S->stream>>>(S->nT, S->nent, S->nB, S->dsa_aslm, S->cell_p, S->ent_cell,
-                                                         S->lag_keys, S->dsa_f, base, z);
+    k_dsa_prolong<<<grid_for(S, n), 256, 0, S->stream>>>(S->nT, S->nent, S->nB, cluster ? 1u : S->dsa_aslm,
+                                                         S->cell_p, S->ent_cell, S->lag_keys, dsa_f_of(S, cluster),
+                                                         base, z);
     ++S->launches;
     return cudaGetLastError();
 }
+// the diffusion correction of one solve: tolerance, engine and iteration cap
+struct DsaPlan {
+    double tol = 0.0;  // 0: no preconditioning
+    bool cluster = false;
+    int maxit = 10000;
+};
 
 // GMRES(m) on (I - T_prec) x = b, x updated in place (device vectors).
 // Stops at ||b - (I - T) x|| <= rtol * bref (the recursion estimate,
-// confirmed by a true residual at the end of a cycle).  With dsa_tol > 0 it
+// confirmed by a true residual at the end of a cycle).  With dsa.tol > 0 it
 // is right-preconditioned by the diffusion correction P^-1 y = y + C sigma_s y
 // in its flexible form (the inexact inner solve varies from step to step, so
 // the preconditioned basis Z is kept and x += Z y).
 static cudaError_t gmres(tr_sweep *S, int prec, int prec_res, const double *b, double *x, int m, double rtol,
                          double bref, double cycle_tol, int max_it, int *its, double *res_out, int *cycles_out,
-                         double dsa_tol = 0.0) {
+                         const DsaPlan &dsa = DsaPlan()) {
     const uint64_t n = S->nJ + S->nB;
     cudaError_t e = krylov_alloc(S, m);
     if (e != cudaSuccess) return e;
-    const bool flex = dsa_tol > 0.0;
+    const bool flex = dsa.tol > 0.0;
     if (flex && (!S->kz || S->kz_m < m)) {
         if ((e = sw_alloc(S, &S->kz, n * (m + 1))) != cudaSuccess) return e;
         S->kz_m = m;
@@ -1751,8 +2015,8 @@ static cudaError_t gmres(tr_sweep *S, int prec, int prec_res, const double *b, d
             const double *vj = S->kv + static_cast<uint64_t>(j) * n;
             if (flex) {
                 double *zj = S->kz + static_cast<uint64_t>(j) * n;
-                if ((e = dsa_solve(S, vj, dsa_tol)) != cudaSuccess) return e;
-                if ((e = dsa_prolong(S, vj, zj)) != cudaSuccess) return e;
+                if ((e = dsa_solve(S, vj, dsa.tol, dsa.cluster, dsa.maxit)) != cudaSuccess) return e;
+                if ((e = dsa_prolong(S, vj, zj, dsa.cluster)) != cudaSuccess) return e;
                 vj = zj;
             }
             if ((e = op_apply(S, prec, vj, w)) != cudaSuccess) return e;
@@ -2060,6 +2324,143 @@ tr_status tr_sweep_balance(tr_sweep *s, const double *J_in, const double *B_in, 
     return sw_cuda(s, e, "tr_sweep_balance");
 }
 
+// The P1 diffusion matrix on the vertices, assembled per row from the
+// vertex -> cell and vertex -> face tables:
+//   K_uv = sum_c [ sigma_a V (1 + d_uv) / 20 + s_i . s_j / (27 sigma_t V) ]
+//        + sum_f A_f (1 + d_uv) / 24       (vacuum / incident faces)
+// (i, j the local indices of u, v in c; the Marshak term 1/2 int phi v over
+// the face's exact area), stored ELL column-major with its Jacobi inverse;
+// then the largest cluster that can be resident (16 CTAs, else 8).
+static cudaError_t dsa_assemble(tr_sweep *s, const tr_mesh_view *m, const tr_physics_view *ph) {
+    const uint32_t nP = m->nP;
+    const int32_t *bc = ph ? ph->face_bc : nullptr;
+    std::vector<std::vector<std::pair<uint32_t, double>>> rows(nP);
+#pragma omp parallel for schedule(dynamic, 256)
+    for (int64_t vi = 0; vi < static_cast<int64_t>(nP); ++vi) {
+        const uint32_t v = static_cast<uint32_t>(vi);
+        auto &row = rows[v];
+        auto add = [&row](uint32_t u, double a) {
+            for (auto &pr : row)
+                if (pr.first == u) {
+                    pr.second += a;
+                    return;
+                }
+            row.emplace_back(u, a);
+        };
+        for (tr_idx t = m->tetstart[v]; t < m->tetstart[v + 1]; ++t) {
+            const uint32_t c = m->tetidx[t], i = m->tetpos[t];
+            const tr_tetrahedron &T = m->mesh[c];
+            const double sav = (ph && ph->kappa_abs_volume) ? ph->kappa_abs_volume[c] : T.kappa_volume;
+            for (uint32_t j = 0; j < 4; ++j) {
+                const double ss = T.s[i][0] * T.s[j][0] + T.s[i][1] * T.s[j][1] + T.s[i][2] * T.s[j][2];
+                add(T.p[j], sav * (i == j ? 2.0 : 1.0) / 20.0 + ss / (27.0 * T.kappa_volume));
+            }
+        }
+        for (tr_idx t = m->nF ? m->facestart[v] : 0; m->nF && t < m->facestart[v + 1]; ++t) {
+            const tr_idx f = m->faceidx[t];
+            if (bc && bc[f] == TR_BC_REFLECTIVE) continue;
+            const tr_face &F = m->bnd[f];
+            if (F.p[0] >= nP || F.p[1] >= nP || F.p[2] >= nP) continue;  // rejected below
+            const double area = std::sqrt(F.s[0] * F.s[0] + F.s[1] * F.s[1] + F.s[2] * F.s[2]);
+            const uint32_t i = m->facepos[t];
+            for (uint32_t j = 0; j < 3; ++j) add(F.p[j], area * (i == j ? 2.0 : 1.0) / 24.0);
+        }
+    }
+    for (uint32_t f = 0; f < m->nF; ++f)
+        if (m->bnd[f].p[0] >= nP || m->bnd[f].p[1] >= nP || m->bnd[f].p[2] >= nP) return cudaErrorInvalidValue;
+    size_t w = 1;
+    for (const auto &r : rows) w = std::max(w, r.size());
+    std::vector<uint32_t> col(w * nP);
+    std::vector<double> val(w * nP, 0.0), dinv(nP, 0.0);
+    for (uint32_t v = 0; v < nP; ++v) {
+        for (size_t j = 0; j < w; ++j) {
+            col[j * nP + v] = j < rows[v].size() ? rows[v][j].first : v;
+            if (j < rows[v].size()) val[j * nP + v] = rows[v][j].second;
+        }
+        for (const auto &pr : rows[v])
+            if (pr.first == v) dinv[v] = pr.second > 0.0 ? 1.0 / pr.second : 0.0;
+    }
+    cudaError_t e = sw_upload(s, &s->ell_col, col);
+    if (e == cudaSuccess) e = sw_upload(s, &s->ell_val, val);
+    if (e == cudaSuccess) e = sw_upload(s, &s->dsa_dinv, dinv);
+    if (e == cudaSuccess) e = sw_alloc(s, &s->dsa_vec, 5ull * nP);
+    if (e == cudaSuccess) e = sw_alloc(s, &s->dsa_stats, 3);
+    if (e != cudaSuccess) return e;
+    s->ell_w = static_cast<uint32_t>(w);
+    // the largest resident cluster
+    int cluster = 0;
+    cudaFuncSetAttribute(k_dsa_cg, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+    for (int cs : {kDsaMaxCluster, 8}) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(cs);
+        cfg.blockDim = dim3(kDsaThreads);
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = cs;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        int nc = 0;
+        if (cudaOccupancyMaxActiveClusters(&nc, k_dsa_cg, &cfg) == cudaSuccess && nc >= 1) {
+            cluster = cs;
+            break;
+        }
+    }
+    cudaGetLastError();  // clear the error a refused cluster size may have left
+    if (!cluster) return cudaSuccess;
+    // aggregates: kDsaAgg contiguous row blocks of each CTA's rows (the
+    // kernel's dsa_agg_bound), A_c = P^T K P inverted by Gauss-Jordan
+    const uint32_t per = (nP + cluster - 1) / cluster, nc = static_cast<uint32_t>(cluster) * kDsaAgg;
+    std::vector<uint32_t> agg(nP, 0);
+    std::vector<char> used(nc, 0);
+    for (int k = 0; k < cluster; ++k) {
+        const uint32_t r0 = std::min<uint32_t>(nP, k * per), r1 = std::min<uint32_t>(nP, r0 + per);
+        for (int g = 0; g < kDsaAgg; ++g) {
+            const uint32_t g0 = r0 + static_cast<uint32_t>((static_cast<uint64_t>(r1 - r0) * g) / kDsaAgg);
+            const uint32_t g1 = r0 + static_cast<uint32_t>((static_cast<uint64_t>(r1 - r0) * (g + 1)) / kDsaAgg);
+            for (uint32_t i = g0; i < g1; ++i) agg[i] = k * kDsaAgg + g;
+            used[k * kDsaAgg + g] = g1 > g0;
+        }
+    }
+    std::vector<double> A(static_cast<size_t>(nc) * nc, 0.0), X(static_cast<size_t>(nc) * nc, 0.0);
+    for (uint32_t v = 0; v < nP; ++v)
+        for (const auto &pr : rows[v]) A[static_cast<size_t>(agg[v]) * nc + agg[pr.first]] += pr.second;
+    for (uint32_t g = 0; g < nc; ++g) {
+        if (!used[g]) A[static_cast<size_t>(g) * nc + g] = 1.0;
+        X[static_cast<size_t>(g) * nc + g] = 1.0;
+    }
+    for (uint32_t c = 0; c < nc; ++c) {
+        uint32_t piv = c;
+        for (uint32_t r = c + 1; r < nc; ++r)
+            if (std::fabs(A[static_cast<size_t>(r) * nc + c]) > std::fabs(A[static_cast<size_t>(piv) * nc + c])) piv = r;
+        const double d = A[static_cast<size_t>(piv) * nc + c];
+        if (!(std::fabs(d) > 0.0) || !std::isfinite(d)) return cudaSuccess;  // singular: no cluster path
+        if (piv != c)
+            for (uint32_t j = 0; j < nc; ++j) {
+                std::swap(A[static_cast<size_t>(piv) * nc + j], A[static_cast<size_t>(c) * nc + j]);
+                std::swap(X[static_cast<size_t>(piv) * nc + j], X[static_cast<size_t>(c) * nc + j]);
+            }
+        for (uint32_t j = 0; j < nc; ++j) {
+            A[static_cast<size_t>(c) * nc + j] /= d;
+            X[static_cast<size_t>(c) * nc + j] /= d;
+        }
+        for (uint32_t r = 0; r < nc; ++r) {
+            if (r == c) continue;
+            const double f = A[static_cast<size_t>(r) * nc + c];
+            if (f == 0.0) continue;
+            for (uint32_t j = 0; j < nc; ++j) {
+                A[static_cast<size_t>(r) * nc + j] -= f * A[static_cast<size_t>(c) * nc + j];
+                X[static_cast<size_t>(r) * nc + j] -= f * X[static_cast<size_t>(c) * nc + j];
+            }
+        }
+    }
+    e = sw_upload(s, &s->dsa_ainv, X);
+    if (e != cudaSuccess) return e;
+    s->dsa_cluster = cluster;
+    return cudaSuccess;
+}
+
 void tr_sweep_opts_default(tr_sweep_opts *o) {
     if (!o) return;
     o->method = TR_SWEEP_GMRES;
@@ -2070,7 +2471,8 @@ void tr_sweep_opts_default(tr_sweep_opts *o) {
     o->inner_tol = 0.0;
     o->max_outer = 30;
     o->precondition = TR_SWEEP_PREC_NONE;
-    o->precond_tol = 1e-3;
+    o->precond_tol = 1e-2;
+    o->precond_engine = TR_SWEEP_DSA_AUTO;
 }
 
 tr_status tr_sweep_enable_dsa(tr_sweep *s, const tr_mesh_view *mesh, const tr_physics_view *phys) {
@@ -2160,6 +2562,10 @@ tr_status tr_sweep_enable_dsa(tr_sweep *s, const tr_mesh_view *mesh, const tr_ph
         s->dsa = nullptr;
         return sw_cuda(s, e, "tr_sweep_enable_dsa");
     }
+    if (nP <= kDsaClusterMaxRows) {
+        e = dsa_assemble(s, mesh, phys);
+        if (e != cudaSuccess) return sw_cuda(s, e, "tr_sweep_enable_dsa: diffusion matrix");
+    }
     return TR_OK;
 }
 
@@ -2179,7 +2585,19 @@ tr_status tr_sweep_solve(tr_sweep *s, const tr_sweep_opts *opts, double *J, doub
     if (dsa && !s->dsa) return sw_err(s, TR_ERR_INVALID_ARG, "precondition DSA needs tr_sweep_enable_dsa");
     if (dsa && !(o.precond_tol > 0.0 && o.precond_tol < 1.0))
         return sw_err(s, TR_ERR_INVALID_ARG, "precond_tol must be in (0, 1)");
-    const double dsa_tol = dsa ? o.precond_tol : 0.0;
+    DsaPlan plan;
+    if (dsa) {
+        if (o.precond_engine < TR_SWEEP_DSA_AUTO || o.precond_engine > TR_SWEEP_DSA_EVEN_PARITY)
+            return sw_err(s, TR_ERR_INVALID_ARG, "bad precond_engine");
+        if (o.precond_engine == TR_SWEEP_DSA_CLUSTER && !s->dsa_cluster)
+            return sw_err(s, TR_ERR_UNSUPPORTED, "the one-cluster diffusion CG is not available for this sweep");
+        plan.tol = o.precond_tol;
+        plan.cluster = s->dsa_cluster > 0 && o.precond_engine != TR_SWEEP_DSA_EVEN_PARITY;
+    }
+    if (plan.cluster) {
+        cudaError_t e0 = cudaMemsetAsync(s->dsa_stats, 0, 3 * sizeof(unsigned long long), s->stream);
+        if (e0 != cudaSuccess) return sw_cuda(s, e0, "tr_sweep_solve");
+    }
     s->prec_error.clear();
     const uint64_t n = s->nJ + s->nB;
     cudaError_t e = krylov_alloc(s, o.restart);
@@ -2219,8 +2637,8 @@ tr_status tr_sweep_solve(tr_sweep *s, const tr_sweep_opts *opts, double *J, doub
                 }
                 if (dsa) {
                     // x <- S(x) + C sigma_s (S(x) - x): the diffusion estimate of the error
-                    if ((e = dsa_solve(s, s->kx, dsa_tol)) != cudaSuccess) break;
-                    e = dsa_prolong(s, s->kt, s->kx);
+                    if ((e = dsa_solve(s, s->kx, plan.tol, plan.cluster, plan.maxit)) != cudaSuccess) break;
+                    e = dsa_prolong(s, s->kt, s->kx, plan.cluster);
                 } else {
                     e = cudaMemcpyAsync(s->kx, s->kt, n * 8, cudaMemcpyDeviceToDevice, st);
                 }
@@ -2231,7 +2649,7 @@ tr_status tr_sweep_solve(tr_sweep *s, const tr_sweep_opts *opts, double *J, doub
                 }
             }
         } else if (o.mode == TR_MODE_FP64) {
-            e = gmres(s, 64, 64, s->kb, s->kx, o.restart, o.tol, bn, 0.0, o.max_iter, &its, &res, nullptr, dsa_tol);
+            e = gmres(s, 64, 64, s->kb, s->kx, o.restart, o.tol, bn, 0.0, o.max_iter, &its, &res, nullptr, plan);
             conv = e == cudaSuccess && res <= o.tol;
         } else {
             // FP32 sweeps inside FP64 defect correction: each GMRES cycle starts
@@ -2240,7 +2658,7 @@ tr_status tr_sweep_solve(tr_sweep *s, const tr_sweep_opts *opts, double *J, doub
             // to x in FP64.  A cycle ends at its restart length, at the target,
             // or (inner_tol > 0) once it has reduced its residual by inner_tol.
             e = gmres(s, 32, 64, s->kb, s->kx, o.restart, o.tol, bn, o.inner_tol, o.max_iter, &its, &res, &outer,
-                      dsa_tol);
+                      plan);
             conv = e == cudaSuccess && res <= o.tol;
         }
     }
@@ -2253,6 +2671,14 @@ tr_status tr_sweep_solve(tr_sweep *s, const tr_sweep_opts *opts, double *J, doub
         return sw_err(s, TR_ERR_CUDA, "tr_sweep_solve: " + s->prec_error);
     }
     if (e != cudaSuccess) return sw_cuda(s, e, "tr_sweep_solve");
+    if (plan.cluster) {
+        unsigned long long st3[3] = {0, 0, 0};
+        e = cudaMemcpy(st3, s->dsa_stats, sizeof(st3), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return sw_cuda(s, e, "tr_sweep_solve");
+        s->dsa_iterations += static_cast<int64_t>(st3[0]);
+        s->dsa_solves += static_cast<int64_t>(st3[1]);
+        if (st3[2]) return sw_err(s, TR_ERR_NAN, "tr_sweep_solve: diffusion CG produced a non-finite residual");
+    }
     if (rep) {
         float ms = 0.0f;
         cudaEventElapsedTime(&ms, s->ev[0], s->ev[1]);
