@@ -60,8 +60,14 @@ def test_single_sweep_fp64_matches_oracle(cuda, which):
         assert rel_err(host(S.psi()), psio) < 1e-12
 
 
-def test_single_sweep_fp32_matches_oracle(cuda):
-    md, ph, S, O = pair(scattering_box(), op.ordinates_product(4, 8))
+@pytest.mark.parametrize("n,polar,azim", [((5, 4, 6), 4, 8), ((5, 4, 6), 10, 16), ((8, 8, 8), 10, 16)])
+def test_single_sweep_fp32_matches_oracle(cuda, n, polar, azim):
+    """32 ordinates: one block per SM; 160 (more than the SMs): the small
+    shared-memory shape with two blocks per SM and a ring of 1,024 positions,
+    so on the 8^3 box (3,072 cells) upwind traces also come from global psi.
+    (On the tangled cube FP32 differs from the oracle by up to 1e-4 with any
+    shape: its inverted elements make some 4x4 systems ill-conditioned.)"""
+    md, ph, S, O = pair(scattering_box(n=n), op.ordinates_product(polar, azim))
     rng = np.random.default_rng(4)
     Jin, Bin = rng.random((md.nT, 4)), rng.random(S.n_extra)
     Jg, Bg = S.apply(dev(Jin), dev(Bin), precision=32)
@@ -153,6 +159,27 @@ def test_dsa_gmres_matches_oracle(cuda, engine):
     assert r1.iterations < r0.iterations / 2, (r1.iterations, r0.iterations)
     assert rel_err(host(J1), Jo) < 1e-8 and rel_err(host(B1), Bo) < 1e-8
     assert r0.precond_solves == 0
+
+
+@pytest.mark.parametrize("which", ["tangled_cube", "scattering_box"])
+def test_dsa_with_lagged_and_incident_faces(cuda, which):
+    """The correction also reaches lagged inflows (cut dependency cycles)
+    and leaves the fixed point unchanged with incident and reflective faces."""
+    case = tangled_cube() if which == "tangled_cube" else scattering_box(albedo=0.95)
+    md, ph = case
+    ords = op.ordinates_product(4, 8)
+    S = tr.Sweep(0, md, ords, ph, dsa=True)
+    if which == "tangled_cube":
+        assert S.n_lag > 0
+    O = op.SweepOracle(md, ords, kappa_abs_volume=ph.kappa_abs_volume, face_bc=ph.face_bc,
+                       face_incident=ph.face_incident)
+    Jo, Bo, info = O.solve(method=1, tol=1e-12)
+    for mode in (tr.TR_MODE_FP64, tr.TR_MODE_MIXED):
+        J, B, rep = S.solve(mode=mode, tol=1e-11 if mode == tr.TR_MODE_FP64 else 1e-9,
+                            precondition=tr._lib.TR_SWEEP_PREC_DSA, precond_tol=1e-4)
+        assert rep.converged and rep.precond_solves > 0
+        tol = 1e-9 if mode == tr.TR_MODE_FP64 else 1e-6
+        assert rel_err(host(J), Jo) < tol and rel_err(host(B), Bo) < tol
 
 
 def test_dsa_engines_agree(cuda):

@@ -371,15 +371,22 @@ struct Slots {
         }
     }
 };
-// level pointers of the block's ordinate, staged in shared memory when
-// there are at most kLevelCap levels (else read from global memory)
-constexpr uint32_t kLevelCap = 4096;
-template <typename T>
-constexpr int ring_bytes() { return sizeof(T) == 4 ? 64 * 1024 : 32 * 1024; }
+// Shared-memory shape of a sweep block: the ring of recent psi by position,
+// the staging slots and the level pointers of its ordinate (staged when
+// there are at most level_cap levels, else read from global memory).  The
+// full shape (FP32 154 KB, FP64 187 KB) fits one block per SM; the small
+// FP32 shape (16 KiB ring, 1024 staged levels: 94 KB) fits two, for sets of
+// more ordinates than SMs.  Measured (FP32, one sweep): Milne slab, 112
+// ordinates, 1.40 ms full / 1.58 ms small; stellar sphere, 308 ordinates,
+// 190 ms full / 142 ms small.
 template <typename T>
 constexpr size_t slots_bytes() { return static_cast<size_t>(Slots<T>::kUnits) * kSlots * 16; }
-template <typename T>
-constexpr size_t sweep_smem() { return ring_bytes<T>() + slots_bytes<T>() + 4ull * (kLevelCap + 1); }
+template <typename T, bool SMALL>
+struct SweepShape {
+    static constexpr int ring_bytes = SMALL ? 16 * 1024 : (sizeof(T) == 4 ? 64 * 1024 : 32 * 1024);
+    static constexpr uint32_t level_cap = SMALL ? 1024 : 4096;
+    static constexpr size_t smem = ring_bytes + slots_bytes<T>() + 4ull * (level_cap + 1);
+};
 
 __device__ __forceinline__ void cp_async16(void *dst, const void *src) {
     const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
@@ -538,21 +545,22 @@ __device__ __forceinline__ void solve4(const T (&a)[4][4], const T (&r)[4], T (&
     for (int i = 0; i < 4; ++i) x[i] = (b[i][0] * r[0] + b[i][1] * r[1] + b[i][2] * r[2] + b[i][3] * r[3]) * inv;
 }
 
-template <typename T>
+template <typename T, bool SMALL>
 __global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, SweepArgs<T> a) {
     using V = typename Vec4<T>::type;
     using Sl = Slots<T>;
+    using Shape = SweepShape<T, SMALL>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    constexpr uint32_t R = ring_bytes<T>() / sizeof(V);
+    constexpr uint32_t R = Shape::ring_bytes / sizeof(V);
     V *ring = reinterpret_cast<V *>(smem_raw);
-    const Slots<T> SL{smem_raw + ring_bytes<T>()};
+    const Slots<T> SL{smem_raw + Shape::ring_bytes};
     const uint32_t q = blockIdx.x, nT = a.nT;
     const T ox = a.ox[q], oy = a.oy[q], oz = a.oz[q];
     const uint4 *task = sc.task + (size_t)q * nT;
     const uint32_t nl = sc.nlev[q];
     const uint32_t *lvl = sc.lvl + (size_t)q * sc.lstride;
-    if (nl <= kLevelCap) {
-        uint32_t *lv = reinterpret_cast<uint32_t *>(smem_raw + ring_bytes<T>() + slots_bytes<T>());
+    if (nl <= Shape::level_cap) {
+        uint32_t *lv = reinterpret_cast<uint32_t *>(smem_raw + Shape::ring_bytes + slots_bytes<T>());
         for (uint32_t L = threadIdx.x; L <= nl; L += blockDim.x) lv[L] = __ldg(lvl + L);
         __syncthreads();
         lvl = lv;
@@ -767,7 +775,12 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], 
         : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
-constexpr int kMomWarps = 4;
+constexpr int kMomWarps = 8;
+constexpr int kMomDepth = 4;  // k-steps of 8 ordinates whose psi loads are in flight together
+// Persistent: the block stages the split weights once, then each warp takes
+// 16-row tiles of psi (rows = cell vertices, columns = ordinates) in a
+// grid-stride loop and runs kMomDepth k-steps per round, all their loads
+// issued before the first product.
 __global__ void __launch_bounds__(32 * kMomWarps) k_moments_tf32x3(uint32_t M, uint32_t nq, uint32_t nqp,
                                                                   const double *W, const float *psi, int nmom,
                                                                   double *mom) {
@@ -781,43 +794,55 @@ __global__ void __launch_bounds__(32 * kMomWarps) k_moments_tf32x3(uint32_t M, u
     }
     __syncthreads();
     const uint32_t lane = threadIdx.x & 31u, g = lane >> 2, t = lane & 3u;
-    const uint64_t r0 = (static_cast<uint64_t>(blockIdx.x) * kMomWarps + (threadIdx.x >> 5)) * 16;
-    if (r0 >= M) return;
-    const bool ok0 = r0 + g < M, ok1 = r0 + g + 8 < M;
-    float d[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
-    for (uint32_t k0 = 0; k0 < nq; k0 += 8) {
-        const uint32_t ka = k0 + t, kb = k0 + t + 4;
-        float av[4];
-        av[0] = (ka < nq && ok0) ? __ldg(psi + static_cast<uint64_t>(ka) * M + r0 + g) : 0.0f;
-        av[1] = (ka < nq && ok1) ? __ldg(psi + static_cast<uint64_t>(ka) * M + r0 + g + 8) : 0.0f;
-        av[2] = (kb < nq && ok0) ? __ldg(psi + static_cast<uint64_t>(kb) * M + r0 + g) : 0.0f;
-        av[3] = (kb < nq && ok1) ? __ldg(psi + static_cast<uint64_t>(kb) * M + r0 + g + 8) : 0.0f;
-        uint32_t ahi[4], alo[4];
+    const uint64_t tiles = (M + 15) / 16, stride = static_cast<uint64_t>(gridDim.x) * kMomWarps;
+    for (uint64_t tile = static_cast<uint64_t>(blockIdx.x) * kMomWarps + (threadIdx.x >> 5); tile < tiles;
+         tile += stride) {
+        const uint64_t r0 = tile * 16;
+        const bool ok0 = r0 + g < M, ok1 = r0 + g + 8 < M;
+        float d[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+        for (uint32_t kk = 0; kk < nq; kk += 8 * kMomDepth) {
+            float av[kMomDepth][4];
 #pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            ahi[i] = to_tf32(av[i]);
-            alo[i] = to_tf32(av[i] - __uint_as_float(ahi[i]));
+            for (int s = 0; s < kMomDepth; ++s) {
+                const uint32_t ka = kk + 8 * s + t, kb = ka + 4;
+                av[s][0] = (ka < nq && ok0) ? __ldg(psi + static_cast<uint64_t>(ka) * M + r0 + g) : 0.0f;
+                av[s][1] = (ka < nq && ok1) ? __ldg(psi + static_cast<uint64_t>(ka) * M + r0 + g + 8) : 0.0f;
+                av[s][2] = (kb < nq && ok0) ? __ldg(psi + static_cast<uint64_t>(kb) * M + r0 + g) : 0.0f;
+                av[s][3] = (kb < nq && ok1) ? __ldg(psi + static_cast<uint64_t>(kb) * M + r0 + g + 8) : 0.0f;
+            }
+#pragma unroll
+            for (int s = 0; s < kMomDepth; ++s) {
+                const uint32_t k0 = kk + 8 * s;
+                if (k0 >= nq) break;  // warp-uniform
+                const uint32_t ka = k0 + t, kb = k0 + t + 4;
+                uint32_t ahi[4], alo[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    ahi[i] = to_tf32(av[s][i]);
+                    alo[i] = to_tf32(av[s][i] - __uint_as_float(ahi[i]));
+                }
+#pragma unroll
+                for (int nt = 0; nt < 2; ++nt) {
+                    const uint32_t n = nt * 8 + g;
+                    const uint32_t bh0 = wsh[n * nqp + ka], bh1 = wsh[n * nqp + kb];
+                    const uint32_t bl0 = wsh[16 * nqp + n * nqp + ka], bl1 = wsh[16 * nqp + n * nqp + kb];
+                    mma_tf32(d[nt], alo, bh0, bh1);   // small products first
+                    mma_tf32(d[nt], ahi, bl0, bl1);
+                    mma_tf32(d[nt], ahi, bh0, bh1);
+                }
+            }
         }
 #pragma unroll
         for (int nt = 0; nt < 2; ++nt) {
-            const uint32_t n = nt * 8 + g;
-            const uint32_t bh0 = wsh[n * nqp + ka], bh1 = wsh[n * nqp + kb];
-            const uint32_t bl0 = wsh[16 * nqp + n * nqp + ka], bl1 = wsh[16 * nqp + n * nqp + kb];
-            mma_tf32(d[nt], alo, bh0, bh1);   // small products first
-            mma_tf32(d[nt], ahi, bl0, bl1);
-            mma_tf32(d[nt], ahi, bh0, bh1);
-        }
-    }
-#pragma unroll
-    for (int nt = 0; nt < 2; ++nt) {
-        const int n0 = nt * 8 + 2 * static_cast<int>(t);
-        if (ok0) {
-            if (n0 < nmom) mom[static_cast<uint64_t>(n0) * M + r0 + g] = d[nt][0];
-            if (n0 + 1 < nmom) mom[static_cast<uint64_t>(n0 + 1) * M + r0 + g] = d[nt][1];
-        }
-        if (ok1) {
-            if (n0 < nmom) mom[static_cast<uint64_t>(n0) * M + r0 + g + 8] = d[nt][2];
-            if (n0 + 1 < nmom) mom[static_cast<uint64_t>(n0 + 1) * M + r0 + g + 8] = d[nt][3];
+            const int n0 = nt * 8 + 2 * static_cast<int>(t);
+            if (ok0) {
+                if (n0 < nmom) mom[static_cast<uint64_t>(n0) * M + r0 + g] = d[nt][0];
+                if (n0 + 1 < nmom) mom[static_cast<uint64_t>(n0 + 1) * M + r0 + g] = d[nt][1];
+            }
+            if (ok1) {
+                if (n0 < nmom) mom[static_cast<uint64_t>(n0) * M + r0 + g + 8] = d[nt][2];
+                if (n0 + 1 < nmom) mom[static_cast<uint64_t>(n0 + 1) * M + r0 + g + 8] = d[nt][3];
+            }
         }
     }
 }
@@ -1713,11 +1738,14 @@ static tr_status sweep_setup(tr_sweep *S, const tr_mesh_view *m, const tr_physic
     if (e == cudaSuccess) e = sw_alloc(S, &S->counter, 4);
     if (e == cudaSuccess) e = cudaMemset(S->counter, 0, 16);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_sweep<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(sweep_smem<double>()));
+        e = cudaFuncSetAttribute(k_sweep<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(SweepShape<double, false>::smem));
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(k_sweep<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 static_cast<int>(sweep_smem<float>()));
+        e = cudaFuncSetAttribute(k_sweep<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(SweepShape<float, false>::smem));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_sweep<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(SweepShape<float, true>::smem));
     if (e == cudaSuccess) e = cudaEventCreate(&S->ev[0]);
     if (e == cudaSuccess) e = cudaEventCreate(&S->ev[1]);
     if (e != cudaSuccess) return sw_cuda(S, e, "sweep: allocation");
@@ -1786,7 +1814,14 @@ static cudaError_t sweep_launch(tr_sweep *S, const T *J, const T *Bin, int with_
     a.psi = psi;
     a.with_ext = with_ext;
     a.lag_base = 4ull * S->nent;
-    k_sweep<T><<<S->nq, kSweepThreads, sweep_smem<T>(), st>>>(geom_of<T>(S), sc, a);
+    bool two_per_sm = false;  // FP32 with more ordinates than SMs: the small shape
+    if constexpr (sizeof(T) == 4) {
+        two_per_sm = S->nq > static_cast<uint32_t>(S->num_sms);
+        if (two_per_sm)
+            k_sweep<T, true><<<S->nq, kSweepThreads, SweepShape<T, true>::smem, st>>>(geom_of<T>(S), sc, a);
+    }
+    if (!two_per_sm)
+        k_sweep<T, false><<<S->nq, kSweepThreads, SweepShape<T, false>::smem, st>>>(geom_of<T>(S), sc, a);
     ++S->launches;
     if (Bout && S->nent) {
         k_reflect_out<T><<<grid_for(S, S->nent), 256, 0, st>>>(S->nT, S->nent, S->ent_cell, S->ent_qout, psi, Bout);
@@ -2249,8 +2284,13 @@ tr_status tr_sweep_moments(tr_sweep *s, int nmom, double *mom) {
     if (s->last_prec == 32 && 2ull * 16 * nqp8 * sizeof(uint32_t) <= 48 * 1024) {  // nq <= 384
         const uint32_t M = 4 * s->nT, nqp = nqp8;
         const uint64_t warps = (M + 15) / 16;
-        const int blocks = static_cast<int>((warps + kMomWarps - 1) / kMomWarps);
         const size_t smem = 2ull * 16 * nqp * sizeof(uint32_t);
+        // persistent grid: as many blocks as are resident (at most one tile per warp)
+        int per_sm = 1;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_moments_tf32x3, 32 * kMomWarps, smem);
+        const uint64_t want = (warps + kMomWarps - 1) / kMomWarps;
+        const int blocks = static_cast<int>(
+            std::max<uint64_t>(1, std::min<uint64_t>(want, static_cast<uint64_t>(std::max(per_sm, 1)) * s->num_sms)));
         k_moments_tf32x3<<<blocks, 32 * kMomWarps, smem, s->stream>>>(M, s->nq, nqp, s->Wm, s->psi32, nmom, mom);
         e = cudaGetLastError();
         ++s->launches;

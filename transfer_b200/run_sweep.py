@@ -1,12 +1,16 @@
-"""Command-line runner of the discrete-ordinates sweep on the Milne slab
-(used to profile the sweep kernel and the accelerated solve)."""
+"""Command-line runner of the discrete-ordinates sweep on the Milne slab or
+the stellar sphere (used to profile the sweep kernel, the moments
+contraction and the accelerated solve)."""
 def _main():
-    """python -m transfer_b200.run_sweep [--precision 32|64] [--sweeps N]
-    [--solve none|gmres|dsa] [--tol T]: N sweeps of the Milne slab
-    (workloads.milne_sweep) with a scattering source and the mean device time
-    of one sweep; with --solve, one GMRES solve to FP64 relative residual T in
-    the given precision (64: FP64, 32: mixed), plain or with the diffusion
-    synthetic acceleration."""
+    """python -m transfer_b200.run_sweep [--workload milne|stellar[:n]]
+    [--precision 32|64] [--sweeps N] [--moments K] [--solve none|gmres|dsa]
+    [--tol T]: N sweeps of the workload (workloads.milne_sweep, or
+    workloads.stellar_sphere with n^3 grid cells, default 96) with a
+    scattering source and the mean device time of one sweep; --moments: K
+    launches of the l <= 3 moment contraction of the last sweep's psi, timed
+    with CUDA events; with --solve, one GMRES solve to FP64 relative residual
+    T in the given precision (64: FP64, 32: mixed), plain or with the
+    diffusion synthetic acceleration."""
     import argparse
 
     import torch
@@ -19,8 +23,14 @@ def _main():
     ap.add_argument("--sweeps", type=int, default=3)
     ap.add_argument("--solve", default="none", choices=("none", "gmres", "dsa"))
     ap.add_argument("--tol", type=float, default=1e-8)
+    ap.add_argument("--workload", default="milne")
+    ap.add_argument("--moments", type=int, default=0)
     args = ap.parse_args()
-    md, ph, ords, desc = W.milne_sweep()
+    if args.workload.startswith("stellar"):
+        n = int(args.workload.split(":")[1]) if ":" in args.workload else 96
+        md, ph, ords, desc = W.stellar_sphere(n=n)
+    else:
+        md, ph, ords, desc = W.milne_sweep()
     S = Sweep(0, md, ords, ph, dsa=args.solve == "dsa")
     J = torch.rand(4 * S.nT, dtype=torch.float64, device="cuda:0")
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -31,6 +41,21 @@ def _main():
     torch.cuda.synchronize()
     print(f"{desc['workload']}: nT {S.nT}, nq {S.nq}, {S.max_levels} levels; FP{args.precision} sweep "
           f"{e0.elapsed_time(e1) / max(args.sweeps, 1):.3f} ms (host-timed, includes the API call)")
+    if args.moments:
+        from ._lib import lib
+        out = torch.zeros(16 * 4 * S.nT, dtype=torch.float64, device="cuda:0")
+        S._c(lib.tr_sweep_moments(S._h, 16, out.data_ptr()))
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(args.moments):
+            S._c(lib.tr_sweep_moments(S._h, 16, out.data_ptr()))
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.moments
+        rb = 4 if args.precision == 32 else 8
+        byt = S.nq * S.nT * 4 * rb + 16 * S.nT * 4 * 8
+        print(f"moments l<=3 of FP{args.precision} psi: {ms:.3f} ms per launch (API call included), "
+              f"{byt / (ms * 1e-3) / 1e9:.0f} GB/s algorithmic (psi read once, 16 FP64 moments written)")
     if args.solve != "none":
         mode = L.TR_MODE_FP64 if args.precision == 64 else L.TR_MODE_MIXED
         prec = L.TR_SWEEP_PREC_DSA if args.solve == "dsa" else L.TR_SWEEP_PREC_NONE

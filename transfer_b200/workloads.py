@@ -16,6 +16,8 @@ generated, seeded).
                Ip = 1 in a 0.05-radius ball at (0.2, 0.5, 0.5), maxk = 5
                (l <= 10; 194-point precision).
 Each returns (MeshData, AngularData, Physics or None, description dict).
+The sweep's problems (milne_sweep, stellar_sphere) return (MeshData,
+Physics, ordinates, description dict).
 """
 import numpy as np
 
@@ -98,6 +100,36 @@ def milne_sweep(n=(8, 8, 160), depth=20.0, albedo=0.999, incident=1.0, n_polar=8
                 ordinates=f"{n_polar}x{n_azim} Gauss-Legendre x azimuth product set ({n_polar * n_azim})",
                 physics=f"sigma_t=1, isotropic scattering albedo {albedo:g}, reflective x/y, vacuum z=0, "
                         f"isotropic inflow I={incident:g} at z={depth:g}")
+    return md, phys, ords, desc
+
+
+def stellar_sphere(n=96, n_polar=14, n_azim=22):
+    """The stellar sphere for the discrete-ordinates sweep: a Kuhn grid of
+    n^3 hexahedra on [-1,1]^3 (jitter +-0.2h) clipped to the tets whose
+    centroid lies in r <= 1 (2,779,622 tets for n = 96), absorption
+    kappa(r) = 10 (1 - r^2) + 0.1 and isotropic scattering sigma_s = 0.5 kappa
+    per tet (sigma_t = 1.5 kappa, albedo 1/3), source B(r) = (1 - r^2)^4,
+    vacuum surface.  Ordinates: 14 Gauss-Legendre cosines x 22 azimuths =
+    308 directions, the mirror-symmetric product set nearest the 302-point
+    Lebedev set (Lebedev rules are generated up to 194 points here).
+    Returns (MeshData, Physics, ordinates, description)."""
+    from .sweep import ordinates_product
+    base = MeshData.kuhn((n, n, n), box=(-1.0, 1.0, -1.0, 1.0, -1.0, 1.0), jitter=0.2, seed=SEED,
+                         kappa=[0.0, 1.0], Ip=[0.0, 0.0], ball=(0.0, 0.0, 0.0, 1.0))
+    tets = base.mesh["p"]
+    cent = base.coords[tets.astype(np.int64)].mean(axis=1)
+    r2 = np.minimum((cent ** 2).sum(axis=1), 1.0)
+    kappa = 10.0 * (1.0 - r2) + 0.1
+    nT = len(tets)
+    md = MeshData.from_tets(base.coords, tets, np.arange(1, nT + 1, dtype=np.int32),
+                            np.concatenate([[0.0], 1.5 * kappa]), np.concatenate([[0.0], (1.0 - r2) ** 4]),
+                            albedo=np.concatenate([[0.0], np.full(nT, 1.0 / 3.0)]))
+    phys = Physics(kappa_abs_volume=md.kappa_abs_volume)
+    ords = ordinates_product(n_polar, n_azim)
+    desc = dict(workload="stellar_sphere", mesh=f"{n}^3 Kuhn grid on [-1,1]^3 clipped to r<=1 ({nT} tets), "
+                                                "jitter 0.2h",
+                ordinates=f"{n_polar}x{n_azim} Gauss-Legendre x azimuth product set ({n_polar * n_azim})",
+                physics="kappa=10(1-r^2)+0.1, sigma_s=0.5 kappa, B=(1-r^2)^4, vacuum surface")
     return md, phys, ords, desc
 
 
