@@ -775,77 +775,128 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], 
         : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
+// The block stages psi through shared memory in stages of kMomK ordinates x
+// kMomRows rows (cell vertices), copied with 16-byte cp.async so that each
+// ordinate's rows are read as whole 1 KB runs, kMomStages stages in
+// flight; each warp then builds its MMA fragments (two 16-row tiles sharing
+// each B fragment) from the stage
+// (row stride padded to kMomRows + 8 words: the fragment reads hit 32
+// distinct banks).  Persistent: the block stages the split weights once and
+// walks row tiles tile = blockIdx.x, + gridDim.x, ...
 constexpr int kMomWarps = 8;
-constexpr int kMomDepth = 4;  // k-steps of 8 ordinates whose psi loads are in flight together
-// Persistent: the block stages the split weights once, then each warp takes
-// 16-row tiles of psi (rows = cell vertices, columns = ordinates) in a
-// grid-stride loop and runs kMomDepth k-steps per round, all their loads
-// issued before the first product.
+constexpr int kMomMT = 2;                          // 16-row MMA tiles per warp
+constexpr int kMomRows = 16 * kMomMT * kMomWarps;  // 256 rows per tile: 1 KB runs per ordinate
+constexpr int kMomK = 16;                          // ordinates per stage
+constexpr int kMomStride = kMomRows + 8;
+constexpr int kMomStages = 4;
+constexpr size_t kMomStageWords = static_cast<size_t>(kMomK) * kMomStride;
+__device__ __forceinline__ void cp_async16_zfill(void *dst, const void *src, bool valid) {
+    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
+    const int n = valid ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src), "r"(n));
+}
 __global__ void __launch_bounds__(32 * kMomWarps) k_moments_tf32x3(uint32_t M, uint32_t nq, uint32_t nqp,
                                                                   const double *W, const float *psi, int nmom,
                                                                   double *mom) {
-    extern __shared__ uint32_t wsh[];  // [2][16][nqp]: hi, lo
-    for (uint32_t i = threadIdx.x; i < 16 * nqp; i += blockDim.x) {
-        const uint32_t n = i / nqp, q = i % nqp;
-        const float w = q < nq ? static_cast<float>(W[static_cast<size_t>(n) * nq + q]) : 0.0f;
+    // split weights in B-fragment order: for k-step ks and lane (g, t) eight
+    // words {hi, hi, lo, lo} at ordinates 8 ks + t, + 4 for moment g, then the
+    // same for moment 8 + g -- two 16-byte loads per lane and k-step
+    extern __shared__ __align__(16) uint32_t wsh[];  // [nqp / 8][32][8]; then the psi stages
+    float *stage = reinterpret_cast<float *>(wsh + 32 * nqp);
+    for (uint32_t i = threadIdx.x; i < 32 * nqp; i += blockDim.x) {
+        const uint32_t ks = i / 256, ln = (i / 8) % 32, j = i % 8;
+        const uint32_t n = (j < 4 ? 0u : 8u) + (ln >> 2), kq = 8 * ks + (ln & 3u) + ((j & 1u) ? 4u : 0u);
+        const float w = kq < nq ? static_cast<float>(W[static_cast<size_t>(n) * nq + kq]) : 0.0f;
         const uint32_t hi = to_tf32(w);
-        wsh[i] = hi;
-        wsh[16 * nqp + i] = to_tf32(w - __uint_as_float(hi));
+        wsh[i] = (j & 2u) ? to_tf32(w - __uint_as_float(hi)) : hi;
     }
-    __syncthreads();
-    const uint32_t lane = threadIdx.x & 31u, g = lane >> 2, t = lane & 3u;
-    const uint64_t tiles = (M + 15) / 16, stride = static_cast<uint64_t>(gridDim.x) * kMomWarps;
-    for (uint64_t tile = static_cast<uint64_t>(blockIdx.x) * kMomWarps + (threadIdx.x >> 5); tile < tiles;
-         tile += stride) {
-        const uint64_t r0 = tile * 16;
-        const bool ok0 = r0 + g < M, ok1 = r0 + g + 8 < M;
-        float d[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
-        for (uint32_t kk = 0; kk < nq; kk += 8 * kMomDepth) {
-            float av[kMomDepth][4];
-#pragma unroll
-            for (int s = 0; s < kMomDepth; ++s) {
-                const uint32_t ka = kk + 8 * s + t, kb = ka + 4;
-                av[s][0] = (ka < nq && ok0) ? __ldg(psi + static_cast<uint64_t>(ka) * M + r0 + g) : 0.0f;
-                av[s][1] = (ka < nq && ok1) ? __ldg(psi + static_cast<uint64_t>(ka) * M + r0 + g + 8) : 0.0f;
-                av[s][2] = (kb < nq && ok0) ? __ldg(psi + static_cast<uint64_t>(kb) * M + r0 + g) : 0.0f;
-                av[s][3] = (kb < nq && ok1) ? __ldg(psi + static_cast<uint64_t>(kb) * M + r0 + g + 8) : 0.0f;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, g = lane >> 2, t = lane & 3u;
+    const uint32_t tiles = (M + kMomRows - 1) / kMomRows, nch = (nq + kMomK - 1) / kMomK;
+    const uint32_t my_tiles = blockIdx.x < tiles ? (tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    const uint64_t total = static_cast<uint64_t>(my_tiles) * nch;  // (tile, chunk) stages of this block
+    // stage s -> row tile and ordinate chunk
+    auto issue = [&](uint64_t s) {
+        if (s < total) {
+            const uint64_t r0 = static_cast<uint64_t>(blockIdx.x + (s / nch) * gridDim.x) * kMomRows;
+            const uint32_t k0 = static_cast<uint32_t>(s % nch) * kMomK;
+            float *dst = stage + (s % kMomStages) * kMomStageWords;
+            for (uint32_t j = threadIdx.x; j < kMomK * (kMomRows / 4); j += blockDim.x) {
+                const uint32_t k = j / (kMomRows / 4), rq = j % (kMomRows / 4);
+                const uint64_t row = r0 + 4 * rq;
+                const bool ok = k0 + k < nq && row < M;
+                const float *src = ok ? psi + static_cast<uint64_t>(k0 + k) * M + row : psi;
+                cp_async16_zfill(dst + k * kMomStride + 4 * rq, src, ok);
             }
+        }
+        cp_async_commit();  // one group per stage, empty past the end
+    };
+    for (int s = 0; s < kMomStages - 1; ++s) issue(s);
+    float d[kMomMT][2][4];
 #pragma unroll
-            for (int s = 0; s < kMomDepth; ++s) {
-                const uint32_t k0 = kk + 8 * s;
-                if (k0 >= nq) break;  // warp-uniform
-                const uint32_t ka = k0 + t, kb = k0 + t + 4;
+    for (int mt = 0; mt < kMomMT; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt) d[mt][nt][0] = d[mt][nt][1] = d[mt][nt][2] = d[mt][nt][3] = 0.f;
+    for (uint64_t s = 0; s < total; ++s) {
+        cp_async_wait<kMomStages - 2>();
+        __syncthreads();  // stage s visible to all; stage s - 1 no longer read (also the weights, s = 0)
+        issue(s + kMomStages - 1);
+        const float *sm = stage + (s % kMomStages) * kMomStageWords;
+        const uint32_t k0 = static_cast<uint32_t>(s % nch) * kMomK, rw = 16 * kMomMT * warp;
+#pragma unroll
+        for (int ks = 0; ks < kMomK / 8; ++ks) {
+            const uint32_t kg = k0 + 8 * ks;
+            if (kg >= nq) break;  // block-uniform
+            const uint32_t kl = 8 * ks + t;
+            const uint4 *wf = reinterpret_cast<const uint4 *>(wsh) + ((kg / 8) * 32 + lane) * 2;
+            const uint4 b0 = wf[0], b1 = wf[1];  // hi, hi, lo, lo of moments g and 8 + g
+#pragma unroll
+            for (int mt = 0; mt < kMomMT; ++mt) {
+                const uint32_t rr = rw + 16 * mt + g;
+                float av[4];
+                av[0] = sm[kl * kMomStride + rr];
+                av[1] = sm[kl * kMomStride + rr + 8];
+                av[2] = sm[(kl + 4) * kMomStride + rr];
+                av[3] = sm[(kl + 4) * kMomStride + rr + 8];
                 uint32_t ahi[4], alo[4];
 #pragma unroll
                 for (int i = 0; i < 4; ++i) {
-                    ahi[i] = to_tf32(av[s][i]);
-                    alo[i] = to_tf32(av[s][i] - __uint_as_float(ahi[i]));
+                    ahi[i] = to_tf32(av[i]);
+                    alo[i] = to_tf32(av[i] - __uint_as_float(ahi[i]));
                 }
-#pragma unroll
-                for (int nt = 0; nt < 2; ++nt) {
-                    const uint32_t n = nt * 8 + g;
-                    const uint32_t bh0 = wsh[n * nqp + ka], bh1 = wsh[n * nqp + kb];
-                    const uint32_t bl0 = wsh[16 * nqp + n * nqp + ka], bl1 = wsh[16 * nqp + n * nqp + kb];
-                    mma_tf32(d[nt], alo, bh0, bh1);   // small products first
-                    mma_tf32(d[nt], ahi, bl0, bl1);
-                    mma_tf32(d[nt], ahi, bh0, bh1);
-                }
+                mma_tf32(d[mt][0], alo, b0.x, b0.y);  // small products first
+                mma_tf32(d[mt][0], ahi, b0.z, b0.w);
+                mma_tf32(d[mt][0], ahi, b0.x, b0.y);
+                mma_tf32(d[mt][1], alo, b1.x, b1.y);
+                mma_tf32(d[mt][1], ahi, b1.z, b1.w);
+                mma_tf32(d[mt][1], ahi, b1.x, b1.y);
             }
         }
+        if (s % nch == nch - 1) {  // last chunk of the tile: write its 16 moments, start the next
 #pragma unroll
-        for (int nt = 0; nt < 2; ++nt) {
-            const int n0 = nt * 8 + 2 * static_cast<int>(t);
-            if (ok0) {
-                if (n0 < nmom) mom[static_cast<uint64_t>(n0) * M + r0 + g] = d[nt][0];
-                if (n0 + 1 < nmom) mom[static_cast<uint64_t>(n0 + 1) * M + r0 + g] = d[nt][1];
-            }
-            if (ok1) {
-                if (n0 < nmom) mom[static_cast<uint64_t>(n0) * M + r0 + g + 8] = d[nt][2];
-                if (n0 + 1 < nmom) mom[static_cast<uint64_t>(n0 + 1) * M + r0 + g + 8] = d[nt][3];
+            for (int mt = 0; mt < kMomMT; ++mt) {
+                const uint64_t r0 =
+                    static_cast<uint64_t>(blockIdx.x + (s / nch) * gridDim.x) * kMomRows + rw + 16 * mt;
+                const bool ok0 = r0 + g < M, ok1 = r0 + g + 8 < M;
+#pragma unroll
+                for (int nt = 0; nt < 2; ++nt) {
+                    const int n0 = nt * 8 + 2 * static_cast<int>(t);
+                    if (ok0) {
+                        if (n0 < nmom) mom[static_cast<uint64_t>(n0) * M + r0 + g] = d[mt][nt][0];
+                        if (n0 + 1 < nmom) mom[static_cast<uint64_t>(n0 + 1) * M + r0 + g] = d[mt][nt][1];
+                    }
+                    if (ok1) {
+                        if (n0 < nmom) mom[static_cast<uint64_t>(n0) * M + r0 + g + 8] = d[mt][nt][2];
+                        if (n0 + 1 < nmom) mom[static_cast<uint64_t>(n0 + 1) * M + r0 + g + 8] = d[mt][nt][3];
+                    }
+                    d[mt][nt][0] = d[mt][nt][1] = d[mt][nt][2] = d[mt][nt][3] = 0.f;
+                }
             }
         }
     }
+    cp_async_wait<0>();
 }
+// shared memory of k_moments_tf32x3 for nqp (multiple of 8) ordinates
+inline size_t moments_smem(uint32_t nqp) { return 32ull * nqp * 4 + kMomStages * kMomStageWords * 4; }
 
 // Adjoint gradient of a boundary functional F (outflow through a set of
 // faces).  With mu_q the adjoint angular flux (the sweep in the reversed
@@ -1359,6 +1410,7 @@ struct tr_sweep {
     std::string prec_error;
     std::vector<void *> allocs;
     int64_t sweeps32 = 0, sweeps64 = 0, launches = 0;
+    bool mom_attr = false;         // k_moments_tf32x3 shared-memory opt-in done
 };
 
 static tr_status sw_err(tr_sweep *s, tr_status st, const std::string &m) {
@@ -2283,12 +2335,17 @@ tr_status tr_sweep_moments(tr_sweep *s, int nmom, double *mom) {
     const uint32_t nqp8 = (s->nq + 7) / 8 * 8;
     if (s->last_prec == 32 && 2ull * 16 * nqp8 * sizeof(uint32_t) <= 48 * 1024) {  // nq <= 384
         const uint32_t M = 4 * s->nT, nqp = nqp8;
-        const uint64_t warps = (M + 15) / 16;
-        const size_t smem = 2ull * 16 * nqp * sizeof(uint32_t);
-        // persistent grid: as many blocks as are resident (at most one tile per warp)
+        const size_t smem = moments_smem(nqp);
+        if (!s->mom_attr) {  // above 48 KB of dynamic shared memory: opt in once
+            e = cudaFuncSetAttribute(k_moments_tf32x3, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(moments_smem(384)));
+            if (e != cudaSuccess) return sw_cuda(s, e, "tr_sweep_moments");
+            s->mom_attr = true;
+        }
+        // persistent grid: as many blocks as are resident, at most one per row tile
         int per_sm = 1;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_moments_tf32x3, 32 * kMomWarps, smem);
-        const uint64_t want = (warps + kMomWarps - 1) / kMomWarps;
+        const uint64_t want = (M + kMomRows - 1) / kMomRows;
         const int blocks = static_cast<int>(
             std::max<uint64_t>(1, std::min<uint64_t>(want, static_cast<uint64_t>(std::max(per_sm, 1)) * s->num_sms)));
         k_moments_tf32x3<<<blocks, 32 * kMomWarps, smem, s->stream>>>(M, s->nq, nqp, s->Wm, s->psi32, nmom, mom);
