@@ -440,6 +440,14 @@ tr_status tr_sweep_solve(tr_sweep *s, const tr_sweep_opts *opts, double *J, doub
  * tables of the mesh view are used): an even-parity context with l = 0 on
  * the same device, with the reflective faces left out of its face list. */
 tr_status tr_sweep_enable_dsa(tr_sweep *s, const tr_mesh_view *mesh, const tr_physics_view *phys);
+/* Replaces the per-cell coefficients (HOST arrays [nT]: sigma_t V, sigma_a V
+ * (NULL: sigma_a = sigma_t), Planck intensity B (NULL: kept)) without
+ * rebuilding geometry or schedule, which depend on neither -- for parameter
+ * studies and gradient steps.  The diffusion operator of
+ * tr_sweep_enable_dsa keeps the coefficients it was built with (it only
+ * preconditions; solves stay exact). */
+tr_status tr_sweep_set_coefficients(tr_sweep *s, const double *kappa_volume, const double *kappa_abs_volume,
+                                    const double *I_p);
 /* Outflow of the last sweep through the boundary faces with face_mask[f]
  * != 0 (HOST array [nF]): F = sum_q w_q sum_f max(Omega_q.s_f, 0) mean_f psi_q
  * (mean intensity x area), FP64. */

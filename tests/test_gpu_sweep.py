@@ -228,6 +228,31 @@ def test_dsa_needs_enable(cuda):
         S2.solve(precondition=tr._lib.TR_SWEEP_PREC_DSA, precond_engine=5)
 
 
+def test_set_coefficients_matches_the_oracle(cuda):
+    """New sigma_t V, sigma_a V and B on an existing sweep (geometry and
+    schedule kept) give the oracle's solution for those coefficients."""
+    md, ph = scattering_box()
+    ords = op.ordinates_product(4, 8)
+    S = tr.Sweep(0, md, ords, ph)
+    rng = np.random.default_rng(9)
+    kv = md.mesh["kappa_volume"] * rng.uniform(0.5, 2.0, md.nT)
+    ka = kv * rng.uniform(0.2, 1.0, md.nT)
+    Ip = rng.uniform(0.0, 1.0, md.nT)
+    S.set_coefficients(kv, ka, Ip)
+    mesh = md.mesh.copy()
+    mesh["kappa_volume"] = kv
+    mesh["I_p"] = Ip
+    md2 = tr.MeshData.from_arrays(tetstart=md.tetstart, tetidx=md.tetidx, tetpos=md.tetpos, facestart=md.facestart,
+                                  faceidx=md.faceidx, facepos=md.facepos, mesh=mesh, bnd=md.bnd, coords=md.coords,
+                                  regions=md.regions, kappa_abs_volume=ka, face_side=md.face_side)
+    O = op.SweepOracle(md2, ords, kappa_abs_volume=ka, face_bc=ph.face_bc, face_incident=ph.face_incident)
+    J, B, rep = S.solve(tol=1e-11)
+    Jo, Bo, info = O.solve(method=1, tol=1e-11)
+    assert rep.converged and rel_err(host(J), Jo) < 1e-9 and rel_err(host(B), Bo) < 1e-9
+    with pytest.raises(tr.TransferError):
+        S.set_coefficients(kv, kv * 2.0)   # sigma_a > sigma_t
+
+
 def test_absorbing_slab_matches_e2_on_gpu(cuda):
     md, ph = absorbing_slab(nx=80, ny=4, nz=4)
     S = tr.Sweep(0, md, tr.ordinates_product(16, 16), ph)

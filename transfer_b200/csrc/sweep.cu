@@ -48,6 +48,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/transfer_b200.h"
@@ -2793,6 +2794,68 @@ tr_status tr_sweep_solve(tr_sweep *s, const tr_sweep_opts *opts, double *J, doub
     }
     if (!conv) return sw_err(s, TR_ERR_NOT_CONVERGED, "tr_sweep_solve: not converged");
     return TR_OK;
+}
+
+// coefficient records [nT][4]: sigma_t V, sigma_s V, sigma_a V B / 4 (the
+// vertex map in the fourth word is kept)
+__global__ void k_set_coef(uint32_t nT, const double *stv, const double *ssv, const double *ext, double *coef64,
+                           float *coef32) {
+    for (uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < nT; c += gridDim.x * blockDim.x) {
+        coef64[4ull * c] = stv[c];
+        coef64[4ull * c + 1] = ssv[c];
+        coef64[4ull * c + 2] = ext[c];
+        coef32[4ull * c] = static_cast<float>(stv[c]);
+        coef32[4ull * c + 1] = static_cast<float>(ssv[c]);
+        coef32[4ull * c + 2] = static_cast<float>(ext[c]);
+    }
+}
+
+tr_status tr_sweep_set_coefficients(tr_sweep *s, const double *kappa_volume, const double *kappa_abs_volume,
+                                    const double *I_p) {
+    SW_CHECK(s);
+    if (!kappa_volume) return sw_err(s, TR_ERR_INVALID_ARG, "tr_sweep_set_coefficients: null kappa_volume");
+    const uint32_t nT = s->nT;
+    cudaSetDevice(s->device);
+    std::vector<double> bpl(nT), stv(nT), ssv(nT), ext(nT);
+    cudaError_t e = cudaSuccess;
+    if (I_p) std::copy(I_p, I_p + nT, bpl.begin());
+    else e = cudaMemcpy(bpl.data(), s->B64, sizeof(double) * nT, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return sw_cuda(s, e, "tr_sweep_set_coefficients");
+    for (uint32_t c = 0; c < nT; ++c) {
+        const double kv = kappa_volume[c], sav = kappa_abs_volume ? kappa_abs_volume[c] : kv;
+        if (!(kv > 0.0) || !(sav >= 0.0) || sav > kv * (1.0 + 1e-12))
+            return sw_err(s, TR_ERR_INVALID_ARG,
+                          "tr_sweep_set_coefficients: need kappa_volume > 0 and 0 <= sigma_a V <= sigma_t V");
+        stv[c] = kv;
+        ssv[c] = kv - sav;
+        ext[c] = sav * bpl[c] / 4.0;
+    }
+    auto up = [&](auto *dst, const std::vector<double> &v) {
+        using D = std::remove_pointer_t<decltype(dst)>;
+        if (e != cudaSuccess) return;
+        if constexpr (std::is_same_v<D, double>) {
+            e = cudaMemcpy(dst, v.data(), sizeof(double) * nT, cudaMemcpyHostToDevice);
+        } else {
+            std::vector<float> f(v.begin(), v.end());
+            e = cudaMemcpy(dst, f.data(), sizeof(float) * nT, cudaMemcpyHostToDevice);
+        }
+    };
+    cudaStreamSynchronize(s->stream);  // nothing in flight reads the old values
+    up(s->stv64, stv);
+    up(s->ssv64, ssv);
+    up(s->ext64, ext);
+    up(s->stv32, stv);
+    up(s->ssv32, ssv);
+    up(s->ext32, ext);
+    if (I_p) up(s->B64, bpl);
+    if (e == cudaSuccess) {
+        k_set_coef<<<grid_for(s, nT), 256, 0, s->stream>>>(nT, s->stv64, s->ssv64, s->ext64, s->coef64, s->coef32);
+        ++s->launches;
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    s->last_prec = 0;  // psi of the last sweep belongs to the old coefficients
+    return sw_cuda(s, e, "tr_sweep_set_coefficients");
 }
 
 tr_status tr_sweep_outflow(tr_sweep *s, const int32_t *face_mask, double *F) {

@@ -26,6 +26,17 @@ def ordinates_product(n_polar, n_azim):
     return x, y, z, w
 
 
+def lebedev(mindegree):
+    """LebedevQuad(mindegree) as an ordinate set (x, y, z, w), weights summing
+    to 1 (rules up to 194 points are generated)."""
+    n = lib.tr_lebedev(int(mindegree), None, None, None, None, 0)
+    if n < 0:
+        raise ValueError(f"no Lebedev rule of degree {mindegree} is generated")
+    x, y, z, w = (np.zeros(n) for _ in range(4))
+    lib.tr_lebedev(int(mindegree), _ptr(x), _ptr(y), _ptr(z), _ptr(w), n)
+    return x, y, z, w
+
+
 class SweepReport(dict):
     __getattr__ = dict.__getitem__
 
@@ -117,6 +128,13 @@ class Sweep:
         if st != L.TR_OK and (raise_on_error or st != L.TR_ERR_NOT_CONVERGED):
             self._c(st)
         return J.view(self.nT, 4), B[:self.n_extra], report
+
+    def set_coefficients(self, kappa_volume, kappa_abs_volume=None, I_p=None):
+        """Per-cell sigma_t V, sigma_a V (None: no scattering) and Planck
+        intensity (None: kept), host arrays [nT]; geometry and schedule stay."""
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+                for a in (kappa_volume, kappa_abs_volume, I_p)]
+        self._c(lib.tr_sweep_set_coefficients(self._h, *(_ptr(a) for a in arrs)))
 
     def outflow(self, face_mask):
         """Outflow of the last sweep through the faces with face_mask != 0."""

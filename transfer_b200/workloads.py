@@ -133,6 +133,35 @@ def stellar_sphere(n=96, n_polar=14, n_azim=22):
     return md, phys, ords, desc
 
 
+def cube64_sweep(n=64, albedo=0.3, degree=23):
+    """The adjoint-gradient problem for the discrete-ordinates sweep: the
+    cube64 mesh (n^3 Kuhn cube, jitter +-0.2h; 1,572,864 tets for n = 64)
+    with sigma_t = exp(0.5 g) per tet (g the unit Gaussian random field of
+    cube64), scattering albedo 0.3, B = 1 in the 0.05-radius ball at
+    (0.2, 0.5, 0.5), vacuum faces; the 194-point Lebedev set (degree 23).
+    The functional is the outflow through the faces at x = 1 (face_mask).
+    Returns (MeshData, Physics, ordinates, face_mask, description)."""
+    from .sweep import lebedev
+    base = MeshData.kuhn((n, n, n), jitter=0.2, seed=SEED, kappa=[0.0, 1.0], Ip=[0.0, 0.0])
+    tets = base.mesh["p"]
+    cent = base.coords[tets.astype(np.int64)].mean(axis=1)
+    sigma_t = np.exp(0.5 * gaussian_random_field(cent))
+    hot = ((cent - np.array([0.2, 0.5, 0.5])) ** 2).sum(axis=1) < 0.05 ** 2
+    nT = len(tets)
+    md = MeshData.from_tets(base.coords, tets, np.arange(1, nT + 1, dtype=np.int32),
+                            np.concatenate([[0.0], sigma_t]), np.concatenate([[0.0], hot.astype(np.float64)]),
+                            albedo=np.concatenate([[0.0], np.full(nT, float(albedo))]))
+    phys = Physics(kappa_abs_volume=md.kappa_abs_volume)
+    ords = lebedev(degree)
+    fx = md.coords[md.bnd["p"][:, :3].astype(np.int64)][..., 0]
+    mask = (fx.min(axis=1) > 1.0 - 1e-9).astype(np.int32)   # faces on x = 1
+    desc = dict(workload="cube64_sweep", mesh=f"{n}^3 Kuhn cube, jitter 0.2h ({nT} tets)",
+                ordinates=f"Lebedev degree {degree} ({len(ords[3])} points)",
+                physics=f"sigma_t=exp(0.5 GRF(l=0.1)) per tet, albedo {albedo:g}, B=1 in r<0.05 at (0.2,0.5,0.5), "
+                        "vacuum", functional="outflow through x = 1")
+    return md, phys, ords, mask, desc
+
+
 def sweep_work(nT, nq, real_bytes=4):
     """Algorithmic (compulsory) work of one sweep of all ordinates: per
     (cell, ordinate) the 16-byte task record is read and psi (4 reals)
