@@ -228,6 +228,24 @@ def test_dsa_needs_enable(cuda):
         S2.solve(precondition=tr._lib.TR_SWEEP_PREC_DSA, precond_engine=5)
 
 
+def test_stellar_sphere_sweep_matches_oracle(cuda):
+    """Configuration 3's shape at a small size (curved vacuum surface, per-tet
+    coefficients, albedo 1/3): one FP64 and one FP32 sweep and the solve."""
+    from transfer_b200 import workloads as W
+    md, ph, _, _ = W.stellar_sphere(n=10, n_polar=4, n_azim=8)
+    md_, ph_, S, O = pair((md, ph), op.ordinates_product(4, 8))
+    rng = np.random.default_rng(12)
+    Jin = rng.random((md.nT, 4))
+    J64, _ = S.apply(dev(Jin), None, precision=64)
+    Jo, _ = O.apply(Jin, None)
+    assert rel_err(host(J64), Jo) < 1e-12
+    J32, _ = S.apply(dev(Jin), None, precision=32)
+    assert rel_err(host(J32), Jo) < 2e-5
+    J, B, rep = S.solve(tol=1e-11)
+    Js, Bs, info = O.solve(method=1, tol=1e-11)
+    assert rep.converged and rel_err(host(J), Js) < 1e-9
+
+
 def test_set_coefficients_matches_the_oracle(cuda):
     """New sigma_t V, sigma_a V and B on an existing sweep (geometry and
     schedule kept) give the oracle's solution for those coefficients."""

@@ -3,6 +3,8 @@
 import importlib.util
 import os
 
+import numpy as np
+
 import transfer_b200 as tr
 from transfer_b200 import workloads as W
 
@@ -31,3 +33,19 @@ def test_bench_module_imports():
     bench = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(bench)
     assert callable(bench.sweep_section) and callable(bench.run_ours) and callable(bench.run_reference)
+
+
+def test_sweep_workloads_at_small_sizes():
+    """The stellar sphere and the cube64 sweep problem, built small: the ball
+    keeps only tets inside r <= 1, coefficients follow the stated profiles,
+    the functional covers the x = 1 faces, the 194-point set sums to 1."""
+    from transfer_b200 import workloads as W
+    md, ph, ords, desc = W.stellar_sphere(n=8, n_polar=2, n_azim=4)
+    cent = md.coords[md.mesh["p"].astype(np.int64)].mean(axis=1)
+    assert (np.linalg.norm(cent, axis=1) <= 1.0 + 1e-12).all() and len(ords[3]) == 8
+    ratio = np.asarray(ph.kappa_abs_volume) / md.mesh["kappa_volume"]
+    assert np.allclose(ratio, 2.0 / 3.0)
+    md, ph, ords, mask, desc = W.cube64_sweep(n=6)
+    assert len(ords[3]) == 194 and abs(ords[3].sum() - 1.0) < 1e-12
+    fx = md.coords[md.bnd["p"][:, :3].astype(np.int64)][..., 0]
+    assert mask.sum() == 2 * 6 * 6 and (fx[mask.astype(bool)] > 1 - 1e-9).all()
