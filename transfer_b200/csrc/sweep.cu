@@ -377,9 +377,10 @@ struct Slots {
 // there are at most level_cap levels, else read from global memory).  The
 // full shape (FP32 154 KB, FP64 187 KB) fits one block per SM; the small
 // FP32 shape (16 KiB ring, 1024 staged levels: 94 KB) fits two, for sets of
-// more ordinates than SMs.  Measured (FP32, one sweep): Milne slab, 112
-// ordinates, 1.40 ms full / 1.58 ms small; stellar sphere, 308 ordinates,
-// 190 ms full / 142 ms small.
+// more ordinates than SMs.  Measured (FP32, one sweep, before the staging of
+// upwind traces older than the ring): Milne slab, 112 ordinates, 1.40 ms
+// full / 1.58 ms small; stellar sphere, 308 ordinates, 190 ms full / 142 ms
+// small.
 template <typename T>
 constexpr size_t slots_bytes() { return static_cast<size_t>(Slots<T>::kUnits) * kSlots * 16; }
 template <typename T, bool SMALL>
@@ -403,10 +404,15 @@ template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N)); }
 
 // fills the slot of position p (record, normals, source, coefficients and
-// the inflow values of non-interior faces, zeros where there are none)
-template <typename T>
+// the inflow values of non-interior faces, zeros where there are none).  An
+// interior inflow whose upwind position is already done (< done_end) but
+// will have left the ring of R positions when p's chunk (ending at e_next)
+// runs gets the upwind cell's psi staged too, from global psi (OLD: the
+// shapes whose ring is short enough for that to happen often).
+template <typename T, bool OLD>
 __device__ __forceinline__ void stage_task(const Slots<T> &S, uint32_t p, const uint4 *task, const Geom<T> &g,
-                                           const SweepArgs<T> &a) {
+                                           const SweepArgs<T> &a, uint32_t done_end, uint32_t e_next, uint32_t R,
+                                           const T *psi) {
     using Sl = Slots<T>;
     const uint32_t sl = p % kSlots;
     const uint4 rec = __ldg(task + p);
@@ -438,6 +444,8 @@ __device__ __forceinline__ void stage_task(const Slots<T> &S, uint32_t p, const 
                 src = g.finc + idx;
                 bcast = true;
             }
+        } else if (OLD && code < done_end && code + R < e_next) {
+            src = psi + 4 * (size_t)__ldg(g.nbr + 4 * (size_t)c + k);  // the upwind cell, in its vertex order
         } else {
             ++t;
             continue;
@@ -473,13 +481,14 @@ __device__ __forceinline__ bool next_chunk(uint32_t &L, uint32_t &c0, const uint
 }
 
 // stages the chunk [c0, min(c0 + 256, end of level L)) from threads shifted
-// by half a block
-template <typename T>
+// by half a block, while positions below done_end are complete
+template <typename T, bool OLD>
 __device__ __forceinline__ void stage_chunk(const Slots<T> &S, uint32_t L, uint32_t c0, const uint32_t *lvl,
-                                            const uint4 *task, const Geom<T> &g, const SweepArgs<T> &a) {
+                                            const uint4 *task, const Geom<T> &g, const SweepArgs<T> &a,
+                                            uint32_t done_end, uint32_t R, const T *psi) {
     const uint32_t e = min(c0 + kSweepThreads, lvl[L + 1]);
     const uint32_t p = c0 + ((threadIdx.x + kSweepThreads / 2) % kSweepThreads);
-    if (p < e) stage_task<T>(S, p, task, g, a);
+    if (p < e) stage_task<T, OLD>(S, p, task, g, a, done_end, e, R, psi);
     cp_async_commit();
 }
 
@@ -553,6 +562,9 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, Sw
     using Shape = SweepShape<T, SMALL>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr uint32_t R = Shape::ring_bytes / sizeof(V);
+    // stage upwind traces older than the ring (FP64 and the small shape: a
+    // ring of 1,024 positions; the full FP32 ring of 4,096 rarely misses)
+    constexpr bool kOld = sizeof(T) == 8 || SMALL;
     V *ring = reinterpret_cast<V *>(smem_raw);
     const Slots<T> SL{smem_raw + Shape::ring_bytes};
     const uint32_t q = blockIdx.x, nT = a.nT;
@@ -571,14 +583,15 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, Sw
     const T c12 = T(1) / T(12), c20 = T(1) / T(20);
 
     uint32_t L = 0, c0 = lvl[0];
-    stage_chunk<T>(SL, L, c0, lvl, task, g, a);
+    uint32_t prev_c0 = 0;  // positions below it were complete when this chunk was staged
+    stage_chunk<T, kOld>(SL, L, c0, lvl, task, g, a, prev_c0, R, psi);
     cp_async_wait<0>();
     __syncthreads();
     for (;;) {
         const uint32_t e0 = min(c0 + kSweepThreads, lvl[L + 1]);  // this chunk is [c0, e0)
         uint32_t nL = L, nc0 = c0;
         const bool more = next_chunk(nL, nc0, lvl, nl);
-        if (more) stage_chunk<T>(SL, nL, nc0, lvl, task, g, a);
+        if (more) stage_chunk<T, kOld>(SL, nL, nc0, lvl, task, g, a, c0, R, psi);
         const uint32_t p = c0 + threadIdx.x;
         if (p < e0) {
             const uint32_t sl = p % kSlots;
@@ -625,6 +638,16 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, Sw
                         const T *src = ring_s + 4 * (size_t)(code % R);
 #pragma unroll
                         for (int j = 0; j < 4; ++j) up[j] = src[(mp >> (2 * (4 * k + j))) & 3u];
+                    } else if (kOld && code < prev_c0) {  // older than the ring, staged with the slot
+                        T upc[4];
+                        SL.template load<4>(sl, Sl::kBv + t * (4 / Sl::kR), upc);
+                        V v;  // selects below, not a dynamically indexed array
+                        v.x = upc[0];
+                        v.y = upc[1];
+                        v.z = upc[2];
+                        v.w = upc[3];
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) up[j] = comp<T>(v, (mp >> (2 * (4 * k + j))) & 3u);
                     } else {                      // older than the ring: global psi
                         const T *src = psi + 4 * (size_t)__ldg(g.nbr + 4 * (size_t)c + k);
 #pragma unroll
@@ -670,6 +693,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, Sw
         __syncthreads();
         if (!more) break;
         L = nL;
+        prev_c0 = c0;
         c0 = nc0;
     }
 }
