@@ -417,6 +417,14 @@ tr_status tr_sweep_levels(tr_sweep *s, int32_t *level);
  * result; B_out: the resulting reflective / lagged inflow (either NULL). */
 tr_status tr_sweep_apply(tr_sweep *s, int precision, const double *J_in, const double *B_in, int with_ext,
                          double *J_out, double *B_out);
+/* tr_sweep_apply for n independent problems (distinct sweeps on one device,
+ * of any sizes and ordinate sets) in ONE launch of the sweep kernel, one
+ * block per (problem, ordinate); per-problem arrays of device pointers (an
+ * array pointer NULL = none for all).  Results equal n separate
+ * tr_sweep_apply calls. */
+tr_status tr_sweep_apply_batch(int n, tr_sweep *const *s, int precision, const double *const *J_in,
+                               const double *const *B_in, int with_ext, double *const *J_out,
+                               double *const *B_out);
 /* psi of the last sweep as FP64, device [nq][nT][4]. */
 tr_status tr_sweep_psi(tr_sweep *s, double *psi);
 /* Angular moments of the last sweep's psi: mom[m][nT][4] = sum_q w_q

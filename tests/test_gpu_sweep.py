@@ -246,6 +246,23 @@ def test_stellar_sphere_sweep_matches_oracle(cuda):
     assert rep.converged and rel_err(host(J), Js) < 1e-9
 
 
+@pytest.mark.parametrize("precision", [64, 32])
+def test_batched_sweep_equals_separate_sweeps(cuda, precision):
+    """Problems of different sizes, ordinate sets, boundary kinds (reflective
+    inflow, cut cycles) in one launch give exactly the separate sweeps."""
+    cases = [(scattering_box(), op.ordinates_product(4, 8)), (tangled_cube(), op.ordinates_product(2, 6)),
+             (absorbing_slab(nx=20), op.ordinates_product(6, 12)), (scattering_box(n=(8, 8, 8)), tr.lebedev(17))]
+    sweeps = [tr.Sweep(0, md, ords, ph) for (md, ph), ords in cases]
+    rng = np.random.default_rng(21)
+    Js = [dev(rng.random(4 * S.nT)) for S in sweeps]
+    Bs = [dev(rng.random(max(S.n_extra, 1))) for S in sweeps]
+    out = tr.sweep_apply_batch(sweeps, precision, Js, Bs)
+    for S, J, B, (Jb, Bb) in zip(sweeps, Js, Bs, out):
+        Jo, Bo = S.apply(J, B if S.n_extra else None, precision=precision)
+        assert torch.equal(Jb, Jo) and torch.equal(Bb, Bo)
+    assert sum(S.nq for S in sweeps) > 148   # the batch ran the two-per-SM shape in FP32
+
+
 def test_set_coefficients_matches_the_oracle(cuda):
     """New sigma_t V, sigma_a V and B on an existing sweep (geometry and
     schedule kept) give the oracle's solution for those coefficients."""

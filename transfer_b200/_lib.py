@@ -204,6 +204,7 @@ PROTOTYPES = [
     ("tr_sweep_solve", S, [P, C.POINTER(tr_sweep_opts), P, P, C.POINTER(tr_sweep_report)]),
     ("tr_sweep_enable_dsa", S, [P, C.POINTER(tr_mesh_view), C.POINTER(tr_physics_view)]),
     ("tr_sweep_set_coefficients", S, [P, P, P, P]),
+    ("tr_sweep_apply_batch", S, [I, P, I, P, P, I, P, P]),
     ("tr_sweep_outflow", S, [P, P, C.POINTER(D)]),
     ("tr_sweep_gradient", S, [P, P, I, P, P, P, P, P]),
     ("tr_sweep_bench", S, [P, I, I, C.POINTER(D)]),

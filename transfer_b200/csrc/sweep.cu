@@ -555,8 +555,10 @@ __device__ __forceinline__ void solve4(const T (&a)[4][4], const T (&r)[4], T (&
     for (int i = 0; i < 4; ++i) x[i] = (b[i][0] * r[0] + b[i][1] * r[1] + b[i][2] * r[2] + b[i][3] * r[3]) * inv;
 }
 
+// one ordinate q of one problem: the body of k_sweep and k_sweep_batch
 template <typename T, bool SMALL>
-__global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, SweepArgs<T> a) {
+__device__ __forceinline__ void sweep_block(const Geom<T> &g, const Sched &sc, const SweepArgs<T> &a,
+                                            const uint32_t q) {
     using V = typename Vec4<T>::type;
     using Sl = Slots<T>;
     using Shape = SweepShape<T, SMALL>;
@@ -567,7 +569,7 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, Sw
     constexpr bool kOld = sizeof(T) == 8 || SMALL;
     V *ring = reinterpret_cast<V *>(smem_raw);
     const Slots<T> SL{smem_raw + Shape::ring_bytes};
-    const uint32_t q = blockIdx.x, nT = a.nT;
+    const uint32_t nT = a.nT;
     const T ox = a.ox[q], oy = a.oy[q], oz = a.oz[q];
     const uint4 *task = sc.task + (size_t)q * nT;
     const uint32_t nl = sc.nlev[q];
@@ -696,6 +698,31 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, Sw
         prev_c0 = c0;
         c0 = nc0;
     }
+}
+template <typename T, bool SMALL>
+__global__ void __launch_bounds__(kSweepThreads) k_sweep(Geom<T> g, Sched sc, SweepArgs<T> a) {
+    sweep_block<T, SMALL>(g, sc, a, blockIdx.x);
+}
+// several problems in one launch: job j owns blocks [block0, block0 + nq)
+template <typename T>
+struct SweepJob {
+    Geom<T> g;
+    Sched sc;
+    SweepArgs<T> a;
+    uint32_t block0;
+};
+template <typename T, bool SMALL>
+__global__ void __launch_bounds__(kSweepThreads) k_sweep_batch(const SweepJob<T> *__restrict__ jobs, int njobs) {
+    int lo = 0, hi = njobs - 1;  // the last job with block0 <= blockIdx.x
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) / 2;
+        if (jobs[mid].block0 <= blockIdx.x) lo = mid;
+        else hi = mid - 1;
+    }
+    const Geom<T> g = jobs[lo].g;
+    const Sched sc = jobs[lo].sc;
+    const SweepArgs<T> a = jobs[lo].a;
+    sweep_block<T, SMALL>(g, sc, a, blockIdx.x - jobs[lo].block0);
 }
 
 // B_out of the reflective faces: the inflow of each (face, incoming q)
@@ -1823,6 +1850,15 @@ static tr_status sweep_setup(tr_sweep *S, const tr_mesh_view *m, const tr_physic
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_sweep<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(SweepShape<float, true>::smem));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_sweep_batch<double, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(SweepShape<double, false>::smem));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_sweep_batch<float, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(SweepShape<float, false>::smem));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_sweep_batch<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 static_cast<int>(SweepShape<float, true>::smem));
     if (e == cudaSuccess) e = cudaEventCreate(&S->ev[0]);
     if (e == cudaSuccess) e = cudaEventCreate(&S->ev[1]);
     if (e != cudaSuccess) return sw_cuda(S, e, "sweep: allocation");
@@ -1868,12 +1904,13 @@ static Geom<T> geom_of(const tr_sweep *S) {
     return g;
 }
 
-// Queues one sweep: J_in, B_in FP64 (null = 0) -> J_out, B_out FP64 (null = skip).
+// The launch arguments of one sweep of S from J, Bin (precision T, null = 0) into psi.
 template <typename T>
-static cudaError_t sweep_launch(tr_sweep *S, const T *J, const T *Bin, int with_ext, T *psi, T *Bout) {
-    cudaStream_t st = S->stream;
-    Sched sc{S->task, S->lvl, S->nlev, S->lstride, S->f4_keys, S->f4_codes, S->n_f4};
-    SweepArgs<T> a;
+static SweepJob<T> make_job(tr_sweep *S, const T *J, const T *Bin, int with_ext, T *psi) {
+    SweepJob<T> j;
+    j.g = geom_of<T>(S);
+    j.sc = Sched{S->task, S->lvl, S->nlev, S->lstride, S->f4_keys, S->f4_codes, S->n_f4};
+    SweepArgs<T> &a = j.a;
     a.nT = S->nT;
     a.nq = S->nq;
     if constexpr (sizeof(T) == 8) {
@@ -1891,24 +1928,35 @@ static cudaError_t sweep_launch(tr_sweep *S, const T *J, const T *Bin, int with_
     a.psi = psi;
     a.with_ext = with_ext;
     a.lag_base = 4ull * S->nent;
-    bool two_per_sm = false;  // FP32 with more ordinates than SMs: the small shape
-    if constexpr (sizeof(T) == 4) {
-        two_per_sm = S->nq > static_cast<uint32_t>(S->num_sms);
-        if (two_per_sm)
-            k_sweep<T, true><<<S->nq, kSweepThreads, SweepShape<T, true>::smem, st>>>(geom_of<T>(S), sc, a);
-    }
-    if (!two_per_sm)
-        k_sweep<T, false><<<S->nq, kSweepThreads, SweepShape<T, false>::smem, st>>>(geom_of<T>(S), sc, a);
-    ++S->launches;
+    j.block0 = 0;
+    return j;
+}
+// reflective and lagged outflow of the sweep in psi into Bout (null = skip), on st
+template <typename T>
+static void sweep_outflow_b(tr_sweep *S, cudaStream_t st, const T *psi, T *Bout) {
     if (Bout && S->nent) {
         k_reflect_out<T><<<grid_for(S, S->nent), 256, 0, st>>>(S->nT, S->nent, S->ent_cell, S->ent_qout, psi, Bout);
         ++S->launches;
     }
     if (Bout && S->nlag) {
         k_lag_out<T><<<grid_for(S, S->nlag), 256, 0, st>>>(S->nT, S->nlag, S->lag_keys, S->nbr, S->map, psi,
-                                                          Bout + a.lag_base);
+                                                          Bout + 4ull * S->nent);
         ++S->launches;
     }
+}
+// Queues one sweep: J_in, B_in FP64 (null = 0) -> J_out, B_out FP64 (null = skip).
+template <typename T>
+static cudaError_t sweep_launch(tr_sweep *S, const T *J, const T *Bin, int with_ext, T *psi, T *Bout) {
+    cudaStream_t st = S->stream;
+    const SweepJob<T> j = make_job<T>(S, J, Bin, with_ext, psi);
+    bool two_per_sm = false;  // FP32 with more ordinates than SMs: the small shape
+    if constexpr (sizeof(T) == 4) {
+        two_per_sm = S->nq > static_cast<uint32_t>(S->num_sms);
+        if (two_per_sm) k_sweep<T, true><<<S->nq, kSweepThreads, SweepShape<T, true>::smem, st>>>(j.g, j.sc, j.a);
+    }
+    if (!two_per_sm) k_sweep<T, false><<<S->nq, kSweepThreads, SweepShape<T, false>::smem, st>>>(j.g, j.sc, j.a);
+    ++S->launches;
+    sweep_outflow_b<T>(S, st, psi, Bout);
     return cudaGetLastError();
 }
 
@@ -2200,6 +2248,67 @@ static cudaError_t gmres(tr_sweep *S, int prec, int prec_res, const double *b, d
     return cudaSuccess;
 }
 
+// One launch of k_sweep_batch over every problem's ordinates, each problem's
+// conversions and reductions before and after it on the same stream.
+template <typename T>
+static cudaError_t batch_sweep(int n, tr_sweep *const *s, cudaStream_t st, const double *const *J_in,
+                               const double *const *B_in, int with_ext, double *const *J_out,
+                               double *const *B_out) {
+    std::vector<SweepJob<T>> jobs(n);
+    uint32_t blocks = 0;
+    for (int i = 0; i < n; ++i) {
+        tr_sweep *S = s[i];
+        const double *Ji = J_in ? J_in[i] : nullptr;
+        const double *Bi = (B_in && S->nB) ? B_in[i] : nullptr;
+        if constexpr (sizeof(T) == 8) {
+            jobs[i] = make_job<T>(S, Ji, Bi, with_ext, S->psi64);
+        } else {
+            if (Ji) {
+                k_to_f32<<<grid_for(S, S->nJ), 256, 0, st>>>(S->nJ, Ji, S->J32);
+                ++S->launches;
+            }
+            if (Bi) {
+                k_to_f32<<<grid_for(S, S->nB), 256, 0, st>>>(S->nB, Bi, S->Bi32);
+                ++S->launches;
+            }
+            jobs[i] = make_job<T>(S, Ji ? S->J32 : nullptr, Bi ? S->Bi32 : nullptr, with_ext, S->psi32);
+        }
+        jobs[i].block0 = blocks;
+        blocks += S->nq;
+    }
+    SweepJob<T> *dj = nullptr;
+    cudaError_t e = cudaMalloc(&dj, sizeof(SweepJob<T>) * n);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dj, jobs.data(), sizeof(SweepJob<T>) * n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        if (sizeof(T) == 4 && blocks > static_cast<uint32_t>(s[0]->num_sms))  // two ordinates per SM
+            k_sweep_batch<T, sizeof(T) == 4><<<blocks, kSweepThreads, SweepShape<T, sizeof(T) == 4>::smem, st>>>(dj, n);
+        else
+            k_sweep_batch<T, false><<<blocks, kSweepThreads, SweepShape<T, false>::smem, st>>>(dj, n);
+        ++s[0]->launches;
+        e = cudaGetLastError();
+    }
+    for (int i = 0; i < n && e == cudaSuccess; ++i) {
+        tr_sweep *S = s[i];
+        double *Jo = J_out ? J_out[i] : nullptr, *Bo = (B_out && S->nB) ? B_out[i] : nullptr;
+        if constexpr (sizeof(T) == 8) {
+            sweep_outflow_b<T>(S, st, S->psi64, Bo);
+            if (Jo) k_scalar_flux<double><<<grid_for(S, S->nT), 256, 0, st>>>(S->nT, S->nq, S->o64[3], S->psi64, Jo);
+            ++S->sweeps64;
+        } else {
+            sweep_outflow_b<T>(S, st, S->psi32, Bo ? S->Bo32 : nullptr);
+            if (Bo) k_to_f64<<<grid_for(S, S->nB), 256, 0, st>>>(S->nB, S->Bo32, Bo);
+            if (Jo) k_scalar_flux<float><<<grid_for(S, S->nT), 256, 0, st>>>(S->nT, S->nq, S->o64[3], S->psi32, Jo);
+            ++S->sweeps32;
+        }
+        S->launches += (Jo ? 1 : 0) + (sizeof(T) == 4 && Bo ? 1 : 0);
+        S->last_prec = static_cast<int>(8 * sizeof(T));
+        e = cudaGetLastError();
+    }
+    const cudaError_t es = cudaStreamSynchronize(st);
+    if (dj) cudaFree(dj);
+    return e != cudaSuccess ? e : es;
+}
+
 // ============================================================================
 // C ABI
 // ============================================================================
@@ -2333,6 +2442,33 @@ tr_status tr_sweep_apply(tr_sweep *s, int precision, const double *J_in, const d
     cudaError_t e = sweep_enqueue(s, precision, J_in, s->nB ? B_in : nullptr, with_ext, J_out, s->nB ? B_out : nullptr);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
     return sw_cuda(s, e, "tr_sweep_apply");
+}
+
+tr_status tr_sweep_apply_batch(int n, tr_sweep *const *s, int precision, const double *const *J_in,
+                               const double *const *B_in, int with_ext, double *const *J_out,
+                               double *const *B_out) {
+    if (n < 1 || !s) return transfer::set_global_error(TR_ERR_INVALID_ARG, "tr_sweep_apply_batch: no sweeps");
+    for (int i = 0; i < n; ++i) {
+        SW_CHECK(s[i]);
+        if (s[i]->device != s[0]->device)
+            return sw_err(s[0], TR_ERR_INVALID_ARG, "tr_sweep_apply_batch: sweeps on different devices");
+        if ((J_in && !aligned16(J_in[i])) || (B_in && !aligned16(B_in[i])) || (J_out && !aligned16(J_out[i])) ||
+            (B_out && !aligned16(B_out[i])))
+            return sw_err(s[0], TR_ERR_INVALID_ARG, "tr_sweep_apply_batch: device vectors must be 16-byte aligned");
+        for (int k = 0; k < i; ++k)
+            if (s[k] == s[i]) return sw_err(s[0], TR_ERR_INVALID_ARG, "tr_sweep_apply_batch: a sweep twice");
+    }
+    if (precision != 32 && precision != 64) return sw_err(s[0], TR_ERR_INVALID_ARG, "precision must be 32 or 64");
+    cudaSetDevice(s[0]->device);
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < n && e == cudaSuccess; ++i) {
+        e = cudaStreamSynchronize(s[i]->stream);  // nothing of a problem's own stream still in flight
+        if (e == cudaSuccess) e = ensure_psi(s[i], precision);
+    }
+    if (e == cudaSuccess)
+        e = precision == 64 ? batch_sweep<double>(n, s, s[0]->stream, J_in, B_in, with_ext, J_out, B_out)
+                            : batch_sweep<float>(n, s, s[0]->stream, J_in, B_in, with_ext, J_out, B_out);
+    return sw_cuda(s[0], e, "tr_sweep_apply_batch");
 }
 
 tr_status tr_sweep_psi(tr_sweep *s, double *psi) {

@@ -154,6 +154,24 @@ class Sweep:
             self._h = None
 
 
+def sweep_apply_batch(sweeps, precision=64, J=None, B=None, with_ext=True):
+    """One sweep of every problem in `sweeps` (distinct Sweep objects on one
+    device) in a single kernel launch (tr_sweep_apply_batch).  J, B: lists of
+    device inputs per problem (None = zero).  Returns [(J_out, B_out)]."""
+    n = len(sweeps)
+    arr = C.c_void_p * n
+
+    def ptrs(lst):
+        return None if lst is None else arr(*(_ptr(x) for x in lst))
+    outs = [(S.vector_J(), S.vector_B()) for S in sweeps]
+    hs = arr(*(S._h for S in sweeps))
+    st = lib.tr_sweep_apply_batch(n, hs, int(precision), ptrs(J), ptrs(B), int(bool(with_ext)),
+                                  arr(*(_ptr(o[0]) for o in outs)), arr(*(_ptr(o[1]) for o in outs)))
+    if st != L.TR_OK:
+        sweeps[0]._c(st)
+    return [(Jo.view(S.nT, 4), Bo[:S.n_extra]) for S, (Jo, Bo) in zip(sweeps, outs)]
+
+
 def adjoint_problem(md, physics, face_mask):
     """The adjoint of the outflow functional through face_mask's faces: the
     same mesh and coefficients without emission, unit isotropic inflow on

@@ -162,6 +162,36 @@ def cube64_sweep(n=64, albedo=0.3, degree=23):
     return md, phys, ords, mask, desc
 
 
+def cube_batch(count=64, lo=2000, hi=400000, seed=SEED):
+    """Configuration 4's independent problems for the sweep: `count` jittered
+    Kuhn cubes (+-0.2h) with tet counts drawn log-uniformly in [lo, hi]
+    (rounded to n^3 hexahedra), per-tet sigma_t lognormal(0, 1), albedo
+    uniform in [0, 0.9], B = 1 in a random sub-box of edge 0.3, vacuum; the
+    50- or 194-point Lebedev set, drawn per problem.  One frequency group.
+    Returns [(MeshData, Physics, ordinates)] and a description."""
+    from .sweep import lebedev
+    rng = np.random.default_rng(seed)
+    sets = {11: lebedev(11), 23: lebedev(23)}
+    out = []
+    for _ in range(count):
+        n = max(2, int(round((np.exp(rng.uniform(np.log(lo), np.log(hi))) / 6.0) ** (1.0 / 3.0))))
+        base = MeshData.kuhn((n, n, n), jitter=0.2, seed=int(rng.integers(1 << 30)), kappa=[0.0, 1.0], Ip=[0.0, 0.0])
+        tets = base.mesh["p"]
+        nT = len(tets)
+        cent = base.coords[tets.astype(np.int64)].mean(axis=1)
+        c0 = rng.uniform(0.0, 0.7, 3)
+        hot = np.all((cent > c0) & (cent < c0 + 0.3), axis=1)
+        md = MeshData.from_tets(base.coords, tets, np.arange(1, nT + 1, dtype=np.int32),
+                                np.concatenate([[0.0], rng.lognormal(0.0, 1.0, nT)]),
+                                np.concatenate([[0.0], hot.astype(np.float64)]),
+                                albedo=np.concatenate([[0.0], np.full(nT, rng.uniform(0.0, 0.9))]))
+        out.append((md, Physics(kappa_abs_volume=md.kappa_abs_volume), sets[11 if rng.random() < 0.5 else 23]))
+    desc = dict(workload="cube_batch", problems=count, tets=f"{lo}-{hi} log-uniform",
+                physics="sigma_t lognormal(0,1) per tet, albedo U[0,0.9] per problem, B=1 in a random 0.3 box",
+                ordinates="Lebedev 50 or 194 per problem")
+    return out, desc
+
+
 def sweep_work(nT, nq, real_bytes=4):
     """Algorithmic (compulsory) work of one sweep of all ordinates: per
     (cell, ordinate) the 16-byte task record is read and psi (4 reals)
