@@ -425,6 +425,17 @@ tr_status tr_sweep_apply(tr_sweep *s, int precision, const double *J_in, const d
 tr_status tr_sweep_apply_batch(int n, tr_sweep *const *s, int precision, const double *const *J_in,
                                const double *const *B_in, int with_ext, double *const *J_out,
                                double *const *B_out);
+/* Source iteration x <- S(x) (with sources, from x = 0) of n independent
+ * problems at once: each iteration is one batched sweep launch plus every
+ * problem's reductions, captured as a CUDA graph and replayed; a problem
+ * whose relative change ||S(x) - x|| / ||S(x)|| falls below tol leaves the
+ * running set (the graph is captured again for the rest), until all have
+ * (or max_iter iterations).  Sweeps in precision 32 or 64 (FP64 iterates and stopping
+ * test).  J[i] (and B[i] if B, for problems with n_extra > 0): device
+ * outputs; iterations[i] (first iteration below tol, 0 if none) and
+ * residual[i] (last relative change): host arrays [n]. */
+tr_status tr_sweep_solve_batch(int n, tr_sweep *const *s, int precision, double tol, int max_iter, double *const *J,
+                               double *const *B, int32_t *iterations, double *residual);
 /* psi of the last sweep as FP64, device [nq][nT][4]. */
 tr_status tr_sweep_psi(tr_sweep *s, double *psi);
 /* Angular moments of the last sweep's psi: mom[m][nT][4] = sum_q w_q

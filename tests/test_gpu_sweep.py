@@ -263,6 +263,26 @@ def test_batched_sweep_equals_separate_sweeps(cuda, precision):
     assert sum(S.nq for S in sweeps) > 148   # the batch ran the two-per-SM shape in FP32
 
 
+def test_batched_source_iteration_matches_separate_solves(cuda):
+    """The graph-replayed batched source iteration reaches each problem's
+    own fixed point (FP64 sweeps; FP32 sweeps to the FP32 floor)."""
+    cases = [(scattering_box(), op.ordinates_product(4, 8)), (tangled_cube(), op.ordinates_product(2, 6)),
+             (absorbing_slab(nx=20), op.ordinates_product(6, 12))]
+    sweeps = [tr.Sweep(0, md, ords, ph) for (md, ph), ords in cases]
+    SI = tr._lib.TR_SWEEP_SOURCE_ITERATION
+    ref = [S.solve(method=SI, tol=1e-13, max_iter=3000) for S in sweeps]
+    out, its, res = tr.sweep_solve_batch(sweeps, 64, tol=1e-13, max_iter=3000)
+    assert (its > 0).all() and (res < 1e-13).all()
+    for (J, B), (Jr, Br, rep) in zip(out, ref):
+        assert rel_err(host(J), host(Jr)) < 1e-11 and rel_err(host(B), host(Br)) < 1e-11
+    out32, its32, res32 = tr.sweep_solve_batch(sweeps, 32, tol=1e-6, max_iter=3000)
+    assert (its32 > 0).all()
+    # FP32 sweeps: 1e-4 of the FP64 fixed point; the tangled cube's inverted
+    # elements make some systems ill-conditioned (FP32 sweeps differ by 1e-4)
+    for (J, B), (Jr, Br, rep), tol in zip(out32, ref, (1e-4, 2e-3, 1e-4)):
+        assert rel_err(host(J), host(Jr)) < tol
+
+
 def test_set_coefficients_matches_the_oracle(cuda):
     """New sigma_t V, sigma_a V and B on an existing sweep (geometry and
     schedule kept) give the oracle's solution for those coefficients."""

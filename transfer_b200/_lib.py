@@ -205,6 +205,7 @@ PROTOTYPES = [
     ("tr_sweep_enable_dsa", S, [P, C.POINTER(tr_mesh_view), C.POINTER(tr_physics_view)]),
     ("tr_sweep_set_coefficients", S, [P, P, P, P]),
     ("tr_sweep_apply_batch", S, [I, P, I, P, P, I, P, P]),
+    ("tr_sweep_solve_batch", S, [I, P, I, D, I, P, P, P, P]),
     ("tr_sweep_outflow", S, [P, P, C.POINTER(D)]),
     ("tr_sweep_gradient", S, [P, P, I, P, P, P, P, P]),
     ("tr_sweep_bench", S, [P, I, I, C.POINTER(D)]),

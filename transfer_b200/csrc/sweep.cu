@@ -2309,6 +2309,124 @@ static cudaError_t batch_sweep(int n, tr_sweep *const *s, cudaStream_t st, const
     return e != cudaSuccess ? e : es;
 }
 
+// One source iteration of every problem, x <- S(x) with sources, queued on st
+// (captured once into a CUDA graph by tr_sweep_solve_batch): per problem
+// x = S->kx [J | B], the new iterate in S->kt, res[2i] = ||S(x) - x||^2 and
+// res[2i + 1] = ||S(x)||^2.
+template <typename T>
+static void batch_si_step(int n, tr_sweep *const *s, cudaStream_t st, const SweepJob<T> *dj, uint32_t blocks,
+                          double *res) {
+    for (int i = 0; i < n; ++i) {
+        tr_sweep *S = s[i];
+        if constexpr (sizeof(T) == 4) {
+            k_to_f32<<<grid_for(S, S->nJ), 256, 0, st>>>(S->nJ, S->kx, S->J32);
+            if (S->nB) k_to_f32<<<grid_for(S, S->nB), 256, 0, st>>>(S->nB, S->kx + S->nJ, S->Bi32);
+        }
+    }
+    if (sizeof(T) == 4 && blocks > static_cast<uint32_t>(s[0]->num_sms))
+        k_sweep_batch<T, sizeof(T) == 4><<<blocks, kSweepThreads, SweepShape<T, sizeof(T) == 4>::smem, st>>>(dj, n);
+    else
+        k_sweep_batch<T, false><<<blocks, kSweepThreads, SweepShape<T, false>::smem, st>>>(dj, n);
+    for (int i = 0; i < n; ++i) {
+        tr_sweep *S = s[i];
+        const uint64_t nx = S->nJ + S->nB;
+        if constexpr (sizeof(T) == 8) {
+            sweep_outflow_b<T>(S, st, S->psi64, S->nB ? S->kt + S->nJ : nullptr);
+            k_scalar_flux<double><<<grid_for(S, S->nT), 256, 0, st>>>(S->nT, S->nq, S->o64[3], S->psi64, S->kt);
+        } else {
+            sweep_outflow_b<T>(S, st, S->psi32, S->nB ? S->Bo32 : nullptr);
+            if (S->nB) k_to_f64<<<grid_for(S, S->nB), 256, 0, st>>>(S->nB, S->Bo32, S->kt + S->nJ);
+            k_scalar_flux<float><<<grid_for(S, S->nT), 256, 0, st>>>(S->nT, S->nq, S->o64[3], S->psi32, S->kt);
+        }
+        k_axpby<<<grid_for(S, nx), 256, 0, st>>>(nx, 1.0, S->kt, -1.0, S->kx);  // kx = S(x) - x
+        k_multidot<<<kDotGrid, 256, 0, st>>>(nx, 1, S->kx, 0, S->kx, S->partials, S->counter, res + 2 * i);
+        k_multidot<<<kDotGrid, 256, 0, st>>>(nx, 1, S->kt, 0, S->kt, S->partials, S->counter, res + 2 * i + 1);
+        cudaMemcpyAsync(S->kx, S->kt, nx * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    }
+}
+// Source iteration of the problems s[0..n) until each one's relative change
+// is below tol: the iteration of the problems still running is captured as a
+// CUDA graph and replayed; when one of them converges it leaves the set and
+// the graph is captured again for the rest.
+template <typename T>
+static cudaError_t batch_si(int n, tr_sweep *const *s, cudaStream_t st, double tol, int max_iter,
+                            int32_t *iterations, double *residual) {
+    SweepJob<T> *dj = nullptr;
+    double *res = nullptr;
+    cudaError_t e = cudaMalloc(&dj, sizeof(SweepJob<T>) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&res, sizeof(double) * 2 * n);
+    for (int i = 0; i < n && e == cudaSuccess; ++i)
+        e = cudaMemsetAsync(s[i]->kx, 0, (s[i]->nJ + s[i]->nB) * sizeof(double), st);
+    for (int i = 0; i < n; ++i) {
+        iterations[i] = 0;
+        residual[i] = 0.0;
+    }
+    std::vector<int> act(n);
+    for (int i = 0; i < n; ++i) act[i] = i;
+    std::vector<tr_sweep *> sub;
+    std::vector<SweepJob<T>> jobs;
+    std::vector<double> hr(2 * n);
+    int it = 0;
+    while (e == cudaSuccess && !act.empty() && it < max_iter) {
+        const int m = static_cast<int>(act.size());
+        sub.assign(m, nullptr);
+        jobs.assign(m, SweepJob<T>());
+        uint32_t blocks = 0;
+        for (int k = 0; k < m; ++k) {
+            tr_sweep *S = s[act[k]];
+            sub[k] = S;
+            const double *Bx = S->nB ? S->kx + S->nJ : nullptr;
+            if constexpr (sizeof(T) == 8) jobs[k] = make_job<T>(S, S->kx, Bx, 1, S->psi64);
+            else jobs[k] = make_job<T>(S, S->J32, Bx ? S->Bi32 : nullptr, 1, S->psi32);
+            jobs[k].block0 = blocks;
+            blocks += S->nq;
+        }
+        e = cudaMemcpyAsync(dj, jobs.data(), sizeof(SweepJob<T>) * m, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        if (e == cudaSuccess) e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            batch_si_step<T>(m, sub.data(), st, dj, blocks, res);
+            const cudaError_t ec = cudaStreamEndCapture(st, &graph);
+            e = cudaGetLastError();
+            if (e == cudaSuccess) e = ec;
+        }
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+        bool changed = false;
+        while (e == cudaSuccess && !changed && it < max_iter) {
+            ++it;
+            e = cudaGraphLaunch(exec, st);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(hr.data(), res, sizeof(double) * 2 * m, cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) break;
+            for (int k = 0; k < m; ++k) {
+                const int i = act[k];
+                const double r = hr[2 * k + 1] > 0.0 ? std::sqrt(hr[2 * k] / hr[2 * k + 1]) : 0.0;
+                residual[i] = r;
+                if (r < tol) {
+                    iterations[i] = it;
+                    changed = true;
+                }
+                s[i]->launches += 8;  // per iteration: conversions, sweep share, outflow, flux, reductions, copy
+                if (sizeof(T) == 8) ++s[i]->sweeps64;
+                else ++s[i]->sweeps32;
+                s[i]->last_prec = static_cast<int>(8 * sizeof(T));
+            }
+        }
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        std::vector<int> keep;
+        for (int i : act)
+            if (!iterations[i]) keep.push_back(i);
+        act.swap(keep);
+    }
+    cudaStreamSynchronize(st);
+    if (dj) cudaFree(dj);
+    if (res) cudaFree(res);
+    return e;
+}
+
 // ============================================================================
 // C ABI
 // ============================================================================
@@ -2469,6 +2587,44 @@ tr_status tr_sweep_apply_batch(int n, tr_sweep *const *s, int precision, const d
         e = precision == 64 ? batch_sweep<double>(n, s, s[0]->stream, J_in, B_in, with_ext, J_out, B_out)
                             : batch_sweep<float>(n, s, s[0]->stream, J_in, B_in, with_ext, J_out, B_out);
     return sw_cuda(s[0], e, "tr_sweep_apply_batch");
+}
+
+tr_status tr_sweep_solve_batch(int n, tr_sweep *const *s, int precision, double tol, int max_iter, double *const *J,
+                               double *const *B, int32_t *iterations, double *residual) {
+    if (n < 1 || !s || !J || !iterations || !residual)
+        return transfer::set_global_error(TR_ERR_INVALID_ARG, "tr_sweep_solve_batch: null argument");
+    for (int i = 0; i < n; ++i) {
+        SW_CHECK(s[i]);
+        if (s[i]->device != s[0]->device)
+            return sw_err(s[0], TR_ERR_INVALID_ARG, "tr_sweep_solve_batch: sweeps on different devices");
+        if (!J[i] || !aligned16(J[i]) || (B && !aligned16(B[i])))
+            return sw_err(s[0], TR_ERR_INVALID_ARG, "tr_sweep_solve_batch: device vectors must be 16-byte aligned");
+        for (int k = 0; k < i; ++k)
+            if (s[k] == s[i]) return sw_err(s[0], TR_ERR_INVALID_ARG, "tr_sweep_solve_batch: a sweep twice");
+    }
+    if (precision != 32 && precision != 64) return sw_err(s[0], TR_ERR_INVALID_ARG, "precision must be 32 or 64");
+    if (!(tol > 0.0) || max_iter < 1) return sw_err(s[0], TR_ERR_INVALID_ARG, "tr_sweep_solve_batch: tol / max_iter");
+    cudaSetDevice(s[0]->device);
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < n && e == cudaSuccess; ++i) {
+        e = cudaStreamSynchronize(s[i]->stream);
+        if (e == cudaSuccess) e = ensure_psi(s[i], precision);
+        if (e == cudaSuccess) e = krylov_alloc(s[i], 1);
+    }
+    cudaStream_t st = s[0]->stream;
+    if (e == cudaSuccess)
+        e = precision == 64 ? batch_si<double>(n, s, st, tol, max_iter, iterations, residual)
+                            : batch_si<float>(n, s, st, tol, max_iter, iterations, residual);
+    for (int i = 0; i < n && e == cudaSuccess; ++i) {
+        e = cudaMemcpyAsync(J[i], s[i]->kx, s[i]->nJ * sizeof(double), cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess && B && s[i]->nB)
+            e = cudaMemcpyAsync(B[i], s[i]->kx + s[i]->nJ, s[i]->nB * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return sw_cuda(s[0], e, "tr_sweep_solve_batch");
+    for (int i = 0; i < n; ++i)
+        if (!iterations[i]) return sw_err(s[0], TR_ERR_NOT_CONVERGED, "tr_sweep_solve_batch: not converged");
+    return TR_OK;
 }
 
 tr_status tr_sweep_psi(tr_sweep *s, double *psi) {

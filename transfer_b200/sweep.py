@@ -172,6 +172,23 @@ def sweep_apply_batch(sweeps, precision=64, J=None, B=None, with_ext=True):
     return [(Jo.view(S.nT, 4), Bo[:S.n_extra]) for S, (Jo, Bo) in zip(sweeps, outs)]
 
 
+def sweep_solve_batch(sweeps, precision=64, tol=1e-10, max_iter=1000, raise_on_error=True):
+    """Source iteration of every problem in `sweeps` at once, one batched
+    sweep launch per iteration replayed from a CUDA graph
+    (tr_sweep_solve_batch).  Returns ([(J, B)], iterations, residuals)."""
+    n = len(sweeps)
+    arr = C.c_void_p * n
+    outs = [(S.vector_J(), S.vector_B()) for S in sweeps]
+    its = np.zeros(n, dtype=np.int32)
+    res = np.zeros(n)
+    st = lib.tr_sweep_solve_batch(n, arr(*(S._h for S in sweeps)), int(precision), float(tol), int(max_iter),
+                                  arr(*(_ptr(o[0]) for o in outs)), arr(*(_ptr(o[1]) for o in outs)), _ptr(its),
+                                  _ptr(res))
+    if st != L.TR_OK and (raise_on_error or st != L.TR_ERR_NOT_CONVERGED):
+        sweeps[0]._c(st)
+    return [(Jo.view(S.nT, 4), Bo[:S.n_extra]) for S, (Jo, Bo) in zip(sweeps, outs)], its, res
+
+
 def adjoint_problem(md, physics, face_mask):
     """The adjoint of the outflow functional through face_mask's faces: the
     same mesh and coefficients without emission, unit isotropic inflow on
