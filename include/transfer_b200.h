@@ -436,6 +436,12 @@ tr_status tr_sweep_apply_batch(int n, tr_sweep *const *s, int precision, const d
  * residual[i] (last relative change): host arrays [n]. */
 tr_status tr_sweep_solve_batch(int n, tr_sweep *const *s, int precision, double tol, int max_iter, double *const *J,
                                double *const *B, int32_t *iterations, double *residual);
+/* Times the FP32 sweep kernel in both shared-memory shapes on this problem
+ * (full: one block per SM; small: two per SM, shorter ring) and keeps the
+ * faster for its later FP32 sweeps (without it: small when there are more
+ * ordinates than SMs).  shape: 0 full / 1 small; ms[2]: mean time of one
+ * sweep in each (either may be NULL).  Results do not depend on the shape. */
+tr_status tr_sweep_autotune(tr_sweep *s, int *shape, double *ms);
 /* psi of the last sweep as FP64, device [nq][nT][4]. */
 tr_status tr_sweep_psi(tr_sweep *s, double *psi);
 /* Angular moments of the last sweep's psi: mom[m][nT][4] = sum_q w_q

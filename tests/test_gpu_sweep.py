@@ -283,6 +283,20 @@ def test_batched_source_iteration_matches_separate_solves(cuda):
         assert rel_err(host(J), host(Jr)) < tol
 
 
+def test_autotune_keeps_results(cuda):
+    """Both shapes are timed, the faster kept; FP32 sweeps are bitwise the
+    same before and after."""
+    md, ph = scattering_box(n=(8, 8, 8))
+    S = tr.Sweep(0, md, op.ordinates_product(4, 8), ph)
+    J = dev(np.random.default_rng(3).random(4 * S.nT))
+    J0, B0 = S.apply(J, None, precision=32)
+    shape, ms_full, ms_small = S.autotune()
+    assert shape in (0, 1) and ms_full > 0 and ms_small > 0
+    assert shape == (1 if ms_small < ms_full else 0)
+    J1, B1 = S.apply(J, None, precision=32)
+    assert torch.equal(J0, J1) and torch.equal(B0, B1)
+
+
 def test_set_coefficients_matches_the_oracle(cuda):
     """New sigma_t V, sigma_a V and B on an existing sweep (geometry and
     schedule kept) give the oracle's solution for those coefficients."""

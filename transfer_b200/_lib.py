@@ -206,6 +206,7 @@ PROTOTYPES = [
     ("tr_sweep_set_coefficients", S, [P, P, P, P]),
     ("tr_sweep_apply_batch", S, [I, P, I, P, P, I, P, P]),
     ("tr_sweep_solve_batch", S, [I, P, I, D, I, P, P, P, P]),
+    ("tr_sweep_autotune", S, [P, P, P]),
     ("tr_sweep_outflow", S, [P, P, C.POINTER(D)]),
     ("tr_sweep_gradient", S, [P, P, I, P, P, P, P, P]),
     ("tr_sweep_bench", S, [P, I, I, C.POINTER(D)]),

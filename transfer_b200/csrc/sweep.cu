@@ -1463,6 +1463,7 @@ struct tr_sweep {
     std::vector<void *> allocs;
     int64_t sweeps32 = 0, sweeps64 = 0, launches = 0;
     bool mom_attr = false;         // k_moments_tf32x3 shared-memory opt-in done
+    int shape32 = -1;              // FP32 sweep shape: -1 by rule, 0 full, 1 small (tr_sweep_autotune)
 };
 
 static tr_status sw_err(tr_sweep *s, tr_status st, const std::string &m) {
@@ -1949,9 +1950,9 @@ template <typename T>
 static cudaError_t sweep_launch(tr_sweep *S, const T *J, const T *Bin, int with_ext, T *psi, T *Bout) {
     cudaStream_t st = S->stream;
     const SweepJob<T> j = make_job<T>(S, J, Bin, with_ext, psi);
-    bool two_per_sm = false;  // FP32 with more ordinates than SMs: the small shape
+    bool two_per_sm = false;  // FP32 with more ordinates than SMs (or as tuned): the small shape
     if constexpr (sizeof(T) == 4) {
-        two_per_sm = S->nq > static_cast<uint32_t>(S->num_sms);
+        two_per_sm = S->shape32 >= 0 ? S->shape32 == 1 : S->nq > static_cast<uint32_t>(S->num_sms);
         if (two_per_sm) k_sweep<T, true><<<S->nq, kSweepThreads, SweepShape<T, true>::smem, st>>>(j.g, j.sc, j.a);
     }
     if (!two_per_sm) k_sweep<T, false><<<S->nq, kSweepThreads, SweepShape<T, false>::smem, st>>>(j.g, j.sc, j.a);
@@ -2624,6 +2625,35 @@ tr_status tr_sweep_solve_batch(int n, tr_sweep *const *s, int precision, double 
     if (e != cudaSuccess) return sw_cuda(s[0], e, "tr_sweep_solve_batch");
     for (int i = 0; i < n; ++i)
         if (!iterations[i]) return sw_err(s[0], TR_ERR_NOT_CONVERGED, "tr_sweep_solve_batch: not converged");
+    return TR_OK;
+}
+
+tr_status tr_sweep_autotune(tr_sweep *s, int *shape, double *ms) {
+    SW_CHECK(s);
+    cudaSetDevice(s->device);
+    cudaError_t e = ensure_psi(s, 32);
+    double t[2] = {0.0, 0.0};
+    for (int c = 0; c < 2 && e == cudaSuccess; ++c) {
+        s->shape32 = c;
+        for (int w = 0; w < 2 && e == cudaSuccess; ++w) e = sweep_enqueue(s, 32, nullptr, nullptr, 1, nullptr, nullptr);
+        if (e == cudaSuccess) e = cudaEventRecord(s->ev[0], s->stream);
+        for (int r = 0; r < 5 && e == cudaSuccess; ++r) e = sweep_enqueue(s, 32, nullptr, nullptr, 1, nullptr, nullptr);
+        if (e == cudaSuccess) e = cudaEventRecord(s->ev[1], s->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+        float f = 0.0f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&f, s->ev[0], s->ev[1]);
+        t[c] = f / 5.0;
+    }
+    if (e != cudaSuccess) {
+        s->shape32 = -1;
+        return sw_cuda(s, e, "tr_sweep_autotune");
+    }
+    s->shape32 = t[1] < t[0] ? 1 : 0;
+    if (shape) *shape = s->shape32;
+    if (ms) {
+        ms[0] = t[0];
+        ms[1] = t[1];
+    }
     return TR_OK;
 }
 

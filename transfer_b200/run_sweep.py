@@ -4,13 +4,14 @@ contraction and the accelerated solve)."""
 def _main():
     """python -m transfer_b200.run_sweep [--workload milne|stellar[:n]]
     [--precision 32|64] [--sweeps N] [--moments K] [--solve none|gmres|dsa]
-    [--tol T]: N sweeps of the workload (workloads.milne_sweep, or
+    [--tol T] [--autotune]: N sweeps of the workload (workloads.milne_sweep, or
     workloads.stellar_sphere with n^3 grid cells, default 96) with a
     scattering source and the mean device time of one sweep; --moments: K
     launches of the l <= 3 moment contraction of the last sweep's psi, timed
     with CUDA events; with --solve, one GMRES solve to FP64 relative residual
     T in the given precision (64: FP64, 32: mixed), plain or with the
-    diffusion synthetic acceleration."""
+    diffusion synthetic acceleration; --autotune times both FP32 sweep shapes
+    first and keeps the faster."""
     import argparse
 
     import torch
@@ -25,6 +26,7 @@ def _main():
     ap.add_argument("--tol", type=float, default=1e-8)
     ap.add_argument("--workload", default="milne")
     ap.add_argument("--moments", type=int, default=0)
+    ap.add_argument("--autotune", action="store_true")
     args = ap.parse_args()
     if args.workload.startswith("stellar"):
         n = int(args.workload.split(":")[1]) if ":" in args.workload else 96
@@ -32,6 +34,10 @@ def _main():
     else:
         md, ph, ords, desc = W.milne_sweep()
     S = Sweep(0, md, ords, ph, dsa=args.solve == "dsa")
+    if args.autotune:
+        shape, t_full, t_small = S.autotune()
+        print(f"autotune: FP32 sweep {t_full:.3f} ms full shape, {t_small:.3f} ms small; keeps "
+              f"{'small' if shape else 'full'}")
     J = torch.rand(4 * S.nT, dtype=torch.float64, device="cuda:0")
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()

@@ -129,6 +129,13 @@ class Sweep:
             self._c(st)
         return J.view(self.nT, 4), B[:self.n_extra], report
 
+    def autotune(self):
+        """tr_sweep_autotune: (shape kept, ms of one FP32 sweep full, small)."""
+        shape = C.c_int()
+        ms = (C.c_double * 2)()
+        self._c(lib.tr_sweep_autotune(self._h, C.byref(shape), ms))
+        return shape.value, ms[0], ms[1]
+
     def set_coefficients(self, kappa_volume, kappa_abs_volume=None, I_p=None):
         """Per-cell sigma_t V, sigma_a V (None: no scattering) and Planck
         intensity (None: kept), host arrays [nT]; geometry and schedule stay."""
