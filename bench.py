@@ -234,6 +234,8 @@ def sweep_section(local, flush, peak, want_cpu):
     for name, mode, prec in (("fp64", tr.TR_MODE_FP64, 0), ("mixed", tr.TR_MODE_MIXED, 0),
                              ("fp64_dsa", tr.TR_MODE_FP64, DSA), ("mixed_dsa", tr.TR_MODE_MIXED, DSA)):
         kw = dict(mode=mode, tol=SWEEP_TOL, restart=40, max_iter=5000, precondition=prec, precond_tol=1e-2)
+        if prec and mode == tr.TR_MODE_MIXED:
+            kw["inner_tol"] = 1e-4   # restart from the FP64 residual before the FP32 sweeps' floor
         S.solve(**kw)   # warm-up
         flush.fill_(1.0)
         torch.cuda.synchronize()
