@@ -261,6 +261,10 @@ def test_batched_sweep_equals_separate_sweeps(cuda, precision):
         Jo, Bo = S.apply(J, B if S.n_extra else None, precision=precision)
         assert torch.equal(Jb, Jo) and torch.equal(Bb, Bo)
     assert sum(S.nq for S in sweeps) > 148   # the batch ran the two-per-SM shape in FP32
+    with pytest.raises(tr.TransferError):    # the same problem twice in one batch
+        tr.sweep_apply_batch([sweeps[0], sweeps[0]], precision)
+    with pytest.raises(tr.TransferError):
+        tr.sweep_apply_batch(sweeps[:1], 16)
 
 
 def test_batched_source_iteration_matches_separate_solves(cuda):
