@@ -2249,6 +2249,16 @@ static cudaError_t gmres(tr_sweep *S, int prec, int prec_res, const double *b, d
     return cudaSuccess;
 }
 
+// Problem order in a batched launch: largest first (cells, then index), so
+// that the blocks with the longest walks start in the first wave and the
+// last wave holds short ones (blocks start in index order).
+static std::vector<int> largest_first(int n, tr_sweep *const *s) {
+    std::vector<int> ord(n);
+    for (int i = 0; i < n; ++i) ord[i] = i;
+    std::stable_sort(ord.begin(), ord.end(), [s](int a, int b) { return s[a]->nT > s[b]->nT; });
+    return ord;
+}
+
 // One launch of k_sweep_batch over every problem's ordinates, each problem's
 // conversions and reductions before and after it on the same stream.
 template <typename T>
@@ -2256,13 +2266,15 @@ static cudaError_t batch_sweep(int n, tr_sweep *const *s, cudaStream_t st, const
                                const double *const *B_in, int with_ext, double *const *J_out,
                                double *const *B_out) {
     std::vector<SweepJob<T>> jobs(n);
+    const std::vector<int> ord = largest_first(n, s);
     uint32_t blocks = 0;
-    for (int i = 0; i < n; ++i) {
+    for (int k = 0; k < n; ++k) {
+        const int i = ord[k];
         tr_sweep *S = s[i];
         const double *Ji = J_in ? J_in[i] : nullptr;
         const double *Bi = (B_in && S->nB) ? B_in[i] : nullptr;
         if constexpr (sizeof(T) == 8) {
-            jobs[i] = make_job<T>(S, Ji, Bi, with_ext, S->psi64);
+            jobs[k] = make_job<T>(S, Ji, Bi, with_ext, S->psi64);
         } else {
             if (Ji) {
                 k_to_f32<<<grid_for(S, S->nJ), 256, 0, st>>>(S->nJ, Ji, S->J32);
@@ -2272,9 +2284,9 @@ static cudaError_t batch_sweep(int n, tr_sweep *const *s, cudaStream_t st, const
                 k_to_f32<<<grid_for(S, S->nB), 256, 0, st>>>(S->nB, Bi, S->Bi32);
                 ++S->launches;
             }
-            jobs[i] = make_job<T>(S, Ji ? S->J32 : nullptr, Bi ? S->Bi32 : nullptr, with_ext, S->psi32);
+            jobs[k] = make_job<T>(S, Ji ? S->J32 : nullptr, Bi ? S->Bi32 : nullptr, with_ext, S->psi32);
         }
-        jobs[i].block0 = blocks;
+        jobs[k].block0 = blocks;
         blocks += S->nq;
     }
     SweepJob<T> *dj = nullptr;
@@ -2362,8 +2374,7 @@ static cudaError_t batch_si(int n, tr_sweep *const *s, cudaStream_t st, double t
         iterations[i] = 0;
         residual[i] = 0.0;
     }
-    std::vector<int> act(n);
-    for (int i = 0; i < n; ++i) act[i] = i;
+    std::vector<int> act = largest_first(n, s);
     std::vector<tr_sweep *> sub;
     std::vector<SweepJob<T>> jobs;
     std::vector<double> hr(2 * n);
