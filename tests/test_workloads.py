@@ -49,3 +49,13 @@ def test_sweep_workloads_at_small_sizes():
     assert len(ords[3]) == 194 and abs(ords[3].sum() - 1.0) < 1e-12
     fx = md.coords[md.bnd["p"][:, :3].astype(np.int64)][..., 0]
     assert mask.sum() == 2 * 6 * 6 and (fx[mask.astype(bool)] > 1 - 1e-9).all()
+
+
+def test_runner_command_lines_parse():
+    """The measurement runners start and print their usage without a GPU."""
+    import subprocess
+    import sys
+    for mod in ("transfer_b200.run_sweep", "transfer_b200.run_batch", "transfer_b200.run_adjoint"):
+        r = subprocess.run([sys.executable, "-m", mod, "--help"], cwd=os.path.dirname(os.path.dirname(__file__)),
+                           capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0 and "usage" in r.stdout, (mod, r.stderr[-500:])
