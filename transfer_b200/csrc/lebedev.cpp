@@ -257,12 +257,14 @@ bool levenberg_marquardt(const Problem &pr, const std::vector<int> &kinds, std::
 
 // canonical orbit parameters; false if the solution is not an admissible
 // rule (non-positive weight, degenerate or repeated orbit)
-bool admissible(const std::vector<int> &kinds, std::vector<double> &v, int no) {
+// negative_ok: the rule may carry a negative orbit weight (the 74-point rule
+// does: its 8-point (1,1,1)/sqrt(3) orbit weighs -0.0296)
+bool admissible(const std::vector<int> &kinds, std::vector<double> &v, int no, bool negative_ok) {
     const double r2 = std::sqrt(0.5), r3 = std::sqrt(1.0 / 3.0), eps = 1e-6;
     std::vector<std::vector<double>> seen(6);
     int pi = no;
     for (int o = 0; o < no; ++o) {
-        if (!(v[o] > 0.0)) return false;
+        if (!(v[o] > 0.0) && !(negative_ok && v[o] < 0.0)) return false;
         const int kind = kinds[o];
         if (kind == 3) {
             double l = std::fabs(v[pi]);
@@ -483,7 +485,7 @@ bool generate(const OrbitSpec &sp, LebedevQuad &q) {
         for (size_t i = 0; i < theta.size(); ++i) v[pr.no + i] = theta[i];
         int pi = pr.no;
         if (!levenberg_marquardt(pr, kinds, v)) continue;
-        if (!admissible(kinds, v, pr.no)) continue;
+        if (!admissible(kinds, v, pr.no, sp.order == 74)) continue;
         std::vector<double> F;
         eval(pr, kinds, v, F, nullptr);
         double worst = 0.0;
