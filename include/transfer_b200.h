@@ -190,9 +190,12 @@ tr_status tr_dot(tr_ctx *ctx, const double *x, const double *y, double *out);
  * 33,554,432 entries, else TR_ERR_INVALID_ARG (message in
  * tr_last_error(NULL)).  Its scratch is one static device array of about
  * 16 KiB per GPU, shared by all calls: calls that overlap on the GPU race
- * and must be ordered by the caller.  The first call on a device looks up
- * that array's device address (set-up work), so make it before any stream
- * capture on that device.  Summation order depends only on nP * aslm, so the
+ * and must be ordered by the caller.  Each call looks up that array's
+ * device address in the current context, so a cudaDeviceReset (or another
+ * context made current) between calls is safe; the first call on a device
+ * also loads the library's module there (set-up work), so make it before
+ * any stream capture on that device.  nP = 0 writes 0.0 to *out.
+ * Summation order depends only on nP * aslm, so the
  * bits do not depend on the GPU; they may differ from tr_dot's in the last
  * places. */
 tr_status tr_dot_noalloc(const double *x, const double *y, uint32_t nP,

@@ -181,6 +181,24 @@ def test_config_additive_keys(tmp_path):
     assert cfg.usePrec() is False and cfg.solType() == 0   # defaults instead of garbage
 
 
+@pytest.mark.parametrize("text,key,line", [
+    ("numregs = 1\n[region 1]\nkappa = x\n", "kappa", 3),
+    ("numregs = 1\nkappa = 1\n", "kappa", 2),
+    ("numregs = 1\n[region 1]\nangorder = 2\n", "angorder", 3),
+    ("# c\n[region 1]\n", "numregs", 2),
+    ("numregs = 2\n[region 3]\n", "region 3", 2),
+    ("numregs = -4\n", "numregs", 1),
+])
+def test_config_error_names_key_and_line(tmp_path, text, key, line):
+    p = tmp_path / "bad.cfg"
+    p.write_text(text)
+    with pytest.raises(tr.TransferError) as ei:
+        tr.Config(p)
+    assert ei.value.status == L.TR_ERR_CONFIG
+    msg = str(ei.value)
+    assert key in msg and f"line {line}" in msg, msg
+
+
 def test_config_missing_file():
     with pytest.raises(tr.TransferError) as ei:
         tr.Config("/nonexistent/radiation.cfg")

@@ -3,7 +3,10 @@ memory (a host whose memory pool owns the device, a loop where cudaMalloc
 would synchronise the device, or a caller without a tr_ctx).  It keeps its
 scratch in one static device array, so these tests check that it agrees
 with tr_dot on two calls in a row (the shared scratch left by the first call
-must not disturb the second) and that it rejects sizes beyond its limit.
+must not disturb the second) and with an FP64 NumPy dot of the same data,
+that an empty vector gives 0.0, that a call at the largest size its scratch
+takes (2048 blocks) is right and leaves the scratch ready for the next call,
+and that it rejects sizes beyond its limit.
 
 This file is named to be collected last; it passes alone in a fresh process
 and after the other tests."""
@@ -16,6 +19,13 @@ import transfer_b200 as tr
 from common import c1_mesh, golden_angular, random_vector, small_mesh
 
 MAX_ENTRIES = 2048 * 256 * 64
+
+
+def numpy_dot(x, y, nP, aslm, slm):
+    """FP64 dot over lm < slm and the scale of its rounding error (sum |x y|)."""
+    a = np.asarray(x).reshape(nP, aslm)[:, :slm]
+    b = np.asarray(y).reshape(nP, aslm)[:, :slm]
+    return float(np.sum(a * b)), float(np.sum(np.abs(a * b)))
 
 
 def call(x, y, nP, aslm, slm, out, stream=None):
@@ -49,6 +59,9 @@ def test_matches_tr_dot_on_two_calls_in_a_row(cuda, mesh, maxk):
     got = out.cpu().numpy()
     for g, r in zip(got, ref):
         assert abs(g / r - 1) < 1e-13
+    for g, x in zip(got, xs[:2]):   # and an FP64 NumPy dot of the same data
+        d, scale = numpy_dot(x, xs[2], nP, aslm, slm)
+        assert abs(g - d) <= 1e-14 * scale
     # same input again: the same bits (the scratch left by earlier calls is reused)
     st = call(x0.data_ptr(), y.data_ptr(), nP, aslm, slm, out.data_ptr() + 8, stream)
     assert st == tr._lib.TR_OK
@@ -71,3 +84,40 @@ def test_rejects_host_memory(cuda):
     st = call(h.ctypes.data, y.data_ptr(), 4, 16, 15, y.data_ptr())
     assert st == tr._lib.TR_ERR_INVALID_ARG
     assert b"device memory" in tr.lib.tr_last_error(None) or b"CUDA pointer" in tr.lib.tr_last_error(None)
+
+
+@pytest.mark.gpu
+def test_empty_vector_gives_zero(cuda):
+    import torch
+    x = torch.ones(16, dtype=torch.float64, device="cuda")
+    out = torch.full((1,), float("nan"), dtype=torch.float64, device="cuda")
+    st = call(x.data_ptr(), x.data_ptr(), 0, 16, 15, out.data_ptr(), torch.cuda.current_stream().cuda_stream)
+    assert st == tr._lib.TR_OK, tr.lib.tr_last_error(None)
+    assert out.cpu().numpy()[0] == 0.0
+
+
+@pytest.mark.gpu
+def test_largest_size_then_a_small_call(cuda):
+    """nP * aslm = 33,554,432 (256 MiB per vector) fills all 2048 blocks of the
+    scratch; the next, small call must still be right (its ticket was reset)."""
+    import torch
+    aslm, slm = 32, 28
+    nP = MAX_ENTRIES // aslm
+    rng = np.random.default_rng(7)
+    xh = rng.random(nP * aslm)
+    yh = rng.standard_normal(nP * aslm)
+    x, y = torch.from_numpy(xh).cuda(), torch.from_numpy(yh).cuda()
+    out = torch.full((2,), float("nan"), dtype=torch.float64, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    st = call(x.data_ptr(), y.data_ptr(), nP, aslm, slm, out.data_ptr(), stream)
+    assert st == tr._lib.TR_OK, tr.lib.tr_last_error(None)
+    d, scale = numpy_dot(xh, yh, nP, aslm, slm)
+    nS = 1000
+    st = call(x.data_ptr(), y.data_ptr(), nS, aslm, slm, out.data_ptr() + 8, stream)
+    assert st == tr._lib.TR_OK, tr.lib.tr_last_error(None)
+    got = out.cpu().numpy()
+    assert abs(got[0] - d) <= 1e-14 * scale
+    ds, scale_s = numpy_dot(xh[:nS * aslm], yh[:nS * aslm], nS, aslm, slm)
+    assert abs(got[1] - ds) <= 1e-14 * scale_s
+    del x, y
+    torch.cuda.empty_cache()

@@ -1,6 +1,18 @@
 // Config parser (see config.h).
+//
+// The keys of radiation.cfg are described by one table (kKeys): the prefix
+// that selects the key, the type of its value, whether it belongs to the
+// global part of the file or to a [region r] section, and the field that
+// receives it.  A line is matched against the prefixes in table order, the
+// way the reference selects its branch (Config.cpp:20-112); the value after
+// '=' is parsed like the reference's sscanf patterns ("key = %d", "key = %lf":
+// blanks optional around '=', leading blanks before the number, anything
+// after the number ignored), and a path takes the rest of the line after
+// "key = ".  Lines that match no key are kept as additive key/value pairs.
 #include "config.h"
 
+#include <cctype>
+#include <cerrno>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -8,100 +20,143 @@
 
 namespace transfer {
 
-static std::string trim(const std::string &s) {
+namespace {
+
+enum class Kind { Int, Real, Path, Count };
+enum class Scope { Global, Region };
+
+// One recognised key.  `field` names the Config member written (see apply()).
+struct KeySpec {
+    const char *prefix;   // selects the key (prefix match, like strncmp)
+    const char *name;     // the key as it appears in messages
+    Kind kind;
+    Scope scope;
+    int field;
+};
+
+enum Field { F_KAPPA, F_IP, F_MESH, F_OUT, F_NREG, F_MAXK, F_DEV, F_SOLTYPE, F_DUMP, F_PREC };
+
+// Order matters only where one prefix is a prefix of another line's key
+// (none of these are); it follows the reference's branch order.
+const KeySpec kKeys[] = {
+    {"kappa", "kappa", Kind::Real, Scope::Region, F_KAPPA},
+    {"Ip", "Ip", Kind::Real, Scope::Region, F_IP},
+    {"meshfile = ", "meshfile", Kind::Path, Scope::Global, F_MESH},
+    {"outfile = ", "outfile", Kind::Path, Scope::Global, F_OUT},
+    {"numregs", "numregs", Kind::Count, Scope::Global, F_NREG},
+    {"angorder", "angorder", Kind::Int, Scope::Global, F_MAXK},
+    {"device", "device", Kind::Int, Scope::Global, F_DEV},
+    {"soltype", "soltype", Kind::Int, Scope::Global, F_SOLTYPE},
+    {"dump", "dump", Kind::Int, Scope::Global, F_DUMP},
+    {"precondition", "precondition", Kind::Int, Scope::Global, F_PREC},
+};
+
+const long kMaxRegions = 1000000;
+
+std::string trim(const std::string &s) {
     size_t a = s.find_first_not_of(" \t\r\n"), b = s.find_last_not_of(" \t\r\n");
     return a == std::string::npos ? std::string() : s.substr(a, b - a + 1);
 }
 
+// After the key's prefix: optional blanks, '=', then the text of the value
+// (blanks before it are left for strtod/strtol, which skip them).
+const char *after_equals(const char *p) {
+    while (*p && std::isspace(static_cast<unsigned char>(*p))) p++;
+    return *p == '=' ? p + 1 : nullptr;
+}
+
+}  // namespace
+
 Config::Config(const char *cfgfile) {
     FILE *f = std::fopen(cfgfile, "r");
-    if (!f) throw ConfigError(std::string("failed to open file `") + cfgfile + "'");
+    if (!f) throw ConfigError(std::string("cannot open configuration file ") + cfgfile);
     char buf[1024];
-    int line = 0, rid = -1;
-    auto die = [&](const std::string &msg) {
+    int line = 0, section = -1;
+    auto fail = [&](const std::string &msg) {
         std::fclose(f);
         std::ostringstream os;
-        os << cfgfile << ":" << line << ": " << msg;
+        os << cfgfile << ", line " << line << ": " << msg;
         throw ConfigError(os.str());
     };
-    auto strip_nl = [](char *b) {
-        size_t n = std::strlen(b);
-        while (n && (b[n - 1] == '\n' || b[n - 1] == '\r')) b[--n] = 0;
+
+    // parse the value of `k` from `text` (the line after the prefix) into
+    // the field; returns false when the line does not hold a value of the
+    // key's type
+    auto apply = [&](const KeySpec &k, const char *text) -> bool {
+        if (k.kind == Kind::Path) {
+            std::string v(text);
+            while (!v.empty() && (v.back() == '\n' || v.back() == '\r')) v.pop_back();
+            (k.field == F_MESH ? meshfn_ : outfn_) = v;
+            return true;
+        }
+        const char *val = after_equals(text);
+        if (!val) return false;
+        char *end = nullptr;
+        errno = 0;
+        if (k.kind == Kind::Real) {
+            double x = std::strtod(val, &end);
+            if (end == val) return false;
+            (k.field == F_KAPPA ? kappa_ : Ip_)[section] = x;
+            return true;
+        }
+        long x = std::strtol(val, &end, 10);
+        if (end == val || errno == ERANGE) return false;
+        switch (k.field) {
+            case F_NREG:
+                if (x < 0 || x > kMaxRegions)
+                    fail("numregs = " + std::to_string(x) + " is outside 0.." + std::to_string(kMaxRegions));
+                nreg_ = static_cast<int>(x);
+                kappa_.assign(nreg_ + 1, 0.0);
+                Ip_.assign(nreg_ + 1, 0.0);
+                region_extra_.assign(nreg_ + 1, std::map<std::string, std::string>());
+                break;
+            case F_MAXK: maxk_ = static_cast<int>(x); break;
+            case F_DEV: dev_ = static_cast<int>(x); break;
+            case F_SOLTYPE: soltype_ = static_cast<int>(x); break;
+            case F_DUMP: dump_ = static_cast<int>(x); break;
+            case F_PREC: prec_ = static_cast<int>(x); break;
+        }
+        return true;
     };
+
     while (std::fgets(buf, sizeof buf, f)) {
         line++;
         if (buf[0] == '#' || buf[0] == '\n') continue;
         if (buf[0] == '[') {
-            if (std::sscanf(buf, "[region %d]", &rid) != 1) die("scanf failed to parse region section");
-            if (nreg_ < 0) die("section appeared before numregs was set");
-            if (rid > nreg_ || rid < 0) die("region id is out of bounds");
+            int r = 0;
+            if (std::sscanf(buf, "[region %d]", &r) != 1)
+                fail("a section header must read [region <number>]");
+            if (nreg_ < 0) fail("[region " + std::to_string(r) + "] comes before numregs");
+            if (r < 0 || r > nreg_)
+                fail("[region " + std::to_string(r) + "] is outside 0..numregs = " + std::to_string(nreg_));
+            section = r;
             continue;
         }
-        if (!std::strncmp(buf, "kappa", 5)) {
-            if (rid < 0) die("kappa parameter outside section");
-            if (std::sscanf(buf, "kappa = %lf", &kappa_[rid]) != 1) die("scanf failed to parse kappa parameter");
+        const KeySpec *key = nullptr;
+        for (const KeySpec &k : kKeys)
+            if (!std::strncmp(buf, k.prefix, std::strlen(k.prefix))) {
+                key = &k;
+                break;
+            }
+        if (key) {
+            const std::string name(key->name);
+            if (key->scope == Scope::Region && section < 0)
+                fail("'" + name + "' belongs in a [region r] section");
+            if (key->scope == Scope::Global && section >= 0)
+                fail("'" + name + "' is a global key but appears in [region " + std::to_string(section) + "]");
+            if (!apply(*key, buf + std::strlen(key->prefix)))
+                fail("'" + name + "' needs a " + (key->kind == Kind::Real ? "number" : "whole number") +
+                     " after '=': " + trim(buf));
             continue;
         }
-        if (!std::strncmp(buf, "Ip", 2)) {
-            if (rid < 0) die("Ip parameter outside section");
-            if (std::sscanf(buf, "Ip = %lf", &Ip_[rid]) != 1) die("scanf failed to parse Ip parameter");
-            continue;
-        }
-        if (!std::strncmp(buf, "meshfile = ", 11)) {
-            if (rid >= 0) die("meshfile parameter in section");
-            strip_nl(buf);
-            meshfn_ = std::string(buf + 11);
-            continue;
-        }
-        if (!std::strncmp(buf, "outfile = ", 10)) {
-            if (rid >= 0) die("outfile parameter in section");
-            strip_nl(buf);
-            outfn_ = std::string(buf + 10);
-            continue;
-        }
-        if (!std::strncmp(buf, "numregs", 7)) {
-            if (rid >= 0) die("numregs parameter in section");
-            if (std::sscanf(buf, "numregs = %d", &nreg_) != 1) die("scanf failed to parse numregs parameter");
-            if (nreg_ < 0 || nreg_ > 1000000) die("numregs out of range");
-            kappa_.assign(nreg_ + 1, 0.0);
-            Ip_.assign(nreg_ + 1, 0.0);
-            region_extra_.assign(nreg_ + 1, std::map<std::string, std::string>());
-            continue;
-        }
-        if (!std::strncmp(buf, "angorder", 8)) {
-            if (rid >= 0) die("angorder parameter in section");
-            if (std::sscanf(buf, "angorder = %d", &maxk_) != 1) die("scanf failed to parse angorder parameter");
-            continue;
-        }
-        if (!std::strncmp(buf, "device", 6)) {
-            if (rid >= 0) die("device parameter in section");
-            if (std::sscanf(buf, "device = %d", &dev_) != 1) die("scanf failed to parse device parameter");
-            continue;
-        }
-        if (!std::strncmp(buf, "soltype", 7)) {
-            if (rid >= 0) die("soltype parameter in section");
-            if (std::sscanf(buf, "soltype = %d", &soltype_) != 1) die("scanf failed to parse soltype parameter");
-            continue;
-        }
-        if (!std::strncmp(buf, "dump", 4)) {
-            if (rid >= 0) die("dump parameter in section");
-            if (std::sscanf(buf, "dump = %d", &dump_) != 1) die("scanf failed to parse dump parameter");
-            continue;
-        }
-        if (!std::strncmp(buf, "precondition", 12)) {
-            if (rid >= 0) die("precondition parameter in section");
-            if (std::sscanf(buf, "precondition = %d", &prec_) != 1)
-                die("scanf failed to parse precondition parameter");
-            continue;
-        }
-        // additive "key = value" lines (silently ignored by the reference)
+        // additive "key = value" lines (the reference skips them)
         std::string s(buf);
         size_t eq = s.find('=');
         if (eq == std::string::npos) continue;
-        std::string key = trim(s.substr(0, eq)), val = trim(s.substr(eq + 1));
-        if (key.empty()) continue;
-        if (rid >= 0) region_extra_[rid][key] = val;
-        else extra_[key] = val;
+        std::string k = trim(s.substr(0, eq)), v = trim(s.substr(eq + 1));
+        if (k.empty()) continue;
+        if (section >= 0) region_extra_[section][k] = v;
+        else extra_[k] = v;
     }
     std::fclose(f);
 }
@@ -115,7 +170,7 @@ double Config::get_double(const std::string &key, double dflt) const {
     if (it == extra_.end()) return dflt;
     char *end = nullptr;
     double v = std::strtod(it->second.c_str(), &end);
-    if (end == it->second.c_str()) throw ConfigError("bad numeric value for " + key);
+    if (end == it->second.c_str()) throw ConfigError("'" + key + "' is not a number: " + it->second);
     return v;
 }
 int Config::get_int(const std::string &key, int dflt) const {
@@ -123,7 +178,7 @@ int Config::get_int(const std::string &key, int dflt) const {
     if (it == extra_.end()) return dflt;
     char *end = nullptr;
     long v = std::strtol(it->second.c_str(), &end, 10);
-    if (end == it->second.c_str()) throw ConfigError("bad integer value for " + key);
+    if (end == it->second.c_str()) throw ConfigError("'" + key + "' is not a whole number: " + it->second);
     return static_cast<int>(v);
 }
 bool Config::region_has(int region, const std::string &key) const {
@@ -135,7 +190,8 @@ double Config::region_double(int region, const std::string &key, double dflt) co
     const std::string &s = region_extra_[region].at(key);
     char *end = nullptr;
     double v = std::strtod(s.c_str(), &end);
-    if (end == s.c_str()) throw ConfigError("bad numeric value for " + key);
+    if (end == s.c_str())
+        throw ConfigError("'" + key + "' of [region " + std::to_string(region) + "] is not a number: " + s);
     return v;
 }
 

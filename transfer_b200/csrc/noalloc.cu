@@ -23,12 +23,14 @@
 //   - two calls whose kernels overlap on the GPU (other streams, other host
 //     threads) race on the array and may return wrong sums: order them.
 // In host code g_dot_scratch names a host-side stand-in, not device memory,
-// so the host never passes it to a kernel: the first call on each device
-// (with that device current) asks cudaGetSymbolAddress for the device
-// address and keeps it.  That first call therefore does set-up work and
-// should come before any stream capture on that device.
-#include <atomic>
-#include <mutex>
+// so the host never passes it to a kernel: every call asks
+// cudaGetSymbolAddress, with the caller's device current, for the array's
+// device address in the current context.  The first call on a device loads
+// this library's module there (set-up work), so that first call should come
+// before any stream capture on that device.  Because the address is looked
+// up again on each call, a cudaDeviceReset, or another CUDA context made
+// current on the same device, between two calls leaves no stale address
+// behind; the array's contents start at zero again in the new context.
 #include <string>
 
 #include "internal.h"
@@ -42,7 +44,6 @@ constexpr int kDotNoAllocPerThread = 64;                           // entries pe
 constexpr size_t kDotNoAllocChunk = size_t(kBlock) * kDotNoAllocPerThread;  // entries per block
 constexpr int kDotNoAllocMaxBlocks = 2048;
 constexpr size_t kDotNoAllocMaxEntries = kDotNoAllocChunk * kDotNoAllocMaxBlocks;  // 33,554,432
-constexpr int kMaxDevices = 64;
 
 // [0, kDotNoAllocMaxBlocks): block partials; slot kDotNoAllocMaxBlocks: the
 // arrival ticket (an unsigned int in the first 4 bytes); the rest pads to 256 B.
@@ -50,37 +51,34 @@ static __device__ __align__(256) double g_dot_scratch[kDotNoAllocMaxBlocks + 32]
 
 // Block b sums the entries [b * chunk, (b + 1) * chunk) with lm < slm; the
 // partition depends only on n, so the result is the same bits on any GPU.
-__global__ void __launch_bounds__(kBlock) k_dot_noalloc(size_t n, uint32_t aslm, uint32_t slm,
+// n <= kDotNoAllocMaxEntries < 2^32, so indices are 32-bit; each thread
+// finds its column (lm) once and steps it by kBlock modulo aslm.
+__global__ void __launch_bounds__(kBlock) k_dot_noalloc(uint32_t n, uint32_t aslm, uint32_t slm,
                                                         const double *__restrict__ x, const double *__restrict__ y,
                                                         double *partials, unsigned int *ticket, double *out) {
-    const size_t base = blockIdx.x * kDotNoAllocChunk + threadIdx.x;
+    uint32_t i = blockIdx.x * static_cast<uint32_t>(kDotNoAllocChunk) + threadIdx.x;
+    uint32_t lm = i % aslm;
+    const uint32_t step = kBlock % aslm;
     double acc = 0.0;
 #pragma unroll 8
     for (int k = 0; k < kDotNoAllocPerThread; ++k) {
-        const size_t i = base + static_cast<size_t>(k) * kBlock;
-        if (i < n && static_cast<uint32_t>(i % aslm) < slm) acc = fma(__ldg(x + i), __ldg(y + i), acc);
+        if (i < n && lm < slm) acc = fma(__ldg(x + i), __ldg(y + i), acc);
+        i += kBlock;
+        lm += step;
+        if (lm >= aslm) lm -= aslm;
     }
     double v[1] = {acc}, tot[1];
     if (grid_reduce<1>(v, partials, ticket, tot) && threadIdx.x == 0) *out = tot[0];
 }
 
-static std::mutex g_setup_mutex;
-static std::atomic<double *> g_scratch_addr[kMaxDevices];
-
-// Device address of g_dot_scratch on the current device (looked up once).
-static tr_status scratch_address(int dev, double **addr) {
-    double *p = g_scratch_addr[dev].load(std::memory_order_acquire);
-    if (!p) {
-        std::lock_guard<std::mutex> lock(g_setup_mutex);
-        p = g_scratch_addr[dev].load(std::memory_order_relaxed);
-        if (!p) {
-            cudaError_t e = cudaGetSymbolAddress(reinterpret_cast<void **>(&p), g_dot_scratch);
-            if (e != cudaSuccess)
-                return set_global_error(TR_ERR_CUDA, std::string("tr_dot_noalloc: cudaGetSymbolAddress: ") +
-                                                         cudaGetErrorString(e));
-            g_scratch_addr[dev].store(p, std::memory_order_release);
-        }
-    }
+// Device address of g_dot_scratch in the current context of the current
+// device (looked up on every call: see the header comment).
+static tr_status scratch_address(double **addr) {
+    double *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(reinterpret_cast<void **>(&p), g_dot_scratch);
+    if (e != cudaSuccess || !p)
+        return set_global_error(TR_ERR_CUDA, std::string("tr_dot_noalloc: cudaGetSymbolAddress: ") +
+                                                 cudaGetErrorString(e));
     *addr = p;
     return TR_OK;
 }
@@ -126,18 +124,16 @@ extern "C" tr_status tr_dot_noalloc(const double *x, const double *y, uint32_t n
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess)
         return set_global_error(TR_ERR_NO_DEVICE, std::string("tr_dot_noalloc: ") + cudaGetErrorString(e));
-    if (dev < 0 || dev >= kMaxDevices)
-        return set_global_error(TR_ERR_UNSUPPORTED, "tr_dot_noalloc: device index beyond 63");
     tr_status st = check_device_ptr(x, dev, "x");
     if (st == TR_OK) st = check_device_ptr(y, dev, "y");
     if (st == TR_OK) st = check_device_ptr(out, dev, "out");
     if (st != TR_OK) return st;
     double *scratch = nullptr;
-    st = scratch_address(dev, &scratch);
+    st = scratch_address(&scratch);
     if (st != TR_OK) return st;
     const int grid = n == 0 ? 1 : static_cast<int>((n + kDotNoAllocChunk - 1) / kDotNoAllocChunk);
     unsigned int *ticket = reinterpret_cast<unsigned int *>(scratch + kDotNoAllocMaxBlocks);
-    k_dot_noalloc<<<grid, kBlock, 0, static_cast<cudaStream_t>(stream)>>>(n, aslm, slm, x, y, scratch, ticket, out);
+    k_dot_noalloc<<<grid, kBlock, 0, static_cast<cudaStream_t>(stream)>>>(static_cast<uint32_t>(n), aslm, slm, x, y, scratch, ticket, out);
     e = cudaGetLastError();
     if (e != cudaSuccess)
         return set_global_error(TR_ERR_CUDA, std::string("tr_dot_noalloc: launch: ") + cudaGetErrorString(e));
