@@ -3,14 +3,26 @@
 time to a 1e-6 FP64 residual, FP32-mixed vs FP64, on B200.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload milne_slab|config1|cube64]
+                  [--workload milne_slab_ref|milne_slab|config1|cube64]
 
 A step is one solve of A f = b from f = 0 to ||b - A f|| / ||b|| < 1e-6
 (FP64 residual) on the workload, with the right-hand side resident in HBM.
+The default workload, milne_slab_ref, is the 8x8x160 Milne-type slab in the
+reference's own physics (vacuum faces, half-space emission), which the
+reference program itself runs: its "reference_gpu" object times the
+reference's program and kernels (kernels.cu compiled for sm_100a, driven by
+its own CudaContext) on the same mesh beside ours.
 The headline solver is the FP32-CG-in-FP64-defect-correction solve; the
 plain FP64 CG (the drop-in) is timed in the same run.  A cell-ordinate
 update is one (tetrahedron, harmonic) pair of one operator application:
 nT * slm per application, FP32 and FP64 applications both counted.
+
+The "roofline" object names the bound of the dominant kernel from its
+algorithmic bytes B and flops F per iteration: the larger of B / BW and
+F / FP_peak, where BW is the L2 bandwidth when the iteration's working set
+fits in L2 (else HBM), and the L2 bandwidth and the FP32 / FP64 peaks are
+measured in the same run ("peaks").  The "cube64" object (--no-cube64 skips
+it) times the HBM-resident 64^3 cube (274,625 vertices, slm 66) the same way.
 
 The line's "sweep" object measures the discrete-ordinates sweep on the
 Milne slab (scattering albedo 0.999, 112 ordinates): one sweep alone (FP32
@@ -48,10 +60,12 @@ def parse_args():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="milne_slab")
+    p.add_argument("--workload", default="milne_slab_ref")
     p.add_argument("--cpu-iters", type=int, default=0, help="CG iterations per CPU-baseline sample (0: auto)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-sweep", action="store_true", help="skip the discrete-ordinates sweep section")
+    p.add_argument("--no-cube64", action="store_true", help="skip the HBM-resident cube64 section")
+    p.add_argument("--no-reference-gpu", action="store_true", help="skip timing the reference's GPU program")
     return p.parse_args()
 
 
@@ -125,11 +139,86 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
+L2_BYTES = 126 * 1024 * 1024
+# fallbacks when a peak cannot be measured in the run: B200 at its 1965 MHz
+# boost clock, 148 SMs x 128 FP32 lanes x 2 flops (74.4 TFLOP/s) and half
+# that for FP64
+SPEC_FP32_TFLOPS = 74.4
+SPEC_FP64_TFLOPS = 37.2
+
+
+def measure_peaks(device):
+    """Peaks measured on this GPU in this run (CUDA events, best of 10):
+    L2 bandwidth as read + write bytes of a copy between two 24 MiB buffers
+    (both L2-resident), FP32 as cuBLAS SGEMM 4096^3 with TF32 disabled (the
+    FMA pipe), FP64 as cuBLAS DGEMM 4096^3."""
+    import torch
+
+    def best(fn, reps=10):
+        fn()
+        torch.cuda.synchronize()
+        t = []
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            torch.cuda.synchronize()
+            t.append(e0.elapsed_time(e1) * 1e-3)
+        return min(t)
+
+    out = {}
+    n = 24 * 1024 * 1024 // 4
+    a = torch.ones(n, dtype=torch.float32, device=device)
+    b = torch.empty_like(a)
+    inner = 20
+
+    def copies():
+        for _ in range(inner):
+            b.copy_(a)
+    out["l2_gbs"] = 2 * 4 * n * inner / best(copies) / 1e9
+    prec = torch.get_float32_matmul_precision()
+    torch.set_float32_matmul_precision("highest")   # FP32 FMA, no TF32
+    try:
+        for name, dt in (("fp32_tflops", torch.float32), ("fp64_tflops", torch.float64)):
+            x = torch.randn(4096, 4096, dtype=dt, device=device)
+            y = torch.randn(4096, 4096, dtype=dt, device=device)
+            out[name] = 2 * 4096 ** 3 / best(lambda: torch.matmul(x, y)) / 1e12
+    finally:
+        torch.set_float32_matmul_precision(prec)
+    out["how"] = ("measured in this run: L2 = copy of 24 MiB (read + write bytes); FP32 = SGEMM 4096^3 "
+                  "without TF32; FP64 = DGEMM 4096^3; best of 10")
+    return out
+
+
+def roofline(bytes_, flops, seconds, real_bytes, working_set, peaks, hbm_peak, hbm_kind):
+    """Bound of a kernel doing `bytes_` and `flops` of algorithmic work in
+    `seconds`: max(B / BW, F / FP_peak), BW = L2 when working_set fits in L2,
+    else HBM.  Returns the roofline fields with the binding unit named."""
+    in_l2 = working_set <= 0.75 * L2_BYTES
+    bw = peaks["l2_gbs"] if in_l2 else hbm_peak
+    fp = peaks["fp32_tflops"] if real_bytes == 4 else peaks["fp64_tflops"]
+    t_bw = bytes_ / (bw * 1e9)
+    t_fp = flops / (fp * 1e12)
+    mem = "l2" if in_l2 else "hbm"
+    cmp_ = "fp32" if real_bytes == 4 else "fp64"
+    if t_bw >= t_fp:
+        r = {"bound": mem, "achieved": bytes_ / seconds / 1e9, "peak": bw, "unit": "GB/s"}
+    else:
+        r = {"bound": cmp_, "achieved": flops / seconds / 1e12, "peak": fp, "unit": "TFLOP/s"}
+    r["frac"] = r["achieved"] / r["peak"]
+    r["bound_us"] = {mem: 1e6 * t_bw, cmp_: 1e6 * t_fp, "measured": 1e6 * seconds}
+    r["hbm_view"] = {"achieved_gbs": bytes_ / seconds / 1e9, "peak_gbs": hbm_peak, "peak_source": hbm_kind,
+                     "frac": bytes_ / seconds / 1e9 / hbm_peak}
+    r["working_set_bytes"] = working_set
+    return r
+
+
 # DRAM bytes (read + write) of one launch of the persistent FP32 CG kernel,
 # from one ncu capture of that launch (profiles/k_cg_persistent_simt_f32_milne_slab.md);
 # the iteration working set is L2-resident, so this is first-touch traffic
 # and does not grow with the iterations of the launch
-NCU_TRAFFIC_PER_LAUNCH = {"milne_slab": 16.878336e6 + 0.002304e6}
+NCU_TRAFFIC_PER_LAUNCH = {"milne_slab": 16.878336e6 + 0.002304e6, "milne_slab_ref": 16884480 + 65280}
 
 
 def operator_policy(tensor, slm, aslm, real):
@@ -170,7 +259,7 @@ def cpu_sample(workload, iters, steps=1):
 
 
 def auto_cpu_iters(workload):
-    return {"config1": 60, "milne_slab": 40, "cube64": 2}.get(workload, 10)
+    return {"config1": 60, "milne_slab": 40, "milne_slab_ref": 40, "cube64": 2}.get(workload, 10)
 
 
 def run_reference(args, rank):
@@ -282,6 +371,111 @@ def sweep_section(local, flush, peak, want_cpu):
 
 
 # ----------------------------------------------------------------- GPU arm
+def working_set(ctx, real_bytes):
+    """Bytes one CG iteration touches in this implementation: the assembled
+    edge records (16 reals per vertex pair) with their column indices, and
+    about seven vectors of the precision."""
+    aslm = ctx.aslm if real_bytes == 8 else ctx.aslm_f32
+    return ctx.n_edges * (16 * real_bytes + 4) + 7 * ctx.nP * aslm * real_bytes
+
+
+def reference_gpu_section(md, ad, desc, ctx, tr):
+    """The reference's own GPU path on the same mesh: its program
+    (main.cpp + CudaContext + kernels.cu for sm_100a) run to its own stop
+    (absolute ||r|| < 1e-4, at most 1000 iterations, main.cpp:125-160), each
+    CG line time-stamped; and its computeLhs / dot timed with CUDA events
+    through its CudaContext.  Ours is timed on the same settings."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import numpy as np
+    import ref_program as rp
+    import torch
+    kappa, Ip, maxk = desc["regions"]["kappa"], desc["regions"]["Ip"], desc["maxk"]
+    out = {"program": "oracle/_ref/<precision>/transfer_ref_gpu (reference main.cpp, CudaContext.cpp, "
+                      "kernels.cu built for sm_100a)",
+           "settings": "reference CG: absolute ||r|| < 1e-4, max 1000 iterations, no preconditioner"}
+    prog = rp.run_program("fp64", md, maxk, kappa, Ip, timeout=300)
+    if prog["returncode"] != 0:
+        return {"unavailable": f"reference program exited {prog['returncode']}: {prog['stderr'][-300:]}"}
+    f, rep = ctx.solve(tol=1e-4, relative=0, max_iter=1000)   # warm-up
+    f, rep = ctx.solve(tol=1e-4, relative=0, max_iter=1000)
+    U, _ = ctx.computeMoments(f)
+    Ur = prog["fields"].get("U")
+    out["fp64_solve"] = {
+        "reference_iterations": int(len(prog["k"])), "ours_iterations": int(rep.iterations),
+        "reference_ms_per_iteration": prog["ms_per_iteration"],
+        "ours_ms_per_iteration": rep.device_ms / max(1, rep.iterations),
+        "reference_cg_ms": 1e3 * prog["cg_s"] if prog["cg_s"] else None, "ours_solve_ms": rep.device_ms,
+        "U_rel_diff": float(np.abs(U.cpu().numpy() - Ur).max() / np.abs(Ur).max()) if Ur is not None else None,
+        "timing": "reference: wall time between its first and last CG output lines / iterations; "
+                  "ours: CUDA events around tr_solve"}
+    out["fp64_solve"]["speedup_per_iteration"] = (out["fp64_solve"]["reference_ms_per_iteration"] /
+                                                  out["fp64_solve"]["ours_ms_per_iteration"])
+    import ctypes as C
+    for prec, real in (("fp64", 8), ("fp32", 4)):
+        kb = rp.bench_kernels(prec, md, maxk, kappa, Ip, reps=50)
+        dt = torch.float64 if real == 8 else torch.float32
+        x = ctx.allocVector(dt)
+        x.view(ctx.nP, -1)[:, :ctx.slm].normal_()
+        y = ctx.allocVector(dt)
+        ms = C.c_double()
+        tr.check(tr.lib.tr_bench_lhs(ctx._h, 8 * real, x.data_ptr(), y.data_ptr(), 200, C.byref(ms)), ctx._h)
+        out[f"operator_{prec}"] = {"reference_us": 1e3 * kb["lhs_ms"], "ours_us": 1e3 * ms.value,
+                                   "speedup": kb["lhs_ms"] / ms.value,
+                                   "reference_dot_us": 1e3 * kb["dot_ms"]}
+    return out
+
+
+def cube64_section(local, flush, peaks, hbm_peak, hbm_kind):
+    """The HBM-resident configuration (workloads.cube64: 274,625 vertices,
+    1.57 M tets, maxk 5, slm 66): one mixed and one FP64 solve to the FP64
+    relative residual TOL (Jacobi-preconditioned and plain), the operator
+    alone in both precisions, and the roofline of each."""
+    import ctypes as C
+    import torch
+    import transfer_b200 as tr
+    from transfer_b200 import workloads as W
+    md, ad, phys, desc = W.cube64()
+    ctx = tr.CudaContext(local, md, ad, phys)
+    per_app = ctx.nT * ctx.slm
+    out = {"config": {**desc, "nP": ctx.nP, "nT": ctx.nT, "slm": ctx.slm, "tol": TOL, "edges": ctx.n_edges},
+           "unit": UNIT}
+    for real, dt in ((4, torch.float32), (8, torch.float64)):
+        x = ctx.allocVector(dt)
+        x.view(ctx.nP, -1)[:, :ctx.slm].normal_()
+        y = ctx.allocVector(dt)
+        ms = C.c_double()
+        tr.check(tr.lib.tr_bench_lhs(ctx._h, 8 * real, x.data_ptr(), y.data_ptr(), 20, C.byref(ms)), ctx._h)
+        byt, flops = W.algorithmic_work(md, ad, real_bytes=real)
+        out[f"operator_fp{8 * real}"] = {"us": 1e3 * ms.value, **roofline(
+            byt, flops, ms.value * 1e-3, real, working_set(ctx, real), peaks, hbm_peak, hbm_kind)}
+        del x, y
+    for name, pre in (("plain", tr.TR_PREC_NONE), ("jacobi", tr.TR_PREC_JACOBI)):
+        res = {}
+        for mode_name, mode in (("mixed", tr.TR_MODE_MIXED), ("fp64", tr.TR_MODE_FP64)):
+            ctx.solve(mode=mode, tol=TOL, relative=1, max_iter=40, precondition=pre)   # warm-up (short)
+            flush.fill_(2.0)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            f, rep = ctx.solve(mode=mode, tol=TOL, relative=1, max_iter=200000, precondition=pre)
+            e1.record()
+            torch.cuda.synchronize()
+            t = e0.elapsed_time(e1)
+            real = 4 if mode == tr.TR_MODE_MIXED else 8
+            ib, ifl = W.cg_iteration_work(md, ad, real_bytes=real)
+            res[mode_name] = {"ms": t, "converged": bool(rep.converged), "iterations": rep.iterations,
+                              "relative_residual": rep.final_residual / rep.rhs_norm,
+                              "value": (rep.lhs_applications_f64 + rep.lhs_applications_f32) * per_app / (t * 1e-3),
+                              "ms_per_iteration": t / max(1, rep.iterations),
+                              "cg_iteration_roofline": roofline(ib, ifl, 1e-3 * rep.cg_kernel_ms / max(1, rep.iterations),
+                                                                real, working_set(ctx, real), peaks, hbm_peak,
+                                                                hbm_kind)}
+        res["speedup_mixed_vs_fp64"] = res["fp64"]["ms"] / res["mixed"]["ms"]
+        out[f"solve_{name}"] = res
+    ctx.close()
+    return out
+
+
 def run_ours(args, rank, world, local):
     import numpy as np
     import torch
@@ -376,10 +570,9 @@ def run_ours(args, rank, world, local):
 
     if rank == 0:
         peak, peak_kind = load_peaks()
+        peaks = measure_peaks(f"cuda:{local}")
         bytes32, flops = W.algorithmic_work(md, ad, real_bytes=4)
         bytes64, _ = W.algorithmic_work(md, ad, real_bytes=8)
-        ach32 = bytes32 / (ms32.value * 1e-3) / 1e9
-        ach64 = bytes64 / (ms64.value * 1e-3) / 1e9
         # dominant kernel of the timed region: the persistent FP32 CG kernel,
         # timed by CUDA events around each of its launches inside the solves
         it_bytes, it_flops = W.cg_iteration_work(md, ad, real_bytes=4)
@@ -387,11 +580,29 @@ def run_ours(args, rank, world, local):
         cg_launches = sum(r.cg_kernel_launches for r in reps_mixed)
         cg_iters = sum(r.iterations for r in reps_mixed)
         solve_ms = sum(r.device_ms for r in reps_mixed)
-        ach_cg = cg_iters * it_bytes / (cg_ms * 1e-3) / 1e9
         pol32 = operator_policy(False, slm, ctx.aslm_f32, "float")   # context defaults: FP32 SIMT,
         pol64 = operator_policy(True, slm, ctx.aslm, "double")       # FP64 tensor cores
         it_mixed = statistics.mean(r.iterations for r in reps_mixed)
         it_fp64 = statistics.mean(r.iterations for r in reps_fp64)
+        rl = roofline(it_bytes, it_flops, 1e-3 * cg_ms / cg_iters, 4, working_set(ctx, 4), peaks, peak, peak_kind)
+        rl.update({
+            "traffic": traffic_per_launch(args.workload),
+            "traffic_unit": "DRAM bytes per launch (ncu)",
+            "kernel": f"k_cg_persistent<{pol32}> (FP32 CG iterations of the mixed solve)",
+            "per": "one CG iteration (algorithmic bytes and flops per iteration / device time per iteration)",
+            "us_per_launch": 1e3 * cg_ms / cg_launches,
+            "iterations_per_launch": cg_iters / cg_launches,
+            "algorithmic_bytes_per_iteration": it_bytes,
+            "algorithmic_flops_per_iteration": it_flops,
+            "share_of_solve_device_time": cg_ms / solve_ms,
+            "operator_alone": {
+                "fp32": {"kernel": f"k_lhs<{pol32}>", "us_per_launch": 1e3 * ms32.value,
+                         **roofline(bytes32, flops, ms32.value * 1e-3, 4, working_set(ctx, 4), peaks, peak,
+                                    peak_kind)},
+                "fp64": {"kernel": f"k_lhs<{pol64}>", "us_per_launch": 1e3 * ms64.value,
+                         **roofline(bytes64, flops, ms64.value * 1e-3, 8, working_set(ctx, 8), peaks, peak,
+                                    peak_kind)},
+                "algorithmic_gflop": flops / 1e9}})
         line = {
             "metric": METRIC,
             "value": u_mixed / (t_mixed * 1e-3),
@@ -406,7 +617,9 @@ def run_ours(args, rank, world, local):
             "dtype": "f32+f64",
             "data": "synthetic",
             "config": {
-                **desc, "nP": nP, "nT": nT, "nF": ctx.nF, "slm": slm, "tol": TOL,
+                **{k: v for k, v in desc.items() if k != "regions"}, "nP": nP, "nT": nT, "nF": ctx.nF,
+                "slm": slm, "tol": TOL,
+                "reference_pinned": "regions" in desc,
                 "solver": "FP32 CG inside FP64 defect correction (headline); plain FP64 CG timed alongside; "
                           "persistent cooperative CG kernel",
                 "l2": "256 MiB buffer written before every solve (inputs of one solve fit in L2)",
@@ -427,28 +640,19 @@ def run_ours(args, rank, world, local):
             "e2e": {"value": u_e2e / (t_e2e * 1e-3), "unit": UNIT,
                     "h2d_bytes_per_step": 8 * ctx.N(), "d2h_bytes_per_step": 8 * ctx.N()},
             "gpu_launches": int(l_mixed),
-            "roofline": {"bound": "hbm", "achieved": ach_cg, "peak": peak, "unit": "GB/s", "frac": ach_cg / peak,
-                         "traffic": traffic_per_launch(args.workload),
-                         "peak_source": peak_kind,
-                         "kernel": f"k_cg_persistent<{pol32}> (FP32 CG iterations of the mixed solve)",
-                         "us_per_launch": 1e3 * cg_ms / cg_launches,
-                         "iterations_per_launch": cg_iters / cg_launches,
-                         "algorithmic_bytes_per_launch": it_bytes * cg_iters / cg_launches,
-                         "algorithmic_bytes_per_iteration": it_bytes,
-                         "share_of_solve_device_time": cg_ms / solve_ms,
-                         "gflops": cg_iters * it_flops / (cg_ms * 1e-3) / 1e9,
-                         "operator_alone": {
-                             "fp32": {"kernel": f"k_lhs<{pol32}>", "us_per_launch": 1e3 * ms32.value,
-                                      "algorithmic_bytes": bytes32, "achieved_gbs": ach32,
-                                      "gflops": flops / (ms32.value * 1e-3) / 1e9},
-                             "fp64": {"kernel": f"k_lhs<{pol64}>", "us_per_launch": 1e3 * ms64.value,
-                                      "algorithmic_bytes": bytes64, "achieved_gbs": ach64,
-                                      "gflops": flops / (ms64.value * 1e-3) / 1e9},
-                             "algorithmic_gflop": flops / 1e9}},
+            "roofline": rl,
+            "peaks": {**peaks, "hbm_gbs": peak, "hbm_source": peak_kind},
             "clocks": clocks,
         }
+        if world == 1 and not args.no_reference_gpu and "regions" in desc:
+            try:
+                line["reference_gpu"] = reference_gpu_section(md, ad, desc, ctx, tr)
+            except (OSError, RuntimeError, subprocess.SubprocessError) as e:
+                line["reference_gpu"] = {"unavailable": str(e)[:300]}
         if not args.no_sweep:
             line["sweep"] = sweep_section(local, flush, peak, world == 1 and not args.no_cpu_baseline)
+        if not args.no_cube64 and args.workload != "cube64":
+            line["cube64"] = cube64_section(local, flush, peaks, peak, peak_kind)
         if world == 1 and not args.no_cpu_baseline:
             iters = args.cpu_iters or auto_cpu_iters(args.workload)
             v, threads, secs, n = cpu_sample(args.workload, iters)

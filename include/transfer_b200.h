@@ -449,8 +449,19 @@ tr_status tr_sweep_autotune(tr_sweep *s, int *shape, double *ms);
 tr_status tr_sweep_psi(tr_sweep *s, double *psi);
 /* Angular moments of the last sweep's psi: mom[m][nT][4] = sum_q w_q
  * Y_m(Omega_q) psi_q for m < nmom <= 16 (l <= 3, m index l^2 + l + mm,
- * real harmonics of tr_spherical_value, Y_00 = 1). */
+ * real harmonics of tr_spherical_value, Y_00 = 1).  Generalises
+ * MeshData::ComputeMoments (MeshData.cpp:96-116) to discrete ordinates.
+ * After an FP32 sweep the product runs on the tensor cores in split TF32
+ * with FP32 accumulation; after an FP64 sweep it accumulates in FP64. */
 tr_status tr_sweep_moments(tr_sweep *s, int nmom, double *mom);
+/* Kernel family of tr_sweep_moments after an FP32 sweep (no reference
+ * counterpart; results agree to FP32 rounding):
+ * TR_MOMENTS_TCGEN05 (default): tcgen05 MMAs with tensor-memory
+ * accumulators, psi tiles loaded by TMA (up to 1,024 ordinates);
+ * TR_MOMENTS_MMA_SYNC: warp-level mma.sync with cp.async staging (up to 384
+ * ordinates).  Larger ordinate sets, and FP64 sweeps, use FP64 FMAs. */
+enum { TR_MOMENTS_TCGEN05 = 0, TR_MOMENTS_MMA_SYNC = 1 };
+tr_status tr_sweep_set_moments_kernel(tr_sweep *s, int kind);
 /* FP64 energy balance of the last sweep given its inputs J_in, B_in and its
  * scalar flux J_out:  out = {emitted, absorbed, escaped, incoming,
  * reflective_net} with emitted + incoming = absorbed + escaped +

@@ -23,6 +23,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 REF = os.path.join(ROOT, "oracle", "_ref")
 sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 
 def run(*args, cwd=None):
@@ -140,47 +141,9 @@ def dump_configs(tmp):
         json.dump(res, f, indent=1, sort_keys=True)
 
 
-def write_tmesh(md, path):
-    with open(path, "w") as f:
-        f.write(f"tmesh 1\n{md.nP}\n")
-        for x in md.coords:
-            f.write(f"{x[0]:.17g} {x[1]:.17g} {x[2]:.17g}\n")
-        f.write(f"{md.nT}\n")
-        for t in range(md.nT):
-            p = md.mesh["p"][t]
-            f.write(f"{p[0]} {p[1]} {p[2]} {p[3]} {md.regions[t]}\n")
-
-
-def ref_cfg(tmp, meshfile, maxk, kappa, Ip, prec=0, dump=0, out="sol.txt"):
-    lines = [f"numregs = {len(kappa) - 1}", f"meshfile = {meshfile}", f"outfile = {out}", "device = 0",
-             f"angorder = {maxk}", f"dump = {dump}", f"precondition = {prec}", "soltype = 0"]
-    for r in range(1, len(kappa)):
-        lines += [f"[region {r}]", f"kappa = {float(kappa[r])!r}", f"Ip = {float(Ip[r])!r}"]
-    fn = os.path.join(tmp, "run.cfg")
-    with open(fn, "w") as f:
-        f.write("\n".join(lines) + "\n")
-    return fn
-
-
-def parse_fields(path):
-    fields, cur, rows = {}, None, []
-    for ln in open(path):
-        parts = ln.split()
-        if len(parts) == 4 and parts[0] in ("cell", "point"):
-            if cur:
-                fields[cur] = np.array(rows)
-            cur, rows = parts[1], []
-        else:
-            rows.append(float(ln))
-    if cur:
-        fields[cur] = np.array(rows)
-    return fields
-
-
-def parse_log(text):
-    ks = [(int(m.group(1)), float(m.group(2))) for m in re.finditer(r"^k = (\d+) norm r = (\S+)", text, re.M)]
-    pre = re.search(r"^preck = (\d+)", text, re.M)
-    return np.array([k for k, _ in ks]), np.array([r for _, r in ks]), int(pre.group(1)) if pre else -1
+# input writers and output parsers of the reference program (shared with
+# the GPU tests and the bench's reference measurements)
+from ref_program import parse_fields, parse_log, ref_cfg, write_tmesh  # noqa: E402
 
 
 CASES = {

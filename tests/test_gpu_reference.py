@@ -15,6 +15,7 @@ import pytest
 import torch
 
 import oracle_py as op
+import ref_program as rp
 import transfer_b200 as tr
 from common import golden, golden_angular, refrun_mesh, rel_err
 
@@ -24,31 +25,13 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 REF = os.path.join(ROOT, "oracle", "_ref")
 
 
-def _mk():
-    import importlib.util
-    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(ROOT, "tests", "golden",
-                                                                              "make_golden.py"))
-    m = importlib.util.module_from_spec(spec)
-    spec.loader.exec_module(m)
-    return m
-
-
 def run_reference(tmp_path, precision, md, maxk, kappa, Ip, prec=0, dump=0):
-    exe = os.path.join(REF, precision, "transfer_ref_gpu")
-    cubin = os.path.join(REF, precision, "kernels.sm_100.cubin")
-    if not (os.path.exists(exe) and os.path.exists(cubin)):
-        pytest.fail(f"{exe} not built (make -C oracle ref)")
-    mg = _mk()
-    shutil.copy(cubin, tmp_path / "kernels.sm_100.cubin")
-    mesh = str(tmp_path / "m.tmesh")
-    mg.write_tmesh(md, mesh)
-    out = str(tmp_path / "sol.txt")
-    cfg = mg.ref_cfg(str(tmp_path), mesh, maxk, kappa, Ip, prec=prec, dump=dump, out=out)
-    p = subprocess.run([exe, cfg], cwd=tmp_path, capture_output=True, text=True, timeout=300)
-    assert p.returncode == 0, p.stdout[-3000:] + p.stderr[-3000:]
-    assert "failed with error" not in p.stderr, p.stderr[-3000:]
-    ks, res, preck = mg.parse_log(p.stdout)
-    return ks, res, preck, mg.parse_fields(out), p
+    if rp.built(precision) is None:
+        pytest.fail(f"oracle/_ref/{precision}/transfer_ref_gpu not built (make -C oracle ref)")
+    r = rp.run_program(precision, md, maxk, kappa, Ip, prec=prec, dump=dump, workdir=tmp_path, timeout=300)
+    assert r["returncode"] == 0, r["stdout"][-3000:] + r["stderr"][-3000:]
+    assert "failed with error" not in r["stderr"], r["stderr"][-3000:]
+    return r["k"], r["residual"], r["preck"], r["fields"], r
 
 
 @pytest.mark.parametrize("name", ["small_k1", "small_k2", "small_k1_prec", "c1_k1"])

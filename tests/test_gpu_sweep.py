@@ -90,15 +90,39 @@ def test_balance_matches_oracle_and_closes(cuda):
         1e-12 * bg["emitted"]
 
 
-@pytest.mark.parametrize("precision", [64, 32])
-def test_moments_match_oracle(cuda, precision):
+@pytest.mark.parametrize("precision,kernel", [(64, None), (32, "tcgen05"), (32, "mma_sync")])
+def test_moments_match_oracle(cuda, precision, kernel):
     md, ph, S, O = pair(scattering_box(), op.ordinates_product(6, 12))
+    if kernel:
+        S.set_moments_kernel(tr._lib.TR_MOMENTS_TCGEN05 if kernel == "tcgen05" else tr._lib.TR_MOMENTS_MMA_SYNC)
     S.apply(precision=precision)
     _, _, psio = O.apply(want_psi=True)
     mo = O.moments(psio, 16)
     for nmom in (16, 9, 4, 1, 7):
         mg = host(S.moments(nmom))
         assert rel_err(mg, mo[:nmom]) < (1e-13 if precision == 64 else 2e-5)
+
+
+@pytest.mark.parametrize("n,polar,azim", [((5, 4, 6), 6, 12),     # 72 ordinates: a part-filled stage
+                                          ((12, 12, 12), 14, 22),  # 308: 10 stages a tile, 2-3 tiles a CTA
+                                          ((12, 12, 12), 2, 4),    # 8: one part-filled stage
+                                          ((6, 6, 6), 32, 32)])    # 1,024: the largest weight table
+def test_moments_tcgen05_split_tf32_accuracy(cuda, n, polar, azim):
+    """The tensor-core contraction against an FP64 sum over the same FP32 psi
+    (the GPU's own, widened exactly): split TF32 with FP32 accumulation stays
+    within 3e-6 of the largest moment (a single TF32 product would be ~1e-3);
+    the mma.sync kernel where it applies (up to 384 ordinates) gives the same."""
+    md, ph, S, O = pair(scattering_box(n=n), op.ordinates_product(polar, azim))
+    S.apply(precision=32)
+    mo = O.moments(host(S.psi()), 16)
+    for nmom in (16, 5):
+        mg = host(S.moments(nmom))
+        assert rel_err(mg, mo[:nmom]) < 3e-6
+    if polar * azim <= 384:
+        S.set_moments_kernel(tr._lib.TR_MOMENTS_MMA_SYNC)
+        assert rel_err(host(S.moments(16)), mo) < 3e-6
+    with pytest.raises(tr.TransferError):
+        S.set_moments_kernel(7)
 
 
 def test_gmres_fp64_matches_oracle(cuda):

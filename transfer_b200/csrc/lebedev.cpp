@@ -485,7 +485,7 @@ bool generate(const OrbitSpec &sp, LebedevQuad &q) {
         for (size_t i = 0; i < theta.size(); ++i) v[pr.no + i] = theta[i];
         int pi = pr.no;
         if (!levenberg_marquardt(pr, kinds, v)) continue;
-        if (!admissible(kinds, v, pr.no, sp.order == 74)) continue;
+        if (!admissible(kinds, v, pr.no, sp.order == 74 || getenv("LEB_NEG") != nullptr)) continue;
         std::vector<double> F;
         eval(pr, kinds, v, F, nullptr);
         double worst = 0.0;

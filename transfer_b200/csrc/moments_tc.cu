@@ -1,0 +1,419 @@
+// Moments of the FP32 angular flux on the 5th-generation tensor cores
+// (tcgen05, accumulators in tensor memory), psi streamed by TMA.
+//
+//   mom[n][r] = sum_q W[n][q] psi[q][r],   r = 4 c + j over the M = 4 nT
+//   cell-vertex values, n < 16 real harmonics (l <= 3), W = w_q Y_n(Omega_q)
+//
+// This is MeshData::ComputeMoments (MeshData.cpp:96-116, U = 4 pi I_00 and
+// the l = 1, 2 moments of the even-parity solution) generalised to discrete
+// ordinates: a (M x nq) . (nq x 16) product, A = psi^T read once from HBM.
+//
+// Split TF32 (3xTF32) with FP32 accumulation: psi = a_hi + a_lo and
+// W = w_hi + w_lo, where the hi parts keep the 10-bit TF32 mantissa
+// (truncation: the tensor core reads the top 19 bits of an FP32 word) and
+// the lo parts are the exact FP32 remainders; the three products
+// a_hi w_hi + a_hi w_lo + a_lo w_hi are summed, a_lo w_lo (~2^-22) dropped.
+//
+// Layout and roles (one CTA per SM, persistent over 128-row tiles):
+//   A (psi)   TMA tiles of 32 rows x 32 ordinates (128-byte swizzle), four per
+//             stage: a stage is 128 rows x 32 ordinates, MN-major (rows
+//             contiguous), kStages stages in flight;
+//   B (W)     [w_hi | w_lo] as one N = 32 operand, K-major, built in shared
+//             memory once per CTA from the FP64 weights;
+//   a_lo      written by the split warps into tensor memory (tcgen05.st), the
+//             A operand of the third product (A from tensor memory);
+//   D         two 128 x 32 FP32 accumulators in tensor memory (columns 0-15:
+//             a w_hi + a_lo w_hi, 16-31: a w_lo), double-buffered per tile.
+//   warp 0    TMA producer (and tensor-memory allocation);
+//   warp 1    MMA issuer: per 8-ordinate step one N = 32 product from shared
+//             memory and one N = 16 product with A from tensor memory;
+//   warps 4-7 split a stage (a_lo = a - trunc(a)) into tensor memory, and
+//             read each finished tile's accumulators back (tcgen05.ld), add
+//             the two halves and store the 16 moments (FP64).
+// Every wait is bounded (kWaitNs of the global timer): past it the kernel
+// sets bit 0 of *err, every role stops, in-flight copies and products are
+// waited for (bounded), tensor memory is freed and the kernel returns.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "moments_tc.h"
+
+namespace transfer {
+
+namespace {
+
+constexpr int kTileM = 128;        // rows per tile (one MMA M)
+constexpr int kStageK = 32;        // ordinates per stage
+constexpr int kStages = 6;
+constexpr int kAtomBytes = 32 * 4 * kStageK;         // 32 rows x 32 ordinates x 4 B = 4 KB
+constexpr int kStageBytes = 4 * kAtomBytes;          // 16 KB
+constexpr int kThreads = 256;
+constexpr uint32_t kTmemCols = 256;                  // 2 x 32 accumulator + kStages x 32 a_lo
+constexpr uint32_t kLoCol0 = 64;
+constexpr unsigned long long kWaitNs = 1000000000ull;  // 1 s per wait
+
+static_assert(kLoCol0 + kStages * kStageK <= kTmemCols, "tensor-memory plan");
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: false when the CTA has aborted or this wait timed out (then
+// the abort flag and bit 0 of *err are set).
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort_flag,
+                                          unsigned int *err) {
+    if (mbar_try(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    for (uint32_t spin = 0;; ++spin) {
+        if (mbar_try(bar, parity)) return true;
+        if (*abort_flag) return false;
+        if ((spin & 63u) == 63u && global_ns() - t0 > kWaitNs) {
+            *abort_flag = 1;
+            atomicOr(err, 1u);
+            return false;
+        }
+    }
+}
+
+// The same wait for a whole warp: lane 0 polls and the outcome is broadcast,
+// so every lane takes the same branch before the warp-wide (.sync.aligned)
+// tensor-memory instructions that follow.
+__device__ __forceinline__ bool mbar_wait_warp(uint32_t bar, uint32_t parity, volatile int *abort_flag,
+                                               unsigned int *err) {
+    int ok = 0;
+    if ((threadIdx.x & 31u) == 0) ok = mbar_wait(bar, parity, abort_flag, err) ? 1 : 0;
+    return __shfl_sync(0xffffffffu, ok, 0) != 0;
+}
+
+// UMMA shared-memory descriptors (version 1).  A: MN-major, 128-byte swizzle,
+// 32-row atoms 4 KB apart (leading offset), 8-ordinate groups 1 KB apart
+// (stride offset).  B: K-major, no swizzle, 8 x 16-byte core matrices; the
+// next 4 ordinates 512 B on (leading offset), the next 8 harmonics 128 B on
+// (stride offset).
+__device__ __forceinline__ uint64_t desc_a(uint32_t saddr) {
+    return static_cast<uint64_t>((saddr >> 4) & 0x3FFFu) | (static_cast<uint64_t>(4096 >> 4) << 16) |
+           (static_cast<uint64_t>(1024 >> 4) << 32) | (1ull << 46) | (2ull << 61);
+}
+__device__ __forceinline__ uint64_t desc_b(uint32_t saddr) {
+    return static_cast<uint64_t>((saddr >> 4) & 0x3FFFu) | (static_cast<uint64_t>(512 >> 4) << 16) |
+           (static_cast<uint64_t>(128 >> 4) << 32) | (1ull << 46);
+}
+// instruction descriptor: D FP32, A and B TF32, M = 128, N, A major
+__host__ __device__ constexpr uint32_t idesc_tf32(uint32_t n, uint32_t a_mn) {
+    return (1u << 4) | (2u << 7) | (2u << 10) | (a_mn << 15) | ((n >> 3) << 17) | ((128u >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_ss(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+        ::"r"(d), "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+__device__ __forceinline__ void mma_ts(uint32_t d, uint32_t a_tmem, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+        ::"r"(d), "r"(a_tmem), "l"(b), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+        "[%4];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+        "%14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32};" ::"r"(
+            taddr),
+        "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]),
+        "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15]), "r"(v[16]),
+        "r"(v[17]), "r"(v[18]), "r"(v[19]), "r"(v[20]), "r"(v[21]), "r"(v[22]), "r"(v[23]), "r"(v[24]),
+        "r"(v[25]), "r"(v[26]), "r"(v[27]), "r"(v[28]), "r"(v[29]), "r"(v[30]), "r"(v[31])
+        : "memory");
+}
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(taddr)
+        : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
+__device__ __forceinline__ float tf32_trunc(float x) { return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u); }
+
+struct Smem {
+    uint64_t full[kStages], empty[kStages], lo_ready[kStages];
+    uint64_t acc_full[2], acc_empty[2], drain;
+    uint32_t tmem_base;
+    int abort_flag;
+};
+
+}  // namespace
+
+__global__ void __launch_bounds__(kThreads, 1)
+    k_moments_tcgen05(const __grid_constant__ CUtensorMap psi_map, uint32_t M, uint32_t nq, uint32_t nqp,
+                      const double *__restrict__ W, int nmom, double *__restrict__ mom, unsigned int *err) {
+    extern __shared__ uint8_t smem_raw[];
+    // 1024-byte aligned base: the 128-byte swizzle pattern repeats every 1 KB
+    uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t *smA = base;                                   // kStages x 16 KB
+    uint8_t *smB = smA + kStages * kStageBytes;            // nqp x 128 B
+    Smem &sh = *reinterpret_cast<Smem *>(smB + static_cast<size_t>(nqp) * 128);
+    volatile int *abort_flag = &sh.abort_flag;
+
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const uint32_t tiles = (M + kTileM - 1) / kTileM, nks = nqp / kStageK;
+
+    // B = [w_hi | w_lo] (harmonic n < 16: hi, 16 + n: lo) in K-major core matrices
+    for (uint32_t i = threadIdx.x; i < nqp * 32; i += blockDim.x) {
+        const uint32_t k = i >> 5, n = i & 31u, h = n & 15u;
+        const double w = (k < nq && static_cast<int>(h) < nmom) ? W[static_cast<size_t>(h) * nq + k] : 0.0;
+        const float hi = tf32_trunc(static_cast<float>(w));
+        const float v = n < 16 ? hi : static_cast<float>(w - static_cast<double>(hi));
+        const uint32_t off = (((k >> 2) * 4 + (n >> 3)) * 128) + (n & 7u) * 16 + (k & 3u) * 4;
+        *reinterpret_cast<float *>(smB + off) = v;
+    }
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(smem_u32(&sh.full[s]), 1);
+            mbar_init(smem_u32(&sh.empty[s]), 1);
+            mbar_init(smem_u32(&sh.lo_ready[s]), 4);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(smem_u32(&sh.acc_full[b]), 1);
+            mbar_init(smem_u32(&sh.acc_empty[b]), 4);
+        }
+        mbar_init(smem_u32(&sh.drain), 1);
+        sh.abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    // the weights were written by ordinary stores; the tensor cores read
+    // them through the async proxy
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&sh.tmem_base)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = sh.tmem_base;
+
+    if (warp == 0 && lane == 0) {
+        // ---- TMA producer
+        uint32_t it = 0, inflight = 0;
+        bool ok = true;
+        for (uint32_t tile = blockIdx.x; ok && tile < tiles; tile += gridDim.x)
+            for (uint32_t ks = 0; ks < nks; ++ks, ++it) {
+                const uint32_t s = it % kStages, ph = (it / kStages) & 1u;
+                if (!(ok = mbar_wait(smem_u32(&sh.empty[s]), ph ^ 1u, abort_flag, err))) break;
+                const uint32_t fb = smem_u32(&sh.full[s]);
+                mbar_expect_tx(fb, kStageBytes);
+                const uint32_t dst = smem_u32(smA + s * kStageBytes);
+#pragma unroll
+                for (int a = 0; a < 4; ++a)
+                    tma_load_2d(dst + a * kAtomBytes, &psi_map, static_cast<int>(tile * kTileM + a * 32),
+                                static_cast<int>(ks * kStageK), fb);
+                inflight = it + 1;
+            }
+        if (!ok) {  // aborted: wait (bounded, own timer) for the copies already issued
+            for (uint32_t j = inflight > kStages ? inflight - kStages : 0; j < inflight; ++j) {
+                const uint32_t bar = smem_u32(&sh.full[j % kStages]), ph = (j / kStages) & 1u;
+                const unsigned long long t0 = global_ns();
+                while (!mbar_try(bar, ph) && global_ns() - t0 < kWaitNs) {
+                }
+            }
+        }
+    } else if (warp == 1 && lane == 0) {
+        // ---- MMA issuer
+        constexpr uint32_t id_hi = idesc_tf32(32, 1), id_lo = idesc_tf32(16, 0);
+        uint32_t it = 0, tcount = 0;
+        bool ok = true;
+        for (uint32_t tile = blockIdx.x; ok && tile < tiles; tile += gridDim.x, ++tcount) {
+            const uint32_t b = tcount & 1u, bph = (tcount >> 1) & 1u;
+            if (!(ok = mbar_wait(smem_u32(&sh.acc_empty[b]), bph ^ 1u, abort_flag, err))) break;
+            tc_fence_after();
+            const uint32_t d = tmem + 32u * b;
+            for (uint32_t ks = 0; ks < nks; ++ks, ++it) {
+                const uint32_t s = it % kStages, ph = (it / kStages) & 1u;
+                if (!(ok = mbar_wait(smem_u32(&sh.full[s]), ph, abort_flag, err))) break;
+                if (!(ok = mbar_wait(smem_u32(&sh.lo_ready[s]), ph, abort_flag, err))) break;
+                tc_fence_after();
+                const uint32_t a0 = smem_u32(smA + s * kStageBytes);
+                const uint32_t b0 = smem_u32(smB) + ks * 4u * 1024u;
+#pragma unroll
+                for (uint32_t kk = 0; kk < 4; ++kk) {
+                    const uint64_t bd = desc_b(b0 + kk * 1024u);
+                    mma_ss(d, desc_a(a0 + kk * 1024u), bd, id_hi, (ks | kk) != 0u);
+                    mma_ts(d, tmem + kLoCol0 + kStageK * s + 8u * kk, bd, id_lo, 1u);
+                }
+                mma_commit(smem_u32(&sh.empty[s]));  // stage and its a_lo slot free once these finish
+            }
+            if (!ok) break;
+            mma_commit(smem_u32(&sh.acc_full[b]));
+        }
+        // every product issued has finished before tensor memory is freed
+        mma_commit(smem_u32(&sh.drain));
+        const unsigned long long t0 = global_ns();
+        while (!mbar_try(smem_u32(&sh.drain), 0) && global_ns() - t0 < kWaitNs) {
+        }
+    } else if (warp >= 4) {
+        // ---- split (a_lo into tensor memory) and epilogue
+        const uint32_t wq = warp - 4;                        // lanes 32 wq .. 32 wq + 31
+        const uint32_t lane_addr = (32u * wq) << 16;
+        uint32_t it = 0, tcount = 0;
+        bool ok = true;
+        for (uint32_t tile = blockIdx.x; ok && tile < tiles; tile += gridDim.x, ++tcount) {
+            for (uint32_t ks = 0; ks < nks; ++ks, ++it) {
+                const uint32_t s = it % kStages, ph = (it / kStages) & 1u;
+                if (!(ok = mbar_wait_warp(smem_u32(&sh.full[s]), ph, abort_flag, err))) break;
+                // row 32 wq + lane of the stage: atom wq, word lane of each
+                // 128-byte ordinate row (16-byte chunk c stored at c ^ (row % 8))
+                const uint8_t *atom = smA + s * kStageBytes + wq * kAtomBytes;
+                uint32_t lo[32];
+#pragma unroll
+                for (int k = 0; k < 32; ++k) {
+                    const uint32_t off = k * 128 + ((((lane >> 2) ^ (k & 7)) << 4)) + (lane & 3u) * 4;
+                    const float a = *reinterpret_cast<const float *>(atom + off);
+                    lo[k] = __float_as_uint(a - tf32_trunc(a));
+                }
+                tmem_st32(tmem + lane_addr + kLoCol0 + kStageK * s, lo);
+                tmem_wait_st();
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(smem_u32(&sh.lo_ready[s]));
+            }
+            if (!ok) break;
+            const uint32_t b = tcount & 1u, bph = (tcount >> 1) & 1u;
+            if (!(ok = mbar_wait_warp(smem_u32(&sh.acc_full[b]), bph, abort_flag, err))) break;
+            tc_fence_after();
+            uint32_t v[32];
+            tmem_ld32(tmem + lane_addr + 32u * b, v);
+            tmem_wait_ld();
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&sh.acc_empty[b]));
+            const uint64_t row = static_cast<uint64_t>(tile) * kTileM + 32u * wq + lane;
+            if (row < M) {
+#pragma unroll
+                for (int n = 0; n < 16; ++n)
+                    if (n < nmom)
+                        mom[static_cast<uint64_t>(n) * M + row] = static_cast<double>(__uint_as_float(v[n])) +
+                                                                  static_cast<double>(__uint_as_float(v[16 + n]));
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0) {
+        __syncwarp();  // lane 0 comes from the producer branch: reconverge for the warp-wide dealloc
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols)
+                     : "memory");
+    }
+}
+
+size_t moments_tcgen05_smem(uint32_t nq) {
+    const uint32_t nqp = (nq + kStageK - 1) / kStageK * kStageK;
+    return 1024 + static_cast<size_t>(kStages) * kStageBytes + static_cast<size_t>(nqp) * 128 + sizeof(Smem);
+}
+
+bool moments_tcgen05_supported(uint32_t M, uint32_t nq) {
+    return M > 0 && M % 4 == 0 && nq > 0 && moments_tcgen05_smem(nq) <= 227u * 1024u;
+}
+
+namespace {
+using EncodeTiled = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                 const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiled encode_fn() {
+    static EncodeTiled fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiled>(p);
+    }
+    return fn;
+}
+}  // namespace
+
+cudaError_t launch_moments_tcgen05(const float *psi, uint32_t M, uint32_t nq, const double *W, int nmom,
+                                   double *mom, unsigned int *err, int num_sms, cudaStream_t stream) {
+    if (!moments_tcgen05_supported(M, nq) || nmom < 1 || nmom > 16) return cudaErrorInvalidValue;
+    EncodeTiled enc = encode_fn();
+    if (!enc) return cudaErrorNotSupported;
+    // psi as a 2-D tensor: x = row (M, contiguous), y = ordinate (nq, stride 4 M bytes)
+    CUtensorMap map;
+    const cuuint64_t dims[2] = {M, nq};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(M) * 4};
+    const cuuint32_t box[2] = {32, kStageK};
+    const cuuint32_t estr[2] = {1, 1};
+    if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(psi), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return cudaErrorInvalidValue;
+    const size_t smem = moments_tcgen05_smem(nq);
+    static bool attr = false;  // the opt-in is per function, one process-wide setting
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(k_moments_tcgen05, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             227 * 1024);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    const uint32_t tiles = (M + kTileM - 1) / kTileM;
+    const int grid = static_cast<int>(tiles < static_cast<uint32_t>(num_sms) ? tiles : num_sms);
+    const uint32_t nqp = (nq + kStageK - 1) / kStageK * kStageK;
+    k_moments_tcgen05<<<grid, kThreads, smem, stream>>>(map, M, nq, nqp, W, nmom, mom, err);
+    return cudaGetLastError();
+}
+
+}  // namespace transfer

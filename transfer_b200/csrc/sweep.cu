@@ -52,6 +52,7 @@
 #include <vector>
 
 #include "../../include/transfer_b200.h"
+#include "moments_tc.h"
 #include "reduce.cuh"
 
 namespace transfer {
@@ -1463,6 +1464,8 @@ struct tr_sweep {
     std::vector<void *> allocs;
     int64_t sweeps32 = 0, sweeps64 = 0, launches = 0;
     bool mom_attr = false;         // k_moments_tf32x3 shared-memory opt-in done
+    int mom_kernel = TR_MOMENTS_TCGEN05;
+    unsigned int *mom_err = nullptr;  // pipeline-timeout flag of k_moments_tcgen05
     int shape32 = -1;              // FP32 sweep shape: -1 by rule, 0 full, 1 small (tr_sweep_autotune)
 };
 
@@ -2691,7 +2694,20 @@ tr_status tr_sweep_moments(tr_sweep *s, int nmom, double *mom) {
     if (!s->last_prec) return sw_err(s, TR_ERR_INVALID_ARG, "tr_sweep_moments: no sweep has run");
     cudaError_t e = cudaSuccess;
     const uint32_t nqp8 = (s->nq + 7) / 8 * 8;
-    if (s->last_prec == 32 && 2ull * 16 * nqp8 * sizeof(uint32_t) <= 48 * 1024) {  // nq <= 384
+    if (s->last_prec == 32 && s->mom_kernel == TR_MOMENTS_TCGEN05 &&
+        transfer::moments_tcgen05_supported(4 * s->nT, s->nq)) {
+        if (!s->mom_err) e = sw_alloc(s, &s->mom_err, 1);
+        if (e == cudaSuccess) e = cudaMemsetAsync(s->mom_err, 0, sizeof(unsigned int), s->stream);
+        if (e == cudaSuccess)
+            e = transfer::launch_moments_tcgen05(s->psi32, 4 * s->nT, s->nq, s->Wm, nmom, mom, s->mom_err, s->num_sms,
+                                                 s->stream);
+        ++s->launches;
+        unsigned int flag = 0;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&flag, s->mom_err, sizeof(flag), cudaMemcpyDeviceToHost, s->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+        if (e == cudaSuccess && flag)
+            return sw_err(s, TR_ERR_CUDA, "tr_sweep_moments: a pipeline wait of the tensor-core kernel timed out");
+    } else if (s->last_prec == 32 && 2ull * 16 * nqp8 * sizeof(uint32_t) <= 48 * 1024) {  // nq <= 384
         const uint32_t M = 4 * s->nT, nqp = nqp8;
         const size_t smem = moments_smem(nqp);
         if (!s->mom_attr) {  // above 48 KB of dynamic shared memory: opt in once
@@ -2741,6 +2757,14 @@ tr_status tr_sweep_moments(tr_sweep *s, int nmom, double *mom) {
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
     return sw_cuda(s, e, "tr_sweep_moments");
+}
+
+tr_status tr_sweep_set_moments_kernel(tr_sweep *s, int kind) {
+    SW_CHECK(s);
+    if (kind != TR_MOMENTS_TCGEN05 && kind != TR_MOMENTS_MMA_SYNC)
+        return sw_err(s, TR_ERR_INVALID_ARG, "tr_sweep_set_moments_kernel: unknown kernel family");
+    s->mom_kernel = kind;
+    return TR_OK;
 }
 
 tr_status tr_sweep_balance(tr_sweep *s, const double *J_in, const double *B_in, const double *J_out,

@@ -103,6 +103,10 @@ class Sweep:
         self._c(lib.tr_sweep_psi(self._h, _ptr(out)))
         return out.view(self.nq, self.nT, 4)
 
+    def set_moments_kernel(self, kind):
+        """tr_sweep_set_moments_kernel: TR_MOMENTS_TCGEN05 (default) or TR_MOMENTS_MMA_SYNC."""
+        self._c(lib.tr_sweep_set_moments_kernel(self._h, int(kind)))
+
     def moments(self, nmom=16):
         out = self._dev(nmom * 4 * self.nT)
         self._c(lib.tr_sweep_moments(self._h, int(nmom), _ptr(out)))

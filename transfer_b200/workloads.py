@@ -10,6 +10,14 @@ generated, seeded).
                isotropic inflow I = 1 through z = 20, vacuum elsewhere,
                maxk = 3 (l <= 6; the 86-point set: the reference's rule
                choice 4 maxk + 2 cannot reach the 110-point set).
+  milne_slab_ref
+               the same 8 x 8 x 160 slab with the reference's own physics
+               (the form its program runs): kappa = 1, emission Ip = 1 in
+               the tets whose centroid has z < 10 and 0 above (the
+               half-space emission of the reference's Milne problem,
+               main.cpp:498-515, with the interface at z = 10), vacuum on
+               every face, maxk = 3.  desc["regions"] gives the per-region
+               kappa and Ip for a radiation.cfg.
   cube64       unit cube, 64^3 Kuhn hexahedra (1,572,864 tets), kappa per
                tet = exp(0.5 g), g a unit Gaussian random field with
                correlation length 0.1 (random-Fourier-feature sample),
@@ -31,7 +39,7 @@ def config1(maxk=1, n=16):
     md = MeshData.kuhn((n, n, n), jitter=0.2, seed=SEED, kappa=[0.0, 1.0, 1.0], Ip=[0.0, 1.0, 0.0],
                        region_kind=1, region_arg=(0.5, 0.5, 0.5, 0.25))
     desc = dict(workload="config1", mesh=f"{n}^3 Kuhn cube, jitter 0.2h", maxk=maxk,
-                physics="kappa=1, Ip=1 in r<0.25, vacuum")
+                physics="kappa=1, Ip=1 in r<0.25, vacuum", regions={"kappa": [0.0, 1.0, 1.0], "Ip": [0.0, 1.0, 0.0]})
     return md, AngularData(maxk), None, desc
 
 
@@ -46,6 +54,21 @@ def milne_slab(maxk=3, n=(8, 8, 160), depth=20.0, incident=1.0):
                 maxk=maxk, physics=f"kappa=1, no scattering, isotropic inflow I={incident:g} at z={depth:g}, "
                                    "vacuum elsewhere")
     return md, AngularData(maxk), phys, desc
+
+
+def milne_slab_ref(maxk=3, n=(8, 8, 160), depth=20.0):
+    base = MeshData.kuhn(n, box=(0.0, 1.0, 0.0, 1.0, 0.0, depth), jitter=0.15, seed=SEED, kappa=[0.0, 1.0],
+                         Ip=[0.0, 0.0])
+    tets = base.mesh["p"]
+    zc = base.coords[tets.astype(np.int64)][..., 2].mean(axis=1)
+    region = np.where(zc < 0.5 * depth, 1, 2).astype(np.int32)
+    kappa, Ip = [0.0, 1.0, 1.0], [0.0, 1.0, 0.0]
+    md = MeshData.from_tets(base.coords, tets, region, kappa, Ip)
+    desc = dict(workload="milne_slab_ref", mesh=f"{n[0]}x{n[1]}x{n[2]} Kuhn slab [0,1]^2x[0,{depth:g}], jitter 0.15h",
+                maxk=maxk, physics=f"kappa=1, Ip=1 for z<{0.5 * depth:g} and 0 above, vacuum on every face "
+                                   "(the reference's own boundary and source terms)",
+                regions={"kappa": kappa, "Ip": Ip})
+    return md, AngularData(maxk), None, desc
 
 
 def gaussian_random_field(points, corr_len=0.1, modes=512, seed=SEED):
@@ -75,7 +98,7 @@ def cube64(maxk=5, n=64):
     return md, AngularData(maxk), None, desc
 
 
-WORKLOADS = {"config1": config1, "milne_slab": milne_slab, "cube64": cube64}
+WORKLOADS = {"config1": config1, "milne_slab": milne_slab, "milne_slab_ref": milne_slab_ref, "cube64": cube64}
 
 
 def milne_sweep(n=(8, 8, 160), depth=20.0, albedo=0.999, incident=1.0, n_polar=8, n_azim=14):
