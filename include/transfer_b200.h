@@ -409,7 +409,22 @@ tr_status tr_ordinates_product(int n_polar, int n_azim, double *x, double *y, do
  * the per-ordinate dependency levels (on the device). */
 tr_status tr_sweep_create(int device, const tr_mesh_view *mesh, const tr_physics_view *phys,
                           const tr_ordinates_view *ord, tr_sweep **out);
+/* Fails (TR_ERR_INVALID_ARG) while the sweep has live frequency groups. */
 tr_status tr_sweep_destroy(tr_sweep *s);
+/* A frequency group of `parent` (no reference counterpart: the reference
+ * solves one grey problem): a sweep over the same mesh, boundary kinds,
+ * ordinates and dependency schedule -- shared with the parent, not copied --
+ * with its own per-cell sigma_t V (kappa_volume), sigma_a V (NULL: no
+ * scattering) and Planck intensity I_p (NULL: the parent's), and its own
+ * angular flux and solver state.  Groups are independent problems (no group
+ * coupling); the batched calls run any mix of parents and groups in one
+ * launch.  The parent must outlive its groups; a group cannot have groups. */
+tr_status tr_sweep_create_group(tr_sweep *parent, const double *kappa_volume, const double *kappa_abs_volume,
+                                const double *I_p, tr_sweep **out);
+/* Frees the angular flux and Krylov work space of a sweep (allocated again
+ * by the next sweep or solve): lets a caller solve many problems in FP64
+ * one after another without holding every problem's work space. */
+tr_status tr_sweep_release_work(tr_sweep *s);
 const char *tr_sweep_last_error(const tr_sweep *s);
 tr_status tr_sweep_info_get(const tr_sweep *s, tr_sweep_info *info);
 /* level[q * nT + c]: dependency level of cell c in ordinate q (host array). */
@@ -439,6 +454,22 @@ tr_status tr_sweep_apply_batch(int n, tr_sweep *const *s, int precision, const d
  * residual[i] (last relative change): host arrays [n]. */
 tr_status tr_sweep_solve_batch(int n, tr_sweep *const *s, int precision, double tol, int max_iter, double *const *J,
                                double *const *B, int32_t *iterations, double *residual);
+/* Form of the batched sweep launch (no reference counterpart; results do
+ * not depend on it): a static grid of one block per (problem, ordinate)
+ * task, or a persistent grid whose blocks draw tasks from an atomic queue
+ * (largest problems first); each with the full shared-memory shape (a ring
+ * of 4,096 upwind positions, one block per SM) or, for FP32, the small one
+ * (1,024 positions, two blocks per SM).  TR_BATCH_RULE (-1): static grid,
+ * small shape for FP32 when the tasks outnumber the SMs. */
+enum { TR_BATCH_RULE = -1, TR_BATCH_STATIC_FULL = 0, TR_BATCH_STATIC_SMALL = 1, TR_BATCH_QUEUE_FULL = 2,
+       TR_BATCH_QUEUE_SMALL = 3 };
+tr_status tr_sweep_set_batch_form(tr_sweep *s, int form);
+/* Autotuner of the batched launch: times one batched sweep of these n
+ * problems (precision 32 or 64) in every form, sets the fastest on all n
+ * (the batched calls use the form of their first sweep) and returns it in
+ * *form; ms[4] (may be NULL): mean time of one batched sweep per form, -1
+ * for a form that does not apply (the small shape in FP64). */
+tr_status tr_sweep_autotune_batch(int n, tr_sweep *const *s, int precision, int *form, double *ms);
 /* Times the FP32 sweep kernel in both shared-memory shapes on this problem
  * (full: one block per SM; small: two per SM, shorter ring) and keeps the
  * faster for its later FP32 sweeps (without it: small when there are more

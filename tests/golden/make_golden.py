@@ -53,7 +53,7 @@ def dump_angular(tmp):
 
 def dump_rules(tmp):
     out = {}
-    for mode, degs in (("lebedev", [2, 6, 10, 13, 14, 17, 18, 22, 26, 29, 30]), ("hemi", [1, 5, 9, 13, 17, 21, 25, 29])):
+    for mode, degs in (("lebedev", [2, 6, 10, 13, 14, 17, 18, 22, 25, 26, 29, 30]), ("hemi", [1, 5, 9, 13, 17, 21, 25, 29])):
         for d in degs:
             fn = os.path.join(tmp, f"{mode}{d}.bin")
             run(os.path.join(REF, "ref_dump"), mode, str(d), fn)

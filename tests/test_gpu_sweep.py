@@ -110,8 +110,11 @@ def test_moments_match_oracle(cuda, precision, kernel):
 def test_moments_tcgen05_split_tf32_accuracy(cuda, n, polar, azim):
     """The tensor-core contraction against an FP64 sum over the same FP32 psi
     (the GPU's own, widened exactly): split TF32 with FP32 accumulation stays
-    within 3e-6 of the largest moment (a single TF32 product would be ~1e-3);
-    the mma.sync kernel where it applies (up to 384 ordinates) gives the same."""
+    within 3e-6 of the largest moment (a single TF32 product would be ~1e-3).
+    The tensor core truncates when it accumulates; the tcgen05 kernel deals
+    the ordinate steps over four accumulators summed in FP64, the mma.sync
+    kernel (up to 384 ordinates) keeps one, and its truncation bias reaches
+    about 4e-6 at 308 ordinates, hence its 1e-5 bound."""
     md, ph, S, O = pair(scattering_box(n=n), op.ordinates_product(polar, azim))
     S.apply(precision=32)
     mo = O.moments(host(S.psi()), 16)
@@ -120,7 +123,7 @@ def test_moments_tcgen05_split_tf32_accuracy(cuda, n, polar, azim):
         assert rel_err(mg, mo[:nmom]) < 3e-6
     if polar * azim <= 384:
         S.set_moments_kernel(tr._lib.TR_MOMENTS_MMA_SYNC)
-        assert rel_err(host(S.moments(16)), mo) < 3e-6
+        assert rel_err(host(S.moments(16)), mo) < 1e-5
     with pytest.raises(tr.TransferError):
         S.set_moments_kernel(7)
 
@@ -397,3 +400,100 @@ def test_adjoint_gradient_rejects_reflective_faces(cuda):
     ords = tr.ordinates_product(2, 4)
     with pytest.raises(tr.TransferError):
         tr.adjoint_gradient(0, md, ords, ph, (md.face_side == 1).astype(np.int32))
+
+
+def test_milne_slab_matches_the_analytic_e1_solution(cuda):
+    """Configuration 2 at full size: the 8x8x160 Milne-type slab (albedo
+    0.999, reflective sides, isotropic inflow at z = 20) with the 110-point
+    Lebedev set, solved in FP64 and in mixed precision (FP32 sweeps in FP64
+    defect correction) to the FP64 residual 1e-8.  With reflective sides it is
+    the 1-D slab whose mean intensity solves the E1 (Peierls) integral
+    equation (oracle/slab_analytic.py); J at every cell vertex agrees with it
+    to the discretisation error of linear-discontinuous elements at h = 1/8
+    mean free path and of the 110-point set (the CPU restatement of the sweep
+    gives the same: max 2.1e-3, mean 1.5e-4 of max J).  The mixed solution is
+    within 1e-6 of the FP64 one."""
+    import slab_analytic as sa
+    from transfer_b200 import workloads as W
+    md, ph, ords, desc = W.milne_sweep()
+    assert len(ords[3]) == 110
+    S = tr.Sweep(0, md, ords, ph, dsa=True)
+    DSA = tr._lib.TR_SWEEP_PREC_DSA
+    J64, _, r64 = S.solve(mode=tr.TR_MODE_FP64, tol=1e-8, restart=40, max_iter=5000, precondition=DSA,
+                          precond_tol=1e-2)
+    Jmx, _, rmx = S.solve(mode=tr.TR_MODE_MIXED, tol=1e-8, restart=40, max_iter=5000, precondition=DSA,
+                          precond_tol=1e-2, inner_tol=1e-4)
+    assert r64.converged and rmx.converged
+    f, est = sa.slab_reference(a=20.0, albedo=0.999, I0=1.0, n=2000)
+    z = md.coords[md.mesh["p"].astype(np.int64)][..., 2]
+    Jref = f(z)
+    scale = np.abs(Jref).max()
+    for J in (host(J64), host(Jmx)):
+        err = np.abs(J - Jref) / scale
+        assert err.max() < 4e-3 and err.mean() < 4e-4, (err.max(), err.mean())
+    assert rel_err(host(Jmx), host(J64)) < 1e-6
+
+
+def test_frequency_group_equals_its_own_sweep(cuda):
+    """A group shares its parent's mesh, ordinates and schedule and has its
+    own coefficients: its sweep is exactly the sweep of a problem created with
+    those coefficients, and the parent's own sweep is unchanged by it."""
+    md, ph = scattering_box()
+    ords = op.ordinates_product(4, 8)
+    P = tr.Sweep(0, md, ords, ph)
+    rng = np.random.default_rng(8)
+    kv = md.mesh["kappa_volume"] * rng.uniform(0.5, 3.0, md.nT)
+    kav = kv * rng.uniform(0.2, 1.0, md.nT)
+    Ip = rng.uniform(0.0, 2.0, md.nT)
+    G = P.create_group(kv, kav, Ip)
+    R = tr.Sweep(0, md, ords, ph)
+    R.set_coefficients(kv, kav, Ip)
+    J, B = dev(rng.random(4 * md.nT)), dev(rng.random(P.n_extra))
+    Jp0, _ = P.apply(J, B, precision=64)
+    for prec in (64, 32):
+        Jg, Bg = G.apply(J, B, precision=prec)
+        Jr, Br = R.apply(J, B, precision=prec)
+        assert torch.equal(Jg, Jr) and torch.equal(Bg, Br)
+    Jp1, _ = P.apply(J, B, precision=64)
+    assert torch.equal(Jp0, Jp1)
+    assert P.device_bytes - G.device_bytes >= 16 * P.nq * P.nT   # the task records are not copied
+    with pytest.raises(tr.TransferError):          # a group of a group
+        G.create_group(kv)
+    assert tr.lib.tr_sweep_destroy(P._h) != tr._lib.TR_OK   # the parent outlives its groups
+    G.release_work()
+    Jg2, _ = G.apply(J, B, precision=64)            # the work space comes back
+    assert torch.equal(Jg2, R.apply(J, B, precision=64)[0])
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_batch_launch_forms_give_identical_results(cuda, precision):
+    """Static grid or work queue, full or small shared-memory shape: one
+    batched sweep of parents and groups gives the separate sweeps' bits; the
+    autotuner times every applicable form and keeps one."""
+    cases = [(scattering_box(), op.ordinates_product(4, 8)), (absorbing_slab(nx=20), op.ordinates_product(6, 12)),
+             (scattering_box(n=(8, 8, 8)), tr.lebedev(17))]
+    sweeps = [tr.Sweep(0, md, ords, ph) for (md, ph), ords in cases]
+    rng = np.random.default_rng(9)
+    for S, ((md, ph), _) in list(zip(sweeps, cases)):
+        for g in range(2):
+            kv = md.mesh["kappa_volume"] * 10.0 ** (g / 3.0)
+            sweeps.append(S.create_group(kv, None if ph.kappa_abs_volume is None else ph.kappa_abs_volume * 10.0 ** (g / 3.0)))
+    Js = [dev(rng.random(4 * S.nT)) for S in sweeps]
+    Bs = [dev(rng.random(max(S.n_extra, 1))) for S in sweeps]
+    ref = [S.apply(J, B if S.n_extra else None, precision=precision) for S, J, B in zip(sweeps, Js, Bs)]
+    L_ = tr._lib
+    forms = [L_.TR_BATCH_STATIC_FULL, L_.TR_BATCH_QUEUE_FULL]
+    if precision == 32:
+        forms += [L_.TR_BATCH_STATIC_SMALL, L_.TR_BATCH_QUEUE_SMALL]
+    for f in forms:
+        sweeps[0].set_batch_form(f)
+        out = tr.sweep_apply_batch(sweeps, precision, Js, Bs)
+        for (Jb, Bb), (Jo, Bo) in zip(out, ref):
+            assert torch.equal(Jb, Jo) and torch.equal(Bb, Bo), f
+    form, ms = tr.sweep_autotune_batch(sweeps, precision)
+    assert form in forms and set(ms) == set(forms) and all(v > 0 for v in ms.values())
+    out = tr.sweep_apply_batch(sweeps, precision, Js, Bs)
+    for (Jb, _), (Jo, _) in zip(out, ref):
+        assert torch.equal(Jb, Jo)
+    with pytest.raises(tr.TransferError):
+        sweeps[0].set_batch_form(4)

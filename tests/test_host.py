@@ -106,18 +106,20 @@ def _sorted_rule(r):
     return r[:, idx]
 
 
-@pytest.mark.parametrize("deg", [2, 6, 10, 13, 14, 17, 18, 22])
+@pytest.mark.parametrize("deg", [2, 6, 10, 13, 14, 17, 18, 22, 25, 26, 29, 30])
 def test_lebedev_matches_reference(deg):
     """The generated rules are the reference's LebedevQuad point sets
-    (LebedevQuad.cpp) up to the order of the points (the 74-point rule of
-    degree 13 included, whose (1,1,1) orbit has a negative weight)."""
+    (LebedevQuad.cpp) up to the order of the points: every rule up to 350
+    points (precision 31), the ones with negative orbit weights included
+    (74, 230 and 266 points)."""
     g = golden("quadrature.npz")[f"lebedev_{deg}"]
     ours = rule(tr.lib.tr_lebedev, deg)
     assert ours.shape == g.shape
     assert np.abs(_sorted_rule(ours) - _sorted_rule(g)).max() < 1e-11
     assert abs(ours[3].sum() - 1.0) < 1e-14
     # exact for the real harmonics up to the rule's precision
-    prec = {6: 3, 26: 7, 50: 11, 74: 13, 86: 15, 110: 17, 146: 19, 194: 23}[g.shape[1]]
+    prec = {6: 3, 26: 7, 50: 11, 74: 13, 86: 15, 110: 17, 146: 19, 194: 23, 230: 25, 266: 27, 302: 29,
+            350: 31}[g.shape[1]]
     x, y, z, w = ours
     for l in range(1, prec + 1):
         for m in range(-l, l + 1):
@@ -125,7 +127,7 @@ def test_lebedev_matches_reference(deg):
             assert abs((w * v).sum()) <= 1e-13 * (np.abs(v).max() * len(v) + 1.0)
 
 
-@pytest.mark.parametrize("deg", [26, 29, 30])
+@pytest.mark.parametrize("deg", [32, 35, 41])
 def test_lebedev_beyond_generated_rules_is_refused(deg):
     assert tr.lib.tr_lebedev(deg, None, None, None, None, 0) == -1
 

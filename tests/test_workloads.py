@@ -23,7 +23,10 @@ def test_work_models_count_the_documented_bytes():
 
 def test_milne_sweep_workload():
     md, ph, ords, desc = W.milne_sweep(n=(2, 2, 8))
-    assert md.nT == 6 * 2 * 2 * 8 and len(ords[3]) == 112 and abs(ords[3].sum() - 1) < 1e-14
+    assert md.nT == 6 * 2 * 2 * 8 and len(ords[3]) == 110 and abs(ords[3].sum() - 1) < 1e-14   # Lebedev 110
+    # mirror-symmetric, as the reflective walls need
+    pts = np.round(np.stack(ords[:3], axis=1), 12)
+    assert {tuple(p) for p in pts} == {(-p[0], p[1], p[2]) for p in pts} == {(p[0], -p[1], p[2]) for p in pts}
     assert (ph.face_bc == tr.TR_BC_REFLECTIVE).sum() == 4 * 2 * 8 * 2
     assert desc["workload"] == "milne_sweep"
 
@@ -59,3 +62,18 @@ def test_runner_command_lines_parse():
         r = subprocess.run([sys.executable, "-m", mod, "--help"], cwd=os.path.dirname(os.path.dirname(__file__)),
                            capture_output=True, text=True, timeout=300)
         assert r.returncode == 0 and "usage" in r.stdout, (mod, r.stderr[-500:])
+
+
+def test_cube_batch_groups():
+    """Configuration 4's problems carry 8 frequency groups: sigma_t scaled by
+    10^(g/3 - 1) from one lognormal base, the problem's albedo in every group."""
+    probs, desc = W.cube_batch(count=3, lo=50, hi=400, groups=8)
+    assert desc["groups"] == 8 and len(probs) == 3
+    for md, ph, ords, gc in probs:
+        assert len(gc) == 7 and len(ords[3]) in (50, 194)
+        kv0 = md.mesh["kappa_volume"]
+        albedo = 1.0 - ph.kappa_abs_volume / kv0
+        assert np.allclose(albedo, albedo[0]) and 0.0 <= albedo[0] <= 0.9
+        for g, (kv, kav) in enumerate(gc, start=1):
+            assert np.allclose(kv / kv0, 10.0 ** (g / 3.0))
+            assert np.allclose(1.0 - kav / kv, albedo[0])

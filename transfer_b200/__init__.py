@@ -13,7 +13,7 @@ from ._lib import (TR_BC_INCIDENT, TR_BC_REFLECTIVE, TR_BC_VACUUM, TR_ENGINE_GRA
 from .core import (FACE_DTYPE, TET_DTYPE, AngularData, Config, CudaContext, MeshData, Physics,  # noqa: F401
                    solve_options, trieig)
 from .sweep import (Sweep, adjoint_gradient, adjoint_problem, lebedev, ordinates_product,  # noqa: F401
-                    sweep_apply_batch, sweep_solve_batch)
+                    sweep_apply_batch, sweep_autotune_batch, sweep_solve_batch)
 
 __all__ = ["AngularData", "Config", "CudaContext", "MeshData", "Physics", "Sweep", "TransferError",
-           "ordinates_product", "lebedev", "sweep_apply_batch", "sweep_solve_batch", "solve_options", "trieig", "lib", "LIB_PATH"]
+           "ordinates_product", "lebedev", "sweep_apply_batch", "sweep_autotune_batch", "sweep_solve_batch", "solve_options", "trieig", "lib", "LIB_PATH"]

@@ -36,6 +36,7 @@ TR_SWEEP_GMRES, TR_SWEEP_SOURCE_ITERATION = 0, 1
 TR_SWEEP_PREC_NONE, TR_SWEEP_PREC_DSA = 0, 1
 TR_SWEEP_DSA_AUTO, TR_SWEEP_DSA_CLUSTER, TR_SWEEP_DSA_EVEN_PARITY = 0, 1, 2
 TR_MOMENTS_TCGEN05, TR_MOMENTS_MMA_SYNC = 0, 1
+TR_BATCH_RULE, TR_BATCH_STATIC_FULL, TR_BATCH_STATIC_SMALL, TR_BATCH_QUEUE_FULL, TR_BATCH_QUEUE_SMALL = -1, 0, 1, 2, 3
 TR_VTK_POINT, TR_VTK_CELL = 0, 1
 TR_VTK_SCALAR, TR_VTK_VECTOR, TR_VTK_TENSOR = 0, 1, 2
 
@@ -201,6 +202,10 @@ PROTOTYPES = [
     ("tr_sweep_psi", S, [P, P]),
     ("tr_sweep_moments", S, [P, I, P]),
     ("tr_sweep_set_moments_kernel", S, [P, I]),
+    ("tr_sweep_create_group", S, [P, P, P, P, P]),
+    ("tr_sweep_release_work", S, [P]),
+    ("tr_sweep_set_batch_form", S, [P, I]),
+    ("tr_sweep_autotune_batch", S, [I, P, I, P, P]),
     ("tr_sweep_balance", S, [P, P, P, P, P]),
     ("tr_sweep_opts_default", None, [C.POINTER(tr_sweep_opts)]),
     ("tr_sweep_solve", S, [P, C.POINTER(tr_sweep_opts), P, P, C.POINTER(tr_sweep_report)]),

@@ -11,15 +11,23 @@
 // (1,1,1)/sqrt 3), b(l) (24, (l,l,m)), c(p) (24, (p,q,0)), d(r,s) (48,
 // (r,s,t)).  For each rule the published orbit structure (Lebedev & Laikov,
 // Doklady Math. 59 (1999) 477) makes the equations a square system in the
-// orbit weights and parameters.  It is solved from seeded random orbit
-// parameters by variable projection (the weights, which enter linearly, by
-// least squares; Levenberg-Marquardt on the parameters) and a final Newton
-// polish of weights and parameters together, until a solution with positive
-// weights and distinct, admissible orbits is found.  Rules up to 194 points
-// (precision 23) are generated this way (194 takes a few seconds, once per
-// process); larger ones are not.  Each generated rule is checked against the
-// exact sphere averages before it is returned and cached.
+// orbit weights and parameters.  It is solved by variable projection (the
+// weights, which enter linearly, by least squares; Levenberg-Marquardt on the
+// orbit parameters) from seeded starts -- stratified ones, the i-th orbit of
+// a family in the i-th slice of its parameter range, alternating with basin
+// hops, small random moves of the best parameters found so far -- and a final
+// Newton polish of weights and parameters together, until a solution with
+// distinct, admissible orbits and the published sign pattern of the weights
+// is found (all positive, except the 74-, 230- and 266-point rules, which
+// carry negative orbit weights).  Rules up to 350 points (precision 31) are
+// generated this way (the larger ones take a few seconds, once per process);
+// larger ones are not.  Each generated rule is checked against the exact
+// sphere averages before it is returned and cached.
+#include <omp.h>
+
+#include <algorithm>
 #include <array>
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <map>
@@ -49,38 +57,50 @@ namespace {
 
 // orbit structure of the rules generated here: counts of a1, a2, a3 and of
 // the b, c, d families
+// negative: bit k set when orbits of kind k (0 a1, 1 a2, 2 a3, 3 b, 4 c, 5 d)
+// carry a negative weight in the published rule (all other weights positive)
 struct OrbitSpec {
     int order, precision, a1, a2, a3, nb, nc, nd;
+    unsigned negative;
 };
 const OrbitSpec kSpecs[] = {
-    {6, 3, 1, 0, 0, 0, 0, 0},     {14, 5, 1, 0, 1, 0, 0, 0},    {26, 7, 1, 1, 1, 0, 0, 0},
-    {38, 9, 1, 0, 1, 0, 1, 0},    {50, 11, 1, 1, 1, 1, 0, 0},   {74, 13, 1, 1, 1, 1, 1, 0},
-    {86, 15, 1, 0, 1, 2, 1, 0},   {110, 17, 1, 0, 1, 3, 1, 0},  {146, 19, 1, 1, 1, 3, 0, 1},
-    {170, 21, 1, 1, 1, 3, 1, 1},  {194, 23, 1, 1, 1, 4, 1, 1},
-};  // larger rules (230 points and up) are not found reliably from random starts
+    {6, 3, 1, 0, 0, 0, 0, 0, 0},     {14, 5, 1, 0, 1, 0, 0, 0, 0},    {26, 7, 1, 1, 1, 0, 0, 0, 0},
+    {38, 9, 1, 0, 1, 0, 1, 0, 0},    {50, 11, 1, 1, 1, 1, 0, 0, 0},   {74, 13, 1, 1, 1, 1, 1, 0, 1u << 2},
+    {86, 15, 1, 0, 1, 2, 1, 0, 0},   {110, 17, 1, 0, 1, 3, 1, 0, 0},  {146, 19, 1, 1, 1, 3, 0, 1, 0},
+    {170, 21, 1, 1, 1, 3, 1, 1, 0},  {194, 23, 1, 1, 1, 4, 1, 1, 0},  {230, 25, 1, 0, 1, 5, 2, 1, 1u << 0},
+    {266, 27, 1, 1, 1, 5, 1, 2, (1u << 0) | (1u << 1)},           {302, 29, 1, 0, 1, 6, 2, 2, 0},
+    {350, 31, 1, 0, 1, 6, 2, 3, 0},
+};
 
-double dfact(int n) {  // n!! for odd n >= -1
-    double r = 1.0;
+// The exact sphere averages, the orbit points and the residuals are templates
+// on the scalar: double for the search, long double (x87 extended, 64-bit
+// mantissa) for the final Newton polish of each rule.
+template <typename T>
+T dfact(int n) {  // n!! for odd n >= -1
+    T r = 1;
     for (; n > 1; n -= 2) r *= n;
     return r;
 }
 // average of x^(2i) y^(2j) z^(2k) over the unit sphere
-double sphere_avg(int i, int j, int k) {
-    return dfact(2 * i - 1) * dfact(2 * j - 1) * dfact(2 * k - 1) / dfact(2 * (i + j + k) + 1);
+template <typename T>
+T sphere_avg(int i, int j, int k) {
+    return dfact<T>(2 * i - 1) * dfact<T>(2 * j - 1) * dfact<T>(2 * k - 1) / dfact<T>(2 * (i + j + k) + 1);
 }
-double factorial(int n) {
-    double r = 1.0;
+template <typename T>
+T factorial(int n) {
+    T r = 1;
     for (int i = 2; i <= n; ++i) r *= i;
     return r;
 }
 // sphere average of p4^A p6^B (multinomial expansion of p4^A)
-double invariant_avg(int A, int B) {
-    double s = 0.0;
+template <typename T>
+T invariant_avg(int A, int B) {
+    T s = 0;
     for (int a = 0; a <= A; ++a)
         for (int b = 0; a + b <= A; ++b) {
             const int c = A - a - b;
-            s += factorial(A) / (factorial(a) * factorial(b) * factorial(c)) *
-                 sphere_avg(2 * a + B, 2 * b + B, 2 * c + B);
+            s += factorial<T>(A) / (factorial<T>(a) * factorial<T>(b) * factorial<T>(c)) *
+                 sphere_avg<T>(2 * a + B, 2 * b + B, 2 * c + B);
         }
     return s;
 }
@@ -94,27 +114,28 @@ struct Problem {
 
 // base point of an orbit and its derivatives with respect to the orbit's
 // parameters (kind: 0 a1, 1 a2, 2 a3, 3 b, 4 c, 5 d)
-void base_point(int kind, const double *prm, double p[3], double dp[2][3]) {
-    const double r2 = std::sqrt(0.5), r3 = std::sqrt(1.0 / 3.0);
+template <typename T>
+void base_point(int kind, const T *prm, T p[3], T dp[2][3]) {
+    const T r2 = std::sqrt(T(0.5)), r3 = std::sqrt(T(1) / T(3));
     for (int i = 0; i < 2; ++i) dp[i][0] = dp[i][1] = dp[i][2] = 0.0;
     switch (kind) {
         case 0: p[0] = 1; p[1] = 0; p[2] = 0; break;
         case 1: p[0] = 0; p[1] = r2; p[2] = r2; break;
         case 2: p[0] = p[1] = p[2] = r3; break;
-        case 3: {
-            const double l = prm[0], m = std::sqrt(std::fmax(1.0 - 2.0 * l * l, 1e-300));
-            p[0] = l; p[1] = l; p[2] = m;
-            dp[0][0] = 1; dp[0][1] = 1; dp[0][2] = -2.0 * l / m;
+        case 3: {  // (l, l, m) by its angle from the z axis: l = sin(al) / sqrt 2, m = cos(al)
+            const T sa = std::sin(prm[0]), ca = std::cos(prm[0]);
+            p[0] = sa * r2; p[1] = sa * r2; p[2] = ca;
+            dp[0][0] = ca * r2; dp[0][1] = ca * r2; dp[0][2] = -sa;
             break;
         }
-        case 4: {
-            const double a = prm[0], q = std::sqrt(std::fmax(1.0 - a * a, 1e-300));
-            p[0] = a; p[1] = q; p[2] = 0;
-            dp[0][0] = 1; dp[0][1] = -a / q;
+        case 4: {  // (p, q, 0) by its angle from the y axis: p = sin(be), q = cos(be)
+            const T sb = std::sin(prm[0]), cb = std::cos(prm[0]);
+            p[0] = sb; p[1] = cb; p[2] = 0;
+            dp[0][0] = cb; dp[0][1] = -sb;
             break;
         }
         default: {
-            const double r = prm[0], s = prm[1], t = std::sqrt(std::fmax(1.0 - r * r - s * s, 1e-300));
+            const T r = prm[0], s = prm[1], t = std::sqrt(std::fmax(T(1) - r * r - s * s, T(1e-300)));
             p[0] = r; p[1] = s; p[2] = t;
             dp[0][0] = 1; dp[0][2] = -r / t;
             dp[1][1] = 1; dp[1][2] = -s / t;
@@ -122,13 +143,14 @@ void base_point(int kind, const double *prm, double p[3], double dp[2][3]) {
     }
 }
 // P = p4^A p6^B at p and its gradient
-double invariant(int A, int B, const double p[3], double g[3]) {
-    const double x2 = p[0] * p[0], y2 = p[1] * p[1], z2 = p[2] * p[2];
-    const double p4 = x2 * x2 + y2 * y2 + z2 * z2, p6 = x2 * y2 * z2;
-    const double P4 = std::pow(p4, A), P6 = std::pow(p6, B);
-    const double dP4 = A ? A * std::pow(p4, A - 1) : 0.0, dP6 = B ? B * std::pow(p6, B - 1) : 0.0;
-    const double d4[3] = {4 * p[0] * x2, 4 * p[1] * y2, 4 * p[2] * z2};
-    const double d6[3] = {2 * p[0] * y2 * z2, 2 * p[1] * x2 * z2, 2 * p[2] * x2 * y2};
+template <typename T>
+T invariant(int A, int B, const T p[3], T g[3]) {
+    const T x2 = p[0] * p[0], y2 = p[1] * p[1], z2 = p[2] * p[2];
+    const T p4 = x2 * x2 + y2 * y2 + z2 * z2, p6 = x2 * y2 * z2;
+    const T P4 = std::pow(p4, A), P6 = std::pow(p6, B);
+    const T dP4 = A ? A * std::pow(p4, A - 1) : T(0), dP6 = B ? B * std::pow(p6, B - 1) : T(0);
+    const T d4[3] = {4 * p[0] * x2, 4 * p[1] * y2, 4 * p[2] * z2};
+    const T d6[3] = {2 * p[0] * y2 * z2, 2 * p[1] * x2 * z2, 2 * p[2] * x2 * y2};
     for (int i = 0; i < 3; ++i) g[i] = dP4 * d4[i] * P6 + P4 * dP6 * d6[i];
     return P4 * P6;
 }
@@ -148,19 +170,20 @@ std::vector<int> orbit_kinds(const OrbitSpec &s) {
 }
 
 // residuals F and Jacobian J (row-major nv x nv) at unknowns v
-void eval(const Problem &pr, const std::vector<int> &kinds, const std::vector<double> &v, std::vector<double> &F,
-          std::vector<double> *J) {
+template <typename T>
+void eval_t(const Problem &pr, const std::vector<T> &target, const std::vector<int> &kinds, const std::vector<T> &v,
+            std::vector<T> &F, std::vector<T> *J) {
     const int ne = static_cast<int>(pr.inv.size()), nv = pr.nv, no = pr.no;
-    F.assign(ne, 0.0);
-    if (J) J->assign(static_cast<size_t>(ne) * nv, 0.0);
+    F.assign(ne, T(0));
+    if (J) J->assign(static_cast<size_t>(ne) * nv, T(0));
     int pi = no;
     for (int o = 0; o < no; ++o) {
         const int kind = kinds[o], np = kParams[kind];
-        double p[3], dp[2][3];
-        base_point(kind, &v[pi], p, dp);
+        T p[3], dp[2][3];
+        base_point<T>(kind, &v[pi], p, dp);
         for (int e = 0; e < ne; ++e) {
-            double g[3];
-            const double P = invariant(pr.inv[e].first, pr.inv[e].second, p, g);
+            T g[3];
+            const T P = invariant<T>(pr.inv[e].first, pr.inv[e].second, p, g);
             F[e] += v[o] * kSize[kind] * P;
             if (J) {
                 (*J)[static_cast<size_t>(e) * nv + o] = kSize[kind] * P;
@@ -173,32 +196,38 @@ void eval(const Problem &pr, const std::vector<int> &kinds, const std::vector<do
     }
     // rows scaled by 1 / target, so that every equation counts to relative precision
     for (int e = 0; e < ne; ++e) {
-        F[e] = F[e] / pr.target[e] - 1.0;
+        F[e] = F[e] / target[e] - T(1);
         if (J)
-            for (int k = 0; k < nv; ++k) (*J)[static_cast<size_t>(e) * nv + k] /= pr.target[e];
+            for (int k = 0; k < nv; ++k) (*J)[static_cast<size_t>(e) * nv + k] /= target[e];
     }
 }
 
+void eval(const Problem &pr, const std::vector<int> &kinds, const std::vector<double> &v, std::vector<double> &F,
+          std::vector<double> *J) {
+    eval_t<double>(pr, pr.target, kinds, v, F, J);
+}
+
 // solves (A) x = b, A n x n (copied), partial pivoting; false if singular
-bool solve_dense(std::vector<double> A, std::vector<double> b, int n, std::vector<double> &x) {
+template <typename T>
+bool solve_dense(std::vector<T> A, std::vector<T> b, int n, std::vector<T> &x) {
     for (int k = 0; k < n; ++k) {
         int piv = k;
         for (int i = k + 1; i < n; ++i)
             if (std::fabs(A[static_cast<size_t>(i) * n + k]) > std::fabs(A[static_cast<size_t>(piv) * n + k])) piv = i;
-        if (A[static_cast<size_t>(piv) * n + k] == 0.0) return false;
+        if (A[static_cast<size_t>(piv) * n + k] == T(0)) return false;
         if (piv != k) {
             for (int j = 0; j < n; ++j) std::swap(A[static_cast<size_t>(k) * n + j], A[static_cast<size_t>(piv) * n + j]);
             std::swap(b[k], b[piv]);
         }
         for (int i = k + 1; i < n; ++i) {
-            const double f = A[static_cast<size_t>(i) * n + k] / A[static_cast<size_t>(k) * n + k];
+            const T f = A[static_cast<size_t>(i) * n + k] / A[static_cast<size_t>(k) * n + k];
             for (int j = k; j < n; ++j) A[static_cast<size_t>(i) * n + j] -= f * A[static_cast<size_t>(k) * n + j];
             b[i] -= f * b[k];
         }
     }
-    x.assign(n, 0.0);
+    x.assign(n, T(0));
     for (int i = n - 1; i >= 0; --i) {
-        double s = b[i];
+        T s = b[i];
         for (int j = i + 1; j < n; ++j) s -= A[static_cast<size_t>(i) * n + j] * x[j];
         x[i] = s / A[static_cast<size_t>(i) * n + i];
     }
@@ -210,6 +239,11 @@ double norm2(const std::vector<double> &F) {
     for (double f : F) s += f * f;
     return s;
 }
+
+// squared norm of the relative residuals below which a rule counts as solved:
+// rounding level (the 230-point rule, whose axis orbit weighs -0.055 against
+// +0.004 to +0.017 elsewhere, stalls at 3e-14 per equation)
+constexpr double kSolvedF = 1e-26;
 
 // Levenberg-Marquardt from v; true when the residual vanishes to rounding
 bool levenberg_marquardt(const Problem &pr, const std::vector<int> &kinds, std::vector<double> &v) {
@@ -249,36 +283,68 @@ bool levenberg_marquardt(const Problem &pr, const std::vector<int> &kinds, std::
                 mu *= 10.0;
             }
         }
-        if (!moved) return f < 1e-30;
+        if (!moved) return f < kSolvedF;
         eval(pr, kinds, v, F, &J);
     }
-    return f < 1e-30;
+    return f < kSolvedF;
+}
+
+// whether the orbit weights w[o] (orbit kinds `kinds`) have the rule's
+// published sign pattern: negative exactly for the kinds in `negative`
+bool sign_pattern(const std::vector<int> &kinds, const double *w, int no, unsigned negative) {
+    for (int o = 0; o < no; ++o) {
+        const bool neg = (negative >> kinds[o]) & 1u;
+        if (neg ? !(w[o] < 0.0) : !(w[o] > 0.0)) return false;
+    }
+    return true;
+}
+
+// Newton steps on weights and parameters together in long double, from a
+// rule solved to double rounding; the rules with large cancellations between
+// orbit weights (230 and 266 points) are otherwise accurate to 1e-8 - 1e-10
+// only.  v is replaced when the extended residual falls below 1e-17.
+void polish_extended(const Problem &pr, const std::vector<int> &kinds, std::vector<double> &v) {
+    using X = long double;
+    const int n = pr.nv;
+    std::vector<X> tgt;
+    for (auto &ab : pr.inv) tgt.push_back(invariant_avg<X>(ab.first, ab.second));
+    std::vector<X> x(v.begin(), v.end()), F, J, d, rhs(n);
+    for (int it = 0; it < 8; ++it) {
+        eval_t<X>(pr, tgt, kinds, x, F, &J);
+        for (int i = 0; i < n; ++i) rhs[i] = -F[i];
+        if (!solve_dense<X>(J, rhs, n, d)) return;
+        for (int i = 0; i < n; ++i) x[i] += d[i];
+    }
+    eval_t<X>(pr, tgt, kinds, x, F, nullptr);
+    X worst = 0;
+    for (X f : F) worst = std::fmax(worst, std::fabs(f));
+    if (!(worst < X(1e-17))) return;
+    for (int i = 0; i < n; ++i) v[i] = static_cast<double>(x[i]);
 }
 
 // canonical orbit parameters; false if the solution is not an admissible
-// rule (non-positive weight, degenerate or repeated orbit)
-// negative_ok: the rule may carry a negative orbit weight (the 74-point rule
-// does: its 8-point (1,1,1)/sqrt(3) orbit weighs -0.0296)
-bool admissible(const std::vector<int> &kinds, std::vector<double> &v, int no, bool negative_ok) {
+// rule (weights off the published sign pattern, degenerate or repeated orbit;
+// the 74-point rule's (1,1,1)/sqrt(3) orbit, for one, weighs -0.0296)
+bool admissible(const std::vector<int> &kinds, std::vector<double> &v, int no, unsigned negative) {
     const double r2 = std::sqrt(0.5), r3 = std::sqrt(1.0 / 3.0), eps = 1e-6;
     std::vector<std::vector<double>> seen(6);
     int pi = no;
     for (int o = 0; o < no; ++o) {
-        if (!(v[o] > 0.0) && !(negative_ok && v[o] < 0.0)) return false;
+        const bool neg = (negative >> kinds[o]) & 1u;
+        if (neg ? !(v[o] < 0.0) : !(v[o] > 0.0)) return false;
         const int kind = kinds[o];
         if (kind == 3) {
-            double l = std::fabs(v[pi]);
+            const double l = std::fabs(std::sin(v[pi])) * r2;
             if (!(l > eps && l < r2 - eps) || std::fabs(l - r3) < eps) return false;
-            v[pi] = l;
+            v[pi] = std::asin(l / r2);  // the angle in (0, pi/2): z > 0
             for (double s : seen[3])
                 if (std::fabs(s - l) < eps) return false;
             seen[3].push_back(l);
         } else if (kind == 4) {
-            double a = std::fabs(v[pi]);
-            if (!(a < 1.0 - eps) || a < eps) return false;
-            a = std::fmin(a, std::sqrt(1.0 - a * a));  // (p, q, 0) and (q, p, 0) are one orbit
-            if (std::fabs(a - r2) < eps) return false;
-            v[pi] = a;
+            // (p, q, 0) and (q, p, 0) are one orbit: keep p = min(|sin|, |cos|)
+            double a = std::fmin(std::fabs(std::sin(v[pi])), std::fabs(std::cos(v[pi])));
+            if (a < eps || std::fabs(a - r2) < eps) return false;
+            v[pi] = std::asin(a);
             for (double s : seen[4])
                 if (std::fabs(s - a) < eps) return false;
             seen[4].push_back(a);
@@ -448,36 +514,57 @@ bool lm_projected(const Problem &pr, const std::vector<int> &kinds, std::vector<
     return f < 1e-24;
 }
 
-bool generate(const OrbitSpec &sp, LebedevQuad &q) {
-    Problem pr;
-    pr.sp = sp;
-    for (int A = 0; 4 * A <= sp.precision - 1; ++A)
-        for (int B = 0; 4 * A + 6 * B <= sp.precision - 1; ++B) pr.inv.push_back({A, B});
-    for (auto &ab : pr.inv) pr.target.push_back(invariant_avg(ab.first, ab.second));
-    const std::vector<int> kinds = orbit_kinds(sp);
-    pr.no = static_cast<int>(kinds.size());
-    pr.nv = pr.no;
-    for (int k : kinds) pr.nv += kParams[k];
-    if (pr.nv != static_cast<int>(pr.inv.size())) return false;  // not a square system
-    Rng rng{0x5EED0000ULL + static_cast<uint64_t>(sp.order)};
-    const double r2 = std::sqrt(0.5);
-    for (int trial = 0; trial < 4000; ++trial) {
-        // random orbit parameters; weights by least squares; then a Newton
-        // polish of weights and parameters together
+// One stream of trials (its own seed) for the rule of `pr`; returns true with
+// the rule in q when it finds an admissible solution, false when `stop` is
+// set (another stream succeeded) or its trials run out.
+bool search(const Problem &pr, const std::vector<int> &kinds, uint64_t seed, int max_trials,
+            const std::atomic<bool> &stop, LebedevQuad &q) {
+    const OrbitSpec &sp = pr.sp;
+    Rng rng{seed};
+    const double r2 = std::sqrt(0.5), kPi = std::acos(-1.0);
+    std::vector<double> best;   // orbit parameters of the smallest projected residual so far
+    double best_f = HUGE_VAL;
+
+    for (int trial = 0; trial < max_trials && !stop.load(std::memory_order_relaxed); ++trial) {
         std::vector<double> theta(pr.nv - pr.no);
-        int ti = 0;
-        for (int k : kinds) {
-            if (k == 3) theta[ti] = 0.02 + (r2 - 0.04) * rng.uniform();
-            if (k == 4) theta[ti] = 0.02 + (r2 - 0.04) * rng.uniform();
-            if (k == 5) {
-                const double a = 0.05 + 0.9 * rng.uniform(), b = 0.05 + 0.9 * rng.uniform();
-                const double sc = std::sqrt(a * a + b * b + 0.3);
-                theta[ti] = a / sc;
-                theta[ti + 1] = b / sc;
+        if ((trial & 1) && !best.empty()) {
+            // basin hop: a small random move of the best parameters so far,
+            // its size log-uniform in [0.002, 0.05]
+            theta = best;
+            const double scale = 0.002 * std::pow(25.0, rng.uniform());
+            for (double &t : theta) t += scale * (2.0 * rng.uniform() - 1.0);
+        } else {
+            // stratified start: the i-th orbit of a family in the i-th slice of its range
+            int ib = 0, ic = 0, id = 0, ti = 0;
+            for (int k : kinds) {
+                // angles: b orbits in (0.05, pi/2 - 0.002), c orbits in (0.05, pi/4 - 0.02)
+                if (k == 3) theta[ti] = 0.05 + (0.5 * kPi - 0.052) * (ib++ + rng.uniform()) / sp.nb;
+                if (k == 4) theta[ti] = 0.05 + (0.25 * kPi - 0.07) * (ic++ + rng.uniform()) / sp.nc;
+                if (k == 5) {  // a point of the octant: azimuth slice, random polar angle
+                    const double ph = 0.25 * kPi * (0.1 + 0.8 * (id++ + rng.uniform()) / sp.nd);
+                    const double th = 0.3 + 0.6 * rng.uniform();
+                    theta[ti] = std::sin(th) * std::cos(ph);
+                    theta[ti + 1] = std::sin(th) * std::sin(ph);
+                }
+                ti += kParams[k];
             }
-            ti += kParams[k];
         }
-        if (!lm_projected(pr, kinds, theta)) continue;
+        const bool solved = lm_projected(pr, kinds, theta);
+        {
+            std::vector<double> w0;
+            const double f0 = norm2(projected_residual(pr, kinds, theta, w0));
+            if (f0 < best_f) {
+                best_f = f0;
+                best = theta;
+            }
+            // a solution of the wrong sign pattern: look elsewhere
+            if (solved && !sign_pattern(kinds, w0.data(), pr.no, sp.negative)) {
+                best.clear();
+                best_f = HUGE_VAL;
+                continue;
+            }
+        }
+        if (!solved) continue;
         std::vector<double> wts;
         projected_residual(pr, kinds, theta, wts);
         std::vector<double> v(pr.nv);
@@ -485,12 +572,13 @@ bool generate(const OrbitSpec &sp, LebedevQuad &q) {
         for (size_t i = 0; i < theta.size(); ++i) v[pr.no + i] = theta[i];
         int pi = pr.no;
         if (!levenberg_marquardt(pr, kinds, v)) continue;
-        if (!admissible(kinds, v, pr.no, sp.order == 74 || getenv("LEB_NEG") != nullptr)) continue;
+        polish_extended(pr, kinds, v);
+        if (!admissible(kinds, v, pr.no, sp.negative)) continue;
         std::vector<double> F;
         eval(pr, kinds, v, F, nullptr);
         double worst = 0.0;
         for (size_t e = 0; e < F.size(); ++e) worst = std::fmax(worst, std::fabs(F[e]));
-        if (worst > 1e-14) continue;
+        if (worst > 1e-13) continue;
         q.x.clear();
         q.y.clear();
         q.z.clear();
@@ -506,6 +594,38 @@ bool generate(const OrbitSpec &sp, LebedevQuad &q) {
     return false;
 }
 
+bool generate(const OrbitSpec &sp, LebedevQuad &q) {
+    Problem pr;
+    pr.sp = sp;
+    for (int A = 0; 4 * A <= sp.precision - 1; ++A)
+        for (int B = 0; 4 * A + 6 * B <= sp.precision - 1; ++B) pr.inv.push_back({A, B});
+    for (auto &ab : pr.inv) pr.target.push_back(invariant_avg<double>(ab.first, ab.second));
+    const std::vector<int> kinds = orbit_kinds(sp);
+    pr.no = static_cast<int>(kinds.size());
+    pr.nv = pr.no;
+    for (int k : kinds) pr.nv += kParams[k];
+    if (pr.nv != static_cast<int>(pr.inv.size())) return false;  // not a square system
+    // independent search streams on the host's threads; the first admissible
+    // solution wins (every stream looks for the same published solution: the
+    // orbit structure and sign pattern single it out; streams differ only in
+    // their rounding)
+    std::atomic<bool> found{false};
+    bool ok = false;
+#pragma omp parallel
+    {
+        LebedevQuad mine;
+        const uint64_t seed = 0x5EED0000ULL + static_cast<uint64_t>(sp.order) + 7919ull * omp_get_thread_num();
+        if (search(pr, kinds, seed, 20000, found, mine)) {
+#pragma omp critical(transfer_lebedev)
+            if (!found.exchange(true)) {
+                q = mine;
+                ok = true;
+            }
+        }
+    }
+    return ok;
+}
+
 std::mutex g_cache_mutex;
 std::map<int, LebedevQuad> g_cache;
 
@@ -516,7 +636,7 @@ LebedevQuad::LebedevQuad(int mindegree) {
     const OrbitSpec *spec = nullptr;
     for (const OrbitSpec &s : kSpecs)
         if (s.order == order) spec = &s;
-    if (!spec) throw std::runtime_error("LebedevQuad: rules above 194 points (precision 23) are not generated");
+    if (!spec) throw std::runtime_error("LebedevQuad: rules above 350 points (precision 31) are not generated");
     std::lock_guard<std::mutex> lock(g_cache_mutex);
     auto it = g_cache.find(order);
     if (it == g_cache.end()) {

@@ -15,21 +15,36 @@
 // a_hi w_hi + a_hi w_lo + a_lo w_hi are summed, a_lo w_lo (~2^-22) dropped.
 //
 // Layout and roles (one CTA per SM, persistent over 128-row tiles):
-//   A (psi)   TMA tiles of 32 rows x 32 ordinates (128-byte swizzle), four per
-//             stage: a stage is 128 rows x 32 ordinates, MN-major (rows
-//             contiguous), kStages stages in flight;
+//   A (psi)   TMA tiles of 32 rows x 32 ordinates, four per stage: a stage is
+//             128 rows x 32 ordinates, MN-major (rows contiguous), as many
+//             stages in flight as shared memory holds beside the weights (up
+//             to kMaxStages, 160 KB: HBM latency under full load needs about
+//             that much in flight per SM; 6 stages reached 3.5 TB/s).  MN-major TF32 operands take one shared-memory
+//             form, the 128-byte swizzle on 32-byte units (atoms of 32 rows x 4
+//             ordinates, 512 B; the 32-byte chunk index of each 128-byte
+//             ordinate row XORed with the row's index mod 4), which TMA writes
+//             in its SWIZZLE_128B_ATOM_32B mode;
 //   B (W)     [w_hi | w_lo] as one N = 32 operand, K-major, built in shared
 //             memory once per CTA from the FP64 weights;
 //   a_lo      written by the split warps into tensor memory (tcgen05.st), the
-//             A operand of the third product (A from tensor memory);
-//   D         two 128 x 32 FP32 accumulators in tensor memory (columns 0-15:
-//             a w_hi + a_lo w_hi, 16-31: a w_lo), double-buffered per tile.
+//             A operand of the third product (A from tensor memory), in
+//             kLoSlots slots of its own, each freed when its products finish;
+//   D         per tile (double-buffered) kAccGroups 128 x 32 FP32 accumulators
+//             of a [w_hi | w_lo], the 8-ordinate steps dealt to them in turn,
+//             and one 128 x 16 accumulator of a_lo w_hi, in tensor memory.  The
+//             tensor core's FP32 accumulation truncates, so each accumulation
+//             into a running sum loses about half an ulp the same way; dealing
+//             the steps over four accumulators and summing them in FP64 cuts
+//             that bias fourfold (80 accumulations into one sum at 308
+//             ordinates left moments 5e-6 low).
 //   warp 0    TMA producer (and tensor-memory allocation);
 //   warp 1    MMA issuer: per 8-ordinate step one N = 32 product from shared
 //             memory and one N = 16 product with A from tensor memory;
-//   warps 4-7 split a stage (a_lo = a - trunc(a)) into tensor memory, and
-//             read each finished tile's accumulators back (tcgen05.ld), add
-//             the two halves and store the 16 moments (FP64).
+//   warps 4-11 split each stage (a_lo = a - trunc(a)) into tensor memory,
+//             two warpgroups of 16 ordinates each;
+//   warps 12-15 read each finished tile's accumulators back (tcgen05.ld), sum
+//             them in FP64 and store the 16 moments, while the split warps
+//             go on with the next tile (the accumulators are double-buffered).
 // Every wait is bounded (kWaitNs of the global timer): past it the kernel
 // sets bit 0 of *err, every role stops, in-flight copies and products are
 // waited for (bounded), tensor memory is freed and the kernel returns.
@@ -46,15 +61,20 @@ namespace {
 
 constexpr int kTileM = 128;        // rows per tile (one MMA M)
 constexpr int kStageK = 32;        // ordinates per stage
-constexpr int kStages = 6;
+constexpr int kMaxStages = 10;     // shared-memory stages (the launch picks how many fit)
+constexpr uint32_t kLoSlots = 4;   // tensor-memory slots of a_lo
 constexpr int kAtomBytes = 32 * 4 * kStageK;         // 32 rows x 32 ordinates x 4 B = 4 KB
 constexpr int kStageBytes = 4 * kAtomBytes;          // 16 KB
-constexpr int kThreads = 256;
-constexpr uint32_t kTmemCols = 256;                  // 2 x 32 accumulator + kStages x 32 a_lo
-constexpr uint32_t kLoCol0 = 64;
+constexpr uint32_t kSplitWarps = 8;                  // warps 4-11; warps 12-15 drain the accumulators
+constexpr int kThreads = 32 * (4 + kSplitWarps + 4);
+constexpr uint32_t kAccGroups = 4;                   // accumulators of a [w_hi | w_lo] per tile
+constexpr uint32_t kBufCols = 160;                   // kAccGroups x 32 + 16 (a_lo w_hi) + 16 spare
+constexpr uint32_t kTmemCols = 512;                  // 2 tile buffers + kLoSlots x 32 a_lo
+constexpr uint32_t kLoCol0 = 2 * kBufCols;
 constexpr unsigned long long kWaitNs = 1000000000ull;  // 1 s per wait
 
-static_assert(kLoCol0 + kStages * kStageK <= kTmemCols, "tensor-memory plan");
+static_assert(kLoCol0 + kLoSlots * kStageK <= kTmemCols, "tensor-memory plan");
+constexpr int kSmemHeader = 1024;  // barriers and flags, ahead of the 1024-aligned stages
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -111,14 +131,14 @@ __device__ __forceinline__ bool mbar_wait_warp(uint32_t bar, uint32_t parity, vo
     return __shfl_sync(0xffffffffu, ok, 0) != 0;
 }
 
-// UMMA shared-memory descriptors (version 1).  A: MN-major, 128-byte swizzle,
-// 32-row atoms 4 KB apart (leading offset), 8-ordinate groups 1 KB apart
-// (stride offset).  B: K-major, no swizzle, 8 x 16-byte core matrices; the
+// UMMA shared-memory descriptors (version 1).  A: MN-major, 128-byte swizzle
+// with a 32-byte base (layout type 1), 32-row atoms 4 KB apart (leading
+// offset), 4-ordinate groups 512 B apart (stride offset).  B: K-major, no swizzle, 8 x 16-byte core matrices; the
 // next 4 ordinates 512 B on (leading offset), the next 8 harmonics 128 B on
 // (stride offset).
 __device__ __forceinline__ uint64_t desc_a(uint32_t saddr) {
     return static_cast<uint64_t>((saddr >> 4) & 0x3FFFu) | (static_cast<uint64_t>(4096 >> 4) << 16) |
-           (static_cast<uint64_t>(1024 >> 4) << 32) | (1ull << 46) | (2ull << 61);
+           (static_cast<uint64_t>(512 >> 4) << 32) | (1ull << 46) | (1ull << 61);
 }
 __device__ __forceinline__ uint64_t desc_b(uint32_t saddr) {
     return static_cast<uint64_t>((saddr >> 4) & 0x3FFFu) | (static_cast<uint64_t>(512 >> 4) << 16) |
@@ -169,6 +189,14 @@ __device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&v)[32
         "r"(v[25]), "r"(v[26]), "r"(v[27]), "r"(v[28]), "r"(v[29]), "r"(v[30]), "r"(v[31])
         : "memory");
 }
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&v)[16]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+        "%14, %15, %16};" ::"r"(taddr),
+        "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]),
+        "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15])
+        : "memory");
+}
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32]) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
@@ -186,7 +214,7 @@ __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.
 __device__ __forceinline__ float tf32_trunc(float x) { return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u); }
 
 struct Smem {
-    uint64_t full[kStages], empty[kStages], lo_ready[kStages];
+    uint64_t full[kMaxStages], empty[kMaxStages], lo_ready[kLoSlots], lo_empty[kLoSlots];
     uint64_t acc_full[2], acc_empty[2], drain;
     uint32_t tmem_base;
     int abort_flag;
@@ -196,13 +224,15 @@ struct Smem {
 
 __global__ void __launch_bounds__(kThreads, 1)
     k_moments_tcgen05(const __grid_constant__ CUtensorMap psi_map, uint32_t M, uint32_t nq, uint32_t nqp,
-                      const double *__restrict__ W, int nmom, double *__restrict__ mom, unsigned int *err) {
+                      const double *__restrict__ W, int nmom, double *__restrict__ mom, unsigned int *err,
+                      uint32_t nstages) {
     extern __shared__ uint8_t smem_raw[];
-    // 1024-byte aligned base: the 128-byte swizzle pattern repeats every 1 KB
+    // 1024-byte aligned base (the swizzle pattern repeats every 512 B)
     uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint8_t *smA = base;                                   // kStages x 16 KB
-    uint8_t *smB = smA + kStages * kStageBytes;            // nqp x 128 B
-    Smem &sh = *reinterpret_cast<Smem *>(smB + static_cast<size_t>(nqp) * 128);
+    static_assert(sizeof(Smem) <= kSmemHeader, "barrier header");
+    Smem &sh = *reinterpret_cast<Smem *>(base);
+    uint8_t *smA = base + kSmemHeader;                     // nstages x 16 KB (1024-aligned)
+    uint8_t *smB = smA + nstages * kStageBytes;            // nqp x 128 B
     volatile int *abort_flag = &sh.abort_flag;
 
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
@@ -218,10 +248,13 @@ __global__ void __launch_bounds__(kThreads, 1)
         *reinterpret_cast<float *>(smB + off) = v;
     }
     if (threadIdx.x == 0) {
-        for (int s = 0; s < kStages; ++s) {
+        for (uint32_t s = 0; s < nstages; ++s) {
             mbar_init(smem_u32(&sh.full[s]), 1);
             mbar_init(smem_u32(&sh.empty[s]), 1);
-            mbar_init(smem_u32(&sh.lo_ready[s]), 4);
+        }
+        for (uint32_t l = 0; l < kLoSlots; ++l) {
+            mbar_init(smem_u32(&sh.lo_ready[l]), kSplitWarps);
+            mbar_init(smem_u32(&sh.lo_empty[l]), 1);
         }
         for (int b = 0; b < 2; ++b) {
             mbar_init(smem_u32(&sh.acc_full[b]), 1);
@@ -252,7 +285,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         bool ok = true;
         for (uint32_t tile = blockIdx.x; ok && tile < tiles; tile += gridDim.x)
             for (uint32_t ks = 0; ks < nks; ++ks, ++it) {
-                const uint32_t s = it % kStages, ph = (it / kStages) & 1u;
+                const uint32_t s = it % nstages, ph = (it / nstages) & 1u;
                 if (!(ok = mbar_wait(smem_u32(&sh.empty[s]), ph ^ 1u, abort_flag, err))) break;
                 const uint32_t fb = smem_u32(&sh.full[s]);
                 mbar_expect_tx(fb, kStageBytes);
@@ -264,8 +297,8 @@ __global__ void __launch_bounds__(kThreads, 1)
                 inflight = it + 1;
             }
         if (!ok) {  // aborted: wait (bounded, own timer) for the copies already issued
-            for (uint32_t j = inflight > kStages ? inflight - kStages : 0; j < inflight; ++j) {
-                const uint32_t bar = smem_u32(&sh.full[j % kStages]), ph = (j / kStages) & 1u;
+            for (uint32_t j = inflight > nstages ? inflight - nstages : 0; j < inflight; ++j) {
+                const uint32_t bar = smem_u32(&sh.full[j % nstages]), ph = (j / nstages) & 1u;
                 const unsigned long long t0 = global_ns();
                 while (!mbar_try(bar, ph) && global_ns() - t0 < kWaitNs) {
                 }
@@ -280,21 +313,25 @@ __global__ void __launch_bounds__(kThreads, 1)
             const uint32_t b = tcount & 1u, bph = (tcount >> 1) & 1u;
             if (!(ok = mbar_wait(smem_u32(&sh.acc_empty[b]), bph ^ 1u, abort_flag, err))) break;
             tc_fence_after();
-            const uint32_t d = tmem + 32u * b;
+            const uint32_t d = tmem + kBufCols * b;
             for (uint32_t ks = 0; ks < nks; ++ks, ++it) {
-                const uint32_t s = it % kStages, ph = (it / kStages) & 1u;
+                const uint32_t s = it % nstages, ph = (it / nstages) & 1u;
+                const uint32_t l = it % kLoSlots, lph = (it / kLoSlots) & 1u;
                 if (!(ok = mbar_wait(smem_u32(&sh.full[s]), ph, abort_flag, err))) break;
-                if (!(ok = mbar_wait(smem_u32(&sh.lo_ready[s]), ph, abort_flag, err))) break;
+                if (!(ok = mbar_wait(smem_u32(&sh.lo_ready[l]), lph, abort_flag, err))) break;
                 tc_fence_after();
                 const uint32_t a0 = smem_u32(smA + s * kStageBytes);
                 const uint32_t b0 = smem_u32(smB) + ks * 4u * 1024u;
 #pragma unroll
                 for (uint32_t kk = 0; kk < 4; ++kk) {
+                    // 8-ordinate step kk of this stage goes to accumulator kk
+                    // (4 steps a stage); each starts from zero in the first stage
                     const uint64_t bd = desc_b(b0 + kk * 1024u);
-                    mma_ss(d, desc_a(a0 + kk * 1024u), bd, id_hi, (ks | kk) != 0u);
-                    mma_ts(d, tmem + kLoCol0 + kStageK * s + 8u * kk, bd, id_lo, 1u);
+                    mma_ss(d + 32u * kk, desc_a(a0 + kk * 1024u), bd, id_hi, ks != 0u);
+                    mma_ts(d + 32u * kAccGroups, tmem + kLoCol0 + kStageK * l + 8u * kk, bd, id_lo, (ks | kk) != 0u);
                 }
-                mma_commit(smem_u32(&sh.empty[s]));  // stage and its a_lo slot free once these finish
+                mma_commit(smem_u32(&sh.empty[s]));     // the stage is free once these finish,
+                mma_commit(smem_u32(&sh.lo_empty[l]));  // and so is its a_lo slot
             }
             if (!ok) break;
             mma_commit(smem_u32(&sh.acc_full[b]));
@@ -304,39 +341,60 @@ __global__ void __launch_bounds__(kThreads, 1)
         const unsigned long long t0 = global_ns();
         while (!mbar_try(smem_u32(&sh.drain), 0) && global_ns() - t0 < kWaitNs) {
         }
-    } else if (warp >= 4) {
-        // ---- split (a_lo into tensor memory) and epilogue
-        const uint32_t wq = warp - 4;                        // lanes 32 wq .. 32 wq + 31
+    } else if (warp >= 4 && warp < 4 + kSplitWarps) {
+        // ---- split: a_lo of 16 ordinates of the stage into tensor memory;
+        // warp w handles lanes 32 (w % 4) .. + 31 and ordinates 16 h .. + 15
+        const uint32_t wq = warp & 3u, h = (warp - 4) >> 2;
         const uint32_t lane_addr = (32u * wq) << 16;
-        uint32_t it = 0, tcount = 0;
+        uint32_t it = 0;
         bool ok = true;
-        for (uint32_t tile = blockIdx.x; ok && tile < tiles; tile += gridDim.x, ++tcount) {
+        for (uint32_t tile = blockIdx.x; ok && tile < tiles; tile += gridDim.x)
             for (uint32_t ks = 0; ks < nks; ++ks, ++it) {
-                const uint32_t s = it % kStages, ph = (it / kStages) & 1u;
+                const uint32_t s = it % nstages, ph = (it / nstages) & 1u;
+                const uint32_t l = it % kLoSlots, lph = (it / kLoSlots) & 1u;
                 if (!(ok = mbar_wait_warp(smem_u32(&sh.full[s]), ph, abort_flag, err))) break;
+                if (!(ok = mbar_wait_warp(smem_u32(&sh.lo_empty[l]), lph ^ 1u, abort_flag, err))) break;
+                tc_fence_after();
                 // row 32 wq + lane of the stage: atom wq, word lane of each
-                // 128-byte ordinate row (16-byte chunk c stored at c ^ (row % 8))
+                // 128-byte ordinate row (32-byte chunk c stored at c ^ (k % 4))
                 const uint8_t *atom = smA + s * kStageBytes + wq * kAtomBytes;
-                uint32_t lo[32];
+                uint32_t lo[16];
 #pragma unroll
-                for (int k = 0; k < 32; ++k) {
-                    const uint32_t off = k * 128 + ((((lane >> 2) ^ (k & 7)) << 4)) + (lane & 3u) * 4;
+                for (int j = 0; j < 16; ++j) {
+                    const uint32_t k = 16u * h + j;
+                    const uint32_t off = k * 128 + (((lane >> 3) ^ (k & 3u)) << 5) + (lane & 7u) * 4;
                     const float a = *reinterpret_cast<const float *>(atom + off);
-                    lo[k] = __float_as_uint(a - tf32_trunc(a));
+                    lo[j] = __float_as_uint(a - tf32_trunc(a));
                 }
-                tmem_st32(tmem + lane_addr + kLoCol0 + kStageK * s, lo);
+                tmem_st16(tmem + lane_addr + kLoCol0 + kStageK * l + 16u * h, lo);
                 tmem_wait_st();
                 tc_fence_before();
                 __syncwarp();
-                if (lane == 0) mbar_arrive(smem_u32(&sh.lo_ready[s]));
+                if (lane == 0) mbar_arrive(smem_u32(&sh.lo_ready[l]));
             }
-            if (!ok) break;
+    } else if (warp >= 4 + kSplitWarps) {
+        // ---- epilogue: each finished tile's accumulators, summed in FP64
+        const uint32_t wq = warp & 3u;
+        const uint32_t lane_addr = (32u * wq) << 16;
+        uint32_t tcount = 0;
+        for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++tcount) {
             const uint32_t b = tcount & 1u, bph = (tcount >> 1) & 1u;
-            if (!(ok = mbar_wait_warp(smem_u32(&sh.acc_full[b]), bph, abort_flag, err))) break;
+            if (!mbar_wait_warp(smem_u32(&sh.acc_full[b]), bph, abort_flag, err)) break;
             tc_fence_after();
-            uint32_t v[32];
-            tmem_ld32(tmem + lane_addr + 32u * b, v);
-            tmem_wait_ld();
+            double acc[16];
+#pragma unroll
+            for (int n = 0; n < 16; ++n) acc[n] = 0.0;
+            const uint32_t t0 = tmem + lane_addr + kBufCols * b;
+#pragma unroll 1
+            for (uint32_t g = 0; g <= kAccGroups; ++g) {  // the kAccGroups sums, then a_lo w_hi (16 columns)
+                uint32_t v[32];
+                tmem_ld32(t0 + 32u * g, v);
+                tmem_wait_ld();
+#pragma unroll
+                for (int n = 0; n < 16; ++n)
+                    acc[n] += static_cast<double>(__uint_as_float(v[n])) +
+                              (g < kAccGroups ? static_cast<double>(__uint_as_float(v[16 + n])) : 0.0);
+            }
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_u32(&sh.acc_empty[b]));
@@ -344,9 +402,7 @@ __global__ void __launch_bounds__(kThreads, 1)
             if (row < M) {
 #pragma unroll
                 for (int n = 0; n < 16; ++n)
-                    if (n < nmom)
-                        mom[static_cast<uint64_t>(n) * M + row] = static_cast<double>(__uint_as_float(v[n])) +
-                                                                  static_cast<double>(__uint_as_float(v[16 + n]));
+                    if (n < nmom) mom[static_cast<uint64_t>(n) * M + row] = acc[n];
             }
         }
     }
@@ -360,13 +416,29 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
 }
 
-size_t moments_tcgen05_smem(uint32_t nq) {
+namespace {
+constexpr size_t kSmemLimit = 227u * 1024u;
+// shared memory of a launch with `stages` stages for nq ordinates: alignment
+// slack, the barrier header, the stages and the weight table
+size_t smem_bytes(uint32_t nq, uint32_t stages) {
     const uint32_t nqp = (nq + kStageK - 1) / kStageK * kStageK;
-    return 1024 + static_cast<size_t>(kStages) * kStageBytes + static_cast<size_t>(nqp) * 128 + sizeof(Smem);
+    return 1024 + kSmemHeader + static_cast<size_t>(stages) * kStageBytes + static_cast<size_t>(nqp) * 128;
+}
+// the most stages (<= kMaxStages) that fit beside the weights; 0 if fewer than 3
+uint32_t stages_for(uint32_t nq) {
+    for (uint32_t st = kMaxStages; st >= 3; --st)
+        if (smem_bytes(nq, st) <= kSmemLimit) return st;
+    return 0;
+}
+}  // namespace
+
+size_t moments_tcgen05_smem(uint32_t nq) {
+    const uint32_t st = stages_for(nq);
+    return st ? smem_bytes(nq, st) : 0;
 }
 
 bool moments_tcgen05_supported(uint32_t M, uint32_t nq) {
-    return M > 0 && M % 4 == 0 && nq > 0 && moments_tcgen05_smem(nq) <= 227u * 1024u;
+    return M > 0 && M % 4 == 0 && nq > 0 && stages_for(nq) != 0;
 }
 
 namespace {
@@ -398,7 +470,7 @@ cudaError_t launch_moments_tcgen05(const float *psi, uint32_t M, uint32_t nq, co
     const cuuint32_t box[2] = {32, kStageK};
     const cuuint32_t estr[2] = {1, 1};
     if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(psi), dims, strides, box, estr,
-            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
         return cudaErrorInvalidValue;
     const size_t smem = moments_tcgen05_smem(nq);
@@ -412,7 +484,7 @@ cudaError_t launch_moments_tcgen05(const float *psi, uint32_t M, uint32_t nq, co
     const uint32_t tiles = (M + kTileM - 1) / kTileM;
     const int grid = static_cast<int>(tiles < static_cast<uint32_t>(num_sms) ? tiles : num_sms);
     const uint32_t nqp = (nq + kStageK - 1) / kStageK * kStageK;
-    k_moments_tcgen05<<<grid, kThreads, smem, stream>>>(map, M, nq, nqp, W, nmom, mom, err);
+    k_moments_tcgen05<<<grid, kThreads, smem, stream>>>(map, M, nq, nqp, W, nmom, mom, err, stages_for(nq));
     return cudaGetLastError();
 }
 

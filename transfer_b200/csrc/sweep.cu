@@ -726,6 +726,36 @@ __global__ void __launch_bounds__(kSweepThreads) k_sweep_batch(const SweepJob<T>
     sweep_block<T, SMALL>(g, sc, a, blockIdx.x - jobs[lo].block0);
 }
 
+// The same tasks taken from a queue: a persistent grid (as many blocks as are
+// resident) in which each block draws task indices from an atomic ticket
+// until they run out.  Task t is ordinate t - block0 of the job owning it, in
+// the jobs' order (largest problems first).  The ticket must be zero at launch
+// (the host clears it before each launch); every draw consumes one index, so
+// the loop ends after at most ntasks / gridDim.x + 1 draws per block.
+template <typename T, bool SMALL>
+__global__ void __launch_bounds__(kSweepThreads) k_sweep_queue(const SweepJob<T> *__restrict__ jobs, int njobs,
+                                                               uint32_t ntasks, unsigned int *ticket) {
+    __shared__ uint32_t drawn;
+    for (;;) {
+        if (threadIdx.x == 0) drawn = atomicAdd(ticket, 1u);
+        __syncthreads();
+        const uint32_t t = drawn;
+        __syncthreads();  // all have read it before thread 0 draws again
+        if (t >= ntasks) break;
+        int lo = 0, hi = njobs - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) / 2;
+            if (jobs[mid].block0 <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        const Geom<T> g = jobs[lo].g;
+        const Sched sc = jobs[lo].sc;
+        const SweepArgs<T> a = jobs[lo].a;
+        sweep_block<T, SMALL>(g, sc, a, t - jobs[lo].block0);
+        __syncthreads();  // the block's shared memory is free for the next task
+    }
+}
+
 // B_out of the reflective faces: the inflow of each (face, incoming q)
 // entry is the outflow of the mirrored ordinate at the same face (same
 // vertex values; the face's opposite vertex left zero)
@@ -1467,6 +1497,13 @@ struct tr_sweep {
     int mom_kernel = TR_MOMENTS_TCGEN05;
     unsigned int *mom_err = nullptr;  // pipeline-timeout flag of k_moments_tcgen05
     int shape32 = -1;              // FP32 sweep shape: -1 by rule, 0 full, 1 small (tr_sweep_autotune)
+    // frequency groups (tr_sweep_create_group): a group shares its parent's
+    // geometry, ordinates, schedule and task records and owns its
+    // coefficients and state; the parent counts its live groups
+    tr_sweep *parent = nullptr;
+    int groups = 0;
+    int batch_cfg = -1;            // batched launch form (tr_sweep_autotune_batch): -1 by rule
+    unsigned int *qticket = nullptr;  // ticket of the work-queue launch (k_sweep_queue)
 };
 
 static tr_status sw_err(tr_sweep *s, tr_status st, const std::string &m) {
@@ -1495,8 +1532,17 @@ static cudaError_t sw_upload(tr_sweep *s, T **p, const std::vector<T> &h) {
     return cudaMemcpy(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice);
 }
 
+// frees one allocation made by sw_alloc (work space released between uses)
+static void sw_release(tr_sweep *s, void *p) {
+    if (!p) return;
+    auto it = std::find(s->allocs.begin(), s->allocs.end(), p);
+    if (it != s->allocs.end()) s->allocs.erase(it);
+    cudaFree(p);
+}
+
 static void sw_free(tr_sweep *s) {
     if (!s) return;
+    if (s->parent) --s->parent->groups;
     int prev = 0;
     cudaGetDevice(&prev);
     cudaSetDevice(s->device);
@@ -1535,6 +1581,9 @@ void sort3(uint32_t *v) {
     if (v[0] > v[1]) std::swap(v[0], v[1]);
 }
 }  // namespace
+
+template <typename T, bool SMALL>
+static cudaError_t queue_setup();  // the work-queue kernels' attributes and occupancy
 
 static tr_status sweep_setup(tr_sweep *S, const tr_mesh_view *m, const tr_physics_view *ph,
                              const tr_ordinates_view *o) {
@@ -1863,6 +1912,9 @@ static tr_status sweep_setup(tr_sweep *S, const tr_mesh_view *m, const tr_physic
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_sweep_batch<float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  static_cast<int>(SweepShape<float, true>::smem));
+    if (e == cudaSuccess) e = queue_setup<double, false>();
+    if (e == cudaSuccess) e = queue_setup<float, false>();
+    if (e == cudaSuccess) e = queue_setup<float, true>();
     if (e == cudaSuccess) e = cudaEventCreate(&S->ev[0]);
     if (e == cudaSuccess) e = cudaEventCreate(&S->ev[1]);
     if (e != cudaSuccess) return sw_cuda(S, e, "sweep: allocation");
@@ -2252,6 +2304,59 @@ static cudaError_t gmres(tr_sweep *S, int prec, int prec_res, const double *b, d
     return cudaSuccess;
 }
 
+// Batched launch forms (tr_sweep_autotune_batch): a static grid of one block
+// per (problem, ordinate) task or a persistent grid drawing tasks from a
+// queue, each with the full shared-memory shape (4,096-position ring, one
+// block per SM) or, for FP32, the small one (1,024 positions, two per SM).
+enum BatchForm { kBatchStaticFull = 0, kBatchStaticSmall = 1, kBatchQueueFull = 2, kBatchQueueSmall = 3 };
+constexpr int kBatchForms = 4;
+
+// resident blocks per SM of the queue kernels (FP64 full, FP32 full, FP32
+// small), found once at sweep set-up -- outside any stream capture
+static int g_queue_per_sm[3] = {0, 0, 0};
+template <typename T, bool SMALL>
+static constexpr int queue_slot() { return sizeof(T) == 8 ? 0 : (SMALL ? 2 : 1); }
+template <typename T, bool SMALL>
+static cudaError_t queue_setup() {
+    cudaError_t e = cudaFuncSetAttribute(k_sweep_queue<T, SMALL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(SweepShape<T, SMALL>::smem));
+    int per_sm = 0;
+    if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_queue<T, SMALL>, kSweepThreads,
+                                                          SweepShape<T, SMALL>::smem);
+    g_queue_per_sm[queue_slot<T, SMALL>()] = std::max(per_sm, 1);
+    return e;
+}
+
+template <typename T, bool SMALL>
+static cudaError_t launch_queue(const SweepJob<T> *dj, int n, uint32_t tasks, unsigned int *ticket, int num_sms,
+                                cudaStream_t st) {
+    const int per_sm = std::max(g_queue_per_sm[queue_slot<T, SMALL>()], 1);
+    const uint32_t grid = std::min<uint32_t>(tasks, static_cast<uint32_t>(per_sm * num_sms));
+    cudaError_t e = cudaMemsetAsync(ticket, 0, sizeof(unsigned int), st);
+    if (e == cudaSuccess)
+        k_sweep_queue<T, SMALL><<<grid, kSweepThreads, SweepShape<T, SMALL>::smem, st>>>(dj, n, tasks, ticket);
+    return e;
+}
+
+// One batched sweep launch in the form the first problem carries (-1: the
+// rule -- static grid, small shape for FP32 when the tasks outnumber the SMs).
+template <typename T>
+static void launch_batch(tr_sweep *s0, const SweepJob<T> *dj, int n, uint32_t tasks, cudaStream_t st) {
+    int form = s0->batch_cfg;
+    if (form < 0) form = (sizeof(T) == 4 && tasks > static_cast<uint32_t>(s0->num_sms)) ? kBatchStaticSmall
+                                                                                        : kBatchStaticFull;
+    const bool small = sizeof(T) == 4 && (form == kBatchStaticSmall || form == kBatchQueueSmall);
+    if (form == kBatchQueueFull || form == kBatchQueueSmall) {
+        if (small) launch_queue<T, sizeof(T) == 4>(dj, n, tasks, s0->qticket, s0->num_sms, st);
+        else launch_queue<T, false>(dj, n, tasks, s0->qticket, s0->num_sms, st);
+    } else if (small) {
+        k_sweep_batch<T, sizeof(T) == 4><<<tasks, kSweepThreads, SweepShape<T, sizeof(T) == 4>::smem, st>>>(dj, n);
+    } else {
+        k_sweep_batch<T, false><<<tasks, kSweepThreads, SweepShape<T, false>::smem, st>>>(dj, n);
+    }
+}
+
 // Problem order in a batched launch: largest first (cells, then index), so
 // that the blocks with the longest walks start in the first wave and the
 // last wave holds short ones (blocks start in index order).
@@ -2295,11 +2400,9 @@ static cudaError_t batch_sweep(int n, tr_sweep *const *s, cudaStream_t st, const
     SweepJob<T> *dj = nullptr;
     cudaError_t e = cudaMalloc(&dj, sizeof(SweepJob<T>) * n);
     if (e == cudaSuccess) e = cudaMemcpyAsync(dj, jobs.data(), sizeof(SweepJob<T>) * n, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && !s[0]->qticket) e = sw_alloc(s[0], &s[0]->qticket, 1);
     if (e == cudaSuccess) {
-        if (sizeof(T) == 4 && blocks > static_cast<uint32_t>(s[0]->num_sms))  // two ordinates per SM
-            k_sweep_batch<T, sizeof(T) == 4><<<blocks, kSweepThreads, SweepShape<T, sizeof(T) == 4>::smem, st>>>(dj, n);
-        else
-            k_sweep_batch<T, false><<<blocks, kSweepThreads, SweepShape<T, false>::smem, st>>>(dj, n);
+        launch_batch<T>(s[0], dj, n, blocks, st);
         ++s[0]->launches;
         e = cudaGetLastError();
     }
@@ -2339,10 +2442,7 @@ static void batch_si_step(int n, tr_sweep *const *s, cudaStream_t st, const Swee
             if (S->nB) k_to_f32<<<grid_for(S, S->nB), 256, 0, st>>>(S->nB, S->kx + S->nJ, S->Bi32);
         }
     }
-    if (sizeof(T) == 4 && blocks > static_cast<uint32_t>(s[0]->num_sms))
-        k_sweep_batch<T, sizeof(T) == 4><<<blocks, kSweepThreads, SweepShape<T, sizeof(T) == 4>::smem, st>>>(dj, n);
-    else
-        k_sweep_batch<T, false><<<blocks, kSweepThreads, SweepShape<T, false>::smem, st>>>(dj, n);
+    launch_batch<T>(s[0], dj, n, blocks, st);
     for (int i = 0; i < n; ++i) {
         tr_sweep *S = s[i];
         const uint64_t nx = S->nJ + S->nB;
@@ -2525,6 +2625,8 @@ tr_status tr_sweep_create(int device, const tr_mesh_view *mesh, const tr_physics
 }
 
 tr_status tr_sweep_destroy(tr_sweep *s) {
+    if (s && s->groups > 0)
+        return sw_err(s, TR_ERR_INVALID_ARG, "tr_sweep_destroy: the sweep still has live frequency groups");
     sw_free(s);
     return TR_OK;
 }
@@ -2626,6 +2728,7 @@ tr_status tr_sweep_solve_batch(int n, tr_sweep *const *s, int precision, double 
         if (e == cudaSuccess) e = ensure_psi(s[i], precision);
         if (e == cudaSuccess) e = krylov_alloc(s[i], 1);
     }
+    if (e == cudaSuccess && !s[0]->qticket) e = sw_alloc(s[0], &s[0]->qticket, 1);  // before any capture
     cudaStream_t st = s[0]->stream;
     if (e == cudaSuccess)
         e = precision == 64 ? batch_si<double>(n, s, st, tol, max_iter, iterations, residual)
@@ -2639,6 +2742,60 @@ tr_status tr_sweep_solve_batch(int n, tr_sweep *const *s, int precision, double 
     if (e != cudaSuccess) return sw_cuda(s[0], e, "tr_sweep_solve_batch");
     for (int i = 0; i < n; ++i)
         if (!iterations[i]) return sw_err(s[0], TR_ERR_NOT_CONVERGED, "tr_sweep_solve_batch: not converged");
+    return TR_OK;
+}
+
+tr_status tr_sweep_autotune_batch(int n, tr_sweep *const *s, int precision, int *form, double *ms) {
+    if (n < 1 || !s) return transfer::set_global_error(TR_ERR_INVALID_ARG, "tr_sweep_autotune_batch: null argument");
+    for (int i = 0; i < n; ++i) {
+        SW_CHECK(s[i]);
+        if (s[i]->device != s[0]->device)
+            return sw_err(s[0], TR_ERR_INVALID_ARG, "tr_sweep_autotune_batch: sweeps on different devices");
+    }
+    if (precision != 32 && precision != 64) return sw_err(s[0], TR_ERR_INVALID_ARG, "precision must be 32 or 64");
+    cudaSetDevice(s[0]->device);
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < n && e == cudaSuccess; ++i) {
+        e = cudaStreamSynchronize(s[i]->stream);
+        if (e == cudaSuccess) e = ensure_psi(s[i], precision);
+    }
+    cudaStream_t st = s[0]->stream;
+    double t[kBatchForms];
+    for (int f = 0; f < kBatchForms; ++f) t[f] = -1.0;
+    int best = -1;
+    for (int f = 0; f < kBatchForms && e == cudaSuccess; ++f) {
+        if (precision == 64 && (f == kBatchStaticSmall || f == kBatchQueueSmall)) continue;  // FP32 only
+        for (int i = 0; i < n; ++i) s[i]->batch_cfg = f;
+        e = precision == 64 ? batch_sweep<double>(n, s, st, nullptr, nullptr, 1, nullptr, nullptr)
+                            : batch_sweep<float>(n, s, st, nullptr, nullptr, 1, nullptr, nullptr);  // warm-up
+        double tot = 0.0;
+        for (int r = 0; r < 3 && e == cudaSuccess; ++r) {
+            e = cudaEventRecord(s[0]->ev[0], st);
+            if (e == cudaSuccess)
+                e = precision == 64 ? batch_sweep<double>(n, s, st, nullptr, nullptr, 1, nullptr, nullptr)
+                                    : batch_sweep<float>(n, s, st, nullptr, nullptr, 1, nullptr, nullptr);
+            if (e == cudaSuccess) e = cudaEventRecord(s[0]->ev[1], st);
+            if (e == cudaSuccess) e = cudaEventSynchronize(s[0]->ev[1]);
+            float ms1 = 0.0f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms1, s[0]->ev[0], s[0]->ev[1]);
+            tot += ms1;
+        }
+        t[f] = tot / 3.0;
+        if (e == cudaSuccess && (best < 0 || t[f] < t[best])) best = f;
+    }
+    for (int i = 0; i < n; ++i) s[i]->batch_cfg = e == cudaSuccess ? best : -1;
+    if (e != cudaSuccess) return sw_cuda(s[0], e, "tr_sweep_autotune_batch");
+    if (form) *form = best;
+    if (ms)
+        for (int f = 0; f < kBatchForms; ++f) ms[f] = t[f];
+    return TR_OK;
+}
+
+tr_status tr_sweep_set_batch_form(tr_sweep *s, int form) {
+    SW_CHECK(s);
+    if (form < -1 || form >= kBatchForms)
+        return sw_err(s, TR_ERR_INVALID_ARG, "tr_sweep_set_batch_form: form must be -1 .. 3");
+    s->batch_cfg = form;
     return TR_OK;
 }
 
@@ -3237,6 +3394,81 @@ tr_status tr_sweep_set_coefficients(tr_sweep *s, const double *kappa_volume, con
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
     s->last_prec = 0;  // psi of the last sweep belongs to the old coefficients
     return sw_cuda(s, e, "tr_sweep_set_coefficients");
+}
+
+tr_status tr_sweep_create_group(tr_sweep *parent, const double *kappa_volume, const double *kappa_abs_volume,
+                                const double *I_p, tr_sweep **out) {
+    SW_CHECK(parent);
+    if (!out || !kappa_volume) return sw_err(parent, TR_ERR_INVALID_ARG, "tr_sweep_create_group: null argument");
+    *out = nullptr;
+    if (parent->parent)
+        return sw_err(parent, TR_ERR_INVALID_ARG, "tr_sweep_create_group: the parent is itself a group");
+    cudaSetDevice(parent->device);
+    tr_sweep *G = new (std::nothrow) tr_sweep();
+    if (!G) return sw_err(parent, TR_ERR_OUT_OF_MEMORY, "tr_sweep_create_group: host allocation");
+    const tr_sweep &P = *parent;
+    // shared: sizes, geometry, boundary tables, ordinates, schedule, records
+    G->device = P.device;
+    G->num_sms = P.num_sms;
+    G->nT = P.nT; G->nF = P.nF; G->nq = P.nq; G->nrefl = P.nrefl; G->nlag = P.nlag; G->maxlev = P.maxlev;
+    G->forced = P.forced; G->lstride = P.lstride; G->nbf = P.nbf; G->nB = P.nB; G->nJ = P.nJ;
+    G->s64 = P.s64; G->s32 = P.s32; G->finc64 = P.finc64; G->finc32 = P.finc32;
+    G->nbr = P.nbr; G->fbc = P.fbc; G->rslot = P.rslot; G->map = P.map; G->bcell = P.bcell; G->bface = P.bface;
+    G->rent = P.rent; G->ent_cell = P.ent_cell; G->ent_qout = P.ent_qout; G->nent = P.nent;
+    for (int i = 0; i < 4; ++i) G->o64[i] = P.o64[i];
+    for (int i = 0; i < 3; ++i) G->o32[i] = P.o32[i];
+    G->Wm = P.Wm; G->vol64 = P.vol64; G->ord_host = P.ord_host;
+    G->task = P.task; G->lvl = P.lvl; G->nlev = P.nlev; G->lag_keys = P.lag_keys; G->f4_keys = P.f4_keys;
+    G->f4_codes = P.f4_codes; G->n_f4 = P.n_f4;
+    G->mom_kernel = P.mom_kernel; G->shape32 = P.shape32;
+    // owned: coefficients (the fourth value of each packed record carries the
+    // shared vertex map, copied from the parent), reductions, events, stream
+    const size_t nT = P.nT;
+    cudaError_t e = cudaStreamCreateWithFlags(&G->stream, cudaStreamNonBlocking);
+    for (double **p : {&G->stv64, &G->ssv64, &G->ext64, &G->B64})
+        if (e == cudaSuccess) e = sw_alloc(G, p, nT);
+    for (float **p : {&G->stv32, &G->ssv32, &G->ext32})
+        if (e == cudaSuccess) e = sw_alloc(G, p, nT);
+    if (e == cudaSuccess) e = sw_alloc(G, &G->coef64, 4 * nT);
+    if (e == cudaSuccess) e = sw_alloc(G, &G->coef32, 4 * nT);
+    if (e == cudaSuccess) e = cudaMemcpy(G->coef64, P.coef64, 32 * nT, cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(G->coef32, P.coef32, 16 * nT, cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(G->B64, P.B64, 8 * nT, cudaMemcpyDeviceToDevice);
+    if (e == cudaSuccess) e = sw_alloc(G, &G->partials, (kMaxRestart + 2ull) * kDotGrid);
+    if (e == cudaSuccess) e = sw_alloc(G, &G->red, 256);
+    if (e == cudaSuccess) e = sw_alloc(G, &G->counter, 4);
+    if (e == cudaSuccess) e = cudaMemset(G->counter, 0, 16);
+    if (e == cudaSuccess) e = cudaEventCreate(&G->ev[0]);
+    if (e == cudaSuccess) e = cudaEventCreate(&G->ev[1]);
+    if (e != cudaSuccess) {
+        sw_free(G);
+        return sw_cuda(parent, e, "tr_sweep_create_group");
+    }
+    G->parent = parent;
+    ++parent->groups;
+    const tr_status st = tr_sweep_set_coefficients(G, kappa_volume, kappa_abs_volume, I_p);
+    if (st != TR_OK) {
+        const std::string msg = G->last_error;
+        sw_free(G);
+        return sw_err(parent, st, msg);
+    }
+    *out = G;
+    return TR_OK;
+}
+
+tr_status tr_sweep_release_work(tr_sweep *s) {
+    SW_CHECK(s);
+    cudaSetDevice(s->device);
+    cudaStreamSynchronize(s->stream);
+    for (void **p : {(void **)&s->psi64, (void **)&s->psi32, (void **)&s->J32, (void **)&s->Bi32, (void **)&s->Bo32,
+                     (void **)&s->kv, (void **)&s->kb, (void **)&s->kx, (void **)&s->kt, (void **)&s->kh,
+                     (void **)&s->kz}) {
+        sw_release(s, *p);
+        *p = nullptr;
+    }
+    s->kv_m = s->kz_m = 0;
+    s->last_prec = 0;
+    return TR_OK;
 }
 
 tr_status tr_sweep_outflow(tr_sweep *s, const int32_t *face_mask, double *F) {

@@ -4,14 +4,15 @@ contraction and the accelerated solve)."""
 def _main():
     """python -m transfer_b200.run_sweep [--workload milne|stellar[:n]]
     [--precision 32|64] [--sweeps N] [--moments K] [--solve none|gmres|dsa]
-    [--tol T] [--autotune]: N sweeps of the workload (workloads.milne_sweep, or
+    [--tol T] [--autotune] [--moments-kernel tcgen05|mma_sync]: N sweeps of the workload (workloads.milne_sweep, or
     workloads.stellar_sphere with n^3 grid cells, default 96) with a
     scattering source and the mean device time of one sweep; --moments: K
     launches of the l <= 3 moment contraction of the last sweep's psi, timed
     with CUDA events; with --solve, one GMRES solve to FP64 relative residual
     T in the given precision (64: FP64, 32: mixed), plain or with the
     diffusion synthetic acceleration; --autotune times both FP32 sweep shapes
-    first and keeps the faster."""
+    first and keeps the faster; --moments-kernel picks the tensor-core
+    kernel family of the FP32 moments (tr_sweep_set_moments_kernel)."""
     import argparse
 
     import torch
@@ -27,6 +28,7 @@ def _main():
     ap.add_argument("--workload", default="milne")
     ap.add_argument("--moments", type=int, default=0)
     ap.add_argument("--autotune", action="store_true")
+    ap.add_argument("--moments-kernel", default="tcgen05", choices=("tcgen05", "mma_sync"))
     args = ap.parse_args()
     if args.workload.startswith("stellar"):
         n = int(args.workload.split(":")[1]) if ":" in args.workload else 96
@@ -34,6 +36,7 @@ def _main():
     else:
         md, ph, ords, desc = W.milne_sweep()
     S = Sweep(0, md, ords, ph, dsa=args.solve == "dsa")
+    S.set_moments_kernel(L.TR_MOMENTS_TCGEN05 if args.moments_kernel == "tcgen05" else L.TR_MOMENTS_MMA_SYNC)
     if args.autotune:
         shape, t_full, t_small = S.autotune()
         print(f"autotune: FP32 sweep {t_full:.3f} ms full shape, {t_small:.3f} ms small; keeps "
@@ -60,7 +63,8 @@ def _main():
         ms = e0.elapsed_time(e1) / args.moments
         rb = 4 if args.precision == 32 else 8
         byt = S.nq * S.nT * 4 * rb + 16 * S.nT * 4 * 8
-        print(f"moments l<=3 of FP{args.precision} psi: {ms:.3f} ms per launch (API call included), "
+        print(f"moments l<=3 of FP{args.precision} psi ({args.moments_kernel if args.precision == 32 else 'fp64'}): "
+              f"{ms:.3f} ms per launch (API call included), "
               f"{byt / (ms * 1e-3) / 1e9:.0f} GB/s algorithmic (psi read once, 16 FP64 moments written)")
     if args.solve != "none":
         mode = L.TR_MODE_FP64 if args.precision == 64 else L.TR_MODE_MIXED

@@ -147,6 +147,31 @@ class Sweep:
                 for a in (kappa_volume, kappa_abs_volume, I_p)]
         self._c(lib.tr_sweep_set_coefficients(self._h, *(_ptr(a) for a in arrs)))
 
+    def create_group(self, kappa_volume, kappa_abs_volume=None, I_p=None):
+        """tr_sweep_create_group: a frequency group with its own per-cell
+        sigma_t V, sigma_a V and Planck intensity, sharing this sweep's mesh,
+        ordinates and schedule.  The group keeps this sweep alive."""
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float64)
+                for a in (kappa_volume, kappa_abs_volume, I_p)]
+        h = C.c_void_p()
+        self._c(lib.tr_sweep_create_group(self._h, *(_ptr(a) for a in arrs), C.byref(h)))
+        g = Sweep.__new__(Sweep)
+        g._torch, g.ordinates, g._keep, g._h, g.device = self._torch, self.ordinates, (self,), h, self.device
+        for k in ("nT", "nF", "nq", "n_extra", "n_reflective", "n_lag", "max_levels", "forced_levels"):
+            setattr(g, k, getattr(self, k))
+        info = L.tr_sweep_info()
+        check(lib.tr_sweep_info_get(h, C.byref(info)))
+        g.device_bytes = info.device_bytes
+        return g
+
+    def release_work(self):
+        """tr_sweep_release_work: frees the angular flux and Krylov work space."""
+        self._c(lib.tr_sweep_release_work(self._h))
+
+    def set_batch_form(self, form):
+        """tr_sweep_set_batch_form (TR_BATCH_*)."""
+        self._c(lib.tr_sweep_set_batch_form(self._h, int(form)))
+
     def outflow(self, face_mask):
         """Outflow of the last sweep through the faces with face_mask != 0."""
         m = np.ascontiguousarray(face_mask, dtype=np.int32)
@@ -181,6 +206,18 @@ def sweep_apply_batch(sweeps, precision=64, J=None, B=None, with_ext=True):
     if st != L.TR_OK:
         sweeps[0]._c(st)
     return [(Jo.view(S.nT, 4), Bo[:S.n_extra]) for S, (Jo, Bo) in zip(sweeps, outs)]
+
+
+def sweep_autotune_batch(sweeps, precision=32):
+    """tr_sweep_autotune_batch: times one batched sweep in each launch form,
+    keeps the fastest on all the sweeps; returns (form, {form: ms})."""
+    arr = (C.c_void_p * len(sweeps))(*[s._h for s in sweeps])
+    form = C.c_int()
+    ms = (C.c_double * 4)()
+    st = lib.tr_sweep_autotune_batch(len(sweeps), arr, int(precision), C.byref(form), ms)
+    if st != L.TR_OK:
+        sweeps[0]._c(st)
+    return form.value, {f: ms[f] for f in range(4) if ms[f] >= 0}
 
 
 def sweep_solve_batch(sweeps, precision=64, tol=1e-10, max_iter=1000, raise_on_error=True):

@@ -101,16 +101,27 @@ def cube64(maxk=5, n=64):
 WORKLOADS = {"config1": config1, "milne_slab": milne_slab, "milne_slab_ref": milne_slab_ref, "cube64": cube64}
 
 
-def milne_sweep(n=(8, 8, 160), depth=20.0, albedo=0.999, incident=1.0, n_polar=8, n_azim=14):
+def _ordinates(lebedev_degree, n_polar, n_azim):
+    """The named Lebedev set, or a Gauss-Legendre x azimuth product set when
+    n_polar and n_azim are given; returns (ordinates, description)."""
+    from .sweep import lebedev, ordinates_product
+    if n_polar is not None and n_azim is not None:
+        return (ordinates_product(n_polar, n_azim),
+                f"{n_polar}x{n_azim} Gauss-Legendre x azimuth product set ({n_polar * n_azim})")
+    ords = lebedev(lebedev_degree)
+    return ords, f"Lebedev degree {lebedev_degree} ({len(ords[3])} points)"
+
+
+def milne_sweep(n=(8, 8, 160), depth=20.0, albedo=0.999, incident=1.0, lebedev_degree=17, n_polar=None,
+                n_azim=None):
     """The Milne-type slab for the discrete-ordinates sweep: 8 x 8 x 160 Kuhn
     hexahedra on [0,1]^2 x [0,20] (61,440 tets, jitter +-0.15h), sigma_t = 1
     with isotropic scattering of albedo 0.999, reflective x / y faces (an
     infinite slab), vacuum at z = 0, isotropic inflow I = 1 at z = 20.
-    Ordinates: 8 Gauss-Legendre cosines x 14 azimuths = 112 directions, the
-    mirror-symmetric product set nearest the 110-point Lebedev set.
+    Ordinates: the 110-point Lebedev set (degree 17; mirror-symmetric, as the
+    reflective walls need), or a product set when n_polar / n_azim are given.
     Returns (MeshData, Physics, ordinates, description)."""
     from ._lib import TR_BC_REFLECTIVE
-    from .sweep import ordinates_product
     md = MeshData.kuhn(n, box=(0.0, 1.0, 0.0, 1.0, 0.0, depth), jitter=0.15, seed=SEED, kappa=[0.0, 1.0],
                        Ip=[0.0, 0.0], albedo=[0.0, albedo])
     side = md.face_side
@@ -118,25 +129,23 @@ def milne_sweep(n=(8, 8, 160), depth=20.0, albedo=0.999, incident=1.0, n_polar=8
     bc[side <= 3] = TR_BC_REFLECTIVE
     bc[side == 5] = TR_BC_INCIDENT
     phys = Physics(kappa_abs_volume=md.kappa_abs_volume, face_bc=bc, face_incident=np.where(side == 5, incident, 0.0))
-    ords = ordinates_product(n_polar, n_azim)
+    ords, odesc = _ordinates(lebedev_degree, n_polar, n_azim)
     desc = dict(workload="milne_sweep", mesh=f"{n[0]}x{n[1]}x{n[2]} Kuhn slab [0,1]^2x[0,{depth:g}], jitter 0.15h",
-                ordinates=f"{n_polar}x{n_azim} Gauss-Legendre x azimuth product set ({n_polar * n_azim})",
+                ordinates=odesc,
                 physics=f"sigma_t=1, isotropic scattering albedo {albedo:g}, reflective x/y, vacuum z=0, "
                         f"isotropic inflow I={incident:g} at z={depth:g}")
     return md, phys, ords, desc
 
 
-def stellar_sphere(n=96, n_polar=14, n_azim=22):
+def stellar_sphere(n=96, lebedev_degree=29, n_polar=None, n_azim=None):
     """The stellar sphere for the discrete-ordinates sweep: a Kuhn grid of
     n^3 hexahedra on [-1,1]^3 (jitter +-0.2h) clipped to the tets whose
     centroid lies in r <= 1 (2,779,622 tets for n = 96), absorption
     kappa(r) = 10 (1 - r^2) + 0.1 and isotropic scattering sigma_s = 0.5 kappa
     per tet (sigma_t = 1.5 kappa, albedo 1/3), source B(r) = (1 - r^2)^4,
-    vacuum surface.  Ordinates: 14 Gauss-Legendre cosines x 22 azimuths =
-    308 directions, the mirror-symmetric product set nearest the 302-point
-    Lebedev set (Lebedev rules are generated up to 194 points here).
+    vacuum surface.  Ordinates: the 302-point Lebedev set (degree 29), or a
+    product set when n_polar / n_azim are given.
     Returns (MeshData, Physics, ordinates, description)."""
-    from .sweep import ordinates_product
     base = MeshData.kuhn((n, n, n), box=(-1.0, 1.0, -1.0, 1.0, -1.0, 1.0), jitter=0.2, seed=SEED,
                          kappa=[0.0, 1.0], Ip=[0.0, 0.0], ball=(0.0, 0.0, 0.0, 1.0))
     tets = base.mesh["p"]
@@ -148,10 +157,10 @@ def stellar_sphere(n=96, n_polar=14, n_azim=22):
                             np.concatenate([[0.0], 1.5 * kappa]), np.concatenate([[0.0], (1.0 - r2) ** 4]),
                             albedo=np.concatenate([[0.0], np.full(nT, 1.0 / 3.0)]))
     phys = Physics(kappa_abs_volume=md.kappa_abs_volume)
-    ords = ordinates_product(n_polar, n_azim)
+    ords, odesc = _ordinates(lebedev_degree, n_polar, n_azim)
     desc = dict(workload="stellar_sphere", mesh=f"{n}^3 Kuhn grid on [-1,1]^3 clipped to r<=1 ({nT} tets), "
                                                 "jitter 0.2h",
-                ordinates=f"{n_polar}x{n_azim} Gauss-Legendre x azimuth product set ({n_polar * n_azim})",
+                ordinates=odesc,
                 physics="kappa=10(1-r^2)+0.1, sigma_s=0.5 kappa, B=(1-r^2)^4, vacuum surface")
     return md, phys, ords, desc
 
@@ -185,13 +194,18 @@ def cube64_sweep(n=64, albedo=0.3, degree=23):
     return md, phys, ords, mask, desc
 
 
-def cube_batch(count=64, lo=2000, hi=400000, seed=SEED):
+def cube_batch(count=64, lo=2000, hi=400000, seed=SEED, groups=8):
     """Configuration 4's independent problems for the sweep: `count` jittered
     Kuhn cubes (+-0.2h) with tet counts drawn log-uniformly in [lo, hi]
-    (rounded to n^3 hexahedra), per-tet sigma_t lognormal(0, 1), albedo
-    uniform in [0, 0.9], B = 1 in a random sub-box of edge 0.3, vacuum; the
-    50- or 194-point Lebedev set, drawn per problem.  One frequency group.
-    Returns [(MeshData, Physics, ordinates)] and a description."""
+    (rounded to n^3 hexahedra), per-tet base sigma_t lognormal(0, 1), albedo
+    uniform in [0, 0.9] per problem, B = 1 in a random sub-box of edge 0.3,
+    vacuum; the 50- or 194-point Lebedev set, drawn per problem.  `groups`
+    frequency groups per problem: group g has sigma_t = base x 10^(g/3 - 1)
+    with the problem's albedo (no coupling between groups).  Returns
+    [(MeshData, Physics, ordinates, group_coefficients)] -- the MeshData and
+    Physics carry group 0, group_coefficients lists (sigma_t V, sigma_a V)
+    per cell for groups 1 .. groups-1 (tr_sweep_create_group) -- and a
+    description."""
     from .sweep import lebedev
     rng = np.random.default_rng(seed)
     sets = {11: lebedev(11), 23: lebedev(23)}
@@ -204,13 +218,18 @@ def cube_batch(count=64, lo=2000, hi=400000, seed=SEED):
         cent = base.coords[tets.astype(np.int64)].mean(axis=1)
         c0 = rng.uniform(0.0, 0.7, 3)
         hot = np.all((cent > c0) & (cent < c0 + 0.3), axis=1)
+        sigma = rng.lognormal(0.0, 1.0, nT)
+        albedo = rng.uniform(0.0, 0.9)
         md = MeshData.from_tets(base.coords, tets, np.arange(1, nT + 1, dtype=np.int32),
-                                np.concatenate([[0.0], rng.lognormal(0.0, 1.0, nT)]),
+                                np.concatenate([[0.0], sigma * 10.0 ** (-1.0)]),
                                 np.concatenate([[0.0], hot.astype(np.float64)]),
-                                albedo=np.concatenate([[0.0], np.full(nT, rng.uniform(0.0, 0.9))]))
-        out.append((md, Physics(kappa_abs_volume=md.kappa_abs_volume), sets[11 if rng.random() < 0.5 else 23]))
-    desc = dict(workload="cube_batch", problems=count, tets=f"{lo}-{hi} log-uniform",
-                physics="sigma_t lognormal(0,1) per tet, albedo U[0,0.9] per problem, B=1 in a random 0.3 box",
+                                albedo=np.concatenate([[0.0], np.full(nT, albedo)]))
+        kv0 = md.mesh["kappa_volume"].copy()
+        gc = [(kv0 * 10.0 ** (g / 3.0), kv0 * 10.0 ** (g / 3.0) * (1.0 - albedo)) for g in range(1, groups)]
+        out.append((md, Physics(kappa_abs_volume=md.kappa_abs_volume), sets[11 if rng.random() < 0.5 else 23], gc))
+    desc = dict(workload="cube_batch", problems=count, groups=groups, tets=f"{lo}-{hi} log-uniform",
+                physics="sigma_t lognormal(0,1) x 10^(g/3-1) per tet and group, albedo U[0,0.9] per problem, "
+                        "B=1 in a random 0.3 box",
                 ordinates="Lebedev 50 or 194 per problem")
     return out, desc
 
