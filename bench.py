@@ -24,6 +24,12 @@ fits in L2 (else HBM), and the L2 bandwidth and the FP32 / FP64 peaks are
 measured in the same run ("peaks").  The "cube64" object (--no-cube64 skips
 it) times the HBM-resident 64^3 cube (274,625 vertices, slm 66) the same way.
 
+The "stellar_sphere" and "cube_batch" objects (--no-configs skips them)
+measure configuration 3 (the 2.78 M-tet ball with the 302-point Lebedev set:
+sweeps, the tensor-core moments, mixed and FP64 GMRES) and configuration 4
+(64 cubes x 8 frequency groups in one autotuned, graph-replayed batched
+source iteration against the plain FP64 solver looped over the pairs).
+
 The line's "sweep" object measures the discrete-ordinates sweep on the
 Milne slab (scattering albedo 0.999, 112 ordinates): one sweep alone (FP32
 and FP64), GMRES solves to the same FP64 residual (FP64 and FP32 sweeps in
@@ -66,6 +72,8 @@ def parse_args():
     p.add_argument("--no-sweep", action="store_true", help="skip the discrete-ordinates sweep section")
     p.add_argument("--no-cube64", action="store_true", help="skip the HBM-resident cube64 section")
     p.add_argument("--no-reference-gpu", action="store_true", help="skip timing the reference's GPU program")
+    p.add_argument("--no-configs", action="store_true",
+                   help="skip the stellar-sphere and batched-cubes sections (configurations 3 and 4)")
     return p.parse_args()
 
 
@@ -237,25 +245,73 @@ def traffic_per_launch(workload):
 
 
 # ----------------------------------------------------------------- CPU arm
-def cpu_sample(workload, iters, steps=1):
-    """FP64 oracle CG iterations on the workload (all host threads);
-    returns (updates/s, threads, seconds, iterations)."""
+# workloads whose meshes the oracle side builds itself (oracle/oracle_mesh.py,
+# equal to the product's, tested): the CPU arms run them without loading the
+# product library
+ORACLE_WORKLOADS = ("config1", "milne_slab_ref")
+
+
+def cpu_problem(workload):
+    """(Oracle, nT, slm, source) for the CPU arms: the oracle's own mesh and
+    angular tables where it builds them, else the product's workload."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import types
     import oracle_py as op
+    if workload in ORACLE_WORKLOADS:
+        import oracle_mesh as om
+        md, maxk = om.workload(workload)
+        ad = types.SimpleNamespace(**op.angular(maxk))
+        return op.Oracle(md, ad), md.nT, ad.slm, "oracle mesh and angular tables (no product library)"
     from transfer_b200 import workloads as W
     md, ad, phys, _ = W.WORKLOADS[workload]()
     kw = {}
     if phys is not None:
         kw = dict(kappa_abs_volume=phys.kappa_abs_volume, face_bc=phys.face_bc, face_incident=phys.face_incident)
-    O = op.Oracle(md, ad, **kw)
+    return op.Oracle(md, ad, **kw), md.nT, ad.slm, "product-built mesh"
+
+
+def cpu_solve_sample(workload, min_seconds=10.0, max_solves=5, O=None):
+    """FP64 CG solves of the oracle (all host threads) to the relative
+    residual TOL from f = 0, repeated until min_seconds have passed (at most
+    max_solves); returns (updates/s, threads, seconds, iterations, solves,
+    source)."""
+    import oracle_py as op
+    O, nT, slm, src = cpu_problem(workload) if O is None else O
     b = O.rhs()
-    total, n = 0.0, 0
-    for _ in range(steps):
+    total, its, solves = 0.0, 0, 0
+    while solves < max_solves and (solves == 0 or total < min_seconds):
         t0 = time.perf_counter()
-        O.cg(b, max_iter=iters, tol=0.0)
+        _, res = O.cg(b, max_iter=200000, tol=TOL, relative=1)
         total += time.perf_counter() - t0
-        n += iters
-    return n * md.nT * ad.slm / total, op.lib.oracle_num_threads(), total, n
+        its += res["iterations"]
+        solves += 1
+    return its * nT * slm / total, op.lib.oracle_num_threads(), total, its, solves, src
+
+
+def cpu_iter_sample(workload, iters):
+    """FP64 oracle CG iterations (a bounded sample, for workloads whose full
+    solve takes the CPU minutes); returns (updates/s, threads, seconds, iterations, source)."""
+    import oracle_py as op
+    O, nT, slm, src = cpu_problem(workload)
+    b = O.rhs()
+    t0 = time.perf_counter()
+    O.cg(b, max_iter=iters, tol=0.0)
+    secs = time.perf_counter() - t0
+    return iters * nT * slm / secs, op.lib.oracle_num_threads(), secs, iters, src
+
+
+def cpu_baseline_of(workload, iters_override=0):
+    """The cpu_baseline object: full solves where they take seconds, else a
+    bounded iteration sample."""
+    if workload in ORACLE_WORKLOADS and not iters_override:
+        v, threads, secs, its, solves, src = cpu_solve_sample(workload)
+        sample = (f"{solves} FP64 CG solve(s) of the CPU restatement to relative residual {TOL:g} on {workload}, "
+                  f"{its} iterations, {secs:.1f} s; {src}")
+    else:
+        iters = iters_override or auto_cpu_iters(workload)
+        v, threads, secs, its, src = cpu_iter_sample(workload, iters)
+        sample = f"{its} FP64 CG iterations of the CPU restatement on {workload} ({secs:.1f} s); {src}"
+    return {"value": v, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample}
 
 
 def auto_cpu_iters(workload):
@@ -263,13 +319,30 @@ def auto_cpu_iters(workload):
 
 
 def run_reference(args, rank):
+    """The reference's CPU path (the oracle restatement, all host threads):
+    each step one FP64 CG solve to the relative residual TOL from f = 0 on
+    the workload (a bounded iteration sample per step for workloads outside
+    ORACLE_WORKLOADS)."""
     if rank != 0:
         return
-    iters = args.cpu_iters or auto_cpu_iters(args.workload)
-    for _ in range(max(0, min(args.warmup, 1))):
-        cpu_sample(args.workload, max(1, iters // 4))
-    v, threads, secs, n = cpu_sample(args.workload, iters, steps=args.steps)
-    sample = f"{n} FP64 CG iterations ({iters} per step) of the CPU restatement on {args.workload}"
+    if args.workload in ORACLE_WORKLOADS and not args.cpu_iters:
+        prob = cpu_problem(args.workload)
+        for _ in range(max(0, min(args.warmup, 1))):
+            cpu_solve_sample(args.workload, min_seconds=0.0, max_solves=1, O=prob)
+        v, threads, secs, its, solves, src = cpu_solve_sample(args.workload, min_seconds=float("inf"),
+                                                              max_solves=args.steps, O=prob)
+        sample = (f"{solves} FP64 CG solves (one per step) of the CPU restatement to relative residual {TOL:g} "
+                  f"on {args.workload}, {its} iterations; {src}")
+    else:
+        iters = args.cpu_iters or auto_cpu_iters(args.workload)
+        secs, its, v = 0.0, 0, 0.0
+        for _ in range(args.steps):
+            v1, threads, s1, i1, src = cpu_iter_sample(args.workload, iters)
+            secs += s1
+            its += i1
+        O, nT, slm, src = cpu_problem(args.workload)
+        v = its * nT * slm / secs
+        sample = f"{its} FP64 CG iterations ({iters} per step) of the CPU restatement on {args.workload}; {src}"
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * secs / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -367,6 +440,134 @@ def sweep_section(local, flush, peak, want_cpu):
         secs = time.perf_counter() - t0
         out["cpu_baseline"] = {"value": n * nT * nq / secs, "unit": out["unit"], "cores": op.lib.oracle_num_threads(),
                                "kind": "port", "sample": f"{n} FP64 sweeps of the CPU restatement ({secs:.1f} s)"}
+    return out
+
+
+# ----------------------------------------------------------------- configurations 3 and 4
+def stellar_section(local, peak):
+    """Configuration 3 (workloads.stellar_sphere: 2.78 M tets of the ball, the
+    302-point Lebedev set): one FP32 and one FP64 sweep alone, the l <= 3
+    moments of the FP32 psi on the tensor cores (tcgen05 and mma.sync
+    kernels), and GMRES to the FP64 residual SWEEP_TOL with FP64 sweeps and
+    with FP32 sweeps in FP64 defect correction, the latter's FP64 energy
+    balance and its difference from the FP64 solution."""
+    import torch
+    import transfer_b200 as tr
+    from transfer_b200 import workloads as W
+    md, ph, ords, desc = W.stellar_sphere()
+    S = tr.Sweep(local, md, ords, ph)
+    nT, nq = S.nT, S.nq
+    out = {"config": {**desc, "nT": nT, "nq": nq, "max_levels": S.max_levels, "tol": SWEEP_TOL},
+           "unit": "cell-ordinate updates/s (nT * nq per sweep)"}
+    for p in (32, 64):
+        ms = S.bench(p, 3)
+        out[f"sweep_fp{p}"] = {"ms": ms, "value": nT * nq / (ms * 1e-3)}
+    S.apply(precision=32)
+    mom_bytes = 4 * nq * nT * 4 + 16 * nT * 4 * 8          # psi read once, 16 FP64 moments written
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for kind, name in ((tr._lib.TR_MOMENTS_TCGEN05, "tcgen05"), (tr._lib.TR_MOMENTS_MMA_SYNC, "mma_sync")):
+        S.set_moments_kernel(kind)
+        S.moments(16)
+        torch.cuda.synchronize()
+        e0.record()
+        for _ in range(10):
+            S.moments(16)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / 10
+        out[f"moments_{name}"] = {"ms": ms, "achieved_gbs": mom_bytes / (ms * 1e-3) / 1e9,
+                                  "frac_of_hbm": mom_bytes / (ms * 1e-3) / 1e9 / peak,
+                                  "algorithmic_bytes": mom_bytes}
+    S.set_moments_kernel(tr._lib.TR_MOMENTS_TCGEN05)
+    sols = {}
+    for name, mode in (("fp64", tr.TR_MODE_FP64), ("mixed", tr.TR_MODE_MIXED)):
+        torch.cuda.synchronize()
+        e0.record()
+        J, B, rep = S.solve(mode=mode, tol=SWEEP_TOL, restart=40, max_iter=500)
+        e1.record()
+        torch.cuda.synchronize()
+        sols[name] = J
+        out[f"solve_{name}"] = {"ms": e0.elapsed_time(e1), "converged": bool(rep.converged),
+                                "iterations": rep.iterations, "sweeps_f32": rep.sweeps_f32,
+                                "sweeps_f64": rep.sweeps_f64, "residual": rep.residual}
+    out["speedup_mixed_vs_fp64"] = out["solve_fp64"]["ms"] / out["solve_mixed"]["ms"]
+    J = sols["mixed"]
+    Jo, _ = S.apply(J, None, precision=64)
+    b = S.balance(J, None, Jo)
+    out["balance_mixed"] = {**b, "relative_imbalance": (b["emitted"] + b["incoming"] - b["absorbed"] - b["escaped"]
+                                                        - b["reflective_net"]) / b["emitted"]}
+    out["mixed_vs_fp64_J"] = float(((J - sols["fp64"]).abs().max() / sols["fp64"].abs().max()).item())
+    del S
+    torch.cuda.empty_cache()
+    return out
+
+
+def batch_section(local):
+    """Configuration 4 (workloads.cube_batch: 64 jittered cubes of 2k-400k
+    tets, 8 frequency groups each, the 50- or 194-point Lebedev set): the
+    batch-launch autotuner over the 512 (problem, group) sweeps, one batched
+    FP32 sweep of all against one call per pair, and source iteration of all
+    pairs to a relative change of 1e-6 -- FP32 sweeps with FP64 iterates in
+    one graph-replayed launch per iteration -- against the plain FP64 solver
+    looped over the pairs."""
+    import gc
+    import torch
+    import transfer_b200 as tr
+    from transfer_b200.run_batch import build
+    tol = 1e-6
+    sweeps, desc = build(64, 2000, 400000, 8)
+    upd = sum(S.nT * S.nq for S in sweeps)
+    out = {"config": {**desc, "sweeps": len(sweeps), "tasks": sum(S.nq for S in sweeps),
+                      "cell_ordinate_updates_per_sweep": upd, "tol": tol},
+           "unit": "cell-ordinate updates/s"}
+    form, ms = tr.sweep_autotune_batch(sweeps, 32)
+    names = {0: "static_full", 1: "static_small", 2: "queue_full", 3: "queue_small"}
+    out["autotune_ms"] = {names[f]: v for f, v in ms.items()}
+    out["autotune_choice"] = names[form]
+    Js = [torch.rand(4 * S.nT, dtype=torch.float64, device=f"cuda:{local}") for S in sweeps]
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    tr.sweep_apply_batch(sweeps, 32, Js, None)
+    torch.cuda.synchronize()
+    e0.record()
+    tr.sweep_apply_batch(sweeps, 32, Js, None)
+    e1.record()
+    torch.cuda.synchronize()
+    tb = e0.elapsed_time(e1)
+    e0.record()
+    for S, J in zip(sweeps, Js):
+        S.apply(J, None, precision=32)
+    e1.record()
+    torch.cuda.synchronize()
+    tl = e0.elapsed_time(e1)
+    out["sweep_batched_fp32"] = {"ms": tb, "value": upd / (tb * 1e-3)}
+    out["sweep_looped_fp32"] = {"ms": tl, "value": upd / (tl * 1e-3)}
+    tr.sweep_solve_batch(sweeps, 32, tol=tol, max_iter=2000)   # warm-up
+    torch.cuda.synchronize()
+    e0.record()
+    res, its, rr = tr.sweep_solve_batch(sweeps, 32, tol=tol, max_iter=2000)
+    e1.record()
+    torch.cuda.synchronize()
+    t_batch = e0.elapsed_time(e1)
+    t_loop, it_loop, dev = 0.0, 0, 0.0
+    SI = tr._lib.TR_SWEEP_SOURCE_ITERATION
+    for S, (J, _) in zip(sweeps, res):
+        S.release_work()
+        e0.record()
+        Jr, _, rep = S.solve(method=SI, mode=tr.TR_MODE_FP64, tol=tol, max_iter=2000)
+        e1.record()
+        torch.cuda.synchronize()
+        t_loop += e0.elapsed_time(e1)
+        it_loop += rep.iterations
+        dev = max(dev, float(((J - Jr).abs().max() / Jr.abs().max()).item()))
+        S.release_work()
+    out["solve_batched_fp32_sweeps"] = {"ms": t_batch, "iterations_max": int(its.max()),
+                                        "form": "one CUDA graph replay per source iteration"}
+    out["solve_looped_fp64"] = {"ms": t_loop, "iterations_total": it_loop}
+    out["speedup_batched_vs_looped_fp64"] = t_loop / t_batch
+    out["max_relative_difference_J"] = dev
+    del sweeps, Js, res
+    gc.collect()
+    torch.cuda.empty_cache()
     return out
 
 
@@ -653,12 +854,11 @@ def run_ours(args, rank, world, local):
             line["sweep"] = sweep_section(local, flush, peak, world == 1 and not args.no_cpu_baseline)
         if not args.no_cube64 and args.workload != "cube64":
             line["cube64"] = cube64_section(local, flush, peaks, peak, peak_kind)
+        if world == 1 and not args.no_configs:
+            line["stellar_sphere"] = stellar_section(local, peak)
+            line["cube_batch"] = batch_section(local)
         if world == 1 and not args.no_cpu_baseline:
-            iters = args.cpu_iters or auto_cpu_iters(args.workload)
-            v, threads, secs, n = cpu_sample(args.workload, iters)
-            line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                                    "sample": f"{n} FP64 CG iterations of the CPU restatement on {args.workload}"
-                                              f" ({secs:.1f} s)"}
+            line["cpu_baseline"] = cpu_baseline_of(args.workload, args.cpu_iters)
         print(json.dumps(line), flush=True)
     ctx.close()
     if pg:
