@@ -555,9 +555,10 @@ double tr_spherical_value(int l, int m, double x, double y, double z);
  * (LebedevQuad.cpp:6269-6277): returns the rule's number of points and, if
  * cap >= that number, fills x, y, z, w (weights sum to 1).  Returns -1 for
  * an unsupported degree.  The Lebedev rules are generated from their
- * defining equations instead of stored tables, up to 194 points (precision
- * 23; the first call for a rule solves it, a few seconds for 194 points);
- * the points may come in another order than the reference's tables. */
+ * defining equations instead of stored tables, up to 350 points (precision
+ * 31; the first call for a rule solves it on the host's threads, at most a
+ * few seconds; later calls use the cached rule); the points may come in
+ * another order than the reference's tables. */
 int tr_hemiquad(int mindegree, double *x, double *y, double *z, double *w, int cap);
 int tr_lebedev(int mindegree, double *x, double *y, double *z, double *w, int cap);
 

@@ -46,7 +46,7 @@ struct HemiQuad {
 
 // Lebedev rule of algebraic precision >= mindegree (LebedevQuad.cpp:6269-6277):
 // the smallest of the tabulated octahedral rules whose precision reaches
-// mindegree; weights sum to 1.  The rules (up to 194 points) are generated
+// mindegree; weights sum to 1.  The rules (up to 350 points) are generated
 // from their defining equations (lebedev.cpp); throws for larger ones.
 struct LebedevQuad {
     int order = 0;

@@ -28,7 +28,7 @@ def ordinates_product(n_polar, n_azim):
 
 def lebedev(mindegree):
     """LebedevQuad(mindegree) as an ordinate set (x, y, z, w), weights summing
-    to 1 (rules up to 194 points are generated)."""
+    to 1 (rules up to 350 points are generated)."""
     n = lib.tr_lebedev(int(mindegree), None, None, None, None, 0)
     if n < 0:
         raise ValueError(f"no Lebedev rule of degree {mindegree} is generated")
