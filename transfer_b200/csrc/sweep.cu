@@ -867,7 +867,10 @@ __device__ __forceinline__ void mma_tf32(float (&d)[4], const uint32_t (&a)[4], 
 // distinct banks).  Persistent: the block stages the split weights once and
 // walks row tiles tile = blockIdx.x, + gridDim.x, ...
 constexpr int kMomWarps = 8;
-constexpr int kMomMT = 2;                          // 16-row MMA tiles per warp
+#ifndef TR_MOM_MT
+#define TR_MOM_MT 2  // tuning macro: 16-row MMA tiles per warp of k_moments_tf32x3
+#endif
+constexpr int kMomMT = TR_MOM_MT;                  // 16-row MMA tiles per warp
 constexpr int kMomRows = 16 * kMomMT * kMomWarps;  // 256 rows per tile: 1 KB runs per ordinate
 constexpr int kMomK = 16;                          // ordinates per stage
 constexpr int kMomStride = kMomRows + 8;
