@@ -146,6 +146,26 @@ def test_engines_agree(cuda):
     assert rs2.converged and rel_err(host(fs2), host(fm)) < 1e-8
 
 
+@pytest.mark.parametrize("maxk", [1, 2, 3])
+def test_mixed_engines_continue_the_same_krylov_space(cuda, maxk):
+    """Across defect corrections the mixed solve's FP32 CG continues with its
+    last direction.  The graph and launch engines start each leg in direction
+    buffer 0 (a leg of m iterations ends in buffer m & 1); the persistent
+    kernel picks buffers by the running count.  Legs of odd and even length
+    follow each other here; all three engines converge in about the same
+    number of inner iterations, graph and launch bitwise alike."""
+    ctx = tr.CudaContext(0, c1_mesh(), golden_angular(maxk))
+    got = {}
+    for eng in (tr.TR_ENGINE_GRAPH, tr.TR_ENGINE_LAUNCH, tr.TR_ENGINE_PERSISTENT):
+        f, r = ctx.solve(mode=tr.TR_MODE_MIXED, tol=1e-10, relative=1, engine=eng)
+        assert r.converged and r.final_residual < 1e-10 * r.rhs_norm
+        got[eng] = (host(f), r)
+    (fg, rg), (fl, rl), (fp, rp) = got[tr.TR_ENGINE_GRAPH], got[tr.TR_ENGINE_LAUNCH], got[tr.TR_ENGINE_PERSISTENT]
+    assert np.array_equal(fg, fl) and rg.iterations == rl.iterations
+    assert rg.iterations <= 1.25 * rp.iterations + 8 and rp.iterations <= 1.25 * rg.iterations + 8
+    assert rel_err(fg, fp) < 1e-8
+
+
 def test_host_buffers_and_explicit_rhs(cuda):
     md, ad = small_mesh(), golden_angular(2)
     ctx = tr.CudaContext(0, md, ad)

@@ -98,6 +98,235 @@ std::vector<T> to_type(const std::vector<double> &v) {
     return o;
 }
 
+// The contraction rounds (the Runs layout of internal.h) of the lists
+// lists[lm] = {(q * 256 + lms, weight)} for L lanes, offsets q * sa + lms
+// into a table of `word`-byte elements.  schedule_runs lays out one choice
+// (the harmonics taken in `order`, chunks of R) and prices it in
+// shared-memory wavefronts; make_runs keeps the cheapest over R and a few
+// harmonic orders.  Within a chunk the entries may come in any order; the
+// order is chosen so that the lanes of a step read distinct banks (word 4:
+// bank = offset mod 32 over the warp; word 8: bank pair = offset mod 16
+// within each half-warp, a 64-bit access being served per 16 lanes).
+struct RunsHost {
+    uint32_t rounds = 0, R = 0, L = 0;
+    std::vector<unsigned char> tab;
+    std::vector<uint32_t> span;  // [slm]: first chunk | end chunk << 16
+    uint64_t cost = UINT64_MAX;  // shared-memory wavefronts of one contraction
+};
+typedef std::pair<uint32_t, double> RunEnt;
+RunsHost schedule_runs(const std::vector<std::vector<RunEnt>> &lists, const std::vector<uint32_t> &order, uint32_t L,
+                       uint32_t sa, int word, uint32_t R) {
+    const uint32_t slm = static_cast<uint32_t>(lists.size());
+    RunsHost H;
+    H.L = L;
+    H.R = R;
+    // chunks of consecutive entries, harmonic after harmonic in `order`
+    std::vector<std::vector<RunEnt>> chunk;
+    H.span.assign(slm, 0u);
+    for (uint32_t lm : order) {
+        const uint32_t c0 = static_cast<uint32_t>(chunk.size());
+        for (size_t i = 0; i < lists[lm].size(); i += R)
+            chunk.emplace_back(lists[lm].begin() + static_cast<std::ptrdiff_t>(i),
+                               lists[lm].begin() + static_cast<std::ptrdiff_t>(std::min(lists[lm].size(), i + R)));
+        H.span[lm] = c0 | static_cast<uint32_t>(chunk.size()) << 16;
+    }
+    H.rounds = std::max<uint32_t>(1, static_cast<uint32_t>((chunk.size() + L - 1) / L));
+    const size_t n = static_cast<size_t>(H.rounds) * R * L;
+    std::vector<double> w(n, 0.0);
+    std::vector<uint32_t> o(n, 0u);
+    // Per round and bank group (FP64: each half-warp; FP32: the warp), the
+    // entries are the edges of a bipartite multigraph lanes x banks, and the
+    // steps 0..R-1 its colours: a proper edge colouring is a schedule whose
+    // every step hits distinct banks.  Edges are coloured one by one; when
+    // the lane's first free colour a is taken at the bank, the bank's free
+    // colour b is swapped with a along the a/b alternating path from the
+    // bank (which cannot reach the lane, the graph being bipartite) --
+    // Konig's construction, which succeeds whenever no bank has more than R
+    // entries.  Entries of a bank that has more take any free step of their
+    // lane (a conflict).  Unused steps (weight 0) read a cell on a bank that
+    // step leaves free, among the cells every vertex writes (rows q < 6,
+    // columns lms < slm): a row's pad column is never written, and 0 times
+    // whatever it holds need not be 0.
+    const uint32_t nbank = word == 8 ? 16 : 32, group = std::min<uint32_t>(L, nbank);
+    std::vector<int> readable(nbank, -1);  // per bank, a written cell on it
+    for (uint32_t q = 0; q < static_cast<uint32_t>(kSymRows); ++q)
+        for (uint32_t lms = 0; lms < slm; ++lms)
+            if (readable[(q * sa + lms) % nbank] < 0) readable[(q * sa + lms) % nbank] = static_cast<int>(q * sa + lms);
+    struct BankEdge {
+        uint32_t lane, bank, off;
+        double w;
+        int colour;
+    };
+    for (uint32_t r = 0; r < H.rounds; ++r)
+        for (uint32_t g0 = 0; g0 < L; g0 += group) {
+            std::vector<BankEdge> ed;
+            for (uint32_t l = g0; l < g0 + group; ++l) {
+                const size_t c = static_cast<size_t>(r) * L + l;
+                if (c >= chunk.size()) continue;
+                for (const RunEnt &x : chunk[c]) {
+                    const uint32_t off = (x.first >> 8) * sa + (x.first & 255u);
+                    ed.push_back(BankEdge{l - g0, off % nbank, off, x.second, -1});
+                }
+            }
+            std::vector<int> at_lane(static_cast<size_t>(group) * R, -1), at_bank(static_cast<size_t>(nbank) * R, -1);
+            auto set = [&](int e, int col) {
+                ed[e].colour = col;
+                at_lane[ed[e].lane * R + col] = e;
+                at_bank[ed[e].bank * R + col] = e;
+            };
+            auto unset = [&](int e) {
+                at_lane[ed[e].lane * R + ed[e].colour] = -1;
+                at_bank[ed[e].bank * R + ed[e].colour] = -1;
+            };
+            std::vector<int> leftover;
+            for (int e = 0; e < static_cast<int>(ed.size()); ++e) {
+                const uint32_t l = ed[e].lane, bk = ed[e].bank;
+                int ca = -1, cb = -1;
+                for (uint32_t c = 0; c < R && ca < 0; ++c)
+                    if (at_lane[l * R + c] < 0) ca = static_cast<int>(c);
+                for (uint32_t c = 0; c < R && cb < 0; ++c)
+                    if (at_bank[bk * R + c] < 0) cb = static_cast<int>(c);
+                if (cb < 0) {
+                    leftover.push_back(e);
+                    continue;
+                }
+                if (at_bank[bk * R + ca] >= 0) {
+                    // swap ca and cb along the path bank -ca- lane -cb- bank ...
+                    std::vector<int> path;
+                    uint32_t node = bk;
+                    bool on_bank = true;
+                    int col = ca;
+                    for (;;) {
+                        const int f = on_bank ? at_bank[node * R + col] : at_lane[node * R + col];
+                        if (f < 0) break;
+                        path.push_back(f);
+                        node = on_bank ? ed[f].lane : ed[f].bank;
+                        on_bank = !on_bank;
+                        col = col == ca ? cb : ca;
+                    }
+                    for (int f : path) unset(f);
+                    for (int f : path) set(f, ed[f].colour == ca ? cb : ca);
+                }
+                set(e, ca);
+            }
+            for (int e : leftover)
+                for (uint32_t c = 0; c < R; ++c)
+                    if (at_lane[ed[e].lane * R + c] < 0) {
+                        ed[e].colour = static_cast<int>(c);
+                        at_lane[ed[e].lane * R + c] = e;
+                        break;
+                    }
+            for (const BankEdge &x : ed) {
+                const size_t at = (static_cast<size_t>(r) * R + static_cast<uint32_t>(x.colour)) * L + g0 + x.lane;
+                w[at] = x.w;
+                o[at] = x.off;
+            }
+            for (uint32_t c = 0; c < R; ++c)
+                for (uint32_t l = 0; l < group; ++l) {
+                    if (at_lane[l * R + c] >= 0) continue;
+                    uint32_t off = 0;  // offset 0 (S[0][0]) when no free bank has a readable cell
+                    for (uint32_t bk = 0; bk < nbank; ++bk)
+                        if (at_bank[bk * R + c] < 0 && readable[bk] >= 0) {
+                            off = static_cast<uint32_t>(readable[bk]);
+                            at_bank[bk * R + c] = static_cast<int>(ed.size());  // taken by this unused step
+                            break;
+                        }
+                    o[(static_cast<size_t>(r) * R + c) * L + g0 + l] = off;
+                }
+        }
+    // price: per step the entry loads (FP32 one 8-byte pair: 2 wavefronts;
+    // FP64 weight and offset: 3) and the table reads (the most distinct
+    // addresses on one bank, per bank group); per round the chunk-sum store
+    const uint32_t nbk = word == 8 ? 16 : 32;
+    uint64_t cost = 0;
+    for (size_t k = 0; k < static_cast<size_t>(H.rounds) * R; ++k) {
+        cost += word == 8 ? 3 : 2;
+        for (uint32_t g0 = 0; g0 < L; g0 += nbk) {
+            std::vector<std::vector<uint32_t>> seen(nbk);
+            uint64_t most = 1;
+            for (uint32_t l = g0; l < std::min(L, g0 + nbk); ++l) {
+                const uint32_t off = o[k * L + l];
+                auto &v = seen[off % nbk];
+                if (std::find(v.begin(), v.end(), off) == v.end()) v.push_back(off);
+                most = std::max<uint64_t>(most, v.size());
+            }
+            cost += most;
+        }
+    }
+    H.cost = cost + 2ull * H.rounds;
+    // storage: FP32 (w, o) pairs; FP64 weights then offsets
+    if (word == 4) {
+        H.tab.resize(n * 8);
+        for (size_t i = 0; i < n; ++i) {
+            const float wf = static_cast<float>(w[i]);
+            std::memcpy(&H.tab[8 * i], &wf, 4);
+            std::memcpy(&H.tab[8 * i + 4], &o[i], 4);
+        }
+    } else {
+        H.tab.resize(n * 12);
+        std::memcpy(H.tab.data(), w.data(), n * 8);
+        std::memcpy(H.tab.data() + n * 8, o.data(), n * 4);
+    }
+    return H;
+}
+
+// The cheapest schedule with at most `cap` chunks (the kernel's room for
+// chunk sums): R over the multiples of 4 up to the longest list, harmonic
+// order the natural one or one of 31 fixed shuffles (SplitMix64 from a
+// constant seed, Fisher-Yates), so that the chunks sharing a round come
+// from harmonics whose lists load different banks.  rounds = 0 when no
+// schedule fits.
+RunsHost make_runs(const std::vector<std::vector<RunEnt>> &lists, uint32_t L, uint32_t sa, int word, uint32_t cap) {
+    const uint32_t slm = static_cast<uint32_t>(lists.size());
+    size_t longest = 0;
+    for (const auto &l : lists) longest = std::max(longest, l.size());
+    std::vector<std::vector<uint32_t>> orders(1, std::vector<uint32_t>(slm));
+    for (uint32_t i = 0; i < slm; ++i) orders[0][i] = i;
+    uint64_t state = 0x5DEECE66Dull;
+    auto next = [&]() {
+        uint64_t z = (state += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    };
+    for (int k = 0; k < 31; ++k) {
+        std::vector<uint32_t> p = orders[0];
+        for (uint32_t i = slm; i > 1; --i) std::swap(p[i - 1], p[next() % i]);
+        orders.push_back(p);
+    }
+    RunsHost best;
+    best.L = L;
+    if (L > 32) return best;
+    for (uint32_t R = 4; R < longest + 4; R += 4) {
+        uint64_t chunks = 0;
+        for (const auto &l : lists) chunks += (l.size() + R - 1) / R;
+        if (chunks > cap || chunks >= 0xFFFFu) continue;
+        for (const auto &ord : orders) {
+            RunsHost h = schedule_runs(lists, ord, L, sa, word, R);
+            if (h.cost < best.cost) best = std::move(h);
+        }
+    }
+    if (best.cost == UINT64_MAX) best.rounds = 0;
+    return best;
+}
+
+template <typename T>
+cudaError_t upload_runs(tr_ctx *c, const RunsHost &h, uint32_t slm, Runs<T> &r) {
+    if (h.rounds == 0 || h.tab.size() != static_cast<size_t>(h.rounds) * h.R * h.L * (sizeof(T) + 4))
+        return cudaErrorInvalidValue;
+    unsigned char *tab = nullptr;
+    uint32_t *st = nullptr;
+    cudaError_t e = upload(c, &tab, h.tab.data(), h.tab.size());
+    if (e == cudaSuccess) e = upload(c, &st, h.span.data(), slm * sizeof(uint32_t));
+    if (e != cudaSuccess) return e;
+    r.rounds = h.rounds;
+    r.R = h.R;
+    r.L = h.L;
+    r.tab = tab;
+    r.span = st;
+    return cudaSuccess;
+}
+
 }  // namespace
 
 cudaError_t operator_init_attributes();
@@ -269,7 +498,6 @@ tr_status ctx_create(int device, const tr_mesh_view *m, const tr_angular_view *a
     // omega[i][lms][lm] and omega_pos[i][lms][lm])
     auto sym_row = [](int i, int j) { return i == j ? i : (i + j == 1 ? 3 : (i + j == 2 ? 4 : 5)); };
     std::vector<std::vector<std::pair<uint32_t, double>>> lists(slm);  // (q * 256 + lms, w)
-    uint32_t ckmax = 0;
     for (tr_idx lm = 0; lm < slm; ++lm) {
         std::vector<double> wsum(kSymRows * slm, 0.0);
         std::vector<char> used(kSymRows * slm, 0);
@@ -285,56 +513,19 @@ tr_status ctx_create(int device, const tr_mesh_view *m, const tr_angular_view *a
         for (int r = 0; r < kSymRows; ++r)
             for (tr_idx lms = 0; lms < slm; ++lms)
                 if (used[r * slm + lms]) lists[lm].push_back({static_cast<uint32_t>(r * 256 + lms), wsum[r * slm + lms]});
-        ckmax = std::max<uint32_t>(ckmax, static_cast<uint32_t>(lists[lm].size()));
     }
     const uint32_t aslm_max = std::max((slm + 7) & ~7u, (slm + 15) & ~15u);
     const uint32_t cls = (aslm_max + 31) & ~31u;
-    const uint32_t sa64 = s_row_stride((slm + 7) & ~7u), sa32 = s_row_stride((slm + 15) & ~15u);
-    // Step k of the contraction has every lane lm read one S-table word; the
-    // entries of each harmonic are ordered so that, step by step, the lanes
-    // of a warp hit distinct shared-memory banks (FP32 S table: bank = word
-    // offset mod 32).  Greedy over the lanes of each 32-lane group.
-    {
-        std::vector<std::vector<std::pair<uint32_t, double>>> rem(slm);
-        for (tr_idx lm = 0; lm < slm; ++lm) rem[lm].swap(lists[lm]);
-        for (uint32_t k = 0; k < ckmax; ++k)
-            for (tr_idx g0 = 0; g0 < slm; g0 += 32) {
-                uint32_t used = 0;
-                for (tr_idx lm = g0; lm < std::min<tr_idx>(slm, g0 + 32); ++lm) {
-                    auto &r = rem[lm];
-                    if (r.empty()) continue;
-                    size_t pick = 0;
-                    for (size_t i = 0; i < r.size(); ++i) {
-                        const uint32_t word = (r[i].first >> 8) * sa32 + (r[i].first & 255u);
-                        if (!(used & (1u << (word % 32)))) {
-                            pick = i;
-                            break;
-                        }
-                    }
-                    const uint32_t word = (r[pick].first >> 8) * sa32 + (r[pick].first & 255u);
-                    used |= 1u << (word % 32);
-                    lists[lm].push_back(r[pick]);
-                    r.erase(r.begin() + static_cast<std::ptrdiff_t>(pick));
-                }
-            }
-    }
+    const uint32_t a64 = (slm + 7) & ~7u, a32 = (slm + 15) & ~15u;
     const uint32_t satc = (slm + 7) / 8 * 8 + 1;
-    const size_t ncon = std::max<size_t>(static_cast<size_t>(ckmax) * cls, 1);
-    std::vector<double> cw64(ncon, 0.0);
-    std::vector<float> cw32(ncon, 0.0f);
-    std::vector<CEnt<double>> ce64(ncon, CEnt<double>{0.0, 0});
-    std::vector<CEnt<float>> ce32(ncon, CEnt<float>{0.0f, 0});
-    std::vector<uint16_t> cotc(ncon, 0);
-    for (tr_idx lm = 0; lm < slm; ++lm)
-        for (size_t k = 0; k < lists[lm].size(); ++k) {
-            const uint32_t r = lists[lm][k].first >> 8, lms = lists[lm][k].first & 255u;
-            const size_t o = k * cls + lm;
-            cw64[o] = lists[lm][k].second;
-            cw32[o] = static_cast<float>(lists[lm][k].second);
-            ce64[o] = CEnt<double>{lists[lm][k].second, r * sa64 + lms};
-            ce32[o] = CEnt<float>{static_cast<float>(lists[lm][k].second), r * sa32 + lms};
-            cotc[o] = static_cast<uint16_t>(r * satc + lms);
-        }
+    // chunk-sum room: the SIMT group slab's part table (runs_part_elems),
+    // rows 11-15 of the tensor-core C table
+    const RunsHost rs64 = make_runs(lists, group_width(a64), s_row_stride(a64), 8,
+                                    runs_part_elems(group_width(a64), harm_per_lane(a64)));
+    const RunsHost rs32 = make_runs(lists, group_width(a32), s_row_stride(a32), 4,
+                                    runs_part_elems(group_width(a32), harm_per_lane(a32)));
+    const RunsHost rt64 = make_runs(lists, 32, satc, 8, 5 * satc);
+    const RunsHost rt32 = make_runs(lists, 32, satc, 4, 5 * satc);
     std::vector<double> O(3 * ss), ang_diag(3 * slm), O_diag(3 * slm);
     const double *On[3] = {a->Ox, a->Oy, a->Oz};
     for (int n = 0; n < 3; ++n) {
@@ -404,14 +595,11 @@ tr_status ctx_create(int device, const tr_mesh_view *m, const tr_angular_view *a
     o32.kind = TR_OPERATOR_SIMT;
     ok(upload(c, &o64.row, row.data(), row.size() * 4));
     ok(upload(c, &o64.col, col.data(), col.size() * 4));
-    o64.ckmax = o32.ckmax = ckmax;
     o64.cls = o32.cls = cls;
-    ok(upload(c, &o64.cw, cw64.data(), cw64.size() * 8));
-    ok(upload(c, &o32.cw, cw32.data(), cw32.size() * 4));
-    ok(upload(c, &o64.ce, ce64.data(), ce64.size() * sizeof(CEnt<double>)));
-    ok(upload(c, &o32.ce, ce32.data(), ce32.size() * sizeof(CEnt<float>)));
-    ok(upload(c, &o64.co_tc, cotc.data(), cotc.size() * 2));
-    o32.co_tc = o64.co_tc;
+    ok(upload_runs(c, rs64, slm, o64.rs));
+    ok(upload_runs(c, rt64, slm, o64.rt));
+    ok(upload_runs(c, rs32, slm, o32.rs));
+    ok(upload_runs(c, rt32, slm, o32.rt));
     ok(upload(c, &o64.coef, coef.data(), coef.size() * 8));
     // operator copy of O_n, rows lms padded to the lane stride cls
     std::vector<double> Opad(3 * static_cast<size_t>(slm) * cls, 0.0);
@@ -424,7 +612,6 @@ tr_status ctx_create(int device, const tr_mesh_view *m, const tr_angular_view *a
     ok(upload(c, &o64.O_diag, O_diag.data(), O_diag.size() * 8));
     ok(upload(c, &o64.dinv, dinv.data(), dinv.size() * 8));
     ok(upload(c, &o64.bmask, bmask.data(), bmask.size()));
-    o64.ang_nnz = o32.ang_nnz = static_cast<uint32_t>(ncon);
     o32.row = o64.row;
     o32.col = o64.col;
     o32.bmask = o64.bmask;

@@ -36,19 +36,40 @@ constexpr int kCoefStride = 16;
 constexpr int kSymRows = 6, kRowM = 6, kRowM0 = 7, kRowE = 8;
 constexpr int kBlock = 256;
 
-// The angular coupling out[lm] = sum_k w[k][lm] * S[o[k][lm]] is stored
-// lane-major: entry k of every harmonic lm is contiguous ([k * cls + lm]),
-// lists padded to the longest one (ckmax) with zero weights, so each step
-// of the contraction is one coalesced, conflict-free load.  o is the offset
-// q * SA + lms of S_sym[q][lms] in the kernel's S table.  The SIMT kernels
-// read (w, o) pairs (CEnt, one vector load per step); the tensor-core
-// kernels read the weights cw and their C-table offsets co_tc.
+// The angular coupling out[lm] = sum_k w_k S[o_k], over the entries k of
+// harmonic lm (o = q * SA + lms addresses S_sym[q][lms] in the kernel's S or
+// C table), runs in rounds of R steps (R a multiple of 4).  Each harmonic's
+// list is cut into chunks of at most R entries; chunk s (chunks numbered
+// harmonic after harmonic, in an order of the harmonics the host picks) is
+// done by lane s mod L in round s / L, which stores its sum to part[s];
+// harmonic lm then adds its chunks span[lm] & 0xFFFF .. (span[lm] >> 16) - 1
+// in order.  R and the harmonic order are chosen per table (the fewest
+// shared-memory wavefronts, bank conflicts included), so long and short
+// lists share the lanes evenly where a list per lane would pad every lane
+// to the longest list (about 1.5x the mean).  Table [rounds * R][L], lane-major; unused entries have w = 0,
+// o = 0.  Storage, one block: FP32 (w, o) pairs, 8 bytes per entry (one
+// vector load per step); FP64 the weights [n] then the offsets [n] (n =
+// rounds * R * L), 8 + 4 bytes per entry.  The SIMT kernels use L = G lanes
+// and the S table; the tensor-core kernels L = 32 and the C table.
 template <typename T>
-struct alignas(2 * sizeof(T)) CEnt {
-    T w;
-    uint32_t o;
+struct Runs {
+    uint32_t rounds = 0, R = 0, L = 0;
+    const unsigned char *tab = nullptr;  // the entries
+    const uint32_t *span = nullptr;      // [slm] chunks of each harmonic: first | end << 16
 };
-static_assert(sizeof(CEnt<float>) == 8 && sizeof(CEnt<double>) == 16, "contraction entry layout");
+template <typename T>
+__host__ __device__ inline size_t runs_entry_bytes(const Runs<T> &r) {
+    return static_cast<size_t>(r.rounds) * r.R * r.L * (sizeof(T) + 4);
+}
+// chunk sums a SIMT group of G lanes with H harmonics per lane has room for
+__host__ __device__ inline constexpr uint32_t runs_part_elems(int G, int H) {
+    return static_cast<uint32_t>(2 * G * H + G);
+}
+// shared-memory bytes of one staged Runs table for slm harmonics
+template <typename T>
+__host__ __device__ inline size_t runs_smem_bytes(const Runs<T> &r, uint32_t slm) {
+    return ((runs_entry_bytes(r) + 15) & ~size_t(15)) + ((4 * size_t(slm) + 15) & ~size_t(15));
+}
 // lanes per vertex (G) and harmonics per lane (H) for a vector stride
 inline constexpr int group_width(uint32_t aslm) { return aslm <= 8 ? 8 : aslm <= 16 ? 16 : 32; }
 inline constexpr int harm_per_lane(uint32_t aslm) {
@@ -64,10 +85,8 @@ struct OpData {
     const uint32_t *row;             // [nP+1]
     const uint32_t *col;             // [nnz]
     const T *coef;                   // [nnz][16]
-    uint32_t ckmax, cls;             // contraction: entries per lm, lane stride
-    const CEnt<T> *ce;               // [ckmax][cls] (weight, SIMT S-table offset)
-    const T *cw;                     // [ckmax][cls] weights
-    const uint16_t *co_tc;           // [ckmax][cls] offsets, tensor-core C table
+    uint32_t cls;                    // lane stride of O
+    Runs<T> rs, rt;                  // contraction runs: SIMT S table, tensor-core C table
     const T *O;                      // [3][slm][cls]: O_n[lms][lm], rows padded to cls
     const T *ang_diag;               // [3][slm]: omega_i[lm][lm]
     const T *O_diag;                 // [3][slm]: O_n[lm][lm]
@@ -89,7 +108,6 @@ struct LhsArgs {
     double *fin_out = nullptr;
     struct CgScalars *cgs = nullptr;
     const int32_t *done = nullptr;
-    uint32_t ang_nnz = 0;
 };
 
 // Scalars of a device-resident CG, one per concurrent solve.
@@ -156,16 +174,13 @@ constexpr int kPersistChunk = 64;  // CG iterations per persistent-kernel launch
 template <typename T>
 struct DeviceOp {
     uint32_t *row = nullptr, *col = nullptr;
-    uint32_t ckmax = 0, cls = 0;
-    CEnt<T> *ce = nullptr;
-    T *cw = nullptr;
-    uint16_t *co_tc = nullptr;
+    uint32_t cls = 0;
+    Runs<T> rs, rt;                  // contraction runs (SIMT, tensor core)
     T *coef = nullptr, *O = nullptr, *ang_diag = nullptr, *O_diag = nullptr;
     T *mask = nullptr;
     T *dinv = nullptr;               // Jacobi: 1 / diag(A), [nP][aslm]
     uint8_t *bmask = nullptr;
     uint32_t aslm = 0;
-    uint32_t ang_nnz = 0;            // ckmax * cls
     int kind = TR_OPERATOR_TENSOR;   // TR_OPERATOR_*
     OpData<T> data(uint32_t nP, uint32_t slm) const {
         OpData<T> d;
@@ -175,11 +190,9 @@ struct DeviceOp {
         d.row = row;
         d.col = col;
         d.coef = coef;
-        d.ckmax = ckmax;
         d.cls = cls;
-        d.ce = ce;
-        d.cw = cw;
-        d.co_tc = co_tc;
+        d.rs = rs;
+        d.rt = rt;
         d.O = O;
         d.ang_diag = ang_diag;
         d.O_diag = O_diag;
@@ -255,6 +268,7 @@ struct tr_ctx {
 
     std::vector<void *> allocations;
     int64_t launches = 0;            // kernels launched (for solve reports)
+    int last_cg_engine = 0;          // the engine the last CG run used (TR_ENGINE_*)
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // solve [0,1], CG launches [2,3]
     double cg_ms = 0.0;              // device time of the CG-iteration launches of a solve
     int64_t cg_launches = 0;         // those launches (persistent kernels or graph replays)

@@ -521,7 +521,7 @@ bool search(const Problem &pr, const std::vector<int> &kinds, uint64_t seed, int
             const std::atomic<bool> &stop, LebedevQuad &q) {
     const OrbitSpec &sp = pr.sp;
     Rng rng{seed};
-    const double r2 = std::sqrt(0.5), kPi = std::acos(-1.0);
+    const double kPi = std::acos(-1.0);
     std::vector<double> best;   // orbit parameters of the smallest projected residual so far
     double best_f = HUGE_VAL;
 

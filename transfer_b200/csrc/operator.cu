@@ -10,9 +10,10 @@
 // memory; the group then walks the chunk NB edges at a time, broadcasting
 // u by shuffle, so NB independent row gathers f[u][*] are in flight at
 // once.  The mass term and the nine spatial sums S_v[3i+j][lm] accumulate
-// in registers.  The angular coupling then runs from shared memory: lane
-// lm sums omega_i[lms][lm] * S_v[3i+pos][lms] over the nonzero (i, lms) of
-// its column (a sparse list staged in shared memory when it fits).
+// in registers.  The angular coupling then runs from shared memory:
+// out[lm] = sum omega_i[lms][lm] * S_v[3i+pos][lms] over the nonzero
+// (i, lms) of column lm, all columns' entries cut into equal runs, one per
+// lane (Runs in internal.h; staged in shared memory when they fit).
 // Boundary vertices add the half-range term from three per-axis sums
 // B_n[lms], skipping absent axes.  One launch computes all of A f (the
 // reference needs two) and, for CG, fuses <p, A p> with a deterministic
@@ -89,20 +90,15 @@ __host__ __device__ constexpr int batch_of(int H) { return H == 1 ? TR_GATHER_BA
 
 __host__ __device__ inline size_t align16(size_t b) { return (b + 15) & ~size_t(15); }
 
-// bytes of the staged contraction tables: (weight, offset) pairs for the
-// SIMT kernels, weights + C-table offsets for the tensor-core ones
-template <typename T>
-__host__ __device__ inline size_t ang_smem_bytes(uint32_t ncon, bool tc) {
-    return tc ? align16(ncon * sizeof(T)) + align16(ncon * sizeof(uint16_t)) : align16(ncon * sizeof(CEnt<T>));
-}
 // per-group shared slab: staged edge coefficients + the S / B table,
 // rounded to 16 bytes so every slab (and its vector stores) stays aligned
 template <int G, int H, typename T>
 __host__ __device__ constexpr size_t group_smem_elems() {
     // two edge-record buffers [2][G][kCoefStride], two neighbour-index
-    // buffers [2][G] (uint32), the S / B table [kSymRows][G*H+1]
+    // buffers [2][G] (uint32), the S / B table [kSymRows][G*H+1], the chunk
+    // sums of the contraction rounds [runs_part_elems(G, H)]
     return (2 * G * kCoefStride + (2 * G * 4 + sizeof(T) - 1) / sizeof(T) + kSymRows * (G * H + 1) +
-            (16 / sizeof(T)) - 1) / (16 / sizeof(T)) * (16 / sizeof(T));
+            runs_part_elems(G, H) + (16 / sizeof(T)) - 1) / (16 / sizeof(T)) * (16 / sizeof(T));
 }
 // Loads of vectors that other blocks of the same launch may have written
 // (persistent kernel) avoid the non-coherent read-only path (ld.global.nc
@@ -132,13 +128,12 @@ __device__ __forceinline__ void gather_row(const T *__restrict__ f, const T *__r
     }
 }
 
-// Shared-memory tables staged once per block: the sparse angular lists and,
-// when small, the three half-range tables O_n.
+// Shared-memory tables staged once per block: the contraction rounds of the
+// kernel's form and, when small, the three half-range tables O_n.
 template <typename T>
 struct Staged {
-    const CEnt<T> *ce;    // SIMT contraction entries [ckmax][cls]
-    const T *cw;          // tensor-core contraction weights [ckmax][cls]
-    const uint16_t *co;   // tensor-core C-table offsets [ckmax][cls]
+    const unsigned char *run;  // Runs entries
+    const uint32_t *rsp;       // chunk span of each harmonic [slm]
     const T *O;
     size_t bytes;
 };
@@ -147,35 +142,21 @@ __host__ __device__ inline size_t O_smem_bytes(uint32_t slm, uint32_t cls) {
     return align16(3 * static_cast<size_t>(slm) * cls * sizeof(T));
 }
 
-// flags: 1 stage the contraction tables, 2 stage O, 4 use the tensor-core
-// (C table) offsets
+// flags: 1 stage the contraction rounds, 2 stage O, 4 the tensor-core
+// rounds (C-table offsets) instead of the SIMT ones
 template <typename T>
 __device__ __forceinline__ Staged<T> stage_tables(const OpData<T> &d, unsigned char *smem, int flags) {
-    const bool tc = (flags & 4) != 0;
-    Staged<T> st{d.ce, d.cw, d.co_tc, d.O, 0};
-    const uint32_t ncon = d.ckmax * d.cls;
-    if ((flags & 1) && tc) {
-        T *sw = reinterpret_cast<T *>(smem);
-        uint16_t *so = reinterpret_cast<uint16_t *>(smem + align16(ncon * sizeof(T)));
-        for (uint32_t i = threadIdx.x; i < ncon; i += blockDim.x) {
-            sw[i] = __ldg(d.cw + i);
-            so[i] = __ldg(d.co_tc + i);
-        }
-        st.cw = sw;
-        st.co = so;
-        st.bytes = ang_smem_bytes<T>(ncon, true);
-    } else if (flags & 1) {
-        typedef typename Vec16<T>::type V;  // one entry is 8 (FP32) or 16 (FP64) bytes
-        CEnt<T> *se = reinterpret_cast<CEnt<T> *>(smem);
-        if (sizeof(CEnt<T>) == 16) {
-            for (uint32_t i = threadIdx.x; i < ncon; i += blockDim.x)
-                reinterpret_cast<V *>(se)[i] = __ldg(reinterpret_cast<const V *>(d.ce) + i);
-        } else {
-            for (uint32_t i = threadIdx.x; i < ncon; i += blockDim.x)
-                reinterpret_cast<uint2 *>(se)[i] = __ldg(reinterpret_cast<const uint2 *>(d.ce) + i);
-        }
-        st.ce = se;
-        st.bytes = ang_smem_bytes<T>(ncon, false);
+    const Runs<T> &R = (flags & 4) ? d.rt : d.rs;
+    Staged<T> st{R.tab, R.span, d.O, 0};
+    if (flags & 1) {
+        const size_t eb = runs_entry_bytes(R);  // a multiple of 16: L, R are multiples of 4
+        uint32_t *ss = reinterpret_cast<uint32_t *>(smem + align16(eb));
+        for (uint32_t i = threadIdx.x; i < eb / 16; i += blockDim.x)
+            reinterpret_cast<uint4 *>(smem)[i] = __ldg(reinterpret_cast<const uint4 *>(R.tab) + i);
+        for (uint32_t i = threadIdx.x; i < d.slm; i += blockDim.x) ss[i] = __ldg(R.span + i);
+        st.run = smem;
+        st.rsp = ss;
+        st.bytes = runs_smem_bytes<T>(R, d.slm);
     }
     if (flags & 2) {
         T *so = reinterpret_cast<T *>(smem + st.bytes);
@@ -188,41 +169,53 @@ __device__ __forceinline__ Staged<T> stage_tables(const OpData<T> &d, unsigned c
     return st;
 }
 
-// out += sum_k cw[k][lm] * S[co[k][lm]]  (lane-major tables: coalesced)
+// entry i of a Runs table of n entries: FP32 one (w, o) pair, FP64 the
+// weight block then the offset block
 template <typename T>
-__device__ __forceinline__ T contract(const Staged<T> &tab, const T *S, uint32_t lm, uint32_t kmax, uint32_t ls,
-                                      T acc0) {
-    const T *w = tab.cw + lm;
-    const uint16_t *o = tab.co + lm;
-    T acc1 = T(0), acc2 = T(0), acc3 = T(0);
-    uint32_t k = 0;
-    for (; k + 3 < kmax; k += 4) {
-        acc0 = fma(w[k * ls], S[o[k * ls]], acc0);
-        acc1 = fma(w[(k + 1) * ls], S[o[(k + 1) * ls]], acc1);
-        acc2 = fma(w[(k + 2) * ls], S[o[(k + 2) * ls]], acc2);
-        acc3 = fma(w[(k + 3) * ls], S[o[(k + 3) * ls]], acc3);
-    }
-    for (; k < kmax; ++k) acc0 = fma(w[k * ls], S[o[k * ls]], acc0);
-    return (acc0 + acc2) + (acc1 + acc3);
+__device__ __forceinline__ void run_entry(const unsigned char *tab, size_t n, size_t i, T &w, uint32_t &o);
+template <>
+__device__ __forceinline__ void run_entry<float>(const unsigned char *tab, size_t, size_t i, float &w, uint32_t &o) {
+    const uint2 e = reinterpret_cast<const uint2 *>(tab)[i];
+    w = __uint_as_float(e.x);
+    o = e.y;
+}
+template <>
+__device__ __forceinline__ void run_entry<double>(const unsigned char *tab, size_t n, size_t i, double &w,
+                                                  uint32_t &o) {
+    w = reinterpret_cast<const double *>(tab)[i];
+    o = reinterpret_cast<const uint32_t *>(tab + 8 * n)[i];
 }
 
-// the SIMT form: (weight, offset) entries at a compile-time lane stride LS
-template <typename T, int LS>
-__device__ __forceinline__ T contract_ls(const CEnt<T> *__restrict__ e, const T *S, uint32_t kmax, T acc0) {
-    T acc1 = T(0), acc2 = T(0), acc3 = T(0);
-    uint32_t k = 0;
-    for (; k + 3 < kmax; k += 4, e += 4 * LS) {
-        const CEnt<T> e0 = e[0], e1 = e[LS], e2 = e[2 * LS], e3 = e[3 * LS];
-        acc0 = fma(e0.w, S[e0.o], acc0);
-        acc1 = fma(e1.w, S[e1.o], acc1);
-        acc2 = fma(e2.w, S[e2.o], acc2);
-        acc3 = fma(e3.w, S[e3.o], acc3);
+// The lane's chunks of the contraction rounds (Runs): in round r the lane
+// sums chunk r * L + lane over R steps (four accumulators, the loads of four
+// steps issued before their FMAs) from the table S and stores the sum to
+// part[r * L + lane].
+template <typename T, int L>
+__device__ __forceinline__ void contract_rounds(const Runs<T> &R, const unsigned char *tab, int lane, const T *S,
+                                                T *part) {
+    const size_t n = static_cast<size_t>(R.rounds) * R.R * L;
+    size_t i = lane;
+    for (uint32_t r = 0; r < R.rounds; ++r) {
+        T a[4] = {T(0), T(0), T(0), T(0)};
+        for (uint32_t j = 0; j < R.R; j += 4, i += 4 * L) {
+            T w[4], x[4];
+            uint32_t o[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) run_entry<T>(tab, n, i + q * L, w[q], o[q]);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) x[q] = S[o[q]];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) a[q] = fma(w[q], x[q], a[q]);
+        }
+        part[r * L + lane] = (a[0] + a[2]) + (a[1] + a[3]);
     }
-    for (; k < kmax; ++k, e += LS) {
-        const CEnt<T> e0 = e[0];
-        acc0 = fma(e0.w, S[e0.o], acc0);
-    }
-    return (acc0 + acc2) + (acc1 + acc3);
+}
+// harmonic lm's coupling: acc0 plus its chunk sums, in chunk order
+template <typename T>
+__device__ __forceinline__ T sum_chunks(const uint32_t *span, const T *part, uint32_t lm, T acc0) {
+    const uint32_t sp = span[lm], c1 = sp >> 16;
+    for (uint32_t c = sp & 0xFFFFu; c < c1; ++c) acc0 += part[c];
+    return acc0;
 }
 
 // the 11 used coefficients of one staged edge record (vector shared loads)
@@ -493,7 +486,7 @@ __device__ __forceinline__ void simt_vertices(const OpData<T> &d, const Staged<T
                                               const Src &src, const Out &fin, double (&dacc)[Out::NV]) {
     constexpr int SA = G * H + 1;  // padded row of the shared S / B tables
     constexpr int NB = batch_of(H);
-    constexpr int LS = G * H < 32 ? 32 : G * H;  // lane stride of the tables (== d.cls, checked at launch)
+    constexpr int LS = G * H < 32 ? 32 : G * H;  // lane stride of O (== d.cls, checked at launch)
     const uint32_t slm = d.slm, aslm = d.aslm;
     T *slab = reinterpret_cast<T *>(smem_groups) + (threadIdx.x / G) * group_smem_elems<G, H, T>();
     uint32_t *scolbuf = reinterpret_cast<uint32_t *>(slab + 2 * G * kCoefStride);  // [2][G]
@@ -595,11 +588,17 @@ __device__ __forceinline__ void simt_vertices(const OpData<T> &d, const Staged<T
 #pragma unroll
             for (int q = 0; q < kSymRows; ++q) sm[q * SA + lane + G * h] = acc[h].S(q);
         tile.sync();
+        // the contraction rounds: the chunk sums land in `part`, then each
+        // harmonic adds its chunks to its mass term
+        T *part = sm + kSymRows * SA;
+        contract_rounds<T, G>(d.rs, tab.run, lane, sm, part);
+        tile.sync();
         T out[H];
 #pragma unroll
         for (int h = 0; h < H; ++h) {
             const uint32_t lm = lane + G * h;
-            out[h] = contract_ls<T, LS>(tab.ce + lm, sm, d.ckmax, acc[h].mass(lm == 0));
+            out[h] = acc[h].mass(lm == 0);
+            if (lm < slm) out[h] = sum_chunks<T>(tab.rsp, part, lm, out[h]);
         }
         // half-range boundary term from the per-axis sums B_n
         if (axes_v) {
@@ -856,12 +855,17 @@ __device__ __forceinline__ double lhs_vertices_tc(const OpData<T> &d, const Stag
           }
         }
         __syncwarp();
-        // epilogue: lane = harmonic
+        // epilogue: the contraction rounds over the C table (chunk sums into
+        // rows 11-15, which the edge records leave zero), then lane = harmonic
+        // adds its chunks, the mass term and the boundary term
+        T *part = sm + 11 * SA;
+        contract_rounds<T, 32>(d.rt, tab.run, lane, sm, part);
+        __syncwarp();
         T *rv = r + static_cast<size_t>(v) * aslm;
         for (uint32_t lm = lane; lm < aslm; lm += 32) {
             T out = T(0);
             if (lm < slm) {
-                T acc0 = contract<T>(tab, sm, lm, d.ckmax, d.cls, sm[(lm == 0 ? kRowM0 : kRowM) * SA + lm]);
+                T acc0 = sum_chunks<T>(tab.rsp, part, lm, sm[(lm == 0 ? kRowM0 : kRowM) * SA + lm]);
                 T acc1 = T(0);
                 if (axes) {
                     for (int n = 0; n < 3; ++n) {
@@ -904,7 +908,7 @@ template <int G, int H, typename T>
 struct SimtOp {
     static constexpr int kMinBlocks = sizeof(T) == 8 ? (H > 2 ? 1 : 2) : (H > 1 ? 2 : TR_SIMT_F32_MINBLOCKS);
     static constexpr int kLanes = G;
-    static constexpr uint32_t kLS = G * H < 32 ? 32 : G * H;  // lane stride of the contraction tables
+    static constexpr uint32_t kLS = G * H < 32 ? 32 : G * H;  // lane stride of the O table
     static constexpr bool kTc = false;
     // the persistent CG kernel runs all resident threads of an SM as one block
     static constexpr int kPersistThreads = kBlock * kMinBlocks > 1024 ? 1024 : kBlock * kMinBlocks;
@@ -1273,15 +1277,26 @@ constexpr size_t kAngSmemBudget = 64 * 1024;
 constexpr size_t kOSmemBudget = 40 * 1024;
 
 template <class Op, typename T>
-static int stage_flags(uint32_t slm, uint32_t cls, uint32_t nnz) {
-    return (ang_smem_bytes<T>(nnz, Op::kTc) <= kAngSmemBudget ? 1 : 0) |
-           (O_smem_bytes<T>(slm, cls) <= kOSmemBudget ? 2 : 0) | (Op::kTc ? 4 : 0);
+static const Runs<T> &op_runs(const OpData<T> &d) {
+    return Op::kTc ? d.rt : d.rs;
 }
 template <class Op, typename T>
-static size_t lhs_smem(uint32_t slm, uint32_t cls, uint32_t nnz, int threads) {
-    const int fl = stage_flags<Op, T>(slm, cls, nnz);
-    return ((fl & 1) ? ang_smem_bytes<T>(nnz, Op::kTc) : 0) + ((fl & 2) ? O_smem_bytes<T>(slm, cls) : 0) +
-           Op::slab_bytes(threads);
+static int stage_flags(const OpData<T> &d) {
+    return (runs_smem_bytes<T>(op_runs<Op>(d), d.slm) <= kAngSmemBudget ? 1 : 0) |
+           (O_smem_bytes<T>(d.slm, d.cls) <= kOSmemBudget ? 2 : 0) | (Op::kTc ? 4 : 0);
+}
+template <class Op, typename T>
+static size_t lhs_smem(const OpData<T> &d, int threads) {
+    const int fl = stage_flags<Op, T>(d);
+    return ((fl & 1) ? runs_smem_bytes<T>(op_runs<Op>(d), d.slm) : 0) +
+           ((fl & 2) ? O_smem_bytes<T>(d.slm, d.cls) : 0) + Op::slab_bytes(threads);
+}
+// the runs of the kernel's form were built for its lanes and the O table for
+// its lane stride
+template <class Op, typename T>
+static bool tables_fit(const OpData<T> &d) {
+    return op_runs<Op>(d).L == static_cast<uint32_t>(Op::kLanes) && op_runs<Op>(d).rounds > 0 &&
+           (!Op::kLS || d.cls == Op::kLS);
 }
 
 // preferred shared-memory carveout (percent of the unified L1/shared array)
@@ -1329,8 +1344,8 @@ static cudaError_t with_op(const DeviceOp<T> &op, uint32_t slm, F &&fn) {
 
 template <class Op, typename T, bool DOT, bool FUSEP, class Fin>
 static cudaError_t launch_one(const tr_ctx *c, const OpData<T> &d, const LhsArgs<T> &a, Fin fin, cudaStream_t s) {
-    if (Op::kLS && d.cls != Op::kLS) return cudaErrorInvalidValue;  // tables built for another lane stride
-    const size_t smem = lhs_smem<Op, T>(d.slm, d.cls, a.ang_nnz, kBlock);
+    if (!tables_fit<Op>(d)) return cudaErrorInvalidValue;
+    const size_t smem = lhs_smem<Op, T>(d, kBlock);
     auto kern = k_lhs<Op, T, DOT, FUSEP, Fin>;
     static size_t opted = 0;  // dynamic shared memory granted so far (per instantiation)
     cudaError_t e = opt_in_smem(kern, smem, opted);
@@ -1347,14 +1362,13 @@ static cudaError_t launch_one(const tr_ctx *c, const OpData<T> &d, const LhsArgs
     const int gpb = kBlock / Op::kLanes;
     const int grid = std::max(1, std::min(c->num_sms * per_sm, static_cast<int>((d.nP + gpb - 1) / gpb)));
     kern<<<grid, kBlock, smem, s>>>(d, a.x, a.pold, a.pnew, a.y, c->partials, c->counters, fin, a.done, a.cgs,
-                                    stage_flags<Op, T>(d.slm, d.cls, a.ang_nnz));
+                                    stage_flags<Op, T>(d));
     return cudaGetLastError();
 }
 
 template <typename T>
 cudaError_t launch_lhs(const tr_ctx *c, const DeviceOp<T> &op, LhsArgs<T> a, cudaStream_t s) {
     const OpData<T> d = op.data(c->nP, c->slm);
-    a.ang_nnz = op.ang_nnz;
     return with_op<T>(op, c->slm, [&](auto tag) -> cudaError_t {
         typedef decltype(tag) Op;
         switch (a.fin_kind) {
@@ -1395,12 +1409,12 @@ cudaError_t launch_lhs_diag(const tr_ctx *c, const DeviceOp<T> &op, const T *f, 
 }
 
 template <class Op, typename T, bool JAC>
-static cudaError_t launch_pcg(const tr_ctx *c, const OpData<T> &d, const PcgArgs<T> &a, uint32_t nnz, cudaStream_t s,
+static cudaError_t launch_pcg(const tr_ctx *c, const OpData<T> &d, const PcgArgs<T> &a, cudaStream_t s,
                               int *grid_out) {
-    if (Op::kLS && d.cls != Op::kLS) return cudaErrorInvalidValue;
+    if (!tables_fit<Op>(d)) return cudaErrorInvalidValue;
     auto kern = k_cg_persistent<Op, T, JAC>;
     constexpr int threads = Op::kPersistThreads;
-    const size_t smem = lhs_smem<Op, T>(d.slm, d.cls, nnz, threads);
+    const size_t smem = lhs_smem<Op, T>(d, threads);
     static size_t opted = 0;
     cudaError_t e = opt_in_smem(kern, smem, opted);
     if (e != cudaSuccess) return e;
@@ -1413,7 +1427,7 @@ static cudaError_t launch_pcg(const tr_ctx *c, const OpData<T> &d, const PcgArgs
     const int need = static_cast<int>((d.nP + gpb - 1) / gpb);
     const int grid = std::max(1, std::min(per_sm * c->num_sms, std::min(need, kMaxGrid)));
     *grid_out = grid;
-    int flags = stage_flags<Op, T>(d.slm, d.cls, nnz);
+    int flags = stage_flags<Op, T>(d);
     OpData<T> dd = d;
     PcgArgs<T> aa = a;
     void *args[] = {&dd, &aa, &flags};
@@ -1424,12 +1438,10 @@ template <typename T>
 cudaError_t launch_cg_persistent(const tr_ctx *c, const DeviceOp<T> &op, const PcgArgs<T> &a, cudaStream_t s,
                                  int *grid_out) {
     const OpData<T> d = op.data(c->nP, c->slm);
-    const uint32_t nnz = op.ang_nnz;
     const bool jac = a.dinv != nullptr;
     return with_op<T>(op, c->slm, [&](auto tag) -> cudaError_t {
         typedef decltype(tag) Op;
-        return jac ? launch_pcg<Op, T, true>(c, d, a, nnz, s, grid_out)
-                   : launch_pcg<Op, T, false>(c, d, a, nnz, s, grid_out);
+        return jac ? launch_pcg<Op, T, true>(c, d, a, s, grid_out) : launch_pcg<Op, T, false>(c, d, a, s, grid_out);
     });
 }
 template cudaError_t launch_cg_persistent<double>(const tr_ctx *, const DeviceOp<double> &, const PcgArgs<double> &,
@@ -1438,11 +1450,11 @@ template cudaError_t launch_cg_persistent<float>(const tr_ctx *, const DeviceOp<
                                                  cudaStream_t, int *);
 
 template <class Op, typename T, bool JAC>
-static cudaError_t launch_sr(const tr_ctx *c, const OpData<T> &d, const SrArgs<T> &a, uint32_t nnz, cudaStream_t s) {
-    if (Op::kLS && d.cls != Op::kLS) return cudaErrorInvalidValue;
+static cudaError_t launch_sr(const tr_ctx *c, const OpData<T> &d, const SrArgs<T> &a, cudaStream_t s) {
+    if (!tables_fit<Op>(d)) return cudaErrorInvalidValue;
     constexpr int threads = Op::kPersistThreads;
     auto kern = k_sr_persistent<Op, T, JAC>;
-    const size_t smem = lhs_smem<Op, T>(d.slm, d.cls, nnz, threads);
+    const size_t smem = lhs_smem<Op, T>(d, threads);
     static size_t opted = 0;
     cudaError_t e = opt_in_smem(kern, smem, opted);
     if (e != cudaSuccess) return e;
@@ -1453,7 +1465,7 @@ static cudaError_t launch_sr(const tr_ctx *c, const OpData<T> &d, const SrArgs<T
     const int gpb = threads / Op::kLanes;
     const int need = static_cast<int>((d.nP + gpb - 1) / gpb);
     const int grid = std::max(1, std::min(per_sm * c->num_sms, std::min(need, kMaxGrid / 2)));
-    int flags = stage_flags<Op, T>(d.slm, d.cls, nnz);
+    int flags = stage_flags<Op, T>(d);
     OpData<T> dd = d;
     SrArgs<T> aa = a;
     void *args[] = {&dd, &aa, &flags};
@@ -1465,14 +1477,13 @@ template <typename T>
 cudaError_t launch_sr_persistent(const tr_ctx *c, const DeviceOp<T> &op, const SrArgs<T> &a, cudaStream_t s) {
     if (op.kind != TR_OPERATOR_SIMT) return cudaErrorNotSupported;
     const OpData<T> d = op.data(c->nP, c->slm);
-    const uint32_t nnz = op.ang_nnz;
     const bool jac = a.dinv != nullptr;
     return with_op<T>(op, c->slm, [&](auto tag) -> cudaError_t {
         typedef decltype(tag) Op;
         if constexpr (Op::kTc) {
             return cudaErrorNotSupported;
         } else {
-            return jac ? launch_sr<Op, T, true>(c, d, a, nnz, s) : launch_sr<Op, T, false>(c, d, a, nnz, s);
+            return jac ? launch_sr<Op, T, true>(c, d, a, s) : launch_sr<Op, T, false>(c, d, a, s);
         }
     });
 }

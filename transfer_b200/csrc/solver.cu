@@ -241,8 +241,10 @@ static tr_status run_cg(tr_ctx *c, int slot, const DeviceOp<T> &op, uint32_t asl
         }
         *iters = k;
         *done_out = done;
+        c->last_cg_engine = TR_ENGINE_PERSISTENT;
         return TR_OK;
     }
+    c->last_cg_engine = engine;
     const int use_graph = (engine == TR_ENGINE_GRAPH);
     static_assert(kCgChunk % 2 == 0, "the p buffers must be back in place after a chunk");
     cudaStream_t st = stream_of(c);
@@ -466,7 +468,7 @@ static tr_status solve_mixed(tr_ctx *c, const tr_solve_opts *o, const double *b,
     // runs in the frame of the normalised residual; frame_scale is that
     // frame's ||r64||).  The single-reduction engine restarts each time.
     bool started = false, restart = true;
-    int k_run = 0;
+    int k_run = 0, leg_k = 0;
     double frame_scale = rn, leg_tol = 0.0;
     while (!converged && outer < max_outer && total < (o->max_iter > 0 ? o->max_iter : 1 << 30)) {
         LAUNCH(launch_to_f32(c, r64, r, so, st));
@@ -520,9 +522,12 @@ static tr_status solve_mixed(tr_ctx *c, const tr_solve_opts *o, const double *b,
                 TRY(cudaMemcpyAsync(&si->tol, &h.tol, sizeof(double), cudaMemcpyHostToDevice, st));
                 TRY(cudaMemcpyAsync(&si->maxit, &h.maxit, sizeof(int32_t), cudaMemcpyHostToDevice, st));
                 LAUNCH(launch_cg_reliable(c, d, r, z, dinv, si, rn / frame_scale, st));
-                // the graph and launch engines take p_old from buffer 0 at the
-                // start of a leg (the persistent kernel from buffer k & 1)
-                if (k_run & 1)
+                // The persistent kernel reads p_old from buffer k & 1 (k the
+                // running iteration count), where its last leg left it.  The
+                // graph and launch engines start every leg at chunk position
+                // 0, reading buffer 0, and a leg of m iterations leaves its
+                // last direction in buffer m & 1.
+                if (c->last_cg_engine != TR_ENGINE_PERSISTENT && (leg_k & 1))
                     TRY(cudaMemcpyAsync(p, c->w32[5], sizeof(float) * c->nP * c->aslm32, cudaMemcpyDeviceToDevice,
                                         st));
             }
@@ -534,6 +539,7 @@ static tr_status solve_mixed(tr_ctx *c, const tr_solve_opts *o, const double *b,
                                base_engine(o->engine), &kc, &done);
             k = kc - k_run;  // iterations of this leg
             k_run = kc;
+            leg_k = k;
             leg_tol = inner_tol;
         }
         if (ts != TR_OK) return ts;

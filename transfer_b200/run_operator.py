@@ -36,7 +36,7 @@ def _main():
     byt, flops = W.algorithmic_work(md, ad, real_bytes=args.precision // 8)
     t = ms.value * 1e-3
     print(f"{desc['workload']}: nP {ctx.nP}, nT {ctx.nT}, slm {ctx.slm}, edges {ctx.n_edges}; FP{args.precision} "
-          f"operator {1e3 * t:.1f} us, {byt / t / 1e9:.0f} GB/s and {flops / t / 1e12:.2f} TFLOP/s algorithmic")
+          f"operator {1e6 * t:.1f} us, {byt / t / 1e9:.0f} GB/s and {flops / t / 1e12:.2f} TFLOP/s algorithmic")
     ctx.close()
 
 
