@@ -43,6 +43,7 @@ restatement of the reference path (the reference has no CPU solve of its
 own) on all host cores, rank 0 only.
 """
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -465,13 +466,17 @@ def stellar_section(local, peak):
     S.apply(precision=32)
     mom_bytes = 4 * nq * nT * 4 + 16 * nT * 4 * 8          # psi read once, 16 FP64 moments written
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    for kind, name in ((tr._lib.TR_MOMENTS_TCGEN05, "tcgen05"), (tr._lib.TR_MOMENTS_MMA_SYNC, "mma_sync")):
+    # one preallocated output: the timed calls are tr_sweep_moments alone (a
+    # fresh zeroed output per call would add a 1.4 GB fill to each)
+    mom = torch.empty(16 * 4 * nT, dtype=torch.float64, device=f"cuda:{local}")
+    for kind, name in ((tr._lib.TR_MOMENTS_TCGEN05, "tcgen05"), (tr._lib.TR_MOMENTS_MMA_SYNC, "mma_sync"),
+                       (tr._lib.TR_MOMENTS_TMA_FFMA2, "tma_ffma2")):
         S.set_moments_kernel(kind)
-        S.moments(16)
+        tr._lib.check(tr._lib.lib.tr_sweep_moments(S._h, 16, ctypes.c_void_p(mom.data_ptr())))
         torch.cuda.synchronize()
         e0.record()
         for _ in range(10):
-            S.moments(16)
+            tr._lib.check(tr._lib.lib.tr_sweep_moments(S._h, 16, ctypes.c_void_p(mom.data_ptr())))
         e1.record()
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / 10

@@ -490,8 +490,12 @@ tr_status tr_sweep_moments(tr_sweep *s, int nmom, double *mom);
  * TR_MOMENTS_TCGEN05 (default): tcgen05 MMAs with tensor-memory
  * accumulators, psi tiles loaded by TMA (up to 1,024 ordinates);
  * TR_MOMENTS_MMA_SYNC: warp-level mma.sync with cp.async staging (up to 384
- * ordinates).  Larger ordinate sets, and FP64 sweeps, use FP64 FMAs. */
-enum { TR_MOMENTS_TCGEN05 = 0, TR_MOMENTS_MMA_SYNC = 1 };
+ * ordinates);
+ * TR_MOMENTS_TMA_FFMA2: psi tiles loaded by TMA, paired FP32 FMAs, each
+ * accumulator over an eighth of the ordinates and the eight partial sums
+ * added in FP64 (up to 1,024 ordinates).
+ * Larger ordinate sets, and FP64 sweeps, use FP64 FMAs. */
+enum { TR_MOMENTS_TCGEN05 = 0, TR_MOMENTS_MMA_SYNC = 1, TR_MOMENTS_TMA_FFMA2 = 2 };
 tr_status tr_sweep_set_moments_kernel(tr_sweep *s, int kind);
 /* FP64 energy balance of the last sweep given its inputs J_in, B_in and its
  * scalar flux J_out:  out = {emitted, absorbed, escaped, incoming,

@@ -90,11 +90,15 @@ def test_balance_matches_oracle_and_closes(cuda):
         1e-12 * bg["emitted"]
 
 
-@pytest.mark.parametrize("precision,kernel", [(64, None), (32, "tcgen05"), (32, "mma_sync")])
+MOMENT_KERNELS = {"tcgen05": tr._lib.TR_MOMENTS_TCGEN05, "mma_sync": tr._lib.TR_MOMENTS_MMA_SYNC,
+                  "tma_ffma2": tr._lib.TR_MOMENTS_TMA_FFMA2}
+
+
+@pytest.mark.parametrize("precision,kernel", [(64, None), (32, "tcgen05"), (32, "mma_sync"), (32, "tma_ffma2")])
 def test_moments_match_oracle(cuda, precision, kernel):
     md, ph, S, O = pair(scattering_box(), op.ordinates_product(6, 12))
     if kernel:
-        S.set_moments_kernel(tr._lib.TR_MOMENTS_TCGEN05 if kernel == "tcgen05" else tr._lib.TR_MOMENTS_MMA_SYNC)
+        S.set_moments_kernel(MOMENT_KERNELS[kernel])
     S.apply(precision=precision)
     _, _, psio = O.apply(want_psi=True)
     mo = O.moments(psio, 16)
@@ -124,6 +128,11 @@ def test_moments_tcgen05_split_tf32_accuracy(cuda, n, polar, azim):
     if polar * azim <= 384:
         S.set_moments_kernel(tr._lib.TR_MOMENTS_MMA_SYNC)
         assert rel_err(host(S.moments(16)), mo) < 1e-5
+    # FFMA2 form: each FP32 accumulator sums an eighth of the ordinates, the
+    # eight partial sums are added in FP64
+    S.set_moments_kernel(tr._lib.TR_MOMENTS_TMA_FFMA2)
+    for nmom in (16, 5):
+        assert rel_err(host(S.moments(nmom)), mo[:nmom]) < 1e-6
     with pytest.raises(tr.TransferError):
         S.set_moments_kernel(7)
 

@@ -35,7 +35,7 @@ TR_OPERATOR_SIMT, TR_OPERATOR_TENSOR = 0, 1
 TR_SWEEP_GMRES, TR_SWEEP_SOURCE_ITERATION = 0, 1
 TR_SWEEP_PREC_NONE, TR_SWEEP_PREC_DSA = 0, 1
 TR_SWEEP_DSA_AUTO, TR_SWEEP_DSA_CLUSTER, TR_SWEEP_DSA_EVEN_PARITY = 0, 1, 2
-TR_MOMENTS_TCGEN05, TR_MOMENTS_MMA_SYNC = 0, 1
+TR_MOMENTS_TCGEN05, TR_MOMENTS_MMA_SYNC, TR_MOMENTS_TMA_FFMA2 = 0, 1, 2
 TR_BATCH_RULE, TR_BATCH_STATIC_FULL, TR_BATCH_STATIC_SMALL, TR_BATCH_QUEUE_FULL, TR_BATCH_QUEUE_SMALL = -1, 0, 1, 2, 3
 TR_VTK_POINT, TR_VTK_CELL = 0, 1
 TR_VTK_SCALAR, TR_VTK_VECTOR, TR_VTK_TENSOR = 0, 1, 2

@@ -62,7 +62,13 @@ namespace {
 constexpr int kTileM = 128;        // rows per tile (one MMA M)
 constexpr int kStageK = 32;        // ordinates per stage
 constexpr int kMaxStages = 10;     // shared-memory stages (the launch picks how many fit)
-constexpr uint32_t kLoSlots = 4;   // tensor-memory slots of a_lo
+// tensor-memory slots of a_lo: how many stages the split warps may run ahead
+// of the products that free them (each slot returns only after its stage's
+// products finish, so the slots bound the stages in flight on that loop)
+#ifndef TR_MOM_LO_SLOTS
+#define TR_MOM_LO_SLOTS 4
+#endif
+constexpr uint32_t kLoSlots = TR_MOM_LO_SLOTS;
 constexpr int kAtomBytes = 32 * 4 * kStageK;         // 32 rows x 32 ordinates x 4 B = 4 KB
 constexpr int kStageBytes = 4 * kAtomBytes;          // 16 KB
 constexpr uint32_t kSplitWarps = 8;                  // warps 4-11; warps 12-15 drain the accumulators
@@ -474,6 +480,202 @@ cudaError_t launch_moments_tcgen05(const float *psi, uint32_t M, uint32_t nq, co
     const int grid = static_cast<int>(tiles < static_cast<uint32_t>(num_sms) ? tiles : num_sms);
     const uint32_t nqp = (nq + kStageK - 1) / kStageK * kStageK;
     k_moments_tcgen05<<<grid, kThreads, smem, stream>>>(map, M, nq, nqp, W, nmom, mom, err, stages_for(nq));
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------ FFMA2 form
+// The same contraction on paired FP32 FMAs (FFMA2: two independent
+// round-to-nearest FMAs per instruction), psi streamed by TMA as above.  The
+// tensor-core form issues eight small MMAs (M 128, N 32 or 16, K 8) per 16 KB
+// stage from one thread, about 1,300 cycles a stage; here the 16 FMAs an
+// element needs take a fraction of the SM's issue rate.  Measured on the
+// 2.78 M-tet sphere with 302 ordinates, both forms take the same time
+// (3.76-3.79 ms, 3.9 TB/s): neither the MMA issue nor the FMAs bound the
+// contraction; a TMA stream of the same tiles with no work at all tops out
+// at 5.1 TB/s.  One TMA box of 128 rows x 32 ordinates per 16 KB stage (rows
+// are the contiguous dimension, no swizzle), up to 8 stages in flight, one
+// producer thread.  8 consumer warps: warp w takes ordinates w, w + 8,
+// w + 16, w + 24 of each stage and lane l rows 4l .. 4l + 3 of the tile (one
+// 16-byte shared load per ordinate, the ordinate's 16 FP32 weights as four
+// broadcast loads), 64 FP32 accumulators per thread (16 moments x 4 rows,
+// paired by rows).  Each accumulator thus sums an eighth of the ordinates;
+// at a tile's end the 8 warps' partial sums meet in shared memory and are
+// added in FP64, in warp order.
+namespace {
+constexpr int kFfRows = 128, kFfK = 32, kFfWarps = 8, kFfThreads = 32 * (kFfWarps + 1);
+constexpr int kFfStageBytes = kFfRows * kFfK * 4;            // 16 KB
+constexpr int kFfMaxStages = 8;
+constexpr int kFfRedBytes = kFfWarps * 16 * kFfRows * 4;     // partial sums, 64 KB
+struct FfSmem {
+    uint64_t full[kFfMaxStages], empty[kFfMaxStages];
+    int abort_flag;
+};
+__device__ __forceinline__ void ff_bar_sync() { asm volatile("bar.sync 1, %0;" ::"r"(32 * kFfWarps) : "memory"); }
+}  // namespace
+
+__global__ void __launch_bounds__(kFfThreads, 1)
+    k_moments_tma_ffma2(const __grid_constant__ CUtensorMap psi_map, uint32_t M, uint32_t nq, uint32_t nqp,
+                        const double *__restrict__ W, int nmom, double *__restrict__ mom, unsigned int *err,
+                        uint32_t nstages) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    static_assert(sizeof(FfSmem) <= kSmemHeader, "barrier header");
+    FfSmem &sh = *reinterpret_cast<FfSmem *>(base);
+    uint8_t *stg = base + kSmemHeader;                                              // nstages x 16 KB
+    float *wsm = reinterpret_cast<float *>(stg + nstages * kFfStageBytes);          // [nqp][16]
+    float *red = wsm + static_cast<size_t>(nqp) * 16;                                // [warp][moment][row]
+    volatile int *abort_flag = &sh.abort_flag;
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const uint32_t tiles = (M + kFfRows - 1) / kFfRows, nks = nqp / kFfK;
+
+    for (uint32_t i = threadIdx.x; i < nqp * 16; i += blockDim.x) {
+        const uint32_t k = i >> 4, n = i & 15u;
+        wsm[i] = (k < nq && static_cast<int>(n) < nmom) ? static_cast<float>(W[static_cast<size_t>(n) * nq + k]) : 0.0f;
+    }
+    if (threadIdx.x == 0) {
+        for (uint32_t s = 0; s < nstages; ++s) {
+            mbar_init(smem_u32(&sh.full[s]), 1);
+            mbar_init(smem_u32(&sh.empty[s]), kFfWarps);
+        }
+        sh.abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    if (warp == kFfWarps) {
+        if (lane != 0) return;
+        // ---- TMA producer
+        uint32_t it = 0, inflight = 0;
+        bool ok = true;
+        for (uint32_t tile = blockIdx.x; ok && tile < tiles; tile += gridDim.x)
+            for (uint32_t ks = 0; ks < nks; ++ks, ++it) {
+                const uint32_t s = it % nstages, ph = (it / nstages) & 1u;
+                if (!(ok = mbar_wait(smem_u32(&sh.empty[s]), ph ^ 1u, abort_flag, err))) break;
+                const uint32_t fb = smem_u32(&sh.full[s]);
+                mbar_expect_tx(fb, kFfStageBytes);
+                tma_load_2d(smem_u32(stg + s * kFfStageBytes), &psi_map, static_cast<int>(tile * kFfRows),
+                            static_cast<int>(ks * kFfK), fb);
+                inflight = it + 1;
+            }
+        if (!ok) {  // aborted: wait (bounded, own timer) for the copies already issued
+            for (uint32_t j = inflight > nstages ? inflight - nstages : 0; j < inflight; ++j) {
+                const uint32_t bar = smem_u32(&sh.full[j % nstages]), ph = (j / nstages) & 1u;
+                const unsigned long long t0 = global_ns();
+                while (!mbar_try(bar, ph) && global_ns() - t0 < kWaitNs) {
+                }
+            }
+        }
+        return;
+    }
+    // ---- consumers (warps 0..7).  Every consumer warp takes the same named
+    // barriers in every tile, also after an abort, so none is left waiting.
+    uint32_t it = 0;
+    bool ok = true;
+    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        float2 a01[16], a23[16];
+#pragma unroll
+        for (int n = 0; n < 16; ++n) a01[n] = a23[n] = make_float2(0.0f, 0.0f);
+        for (uint32_t ks = 0; ks < nks; ++ks, ++it) {
+            const uint32_t s = it % nstages, ph = (it / nstages) & 1u;
+            if (ok) ok = mbar_wait_warp(smem_u32(&sh.full[s]), ph, abort_flag, err);
+            if (!ok) continue;
+            const uint8_t *st = stg + s * kFfStageBytes;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const uint32_t k = warp + 8u * j;
+                const float4 v = *reinterpret_cast<const float4 *>(st + k * (kFfRows * 4) + lane * 16);
+                const float4 *wq = reinterpret_cast<const float4 *>(wsm + (ks * kFfK + k) * 16);
+                float wv[16];
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    const float4 t = wq[c];
+                    wv[4 * c] = t.x;
+                    wv[4 * c + 1] = t.y;
+                    wv[4 * c + 2] = t.z;
+                    wv[4 * c + 3] = t.w;
+                }
+                const float2 p01 = make_float2(v.x, v.y), p23 = make_float2(v.z, v.w);
+#pragma unroll
+                for (int n = 0; n < 16; ++n) {
+                    const float2 ww = make_float2(wv[n], wv[n]);
+                    a01[n] = __ffma2_rn(ww, p01, a01[n]);
+                    a23[n] = __ffma2_rn(ww, p23, a23[n]);
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&sh.empty[s]));
+        }
+        if (ok) {
+#pragma unroll
+            for (int n = 0; n < 16; ++n)
+                *reinterpret_cast<float4 *>(red + (warp * 16 + n) * kFfRows + 4 * lane) =
+                    make_float4(a01[n].x, a01[n].y, a23[n].x, a23[n].y);
+        }
+        ff_bar_sync();
+        if (!*abort_flag) {
+            // 16 moments x 128 rows over the 256 consumer threads
+            const uint32_t row = threadIdx.x & (kFfRows - 1), n0 = threadIdx.x >> 7;
+            const uint64_t grow = static_cast<uint64_t>(tile) * kFfRows + row;
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const uint32_t n = n0 + 2u * i;
+                double sum = 0.0;
+#pragma unroll
+                for (int w = 0; w < kFfWarps; ++w) sum += static_cast<double>(red[(w * 16 + n) * kFfRows + row]);
+                if (grow < M && static_cast<int>(n) < nmom) mom[static_cast<uint64_t>(n) * M + grow] = sum;
+            }
+        }
+        ff_bar_sync();
+    }
+}
+
+namespace {
+// shared memory of the FFMA2 form with `stages` stages for nq ordinates
+size_t ff_smem_bytes(uint32_t nq, uint32_t stages) {
+    const uint32_t nqp = (nq + kFfK - 1) / kFfK * kFfK;
+    return 1024 + kSmemHeader + static_cast<size_t>(stages) * kFfStageBytes + static_cast<size_t>(nqp) * 64 +
+           kFfRedBytes;
+}
+uint32_t ff_stages_for(uint32_t nq) {
+    for (uint32_t st = kFfMaxStages; st >= 3; --st)
+        if (ff_smem_bytes(nq, st) <= kSmemLimit) return st;
+    return 0;
+}
+}  // namespace
+
+bool moments_tma_ffma2_supported(uint32_t M, uint32_t nq) {
+    return M > 0 && M % 4 == 0 && nq > 0 && ff_stages_for(nq) != 0;
+}
+
+cudaError_t launch_moments_tma_ffma2(const float *psi, uint32_t M, uint32_t nq, const double *W, int nmom,
+                                     double *mom, unsigned int *err, int num_sms, cudaStream_t stream) {
+    if (!moments_tma_ffma2_supported(M, nq) || nmom < 1 || nmom > 16) return cudaErrorInvalidValue;
+    if (reinterpret_cast<uintptr_t>(psi) % 16) return cudaErrorInvalidValue;
+    EncodeTiled enc = encode_fn();
+    if (!enc) return cudaErrorNotSupported;
+    // psi as a 2-D tensor: x = row (M, contiguous), y = ordinate (nq, stride 4 M bytes)
+    CUtensorMap map;
+    const cuuint64_t dims[2] = {M, nq};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(M) * 4};
+    const cuuint32_t box[2] = {kFfRows, kFfK};
+    const cuuint32_t estr[2] = {1, 1};
+    if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(psi), dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return cudaErrorInvalidValue;
+    const uint32_t stages = ff_stages_for(nq);
+    const size_t smem = ff_smem_bytes(nq, stages);
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(k_moments_tma_ffma2, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             static_cast<int>(kSmemLimit));
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    const uint32_t tiles = (M + kFfRows - 1) / kFfRows;
+    const int grid = static_cast<int>(tiles < static_cast<uint32_t>(num_sms) ? tiles : num_sms);
+    const uint32_t nqp = (nq + kFfK - 1) / kFfK * kFfK;
+    k_moments_tma_ffma2<<<grid, kFfThreads, smem, stream>>>(map, M, nq, nqp, W, nmom, mom, err, stages);
     return cudaGetLastError();
 }
 

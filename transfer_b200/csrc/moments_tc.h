@@ -1,5 +1,5 @@
-// Moments of FP32 psi on the tcgen05 tensor cores with TMA-staged tiles
-// (moments_tc.cu).
+// Moments of FP32 psi with TMA-staged tiles (moments_tc.cu): on the tcgen05
+// tensor cores, or on paired FP32 FMAs.
 #pragma once
 #include <cuda_runtime.h>
 
@@ -18,5 +18,10 @@ bool moments_tcgen05_supported(uint32_t M, uint32_t nq);
 // a pipeline wait of the kernel gave up (the caller clears it before).
 cudaError_t launch_moments_tcgen05(const float *psi, uint32_t M, uint32_t nq, const double *W, int nmom,
                                    double *mom, unsigned int *err, int num_sms, cudaStream_t stream);
+// The same product on paired FP32 FMAs (FFMA2), psi still loaded by TMA; the
+// same arguments and error word.
+bool moments_tma_ffma2_supported(uint32_t M, uint32_t nq);
+cudaError_t launch_moments_tma_ffma2(const float *psi, uint32_t M, uint32_t nq, const double *W, int nmom,
+                                     double *mom, unsigned int *err, int num_sms, cudaStream_t stream);
 
 }  // namespace transfer

@@ -82,11 +82,20 @@ struct FinAlpha {  // CG step length alpha = (r,z) / (p, A p)
     __device__ void operator()(double pAp) const { s->alpha = s->nrz / pAp; }
 };
 
-// neighbour rows gathered at once per lane (loads in flight)
+// neighbour rows gathered at once per lane (loads in flight).  With one
+// harmonic per lane the persistent CG kernels (one block of 24 warps per SM,
+// which wait at grid barriers between iterations) gain from 8 rows in flight
+// (the mixed solve on milne_slab_ref 2% faster), the operator launched alone
+// (3 blocks of 8 warps per SM) from 4 (6% faster alone).
 #ifndef TR_GATHER_BATCH1
 #define TR_GATHER_BATCH1 4
 #endif
-__host__ __device__ constexpr int batch_of(int H) { return H == 1 ? TR_GATHER_BATCH1 : H == 2 ? 4 : 2; }
+#ifndef TR_GATHER_BATCH1_PERSISTENT
+#define TR_GATHER_BATCH1_PERSISTENT 8
+#endif
+__host__ __device__ constexpr int batch_of(int H, bool persistent = false) {
+    return H == 1 ? (persistent ? TR_GATHER_BATCH1_PERSISTENT : TR_GATHER_BATCH1) : H == 2 ? 4 : 2;
+}
 
 __host__ __device__ inline size_t align16(size_t b) { return (b + 15) & ~size_t(15); }
 
@@ -347,6 +356,7 @@ __device__ __forceinline__ void stage_edges_async(const OpData<T> &d, uint32_t b
 // plain operator input (x_u = f[u]) or CG's fused direction (z[u] + beta p_old[u])
 template <int G, int H, typename T, bool FUSEP, bool COH>
 struct SrcDir {
+    static constexpr bool kPersistent = COH;  // the persistent kernels read rows written in the same launch
     const T *f, *pold;
     T beta;
     uint32_t aslm, slm;
@@ -413,6 +423,7 @@ __device__ __forceinline__ T sr_u(T r, T w, T s, T dv, T alpha, T beta, T &s1, T
 }
 template <int G, int H, typename T, bool JAC>
 struct SrcSr {
+    static constexpr bool kPersistent = true;
     SrStep<T> st;
     uint32_t aslm, slm;
     __device__ __forceinline__ void row(uint32_t u, int lane, T (&x)[H]) const {
@@ -485,7 +496,7 @@ template <int G, int H, typename T, class Src, class Out>
 __device__ __forceinline__ void simt_vertices(const OpData<T> &d, const Staged<T> &tab, unsigned char *smem_groups,
                                               const Src &src, const Out &fin, double (&dacc)[Out::NV]) {
     constexpr int SA = G * H + 1;  // padded row of the shared S / B tables
-    constexpr int NB = batch_of(H);
+    constexpr int NB = batch_of(H, Src::kPersistent);
     constexpr int LS = G * H < 32 ? 32 : G * H;  // lane stride of O (== d.cls, checked at launch)
     const uint32_t slm = d.slm, aslm = d.aslm;
     T *slab = reinterpret_cast<T *>(smem_groups) + (threadIdx.x / G) * group_smem_elems<G, H, T>();

@@ -2854,19 +2854,22 @@ tr_status tr_sweep_moments(tr_sweep *s, int nmom, double *mom) {
     if (!s->last_prec) return sw_err(s, TR_ERR_INVALID_ARG, "tr_sweep_moments: no sweep has run");
     cudaError_t e = cudaSuccess;
     const uint32_t nqp8 = (s->nq + 7) / 8 * 8;
-    if (s->last_prec == 32 && s->mom_kernel == TR_MOMENTS_TCGEN05 &&
-        transfer::moments_tcgen05_supported(4 * s->nT, s->nq)) {
+    const bool tc = s->mom_kernel == TR_MOMENTS_TCGEN05 && transfer::moments_tcgen05_supported(4 * s->nT, s->nq);
+    const bool ff = s->mom_kernel == TR_MOMENTS_TMA_FFMA2 && transfer::moments_tma_ffma2_supported(4 * s->nT, s->nq);
+    if (s->last_prec == 32 && (tc || ff)) {
         if (!s->mom_err) e = sw_alloc(s, &s->mom_err, 1);
         if (e == cudaSuccess) e = cudaMemsetAsync(s->mom_err, 0, sizeof(unsigned int), s->stream);
         if (e == cudaSuccess)
-            e = transfer::launch_moments_tcgen05(s->psi32, 4 * s->nT, s->nq, s->Wm, nmom, mom, s->mom_err, s->num_sms,
-                                                 s->stream);
+            e = tc ? transfer::launch_moments_tcgen05(s->psi32, 4 * s->nT, s->nq, s->Wm, nmom, mom, s->mom_err,
+                                                      s->num_sms, s->stream)
+                   : transfer::launch_moments_tma_ffma2(s->psi32, 4 * s->nT, s->nq, s->Wm, nmom, mom, s->mom_err,
+                                                        s->num_sms, s->stream);
         ++s->launches;
         unsigned int flag = 0;
         if (e == cudaSuccess) e = cudaMemcpyAsync(&flag, s->mom_err, sizeof(flag), cudaMemcpyDeviceToHost, s->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
         if (e == cudaSuccess && flag)
-            return sw_err(s, TR_ERR_CUDA, "tr_sweep_moments: a pipeline wait of the tensor-core kernel timed out");
+            return sw_err(s, TR_ERR_CUDA, "tr_sweep_moments: a pipeline wait of the TMA-fed kernel timed out");
     } else if (s->last_prec == 32 && 2ull * 16 * nqp8 * sizeof(uint32_t) <= 48 * 1024) {  // nq <= 384
         const uint32_t M = 4 * s->nT, nqp = nqp8;
         const size_t smem = moments_smem(nqp);
@@ -2921,7 +2924,7 @@ tr_status tr_sweep_moments(tr_sweep *s, int nmom, double *mom) {
 
 tr_status tr_sweep_set_moments_kernel(tr_sweep *s, int kind) {
     SW_CHECK(s);
-    if (kind != TR_MOMENTS_TCGEN05 && kind != TR_MOMENTS_MMA_SYNC)
+    if (kind != TR_MOMENTS_TCGEN05 && kind != TR_MOMENTS_MMA_SYNC && kind != TR_MOMENTS_TMA_FFMA2)
         return sw_err(s, TR_ERR_INVALID_ARG, "tr_sweep_set_moments_kernel: unknown kernel family");
     s->mom_kernel = kind;
     return TR_OK;

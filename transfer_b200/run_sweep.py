@@ -28,7 +28,7 @@ def _main():
     ap.add_argument("--workload", default="milne")
     ap.add_argument("--moments", type=int, default=0)
     ap.add_argument("--autotune", action="store_true")
-    ap.add_argument("--moments-kernel", default="tcgen05", choices=("tcgen05", "mma_sync"))
+    ap.add_argument("--moments-kernel", default="tcgen05", choices=("tcgen05", "mma_sync", "tma_ffma2"))
     args = ap.parse_args()
     if args.workload.startswith("stellar"):
         n = int(args.workload.split(":")[1]) if ":" in args.workload else 96
@@ -36,7 +36,8 @@ def _main():
     else:
         md, ph, ords, desc = W.milne_sweep()
     S = Sweep(0, md, ords, ph, dsa=args.solve == "dsa")
-    S.set_moments_kernel(L.TR_MOMENTS_TCGEN05 if args.moments_kernel == "tcgen05" else L.TR_MOMENTS_MMA_SYNC)
+    S.set_moments_kernel({"tcgen05": L.TR_MOMENTS_TCGEN05, "mma_sync": L.TR_MOMENTS_MMA_SYNC,
+                          "tma_ffma2": L.TR_MOMENTS_TMA_FFMA2}[args.moments_kernel])
     if args.autotune:
         shape, t_full, t_small = S.autotune()
         print(f"autotune: FP32 sweep {t_full:.3f} ms full shape, {t_small:.3f} ms small; keeps "

@@ -104,7 +104,8 @@ class Sweep:
         return out.view(self.nq, self.nT, 4)
 
     def set_moments_kernel(self, kind):
-        """tr_sweep_set_moments_kernel: TR_MOMENTS_TCGEN05 (default) or TR_MOMENTS_MMA_SYNC."""
+        """tr_sweep_set_moments_kernel: TR_MOMENTS_TCGEN05 (default), TR_MOMENTS_MMA_SYNC or
+        TR_MOMENTS_TMA_FFMA2."""
         self._c(lib.tr_sweep_set_moments_kernel(self._h, int(kind)))
 
     def moments(self, nmom=16):
