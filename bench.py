@@ -742,11 +742,13 @@ def run_ours(args, rank, world, local):
     ctx.solve(**fp64, **jac)
     t_mixed_j, _, _, reps_mixed_j, _ = timed({**mixed, **jac}, args.steps)
     t_fp64_j, _, _, reps_fp64_j, _ = timed({**fp64, **jac}, args.steps)
-    # end to end through the C ABI with host buffers (pinned staging inside)
+    # end to end through the C ABI with host buffers: b from and f to
+    # page-locked host memory (which tr_solve_host copies by DMA directly)
     b = ctx.allocVector()
     ctx.computeRhs(b)
-    b_host = b.cpu().numpy()
-    f_host = np.zeros(ctx.N())
+    b_host = torch.empty(ctx.N(), dtype=torch.float64).pin_memory().numpy()
+    b_host[:] = b.cpu().numpy()
+    f_host = torch.zeros(ctx.N(), dtype=torch.float64).pin_memory().numpy()
     ctx.solve_host(b_host, f_host, **mixed)   # allocate the staging buffers once
     t_e2e, u_e2e = 0.0, 0
     for s in range(args.steps):

@@ -277,7 +277,9 @@ void tr_solve_opts_default(tr_solve_opts *opts);   /* reference settings */
  * f: device vector (output). */
 tr_status tr_solve(tr_ctx *ctx, const tr_solve_opts *opts, const double *b,
                    double *f, tr_solve_report *report);
-/* Same with HOST buffers: copies b in (pinned staging) and f out. */
+/* Same with HOST buffers: copies b in and f out.  Page-locked buffers
+ * (cudaMallocHost, cudaHostRegister, torch pin_memory) are copied by DMA
+ * directly; pageable ones through the context's pinned staging buffers. */
 tr_status tr_solve_host(tr_ctx *ctx, const tr_solve_opts *opts,
                         const double *b_host, double *f_host,
                         tr_solve_report *report);

@@ -176,6 +176,16 @@ def test_host_buffers_and_explicit_rhs(cuda):
     f0, r0 = ctx.solve(tol=1e-10, relative=1)
     assert r1.iterations == rh.iterations == r0.iterations
     assert np.array_equal(host(f1), fh) and torch.equal(f0, f1)
+    # page-locked caller buffers are copied by DMA directly: same solution;
+    # then a pageable b with a page-locked f (staging in, direct out)
+    bp = torch.empty(ctx.N(), dtype=torch.float64).pin_memory().numpy()
+    bp[:] = host(b)
+    fp = torch.full((ctx.N(),), -1.0, dtype=torch.float64).pin_memory().numpy()
+    fp, rp = ctx.solve_host(b_host=bp, f_host=fp, tol=1e-10, relative=1)
+    assert rp.iterations == rh.iterations and np.array_equal(fp, fh)
+    fp[:] = -1.0
+    fq, rq = ctx.solve_host(b_host=host(b).copy(), f_host=fp, tol=1e-10, relative=1)
+    assert rq.iterations == rh.iterations and np.array_equal(fq, fh)
 
 
 def test_iteration_limit_and_zero_rhs(cuda):

@@ -275,6 +275,17 @@ tr_status tr_solve(tr_ctx *c, const tr_solve_opts *o, const double *b, double *f
     return s;
 }
 
+// true when p is page-locked host memory (cudaMallocHost or registered),
+// which copies can reach by DMA without staging
+static bool page_locked(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
 tr_status tr_solve_host(tr_ctx *c, const tr_solve_opts *o, const double *b_host, double *f_host,
                         tr_solve_report *rep) {
     CHECK_CTX(c);
@@ -282,7 +293,10 @@ tr_status tr_solve_host(tr_ctx *c, const tr_solve_opts *o, const double *b_host,
     tr_status s = check_opts(c, o);
     if (s != TR_OK) return s;
     const size_t bytes = sizeof(double) * c->nP * c->aslm;
-    if (c->stage_bytes < bytes) {
+    // page-locked caller buffers are copied directly; pageable ones go
+    // through the context's pinned staging buffers
+    const bool b_locked = b_host && page_locked(b_host), f_locked = page_locked(f_host);
+    if ((!b_locked || !f_locked) && c->stage_bytes < bytes) {
         if (c->stage_in) cudaFreeHost(c->stage_in);
         if (c->stage_out) cudaFreeHost(c->stage_out);
         c->stage_in = c->stage_out = nullptr;
@@ -298,9 +312,13 @@ tr_status tr_solve_host(tr_ctx *c, const tr_solve_opts *o, const double *b_host,
     // device buffers for b and f owned by the context
     double *db = nullptr;
     if (b_host) {
-        std::memcpy(c->stage_in, b_host, bytes);
+        const void *src = b_host;
+        if (!b_locked) {
+            std::memcpy(c->stage_in, b_host, bytes);
+            src = c->stage_in;
+        }
         db = c->io[0];
-        s = check_cuda(c, cudaMemcpyAsync(db, c->stage_in, bytes, cudaMemcpyHostToDevice, st), "H2D b");
+        s = check_cuda(c, cudaMemcpyAsync(db, src, bytes, cudaMemcpyHostToDevice, st), "H2D b");
         if (s != TR_OK) return s;
     }
     double *df = c->io[1];
@@ -308,10 +326,11 @@ tr_status tr_solve_host(tr_ctx *c, const tr_solve_opts *o, const double *b_host,
     if (!rep) rep = &local;
     tr_status ss = solve(c, o, db, df, rep);
     if (ss != TR_OK && ss != TR_ERR_NOT_CONVERGED) return ss;
-    s = check_cuda(c, cudaMemcpyAsync(c->stage_out, df, bytes, cudaMemcpyDeviceToHost, st), "D2H f");
+    s = check_cuda(c, cudaMemcpyAsync(f_locked ? f_host : c->stage_out, df, bytes, cudaMemcpyDeviceToHost, st),
+                   "D2H f");
     if (s == TR_OK) s = check_cuda(c, cudaStreamSynchronize(st), "D2H f");
     if (s != TR_OK) return s;
-    std::memcpy(f_host, c->stage_out, bytes);
+    if (!f_locked) std::memcpy(f_host, c->stage_out, bytes);
     return ss;
 }
 
