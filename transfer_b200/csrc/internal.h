@@ -169,7 +169,13 @@ struct CachedGraph {
     bool valid = false;
 };
 constexpr int kCgChunk = 16;       // CG iterations per captured graph / status read (even)
-constexpr int kPersistChunk = 64;  // CG iterations per persistent-kernel launch
+// CG iterations per persistent-kernel launch: the host reads the status
+// (iterations, stop flag) between launches, one launch, copy and stream
+// synchronisation each
+#ifndef TR_PERSIST_CHUNK
+#define TR_PERSIST_CHUNK 1024
+#endif
+constexpr int kPersistChunk = TR_PERSIST_CHUNK;
 
 template <typename T>
 struct DeviceOp {
