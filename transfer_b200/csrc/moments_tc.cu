@@ -37,9 +37,12 @@
 //             the steps over four accumulators and summing them in FP64 cuts
 //             that bias fourfold (80 accumulations into one sum at 308
 //             ordinates left moments 5e-6 low).
-//   warp 0    TMA producer (and tensor-memory allocation);
+//   warp 0    TMA producer (and tensor-memory allocation), with warp 3 a
+//             second producer of alternate stages;
 //   warp 1    MMA issuer: per 8-ordinate step one N = 32 product from shared
-//             memory and one N = 16 product with A from tensor memory;
+//             memory and one N = 16 product with A from tensor memory; with
+//             warp 2 a second issuer of alternate stages (its own a_lo w_hi
+//             sum, accumulators 2 and 3);
 //   warps 4-11 split each stage (a_lo = a - trunc(a)) into tensor memory,
 //             two warpgroups of 16 ordinates each;
 //   warps 12-15 read each finished tile's accumulators back (tcgen05.ld), sum
@@ -69,12 +72,18 @@ constexpr int kMaxStages = 10;     // shared-memory stages (the launch picks how
 #define TR_MOM_LO_SLOTS 4
 #endif
 constexpr uint32_t kLoSlots = TR_MOM_LO_SLOTS;
+static_assert(kLoSlots % 2 == 0, "two issuers take alternate a_lo slots");
 constexpr int kAtomBytes = 32 * 4 * kStageK;         // 32 rows x 32 ordinates x 4 B = 4 KB
 constexpr int kStageBytes = 4 * kAtomBytes;          // 16 KB
 constexpr uint32_t kSplitWarps = 8;                  // warps 4-11; warps 12-15 drain the accumulators
 constexpr int kThreads = 32 * (4 + kSplitWarps + 4);
 constexpr uint32_t kAccGroups = 4;                   // accumulators of a [w_hi | w_lo] per tile
-constexpr uint32_t kBufCols = 160;                   // kAccGroups x 32 + 16 (a_lo w_hi) + 16 spare
+constexpr uint32_t kBufCols = 160;                   // kAccGroups x 32 + 2 x 16 (a_lo w_hi, one per issuer)
+// MMA-issuing (and TMA-producing) threads: 1, or 2 taking alternate stages
+// where a tile has at least two stages (more than 32 ordinates)
+#ifndef TR_MOM_ISSUERS
+#define TR_MOM_ISSUERS 2
+#endif
 constexpr uint32_t kTmemCols = 512;                  // 2 tile buffers + kLoSlots x 32 a_lo
 constexpr uint32_t kLoCol0 = 2 * kBufCols;
 constexpr unsigned long long kWaitNs = 1000000000ull;  // 1 s per wait
@@ -220,7 +229,7 @@ struct Smem {
 __global__ void __launch_bounds__(kThreads, 1)
     k_moments_tcgen05(const __grid_constant__ CUtensorMap psi_map, uint32_t M, uint32_t nq, uint32_t nqp,
                       const double *__restrict__ W, int nmom, double *__restrict__ mom, unsigned int *err,
-                      uint32_t nstages) {
+                      uint32_t nstages, uint32_t issuers) {
     extern __shared__ uint8_t smem_raw[];
     // 1024-byte aligned base (the swizzle pattern repeats every 512 B)
     uint8_t *base = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -252,10 +261,10 @@ __global__ void __launch_bounds__(kThreads, 1)
             mbar_init(smem_u32(&sh.lo_empty[l]), 1);
         }
         for (int b = 0; b < 2; ++b) {
-            mbar_init(smem_u32(&sh.acc_full[b]), 1);
+            mbar_init(smem_u32(&sh.acc_full[b]), issuers);
             mbar_init(smem_u32(&sh.acc_empty[b]), 4);
         }
-        mbar_init(smem_u32(&sh.drain), 1);
+        mbar_init(smem_u32(&sh.drain), issuers);
         sh.abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -274,12 +283,17 @@ __global__ void __launch_bounds__(kThreads, 1)
     tc_fence_after();
     const uint32_t tmem = sh.tmem_base;
 
-    if (warp == 0 && lane == 0) {
-        // ---- TMA producer
+    if ((warp == 0 || (warp == 3 && issuers == 2)) && lane == 0) {
+        // ---- TMA producer(s).  With two, producer i (warps 0 and 3) fills
+        // the stages it = i mod 2 (with the two MMA issuers, 4.39 -> 3.21 ms
+        // on the 2.78 M-tet sphere with 302 ordinates; issuing each stage's
+        // four copies from four lanes changed nothing).
+        const uint32_t me = warp == 0 ? 0u : 1u;
         uint32_t it = 0, inflight = 0;
         bool ok = true;
         for (uint32_t tile = blockIdx.x; ok && tile < tiles; tile += gridDim.x)
             for (uint32_t ks = 0; ks < nks; ++ks, ++it) {
+                if (issuers == 2 && (it & 1u) != me) continue;
                 const uint32_t s = it % nstages, ph = (it / nstages) & 1u;
                 if (!(ok = mbar_wait(smem_u32(&sh.empty[s]), ph ^ 1u, abort_flag, err))) break;
                 const uint32_t fb = smem_u32(&sh.full[s]);
@@ -291,16 +305,23 @@ __global__ void __launch_bounds__(kThreads, 1)
                                 static_cast<int>(ks * kStageK), fb);
                 inflight = it + 1;
             }
-        if (!ok) {  // aborted: wait (bounded, own timer) for the copies already issued
+        if (!ok) {  // aborted: wait (bounded, own timer) for the copies this thread issued
             for (uint32_t j = inflight > nstages ? inflight - nstages : 0; j < inflight; ++j) {
+                if (issuers == 2 && (j & 1u) != me) continue;
                 const uint32_t bar = smem_u32(&sh.full[j % nstages]), ph = (j / nstages) & 1u;
                 const unsigned long long t0 = global_ns();
                 while (!mbar_try(bar, ph) && global_ns() - t0 < kWaitNs) {
                 }
             }
         }
-    } else if (warp == 1 && lane == 0) {
-        // ---- MMA issuer
+    } else if ((warp == 1 || (warp == 2 && issuers == 2)) && lane == 0) {
+        // ---- MMA issuer(s).  With two issuers, issuer i takes the stages
+        // it = i mod 2 (nstages and kLoSlots are even then, so every barrier
+        // phase an issuer waits for follows one it consumed itself) into
+        // accumulators 2i and 2i + 1 and its own a_lo w_hi sum (columns
+        // 128 + 16 i); one thread issuing the stage's eight MMAs and two
+        // commits took ~1,300 cycles a stage and bound the kernel.
+        const uint32_t me = warp - 1;
         constexpr uint32_t id_hi = idesc_tf32(32, 1), id_lo = idesc_tf32(16, 0);
         uint32_t it = 0, tcount = 0;
         bool ok = true;
@@ -309,7 +330,9 @@ __global__ void __launch_bounds__(kThreads, 1)
             if (!(ok = mbar_wait(smem_u32(&sh.acc_empty[b]), bph ^ 1u, abort_flag, err))) break;
             tc_fence_after();
             const uint32_t d = tmem + kBufCols * b;
+            bool started = false;  // this issuer's accumulators of the tile hold a sum
             for (uint32_t ks = 0; ks < nks; ++ks, ++it) {
+                if (issuers == 2 && (it & 1u) != me) continue;
                 const uint32_t s = it % nstages, ph = (it / nstages) & 1u;
                 const uint32_t l = it % kLoSlots, lph = (it / kLoSlots) & 1u;
                 if (!(ok = mbar_wait(smem_u32(&sh.full[s]), ph, abort_flag, err))) break;
@@ -317,14 +340,19 @@ __global__ void __launch_bounds__(kThreads, 1)
                 tc_fence_after();
                 const uint32_t a0 = smem_u32(smA + s * kStageBytes);
                 const uint32_t b0 = smem_u32(smB) + ks * 4u * 1024u;
+                const uint32_t dlo = d + 32u * kAccGroups + 16u * me;
 #pragma unroll
                 for (uint32_t kk = 0; kk < 4; ++kk) {
-                    // 8-ordinate step kk of this stage goes to accumulator kk
-                    // (4 steps a stage); each starts from zero in the first stage
+                    // one issuer: 8-ordinate step kk goes to accumulator kk;
+                    // two: steps 0-1 to accumulator 2 me, 2-3 to 2 me + 1.
+                    // Each starts from zero with the issuer's first stage.
                     const uint64_t bd = desc_b(b0 + kk * 1024u);
-                    mma_ss(d + 32u * kk, desc_a(a0 + kk * 1024u), bd, id_hi, ks != 0u);
-                    mma_ts(d + 32u * kAccGroups, tmem + kLoCol0 + kStageK * l + 8u * kk, bd, id_lo, (ks | kk) != 0u);
+                    const uint32_t g = issuers == 2 ? 2u * me + (kk >> 1) : kk;
+                    const bool acc_hi = started || (issuers == 2 && (kk & 1u));
+                    mma_ss(d + 32u * g, desc_a(a0 + kk * 1024u), bd, id_hi, acc_hi ? 1u : 0u);
+                    mma_ts(dlo, tmem + kLoCol0 + kStageK * l + 8u * kk, bd, id_lo, (started || kk) ? 1u : 0u);
                 }
+                started = true;
                 mma_commit(smem_u32(&sh.empty[s]));     // the stage is free once these finish,
                 mma_commit(smem_u32(&sh.lo_empty[l]));  // and so is its a_lo slot
             }
@@ -388,7 +416,8 @@ __global__ void __launch_bounds__(kThreads, 1)
 #pragma unroll
                 for (int n = 0; n < 16; ++n)
                     acc[n] += static_cast<double>(__uint_as_float(v[n])) +
-                              (g < kAccGroups ? static_cast<double>(__uint_as_float(v[16 + n])) : 0.0);
+                              ((g < kAccGroups || issuers == 2) ? static_cast<double>(__uint_as_float(v[16 + n]))
+                                                                : 0.0);
             }
             tc_fence_before();
             __syncwarp();
@@ -479,7 +508,10 @@ cudaError_t launch_moments_tcgen05(const float *psi, uint32_t M, uint32_t nq, co
     const uint32_t tiles = (M + kTileM - 1) / kTileM;
     const int grid = static_cast<int>(tiles < static_cast<uint32_t>(num_sms) ? tiles : num_sms);
     const uint32_t nqp = (nq + kStageK - 1) / kStageK * kStageK;
-    k_moments_tcgen05<<<grid, kThreads, smem, stream>>>(map, M, nq, nqp, W, nmom, mom, err, stages_for(nq));
+    const uint32_t issuers = (TR_MOM_ISSUERS == 2 && nqp >= 2 * kStageK) ? 2u : 1u;
+    uint32_t stages = stages_for(nq);
+    if (issuers == 2) stages &= ~1u;  // even: a stage's barrier phases then alternate with one issuer
+    k_moments_tcgen05<<<grid, kThreads, smem, stream>>>(map, M, nq, nqp, W, nmom, mom, err, stages, issuers);
     return cudaGetLastError();
 }
 
