@@ -323,6 +323,30 @@ def test_batched_source_iteration_matches_separate_solves(cuda):
         assert rel_err(host(J), host(Jr)) < tol
 
 
+def test_batched_source_iteration_in_every_launch_form(cuda):
+    """Each launch form of the batched source iteration, set on the first
+    sweep only, with the smallest problem first: the graph replays the form
+    (and the work-queue ticket) of the first sweep the caller passed, not of
+    the largest problem still running."""
+    cases = [(absorbing_slab(nx=20), op.ordinates_product(2, 6)), (scattering_box(), op.ordinates_product(4, 8)),
+             (scattering_box(n=(8, 8, 8)), op.ordinates_product(4, 8))]
+    sweeps = [tr.Sweep(0, md, ords, ph) for (md, ph), ords in cases]
+    assert sweeps[0].nT < max(S.nT for S in sweeps)
+    SI = tr._lib.TR_SWEEP_SOURCE_ITERATION
+    ref = [S.solve(method=SI, tol=1e-12, max_iter=3000) for S in sweeps]
+    L_ = tr._lib
+    for precision, forms in ((64, [L_.TR_BATCH_STATIC_FULL, L_.TR_BATCH_QUEUE_FULL]),
+                             (32, [L_.TR_BATCH_STATIC_FULL, L_.TR_BATCH_QUEUE_FULL, L_.TR_BATCH_STATIC_SMALL,
+                                   L_.TR_BATCH_QUEUE_SMALL])):
+        for f in forms:
+            sweeps[0].set_batch_form(f)
+            tol = 1e-12 if precision == 64 else 1e-6
+            out, its, res = tr.sweep_solve_batch(sweeps, precision, tol=tol, max_iter=3000)
+            assert (its > 0).all(), (precision, f)
+            for (J, _), (Jr, _, _) in zip(out, ref):
+                assert rel_err(host(J), host(Jr)) < (1e-10 if precision == 64 else 1e-4), (precision, f)
+
+
 def test_autotune_keeps_results(cuda):
     """Both shapes are timed, the faster kept; FP32 sweeps are bitwise the
     same before and after."""

@@ -384,11 +384,19 @@ struct Slots {
 // small.
 template <typename T>
 constexpr size_t slots_bytes() { return static_cast<size_t>(Slots<T>::kUnits) * kSlots * 16; }
+// Task records are fetched one chunk earlier than the rest of a slot: while
+// chunk i is computed, the records of chunk i + 2 are copied (cp.async) into
+// a ring of three chunks' positions, and the slots of chunk i + 1 are filled
+// from records already in shared memory.  Each chunk's staging is then one
+// global-memory round trip (record-dependent loads only), not two (record,
+// then what it names).
+constexpr uint32_t kRecSlots = 3 * kSweepThreads;
+constexpr size_t recs_bytes = static_cast<size_t>(kRecSlots) * 16;
 template <typename T, bool SMALL>
 struct SweepShape {
     static constexpr int ring_bytes = SMALL ? 16 * 1024 : (sizeof(T) == 4 ? 64 * 1024 : 32 * 1024);
     static constexpr uint32_t level_cap = SMALL ? 1024 : 4096;
-    static constexpr size_t smem = ring_bytes + slots_bytes<T>() + 4ull * (level_cap + 1);
+    static constexpr size_t smem = ring_bytes + slots_bytes<T>() + recs_bytes + 4ull * (level_cap + 1);
 };
 
 __device__ __forceinline__ void cp_async16(void *dst, const void *src) {
@@ -411,12 +419,12 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 // runs gets the upwind cell's psi staged too, from global psi (OLD: the
 // shapes whose ring is short enough for that to happen often).
 template <typename T, bool OLD>
-__device__ __forceinline__ void stage_task(const Slots<T> &S, uint32_t p, const uint4 *task, const Geom<T> &g,
+__device__ __forceinline__ void stage_task(const Slots<T> &S, uint32_t p, const uint4 *recs, const Geom<T> &g,
                                            const SweepArgs<T> &a, uint32_t done_end, uint32_t e_next, uint32_t R,
                                            const T *psi) {
     using Sl = Slots<T>;
     const uint32_t sl = p % kSlots;
-    const uint4 rec = __ldg(task + p);
+    const uint4 rec = recs[p % kRecSlots];
     *reinterpret_cast<uint4 *>(S.unit(sl, Sl::kRec)) = rec;
     const uint32_t c = rec.x & kCellMask, mask = rec.x >> 28;
 #pragma unroll
@@ -485,12 +493,20 @@ __device__ __forceinline__ bool next_chunk(uint32_t &L, uint32_t &c0, const uint
 // by half a block, while positions below done_end are complete
 template <typename T, bool OLD>
 __device__ __forceinline__ void stage_chunk(const Slots<T> &S, uint32_t L, uint32_t c0, const uint32_t *lvl,
-                                            const uint4 *task, const Geom<T> &g, const SweepArgs<T> &a,
+                                            const uint4 *recs, const Geom<T> &g, const SweepArgs<T> &a,
                                             uint32_t done_end, uint32_t R, const T *psi) {
     const uint32_t e = min(c0 + kSweepThreads, lvl[L + 1]);
     const uint32_t p = c0 + ((threadIdx.x + kSweepThreads / 2) % kSweepThreads);
-    if (p < e) stage_task<T, OLD>(S, p, task, g, a, done_end, e, R, psi);
-    cp_async_commit();
+    if (p < e) stage_task<T, OLD>(S, p, recs, g, a, done_end, e, R, psi);
+}
+
+// copies the task records of the chunk [c0, min(c0 + 256, end of level L))
+// into the record ring (not committed: the caller's commit covers them)
+__device__ __forceinline__ void fetch_records(uint4 *recs, uint32_t L, uint32_t c0, const uint32_t *lvl,
+                                              const uint4 *task) {
+    const uint32_t e = min(c0 + kSweepThreads, lvl[L + 1]);
+    const uint32_t p = c0 + ((threadIdx.x + kSweepThreads / 2) % kSweepThreads);
+    if (p < e) cp_async16(recs + p % kRecSlots, task + p);
 }
 
 // upwind trace of one inflow face from its source code
@@ -576,7 +592,7 @@ __device__ __forceinline__ void sweep_block(const Geom<T> &g, const Sched &sc, c
     const uint32_t nl = sc.nlev[q];
     const uint32_t *lvl = sc.lvl + (size_t)q * sc.lstride;
     if (nl <= Shape::level_cap) {
-        uint32_t *lv = reinterpret_cast<uint32_t *>(smem_raw + Shape::ring_bytes + slots_bytes<T>());
+        uint32_t *lv = reinterpret_cast<uint32_t *>(smem_raw + Shape::ring_bytes + slots_bytes<T>() + recs_bytes);
         for (uint32_t L = threadIdx.x; L <= nl; L += blockDim.x) lv[L] = __ldg(lvl + L);
         __syncthreads();
         lvl = lv;
@@ -585,16 +601,31 @@ __device__ __forceinline__ void sweep_block(const Geom<T> &g, const Sched &sc, c
     T *psi = a.psi + (size_t)q * nT * 4;
     const T c12 = T(1) / T(12), c20 = T(1) / T(20);
 
+    uint4 *recs = reinterpret_cast<uint4 *>(smem_raw + Shape::ring_bytes + slots_bytes<T>());
     uint32_t L = 0, c0 = lvl[0];
     uint32_t prev_c0 = 0;  // positions below it were complete when this chunk was staged
-    stage_chunk<T, kOld>(SL, L, c0, lvl, task, g, a, prev_c0, R, psi);
-    cp_async_wait<0>();
-    __syncthreads();
+    {  // records of the first two chunks, then the first chunk's slots
+        fetch_records(recs, L, c0, lvl, task);
+        uint32_t L1 = L, c1 = c0;
+        if (next_chunk(L1, c1, lvl, nl)) fetch_records(recs, L1, c1, lvl, task);
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncthreads();
+        stage_chunk<T, kOld>(SL, L, c0, lvl, recs, g, a, prev_c0, R, psi);
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncthreads();
+    }
     for (;;) {
         const uint32_t e0 = min(c0 + kSweepThreads, lvl[L + 1]);  // this chunk is [c0, e0)
         uint32_t nL = L, nc0 = c0;
         const bool more = next_chunk(nL, nc0, lvl, nl);
-        if (more) stage_chunk<T, kOld>(SL, nL, nc0, lvl, task, g, a, c0, R, psi);
+        if (more) {
+            uint32_t nnL = nL, nnc0 = nc0;
+            if (next_chunk(nnL, nnc0, lvl, nl)) fetch_records(recs, nnL, nnc0, lvl, task);
+            stage_chunk<T, kOld>(SL, nL, nc0, lvl, recs, g, a, c0, R, psi);
+        }
+        cp_async_commit();
         const uint32_t p = c0 + threadIdx.x;
         if (p < e0) {
             const uint32_t sl = p % kSlots;
@@ -2434,10 +2465,13 @@ static cudaError_t batch_sweep(int n, tr_sweep *const *s, cudaStream_t st, const
 // One source iteration of every problem, x <- S(x) with sources, queued on st
 // (captured once into a CUDA graph by tr_sweep_solve_batch): per problem
 // x = S->kx [J | B], the new iterate in S->kt, res[2i] = ||S(x) - x||^2 and
-// res[2i + 1] = ||S(x)||^2.
+// res[2i + 1] = ||S(x)||^2.  s0 is the caller's first sweep, whose launch
+// form and work-queue ticket the batched launch uses: s[0] is the largest
+// problem still running, which need not own a ticket (a queue-form launch
+// once found a null ticket there when the first problem was not the largest).
 template <typename T>
-static void batch_si_step(int n, tr_sweep *const *s, cudaStream_t st, const SweepJob<T> *dj, uint32_t blocks,
-                          double *res) {
+static void batch_si_step(tr_sweep *s0, int n, tr_sweep *const *s, cudaStream_t st, const SweepJob<T> *dj,
+                          uint32_t blocks, double *res) {
     for (int i = 0; i < n; ++i) {
         tr_sweep *S = s[i];
         if constexpr (sizeof(T) == 4) {
@@ -2445,7 +2479,7 @@ static void batch_si_step(int n, tr_sweep *const *s, cudaStream_t st, const Swee
             if (S->nB) k_to_f32<<<grid_for(S, S->nB), 256, 0, st>>>(S->nB, S->kx + S->nJ, S->Bi32);
         }
     }
-    launch_batch<T>(s[0], dj, n, blocks, st);
+    launch_batch<T>(s0, dj, n, blocks, st);  // the caller's first sweep: launch form and queue ticket
     for (int i = 0; i < n; ++i) {
         tr_sweep *S = s[i];
         const uint64_t nx = S->nJ + S->nB;
@@ -2505,7 +2539,7 @@ static cudaError_t batch_si(int n, tr_sweep *const *s, cudaStream_t st, double t
         cudaGraphExec_t exec = nullptr;
         if (e == cudaSuccess) e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
         if (e == cudaSuccess) {
-            batch_si_step<T>(m, sub.data(), st, dj, blocks, res);
+            batch_si_step<T>(s[0], m, sub.data(), st, dj, blocks, res);
             const cudaError_t ec = cudaStreamEndCapture(st, &graph);
             e = cudaGetLastError();
             if (e == cudaSuccess) e = ec;
