@@ -600,7 +600,13 @@ tr_status ctx_create(int device, const tr_mesh_view *m, const tr_angular_view *a
     ok(upload_runs(c, rt64, slm, o64.rt));
     ok(upload_runs(c, rs32, slm, o32.rs));
     ok(upload_runs(c, rt32, slm, o32.rt));
-    ok(upload(c, &o64.coef, coef.data(), coef.size() * 8));
+    // device records in two halves: rows 0-7 of every edge, then rows 8-15
+    std::vector<double> coef_split(coef.size());
+    for (size_t e = 0; e < nnz; ++e)
+        for (int q = 0; q < kCoefStride; ++q)
+            coef_split[(q < kCoefHalf ? e : nnz + e) * kCoefHalf + q % kCoefHalf] = coef[e * kCoefStride + q];
+    o64.nnz = o32.nnz = nnz;
+    ok(upload(c, &o64.coef, coef_split.data(), coef_split.size() * 8));
     // operator copy of O_n, rows lms padded to the lane stride cls
     std::vector<double> Opad(3 * static_cast<size_t>(slm) * cls, 0.0);
     for (int n = 0; n < 3; ++n)
@@ -616,7 +622,7 @@ tr_status ctx_create(int device, const tr_mesh_view *m, const tr_angular_view *a
     o32.col = o64.col;
     o32.bmask = o64.bmask;
     {
-        auto c32 = to_type<float>(coef);
+        auto c32 = to_type<float>(coef_split);
         ok(upload(c, &o32.coef, c32.data(), c32.size() * 4));
         auto O32 = to_type<float>(Opad);
         ok(upload(c, &o32.O, O32.data(), O32.size() * 4));

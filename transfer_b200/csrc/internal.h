@@ -32,7 +32,13 @@ namespace transfer {
 //         omega_ij = omega_ji, so only S_ij + S_ji enters the operator)
 //   6, 7  M, M0 (mass; M0 for l = 0)
 //   8-10  E_x, E_y, E_z (boundary)      11-15 zero
+// In device memory the record is kept in two halves of kCoefHalf values,
+// coef[nnz][8] (rows 0-7, read for every edge) and coef_bnd[nnz][8] (rows
+// 8-15, read only at vertices with boundary faces), so that interior
+// vertices move half the record bytes.  Shared-memory staging keeps the
+// whole 16-value record.
 constexpr int kCoefStride = 16;
+constexpr int kCoefHalf = 8;
 constexpr int kSymRows = 6, kRowM = 6, kRowM0 = 7, kRowE = 8;
 constexpr int kBlock = 256;
 
@@ -84,7 +90,8 @@ struct OpData {
     uint32_t nP, slm, aslm;          // aslm: vector stride of this precision
     const uint32_t *row;             // [nP+1]
     const uint32_t *col;             // [nnz]
-    const T *coef;                   // [nnz][16]
+    const T *coef;                   // [nnz][8]: record rows 0-7
+    const T *coef_bnd;               // [nnz][8]: record rows 8-15 (boundary couplings)
     uint32_t cls;                    // lane stride of O
     Runs<T> rs, rt;                  // contraction runs: SIMT S table, tensor-core C table
     const T *O;                      // [3][slm][cls]: O_n[lms][lm], rows padded to cls
@@ -182,7 +189,8 @@ struct DeviceOp {
     uint32_t *row = nullptr, *col = nullptr;
     uint32_t cls = 0;
     Runs<T> rs, rt;                  // contraction runs (SIMT, tensor core)
-    T *coef = nullptr, *O = nullptr, *ang_diag = nullptr, *O_diag = nullptr;
+    T *coef = nullptr, *O = nullptr, *ang_diag = nullptr, *O_diag = nullptr;  // coef: [2][nnz][8]
+    size_t nnz = 0;
     T *mask = nullptr;
     T *dinv = nullptr;               // Jacobi: 1 / diag(A), [nP][aslm]
     uint8_t *bmask = nullptr;
@@ -196,6 +204,7 @@ struct DeviceOp {
         d.row = row;
         d.col = col;
         d.coef = coef;
+        d.coef_bnd = coef ? coef + nnz * kCoefHalf : nullptr;
         d.cls = cls;
         d.rs = rs;
         d.rt = rt;

@@ -332,17 +332,23 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 // queue the edges [base, base + cnt) of a vertex into one staging buffer:
-// lane l < cnt copies edge base + l (its neighbour index and 16-value record)
+// lane l < cnt copies edge base + l (its neighbour index and record rows
+// 0-7; rows 8-15 only for a vertex with boundary faces, bnd)
 template <typename T>
 __device__ __forceinline__ void stage_edges_async(const OpData<T> &d, uint32_t base, int cnt, int lane, T *scoef,
-                                                  uint32_t *scol) {
+                                                  uint32_t *scol, bool bnd) {
     if (lane < cnt) {
         cp_async4(scol + lane, d.col + base + lane);
-        const T *src = d.coef + static_cast<size_t>(base + lane) * kCoefStride;
+        constexpr int kChunks = kCoefHalf * static_cast<int>(sizeof(T)) / 16, kPer = 16 / sizeof(T);
+        const T *src = d.coef + static_cast<size_t>(base + lane) * kCoefHalf;
         T *dst = scoef + lane * kCoefStride;
 #pragma unroll
-        for (int q = 0; q < kCoefStride * static_cast<int>(sizeof(T)) / 16; ++q)
-            cp_async16(dst + q * (16 / sizeof(T)), src + q * (16 / sizeof(T)));
+        for (int q = 0; q < kChunks; ++q) cp_async16(dst + q * kPer, src + q * kPer);
+        if (bnd) {
+            const T *srcb = d.coef_bnd + static_cast<size_t>(base + lane) * kCoefHalf;
+#pragma unroll
+            for (int q = 0; q < kChunks; ++q) cp_async16(dst + kCoefHalf + q * kPer, srcb + q * kPer);
+        }
     }
     cp_async_commit();
 }
@@ -527,7 +533,7 @@ __device__ __forceinline__ void simt_vertices(const OpData<T> &d, const Staged<T
         e0 = __ldg(d.row + v);
         e1 = __ldg(d.row + v + 1);
         axes = __ldg(d.bmask + v);
-        stage_edges_async<T>(d, e0, min(static_cast<int>(e1 - e0), G), lane, slab, scolbuf);
+        stage_edges_async<T>(d, e0, min(static_cast<int>(e1 - e0), G), lane, slab, scolbuf, axes != 0);
     }
     while (v < vb1) {
         uint32_t vn = 0;
@@ -552,7 +558,7 @@ __device__ __forceinline__ void simt_vertices(const OpData<T> &d, const Staged<T
             const int cnt = min(static_cast<int>(e1 - base), G);
             if (base != e0) {  // further chunks of a vertex with more than G edges
                 tile.sync();
-                stage_edges_async<T>(d, base, cnt, lane, scoef, scol);
+                stage_edges_async<T>(d, base, cnt, lane, scoef, scol, axes != 0);
             }
             cp_async_wait_all();
             tile.sync();
@@ -587,7 +593,7 @@ __device__ __forceinline__ void simt_vertices(const OpData<T> &d, const Staged<T
         cur ^= 1;
         if (vn < vb1)
             stage_edges_async<T>(d, e0n, min(static_cast<int>(e1n - e0n), G), lane, slab + cur * G * kCoefStride,
-                                 scolbuf + cur * G);
+                                 scolbuf + cur * G, axesn != 0);
         e0 = e0n;
         e1 = e1n;
         const uint32_t axes_v = axes;
@@ -758,12 +764,12 @@ __device__ __forceinline__ double lhs_vertices_tc(const OpData<T> &d, const Stag
                 const uint32_t ea = base + t, eb = base + t + 4;
                 va = ea < e1;
                 vb = eb < e1;
-                const float *ca = d.coef + static_cast<size_t>(va ? ea : e0) * kCoefStride;
-                const float *cb = d.coef + static_cast<size_t>(vb ? eb : e0) * kCoefStride;
-                a[0] = va ? __ldg(ca + g) : 0.0f;
-                a[1] = va ? __ldg(ca + g + 8) : 0.0f;
-                a[2] = vb ? __ldg(cb + g) : 0.0f;
-                a[3] = vb ? __ldg(cb + g + 8) : 0.0f;
+                const size_t oa = static_cast<size_t>(va ? ea : e0) * kCoefHalf;
+                const size_t ob = static_cast<size_t>(vb ? eb : e0) * kCoefHalf;
+                a[0] = va ? __ldg(d.coef + oa + g) : 0.0f;
+                a[1] = (va && axes) ? __ldg(d.coef_bnd + oa + g) : 0.0f;
+                a[2] = vb ? __ldg(d.coef + ob + g) : 0.0f;
+                a[3] = (vb && axes) ? __ldg(d.coef_bnd + ob + g) : 0.0f;
                 ua = va ? __ldg(d.col + ea) : 0u;
                 ub = vb ? __ldg(d.col + eb) : 0u;
             };
@@ -829,9 +835,9 @@ __device__ __forceinline__ double lhs_vertices_tc(const OpData<T> &d, const Stag
                 for (int k = 0; k < KB; ++k) {
                     const uint32_t ea = base + 4 * k + t;
                     va[k] = ea < e1;
-                    const double *ca = d.coef + static_cast<size_t>(va[k] ? ea : e0) * kCoefStride;
-                    alo[k] = va[k] ? __ldg(ca + g) : 0.0;
-                    ahi[k] = (va[k] && axes) ? __ldg(ca + g + 8) : 0.0;
+                    const size_t oa = static_cast<size_t>(va[k] ? ea : e0) * kCoefHalf;
+                    alo[k] = va[k] ? __ldg(d.coef + oa + g) : 0.0;
+                    ahi[k] = (va[k] && axes) ? __ldg(d.coef_bnd + oa + g) : 0.0;
                     ua[k] = va[k] ? __ldg(d.col + ea) : 0u;
                 }
                 double xa[KB][NTH];
@@ -984,9 +990,10 @@ __global__ void __launch_bounds__(kBlock) k_lhs_diag(const OpData<T> d, const T 
 #pragma unroll 2
         for (uint32_t e = __ldg(d.row + v); e < e1; ++e) {
             const uint32_t u = __ldg(d.col + e);
-            const T *c = d.coef + static_cast<size_t>(e) * kCoefStride;
+            const T *c = d.coef + static_cast<size_t>(e) * kCoefHalf;
+            const T *cb = d.coef_bnd + static_cast<size_t>(e) * kCoefHalf;
             const T K0 = __ldg(c), K4 = __ldg(c + 1), K8 = __ldg(c + 2), M = __ldg(c + kRowM), M0 = __ldg(c + kRowM0);
-            const T E0 = __ldg(c + kRowE), E1 = __ldg(c + kRowE + 1), E2 = __ldg(c + kRowE + 2);
+            const T E0 = __ldg(cb), E1 = __ldg(cb + 1), E2 = __ldg(cb + 2);
             T x[H];
             gather_row<G, H, T, false>(f, nullptr, T(0), u, aslm, slm, lane, x);
 #pragma unroll
