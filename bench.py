@@ -224,10 +224,12 @@ def roofline(bytes_, flops, seconds, real_bytes, working_set, peaks, hbm_peak, h
 
 
 # DRAM bytes (read + write) of one launch of the persistent FP32 CG kernel,
-# from one ncu capture of that launch (profiles/k_cg_persistent_simt_f32_milne_slab.md);
-# the iteration working set is L2-resident, so this is first-touch traffic
-# and does not grow with the iterations of the launch
-NCU_TRAFFIC_PER_LAUNCH = {"milne_slab": 16.878336e6 + 0.002304e6, "milne_slab_ref": 16884480 + 65280}
+# from one ncu capture of that launch (profiles/milne_slab_ref_launch_list.md,
+# with the edge records in two halves; milne_slab: the one-record layout,
+# profiles/k_cg_persistent_simt_f32_milne_slab.md); the iteration working set
+# is L2-resident, so this is first-touch traffic and does not grow with the
+# iterations of the launch
+NCU_TRAFFIC_PER_LAUNCH = {"milne_slab": 16.878336e6 + 0.002304e6, "milne_slab_ref": 13250048 + 156160}
 
 
 def operator_policy(tensor, slm, aslm, real):
