@@ -635,8 +635,9 @@ def reference_gpu_section(md, ad, desc, ctx, tr):
 
 def cube64_section(local, flush, peaks, hbm_peak, hbm_kind):
     """The HBM-resident configuration (workloads.cube64: 274,625 vertices,
-    1.57 M tets, maxk 5, slm 66): one mixed and one FP64 solve to the FP64
-    relative residual TOL (Jacobi-preconditioned and plain), the operator
+    1.57 M tets, maxk 5, slm 66): the operator autotuner's timings and
+    choice, one mixed and one FP64 solve to the FP64 relative residual TOL
+    (Jacobi-preconditioned and plain) with the chosen families, the operator
     alone in both precisions, and the roofline of each."""
     import ctypes as C
     import torch
@@ -647,6 +648,12 @@ def cube64_section(local, flush, peaks, hbm_peak, hbm_kind):
     per_app = ctx.nT * ctx.slm
     out = {"config": {**desc, "nP": ctx.nP, "nT": ctx.nT, "slm": ctx.slm, "tol": TOL, "edges": ctx.n_edges},
            "unit": UNIT}
+    # the operator autotuner keeps the kernel family whose persistent CG
+    # iteration is faster, per precision
+    kinds, tms = ctx.autotune_operator(20)
+    fam = {tr.TR_OPERATOR_SIMT: "simt", tr.TR_OPERATOR_TENSOR: "tensor"}
+    out["operator_autotune"] = {"us_per_cg_iteration": {f"fp{p}_{fam[k]}": 1e3 * v for (p, k), v in tms.items()},
+                                "kept": {p: fam[k] for p, k in kinds.items()}}
     for real, dt in ((4, torch.float32), (8, torch.float64)):
         x = ctx.allocVector(dt)
         x.view(ctx.nP, -1)[:, :ctx.slm].normal_()

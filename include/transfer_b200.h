@@ -152,6 +152,17 @@ tr_status tr_ctx_info_get(const tr_ctx *ctx, tr_ctx_info *info);
  * uses TENSOR for FP64 and SIMT for FP32; this call sets both precisions. */
 enum { TR_OPERATOR_SIMT = 0, TR_OPERATOR_TENSOR = 1 };
 tr_status tr_ctx_set_operator(tr_ctx *ctx, int kind);
+/* Operator autotuner (no reference counterpart): for each precision, times
+ * both kernel families as the solver runs them -- `iters` iterations of the
+ * persistent CG on this context's right-hand side (FP64 mode for FP64, the
+ * mixed mode's FP32 CG for FP32), device time of the CG launches per
+ * iteration, the second of two runs -- and keeps the faster for that
+ * precision.  ms receives the milliseconds per CG iteration: {FP64 SIMT,
+ * FP64 tensor, FP32 SIMT, FP32 tensor}.  Allocates the solver work space if
+ * no solve has done so yet. */
+tr_status tr_ctx_autotune_operator(tr_ctx *ctx, int iters, double ms[4]);
+/* The kernel family in use: kinds[0] for FP64, kinds[1] for FP32. */
+tr_status tr_ctx_get_operator(const tr_ctx *ctx, int kinds[2]);
 /* cudaStream_t passed as void*; NULL selects the context's own stream. */
 tr_status tr_ctx_set_stream(tr_ctx *ctx, void *stream);
 const char *tr_last_error(const tr_ctx *ctx);

@@ -262,3 +262,37 @@ def test_uneven_cube_batch_matches_oracle(cuda):
         U, _ = ctx.computeMoments(f)
         Uo, _ = O.moments(fo)
         assert rel_err(host(U), Uo) < 1e-10, n
+
+
+def test_operator_autotuner_keeps_the_faster_family_per_precision(cuda):
+    """tr_ctx_autotune_operator times the SIMT and tensor-core families in
+    each precision on the context's mesh and keeps the faster one per
+    precision; solves with the chosen families give the solutions of the
+    default families."""
+    ctx = tr.CudaContext(0, c1_mesh(), golden_angular(3))
+    f0, r0 = ctx.solve(tol=1e-10, relative=1)
+    m0, q0 = ctx.solve(mode=tr.TR_MODE_MIXED, tol=1e-10, relative=1)
+    assert ctx.operator_kinds() == {"fp64": tr.TR_OPERATOR_TENSOR, "fp32": tr.TR_OPERATOR_SIMT}
+    kinds, ms = ctx.autotune_operator(5)
+    S, T = tr.TR_OPERATOR_SIMT, tr.TR_OPERATOR_TENSOR
+    assert set(ms) == {(64, S), (64, T), (32, S), (32, T)} and all(v > 0 for v in ms.values())
+    assert kinds["fp64"] == (T if ms[(64, T)] < ms[(64, S)] else S)
+    assert kinds["fp32"] == (T if ms[(32, T)] < ms[(32, S)] else S)
+    assert ctx.operator_kinds() == kinds
+    f1, r1 = ctx.solve(tol=1e-10, relative=1)
+    m1, q1 = ctx.solve(mode=tr.TR_MODE_MIXED, tol=1e-10, relative=1)
+    assert r1.converged and q1.converged
+    assert rel_err(host(f1), host(f0)) < 1e-9 and rel_err(host(m1), host(m0)) < 1e-8
+    with pytest.raises(tr.TransferError):
+        ctx.autotune_operator(0)
+
+
+def test_mixed_solve_with_the_tensor_core_fp32_operator(cuda):
+    """The FP32 CG of the mixed mode on the split-TF32 tensor-core operator
+    (the faster FP32 family on large meshes) reaches the FP64 solution."""
+    ctx = tr.CudaContext(0, c1_mesh(), golden_angular(5))
+    f, r = ctx.solve(tol=1e-10, relative=1)
+    ctx.set_operator(tr.TR_OPERATOR_TENSOR)
+    for eng in (tr.TR_ENGINE_PERSISTENT, tr.TR_ENGINE_GRAPH):
+        m, q = ctx.solve(mode=tr.TR_MODE_MIXED, tol=1e-10, relative=1, engine=eng)
+        assert q.converged and rel_err(host(m), host(f)) < 1e-8

@@ -143,6 +143,8 @@ PROTOTYPES = [
     ("tr_ctx_destroy", S, [P]),
     ("tr_ctx_info_get", S, [P, C.POINTER(tr_ctx_info)]),
     ("tr_ctx_set_operator", S, [P, I]),
+    ("tr_ctx_autotune_operator", S, [P, I, P]),
+    ("tr_ctx_get_operator", S, [P, P]),
     ("tr_ctx_set_stream", S, [P, P]),
     ("tr_compute_lhs", S, [P, P, P]),
     ("tr_compute_lhs_diag", S, [P, P, P]),

@@ -459,6 +459,22 @@ class CudaContext:
         """TR_OPERATOR_TENSOR (default) or TR_OPERATOR_SIMT."""
         self._c(lib.tr_ctx_set_operator(self._h, int(kind)))
 
+    def autotune_operator(self, iters=10):
+        """tr_ctx_autotune_operator: times `iters` persistent CG iterations
+        with each operator family in each precision and keeps the faster per
+        precision.  Returns ({"fp64": kind, "fp32": kind},
+        {(precision, kind): ms per CG iteration})."""
+        ms = (C.c_double * 4)()
+        self._c(lib.tr_ctx_autotune_operator(self._h, int(iters), ms))
+        simt, tensor = L.TR_OPERATOR_SIMT, L.TR_OPERATOR_TENSOR
+        return self.operator_kinds(), {(64, simt): ms[0], (64, tensor): ms[1], (32, simt): ms[2], (32, tensor): ms[3]}
+
+    def operator_kinds(self):
+        """tr_ctx_get_operator: {"fp64": kind, "fp32": kind}."""
+        k = (C.c_int * 2)()
+        self._c(lib.tr_ctx_get_operator(self._h, k))
+        return {"fp64": k[0], "fp32": k[1]}
+
     def set_stream(self, stream):
         self._c(lib.tr_ctx_set_stream(self._h, _ptr(stream) if stream is not None else None))
 
