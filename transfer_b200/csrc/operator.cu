@@ -1098,6 +1098,20 @@ __device__ __forceinline__ void sum_partials(const double *partials, double (&to
 // ||r||^2 and (r, z); after a second barrier every block takes the stop
 // test and beta.  The scalars never leave the device; block 0 mirrors them
 // (and the residual history) into CgScalars for the host.
+// Whether the persistent CG forms the direction inside the operator's
+// gather (one grid barrier fewer per iteration, every neighbour row read
+// from two vectors) or in its own vector pass before the operator.  The
+// SIMT family fuses; the tensor-core family takes the separate pass unless
+// built with TR_PERSIST_FUSE_TC=1 (its gathers are what bound it).
+#ifndef TR_PERSIST_FUSE_TC
+#define TR_PERSIST_FUSE_TC 0
+#endif
+#ifndef TR_PERSIST_FUSE_SIMT
+#define TR_PERSIST_FUSE_SIMT 1
+#endif
+template <class Op>
+constexpr bool kPersistFuseP = Op::kTc ? TR_PERSIST_FUSE_TC : TR_PERSIST_FUSE_SIMT;
+
 template <class Op, typename T, bool JAC>
 __global__ void __launch_bounds__(Op::kPersistThreads, 1)
     k_cg_persistent(const OpData<T> d, const PcgArgs<T> a, int stage_flags) {
@@ -1118,9 +1132,27 @@ __global__ void __launch_bounds__(Op::kPersistThreads, 1)
         const int parity = k & 1;
         const T *pold = parity ? a.p1 : a.p0;
         T *pnew = parity ? a.p0 : a.p1;
-        // phase A: p = z + beta p_old, A p, <p, A p>
-        const double dacc = Op::template run<true, true, true>(d, tab, smem_raw + tab.bytes, JAC ? a.z : a.r, pold,
-                                                               pnew, a.Ap, static_cast<T>(beta));
+        double dacc;
+        if constexpr (kPersistFuseP<Op>) {
+            // phase A: p = z + beta p_old inside the operator's gather, A p, <p, A p>
+            dacc = Op::template run<true, true, true>(d, tab, smem_raw + tab.bytes, JAC ? a.z : a.r, pold, pnew,
+                                                      a.Ap, static_cast<T>(beta));
+        } else {
+            // p = z + beta p_old as its own vector pass, then A p, <p, A p>:
+            // the operator gathers each neighbour row once instead of two
+            const T bt = static_cast<T>(beta);
+            const V *zs = reinterpret_cast<const V *>(JAC ? a.z : a.r);
+            for (uint32_t iv = blockIdx.x * blockDim.x + threadIdx.x; iv < a.nvec; iv += gridDim.x * blockDim.x) {
+                const V zv = __ldcg(zs + iv), qv = __ldcg(reinterpret_cast<const V *>(pold) + iv);
+                V pv;
+#pragma unroll
+                for (int q = 0; q < O::W; ++q) O::set(pv, q, fma(bt, O::get(qv, q), O::get(zv, q)));
+                reinterpret_cast<V *>(pnew)[iv] = pv;
+            }
+            if (!grid_barrier(a.bar, a.err, target)) return;
+            dacc = Op::template run<true, false, true>(d, tab, smem_raw + tab.bytes, pnew, nullptr, nullptr, a.Ap,
+                                                       T(0));
+        }
         const double bs = block_sum(dacc, sh);
         if (threadIdx.x == 0) a.partials[blockIdx.x] = bs;
         if (!grid_barrier(a.bar, a.err, target)) return;
