@@ -1343,29 +1343,39 @@ __global__ void k_axpby(uint64_t n, double alpha, const double *x, double beta, 
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
         y[i] = alpha * x[i] + beta * y[i];
 }
-// out[i] = <V_i, w> for i < k; V rows of length n with stride ld.  Eight
-// rows per pass over w (w is read k/8 times, each V row once), one partial
-// per block and row, summed in a fixed order by the last block.
+// out[i] = <V_i, w> for i < k; V rows of length n with stride ld.  Each V
+// row is read once, one partial per block and row, summed in a fixed order
+// by the last block.
 __global__ void k_multidot(uint64_t n, int k, const double *V, uint64_t ld, const double *w, double *partials,
                            unsigned int *counter, double *out) {
-    __shared__ double sh[32];
+    // launched with 256 threads (kMultidotWarps warps); k <= kMaxRestart + 2
+    constexpr int kMultidotWarps = 8;
+    __shared__ double red[kMultidotWarps][kMaxRestart + 2];
     __shared__ bool am_last;
-    const uint64_t tid = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x, nth = (uint64_t)gridDim.x * blockDim.x;
-    for (int i0 = 0; i0 < k; i0 += 8) {
-        const int m = k - i0 < 8 ? k - i0 : 8;
-        double acc[8] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
-        for (uint64_t t = tid; t < n; t += nth) {
-            const double wt = w[t];
+    const unsigned int lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    // block b takes the contiguous range [b0, b1) of every vector, so that
+    // each V_i streams in long runs and the block's part of w, read again
+    // for every i, stays in L1; one warp-shuffle sum per (warp, vector) and
+    // a single block barrier for all k (the grid-stride form with eight
+    // vectors per pass and a block reduction per vector ran at about half
+    // the copy rate)
+    const uint64_t chunk = (n + gridDim.x - 1) / gridDim.x;
+    const uint64_t b0 = min(n, static_cast<uint64_t>(blockIdx.x) * chunk), b1 = min(n, b0 + chunk);
+    for (int i = 0; i < k; ++i) {
+        const double *Vi = V + static_cast<uint64_t>(i) * ld;
+        double acc = 0.0;
+#pragma unroll 4
+        for (uint64_t t = b0 + threadIdx.x; t < b1; t += blockDim.x) acc = fma(Vi[t], __ldg(w + t), acc);
 #pragma unroll
-            for (int ii = 0; ii < 8; ++ii)
-                if (ii < m) acc[ii] += V[(uint64_t)(i0 + ii) * ld + t] * wt;
-        }
+        for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) red[warp][i] = acc;
+    }
+    __syncthreads();
+    for (int i = static_cast<int>(threadIdx.x); i < k; i += blockDim.x) {
+        double sum = 0.0;
 #pragma unroll
-        for (int ii = 0; ii < 8; ++ii) {
-            if (ii >= m) break;
-            const double sum = block_sum(acc[ii], sh);
-            if (threadIdx.x == 0) partials[(uint64_t)(i0 + ii) * gridDim.x + blockIdx.x] = sum;
-        }
+        for (int q = 0; q < kMultidotWarps; ++q) sum += red[q][i];
+        partials[static_cast<uint64_t>(i) * gridDim.x + blockIdx.x] = sum;
     }
     __threadfence();
     __syncthreads();
@@ -1373,12 +1383,15 @@ __global__ void k_multidot(uint64_t n, int k, const double *V, uint64_t ld, cons
     __syncthreads();
     if (!am_last) return;
     __threadfence();
-    for (int i = 0; i < k; ++i) {
+    // the last block sums the k partial columns, one warp per column (in a
+    // fixed order: lanes stride the blocks, then a shuffle tree)
+    for (int i = static_cast<int>(warp); i < k; i += kMultidotWarps) {
         double acc = 0.0;
-        for (unsigned int b = threadIdx.x; b < gridDim.x; b += blockDim.x)
-            acc += __ldcg(partials + (uint64_t)i * gridDim.x + b);
-        double sum = block_sum(acc, sh);
-        if (threadIdx.x == 0) out[i] = sum;
+#pragma unroll 4
+        for (unsigned int b = lane; b < gridDim.x; b += 32) acc += __ldcg(partials + (uint64_t)i * gridDim.x + b);
+#pragma unroll
+        for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+        if (lane == 0) out[i] = acc;
     }
     if (threadIdx.x == 0) *counter = 0u;
 }
