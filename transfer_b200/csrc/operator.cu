@@ -1029,10 +1029,14 @@ __global__ void __launch_bounds__(kBlock) k_lhs_diag(const OpData<T> d, const T 
 // Bounded grid barrier for a co-resident (cooperatively launched) grid.
 // *count is a monotone arrival counter that the host zeroes before every
 // launch; barrier number n of the launch completes when it reaches
-// n * gridDim.x (`target` carries that per block).  One fire-and-forget add
-// per block and a poll: the critical path is one fence, one add and one
-// load.  Gives up after kBarrierPolls polls, or as soon as another block
-// has given up: sets *err and returns false.
+// n * gridDim.x (`target` carries that per block).  After the block barrier
+// thread 0 arrives with a release reduction (publishing the block's writes)
+// and polls with acquire loads (making the other blocks' writes visible),
+// then the block barrier again.  Measured on a B200 (148 blocks of 768
+// threads, 20,000 barriers in one launch): 1.37 us per barrier, against
+// 1.56 us for a fence + relaxed add and volatile polls with a 32 ns sleep.
+// Gives up after max_polls polls, or as soon as another block has given up:
+// sets *err and returns false.
 constexpr unsigned int kBarrierPolls = 1u << 24;
 __device__ __forceinline__ bool grid_barrier(unsigned int *count, int *err, unsigned int &target,
                                              unsigned int max_polls = kBarrierPolls) {
@@ -1041,18 +1045,18 @@ __device__ __forceinline__ bool grid_barrier(unsigned int *count, int *err, unsi
     target += gridDim.x;
     if (threadIdx.x == 0) {
         ok = 1;
-        __threadfence();  // this block's writes before its arrival
-        atomicAdd(count, 1u);
+        asm volatile("red.release.gpu.global.add.u32 [%0], 1;" ::"l"(count) : "memory");
         unsigned int polls = 0;
-        while (*reinterpret_cast<volatile unsigned int *>(count) < target) {
+        for (;;) {
+            unsigned int v;
+            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(count) : "memory");
+            if (v >= target) break;
             if (++polls > max_polls || *reinterpret_cast<volatile int *>(err)) {
                 atomicExch(err, 1);
                 ok = 0;
                 break;
             }
-            __nanosleep(32);
         }
-        __threadfence();  // the other blocks' writes before this block's reads
     }
     __syncthreads();
     return ok != 0;
