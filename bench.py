@@ -487,6 +487,9 @@ def stellar_section(local, peak):
                                   "algorithmic_bytes": mom_bytes}
     S.set_moments_kernel(tr._lib.TR_MOMENTS_TCGEN05)
     sols = {}
+    # warm-up: one Krylov step allocates the GMRES basis (41 vectors of
+    # 89 MB), which the timed solves then share
+    S.solve(raise_on_error=False, mode=tr.TR_MODE_FP64, tol=SWEEP_TOL, restart=40, max_iter=1)
     for name, mode in (("fp64", tr.TR_MODE_FP64), ("mixed", tr.TR_MODE_MIXED)):
         torch.cuda.synchronize()
         e0.record()
