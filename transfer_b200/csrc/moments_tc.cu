@@ -30,8 +30,10 @@
 //             A operand of the third product (A from tensor memory), in
 //             kLoSlots slots of its own, each freed when its products finish;
 //   D         per tile (double-buffered) kAccGroups 128 x 32 FP32 accumulators
-//             of a [w_hi | w_lo], the 8-ordinate steps dealt to them in turn,
-//             and one 128 x 16 accumulator of a_lo w_hi, in tensor memory.  The
+//             of a [w_hi | w_lo], the 8-ordinate steps dealt to them in turn
+//             (with two issuers, issuer i's steps to accumulators 2i and
+//             2i + 1), and a 128 x 16 accumulator of a_lo w_hi per issuer,
+//             in tensor memory.  The
 //             tensor core's FP32 accumulation truncates, so each accumulation
 //             into a running sum loses about half an ulp the same way; dealing
 //             the steps over four accumulators and summing them in FP64 cuts
