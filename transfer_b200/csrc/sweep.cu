@@ -871,6 +871,57 @@ __global__ void k_moments_simt(uint32_t nT, uint32_t nq, const double *W, const 
     }
 }
 
+// All 16 moments (l <= 3) of FP64 psi, streamed like the scalar flux: each
+// thread owns two consecutive vertex values (rows 2 t, 2 t + 1 of the 4 nT;
+// a warp reads 512 contiguous bytes of each ordinate row) and keeps their
+// 16 moment sums, 32 FP64 registers, so that more warps stay resident than
+// with the 64 sums of a whole cell; the weights of 32 ordinates at a time
+// sit in shared memory.  Same FP64 sums in the same ordinate order as
+// k_moments_simt<double, 16>.
+constexpr int kMom64Chunk = 32;
+__global__ void __launch_bounds__(256) k_moments_f64_16(uint32_t nT, uint32_t nq, const double *W, const double *psi,
+                                                         double *mom) {
+    __shared__ __align__(16) double ws[kMom64Chunk][16];
+    const uint64_t M2 = 2ull * nT;  // row pairs
+    const uint64_t stride = 4ull * nT;
+    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < M2; base += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t r2 = base + threadIdx.x;
+        const bool live = r2 < M2;
+        double acc[16][2];
+#pragma unroll
+        for (int m = 0; m < 16; ++m) acc[m][0] = acc[m][1] = 0.0;
+        for (uint32_t q0 = 0; q0 < nq; q0 += kMom64Chunk) {
+            const uint32_t nc = min(static_cast<uint32_t>(kMom64Chunk), nq - q0);
+            __syncthreads();  // the previous chunk's weights have been read
+            for (uint32_t i = threadIdx.x; i < kMom64Chunk * 16; i += blockDim.x) {
+                const uint32_t qq = i >> 4, m = i & 15u;
+                ws[qq][m] = qq < nc ? __ldg(W + (size_t)m * nq + q0 + qq) : 0.0;
+            }
+            __syncthreads();
+            if (live) {
+                const double2 *pr = reinterpret_cast<const double2 *>(psi + (size_t)q0 * stride) + r2;
+                for (uint32_t qq = 0; qq < nc; ++qq) {
+                    const double2 v = pr[(size_t)qq * (stride / 2)];
+                    const double2 *wq = reinterpret_cast<const double2 *>(ws[qq]);
+#pragma unroll
+                    for (int h = 0; h < 8; ++h) {
+                        const double2 w2 = wq[h];
+                        acc[2 * h][0] += w2.x * v.x;
+                        acc[2 * h][1] += w2.x * v.y;
+                        acc[2 * h + 1][0] += w2.y * v.x;
+                        acc[2 * h + 1][1] += w2.y * v.y;
+                    }
+                }
+            }
+        }
+        if (live) {
+#pragma unroll
+            for (int m = 0; m < 16; ++m)
+                reinterpret_cast<double2 *>(mom + (size_t)m * stride)[r2] = make_double2(acc[m][0], acc[m][1]);
+        }
+    }
+}
+
 // Moments of FP32 psi on the tensor cores in split TF32 (3 products, FP32
 // accumulation): D[r][n] = sum_q A[r][q] W[n][q] with A[r][q] = psi[q][r]
 // (r = 4c + j over the M = 4 nT vertex values), N = 16 harmonics (l <= 3).
@@ -2949,7 +3000,8 @@ tr_status tr_sweep_moments(tr_sweep *s, int nmom, double *mom) {
             if (nb == 1) k_moments_simt<double, 1><<<gr, 128, 0, s->stream>>>(s->nT, s->nq, s->Wm, s->psi64, out);
             else if (nb == 4) k_moments_simt<double, 4><<<gr, 128, 0, s->stream>>>(s->nT, s->nq, s->Wm, s->psi64, out);
             else if (nb == 9) k_moments_simt<double, 9><<<gr, 128, 0, s->stream>>>(s->nT, s->nq, s->Wm, s->psi64, out);
-            else k_moments_simt<double, 16><<<gr, 128, 0, s->stream>>>(s->nT, s->nq, s->Wm, s->psi64, out);
+            else k_moments_f64_16<<<grid_for(s, 2ull * s->nT, 256), 256, 0, s->stream>>>(s->nT, s->nq, s->Wm,
+                                                                                        s->psi64, out);
             e = cudaGetLastError();
             ++s->launches;
         } else if (e == cudaSuccess) {
